@@ -1,0 +1,199 @@
+/*
+ * wp_api.h -- C ABI of the B200 (sm_100a) WaveletPotentials projection-and-recovery path.
+ *
+ * Every entry point takes plain pointers and sizes.  Field pointers are DEVICE pointers in the
+ * reference layout (Utils.h:46-47: y fastest, element (x,y,z) of extents (DX,DY,DZ) at
+ * y + x*DY + z*DX*DY) and MAC shapes (TestLocalProjection.cpp:536-542):
+ *   xv (nx+1,ny,nz)  yv (nx,ny+1,nz)  zv (nx,ny,nz+1)  cells (nx,ny,nz)
+ *   qx (nx,ny+1,nz+1) qy (nx+1,ny,nz+1) qz (nx+1,ny+1,nz); 2D: xv (nx+1,ny) yv (nx,ny+1) qz (nx+1,ny+1)
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).  Calls are
+ * asynchronous on that stream unless they return a host scalar.  Errors come back as wp_status;
+ * nothing calls exit().  wp_last_error() gives the message of the last failure on this thread.
+ * Handles are independent: one handle per stream/thread, no process-wide mutable state.
+ *
+ * The reference exposes no C ABI (cuWHHD_Export.h only defines an empty CUWHHD_API macro); each
+ * declaration below names the reference C++ entry point it replaces.
+ */
+#ifndef WP_API_H
+#define WP_API_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define CUWHHD_API __declspec(dllexport)
+#else
+#define CUWHHD_API __attribute__((visibility("default")))
+#endif
+
+typedef enum wp_status {
+    WP_OK = 0,
+    WP_ERR_INVALID_ARG = 1,   /* bad shape, null pointer, unknown enum */
+    WP_ERR_UNSUPPORTED = 2,   /* valid request outside the implemented path (e.g. domain bc 'd') */
+    WP_ERR_CUDA = 3,          /* a CUDA runtime call or launch failed */
+    WP_ERR_WORKSPACE = 4,     /* caller workspace too small */
+    WP_ERR_NOT_CONVERGED = 5, /* solve hit its cycle cap before the tolerance */
+    WP_ERR_NONFINITE = 6      /* NaN/Inf met in the input or residual */
+} wp_status;
+
+/* wavelet ids: same numeric values as the reference enum WaveletType (WaveletTypes.h:7-27) */
+#define WP_CDF4_6 7
+#define WP_CDF3_7 11
+
+/* precision modes of the multigrid solve */
+#define WP_PREC_FP32 0  /* FP32 V-cycles, FP32 iterate; residual norms accumulated in FP64 */
+#define WP_PREC_MIXED 1 /* FP32 V-cycles inside FP64 iterative refinement (FP64 defect + iterate) */
+#define WP_PREC_FP64 2  /* FP64 V-cycles throughout (the reference's default DTYPE) */
+
+CUWHHD_API const char* wp_last_error(void);
+CUWHHD_API int wp_version(void);
+
+/* Instrumentation (no reference counterpart): number of kernels this library has launched since
+   the last reset, and optional per-kernel-class timing with CUDA events on the launching stream.
+   wp_profile_collect() synchronizes the device and returns the number of kernel classes;
+   wp_profile_entry() reads one (name, launches, total ms, algorithmic bytes moved). */
+CUWHHD_API void wp_profile_enable(int on);
+CUWHHD_API void wp_profile_reset(void);
+CUWHHD_API long long wp_launch_count(void);
+CUWHHD_API int wp_profile_collect(void);
+CUWHHD_API int wp_profile_entry(int i, char* name, int name_cap, long long* launches, double* ms, double* bytes);
+
+/* ------------------------------------------------------------------ 1D transforms ------- */
+/* Full-depth multilevel 1D lifting transform (CDF3.7 / CDF4.6, bc 'n' | 'd' | 'z') along
+   direction 'x' | 'y' | 'z' of a (dim_x, dim_y, dim_z) array; dst may equal src.
+   Replaces CuWHHDForward::Solve1D(dst, src, int3 dim, level, direction, bc, type, is_forward)
+   (cuWHHDForward.cuh:20-23, cuWHHDForward.cu:1122-1153). */
+CUWHHD_API wp_status wp_dwt1d(float* dst, const float* src, int dim_x, int dim_y, int dim_z, int levels,
+                              char direction, char bc, int wavelet, int forward, void* stream);
+CUWHHD_API wp_status wp_dwt1d_f64(double* dst, const double* src, int dim_x, int dim_y, int dim_z, int levels,
+                                  char direction, char bc, int wavelet, int forward, void* stream);
+
+/* Diagonal band of the inner-product table ||B_i||^2 of the synthesis basis, computed on the GPU
+   in FP64 and copied to host `out[dim]` (synchronous).  Replaces CuGetInnerProduct::GenerateIp
+   (cuGetInnerProduct.cu:92-126; only band 0 is read by the projection kernels). */
+CUWHHD_API wp_status wp_ip_diag(double* out, int dim, int wavelet, char bc);
+
+/* ---------------------------------------------------------- potential recovery 3D ------- */
+typedef struct wp_recover3d wp_recover3d;
+/* Replaces CuWaveletPotentialRecover3D(int3 dim, DTYPE3 dx, char bc, WaveletType curl,
+   WaveletType div) (cuWaveletPotentialRecover3D.cuh:11-12, .cu:6-12).  nx,ny,nz powers of two
+   >= 4; bc 'n' (zero-normal-flux walls).  Allocates its own temporaries on the current device. */
+CUWHHD_API wp_status wp_recover3d_create(wp_recover3d** h, int nx, int ny, int nz, double dx, double dy, double dz,
+                                         char bc, int curl_wavelet, int div_wavelet);
+/* Replaces CuWaveletPotentialRecover3D::Solve(qx,qy,qz,xv,yv,zv) (cuWaveletPotentialRecover3D.cu:16-61):
+   forward analysis, local projection, inverse synthesis.  xv..zv are read only. */
+CUWHHD_API wp_status wp_recover3d_run(wp_recover3d* h, float* qx, float* qy, float* qz, const float* xv,
+                                      const float* yv, const float* zv, void* stream);
+/* Replaces CuDivLocalProject3D::ProjectLocal_q_ccc(qx,qy,qz,xv_lwt,yv_lwt,zv_lwt,levels)
+   (cuDivLocalProject3D.cu:5273-5308): coefficient-space projection only. */
+CUWHHD_API wp_status wp_recover3d_project(wp_recover3d* h, float* qx, float* qy, float* qz, const float* xv_lwt,
+                                          const float* yv_lwt, const float* zv_lwt, void* stream);
+CUWHHD_API wp_status wp_recover3d_destroy(wp_recover3d* h);
+
+/* ---------------------------------------------------------- potential recovery 2D ------- */
+typedef struct wp_recover2d wp_recover2d;
+/* Replaces CuWaveletPotentialRecover2D(int2 dim, DTYPE2 dx, char bc, curl, div)
+   (cuWaveletPotentialRecover2D.cuh:11-12). */
+CUWHHD_API wp_status wp_recover2d_create(wp_recover2d** h, int nx, int ny, double dx, double dy, char bc,
+                                         int curl_wavelet, int div_wavelet);
+/* Replaces CuWaveletPotentialRecover2D::Solve(qz, xv, yv) (cuWaveletPotentialRecover2D.cu:16-36). */
+CUWHHD_API wp_status wp_recover2d_run(wp_recover2d* h, float* qz, const float* xv, const float* yv, void* stream);
+/* Replaces CuDivLocalProject::ProjectSingle(qz, xv_lwt, yv_lwt) (cuDivLocalProject.cu:2162-2198). */
+CUWHHD_API wp_status wp_recover2d_project(wp_recover2d* h, float* qz, const float* xv_lwt, const float* yv_lwt,
+                                          void* stream);
+CUWHHD_API wp_status wp_recover2d_destroy(wp_recover2d* h);
+
+/* ---------------------------------------------------- fractional multigrid 3D / 2D ------- */
+/* coarse-to-fine transfer of the V-cycle */
+#define WP_PROLONG_CONSTANT 0  /* the reference's piecewise-constant prolongation (cuProlongate3D.cu:594-617) */
+#define WP_PROLONG_TRILINEAR 1 /* cell-centred trilinear: h-independent convergence for V(2,2), omega 2/3 */
+
+typedef struct wp_mg_params {
+    int max_cycles;   /* cap on V-cycles (or refinement steps) */
+    int nu1, nu2;     /* pre / post weighted-Jacobi sweeps */
+    double omega;     /* Jacobi weight (reference default 0.8, cuMultigridFrac3D.cuh:17) */
+    double rel_tol;   /* stop when ||f - A p|| / ||f|| <= rel_tol; <= 0 runs exactly max_cycles */
+    int precision;    /* WP_PREC_FP32 | WP_PREC_MIXED | WP_PREC_FP64 */
+    int prolongation; /* WP_PROLONG_CONSTANT | WP_PROLONG_TRILINEAR */
+} wp_mg_params;
+
+typedef struct wp_mg_report {
+    int cycles;             /* V-cycles executed */
+    double rel_residual;    /* final ||f - A p|| / ||f|| (FP64) */
+    double history[64];     /* per-cycle relative residual (first min(cycles,64)) */
+} wp_mg_report;
+
+typedef struct wp_mgfrac3d wp_mgfrac3d;
+/* Replaces CuMultigridFrac3D(Ax, Ay, Az, int3 dim, DTYPE3 dx, char bc) (cuMultigridFrac3D.cuh:15,
+   .cu:9-134): copies the face fractions and builds the coarse hierarchy (ceil halving until the
+   smallest extent is 1).  bc 'n' only. */
+CUWHHD_API wp_status wp_mgfrac3d_create(wp_mgfrac3d** h, const float* ax, const float* ay, const float* az, int nx,
+                                        int ny, int nz, double dx, double dy, double dz, char bc, void* stream);
+/* Replaces CuMultigridFrac3D::Solve(dst, pre_v, f, n_iters, nu1, nu2, weight) (cuMultigridFrac3D.cu:249-265):
+   exactly n_iters V-cycles in FP32.  pre_v may be NULL (zero start) or equal dst. */
+CUWHHD_API wp_status wp_mgfrac3d_solve(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f, int n_iters,
+                                       int nu1, int nu2, double weight, void* stream);
+/* Tolerance-driven solve with a precision mode; synchronous (reads residual norms on the host).
+   Solves the compatible problem A p = f - m, m = mean of f over the active cells (diag > 0), so the
+   FP32 rounding of f does not floor the residual; the residual reported is ||f - m - A p|| / ||f||.
+   Returns WP_ERR_NOT_CONVERGED (dst still holds the last iterate) when max_cycles is reached. */
+CUWHHD_API wp_status wp_mgfrac3d_solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f,
+                                           const wp_mg_params* params, wp_mg_report* report, void* stream);
+/* Replaces CuMultigridFrac3D::GetResdualError(dst, f) (cuMultigridFrac3D.cu:329-333): returns
+   ||f - A v||_2 / ||f||_2 with FP64 accumulation (synchronous). */
+CUWHHD_API wp_status wp_mgfrac3d_residual(wp_mgfrac3d* h, const float* v, const float* f, double* rel_residual,
+                                          void* stream);
+/* Copies the FP64 iterate of the last WP_PREC_MIXED / WP_PREC_FP64 solve into dst (device, cells);
+   WP_ERR_INVALID_ARG if the handle has not run such a solve.  No reference counterpart (the
+   reference iterate is DTYPE). */
+CUWHHD_API wp_status wp_mgfrac3d_iterate64(wp_mgfrac3d* h, double* dst, void* stream);
+CUWHHD_API wp_status wp_mgfrac3d_destroy(wp_mgfrac3d* h);
+
+typedef struct wp_mgfrac2d wp_mgfrac2d;
+/* Replaces CuMultigridFrac2D(Ax, Ay, int2 dim, DTYPE2 dx, char bc) (cuMultigridFrac2D.cu:28-111). */
+CUWHHD_API wp_status wp_mgfrac2d_create(wp_mgfrac2d** h, const float* ax, const float* ay, int nx, int ny, double dx,
+                                        double dy, char bc, void* stream);
+/* Replaces CuMultigridFrac2D::Solve (cuMultigridFrac2D.cu:151-166). */
+CUWHHD_API wp_status wp_mgfrac2d_solve(wp_mgfrac2d* h, float* dst, const float* pre_v, const float* f, int n_iters,
+                                       int nu1, int nu2, double weight, void* stream);
+CUWHHD_API wp_status wp_mgfrac2d_solve_tol(wp_mgfrac2d* h, float* dst, const float* pre_v, const float* f,
+                                           const wp_mg_params* params, wp_mg_report* report, void* stream);
+/* Replaces CuWeightedJacobi::GetFracRhs(v, f, Ax, Ay, dim, dx, dy, dx_e, bc) (cuWeightedJacobi.cu:789-811). */
+CUWHHD_API wp_status wp_mgfrac2d_residual(wp_mgfrac2d* h, const float* v, const float* f, double* rel_residual,
+                                          void* stream);
+CUWHHD_API wp_status wp_mgfrac2d_destroy(wp_mgfrac2d* h);
+
+/* ------------------------------------------------------------- field operators ------- */
+/* b = -div(a u) (CuConvergence::GetB_3d_frac_vel, cuConvergence.cu:427-447).  ax, ay, az all NULL
+   means fully open faces (the divergence of an already fraction-weighted field). */
+CUWHHD_API wp_status wp_divergence_frac3d(float* b, const float* xv, const float* yv, const float* zv, const float* ax,
+                                          const float* ay, const float* az, int nx, int ny, int nz, double dx,
+                                          double dy, double dz, void* stream);
+CUWHHD_API wp_status wp_divergence_frac2d(float* b, const float* xv, const float* yv, const float* ax, const float* ay,
+                                          int nx, int ny, double dx, double dy, void* stream);
+/* u <- (u - grad p) [* a]: CuGradient::Gradient3D_Frac_P (cuGradient.cu:2520-2540) followed by
+   CudaMatAdd(-1) and CudaMatMul(a) (TestLocalProjection.cpp:672-680), fused. */
+CUWHHD_API wp_status wp_grad_subtract_frac3d(float* xv, float* yv, float* zv, const float* p, const float* ax,
+                                             const float* ay, const float* az, int nx, int ny, int nz, double dx,
+                                             double dy, double dz, int multiply_frac, void* stream);
+CUWHHD_API wp_status wp_grad_subtract_frac2d(float* xv, float* yv, const float* p, const float* ax, const float* ay,
+                                             int nx, int ny, double dx, double dy, int multiply_frac, void* stream);
+/* max |x| over n elements, FP64 result to host (CudaFindMaxValue, cudaMath.cu:1269-1280, without
+   copying the array to the host).  Synchronous. */
+CUWHHD_API wp_status wp_max_abs(const float* x, size_t n, double* out, void* stream);
+
+/* Signed distance (positive in fluid) to a union of spheres at cell centres (cuInitLsSphere,
+   cuSolidLevelSet3D.cu:11-27); centers/radii are HOST arrays (3*count, count). */
+CUWHHD_API wp_status wp_sdf_spheres3d(float* sdf, int nx, int ny, int nz, double dx, const double* centers,
+                                      const double* radii, int count, void* stream);
+/* Face open fractions from a level set (cuGetAx/Ay/Az, cuSolidLevelSet3D.cu:36-90). */
+CUWHHD_API wp_status wp_fractions3d(float* ax, float* ay, float* az, const float* sdf, int nx, int ny, int nz,
+                                    double dx, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,298 @@
+"""FP64 CPU oracle of the WaveletPotentials projection-and-recovery path (ctypes wrapper).
+
+TEST INFRASTRUCTURE ONLY.  tests/, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` /
+``--impl reference`` legs of ``bench.py`` use it as the checker; the product package never
+imports it.  The arithmetic lives in ``wp_oracle.c`` (a plain-C restatement of the reference
+algorithm, each routine citing the reference file:line it follows).
+
+Arrays use the reference layout (``Utils.h:46-47``): a 3D array with extents (DX, DY, DZ) is a
+numpy array of shape (DZ, DX, DY), so y is the fastest index; 2D arrays are (DX, DY).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwp_oracle.so")
+CDF4_6 = 7
+CDF3_7 = 11
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile wp_oracle.c into libwp_oracle.so (gcc, OpenMP)."""
+    src = os.path.join(HERE, "wp_oracle.c")
+    if not force and os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= os.path.getmtime(src):
+        return LIB_PATH
+    cmd = ["gcc", "-O2", "-fopenmp", "-shared", "-fPIC", "-std=gnu11", "-o", LIB_PATH, src, "-lm"]
+    subprocess.check_call(cmd)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        d = ctypes.c_double
+        i = ctypes.c_int
+        p = ctypes.c_void_p
+        c = ctypes.c_char
+        sig = {
+            "or_dwt_line": (i, [p, i, i, i, c, i]),
+            "or_dwt_axis": (i, [p, i, i, i, i, c, i, c, i]),
+            "or_ip_diag": (i, [p, i, i, c]),
+            "or_project3d": (i, [p, p, p, p, p, p, i, i, i, d, d, d]),
+            "or_project2d": (i, [p, p, p, i, i, d, d]),
+            "or_recover3d": (i, [p, p, p, p, p, p, i, i, i, d, d, d, c]),
+            "or_recover2d": (i, [p, p, p, i, i, d, d, c]),
+            "or_curl3d": (None, [p, p, p, p, p, p, i, i, i, d, d, d]),
+            "or_curl2d": (None, [p, p, p, i, i, d, d]),
+            "or_divergence3d": (None, [p, p, p, p, p, p, p, i, i, i, d, d, d]),
+            "or_divergence2d": (None, [p, p, p, p, p, i, i, d, d]),
+            "or_grad_subtract3d": (None, [p, p, p, p, p, p, p, i, i, i, d, d, d, i]),
+            "or_grad_subtract2d": (None, [p, p, p, p, p, i, i, d, d, i]),
+            "or_sdf_spheres3d": (None, [p, i, i, i, d, p, p, i]),
+            "or_sdf_boxes3d": (None, [p, i, i, i, d, p, p, i]),
+            "or_fractions3d": (None, [p, p, p, p, i, i, i, d]),
+            "or_fractions2d": (None, [p, p, p, i, i, d]),
+            "or_mgfrac3d_solve": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, i, p]),
+            "or_mgfrac2d_solve": (i, [p, p, p, p, p, i, i, d, d, i, i, i, d, i, p]),
+            "or_frac_residual3d": (d, [p, p, p, p, p, p, i, i, i, d, d, d]),
+            "or_frac_residual2d": (d, [p, p, p, p, p, i, i, d, d]),
+            "or_dst3d_poisson": (None, [p, p, i, i, i, d, d, d]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    return _lib
+
+
+def _p(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], (a.dtype, a.flags)
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"oracle {what} failed with code {rc}")
+
+
+# ---------------------------------------------------------------- transforms
+def dwt_line(line, levels: int, wavelet: int, bc: str, forward: bool) -> np.ndarray:
+    out = _f64(line).copy()
+    _check(lib().or_dwt_line(_p(out), out.size, levels, wavelet, bc.encode(), int(forward)), "dwt_line")
+    return out
+
+
+def dwt_axis(arr, levels: int, axis: str, wavelet: int, bc: str, forward: bool) -> np.ndarray:
+    """arr: 3D array of shape (DZ, DX, DY) or 2D (DX, DY)."""
+    a = _f64(arr).copy()
+    shp = a.shape if a.ndim == 3 else (1,) + a.shape
+    dz, dx, dy = shp
+    _check(lib().or_dwt_axis(_p(a), dx, dy, dz, levels, axis.encode(), wavelet, bc.encode(), int(forward)),
+           "dwt_axis")
+    return a
+
+
+def ip_diag(dim: int, wavelet: int, bc: str) -> np.ndarray:
+    out = np.zeros(dim)
+    _check(lib().or_ip_diag(_p(out), dim, wavelet, bc.encode()), "ip_diag")
+    return out
+
+
+# ------------------------------------------------------------- shapes helpers
+def mac_shapes3d(nx, ny, nz):
+    return {"xv": (nz, nx + 1, ny), "yv": (nz, nx, ny + 1), "zv": (nz + 1, nx, ny),
+            "qx": (nz + 1, nx, ny + 1), "qy": (nz + 1, nx + 1, ny), "qz": (nz, nx + 1, ny + 1),
+            "p": (nz, nx, ny)}
+
+
+def mac_shapes2d(nx, ny):
+    return {"xv": (nx + 1, ny), "yv": (nx, ny + 1), "qz": (nx + 1, ny + 1), "p": (nx, ny)}
+
+
+# ----------------------------------------------------------------- projection
+def project3d(xv, yv, zv, n, d):
+    nx, ny, nz = n
+    s = mac_shapes3d(nx, ny, nz)
+    qx, qy, qz = (np.zeros(s[k]) for k in ("qx", "qy", "qz"))
+    _check(lib().or_project3d(_p(qx), _p(qy), _p(qz), _p(_f64(xv)), _p(_f64(yv)), _p(_f64(zv)), nx, ny, nz, *d),
+           "project3d")
+    return qx, qy, qz
+
+
+def project2d(xv, yv, n, d):
+    nx, ny = n
+    qz = np.zeros((nx + 1, ny + 1))
+    _check(lib().or_project2d(_p(qz), _p(_f64(xv)), _p(_f64(yv)), nx, ny, *d), "project2d")
+    return qz
+
+
+def recover3d(xv, yv, zv, n, d, bc="n"):
+    nx, ny, nz = n
+    s = mac_shapes3d(nx, ny, nz)
+    qx, qy, qz = (np.zeros(s[k]) for k in ("qx", "qy", "qz"))
+    _check(lib().or_recover3d(_p(qx), _p(qy), _p(qz), _p(_f64(xv)), _p(_f64(yv)), _p(_f64(zv)), nx, ny, nz, *d,
+                              bc.encode()), "recover3d")
+    return qx, qy, qz
+
+
+def recover2d(xv, yv, n, d, bc="n"):
+    nx, ny = n
+    qz = np.zeros((nx + 1, ny + 1))
+    _check(lib().or_recover2d(_p(qz), _p(_f64(xv)), _p(_f64(yv)), nx, ny, *d, bc.encode()), "recover2d")
+    return qz
+
+
+def curl3d(qx, qy, qz, n, d):
+    nx, ny, nz = n
+    s = mac_shapes3d(nx, ny, nz)
+    xv, yv, zv = (np.zeros(s[k]) for k in ("xv", "yv", "zv"))
+    lib().or_curl3d(_p(xv), _p(yv), _p(zv), _p(_f64(qx)), _p(_f64(qy)), _p(_f64(qz)), nx, ny, nz, *d)
+    return xv, yv, zv
+
+
+def curl2d(qz, n, d):
+    nx, ny = n
+    xv, yv = np.zeros((nx + 1, ny)), np.zeros((nx, ny + 1))
+    lib().or_curl2d(_p(xv), _p(yv), _p(_f64(qz)), nx, ny, *d)
+    return xv, yv
+
+
+# -------------------------------------------------------- divergence / gradient
+def divergence3d(xv, yv, zv, ax, ay, az, n, d):
+    nx, ny, nz = n
+    b = np.zeros((nz, nx, ny))
+    lib().or_divergence3d(_p(b), _p(_f64(xv)), _p(_f64(yv)), _p(_f64(zv)), _p(_f64(ax)), _p(_f64(ay)),
+                          _p(_f64(az)), nx, ny, nz, *d)
+    return b
+
+
+def divergence2d(xv, yv, ax, ay, n, d):
+    nx, ny = n
+    b = np.zeros((nx, ny))
+    lib().or_divergence2d(_p(b), _p(_f64(xv)), _p(_f64(yv)), _p(_f64(ax)), _p(_f64(ay)), nx, ny, *d)
+    return b
+
+
+def grad_subtract3d(xv, yv, zv, p, ax, ay, az, n, d, multiply_frac=True):
+    nx, ny, nz = n
+    xo, yo, zo = _f64(xv).copy(), _f64(yv).copy(), _f64(zv).copy()
+    lib().or_grad_subtract3d(_p(xo), _p(yo), _p(zo), _p(_f64(p)), _p(_f64(ax)), _p(_f64(ay)), _p(_f64(az)),
+                             nx, ny, nz, *d, int(multiply_frac))
+    return xo, yo, zo
+
+
+def grad_subtract2d(xv, yv, p, ax, ay, n, d, multiply_frac=True):
+    nx, ny = n
+    xo, yo = _f64(xv).copy(), _f64(yv).copy()
+    lib().or_grad_subtract2d(_p(xo), _p(yo), _p(_f64(p)), _p(_f64(ax)), _p(_f64(ay)), nx, ny, *d,
+                             int(multiply_frac))
+    return xo, yo
+
+
+# --------------------------------------------------------------------- solids
+def sdf_spheres3d(n, dx, centers, radii):
+    nx, ny, nz = n
+    sdf = np.zeros((nz, nx, ny))
+    c = _f64(np.reshape(centers, (-1, 3)))
+    r = _f64(np.reshape(radii, (-1,)))
+    lib().or_sdf_spheres3d(_p(sdf), nx, ny, nz, dx, _p(c), _p(r), r.size)
+    return sdf
+
+
+def sdf_boxes3d(sdf, n, dx, lo, hi):
+    nx, ny, nz = n
+    out = _f64(sdf).copy()
+    lo_, hi_ = _f64(np.reshape(lo, (-1, 3))), _f64(np.reshape(hi, (-1, 3)))
+    lib().or_sdf_boxes3d(_p(out), nx, ny, nz, dx, _p(lo_), _p(hi_), lo_.shape[0])
+    return out
+
+
+def fractions3d(sdf, n, dx):
+    nx, ny, nz = n
+    s = mac_shapes3d(nx, ny, nz)
+    ax, ay, az = (np.zeros(s[k]) for k in ("xv", "yv", "zv"))
+    lib().or_fractions3d(_p(ax), _p(ay), _p(az), _p(_f64(sdf)), nx, ny, nz, dx)
+    return ax, ay, az
+
+
+def fractions2d(sdf, n, dx):
+    nx, ny = n
+    ax, ay = np.zeros((nx + 1, ny)), np.zeros((nx, ny + 1))
+    lib().or_fractions2d(_p(ax), _p(ay), _p(_f64(sdf)), nx, ny, dx)
+    return ax, ay
+
+
+# ------------------------------------------------------------------ multigrid
+PROLONG_CONSTANT = 0   # the reference's V-cycle
+PROLONG_TRILINEAR = 1  # convergent variant
+
+
+def mgfrac3d_solve(f, ax, ay, az, n, d, ncycles, nu1, nu2, omega, p0=None, prolong=PROLONG_CONSTANT):
+    nx, ny, nz = n
+    p = np.zeros((nz, nx, ny))
+    hist = np.zeros(max(ncycles, 1))
+    lib().or_mgfrac3d_solve(_p(p), _p(None if p0 is None else _f64(p0)), _p(_f64(f)), _p(_f64(ax)),
+                            _p(_f64(ay)), _p(_f64(az)), nx, ny, nz, *d, ncycles, nu1, nu2, omega, prolong,
+                            _p(hist))
+    return p, hist[:ncycles]
+
+
+def mgfrac2d_solve(f, ax, ay, n, d, ncycles, nu1, nu2, omega, p0=None, prolong=PROLONG_CONSTANT):
+    nx, ny = n
+    p = np.zeros((nx, ny))
+    hist = np.zeros(max(ncycles, 1))
+    lib().or_mgfrac2d_solve(_p(p), _p(None if p0 is None else _f64(p0)), _p(_f64(f)), _p(_f64(ax)),
+                            _p(_f64(ay)), nx, ny, *d, ncycles, nu1, nu2, omega, prolong, _p(hist))
+    return p, hist[:ncycles]
+
+
+def frac_residual3d(p, f, ax, ay, az, n, d):
+    nx, ny, nz = n
+    r = np.zeros((nz, nx, ny))
+    rel = lib().or_frac_residual3d(_p(r), _p(_f64(p)), _p(_f64(f)), _p(_f64(ax)), _p(_f64(ay)), _p(_f64(az)),
+                                   nx, ny, nz, *d)
+    return rel, r
+
+
+def frac_residual2d(p, f, ax, ay, n, d):
+    nx, ny = n
+    r = np.zeros((nx, ny))
+    rel = lib().or_frac_residual2d(_p(r), _p(_f64(p)), _p(_f64(f)), _p(_f64(ax)), _p(_f64(ay)), nx, ny, *d)
+    return rel, r
+
+
+def dst3d_poisson(f, n, d):
+    nx, ny, nz = n
+    p = np.zeros((nz, nx, ny))
+    lib().or_dst3d_poisson(_p(p), _p(_f64(f)), nx, ny, nz, *d)
+    return p
+
+
+# -------------------------------------------------------------------- metrics
+def rel_l2(ref, got) -> float:
+    """Relative L2 error, CalculateErrorL2 (Utils.cpp:184-210): sqrt(sum (a-b)^2 / sum a^2)."""
+    ref = np.asarray(ref, dtype=np.float64)
+    got = np.asarray(got, dtype=np.float64)
+    den = float(np.sum(ref * ref))
+    return float(np.sqrt(np.sum((ref - got) ** 2) / den)) if den > 0 else float(np.sqrt(np.sum(got * got)))
+
+
+def rel_l2_multi(refs, gots) -> float:
+    num = sum(float(np.sum((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2)) for a, b in zip(refs, gots))
+    den = sum(float(np.sum(np.asarray(a, np.float64) ** 2)) for a in refs)
+    return float(np.sqrt(num / den)) if den > 0 else float(np.sqrt(num))

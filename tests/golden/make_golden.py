@@ -1,0 +1,174 @@
+"""Generate the golden fixtures in this directory from the reference's own CUDA build.
+
+Run on a GPU host after ``make -C oracle/refharness`` has built ``oracle/_ref/ref_driver`` from the
+unmodified reference sources (FP64, the reference default):
+
+    python tests/golden/make_golden.py
+
+Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
+(CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D::ProjectLocal_q_ccc,
+CuDivLocalProject::ProjectSingle, CuWaveletPotentialRecover3D/2D::Solve, CuMultigridFrac3D/2D::Solve,
+CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P, CuSolidLevelSet3D) and stores inputs
+and reference outputs as ``<case>.npz``.  The CPU tests pin the FP64 oracle against these files;
+the GPU tests compare the CUDA kernels with the oracle on the same inputs.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+CDF4_6, CDF3_7 = 7, 11
+
+
+def run(op, inputs: dict, params, outputs: dict):
+    """inputs: name -> array; outputs: name -> shape. Returns dict of output arrays."""
+    with tempfile.TemporaryDirectory() as tin, tempfile.TemporaryDirectory() as tout:
+        for k, v in inputs.items():
+            np.ascontiguousarray(v, dtype=np.float64).tofile(os.path.join(tin, k + ".bin"))
+        cmd = [DRIVER, op, tin, tout] + [str(p) for p in params]
+        subprocess.run(cmd, check=True, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=600)
+        return {k: np.fromfile(os.path.join(tout, k + ".bin"), dtype=np.float64).reshape(s)
+                for k, s in outputs.items()}
+
+
+def save(name, **arrays):
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+    print("wrote", name, {k: np.shape(v) for k, v in arrays.items()})
+
+
+def shapes3(n):
+    nx, ny, nz = n
+    return {"xv": (nz, nx + 1, ny), "yv": (nz, nx, ny + 1), "zv": (nz + 1, nx, ny),
+            "qx": (nz + 1, nx, ny + 1), "qy": (nz + 1, nx + 1, ny), "qz": (nz, nx + 1, ny + 1), "p": (nz, nx, ny)}
+
+
+def main():
+    if not os.path.exists(DRIVER):
+        sys.exit(f"{DRIVER} missing: run make -C oracle/refharness first (needs nvcc and the reference sources)")
+    rng = np.random.default_rng(20261203)
+
+    # 1D transforms along every axis, both wavelets, both boundary types, both directions
+    dwt = {}
+    for wav, ext in ((CDF3_7, 0), (CDF4_6, 1)):
+        for bc in "nd":
+            for fwd in (1, 0):
+                for axis, (L, other) in {"y": (4, (3, 2)), "x": (5, (4, 3)), "z": (3, (5, 2))}.items():
+                    n = (1 << L) + ext
+                    if axis == "y":
+                        DX, DY, DZ = other[0], n, other[1]
+                    elif axis == "x":
+                        DX, DY, DZ = n, other[0], other[1]
+                    else:
+                        DX, DY, DZ = other[0], other[1], n
+                    a = rng.standard_normal((DZ, DX, DY))
+                    out = run("dwt1d", {"a": a}, [DX, DY, DZ, L, axis, bc, wav, fwd], {"c": (DZ, DX, DY)})
+                    key = f"w{wav}_{bc}_{'f' if fwd else 'i'}_{axis}"
+                    dwt[key + "_in"] = a
+                    dwt[key + "_out"] = out["c"]
+                    dwt[key + "_meta"] = np.array([DX, DY, DZ, L, ord(axis), ord(bc), wav, fwd])
+    # long lines: the full 256-point y transform (the 256^3 line length)
+    for wav, ext, bc in ((CDF3_7, 0, "n"), (CDF4_6, 1, "d")):
+        for fwd in (1, 0):
+            n = 256 + ext
+            a = rng.standard_normal((1, 2, n))
+            out = run("dwt1d", {"a": a}, [2, n, 1, 8, "y", bc, wav, fwd], {"c": (1, 2, n)})
+            key = f"w{wav}_{bc}_{'f' if fwd else 'i'}_long"
+            dwt[key + "_in"] = a
+            dwt[key + "_out"] = out["c"]
+            dwt[key + "_meta"] = np.array([2, n, 1, 8, ord("y"), ord(bc), wav, fwd])
+    save("dwt1d", **dwt)
+
+    # inner-product tables (8 bands of length dim; band 0 is the diagonal)
+    ips = {}
+    for n in (16, 32, 64):
+        for wav, bc, dim in ((CDF3_7, "n", n), (CDF3_7, "d", n), (CDF4_6, "d", n + 1), (CDF4_6, "n", n + 1)):
+            out = run("ip", {}, [dim, wav, bc], {"ip": (8, dim)})
+            ips[f"ip_{dim}_{wav}_{bc}"] = out["ip"]
+    save("ip_tables", **ips)
+
+    # pointwise projections on random coefficient arrays
+    n3 = (16, 8, 32)
+    s = shapes3(n3)
+    xv, yv, zv = (rng.standard_normal(s[k]) for k in ("xv", "yv", "zv"))
+    h = 1.0 / 16
+    out = run("project3d", {"xv": xv, "yv": yv, "zv": zv}, [*n3, h], {k: s[k] for k in ("qx", "qy", "qz")})
+    save("project3d", n=np.array(n3), h=h, xv=xv, yv=yv, zv=zv, **out)
+    n2 = (32, 16)
+    xv2, yv2 = rng.standard_normal((n2[0] + 1, n2[1])), rng.standard_normal((n2[0], n2[1] + 1))
+    out = run("project2d", {"xv": xv2, "yv": yv2}, [*n2, 1.0 / 32], {"qz": (n2[0] + 1, n2[1] + 1)})
+    save("project2d", n=np.array(n2), h=1.0 / 32, xv=xv2, yv=yv2, **out)
+
+    # full potential recovery (random fields with zero wall-normal velocity)
+    for tag, n3 in (("recover3d_16", (16, 16, 16)), ("recover3d_aniso", (8, 16, 32))):
+        s = shapes3(n3)
+        xv, yv, zv = (rng.standard_normal(s[k]) for k in ("xv", "yv", "zv"))
+        xv[:, 0, :] = xv[:, -1, :] = 0
+        yv[:, :, 0] = yv[:, :, -1] = 0
+        zv[0] = zv[-1] = 0
+        h = 1.0 / n3[0]
+        out = run("recover3d", {"xv": xv, "yv": yv, "zv": zv}, [*n3, h], {k: s[k] for k in ("qx", "qy", "qz")})
+        save(tag, n=np.array(n3), h=h, xv=xv, yv=yv, zv=zv, **out)
+    for tag, n2 in (("recover2d_32", (32, 32)), ("recover2d_aniso", (64, 16))):
+        xv2, yv2 = rng.standard_normal((n2[0] + 1, n2[1])), rng.standard_normal((n2[0], n2[1] + 1))
+        xv2[0] = xv2[-1] = 0
+        yv2[:, 0] = yv2[:, -1] = 0
+        h = 1.0 / n2[0]
+        out = run("recover2d", {"xv": xv2, "yv": yv2}, [*n2, h], {"qz": (n2[0] + 1, n2[1] + 1)})
+        save(tag, n=np.array(n2), h=h, xv=xv2, yv=yv2, **out)
+
+    # solid fractions from a sphere level set (TestLocalProjection.cpp:621-627 geometry)
+    fr = {}
+    for n, r in ((16, 0.245), (32, 0.2)):
+        h = 1.0 / n
+        out = run("frac3d", {}, [n, h, 0.5, 0.5, 0.5, r], {k: shapes3((n, n, n))[k2] for k, k2 in
+                                                           (("ax", "xv"), ("ay", "yv"), ("az", "zv"))})
+        for k, v in out.items():
+            fr[f"{k}_{n}"] = v
+        fr[f"r_{n}"] = np.array(r)
+    save("fractions3d", **fr)
+
+    # divergence and gradient update with fractions
+    n = 16
+    s = shapes3((n, n, n))
+    ax, ay, az = fr["ax_16"], fr["ay_16"], fr["az_16"]
+    xv, yv, zv = (rng.standard_normal(s[k]) for k in ("xv", "yv", "zv"))
+    p = rng.standard_normal(s["p"])
+    out = run("div3d", {"xv": xv, "yv": yv, "zv": zv, "ax": ax, "ay": ay, "az": az}, [n, n, n, 1.0 / n],
+              {"b": s["p"]})
+    out2 = run("grad3d", {"xv": xv, "yv": yv, "zv": zv, "ax": ax, "ay": ay, "az": az, "p": p}, [n, n, n, 1.0 / n],
+               {"xv": s["xv"], "yv": s["yv"], "zv": s["zv"]})
+    save("divgrad3d", n=np.array([n, n, n]), h=1.0 / n, xv=xv, yv=yv, zv=zv, p=p, ax=ax, ay=ay, az=az, b=out["b"],
+         xv_out=out2["xv"], yv_out=out2["yv"], zv_out=out2["zv"])
+
+    # fractional multigrid: per-cycle residual history and the solution
+    for tag, n, frs, cyc, nu, w in (("mg3d_16", 16, "16", 6, (2, 2), 2.0 / 3.0), ("mg3d_32", 32, "32", 4, (3, 3), 0.8)):
+        s = shapes3((n, n, n))
+        ax, ay, az = fr["ax_" + frs], fr["ay_" + frs], fr["az_" + frs]
+        xv, yv, zv = (rng.standard_normal(s[k]) for k in ("xv", "yv", "zv"))
+        xv[:, 0, :] = xv[:, -1, :] = 0
+        yv[:, :, 0] = yv[:, :, -1] = 0
+        zv[0] = zv[-1] = 0
+        f = run("div3d", {"xv": xv, "yv": yv, "zv": zv, "ax": ax, "ay": ay, "az": az}, [n, n, n, 1.0 / n],
+                {"b": s["p"]})["b"]
+        out = run("mg3d", {"f": f, "ax": ax, "ay": ay, "az": az}, [n, n, n, 1.0 / n, cyc, nu[0], nu[1], w],
+                  {"p": s["p"], "hist": (cyc,)})
+        save(tag, n=np.array([n, n, n]), h=1.0 / n, f=f, ax=ax, ay=ay, az=az, ncycles=cyc, nu=np.array(nu), omega=w,
+             **out)
+    n2 = (32, 32)
+    ax2 = np.clip(rng.uniform(-0.3, 1.3, (n2[0] + 1, n2[1])), 0, 1)
+    ay2 = np.clip(rng.uniform(-0.3, 1.3, (n2[0], n2[1] + 1)), 0, 1)
+    f2 = rng.standard_normal(n2)
+    f2 -= f2.mean()
+    out = run("mg2d", {"f": f2, "ax": ax2, "ay": ay2}, [*n2, 1.0 / 32, 5, 5, 5, 0.8], {"p": n2, "hist": (5,)})
+    save("mg2d_32", n=np.array(n2), h=1.0 / 32, f=f2, ax=ax2, ay=ay2, ncycles=5, nu=np.array([5, 5]), omega=0.8, **out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,105 @@
+"""Pins the FP64 oracle to the reference's own CUDA build (FP64): tests/golden/*.npz were produced
+by tests/golden/make_golden.py through oracle/_ref/ref_driver on a B200."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+
+def test_dwt1d_matches_reference(oracle):
+    d = load_golden("dwt1d")
+    cases = [k[:-5] for k in d.files if k.endswith("_meta")]
+    assert len(cases) >= 28
+    for b in cases:
+        DX, DY, DZ, L, ax, bc, wav, fwd = (int(v) for v in d[b + "_meta"])
+        out = oracle.dwt_axis(d[b + "_in"], L, chr(ax), wav, chr(bc), bool(fwd))
+        ref = d[b + "_out"]
+        err = np.max(np.abs(out - ref)) / np.max(np.abs(ref))
+        assert err < 1e-12, (b, err)
+
+
+def test_ip_tables_match_reference(oracle):
+    ip = load_golden("ip_tables")
+    for k in ip.files:
+        _, dim, wav, bc = k.split("_")
+        mine = oracle.ip_diag(int(dim), int(wav), bc)
+        # the reference forms B B^T through a float tile and a float accumulator (cudaMath.cu:677-753)
+        np.testing.assert_allclose(mine, ip[k][0], rtol=1e-6, err_msg=k)
+
+
+@pytest.mark.parametrize("name", ["project3d"])
+def test_project3d_matches_reference(oracle, name):
+    p = load_golden(name)
+    n = tuple(int(v) for v in p["n"])
+    h = float(p["h"])
+    qs = oracle.project3d(p["xv"], p["yv"], p["zv"], n, (h, h, h))
+    for key, q in zip(("qx", "qy", "qz"), qs):
+        assert oracle.rel_l2(p[key], q) < 1e-6, key
+
+
+def test_project2d_matches_reference(oracle):
+    p = load_golden("project2d")
+    n = tuple(int(v) for v in p["n"])
+    h = float(p["h"])
+    assert oracle.rel_l2(p["qz"], oracle.project2d(p["xv"], p["yv"], n, (h, h))) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["recover3d_16", "recover3d_aniso"])
+def test_recover3d_matches_reference(oracle, name):
+    p = load_golden(name)
+    n = tuple(int(v) for v in p["n"])
+    h = float(p["h"])
+    qs = oracle.recover3d(p["xv"], p["yv"], p["zv"], n, (h, h, h))
+    for key, q in zip(("qx", "qy", "qz"), qs):
+        assert oracle.rel_l2(p[key], q) < 1e-6, key
+
+
+@pytest.mark.parametrize("name", ["recover2d_32", "recover2d_aniso"])
+def test_recover2d_matches_reference(oracle, name):
+    p = load_golden(name)
+    n = tuple(int(v) for v in p["n"])
+    h = float(p["h"])
+    assert oracle.rel_l2(p["qz"], oracle.recover2d(p["xv"], p["yv"], n, (h, h))) < 1e-6
+
+
+def test_fractions_match_reference(oracle):
+    fr = load_golden("fractions3d")
+    for n in (16, 32):
+        r = float(fr[f"r_{n}"])
+        sdf = oracle.sdf_spheres3d((n,) * 3, 1.0 / n, [[0.5, 0.5, 0.5]], [r])
+        mine = oracle.fractions3d(sdf, (n,) * 3, 1.0 / n)
+        for m, k in zip(mine, ("ax", "ay", "az")):
+            # the reference takes sqrtf of the FP64 argument (cuSolidLevelSet3D.cu:32)
+            assert np.max(np.abs(m - fr[f"{k}_{n}"])) < 1e-6
+
+
+def test_divergence_and_gradient_match_reference(oracle):
+    p = load_golden("divgrad3d")
+    n = tuple(int(v) for v in p["n"])
+    h = float(p["h"])
+    b = oracle.divergence3d(p["xv"], p["yv"], p["zv"], p["ax"], p["ay"], p["az"], n, (h,) * 3)
+    assert oracle.rel_l2(p["b"], b) < 1e-13
+    u = oracle.grad_subtract3d(p["xv"], p["yv"], p["zv"], p["p"], p["ax"], p["ay"], p["az"], n, (h,) * 3, True)
+    for key, m in zip(("xv", "yv", "zv"), u):
+        assert oracle.rel_l2(p[key + "_out"], m) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["mg3d_16", "mg3d_32"])
+def test_mg3d_matches_reference_per_cycle(oracle, name):
+    p = load_golden(name)
+    n = tuple(int(v) for v in p["n"])
+    h = float(p["h"])
+    sol, hist = oracle.mgfrac3d_solve(p["f"], p["ax"], p["ay"], p["az"], n, (h,) * 3, int(p["ncycles"]),
+                                      int(p["nu"][0]), int(p["nu"][1]), float(p["omega"]))
+    np.testing.assert_allclose(hist, p["hist"], rtol=1e-9)
+    assert oracle.rel_l2(p["p"], sol) < 1e-11
+
+
+def test_mg2d_matches_reference_per_cycle(oracle):
+    p = load_golden("mg2d_32")
+    n = tuple(int(v) for v in p["n"])
+    h = float(p["h"])
+    sol, hist = oracle.mgfrac2d_solve(p["f"], p["ax"], p["ay"], n, (h,) * 2, int(p["ncycles"]), int(p["nu"][0]),
+                                      int(p["nu"][1]), float(p["omega"]))
+    np.testing.assert_allclose(hist, p["hist"], rtol=1e-9)
+    assert oracle.rel_l2(p["p"], sol) < 1e-11

@@ -1,0 +1,112 @@
+"""Size-independent properties of the oracle (the reference ships no golden data, so these are the
+self-consistency invariants its experiments rely on, TestLocalProjection.cpp:526-790)."""
+import numpy as np
+import pytest
+
+from waveletpotentials_b200 import fields
+
+
+@pytest.mark.parametrize("wav,ext", [(11, 0), (7, 1)])
+@pytest.mark.parametrize("bc", ["n", "d"])
+@pytest.mark.parametrize("levels", [2, 3, 5, 8])
+def test_perfect_reconstruction(oracle, wav, ext, bc, levels):
+    rng = np.random.default_rng(levels)
+    x = rng.standard_normal((1 << levels) + ext)
+    if wav == 7 and bc == "d":
+        x[0] = x[-1] = 0.0  # the odd-extension (Dirichlet) div wavelet is invertible on zero-boundary data
+    c = oracle.dwt_line(x, levels, wav, bc, True)
+    np.testing.assert_allclose(oracle.dwt_line(c, levels, wav, bc, False), x, atol=1e-12)
+
+
+def _divfree3d(oracle, n, seed):
+    rng = np.random.default_rng(seed)
+    s = oracle.mac_shapes3d(*n)
+    qx, qy, qz = (rng.standard_normal(s[k]) for k in ("qx", "qy", "qz"))
+    qx[0] = qx[-1] = 0
+    qx[:, :, 0] = qx[:, :, -1] = 0
+    qy[0] = qy[-1] = 0
+    qy[:, 0, :] = qy[:, -1, :] = 0
+    qz[:, 0, :] = qz[:, -1, :] = 0
+    qz[:, :, 0] = qz[:, :, -1] = 0
+    d = tuple(1.0 / v for v in n)
+    return oracle.curl3d(qx, qy, qz, n, (d[0], d[0], d[0])), (d[0],) * 3
+
+
+@pytest.mark.parametrize("n", [(8, 8, 8), (16, 16, 16), (8, 16, 32)])
+def test_recovery_reproduces_divergence_free_fields(oracle, n):
+    (xv, yv, zv), d = _divfree3d(oracle, n, 3)
+    qs = oracle.recover3d(xv, yv, zv, n, d)
+    ux, uy, uz = oracle.curl3d(*qs, n, d)
+    assert oracle.rel_l2_multi([xv, yv, zv], [ux, uy, uz]) < 1e-11
+
+
+def test_recovery2d_reproduces_divergence_free_fields(oracle):
+    n = (64, 32)
+    rng = np.random.default_rng(4)
+    qz = rng.standard_normal((n[0] + 1, n[1] + 1))
+    qz[0] = qz[-1] = 0
+    qz[:, 0] = qz[:, -1] = 0
+    d = (1.0 / 64, 1.0 / 64)
+    xv, yv = oracle.curl2d(qz, n, d)
+    ux, uy = oracle.curl2d(oracle.recover2d(xv, yv, n, d), n, d)
+    assert oracle.rel_l2_multi([xv, yv], [ux, uy]) < 1e-11
+
+
+def test_projection_is_linear(oracle):
+    n = (16, 16, 16)
+    rng = np.random.default_rng(5)
+    s = oracle.mac_shapes3d(*n)
+    a = [rng.standard_normal(s[k]) for k in ("xv", "yv", "zv")]
+    b = [rng.standard_normal(s[k]) for k in ("xv", "yv", "zv")]
+    d = (1 / 16,) * 3
+    qa = oracle.recover3d(*a, n, d)
+    qb = oracle.recover3d(*b, n, d)
+    qab = oracle.recover3d(*[2 * x - 3 * y for x, y in zip(a, b)], n, d)
+    for u, v, w in zip(qa, qb, qab):
+        np.testing.assert_allclose(w, 2 * u - 3 * v, atol=1e-9)
+
+
+def test_multigrid_trilinear_converges_h_independently(oracle):
+    for n in (16, 32):
+        nn = (n,) * 3
+        h = 1.0 / n
+        sdf = oracle.sdf_spheres3d(nn, h, [[0.5, 0.5, 0.5]], [0.2])
+        ax, ay, az = oracle.fractions3d(sdf, nn, h)
+        xv, yv, zv = fields.velocity3d(nn, 1)
+        f = oracle.divergence3d(xv, yv, zv, ax, ay, az, nn, (h,) * 3)
+        _, hist = oracle.mgfrac3d_solve(f, ax, ay, az, nn, (h,) * 3, 12, 2, 2, 2 / 3, prolong=oracle.PROLONG_TRILINEAR)
+        assert hist[-1] < 1e-6
+        assert hist[-1] / hist[-2] < 0.5
+
+
+def test_reference_vcycle_stalls_at_omega_two_thirds(oracle):
+    """The reference V(2,2), omega 2/3 cycle (constant prolongation) stops converging at 64^3."""
+    n = 64
+    nn = (n,) * 3
+    h = 1.0 / n
+    ones = [np.ones(s) for s in (oracle.mac_shapes3d(*nn)[k] for k in ("xv", "yv", "zv"))]
+    xv, yv, zv = fields.velocity3d(nn, 2)
+    f = oracle.divergence3d(xv, yv, zv, *ones, nn, (h,) * 3)
+    _, hist = oracle.mgfrac3d_solve(f, *ones, nn, (h,) * 3, 12, 2, 2, 2 / 3)
+    assert hist[-1] > hist.min() * 1.5
+
+
+def test_dst_poisson_solves_dirichlet_laplacian(oracle):
+    n = (12, 10, 8)
+    h = 0.1
+    rng = np.random.default_rng(6)
+    f = rng.standard_normal((n[2], n[0], n[1]))
+    p = oracle.dst3d_poisson(f, n, (h, h, h))
+    pp = np.pad(p, 1)
+    lap = (6 * pp[1:-1, 1:-1, 1:-1] - pp[:-2, 1:-1, 1:-1] - pp[2:, 1:-1, 1:-1] - pp[1:-1, :-2, 1:-1]
+           - pp[1:-1, 2:, 1:-1] - pp[1:-1, 1:-1, :-2] - pp[1:-1, 1:-1, 2:]) / (h * h)
+    np.testing.assert_allclose(lap, f, atol=1e-9)
+
+
+def test_generated_velocity_has_compatible_divergence(oracle):
+    n = (24, 16, 32)
+    xv, yv, zv = fields.velocity3d(n, 7)
+    assert np.all(xv[:, 0, :] == 0) and np.all(yv[:, :, 0] == 0) and np.all(zv[0] == 0)
+    ones = [np.ones_like(a) for a in (xv, yv, zv)]
+    b = oracle.divergence3d(xv, yv, zv, *ones, n, (1 / 24,) * 3)
+    assert abs(b.sum()) < 1e-8 * np.abs(b).sum()

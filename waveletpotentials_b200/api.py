@@ -1,0 +1,388 @@
+"""Host-side mirror of the reference's C++ entry points for the projection-and-recovery path.
+
+Class and method names follow the reference (CuWHHDForward::Solve1D, CuWaveletPotentialRecover3D,
+CuDivLocalProject3D::ProjectLocal_q_ccc, CuMultigridFrac3D::Solve / GetResdualError,
+CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P, CuSolidLevelSet3D) so code written
+against the reference reads the same.  Arguments are torch CUDA float32 tensors in the reference
+layout: a 3D array with extents (DX, DY, DZ) has torch shape (DZ, DX, DY) (y contiguous); 2D arrays
+are (DX, DY).  Every call goes through the C ABI of libwp_b200.so (include/wp_api.h); errors
+raise WPError instead of exiting the process.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONSTANT, PROLONG_TRILINEAR, MgParams, \
+    MgReport, WPError, check, lib
+
+__all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRecover2D", "CuMultigridFrac3D",
+           "CuMultigridFrac2D", "CuConvergence", "CuGradient", "CuSolidLevelSet3D", "Projector3D", "max_abs",
+           "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
+           "PROLONG_TRILINEAR", "mac_shapes3d", "mac_shapes2d"]
+
+
+def mac_shapes3d(nx, ny, nz):
+    return {"xv": (nz, nx + 1, ny), "yv": (nz, nx, ny + 1), "zv": (nz + 1, nx, ny),
+            "qx": (nz + 1, nx, ny + 1), "qy": (nz + 1, nx + 1, ny), "qz": (nz, nx + 1, ny + 1), "p": (nz, nx, ny)}
+
+
+def mac_shapes2d(nx, ny):
+    return {"xv": (nx + 1, ny), "yv": (nx, ny + 1), "qz": (nx + 1, ny + 1), "p": (nx, ny)}
+
+
+def _stream(stream):
+    if stream is None:
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, torch.cuda.Stream):
+        return ctypes.c_void_p(stream.cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+def _ptr(t: torch.Tensor | None, shape=None, dtype=torch.float32, name="tensor"):
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise WPError(1, name, "expected a CUDA tensor")
+    if t.dtype != dtype:
+        raise WPError(1, name, f"expected {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise WPError(1, name, "expected a contiguous tensor")
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise WPError(1, name, f"expected shape {tuple(shape)}, got {tuple(t.shape)}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _c(ch: str):
+    return ctypes.c_char(ch.encode())
+
+
+def _dims3(dim):
+    nx, ny, nz = (int(v) for v in dim)
+    return nx, ny, nz
+
+
+def _dx3(dx):
+    if isinstance(dx, (int, float)):
+        return float(dx), float(dx), float(dx)
+    return tuple(float(v) for v in dx)
+
+
+class CuWHHDForward:
+    """CuWHHDForward::Solve1D (cuWHHDForward.cu:1122-1153): full-depth 1D transform along one axis."""
+
+    @staticmethod
+    def Solve1D(dst, src, dim, level, direction, bc="n", rsw_type=CDF3_7, is_forward=True, stream=None):
+        dx, dy, dz = _dims3(dim)
+        src = dst if src is None else src
+        dt = dst.dtype
+        if dt not in (torch.float32, torch.float64):
+            raise WPError(1, "Solve1D", "float32 or float64 tensors only")
+        shape = (dz, dx, dy)
+        fn = lib().wp_dwt1d if dt == torch.float32 else lib().wp_dwt1d_f64
+        check(fn(_ptr(dst, shape, dt, "dst"), _ptr(src, shape, dt, "src"), dx, dy, dz, int(level),
+                 _c(direction), _c(bc), int(rsw_type), int(bool(is_forward)), _stream(stream)), "wp_dwt1d")
+
+
+def ip_diag(dim: int, wavelet: int, bc: str):
+    """Diagonal inner-product table (CuGetInnerProduct::GenerateIp band 0), computed on the GPU."""
+    import numpy as np
+    out = np.zeros(int(dim))
+    check(lib().wp_ip_diag(out.ctypes.data_as(ctypes.c_void_p), int(dim), int(wavelet), _c(bc)), "wp_ip_diag")
+    return out
+
+
+class CuWaveletPotentialRecover3D:
+    """CuWaveletPotentialRecover3D (cuWaveletPotentialRecover3D.cuh:11-15)."""
+
+    def __init__(self, dim, dx, bc="n", type_w_curl=CDF3_7, type_w_div=CDF4_6):
+        self.dim = _dims3(dim)
+        self.dx = _dx3(dx)
+        self.shapes = mac_shapes3d(*self.dim)
+        h = ctypes.c_void_p()
+        check(lib().wp_recover3d_create(ctypes.byref(h), *self.dim, *self.dx, _c(bc), int(type_w_curl),
+                                        int(type_w_div)), "wp_recover3d_create")
+        self._h = h
+
+    def Solve(self, qx, qy, qz, xv, yv, zv, stream=None):
+        s = self.shapes
+        check(lib().wp_recover3d_run(self._h, _ptr(qx, s["qx"]), _ptr(qy, s["qy"]), _ptr(qz, s["qz"]),
+                                     _ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]), _stream(stream)),
+              "wp_recover3d_run")
+
+    def ProjectLocal_q_ccc(self, qx, qy, qz, xv_lwt, yv_lwt, zv_lwt, stream=None):
+        s = self.shapes
+        check(lib().wp_recover3d_project(self._h, _ptr(qx, s["qx"]), _ptr(qy, s["qy"]), _ptr(qz, s["qz"]),
+                                         _ptr(xv_lwt, s["xv"]), _ptr(yv_lwt, s["yv"]), _ptr(zv_lwt, s["zv"]),
+                                         _stream(stream)), "wp_recover3d_project")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().wp_recover3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CuWaveletPotentialRecover2D:
+    """CuWaveletPotentialRecover2D (cuWaveletPotentialRecover2D.cuh:11-15)."""
+
+    def __init__(self, dim, dx, bc="n", type_w_curl=CDF3_7, type_w_div=CDF4_6):
+        self.dim = tuple(int(v) for v in dim)
+        self.dx = (float(dx), float(dx)) if isinstance(dx, (int, float)) else tuple(float(v) for v in dx)
+        self.shapes = mac_shapes2d(*self.dim)
+        h = ctypes.c_void_p()
+        check(lib().wp_recover2d_create(ctypes.byref(h), *self.dim, *self.dx, _c(bc), int(type_w_curl),
+                                        int(type_w_div)), "wp_recover2d_create")
+        self._h = h
+
+    def Solve(self, qz, xv, yv, stream=None):
+        s = self.shapes
+        check(lib().wp_recover2d_run(self._h, _ptr(qz, s["qz"]), _ptr(xv, s["xv"]), _ptr(yv, s["yv"]),
+                                     _stream(stream)), "wp_recover2d_run")
+
+    def ProjectSingle(self, qz, xv_lwt, yv_lwt, stream=None):
+        s = self.shapes
+        check(lib().wp_recover2d_project(self._h, _ptr(qz, s["qz"]), _ptr(xv_lwt, s["xv"]), _ptr(yv_lwt, s["yv"]),
+                                         _stream(stream)), "wp_recover2d_project")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().wp_recover2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _report(r: MgReport) -> dict:
+    return {"cycles": r.cycles, "rel_residual": r.rel_residual, "history": list(r.history[:min(r.cycles, 64)])}
+
+
+class CuMultigridFrac3D:
+    """CuMultigridFrac3D (cuMultigridFrac3D.cuh:15-18)."""
+
+    def __init__(self, ax, ay, az, dim, dx, bc="n", stream=None):
+        self.dim = _dims3(dim)
+        self.dx = _dx3(dx)
+        s = mac_shapes3d(*self.dim)
+        self.cells = s["p"]
+        h = ctypes.c_void_p()
+        check(lib().wp_mgfrac3d_create(ctypes.byref(h), _ptr(ax, s["xv"], name="ax"), _ptr(ay, s["yv"], name="ay"),
+                                       _ptr(az, s["zv"], name="az"), *self.dim, *self.dx, _c(bc), _stream(stream)),
+              "wp_mgfrac3d_create")
+        self._h = h
+
+    def Solve(self, dst, pre_v, f, n_iters=10, nu1=2, nu2=2, weight=0.8, stream=None):
+        """Exactly n_iters FP32 V-cycles of the reference algorithm (cuMultigridFrac3D.cu:249-265)."""
+        c = self.cells
+        check(lib().wp_mgfrac3d_solve(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), int(n_iters), int(nu1),
+                                      int(nu2), float(weight), _stream(stream)), "wp_mgfrac3d_solve")
+
+    def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, stream=None) -> dict:
+        c = self.cells
+        prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), int(precision),
+                       int(prolongation))
+        rep = MgReport()
+        st = lib().wp_mgfrac3d_solve_tol(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), ctypes.byref(prm),
+                                         ctypes.byref(rep), _stream(stream))
+        out = _report(rep)
+        out["status"] = _lib.STATUS.get(st, st)
+        if raise_on_fail and st != 0:
+            check(st, "wp_mgfrac3d_solve_tol")
+        return out
+
+    def Iterate64(self, stream=None):
+        """FP64 iterate of the last mixed / FP64 solve, as a numpy array."""
+        t = torch.empty(self.cells, device="cuda", dtype=torch.float64)
+        check(lib().wp_mgfrac3d_iterate64(self._h, ctypes.c_void_p(t.data_ptr()), _stream(stream)),
+              "wp_mgfrac3d_iterate64")
+        return t.cpu().numpy()
+
+    def GetResdualError(self, dst, f, stream=None) -> float:
+        out = ctypes.c_double()
+        c = self.cells
+        check(lib().wp_mgfrac3d_residual(self._h, _ptr(dst, c), _ptr(f, c), ctypes.byref(out), _stream(stream)),
+              "wp_mgfrac3d_residual")
+        return out.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().wp_mgfrac3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CuMultigridFrac2D:
+    """CuMultigridFrac2D (cuMultigridFrac2D.cuh:15-17)."""
+
+    def __init__(self, ax, ay, dim, dx, bc="n", stream=None):
+        self.dim = tuple(int(v) for v in dim)
+        self.dx = (float(dx), float(dx)) if isinstance(dx, (int, float)) else tuple(float(v) for v in dx)
+        s = mac_shapes2d(*self.dim)
+        self.cells = s["p"]
+        h = ctypes.c_void_p()
+        check(lib().wp_mgfrac2d_create(ctypes.byref(h), _ptr(ax, s["xv"], name="ax"), _ptr(ay, s["yv"], name="ay"),
+                                       *self.dim, *self.dx, _c(bc), _stream(stream)), "wp_mgfrac2d_create")
+        self._h = h
+
+    def Solve(self, dst, pre_v, f, n_iters=10, nu1=2, nu2=2, weight=0.8, stream=None):
+        c = self.cells
+        check(lib().wp_mgfrac2d_solve(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), int(n_iters), int(nu1),
+                                      int(nu2), float(weight), _stream(stream)), "wp_mgfrac2d_solve")
+
+    def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, stream=None) -> dict:
+        c = self.cells
+        prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), int(precision),
+                       int(prolongation))
+        rep = MgReport()
+        st = lib().wp_mgfrac2d_solve_tol(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), ctypes.byref(prm),
+                                         ctypes.byref(rep), _stream(stream))
+        out = _report(rep)
+        out["status"] = _lib.STATUS.get(st, st)
+        if raise_on_fail and st != 0:
+            check(st, "wp_mgfrac2d_solve_tol")
+        return out
+
+    def GetResdualError(self, dst, f, stream=None) -> float:
+        out = ctypes.c_double()
+        c = self.cells
+        check(lib().wp_mgfrac2d_residual(self._h, _ptr(dst, c), _ptr(f, c), ctypes.byref(out), _stream(stream)),
+              "wp_mgfrac2d_residual")
+        return out.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().wp_mgfrac2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CuConvergence:
+    """CuConvergence::GetB_3d_frac_vel / GetB_2d_frac_vel: b = -div(a u)."""
+
+    @staticmethod
+    def GetB_3d_frac_vel(b, xv, yv, zv, ax, ay, az, dim, dx, bc="n", stream=None):
+        nx, ny, nz = _dims3(dim)
+        s = mac_shapes3d(nx, ny, nz)
+        check(lib().wp_divergence_frac3d(_ptr(b, s["p"]), _ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]),
+                                         _ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(az, s["zv"]), nx, ny, nz,
+                                         *_dx3(dx), _stream(stream)), "wp_divergence_frac3d")
+
+    @staticmethod
+    def GetB_2d_frac_vel(b, xv, yv, ax, ay, dim, dx, bc="n", stream=None):
+        nx, ny = (int(v) for v in dim)
+        s = mac_shapes2d(nx, ny)
+        d = (float(dx), float(dx)) if isinstance(dx, (int, float)) else tuple(float(v) for v in dx)
+        check(lib().wp_divergence_frac2d(_ptr(b, s["p"]), _ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(ax, s["xv"]),
+                                         _ptr(ay, s["yv"]), nx, ny, *d, _stream(stream)), "wp_divergence_frac2d")
+
+
+class CuGradient:
+    """CuGradient::Gradient3D_Frac_P + CudaMatAdd(-1) + CudaMatMul(a), fused: u <- (u - grad p) [* a]."""
+
+    @staticmethod
+    def SubtractGradient3D_Frac_P(xv, yv, zv, p, ax, ay, az, dim, dx, multiply_frac=True, stream=None):
+        nx, ny, nz = _dims3(dim)
+        s = mac_shapes3d(nx, ny, nz)
+        check(lib().wp_grad_subtract_frac3d(_ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]), _ptr(p, s["p"]),
+                                            _ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(az, s["zv"]), nx, ny, nz,
+                                            *_dx3(dx), int(bool(multiply_frac)), _stream(stream)),
+              "wp_grad_subtract_frac3d")
+
+    @staticmethod
+    def SubtractGradient2D_Frac_P(xv, yv, p, ax, ay, dim, dx, multiply_frac=True, stream=None):
+        nx, ny = (int(v) for v in dim)
+        s = mac_shapes2d(nx, ny)
+        d = (float(dx), float(dx)) if isinstance(dx, (int, float)) else tuple(float(v) for v in dx)
+        check(lib().wp_grad_subtract_frac2d(_ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(p, s["p"]), _ptr(ax, s["xv"]),
+                                            _ptr(ay, s["yv"]), nx, ny, *d, int(bool(multiply_frac)),
+                                            _stream(stream)), "wp_grad_subtract_frac2d")
+
+
+def max_abs(t: torch.Tensor, stream=None) -> float:
+    """CudaFindMaxValue without the host copy of the array."""
+    out = ctypes.c_double()
+    check(lib().wp_max_abs(_ptr(t), t.numel(), ctypes.byref(out), _stream(stream)), "wp_max_abs")
+    return out.value
+
+
+class CuSolidLevelSet3D:
+    """CuSolidLevelSet3D: sphere level set (positive in fluid) and face open fractions."""
+
+    def __init__(self, dim, dx):
+        self.dim = _dims3(dim)
+        self.dx = float(dx)
+        nx, ny, nz = self.dim
+        self.ls = torch.empty((nz, nx, ny), device="cuda", dtype=torch.float32)
+
+    def InitLsSpheres(self, centers, radii, stream=None):
+        import numpy as np
+        c = np.ascontiguousarray(np.reshape(centers, (-1, 3)), dtype=np.float64)
+        r = np.ascontiguousarray(np.reshape(radii, (-1,)), dtype=np.float64)
+        check(lib().wp_sdf_spheres3d(_ptr(self.ls), *self.dim, self.dx, c.ctypes.data_as(ctypes.c_void_p),
+                                     r.ctypes.data_as(ctypes.c_void_p), int(r.size), _stream(stream)),
+              "wp_sdf_spheres3d")
+
+    def InitLsSphere(self, center, radius, stream=None):
+        self.InitLsSpheres([center], [radius], stream)
+
+    def GetFrac(self, ax, ay, az, stream=None):
+        s = mac_shapes3d(*self.dim)
+        check(lib().wp_fractions3d(_ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(az, s["zv"]), _ptr(self.ls), *self.dim,
+                                   self.dx, _stream(stream)), "wp_fractions3d")
+
+
+class Projector3D:
+    """One projection of a MAC velocity field (the composition of TestLocalProjection.cpp:666-767):
+    b = -div(a u) -> fractional multigrid solve to tolerance -> u <- a (u - grad p) -> max|div| check
+    -> wavelet potential recovery q.
+    """
+
+    def __init__(self, ax, ay, az, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, stream=None):
+        self.dim = _dims3(dim)
+        self.dx = _dx3(dx)
+        self.ax, self.ay, self.az = ax, ay, az
+        self.mg = CuMultigridFrac3D(ax, ay, az, self.dim, self.dx, "n", stream)
+        self.rec = CuWaveletPotentialRecover3D(self.dim, self.dx, "n")
+        self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
+                         prolongation=prolongation)
+        s = mac_shapes3d(*self.dim)
+        self.shapes = s
+        self.b = torch.empty(s["p"], device="cuda", dtype=torch.float32)
+        self.p = torch.empty(s["p"], device="cuda", dtype=torch.float32)
+
+    def run(self, xv, yv, zv, qx, qy, qz, pre_p=None, stream=None) -> dict:
+        """Projects (xv, yv, zv) in place (result a (u - grad p)) and writes the potential q."""
+        CuConvergence.GetB_3d_frac_vel(self.b, xv, yv, zv, self.ax, self.ay, self.az, self.dim, self.dx,
+                                       stream=stream)
+        rep = self.mg.SolveTol(self.p, pre_p, self.b, raise_on_fail=False, stream=stream, **self.opts)
+        CuGradient.SubtractGradient3D_Frac_P(xv, yv, zv, self.p, self.ax, self.ay, self.az, self.dim, self.dx,
+                                             multiply_frac=True, stream=stream)
+        # -div of the fraction-weighted projected field (open-face divergence of a (u - grad p))
+        CuConvergence.GetB_3d_frac_vel(self.b, xv, yv, zv, None, None, None, self.dim, self.dx, stream=stream)
+        rep["max_abs_div"] = max_abs(self.b, stream)
+        self.rec.Solve(qx, qy, qz, xv, yv, zv, stream)
+        return rep

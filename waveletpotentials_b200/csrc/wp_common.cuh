@@ -1,0 +1,58 @@
+// wp_common.cuh -- shared definitions for the sm_100a WaveletPotentials kernels.
+//
+// Layout (the reference's, Utils.h:46-47): element (x, y, z) of an array with extents
+// (DX, DY, DZ) lives at y + x*DY + z*DX*DY; y is contiguous.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/wp_api.h"
+
+#define WP_CUDA_TRY(expr)                                   \
+    do {                                                    \
+        cudaError_t _e = (expr);                            \
+        if (_e != cudaSuccess) { wp_set_cuda_error(_e, #expr, __FILE__, __LINE__); return WP_ERR_CUDA; } \
+    } while (0)
+
+#define WP_LAUNCH_CHECK()                                   \
+    do {                                                    \
+        cudaError_t _e = cudaGetLastError();                \
+        if (_e != cudaSuccess) { wp_set_cuda_error(_e, "kernel launch", __FILE__, __LINE__); return WP_ERR_CUDA; } \
+    } while (0)
+
+void wp_set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+void wp_set_error_msg(const char* msg);
+
+// wavelet ids (same values as the reference enum, WaveletTypes.h:7-27)
+enum { WP_ID_CDF4_6 = 7, WP_ID_CDF3_7 = 11 };
+
+static inline int wp_ilog2(int n) {
+    int l = 0;
+    while ((1 << (l + 1)) <= n) ++l;
+    return l;
+}
+static inline bool wp_is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+static inline int wp_half_up(int n) { return (n & 1) ? (n >> 1) + 1 : (n >> 1); }
+static inline unsigned wp_cdiv(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+// Number of SMs of the current device (cached per process; 148 on B200).
+int wp_sm_count();
+
+// Launch accounting (always) and per-kernel-class event timing (when enabled): wrap a launch as
+//   WP_KERNEL("name", algorithmic_bytes, stream, kernel<<<g, b, smem, stream>>>(...));
+int wp_prof_start(cudaStream_t s);
+void wp_prof_stop(int tok, const char* name, double bytes, cudaStream_t s);
+#define WP_KERNEL(name, bytes, stream, ...)                         \
+    do {                                                            \
+        const int _tok = wp_prof_start(stream);                     \
+        __VA_ARGS__;                                                \
+        WP_LAUNCH_CHECK();                                          \
+        wp_prof_stop(_tok, name, (double)(bytes), stream);          \
+    } while (0)
+
+// transform along one axis (wp_dwt.cu); T = float or double
+template <typename T>
+wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int levels, char axis, int wavelet,
+                             char bc, int forward, cudaStream_t stream);

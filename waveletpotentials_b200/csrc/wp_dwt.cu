@@ -1,0 +1,513 @@
+// wp_dwt.cu -- full-depth multilevel CDF3.7 / CDF4.6 lifting transforms along one axis.
+//
+// Reference behaviour: CuWHHDForward::Solve1D and the cuWHHDForward_{y,x,z}_ml /
+// cuWHHDBackward_{y,x,z}_ml kernels (cuWHHDForward.cu:5-742, 1122-1253) with the step functions
+// and boundary rules of cuWaveletCompute.cuh (CDF3.7: :876-900, :944-964, reflection :180-228,
+// :600-631; CDF4.6: :925-942, :983-1002, reflection :336-375, :716-752; base matrices :773-874).
+// Output layout (Mallat order): [base (4+ext) | d level 2 (4) | d level 3 (8) | ... | d level L-1 (n/2)].
+//
+// B200 design: one CTA owns a tile of C whole lines (C = 32/16/8/4 columns) staged in shared
+// memory as S[position][column] (column pitch C+1 so both the y-contiguous load and the
+// column-parallel lifting are bank-conflict free).  All levels run on chip; global memory is
+// read once and written once per pass, coalesced along y for every axis (for the x and z axes
+// the C columns are C consecutive y; for the y axis the tile is C consecutive whole lines,
+// one contiguous span).  Each thread lifts a chunk of 8 coefficient pairs per level from a
+// register window of 8+8 pairs (4-pair halo each side), so the lifting taps never touch
+// shared memory twice and need no shuffles.
+#include "wp_common.cuh"
+
+#include <cstdio>
+#include <cstring>
+
+namespace {
+
+constexpr int CH = 8;        // coefficient pairs per thread per level
+constexpr int WIN = CH + 8;  // register window (4-pair halo on each side)
+constexpr int NT = 256;      // threads per CTA
+
+// lifting constants (cuWaveletCompute.cuh:13-23, :139-148)
+#define WP_SQ2 1.41421356237309504880168872420969807856967187537694
+struct K37 {
+    static constexpr double fu1 = -1.0 / 3.0;
+    static constexpr double fp0 = -3.0 / 8.0, fp1 = -9.0 / 8.0;
+    static constexpr double q0 = -0.003797743055556, q1 = 0.032552083333333, q2 = -0.137044270833333,
+                            q3 = 0.444444444444444, q4 = 0.137044270833333, q5 = -0.032552083333333,
+                            q6 = 0.003797743055556;
+    static constexpr double scl0 = 3.0 / 1.414213562373095048801, scl1 = 1.414213562373095048801 / 3.0;
+};
+struct K46 {
+    static constexpr double fu1_0 = -0.25, fu1_1 = -0.25;
+    static constexpr double fp0 = -1.0, fp1 = -1.0;
+    static constexpr double c0 = 0.008544921875000, c1 = -0.064697265625000, c2 = 0.243652343750000,
+                            c3 = 0.243652343750000, c4 = -0.064697265625000, c5 = 0.008544921875000;
+    static constexpr double scl0 = 2.0 * WP_SQ2, scl1 = -1.0 / (2.0 * WP_SQ2);
+    static constexpr double scli0 = 1.0 / (2.0 * WP_SQ2), scli1 = -(2.0 * WP_SQ2);
+};
+
+// base-level matrices, row-major, in this order: 37n, 37d, 46n, 46d (forward), then inverses
+__constant__ double c_base37[4][16];
+__constant__ double c_base46[4][25];
+
+const double h_base37[4][16] = {
+    {0.500000000000000, 0.500000000000000, 0.500000000000000, 0.500000000000000, -0.399902343750000,
+     -0.200195312500000, 0.200195312500000, 0.399902343750000, -0.353553390593274, 0.530330085889911,
+     -0.176776695296637, 0, 0, 0.176776695296637, -0.530330085889911, 0.353553390593274},
+    {0.800781250000000, 1.599609375000000, 1.599609375000000, 0.800781250000000, -1.000000000000000,
+     -1.000000000000000, 1.000000000000000, 1.000000000000000, -0.707106781186548, 0.530330085889911,
+     -0.176776695296637, 0, 0, 0.176776695296637, -0.530330085889911, 0.707106781186548},
+    {0.500000000000000, -1.000000000000000, -0.990225707247567, 0.423987855125528, 0.500000000000000,
+     -0.500000000000000, 1.272654099342585, -0.141559463030510, 0.500000000000000, 0.500000000000000,
+     0.141559463030510, -1.272654099342585, 0.500000000000000, 1.000000000000000, -0.423987855125528,
+     0.990225707247567},
+    {0.125000000000000, -0.250000000000000, -0.919100708749311, 0.211993927562764, 0.250000000000000,
+     -0.250000000000000, 0.636672316654294, 0.070434464532254, 0.250000000000000, 0.250000000000000,
+     -0.070434464532254, -0.636672316654294, 0.125000000000000, 0.250000000000000, -0.211993927562764,
+     0.919100708749311}};
+const double h_base46[4][25] = {
+    {1.851562500000001, 2.097656250000000, 0.500000000000000, -1.097656250000000, -1.351562500000000,
+     -1.351562500000000, -1.097656250000000, 0.500000000000000, 2.097656250000000, 1.851562500000001,
+     1.000000000000000, 0.000000000000000, -2.000000000000000, 0.000000000000000, 1.000000000000000,
+     0.353553390593274, -0.618718433538229, 0.353553390593274, -0.088388347648318, 0,
+     0, -0.088388347648318, 0.353553390593274, -0.618718433538229, 0.353553390593274},
+    {2.102851867675782, 0, 0, 0, 0, 0, 0, 0, 0, 2.102851867675782, 0.683105468750000, -0.199707031250000,
+     -0.400390625000000, -0.199707031250000, 0.683105468750000, 0.353553390593274, -0.441941738241592,
+     0.353553390593274, -0.088388347648318, 0, 0, -0.088388347648318, 0.353553390593274, -0.441941738241592,
+     0.353553390593274},
+    {0.343750000000000, 0.156250000000000, 0.250000000000000, 0.918410174783309, -0.211303393596761,
+     0.312500000000000, 0.187500000000000, 0, -0.919791242715314, 0.212684461528766,
+     0.250000000000000, 0.250000000000000, -0.250000000000000, 0.353553390593274, 0.353553390593274,
+     0.187500000000000, 0.312500000000000, 0, 0.212684461528766, -0.919791242715314,
+     0.156250000000000, 0.343750000000000, 0.250000000000000, -0.211303393596761, 0.918410174783309},
+    {0.281250000000000, 0, 0, 0, 0, 0.312500000000000, 0.125000000000000, -1.000000000000000,
+     -1.980451414495135, 0.847975710251055, 0.234375000000000, 0.234375000000000, -1.500000000000000,
+     0.564856784190035, 0.564856784190035, 0.125000000000000, 0.312500000000000, -1.000000000000000,
+     0.847975710251055, -1.980451414495135, 0, 0.281250000000000, 0, 0, 0}};
+
+// forward reflection of pair k at a level of even length L (+ext): cuWT_CDF3_5_{n,d} / cuWT_CDF4_4_{n,d}
+template <int WAV>
+__device__ __forceinline__ void fwd_reflect(int k, int L, int bcd, int& ai, int& di, float& sa, float& sd) {
+    int a = 2 * k, d = 2 * k + 1;
+    float s_a = 1.f, s_d = 1.f;
+    if (WAV == WP_ID_CDF3_7) {
+        if (a < 0) { a = -1 - a; if (bcd) s_a = -1.f; }
+        else if (a >= L) { a = 2 * L - 1 - a; if (bcd) s_a = -1.f; }
+        if (d < 0) { d = -1 - d; if (bcd) s_d = -1.f; }
+        else if (d >= L) { d = 2 * L - 1 - d; if (bcd) s_d = -1.f; }
+    } else {
+        const int a0 = a;
+        if (a < 0) { a = -a; d = -d; if (bcd) { s_a = -1.f; s_d = -1.f; } }
+        else if (a >= L) { a = 2 * L - a; d = 2 * L - d; if (bcd) { s_a = -1.f; s_d = -1.f; } }
+        if (bcd && a0 == L) s_a = 1.f;
+    }
+    ai = a; di = d; sa = s_a; sd = s_d;
+}
+
+// inverse reflection of index k (a has L+ext entries, d has L): cuWT_CDF3_5_{n,d}_i / cuWT_CDF4_4_{n,d}_i
+template <int WAV>
+__device__ __forceinline__ void inv_reflect(int k, int L, int bcd, int& ai, int& di, float& sa, float& sd) {
+    int a = k, d = k;
+    float s_a = 1.f, s_d = 1.f;
+    if (WAV == WP_ID_CDF3_7) {
+        if (a < 0) { a = -1 - a; if (bcd) s_a = -1.f; else s_d = -1.f; }
+        else if (a >= L) { a = 2 * L - 1 - a; if (bcd) s_a = -1.f; else s_d = -1.f; }
+        d = a;
+    } else if (!bcd) {
+        if (a < 0) { a = -a; d = -d - 1; }
+        else if (a >= L) { a = 2 * L - a; d = 2 * L - d - 1; }
+    } else {
+        if (a < 0) { a = -a; d = -d - 1; s_d = -1.f; s_a = -1.f; }
+        else if (a >= L) { d = 2 * L - d - 1; s_d = -1.f; }
+        if (a > L) { a = 2 * L - a; s_a = -1.f; }
+    }
+    ai = a; di = d; sa = s_a; sd = s_d;
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+struct TileGeom {
+    long s_in;    // stride between consecutive lines of a tile
+    long s_out;   // stride of the outer line index
+    long pstride; // stride along the transform axis
+    int ni;       // lines along the inner index
+    int contiguous; // 1: lines are contiguous (y axis)
+};
+
+template <int WAV, bool FWD, typename T, int C>
+__global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src, T* __restrict__ dst, int N,
+                                                      int levels, int bcd, TileGeom g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    constexpr int CP = C + 1;
+    const int tid = threadIdx.x;
+    const int ext = N & 1;
+    const int i0 = blockIdx.x * C;
+    const long obase = (long)blockIdx.y * g.s_out;
+    T* buf[3] = {sm, sm + (size_t)N * CP, sm + 2 * (size_t)N * CP};
+
+    // ---- load the tile: C lines of N samples
+    if (g.contiguous) {
+        for (int i = tid; i < C * N; i += NT) {
+            int col = i / N, p = i - col * N;
+            T v = T(0);
+            if (i0 + col < g.ni) v = src[obase + (long)(i0 + col) * g.s_in + p];
+            buf[0][p * CP + col] = v;
+        }
+    } else {
+        for (int i = tid; i < C * N; i += NT) {
+            int col = i % C, p = i / C;
+            T v = T(0);
+            if (i0 + col < g.ni) v = src[obase + (long)(i0 + col) * g.s_in + (long)p * g.pstride];
+            buf[0][p * CP + col] = v;
+        }
+    }
+    __syncthreads();
+
+    const int nb = 4 + ext;
+    int outbuf;
+    if (FWD) {
+        int cur = 0;
+        for (int l = levels - 1; l >= 2; --l) {
+            const int L = 1 << (l + 1);
+            const int M = (L >> 1) + ext;
+            const int nd = L >> 1;
+            const int lim = L + ext - 1;
+            const T* S = buf[cur];
+            T* D = buf[cur ^ 1];
+            const int nch = (M + CH - 1) / CH;
+            for (int t = tid; t < C * nch; t += NT) {
+                const int col = t % C, k0 = (t / C) * CH;
+                T A[WIN], Dd[WIN];
+#pragma unroll
+                for (int w = 0; w < WIN; ++w) {
+                    int ai, di; float sa, sd;
+                    fwd_reflect<WAV>(k0 - 4 + w, L, bcd, ai, di, sa, sd);
+                    ai = clampi(ai, 0, lim);
+                    di = clampi(di, 0, lim);
+                    A[w] = T(sa) * S[ai * CP + col];
+                    Dd[w] = T(sd) * S[di * CP + col];
+                }
+                if (WAV == WP_ID_CDF3_7) {
+#pragma unroll
+                    for (int w = WIN - 1; w >= 1; --w) A[w] = A[w] + T(K37::fu1) * Dd[w - 1];
+#pragma unroll
+                    for (int w = 1; w < WIN - 1; ++w) Dd[w] = Dd[w] + T(K37::fp0) * A[w + 1] + T(K37::fp1) * A[w];
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4;
+                        T s = A[w] + T(K37::q6) * Dd[w - 3] + T(K37::q5) * Dd[w - 2] + T(K37::q4) * Dd[w - 1] +
+                              T(K37::q3) * Dd[w] + T(K37::q2) * Dd[w + 1] + T(K37::q1) * Dd[w + 2] +
+                              T(K37::q0) * Dd[w + 3];
+                        const int k = k0 + j;
+                        if (k < M) D[k * CP + col] = s * T(K37::scl0);
+                        if (k < nd) D[(M + k) * CP + col] = Dd[w] * T(K37::scl1);
+                    }
+                } else {
+#pragma unroll
+                    for (int w = WIN - 1; w >= 1; --w)
+                        A[w] = A[w] + T(K46::fu1_1) * Dd[w - 1] + T(K46::fu1_0) * Dd[w];
+#pragma unroll
+                    for (int w = 1; w < WIN - 1; ++w) Dd[w] = Dd[w] + T(K46::fp1) * A[w] + T(K46::fp0) * A[w + 1];
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4;
+                        T s = A[w] + T(K46::c5) * Dd[w - 3] + T(K46::c4) * Dd[w - 2] + T(K46::c3) * Dd[w - 1] +
+                              T(K46::c2) * Dd[w] + T(K46::c1) * Dd[w + 1] + T(K46::c0) * Dd[w + 2];
+                        const int k = k0 + j;
+                        if (k < M) D[k * CP + col] = s * T(K46::scl0);
+                        if (k < nd) D[(M + k) * CP + col] = Dd[w] * T(K46::scl1);
+                    }
+                }
+            }
+            __syncthreads();
+            cur ^= 1;
+        }
+        // base level: nb x nb matrix on the remaining approximation coefficients
+        const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[bcd] : c_base46[bcd];
+        if (tid < C) {
+            T a[5], o[5];
+            for (int i = 0; i < nb; ++i) a[i] = buf[cur][i * CP + tid];
+            for (int i = 0; i < nb; ++i) {
+                T s = T(0);
+                for (int j = 0; j < nb; ++j) s += T(mat[i * nb + j]) * a[j];
+                o[i] = s;
+            }
+            for (int i = 0; i < nb; ++i) buf[cur ^ 1][i * CP + tid] = o[i];
+        }
+        __syncthreads();
+        outbuf = -1;  // position dependent, resolved below
+    } else {
+        const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[2 + bcd] : c_base46[2 + bcd];
+        if (tid < C) {
+            T a[5], o[5];
+            for (int i = 0; i < nb; ++i) a[i] = buf[0][i * CP + tid];
+            for (int i = 0; i < nb; ++i) {
+                T s = T(0);
+                for (int j = 0; j < nb; ++j) s += T(mat[i * nb + j]) * a[j];
+                o[i] = s;
+            }
+            for (int i = 0; i < nb; ++i) buf[1][i * CP + tid] = o[i];
+        }
+        __syncthreads();
+        int cur = 1;
+        for (int l = 2; l < levels; ++l) {
+            const int L = 1 << l;
+            const int NA = L + ext;
+            const T* Sa = buf[cur];
+            const T* Sd = buf[0] + (size_t)NA * CP;
+            T* D = buf[3 - cur];
+            const int nch = (NA + CH - 1) / CH;
+            for (int t = tid; t < C * nch; t += NT) {
+                const int col = t % C, k0 = (t / C) * CH;
+                T A[WIN], Dd[WIN], SA[WIN], SD[WIN];
+#pragma unroll
+                for (int w = 0; w < WIN; ++w) {
+                    int ai, di; float sa, sd;
+                    inv_reflect<WAV>(k0 - 4 + w, L, bcd, ai, di, sa, sd);
+                    ai = clampi(ai, 0, NA - 1);
+                    di = clampi(di, 0, L - 1);
+                    A[w] = Sa[ai * CP + col];
+                    Dd[w] = Sd[di * CP + col];
+                    SA[w] = T(sa);
+                    SD[w] = T(sd);
+                }
+                if (WAV == WP_ID_CDF3_7) {
+#pragma unroll
+                    for (int w = 0; w < WIN; ++w) {
+                        A[w] = SA[w] * A[w] * T(K37::scl1);
+                        Dd[w] = SD[w] * Dd[w] * T(K37::scl0);
+                    }
+#pragma unroll
+                    for (int w = 3; w < WIN - 3; ++w)
+                        A[w] = A[w] - (T(K37::q6) * Dd[w - 3] + T(K37::q5) * Dd[w - 2] + T(K37::q4) * Dd[w - 1] +
+                                       T(K37::q3) * Dd[w] + T(K37::q2) * Dd[w + 1] + T(K37::q1) * Dd[w + 2] +
+                                       T(K37::q0) * Dd[w + 3]);
+#pragma unroll
+                    for (int w = 3; w < WIN - 4; ++w) Dd[w] = Dd[w] - (T(K37::fp1) * A[w] + T(K37::fp0) * A[w + 1]);
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4, k = k0 + j;
+                        const T av = A[w] - T(K37::fu1) * Dd[w - 1];
+                        if (k < NA) D[(2 * k) * CP + col] = av;
+                        if (k < L) D[(2 * k + 1) * CP + col] = Dd[w];
+                    }
+                } else {
+#pragma unroll
+                    for (int w = 0; w < WIN; ++w) {
+                        Dd[w] = SD[w] * Dd[w] * T(K46::scli1);
+                        A[w] = SA[w] * A[w] * T(K46::scli0);
+                    }
+#pragma unroll
+                    for (int w = 3; w < WIN - 2; ++w)
+                        A[w] = SA[w] * (A[w] - (T(K46::c5) * Dd[w - 3] + T(K46::c4) * Dd[w - 2] +
+                                                T(K46::c3) * Dd[w - 1] + T(K46::c2) * Dd[w] +
+                                                T(K46::c1) * Dd[w + 1] + T(K46::c0) * Dd[w + 2]));
+#pragma unroll
+                    for (int w = 0; w < WIN; ++w) Dd[w] = SD[w] * Dd[w];
+#pragma unroll
+                    for (int w = 3; w < WIN - 3; ++w)
+                        Dd[w] = SD[w] * (Dd[w] - (T(K46::fp1) * A[w] + T(K46::fp0) * A[w + 1]));
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4, k = k0 + j;
+                        const T av = A[w] - (T(K46::fu1_1) * Dd[w - 1] + T(K46::fu1_0) * Dd[w]);
+                        if (k < NA) D[(2 * k) * CP + col] = av;
+                        if (k < L) D[(2 * k + 1) * CP + col] = Dd[w];
+                    }
+                }
+            }
+            __syncthreads();
+            cur = 3 - cur;
+        }
+        outbuf = cur;
+    }
+
+    // ---- store the tile
+    const int basebuf = (levels - 1) & 1;
+    if (g.contiguous) {
+        for (int i = tid; i < C * N; i += NT) {
+            int col = i / N, p = i - col * N;
+            if (i0 + col >= g.ni) continue;
+            int b = outbuf;
+            if (b < 0) b = (p < nb) ? basebuf : ((levels - (31 - __clz(p - ext))) & 1);
+            dst[obase + (long)(i0 + col) * g.s_in + p] = buf[b][p * CP + col];
+        }
+    } else {
+        for (int i = tid; i < C * N; i += NT) {
+            int col = i % C, p = i / C;
+            if (i0 + col >= g.ni) continue;
+            int b = outbuf;
+            if (b < 0) b = (p < nb) ? basebuf : ((levels - (31 - __clz(p - ext))) & 1);
+            dst[obase + (long)(i0 + col) * g.s_in + (long)p * g.pstride] = buf[b][p * CP + col];
+        }
+    }
+}
+
+bool g_const_ready[64] = {false};
+
+cudaError_t ensure_constants() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && g_const_ready[dev]) return cudaSuccess;
+    double b37[4][16], b46[4][25];
+    memcpy(b37, h_base37, sizeof(b37));
+    memcpy(b46, h_base46, sizeof(b46));
+    // stored order: forward n, forward d, inverse n, inverse d
+    e = cudaMemcpyToSymbol(c_base37, b37, sizeof(b37));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_base46, b46, sizeof(b46));
+    if (e != cudaSuccess) return e;
+    if (dev < 64) g_const_ready[dev] = true;
+    return cudaSuccess;
+}
+
+template <int WAV, bool FWD, typename T, int C>
+cudaError_t launch_one(const T* src, T* dst, int N, int levels, int bcd, TileGeom g, int nouter, cudaStream_t s) {
+    const size_t smem = (size_t)(FWD ? 2 : 3) * N * (C + 1) * sizeof(T);
+    auto kern = dwt_tile_kernel<WAV, FWD, T, C>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((g.ni + C - 1) / C, nouter);
+    const int tok = wp_prof_start(s);
+    kern<<<grid, NT, smem, s>>>(src, dst, N, levels, bcd, g);
+    e = cudaGetLastError();
+    // algorithmic bytes: every element of the transformed array read once and written once
+    wp_prof_stop(tok, FWD ? "dwt_forward" : "dwt_inverse", 2.0 * sizeof(T) * N * (double)g.ni * nouter, s);
+    return e;
+}
+
+template <int WAV, bool FWD, typename T>
+cudaError_t launch_c(const T* src, T* dst, int N, int levels, int bcd, TileGeom g, int nouter, cudaStream_t s) {
+    // widest tile whose staging fits ~100 KB (two CTAs per SM) while keeping >= 2 CTAs per SM busy
+    const int nbuf = FWD ? 2 : 3;
+    int C = 32;
+    const long sms = wp_sm_count();
+    while (C > 4) {
+        const size_t smem = (size_t)nbuf * N * (C + 1) * sizeof(T);
+        const long ctas = (long)((g.ni + C - 1) / C) * nouter;
+        if (smem <= 100 * 1024 && ctas >= 2 * sms) break;
+        C >>= 1;
+    }
+    const size_t smem = (size_t)nbuf * N * (C + 1) * sizeof(T);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    switch (C) {
+        case 32: return launch_one<WAV, FWD, T, 32>(src, dst, N, levels, bcd, g, nouter, s);
+        case 16: return launch_one<WAV, FWD, T, 16>(src, dst, N, levels, bcd, g, nouter, s);
+        case 8: return launch_one<WAV, FWD, T, 8>(src, dst, N, levels, bcd, g, nouter, s);
+        default: return launch_one<WAV, FWD, T, 4>(src, dst, N, levels, bcd, g, nouter, s);
+    }
+}
+
+}  // namespace
+
+template <typename T>
+wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int levels, char axis, int wavelet,
+                             char bc, int forward, cudaStream_t stream) {
+    if (!dst || DX <= 0 || DY <= 0 || DZ <= 0) { wp_set_error_msg("wp_dwt1d: bad arguments"); return WP_ERR_INVALID_ARG; }
+    if (!src) src = dst;
+    if (wavelet != WP_ID_CDF3_7 && wavelet != WP_ID_CDF4_6) { wp_set_error_msg("wp_dwt1d: wavelet must be CDF3.7 or CDF4.6"); return WP_ERR_UNSUPPORTED; }
+    if (bc == 'z') bc = (wavelet == WP_ID_CDF3_7) ? 'd' : 'n';  // cuWHHDForward.cu:886-891, :970-975
+    if (bc != 'n' && bc != 'd') { wp_set_error_msg("wp_dwt1d: bc must be 'n', 'd' or 'z'"); return WP_ERR_INVALID_ARG; }
+    TileGeom g;
+    int N, nouter;
+    switch (axis) {
+        case 'y': case 'Y': N = DY; g.s_in = DY; g.ni = DX; g.s_out = (long)DX * DY; nouter = DZ; g.pstride = 1; g.contiguous = 1; break;
+        case 'x': case 'X': N = DX; g.s_in = 1; g.ni = DY; g.s_out = (long)DX * DY; nouter = DZ; g.pstride = DY; g.contiguous = 0; break;
+        case 'z': case 'Z': N = DZ; g.s_in = 1; g.ni = DY; g.s_out = DY; nouter = DX; g.pstride = (long)DX * DY; g.contiguous = 0; break;
+        default: wp_set_error_msg("wp_dwt1d: direction must be x, y or z"); return WP_ERR_INVALID_ARG;
+    }
+    const int ext = N & 1;
+    if (levels < 2 || levels > 12 || (1 << levels) != N - ext) {
+        wp_set_error_msg("wp_dwt1d: line length must be 2^levels (+1), levels in [2, 12]");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (nouter > 65535) { wp_set_error_msg("wp_dwt1d: outer extent too large"); return WP_ERR_UNSUPPORTED; }
+    WP_CUDA_TRY(ensure_constants());
+    const int bcd = (bc == 'd');
+    cudaError_t e;
+    if (wavelet == WP_ID_CDF3_7)
+        e = forward ? launch_c<WP_ID_CDF3_7, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF3_7, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    else
+        e = forward ? launch_c<WP_ID_CDF4_6, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF4_6, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    if (e != cudaSuccess) { wp_set_cuda_error(e, "dwt launch", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    return WP_OK;
+}
+
+template wp_status wp_dwt_axis_launch<float>(float*, const float*, int, int, int, int, char, int, char, int, cudaStream_t);
+template wp_status wp_dwt_axis_launch<double>(double*, const double*, int, int, int, int, char, int, char, int,
+                                              cudaStream_t);
+
+extern "C" CUWHHD_API wp_status wp_dwt1d(float* dst, const float* src, int dim_x, int dim_y, int dim_z, int levels,
+                                         char direction, char bc, int wavelet, int forward, void* stream) {
+    return wp_dwt_axis_launch<float>(dst, src, dim_x, dim_y, dim_z, levels, direction, wavelet, bc, forward,
+                                     (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_dwt1d_f64(double* dst, const double* src, int dim_x, int dim_y, int dim_z,
+                                             int levels, char direction, char bc, int wavelet, int forward,
+                                             void* stream) {
+    return wp_dwt_axis_launch<double>(dst, src, dim_x, dim_y, dim_z, levels, direction, wavelet, bc, forward,
+                                      (cudaStream_t)stream);
+}
+
+// ---- inner-product diagonal: inverse-transform the identity in FP64, sum squares per row
+namespace {
+__global__ void eye_kernel(double* m, int dim) {
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long n = (long)dim * dim;
+    if (i < n) m[i] = (i / dim == i % dim) ? 1.0 : 0.0;
+}
+__global__ void row_sumsq_kernel(const double* m, double* out, int dim) {
+    int row = blockIdx.x;
+    double s = 0.0;
+    for (int j = threadIdx.x; j < dim; j += blockDim.x) {
+        double v = m[(long)row * dim + j];
+        s += v * v;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[row] = red[0];
+}
+}  // namespace
+
+wp_status wp_ip_diag_device(double* d_out, int dim, int wavelet, char bc, cudaStream_t s) {
+    int levels = 0;
+    while ((2 << levels) <= dim) ++levels;
+    double* m = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&m, sizeof(double) * (size_t)dim * dim, s));
+    {
+        const int tok = wp_prof_start(s);
+        eye_kernel<<<wp_cdiv((size_t)dim * dim, 256), 256, 0, s>>>(m, dim);
+        wp_prof_stop(tok, "ip_identity", 8.0 * dim * dim, s);
+    }
+    wp_status st = wp_dwt_axis_launch<double>(m, m, dim, dim, 1, levels, 'y', wavelet, bc, 0, s);
+    if (st == WP_OK) {
+        const int tok = wp_prof_start(s);
+        row_sumsq_kernel<<<dim, 256, 0, s>>>(m, d_out, dim);
+        cudaError_t e = cudaGetLastError();
+        wp_prof_stop(tok, "ip_rowsumsq", 8.0 * dim * dim, s);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "row_sumsq", __FILE__, __LINE__); st = WP_ERR_CUDA; }
+    }
+    cudaFreeAsync(m, s);
+    return st;
+}
+
+extern "C" CUWHHD_API wp_status wp_ip_diag(double* out, int dim, int wavelet, char bc) {
+    if (!out || dim < 4) { wp_set_error_msg("wp_ip_diag: bad arguments"); return WP_ERR_INVALID_ARG; }
+    double* d = nullptr;
+    WP_CUDA_TRY(cudaMalloc((void**)&d, sizeof(double) * dim));
+    wp_status st = wp_ip_diag_device(d, dim, wavelet, bc, 0);
+    if (st == WP_OK) {
+        cudaError_t e = cudaMemcpy(out, d, sizeof(double) * dim, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "wp_ip_diag copy", __FILE__, __LINE__); st = WP_ERR_CUDA; }
+    }
+    cudaFree(d);
+    return st;
+}

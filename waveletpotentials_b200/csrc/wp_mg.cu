@@ -1,0 +1,770 @@
+// wp_mg.cu -- solid-aware (cut-cell) fractional multigrid for -div(a grad p) = f with zero-flux
+// walls, 3D and 2D, in FP32, FP64 and mixed precision (FP32 V-cycles inside FP64 iterative
+// refinement).
+//
+// Reference behaviour: CuMultigridFrac3D (cuMultigridFrac3D.cu:9-134 hierarchy, :249-327 V-cycle),
+// weighted Jacobi cuWjFrac3D_n (cuWeightedJacobi3D.cu:620-695), residual cuWjGetFracRes_3d_n
+// (:1107-1181), relative residual GetFracRhs (:1384-1407), coarsest 50-sweep solve
+// cuWjFrac3D_kernel_n (:1473-1545), cell restriction cuRestrict3D_p1_d{x,y,z} (cuRestrict3D.cu:801-970),
+// face-fraction coarsening SolveP1Ax/Ay/Az (:972-1145), piecewise-constant prolongation
+// cuProlongate3D_p1_* (cuProlongate3D.cu:353-424, 594-617), coarse spacing cuRestrictDx
+// (cuMultigridFrac2D.cu:4-17); 2D: CuMultigridFrac2D (cuMultigridFrac2D.cu:28-215, coarsest = 10
+// ordinary sweeps) and cuWeightedJacobi_frac_n (cuWeightedJacobi.cu:292-347).
+//
+// Operator: A v = sum_f cf (v - v_nb) over interior faces, cf = a_f * 2 / ((d_nb + d) d); a cell
+// whose diagonal is <= 1e-12 is fixed to 0.  Kernels: one sweep / fused prolongation+sweep /
+// fused residual+restriction per level (the reference uses 1 + 3 + 3 launches for the latter),
+// a single-CTA coarsest solve, and FP64 defect / norm kernels for the refinement loop.
+#include "wp_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace {
+
+constexpr double kEps = 1e-12;
+constexpr int kMaxLevels = 24;
+
+template <typename T>
+struct Lvl {
+    int nx, ny, nz;
+    const float* ax;
+    const float* ay;
+    const float* az;
+    const T* glo[3];  // per-axis factor of the lower face, 0 at the wall
+    const T* ghi[3];  // per-axis factor of the upper face, 0 at the wall
+    const double* d[3];
+};
+
+// diag and off-diagonal sum of row (x,y,z) applied to v (optionally plus the prolonged coarse
+// correction vc, i.e. v + P vc, piecewise constant)
+template <typename T, typename TV, bool PROL>
+__device__ __forceinline__ void row(const Lvl<T>& L, const TV* __restrict__ v, const TV* __restrict__ vc, int ncx,
+                                    int ncy, int x, int y, int z, T& diag, T& off, T& vcen) {
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const long sxy = (long)nx * ny;
+    const long i = y + (long)x * ny + z * sxy;
+    auto V = [&](int xx, int yy, int zz, long ii) -> T {
+        T r = (T)v[ii];
+        if (PROL) r += (T)vc[(yy >> 1) + (long)(xx >> 1) * ncy + (long)(zz >> 1) * ncx * ncy];
+        return r;
+    };
+    vcen = V(x, y, z, i);
+    const long iax = y + (long)x * ny + (long)z * (nx + 1) * ny;
+    const long iay = y + (long)x * (ny + 1) + (long)z * nx * (ny + 1);
+    T dg = 0, od = 0, cf;
+    if (y > 0) { cf = (T)L.ay[iay] * L.glo[1][y]; dg += cf; od -= cf * V(x, y - 1, z, i - 1); }
+    if (y < ny - 1) { cf = (T)L.ay[iay + 1] * L.ghi[1][y]; dg += cf; od -= cf * V(x, y + 1, z, i + 1); }
+    if (x > 0) { cf = (T)L.ax[iax] * L.glo[0][x]; dg += cf; od -= cf * V(x - 1, y, z, i - ny); }
+    if (x < nx - 1) { cf = (T)L.ax[iax + ny] * L.ghi[0][x]; dg += cf; od -= cf * V(x + 1, y, z, i + ny); }
+    if (z > 0) { cf = (T)L.az[i] * L.glo[2][z]; dg += cf; od -= cf * V(x, y, z - 1, i - sxy); }
+    if (z < nz - 1) { cf = (T)L.az[i + sxy] * L.ghi[2][z]; dg += cf; od -= cf * V(x, y, z + 1, i + sxy); }
+    diag = dg;
+    off = od;
+}
+
+template <typename T, bool PROL>
+__global__ void __launch_bounds__(256) jacobi_kernel(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ f,
+                                                     Lvl<T> L, T w, const T* __restrict__ vc, int ncx, int ncy) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= L.ny || x >= L.nx) return;
+    T dg, od, c;
+    row<T, T, PROL>(L, src, vc, ncx, ncy, x, y, z, dg, od, c);
+    const long i = y + (long)x * L.ny + (long)z * L.nx * L.ny;
+    dst[i] = dg > (T)kEps ? ((T)1 - w) * c + w * (f[i] - od) / dg : (T)0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) prolong_add_kernel(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny,
+                                                          int nz, int ncx, int ncy) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    v[y + (long)x * ny + (long)z * nx * ny] += vc[(y >> 1) + (long)(x >> 1) * ncy + (long)(z >> 1) * ncx * ncy];
+}
+
+// cell-centred trilinear prolongation added into the fine iterate (weights 3/4, 1/4 per axis,
+// the missing neighbour at a wall repeats the parent; 2D when nz == 1).  The reference's
+// piecewise-constant prolongation (cuProlongate3D.cu:594-617) with its averaging restriction gives
+// a coarse correction twice the Galerkin one (R A P = 2 A_coarse) and the V(2,2), omega = 2/3
+// cycle stalls and then diverges beyond 64^3; this prolongation restores h-independent convergence.
+template <typename T>
+__global__ void __launch_bounds__(256) prolong_tri_add_kernel(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny,
+                                                              int nz, int ncx, int ncy, int ncz) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    const int px = x >> 1, py = y >> 1, pz = z >> 1;
+    int qx = (x & 1) ? px + 1 : px - 1, qy = (y & 1) ? py + 1 : py - 1, qz = (z & 1) ? pz + 1 : pz - 1;
+    if (qx < 0 || qx >= ncx) qx = px;
+    if (qy < 0 || qy >= ncy) qy = py;
+    if (qz < 0 || qz >= ncz) qz = pz;
+    const long sc = (long)ncx * ncy;
+    auto C = [&](int xx, int yy, int zz) -> T { return vc[yy + (long)xx * ncy + zz * sc]; };
+    T acc;
+    const T a = (T)0.75, b = (T)0.25;
+    if (ncz == 1 && nz == 1) {
+        acc = a * (a * C(px, py, 0) + b * C(px, qy, 0)) + b * (a * C(qx, py, 0) + b * C(qx, qy, 0));
+    } else {
+        const T lo = a * (a * C(px, py, pz) + b * C(px, qy, pz)) + b * (a * C(qx, py, pz) + b * C(qx, qy, pz));
+        const T hi = a * (a * C(px, py, qz) + b * C(px, qy, qz)) + b * (a * C(qx, py, qz) + b * C(qx, qy, qz));
+        acc = a * lo + b * hi;
+    }
+    v[y + (long)x * ny + (long)z * nx * ny] += acc;
+}
+
+// coarse f = spacing-weighted average of the fine residuals of the (up to 8) children
+template <typename T>
+__global__ void __launch_bounds__(256) resid_restrict_kernel(T* __restrict__ fc, const T* __restrict__ v,
+                                                             const T* __restrict__ f, Lvl<T> L, int ncx, int ncy,
+                                                             int ncz) {
+    const int cy = blockIdx.x * 32 + threadIdx.x, cx = blockIdx.y * 8 + threadIdx.y, cz = blockIdx.z;
+    if (cy >= ncy || cx >= ncx) return;
+    T acc = 0;
+    double wsum[3];
+    int cnt[3];
+    const int c3[3] = {cx, cy, cz};
+    const int n3[3] = {L.nx, L.ny, L.nz};
+    for (int a = 0; a < 3; ++a) {
+        const int i0 = 2 * c3[a];
+        cnt[a] = (i0 + 1 < n3[a]) ? 2 : 1;
+        wsum[a] = L.d[a][i0] + (cnt[a] == 2 ? L.d[a][i0 + 1] : 0.0);
+    }
+    for (int cz2 = 0; cz2 < cnt[2]; ++cz2)
+        for (int cx2 = 0; cx2 < cnt[0]; ++cx2)
+            for (int cy2 = 0; cy2 < cnt[1]; ++cy2) {
+                const int x = 2 * cx + cx2, y = 2 * cy + cy2, z = 2 * cz + cz2;
+                T dg, od, c;
+                row<T, T, false>(L, v, nullptr, 0, 0, x, y, z, dg, od, c);
+                const long i = y + (long)x * L.ny + (long)z * L.nx * L.ny;
+                const T r = dg > (T)kEps ? f[i] - (dg * c + od) : (T)0;
+                const T wgt = (T)(L.d[0][x] / wsum[0] * (L.d[1][y] / wsum[1]) * (L.d[2][z] / wsum[2]));
+                acc += wgt * r;
+            }
+    fc[cy + (long)cx * ncy + (long)cz * ncx * ncy] = acc;
+}
+
+// coarsest level: `iters` weighted-Jacobi sweeps of the whole (small) grid inside one CTA
+template <typename T>
+__global__ void __launch_bounds__(1024) coarsest_kernel(T* __restrict__ v, const T* __restrict__ f, Lvl<T> L, T w,
+                                                        int iters) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* b0 = reinterpret_cast<T*>(smem_raw);
+    const int n = L.nx * L.ny * L.nz;
+    T* b1 = b0 + n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) b0[i] = v[i];
+    __syncthreads();
+    T* cur = b0;
+    T* nxt = b1;
+    for (int it = 0; it < iters; ++it) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int y = i % L.ny, x = (i / L.ny) % L.nx, z = i / (L.ny * L.nx);
+            T dg, od, c;
+            row<T, T, false>(L, cur, nullptr, 0, 0, x, y, z, dg, od, c);
+            nxt[i] = dg > (T)kEps ? ((T)1 - w) * c + w * (f[i] - od) / dg : (T)0;
+        }
+        __syncthreads();
+        T* t = cur; cur = nxt; nxt = t;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v[i] = cur[i];
+}
+
+// FP64 defect r = (f - m) - A p of an iterate p (float or double) on active cells (diag > eps),
+// where m is the mean of f over the active cells (0 keeps the reference's plain f - A p);
+// optional FP32 copy of r; adds sum r^2 into acc[0]
+template <typename TP>
+__global__ void __launch_bounds__(256) defect64_kernel(float* __restrict__ r32, const TP* __restrict__ p,
+                                                       const float* __restrict__ f, Lvl<double> L, double m,
+                                                       double* __restrict__ acc) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    double r = 0.0;
+    if (y < L.ny && x < L.nx) {
+        double dg, od, c;
+        row<double, TP, false>(L, p, nullptr, 0, 0, x, y, z, dg, od, c);
+        const long i = y + (long)x * L.ny + (long)z * L.nx * L.ny;
+        r = dg > kEps ? ((double)f[i] - m) - (dg * c + od) : 0.0;
+        if (r32) r32[i] = (float)r;
+    }
+    double s = r * r;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double red[8];
+    const int lane = threadIdx.x + 32 * threadIdx.y;
+    if ((lane & 31) == 0) red[lane >> 5] = s;
+    __syncthreads();
+    if (lane == 0) {
+        double t = 0.0;
+        for (int k = 0; k < 8; ++k) t += red[k];
+        atomicAdd(acc, t);
+    }
+}
+
+// sum of f and number of cells over the active cells (diag > eps) into acc[0], acc[1].  With zero-flux
+// walls the operator's null space is the constant on the active cells, so a right-hand side stored
+// in FP32 carries an incompatible constant part of FP32 rounding size that floors the residual
+// (about 2e-10 relative at 64^3); the tolerance-driven solve removes that mean in FP64.
+__global__ void __launch_bounds__(256) active_sum_kernel(const float* __restrict__ f, Lvl<double> L,
+                                                         double* __restrict__ acc) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    double sf = 0.0, cnt = 0.0;
+    if (y < L.ny && x < L.nx) {
+        double dg, od, c;
+        row<double, float, false>(L, f, nullptr, 0, 0, x, y, z, dg, od, c);
+        if (dg > kEps) { sf = (double)c; cnt = 1.0; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sf += __shfl_xor_sync(0xffffffffu, sf, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    }
+    __shared__ double red[2][8];
+    const int lane = threadIdx.x + 32 * threadIdx.y;
+    if ((lane & 31) == 0) { red[0][lane >> 5] = sf; red[1][lane >> 5] = cnt; }
+    __syncthreads();
+    if (lane == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < 8; ++k) { a += red[0][k]; b += red[1][k]; }
+        atomicAdd(acc, a);
+        atomicAdd(acc + 1, b);
+    }
+}
+
+// FP64 right-hand side of the compatible problem: f - m on active cells, 0 elsewhere
+__global__ void __launch_bounds__(256) rhs64_kernel(double* __restrict__ out, const float* __restrict__ f, Lvl<double> L,
+                                                    double m) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= L.ny || x >= L.nx) return;
+    double dg, od, c;
+    row<double, float, false>(L, f, nullptr, 0, 0, x, y, z, dg, od, c);
+    out[y + (long)x * L.ny + (long)z * L.nx * L.ny] = dg > kEps ? (double)c - m : 0.0;
+}
+
+template <typename TS>
+__global__ void __launch_bounds__(256) sumsq_kernel(const TS* __restrict__ a, long n, double* __restrict__ acc) {
+    double s = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double v = (double)a[i];
+        s += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+        atomicAdd(acc, t);
+    }
+}
+
+__global__ void add_correction_kernel(double* __restrict__ p, const float* __restrict__ e, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] += (double)e[i];
+}
+
+template <typename TD, typename TS>
+__global__ void convert_kernel(TD* __restrict__ d, const TS* __restrict__ s, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) d[i] = (TD)s[i];
+}
+
+// coarse face fractions: inject even faces along the face's own axis, average the (up to) two
+// children along the two others (cuRestrict3D.cu:972-1145)
+__global__ void coarsen_faces_kernel(float* __restrict__ dst, const float* __restrict__ src, int fnx, int fny, int fnz,
+                                     int cnx, int cny, int cnz, int axis) {
+    const int fe[3] = {fnx + (axis == 0), fny + (axis == 1), fnz + (axis == 2)};
+    const int ce[3] = {cnx + (axis == 0), cny + (axis == 1), cnz + (axis == 2)};
+    const long total = (long)ce[0] * ce[1] * ce[2];
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const int c[3] = {(int)((t / ce[1]) % ce[0]), (int)(t % ce[1]), (int)(t / ((long)ce[0] * ce[1]))};
+        int lo[3], cnt[3];
+        for (int a = 0; a < 3; ++a) {
+            if (a == axis) {
+                int s = 2 * c[a];
+                if ((fe[a] & 1) == 0 && c[a] == ce[a] - 1) s = 2 * c[a] - 1;
+                lo[a] = s;
+                cnt[a] = 1;
+            } else {
+                lo[a] = 2 * c[a];
+                cnt[a] = (2 * c[a] + 1 < fe[a]) ? 2 : 1;
+            }
+        }
+        float acc = 0.f;
+        const float wt = 1.f / (float)(cnt[0] * cnt[1] * cnt[2]);
+        for (int k = 0; k < cnt[2]; ++k)
+            for (int i = 0; i < cnt[0]; ++i)
+                for (int j = 0; j < cnt[1]; ++j)
+                    acc += src[(lo[1] + j) + (long)(lo[0] + i) * fe[1] + (long)(lo[2] + k) * fe[0] * fe[1]];
+        dst[c[1] + (long)c[0] * ce[1] + (long)c[2] * ce[0] * ce[1]] = acc * wt;
+    }
+}
+
+struct Level {
+    int n[3];
+    long cells;
+    float* frac[3];   // ax, ay, az (level-owned copies)
+    double* tab64;    // per axis: glo[n], ghi[n], d[n]
+    float* tab32;     // per axis: glo[n], ghi[n]
+    float *v, *t, *f; // FP32 work
+    double *v64, *t64, *f64;
+};
+
+template <typename T>
+Lvl<T> view(const Level& L);
+template <>
+Lvl<float> view<float>(const Level& L) {
+    Lvl<float> o;
+    o.nx = L.n[0]; o.ny = L.n[1]; o.nz = L.n[2];
+    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2];
+    long off64 = 0, off32 = 0;
+    for (int a = 0; a < 3; ++a) {
+        o.glo[a] = L.tab32 + off32;
+        o.ghi[a] = L.tab32 + off32 + L.n[a];
+        o.d[a] = L.tab64 + off64 + 2 * L.n[a];
+        off32 += 2 * L.n[a];
+        off64 += 3 * L.n[a];
+    }
+    return o;
+}
+template <>
+Lvl<double> view<double>(const Level& L) {
+    Lvl<double> o;
+    o.nx = L.n[0]; o.ny = L.n[1]; o.nz = L.n[2];
+    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2];
+    long off64 = 0;
+    for (int a = 0; a < 3; ++a) {
+        o.glo[a] = L.tab64 + off64;
+        o.ghi[a] = L.tab64 + off64 + L.n[a];
+        o.d[a] = L.tab64 + off64 + 2 * L.n[a];
+        off64 += 3 * L.n[a];
+    }
+    return o;
+}
+
+dim3 grid_of(int nx, int ny, int nz) { return dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz); }
+
+}  // namespace
+
+struct wp_mgfrac3d {
+    int dims;          // 2 or 3 (2D problems use nz = 1)
+    int last64;        // 0: none, 1: p64 (mixed), 2: lv[0].v64 (fp64) holds the last FP64 iterate
+    int nl;
+    Level lv[kMaxLevels];
+    int coarsest_iters;
+    double* acc;       // device reduction slots
+    double* p64;       // FP64 iterate for mixed precision
+    float* r32;        // FP32 defect (right-hand side of correction cycles)
+    const float* fin;  // finest right-hand side of the current solve
+    const double* fin64;
+};
+
+namespace {
+
+wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, const float* az, int nx, int ny, int nz,
+                          double dx, double dy, double dz, cudaStream_t s) {
+    int n[3] = {nx, ny, nz};
+    const int dims = h->dims;
+    auto mn = [&](const int* e) { return dims == 2 ? (e[0] < e[1] ? e[0] : e[1]) : std::min(e[0], std::min(e[1], e[2])); };
+    std::vector<double> hd[3];
+    hd[0].assign(nx, dx);
+    hd[1].assign(ny, dy);
+    hd[2].assign(nz, dz);
+    int nl = 0;
+    while (mn(n) > 1 && nl < kMaxLevels) {
+        Level& L = h->lv[nl];
+        for (int a = 0; a < 3; ++a) L.n[a] = n[a];
+        L.cells = (long)n[0] * n[1] * n[2];
+        const long fs[3] = {(long)(n[0] + 1) * n[1] * n[2], (long)n[0] * (n[1] + 1) * n[2],
+                            dims == 2 ? 1 : (long)n[0] * n[1] * (n[2] + 1)};
+        for (int a = 0; a < 3; ++a) WP_CUDA_TRY(cudaMalloc((void**)&L.frac[a], sizeof(float) * fs[a]));
+        if (nl == 0) {
+            WP_CUDA_TRY(cudaMemcpyAsync(L.frac[0], ax, sizeof(float) * fs[0], cudaMemcpyDeviceToDevice, s));
+            WP_CUDA_TRY(cudaMemcpyAsync(L.frac[1], ay, sizeof(float) * fs[1], cudaMemcpyDeviceToDevice, s));
+            if (dims == 3) WP_CUDA_TRY(cudaMemcpyAsync(L.frac[2], az, sizeof(float) * fs[2], cudaMemcpyDeviceToDevice, s));
+            else WP_CUDA_TRY(cudaMemsetAsync(L.frac[2], 0, sizeof(float), s));
+        } else {
+            const Level& F = h->lv[nl - 1];
+            for (int a = 0; a < dims; ++a) {
+                WP_KERNEL("coarsen_faces", 4.0 * 9 * fs[a], s,
+                          coarsen_faces_kernel<<<wp_cdiv(fs[a], 256) > 4096 ? 4096 : wp_cdiv(fs[a], 256), 256, 0, s>>>(
+                              L.frac[a], F.frac[a], F.n[0], F.n[1], F.n[2], n[0], n[1], n[2], a));
+            }
+            if (dims == 2) WP_CUDA_TRY(cudaMemsetAsync(L.frac[2], 0, sizeof(float), s));
+        }
+        // spacing tables; 2D problems have a single z layer with no z faces (tables all zero)
+        std::vector<double> t64;
+        std::vector<float> t32;
+        for (int a = 0; a < 3; ++a) {
+            const int m = n[a];
+            std::vector<double> lo(m, 0.0), hi(m, 0.0);
+            for (int i = 0; i < m; ++i) {
+                if (i > 0) lo[i] = 2.0 / ((hd[a][i - 1] + hd[a][i]) * hd[a][i]);
+                if (i < m - 1) hi[i] = 2.0 / ((hd[a][i + 1] + hd[a][i]) * hd[a][i]);
+            }
+            t64.insert(t64.end(), lo.begin(), lo.end());
+            t64.insert(t64.end(), hi.begin(), hi.end());
+            t64.insert(t64.end(), hd[a].begin(), hd[a].end());
+            for (double v : lo) t32.push_back((float)v);
+            for (double v : hi) t32.push_back((float)v);
+        }
+        WP_CUDA_TRY(cudaMalloc((void**)&L.tab64, sizeof(double) * t64.size()));
+        WP_CUDA_TRY(cudaMalloc((void**)&L.tab32, sizeof(float) * t32.size()));
+        WP_CUDA_TRY(cudaMemcpy(L.tab64, t64.data(), sizeof(double) * t64.size(), cudaMemcpyHostToDevice));
+        WP_CUDA_TRY(cudaMemcpy(L.tab32, t32.data(), sizeof(float) * t32.size(), cudaMemcpyHostToDevice));
+        WP_CUDA_TRY(cudaMalloc((void**)&L.v, sizeof(float) * L.cells));
+        WP_CUDA_TRY(cudaMalloc((void**)&L.t, sizeof(float) * L.cells));
+        WP_CUDA_TRY(cudaMalloc((void**)&L.f, sizeof(float) * L.cells));
+        WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * L.cells, s));
+        ++nl;
+        // next level: ceil halving, coarse spacing = sum of the two fine spacings (cuRestrictDx)
+        for (int a = 0; a < dims; ++a) {
+            const int m = wp_half_up(n[a]);
+            std::vector<double> c(m);
+            for (int i = 0; i < m; ++i) c[i] = hd[a][2 * i] + (2 * i + 1 < n[a] ? hd[a][2 * i + 1] : 0.0);
+            hd[a] = c;
+            n[a] = m;
+        }
+    }
+    h->nl = nl;
+    return WP_OK;
+}
+
+wp_status ensure_fp64(wp_mgfrac3d* h) {
+    for (int l = 0; l < h->nl; ++l) {
+        Level& L = h->lv[l];
+        if (L.v64) continue;
+        WP_CUDA_TRY(cudaMalloc((void**)&L.v64, sizeof(double) * L.cells));
+        WP_CUDA_TRY(cudaMalloc((void**)&L.t64, sizeof(double) * L.cells));
+        WP_CUDA_TRY(cudaMalloc((void**)&L.f64, sizeof(double) * L.cells));
+    }
+    return WP_OK;
+}
+
+template <typename T>
+struct Bufs;
+template <>
+struct Bufs<float> {
+    static float*& v(Level& L) { return L.v; }
+    static float*& t(Level& L) { return L.t; }
+    static float*& f(Level& L) { return L.f; }
+};
+template <>
+struct Bufs<double> {
+    static double*& v(Level& L) { return L.v64; }
+    static double*& t(Level& L) { return L.t64; }
+    static double*& f(Level& L) { return L.f64; }
+};
+
+template <typename T>
+wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s) {
+    const Lvl<T> V = view<T>(L);
+    const dim3 g = grid_of(L.n[0], L.n[1], L.n[2]);
+    for (int k = 0; k < sweeps; ++k) {
+        WP_KERNEL("jacobi", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
+                  jacobi_kernel<T, false><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::t(L), Bufs<T>::v(L), f, V, w, nullptr, 0, 0));
+        T* tmp = Bufs<T>::v(L);
+        Bufs<T>::v(L) = Bufs<T>::t(L);
+        Bufs<T>::t(L) = tmp;
+    }
+    return WP_OK;
+}
+
+template <typename T>
+wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int prolong, cudaStream_t s) {
+    Level& L = h->lv[l];
+    const dim3 g = grid_of(L.n[0], L.n[1], L.n[2]);
+    wp_status st;
+    if (l < h->nl - 1) {
+        if ((st = smooth<T>(L, f, nu1, w, s)) != WP_OK) return st;
+        Level& C = h->lv[l + 1];
+        WP_KERNEL("resid_restrict", (double)L.cells * (2.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
+                  resid_restrict_kernel<T><<<grid_of(C.n[0], C.n[1], C.n[2]), dim3(32, 8), 0, s>>>(
+                      Bufs<T>::f(C), Bufs<T>::v(L), f, view<T>(L), C.n[0], C.n[1], C.n[2]));
+        WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(C), 0, sizeof(T) * C.cells, s));
+        if ((st = vcycle<T>(h, l + 1, Bufs<T>::f(C), nu1, nu2, w, prolong, s)) != WP_OK) return st;
+        if (prolong == WP_PROLONG_TRILINEAR) {
+            WP_KERNEL("prolong_trilinear", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
+                      prolong_tri_add_kernel<T><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::v(L), Bufs<T>::v(C), L.n[0], L.n[1],
+                                                                         L.n[2], C.n[0], C.n[1], C.n[2]));
+            if ((st = smooth<T>(L, f, nu2, w, s)) != WP_OK) return st;
+        } else if (nu2 > 0) {
+            // first post-sweep reads v + P vc directly (prolongation fused into the sweep)
+            WP_KERNEL("jacobi_prolong", (double)L.cells * (3.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
+                      jacobi_kernel<T, true><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::t(L), Bufs<T>::v(L), f, view<T>(L), w,
+                                                                       Bufs<T>::v(C), C.n[0], C.n[1]));
+            T* tmp = Bufs<T>::v(L);
+            Bufs<T>::v(L) = Bufs<T>::t(L);
+            Bufs<T>::t(L) = tmp;
+            if ((st = smooth<T>(L, f, nu2 - 1, w, s)) != WP_OK) return st;
+        } else {
+            WP_KERNEL("prolong_constant", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
+                      prolong_add_kernel<T><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::v(L), Bufs<T>::v(C), L.n[0], L.n[1],
+                                                                     L.n[2], C.n[0], C.n[1]));
+        }
+    } else {
+        const size_t smem = 2 * sizeof(T) * L.cells;
+        if (smem <= 200 * 1024) {
+            auto k = coarsest_kernel<T>;
+            WP_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            WP_KERNEL("coarsest", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
+                      k<<<1, 1024, smem, s>>>(Bufs<T>::v(L), f, view<T>(L), w, h->coarsest_iters));
+        } else {
+            if ((st = smooth<T>(L, f, h->coarsest_iters, w, s)) != WP_OK) return st;
+        }
+    }
+    return WP_OK;
+}
+
+// mean of f over the active cells of the finest level (synchronous)
+wp_status active_mean(wp_mgfrac3d* h, const float* f, double* m, cudaStream_t s) {
+    Level& L = h->lv[0];
+    WP_CUDA_TRY(cudaMemsetAsync(h->acc + 2, 0, 2 * sizeof(double), s));
+    WP_KERNEL("active_sum", (double)L.cells * 16.0, s,
+              active_sum_kernel<<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(f, view<double>(L), h->acc + 2));
+    double hv[2];
+    WP_CUDA_TRY(cudaMemcpyAsync(hv, h->acc + 2, sizeof(hv), cudaMemcpyDeviceToHost, s));
+    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    *m = hv[1] > 0 ? hv[0] / hv[1] : 0.0;
+    return WP_OK;
+}
+
+template <typename TP>
+wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r32, double* norm_r2,
+                 double* norm_f2, cudaStream_t s) {
+    Level& L = h->lv[0];
+    WP_CUDA_TRY(cudaMemsetAsync(h->acc, 0, 2 * sizeof(double), s));
+    WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 16.0 + (r32 ? 4.0 : 0.0)), s,
+              defect64_kernel<TP><<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(r32, p, f, view<double>(L),
+                                                                                         m, h->acc));
+    if (norm_f2) {
+        const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
+        WP_KERNEL("sumsq", 4.0 * L.cells, s, sumsq_kernel<float><<<b, 256, 0, s>>>(f, L.cells, h->acc + 1));
+    }
+    double hv[2];
+    WP_CUDA_TRY(cudaMemcpyAsync(hv, h->acc, sizeof(hv), cudaMemcpyDeviceToHost, s));
+    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    *norm_r2 = hv[0];
+    if (norm_f2) *norm_f2 = hv[1];
+    return WP_OK;
+}
+
+void destroy_levels(wp_mgfrac3d* h) {
+    for (int l = 0; l < kMaxLevels; ++l) {
+        Level& L = h->lv[l];
+        for (int a = 0; a < 3; ++a) if (L.frac[a]) cudaFree(L.frac[a]);
+        void* ps[] = {L.tab64, L.tab32, L.v, L.t, L.f, L.v64, L.t64, L.f64};
+        for (void* p : ps) if (p) cudaFree(p);
+    }
+    if (h->acc) cudaFree(h->acc);
+    if (h->p64) cudaFree(h->p64);
+    if (h->r32) cudaFree(h->r32);
+}
+
+wp_status create_common(wp_mgfrac3d** out, int dims, const float* ax, const float* ay, const float* az, int nx, int ny,
+                        int nz, double dx, double dy, double dz, char bc, cudaStream_t s) {
+    if (!out) { wp_set_error_msg("wp_mgfrac_create: null handle"); return WP_ERR_INVALID_ARG; }
+    *out = nullptr;
+    if (!ax || !ay || (dims == 3 && !az) || nx < 2 || ny < 2 || (dims == 3 && nz < 2) || nz > 65535 ||
+        !(dx > 0) || !(dy > 0) || !(dz > 0)) {
+        wp_set_error_msg("wp_mgfrac_create: bad arguments (extents >= 2, spacings > 0, fraction pointers)");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (bc != 'n') { wp_set_error_msg("wp_mgfrac_create: only bc 'n' (zero-flux walls) is implemented"); return WP_ERR_UNSUPPORTED; }
+    wp_mgfrac3d* h = new (std::nothrow) wp_mgfrac3d();
+    if (!h) return WP_ERR_INVALID_ARG;
+    h->dims = dims;
+    h->coarsest_iters = dims == 3 ? 50 : 10;
+    wp_status st = build_hierarchy(h, ax, ay, az, nx, ny, nz, dx, dy, dz, s);
+    if (st == WP_OK) {
+        cudaError_t e = cudaMalloc((void**)&h->acc, 4 * sizeof(double));
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "mg create", __FILE__, __LINE__); st = WP_ERR_CUDA; }
+    }
+    if (st != WP_OK) { destroy_levels(h); delete h; return st; }
+    *out = h;
+    return WP_OK;
+}
+
+wp_status solve_fixed(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f, int n_iters, int nu1, int nu2,
+                      double weight, cudaStream_t s) {
+    if (!h || !dst || !f || n_iters < 0 || nu1 < 0 || nu2 < 0) { wp_set_error_msg("wp_mgfrac_solve: bad arguments"); return WP_ERR_INVALID_ARG; }
+    Level& L = h->lv[0];
+    if (pre_v) WP_CUDA_TRY(cudaMemcpyAsync(L.v, pre_v, sizeof(float) * L.cells, cudaMemcpyDeviceToDevice, s));
+    else WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * L.cells, s));
+    for (int c = 0; c < n_iters; ++c) {
+        wp_status st = vcycle<float>(h, 0, f, nu1, nu2, (float)weight, WP_PROLONG_CONSTANT, s);
+        if (st != WP_OK) return st;
+    }
+    WP_CUDA_TRY(cudaMemcpyAsync(dst, L.v, sizeof(float) * L.cells, cudaMemcpyDeviceToDevice, s));
+    return WP_OK;
+}
+
+wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f, const wp_mg_params* prm,
+                    wp_mg_report* rep, cudaStream_t s) {
+    if (!h || !dst || !f || !prm || prm->max_cycles < 0 || prm->nu1 < 0 || prm->nu2 < 0 ||
+        (prm->prolongation != WP_PROLONG_CONSTANT && prm->prolongation != WP_PROLONG_TRILINEAR)) {
+        wp_set_error_msg("wp_mgfrac_solve_tol: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    Level& L = h->lv[0];
+    const long n = L.cells;
+    const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
+    wp_mg_report r;
+    memset(&r, 0, sizeof(r));
+    double nr2 = 0.0, nf2 = 0.0, m = 0.0;
+    wp_status st = active_mean(h, f, &m, s);
+    if (st != WP_OK) return st;
+    const bool use_tol = prm->rel_tol > 0.0;
+    if (prm->precision == WP_PREC_FP32 || prm->precision == WP_PREC_FP64) {
+        const bool f64 = prm->precision == WP_PREC_FP64;
+        if (f64) {
+            if ((st = ensure_fp64(h)) != WP_OK) return st;
+            WP_KERNEL("rhs64", 28.0 * n, s,
+                      rhs64_kernel<<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(L.f64, f, view<double>(L), m));
+            if (pre_v) WP_KERNEL("convert", 12.0 * n, s, convert_kernel<double, float><<<cb, 256, 0, s>>>(L.v64, pre_v, n));
+            else WP_CUDA_TRY(cudaMemsetAsync(L.v64, 0, sizeof(double) * n, s));
+        } else {
+            if (pre_v) WP_CUDA_TRY(cudaMemcpyAsync(L.v, pre_v, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+            else WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
+        }
+        if (f64) st = defect<double>(h, L.v64, f, m, nullptr, &nr2, &nf2, s);
+        else st = defect<float>(h, L.v, f, m, nullptr, &nr2, &nf2, s);
+        if (st != WP_OK) return st;
+        if (!(nf2 > 0.0)) nf2 = 1.0;
+        double rel = std::sqrt(nr2 / nf2);
+        while (!(use_tol && rel <= prm->rel_tol) && r.cycles < prm->max_cycles) {
+            st = f64 ? vcycle<double>(h, 0, L.f64, prm->nu1, prm->nu2, prm->omega, prm->prolongation, s)
+                     : vcycle<float>(h, 0, f, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+            if (st != WP_OK) return st;
+            if (f64) st = defect<double>(h, L.v64, f, m, nullptr, &nr2, nullptr, s);
+            else st = defect<float>(h, L.v, f, m, nullptr, &nr2, nullptr, s);
+            if (st != WP_OK) return st;
+            rel = std::sqrt(nr2 / nf2);
+            if (r.cycles < 64) r.history[r.cycles] = rel;
+            ++r.cycles;
+            if (!std::isfinite(rel)) break;
+        }
+        r.rel_residual = rel;
+        h->last64 = f64 ? 2 : 0;
+        if (f64) WP_KERNEL("convert", 12.0 * n, s, convert_kernel<float, double><<<cb, 256, 0, s>>>(dst, L.v64, n));
+        else WP_CUDA_TRY(cudaMemcpyAsync(dst, L.v, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+    } else if (prm->precision == WP_PREC_MIXED) {
+        if (!h->p64) WP_CUDA_TRY(cudaMalloc((void**)&h->p64, sizeof(double) * n));
+        if (!h->r32) WP_CUDA_TRY(cudaMalloc((void**)&h->r32, sizeof(float) * n));
+        if (pre_v) WP_KERNEL("convert", 12.0 * n, s, convert_kernel<double, float><<<cb, 256, 0, s>>>(h->p64, pre_v, n));
+        else WP_CUDA_TRY(cudaMemsetAsync(h->p64, 0, sizeof(double) * n, s));
+        if ((st = defect<double>(h, h->p64, f, m, h->r32, &nr2, &nf2, s)) != WP_OK) return st;
+        if (!(nf2 > 0.0)) nf2 = 1.0;
+        double rel = std::sqrt(nr2 / nf2);
+        while (!(use_tol && rel <= prm->rel_tol) && r.cycles < prm->max_cycles) {
+            // one FP32 V-cycle on the FP32 defect from a zero start, FP64 update, FP64 defect
+            WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
+            if ((st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s)) !=
+                WP_OK)
+                return st;
+            WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+            if ((st = defect<double>(h, h->p64, f, m, h->r32, &nr2, nullptr, s)) != WP_OK) return st;
+            rel = std::sqrt(nr2 / nf2);
+            if (r.cycles < 64) r.history[r.cycles] = rel;
+            ++r.cycles;
+            if (!std::isfinite(rel)) break;
+        }
+        r.rel_residual = rel;
+        h->last64 = 1;
+        WP_KERNEL("convert", 12.0 * n, s, convert_kernel<float, double><<<cb, 256, 0, s>>>(dst, h->p64, n));
+    } else {
+        wp_set_error_msg("wp_mgfrac_solve_tol: unknown precision mode");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (rep) *rep = r;
+    if (!std::isfinite(r.rel_residual)) { wp_set_error_msg("multigrid: non-finite residual"); return WP_ERR_NONFINITE; }
+    if (use_tol && r.rel_residual > prm->rel_tol) { wp_set_error_msg("multigrid: cycle cap reached before tolerance"); return WP_ERR_NOT_CONVERGED; }
+    return WP_OK;
+}
+
+wp_status residual_rel(wp_mgfrac3d* h, const float* v, const float* f, double* rel, cudaStream_t s) {
+    if (!h || !v || !f || !rel) { wp_set_error_msg("wp_mgfrac_residual: null pointer"); return WP_ERR_INVALID_ARG; }
+    double nr2 = 0.0, nf2 = 0.0;
+    wp_status st = defect<float>(h, v, f, 0.0, nullptr, &nr2, &nf2, s);
+    if (st != WP_OK) return st;
+    *rel = std::sqrt(nr2) / std::sqrt(nf2);
+    return WP_OK;
+}
+
+}  // namespace
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_create(wp_mgfrac3d** h, const float* ax, const float* ay, const float* az,
+                                                   int nx, int ny, int nz, double dx, double dy, double dz, char bc,
+                                                   void* stream) {
+    return create_common(h, 3, ax, ay, az, nx, ny, nz, dx, dy, dz, bc, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_solve(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f,
+                                                  int n_iters, int nu1, int nu2, double weight, void* stream) {
+    return solve_fixed(h, dst, pre_v, f, n_iters, nu1, nu2, weight, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f,
+                                                      const wp_mg_params* params, wp_mg_report* report, void* stream) {
+    return solve_tol(h, dst, pre_v, f, params, report, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_residual(wp_mgfrac3d* h, const float* v, const float* f, double* rel,
+                                                     void* stream) {
+    return residual_rel(h, v, f, rel, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_iterate64(wp_mgfrac3d* h, double* dst, void* stream) {
+    if (!h || !dst || h->last64 == 0) { wp_set_error_msg("wp_mgfrac3d_iterate64: no FP64 iterate available"); return WP_ERR_INVALID_ARG; }
+    const double* src = h->last64 == 1 ? h->p64 : h->lv[0].v64;
+    WP_CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * h->lv[0].cells, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_destroy(wp_mgfrac3d* h) {
+    if (!h) return WP_OK;
+    destroy_levels(h);
+    delete h;
+    return WP_OK;
+}
+
+// 2D shares the implementation: a single z layer with no z faces
+struct wp_mgfrac2d {
+    wp_mgfrac3d* impl;
+};
+
+extern "C" CUWHHD_API wp_status wp_mgfrac2d_create(wp_mgfrac2d** h, const float* ax, const float* ay, int nx, int ny,
+                                                   double dx, double dy, char bc, void* stream) {
+    if (!h) { wp_set_error_msg("wp_mgfrac2d_create: null handle"); return WP_ERR_INVALID_ARG; }
+    *h = nullptr;
+    wp_mgfrac3d* impl = nullptr;
+    wp_status st = create_common(&impl, 2, ax, ay, nullptr, nx, ny, 1, dx, dy, 1.0, bc, (cudaStream_t)stream);
+    if (st != WP_OK) return st;
+    wp_mgfrac2d* o = new (std::nothrow) wp_mgfrac2d();
+    if (!o) { wp_mgfrac3d_destroy(impl); return WP_ERR_INVALID_ARG; }
+    o->impl = impl;
+    *h = o;
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac2d_solve(wp_mgfrac2d* h, float* dst, const float* pre_v, const float* f,
+                                                  int n_iters, int nu1, int nu2, double weight, void* stream) {
+    if (!h) return WP_ERR_INVALID_ARG;
+    return solve_fixed(h->impl, dst, pre_v, f, n_iters, nu1, nu2, weight, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac2d_solve_tol(wp_mgfrac2d* h, float* dst, const float* pre_v, const float* f,
+                                                      const wp_mg_params* params, wp_mg_report* report, void* stream) {
+    if (!h) return WP_ERR_INVALID_ARG;
+    return solve_tol(h->impl, dst, pre_v, f, params, report, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac2d_residual(wp_mgfrac2d* h, const float* v, const float* f, double* rel,
+                                                     void* stream) {
+    if (!h) return WP_ERR_INVALID_ARG;
+    return residual_rel(h->impl, v, f, rel, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac2d_destroy(wp_mgfrac2d* h) {
+    if (!h) return WP_OK;
+    wp_mgfrac3d_destroy(h->impl);
+    delete h;
+    return WP_OK;
+}

@@ -1,0 +1,303 @@
+// wp_ops.cu -- field operators around the solver: divergence, gradient update, max-abs, solid
+// level sets and face fractions (3D and 2D).
+//
+// Reference behaviour: cuGetB_vel_frac_3d(_n) (cuConvergence.cu:40-122; the _n variant computes a
+// boundary term it never uses, so both return b = -div(a u)), cuGetB_vel_frac_2d (:483-530),
+// cuGradient3D_frac_p_n (cuGradient.cu:1841-1891) followed by CudaMatAdd(-1) / CudaMatMul(a)
+// (TestLocalProjection.cpp:672-680), CudaFindMaxValue (cudaMath.cu:1269-1280), cuInitLsSphere /
+// cuComputeFrac / cuGetAx,Ay,Az (cuSolidLevelSet3D.cu:11-90).
+// All kernels map threadIdx.x to y (the contiguous index) so every access is coalesced.
+#include "wp_common.cuh"
+
+#include <cstring>
+#include <vector>
+
+namespace {
+
+constexpr float kEps = 1e-12f;
+
+// FRAC = false treats every face as fully open (a = 1): the divergence of an already a-weighted field
+template <bool FRAC>
+__global__ void __launch_bounds__(256) div3d_kernel(float* __restrict__ b, const float* __restrict__ xv,
+                                                    const float* __restrict__ yv, const float* __restrict__ zv,
+                                                    const float* __restrict__ ax, const float* __restrict__ ay,
+                                                    const float* __restrict__ az, int nx, int ny, int nz, float dxi,
+                                                    float dyi, float dzi) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    const long sxv = (long)(nx + 1) * ny, syv = (long)nx * (ny + 1), szv = (long)nx * ny;
+    const long ix = y + (long)x * ny + z * sxv, iy = y + (long)x * (ny + 1) + z * syv, iz = y + (long)x * ny + z * szv;
+    float v;
+    if (FRAC)
+        v = (xv[ix + ny] * ax[ix + ny] - xv[ix] * ax[ix]) * dxi + (yv[iy + 1] * ay[iy + 1] - yv[iy] * ay[iy]) * dyi +
+            (zv[iz + szv] * az[iz + szv] - zv[iz] * az[iz]) * dzi;
+    else
+        v = (xv[ix + ny] - xv[ix]) * dxi + (yv[iy + 1] - yv[iy]) * dyi + (zv[iz + szv] - zv[iz]) * dzi;
+    b[iz] = -v;
+}
+
+__global__ void __launch_bounds__(256) div2d_kernel(float* __restrict__ b, const float* __restrict__ xv,
+                                                    const float* __restrict__ yv, const float* __restrict__ ax,
+                                                    const float* __restrict__ ay, int nx, int ny, float dxi, float dyi) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
+    if (y >= ny || x >= nx) return;
+    const long ix = y + (long)x * ny, iy = y + (long)x * (ny + 1);
+    b[ix] = -((xv[ix + ny] * ax[ix + ny] - xv[ix] * ax[ix]) * dxi + (yv[iy + 1] * ay[iy + 1] - yv[iy] * ay[iy]) * dyi);
+}
+
+// u <- (u - grad p) [* a] on all faces; grad p = 0 on wall faces and where a <= eps
+__global__ void __launch_bounds__(256) grad3d_kernel(float* __restrict__ xv, float* __restrict__ yv, float* __restrict__ zv,
+                                                     const float* __restrict__ p, const float* __restrict__ ax,
+                                                     const float* __restrict__ ay, const float* __restrict__ az,
+                                                     int nx, int ny, int nz, float gx, float gy, float gz, int mul) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    const long sp = (long)nx * ny;
+    // x faces: (x in [0,nx], y in [0,ny), z in [0,nz))
+    if (y < ny && x <= nx && z < nz) {
+        const long i = y + (long)x * ny + (long)z * (nx + 1) * ny;
+        const float a = ax[i];
+        float g = 0.f;
+        if (x > 0 && x < nx && a > kEps) {
+            const long ip = y + (long)x * ny + z * sp;
+            g = (p[ip] - p[ip - ny]) * gx;
+        }
+        float u = xv[i] - g;
+        xv[i] = mul ? u * a : u;
+    }
+    if (y <= ny && x < nx && z < nz) {
+        const long i = y + (long)x * (ny + 1) + (long)z * nx * (ny + 1);
+        const float a = ay[i];
+        float g = 0.f;
+        if (y > 0 && y < ny && a > kEps) {
+            const long ip = y + (long)x * ny + z * sp;
+            g = (p[ip] - p[ip - 1]) * gy;
+        }
+        float u = yv[i] - g;
+        yv[i] = mul ? u * a : u;
+    }
+    if (y < ny && x < nx && z <= nz) {
+        const long i = y + (long)x * ny + (long)z * sp;
+        const float a = az[i];
+        float g = 0.f;
+        if (z > 0 && z < nz && a > kEps) g = (p[i] - p[i - sp]) * gz;
+        float u = zv[i] - g;
+        zv[i] = mul ? u * a : u;
+    }
+}
+
+__global__ void __launch_bounds__(256) grad2d_kernel(float* __restrict__ xv, float* __restrict__ yv, const float* __restrict__ p,
+                                                     const float* __restrict__ ax, const float* __restrict__ ay, int nx,
+                                                     int ny, float gx, float gy, int mul) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
+    if (y < ny && x <= nx) {
+        const long i = y + (long)x * ny;
+        const float a = ax[i];
+        float g = 0.f;
+        if (x > 0 && x < nx && a > kEps) g = (p[i] - p[i - ny]) * gx;
+        float u = xv[i] - g;
+        xv[i] = mul ? u * a : u;
+    }
+    if (y <= ny && x < nx) {
+        const long i = y + (long)x * (ny + 1);
+        const float a = ay[i];
+        float g = 0.f;
+        if (y > 0 && y < ny && a > kEps) {
+            const long ip = y + (long)x * ny;
+            g = (p[ip] - p[ip - 1]) * gy;
+        }
+        float u = yv[i] - g;
+        yv[i] = mul ? u * a : u;
+    }
+}
+
+// max |x|: non-negative floats order like their bit patterns
+__global__ void __launch_bounds__(256) maxabs_kernel(const float* __restrict__ x, size_t n, unsigned int* out) {
+    float m = 0.f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float v = fabsf(x[i]);
+        m = (v > m || v != v) ? v : m;  // NaN propagates
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        float t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (t > m || t != t) ? t : m;
+    }
+    __shared__ float red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = (red[w] > m || red[w] != red[w]) ? red[w] : m;
+        atomicMax(out, __float_as_uint(m));
+    }
+}
+
+struct Sphere {
+    float c[3];
+    float r;
+};
+
+__global__ void __launch_bounds__(256) sdf_spheres_kernel(float* __restrict__ sdf, int nx, int ny, int nz, float h,
+                                                          const Sphere* __restrict__ sp, int count) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    const float px = (x + 0.5f) * h, py = (y + 0.5f) * h, pz = (z + 0.5f) * h;
+    float best = 1e30f;
+    for (int s = 0; s < count; ++s) {
+        const float dx = px - sp[s].c[0], dy = py - sp[s].c[1], dz = pz - sp[s].c[2];
+        best = fminf(best, sqrtf(dx * dx + dy * dy + dz * dz) - sp[s].r);
+    }
+    sdf[y + (long)x * ny + (long)z * nx * ny] = best;
+}
+
+__device__ __forceinline__ float frac_from_ls(float h, float l, float r) {
+    const float dif = r - l;
+    const float d = sqrtf(fmaxf(h * h - dif * dif, 1e-14f));
+    return 1.f - fminf(fmaxf((1.f - (r + l) / d) * 0.5f, 0.f), 1.f);
+}
+
+__global__ void __launch_bounds__(256) frac3d_kernel(float* __restrict__ ax, float* __restrict__ ay, float* __restrict__ az,
+                                                     const float* __restrict__ ls, int nx, int ny, int nz, float h) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    const long s = (long)nx * ny;
+    if (y < ny && x <= nx && z < nz) {
+        const int xl = max(x - 1, 0), xr = min(x, nx - 1);
+        ax[y + (long)x * ny + (long)z * (nx + 1) * ny] = frac_from_ls(h, ls[y + (long)xl * ny + z * s], ls[y + (long)xr * ny + z * s]);
+    }
+    if (y <= ny && x < nx && z < nz) {
+        const int yl = max(y - 1, 0), yr = min(y, ny - 1);
+        ay[y + (long)x * (ny + 1) + (long)z * nx * (ny + 1)] = frac_from_ls(h, ls[yl + (long)x * ny + z * s], ls[yr + (long)x * ny + z * s]);
+    }
+    if (y < ny && x < nx && z <= nz) {
+        const int zl = max(z - 1, 0), zr = min(z, nz - 1);
+        az[y + (long)x * ny + (long)z * s] = frac_from_ls(h, ls[y + (long)x * ny + zl * s], ls[y + (long)x * ny + zr * s]);
+    }
+}
+
+}  // namespace
+
+extern "C" CUWHHD_API wp_status wp_divergence_frac3d(float* b, const float* xv, const float* yv, const float* zv,
+                                                     const float* ax, const float* ay, const float* az, int nx, int ny,
+                                                     int nz, double dx, double dy, double dz, void* stream) {
+    const bool frac = ax || ay || az;
+    if (!b || !xv || !yv || !zv || (frac && (!ax || !ay || !az)) || nx <= 0 || ny <= 0 || nz <= 0 || nz > 65535) {
+        wp_set_error_msg("wp_divergence_frac3d: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    dim3 grid(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz);
+    const float dxi = (float)(1.0 / dx), dyi = (float)(1.0 / dy), dzi = (float)(1.0 / dz);
+    cudaStream_t s = (cudaStream_t)stream;
+    const double faces = (double)(nx + 1) * ny * nz * 3, cells = (double)nx * ny * nz;
+    if (frac)
+        WP_KERNEL("divergence", 4.0 * (2 * faces + cells), s,
+                  div3d_kernel<true><<<grid, dim3(32, 8), 0, s>>>(b, xv, yv, zv, ax, ay, az, nx, ny, nz, dxi, dyi, dzi));
+    else
+        WP_KERNEL("divergence", 4.0 * (faces + cells), s,
+                  div3d_kernel<false><<<grid, dim3(32, 8), 0, s>>>(b, xv, yv, zv, ax, ay, az, nx, ny, nz, dxi, dyi, dzi));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_divergence_frac2d(float* b, const float* xv, const float* yv, const float* ax,
+                                                     const float* ay, int nx, int ny, double dx, double dy, void* stream) {
+    if (!b || !xv || !yv || !ax || !ay || nx <= 0 || ny <= 0) { wp_set_error_msg("wp_divergence_frac2d: bad arguments"); return WP_ERR_INVALID_ARG; }
+    dim3 grid(wp_cdiv(ny, 32), wp_cdiv(nx, 8));
+    cudaStream_t s = (cudaStream_t)stream;
+    WP_KERNEL("divergence2d", 4.0 * (4.0 * (nx + 1) * ny + (double)nx * ny), s,
+              div2d_kernel<<<grid, dim3(32, 8), 0, s>>>(b, xv, yv, ax, ay, nx, ny, (float)(1.0 / dx), (float)(1.0 / dy)));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_grad_subtract_frac3d(float* xv, float* yv, float* zv, const float* p, const float* ax,
+                                                        const float* ay, const float* az, int nx, int ny, int nz,
+                                                        double dx, double dy, double dz, int multiply_frac, void* stream) {
+    if (!xv || !yv || !zv || !p || !ax || !ay || !az || nx <= 0 || ny <= 0 || nz <= 0 || nz >= 65535) {
+        wp_set_error_msg("wp_grad_subtract_frac3d: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    dim3 grid(wp_cdiv(ny + 1, 32), wp_cdiv(nx + 1, 8), nz + 1);
+    // (p_r - p_l) / (dx_l + dx_r) * 2 with uniform spacing (cuGradient.cu:1862)
+    cudaStream_t s = (cudaStream_t)stream;
+    const double faces = (double)(nx + 1) * ny * nz * 3, cells = (double)nx * ny * nz;
+    WP_KERNEL("grad_subtract", 4.0 * (3 * faces + cells), s,
+              grad3d_kernel<<<grid, dim3(32, 8), 0, s>>>(xv, yv, zv, p, ax, ay, az, nx, ny, nz, (float)(2.0 / (dx + dx)),
+                                                         (float)(2.0 / (dy + dy)), (float)(2.0 / (dz + dz)),
+                                                         multiply_frac));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_grad_subtract_frac2d(float* xv, float* yv, const float* p, const float* ax, const float* ay,
+                                                        int nx, int ny, double dx, double dy, int multiply_frac, void* stream) {
+    if (!xv || !yv || !p || !ax || !ay || nx <= 0 || ny <= 0) { wp_set_error_msg("wp_grad_subtract_frac2d: bad arguments"); return WP_ERR_INVALID_ARG; }
+    dim3 grid(wp_cdiv(ny + 1, 32), wp_cdiv(nx + 1, 8));
+    cudaStream_t s = (cudaStream_t)stream;
+    WP_KERNEL("grad_subtract2d", 4.0 * (6.0 * (nx + 1) * ny + (double)nx * ny), s,
+              grad2d_kernel<<<grid, dim3(32, 8), 0, s>>>(xv, yv, p, ax, ay, nx, ny, (float)(2.0 / (dx + dx)),
+                                                         (float)(2.0 / (dy + dy)), multiply_frac));
+    return WP_OK;
+}
+
+wp_status wp_max_abs_device(const float* x, size_t n, unsigned int* d_out, cudaStream_t s) {
+    WP_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned int), s));
+    if (n == 0) return WP_OK;
+    unsigned blocks = wp_cdiv(n, 256);
+    const unsigned cap = (unsigned)wp_sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    WP_KERNEL("max_abs", 4.0 * n, s, maxabs_kernel<<<blocks, 256, 0, s>>>(x, n, d_out));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_max_abs(const float* x, size_t n, double* out, void* stream) {
+    if ((!x && n) || !out) { wp_set_error_msg("wp_max_abs: null pointer"); return WP_ERR_INVALID_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned int* d = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(unsigned int), s));
+    wp_status st = wp_max_abs_device(x, n, d, s);
+    unsigned int bits = 0;
+    if (st == WP_OK) {
+        cudaError_t e = cudaMemcpyAsync(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "wp_max_abs", __FILE__, __LINE__); st = WP_ERR_CUDA; }
+    }
+    cudaFreeAsync(d, s);
+    float f;
+    memcpy(&f, &bits, sizeof(f));
+    *out = (double)f;
+    return st;
+}
+
+extern "C" CUWHHD_API wp_status wp_sdf_spheres3d(float* sdf, int nx, int ny, int nz, double dx, const double* centers,
+                                                 const double* radii, int count, void* stream) {
+    if (!sdf || nx <= 0 || ny <= 0 || nz <= 0 || count < 0 || (count > 0 && (!centers || !radii)) || count > 4096) {
+        wp_set_error_msg("wp_sdf_spheres3d: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<Sphere> hs(count > 0 ? count : 1);
+    for (int i = 0; i < count; ++i) {
+        hs[i].c[0] = (float)centers[3 * i];
+        hs[i].c[1] = (float)centers[3 * i + 1];
+        hs[i].c[2] = (float)centers[3 * i + 2];
+        hs[i].r = (float)radii[i];
+    }
+    Sphere* d = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(Sphere) * hs.size(), s));
+    WP_CUDA_TRY(cudaMemcpyAsync(d, hs.data(), sizeof(Sphere) * hs.size(), cudaMemcpyHostToDevice, s));
+    dim3 grid(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz);
+    const int tok = wp_prof_start(s);
+    sdf_spheres_kernel<<<grid, dim3(32, 8), 0, s>>>(sdf, nx, ny, nz, (float)dx, d, count);
+    cudaError_t e = cudaGetLastError();
+    wp_prof_stop(tok, "sdf_spheres", 4.0 * nx * ny * nz, s);
+    // the host staging vector must outlive the async copy
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFreeAsync(d, s);
+    if (e != cudaSuccess || e2 != cudaSuccess) { wp_set_cuda_error(e != cudaSuccess ? e : e2, "sdf", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_fractions3d(float* ax, float* ay, float* az, const float* sdf, int nx, int ny, int nz,
+                                               double dx, void* stream) {
+    if (!ax || !ay || !az || !sdf || nx <= 0 || ny <= 0 || nz <= 0 || nz >= 65535) { wp_set_error_msg("wp_fractions3d: bad arguments"); return WP_ERR_INVALID_ARG; }
+    dim3 grid(wp_cdiv(ny + 1, 32), wp_cdiv(nx + 1, 8), nz + 1);
+    cudaStream_t s = (cudaStream_t)stream;
+    WP_KERNEL("fractions", 4.0 * (4.0 * nx * ny * nz), s,
+              frac3d_kernel<<<grid, dim3(32, 8), 0, s>>>(ax, ay, az, sdf, nx, ny, nz, (float)dx));
+    return WP_OK;
+}

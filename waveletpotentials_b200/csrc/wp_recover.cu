@@ -1,0 +1,323 @@
+// wp_recover.cu -- local divergence-free projection in wavelet space and the potential-recovery
+// pipelines (3D and 2D).
+//
+// Reference behaviour:
+//   3D projection cuProjectLocal_q_3d_dq_ccc (cuDivLocalProject3D.cu:4013-4246), launched by
+//   CuDivLocalProject3D::ProjectLocal_q_ccc (:5273-5308); the wall bc 'n' makes the div-wavelet
+//   bc 'd' so this is the kernel on the configured path.  Coefficient index (x,y,z) in [0,n)^3
+//   reads xv(x+1,y,z), yv(x,y+1,z), zv(x,y,z+1), writes qx(x,y+1,z+1), qy(x+1,y,z+1), qz(x+1,y+1,z):
+//   interior q = (s x v)/|s|^2 with s_i = 4/(dx_i (2^j_i + 1e-12)), j_i = L_i - bitlen(i) + 1;
+//   faces (one index 0): a one-component ratio weighted by the inner-product tables
+//   (ip_proj = ||B||^2 of CDF3.7 'n' on n points, ip_base = ||B||^2 of CDF4.6 'd' on n+1 points);
+//   edges and corner: 0.  Every other q entry is 0.
+//   2D projection cuProjectLocal_q_single (cuDivLocalProject.cu:765-1045): both of its passes
+//   evaluate the same pointwise ratio (the neighbour terms it computes are unused), so
+//   qz(i+1,j+1) = P(i,j) for i,j >= 1 and qz = 0 on the rows/columns 0 and 1.
+//   Pipelines CuWaveletPotentialRecover3D::Solve (cuWaveletPotentialRecover3D.cu:16-61) and
+//   CuWaveletPotentialRecover2D::Solve (cuWaveletPotentialRecover2D.cu:16-36).
+#include "wp_common.cuh"
+
+#include <cmath>
+#include <cstdlib>
+#include <new>
+#include <vector>
+
+wp_status wp_ip_diag_device(double* d_out, int dim, int wavelet, char bc, cudaStream_t s);
+
+namespace {
+
+constexpr float kEps = 1e-12f;
+
+// per-axis table of length n: [scale s_i | ip_proj[i] | ip_base[i+1]]
+struct AxisTab {
+    const float* s;
+    const float* ip0;
+    const float* ip1;
+};
+
+__global__ void __launch_bounds__(256) project3d_kernel(float* __restrict__ qx, float* __restrict__ qy,
+                                                        float* __restrict__ qz, const float* __restrict__ xv,
+                                                        const float* __restrict__ yv, const float* __restrict__ zv,
+                                                        int nx, int ny, int nz, AxisTab tx, AxisTab ty, AxisTab tz) {
+    const int y = blockIdx.x * 32 + threadIdx.x;
+    const int x = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    const long sxv = (long)(nx + 1) * ny, syv = (long)nx * (ny + 1), szv = (long)nx * ny;
+    const long sqx = (long)nx * (ny + 1), sqy = (long)(nx + 1) * ny, sqz = (long)(nx + 1) * (ny + 1);
+    const float xin = xv[y + (long)(x + 1) * ny + z * sxv];
+    const float yin = yv[(y + 1) + (long)x * (ny + 1) + z * syv];
+    const float zin = zv[y + (long)x * ny + (z + 1) * szv];
+    const float sx = tx.s[x], sy = ty.s[y], sz = tz.s[z];
+    float oX = 0.f, oY = 0.f, oZ = 0.f;
+    if (x > 0 && y > 0 && z > 0) {
+        const float inv = 1.f / (sy * sy + sx * sx + sz * sz);
+        oZ = (sy * xin - sx * yin) * inv;
+        oX = (sz * yin - sy * zin) * inv;
+        oY = (sx * zin - sz * xin) * inv;
+    } else {
+        const float ip0x = tx.ip0[x], ip1x = tx.ip1[x], ip0y = ty.ip0[y], ip1y = ty.ip1[y];
+        const float ip0z = tz.ip0[z], ip1z = tz.ip1[z];
+        if (x == 0 && y > 0 && z > 0) {
+            const float szByBz = sz * ip0x * ip1y * ip0z, syByBz = sy * ip0x * ip0y * ip1z;
+            oX = (yin * szByBz - zin * syByBz) / (sy * syByBz + sz * szByBz + kEps);
+        } else if (y == 0 && x > 0 && z > 0) {
+            const float sxBxBz = sx * ip0x * ip0y * ip1z, szBxBz = sz * ip1x * ip0y * ip0z;
+            oY = (zin * sxBxBz - xin * szBxBz) / (sx * sxBxBz + sz * szBxBz + kEps);
+        } else if (z == 0 && x > 0 && y > 0) {
+            const float syBxBy = sy * ip1x * ip0y * ip0z, sxBxBy = sx * ip0x * ip1y * ip0z;
+            oZ = (xin * syBxBy - yin * sxBxBy) / (sx * sxBxBy + sy * syBxBy + kEps);
+        }
+    }
+    qx[(y + 1) + (long)x * (ny + 1) + (z + 1) * sqx] = oX;
+    qy[y + (long)(x + 1) * ny + (z + 1) * sqy] = oY;
+    qz[(y + 1) + (long)(x + 1) * (ny + 1) + z * sqz] = oZ;
+    // entries of q no main write reaches (an index 0 on a potential-staggered axis)
+    if (y == 0) {
+        qx[(long)x * (ny + 1) + (z + 1) * sqx] = 0.f;
+        qz[(long)(x + 1) * (ny + 1) + z * sqz] = 0.f;
+    }
+    if (z == 0) {
+        qx[(y + 1) + (long)x * (ny + 1)] = 0.f;
+        qy[y + (long)(x + 1) * ny] = 0.f;
+    }
+    if (x == 0) {
+        qy[y + (z + 1) * sqy] = 0.f;
+        qz[(y + 1) + z * sqz] = 0.f;
+    }
+    if (y == 0 && z == 0) qx[(long)x * (ny + 1)] = 0.f;
+    if (x == 0 && z == 0) qy[y] = 0.f;
+    if (x == 0 && y == 0) qz[z * sqz] = 0.f;
+}
+
+__global__ void __launch_bounds__(256) project2d_kernel(float* __restrict__ qz, const float* __restrict__ xv,
+                                                        const float* __restrict__ yv, int nx, int ny, AxisTab tx,
+                                                        AxisTab ty) {
+    const int y = blockIdx.x * 32 + threadIdx.x;  // qz index along y in [0, ny]
+    const int x = blockIdx.y * 8 + threadIdx.y;   // qz index along x in [0, nx]
+    if (y > ny || x > nx) return;
+    float out = 0.f;
+    if (x >= 2 && y >= 2) {
+        const int i = x - 1, j = y - 1;
+        const float sx = tx.s[i], sy = ty.s[j];
+        const float ip0x = tx.ip0[i], ip1x = tx.ip1[i], ip0y = ty.ip0[j], ip1y = ty.ip1[j];
+        const float xin = xv[j + (long)x * ny];
+        const float yin = yv[y + (long)i * (ny + 1)];
+        const float mid = sx * sx * ip0x * ip1y + sy * sy * ip1x * ip0y + kEps;
+        out = (xin * sy * ip1x * ip0y - yin * sx * ip0x * ip1y) / mid;
+    }
+    qz[y + (long)x * (ny + 1)] = out;
+}
+
+// Builds the per-axis table [s | ip0 | ip1] (length 3n floats) on the device.
+wp_status build_axis_table(float** d_tab, int n, double h, cudaStream_t s) {
+    const int L = wp_ilog2(n);
+    double* d_ip = nullptr;
+    WP_CUDA_TRY(cudaMalloc((void**)&d_ip, sizeof(double) * (2 * n + 1)));
+    wp_status st = wp_ip_diag_device(d_ip, n, WP_ID_CDF3_7, 'n', s);
+    if (st == WP_OK) st = wp_ip_diag_device(d_ip + n, n + 1, WP_ID_CDF4_6, 'd', s);
+    std::vector<double> ip(2 * n + 1);
+    if (st == WP_OK) {
+        cudaError_t e = cudaMemcpyAsync(ip.data(), d_ip, sizeof(double) * (2 * n + 1), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "ip table copy", __FILE__, __LINE__); st = WP_ERR_CUDA; }
+    }
+    cudaFree(d_ip);
+    if (st != WP_OK) return st;
+    std::vector<float> tab(3 * n);
+    for (int i = 0; i < n; ++i) {
+        int bl = 0;
+        for (int v = i; v > 0; v >>= 1) ++bl;
+        const int j = L - bl + 1;
+        tab[i] = (float)(4.0 / h / ((double)(1 << j) + 1e-12));
+        tab[n + i] = (float)ip[i];          // ip_proj[i]  (CDF3.7 'n', n points)
+        tab[2 * n + i] = (float)ip[n + i + 1];  // ip_base[i+1] (CDF4.6 'd', n+1 points)
+    }
+    WP_CUDA_TRY(cudaMalloc((void**)d_tab, sizeof(float) * 3 * n));
+    WP_CUDA_TRY(cudaMemcpy(*d_tab, tab.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice));
+    return WP_OK;
+}
+
+AxisTab view(const float* t, int n) { return AxisTab{t, t + n, t + 2 * n}; }
+
+bool check_wavelets(int curl, int div) { return curl == WP_ID_CDF3_7 && div == WP_ID_CDF4_6; }
+
+}  // namespace
+
+struct wp_recover3d {
+    int n[3];
+    int L[3];
+    double h[3];
+    float* tab[3];
+    float* tmp[3];
+};
+
+extern "C" CUWHHD_API wp_status wp_recover3d_create(wp_recover3d** out, int nx, int ny, int nz, double dx, double dy,
+                                                    double dz, char bc, int curl_wavelet, int div_wavelet) {
+    if (!out) { wp_set_error_msg("wp_recover3d_create: null handle"); return WP_ERR_INVALID_ARG; }
+    *out = nullptr;
+    if (!wp_is_pow2(nx) || !wp_is_pow2(ny) || !wp_is_pow2(nz) || nx < 4 || ny < 4 || nz < 4 || nx > 4096 ||
+        ny > 4096 || nz > 4096 || !(dx > 0) || !(dy > 0) || !(dz > 0)) {
+        wp_set_error_msg("wp_recover3d_create: extents must be powers of two in [4, 4096] and spacings > 0");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (bc != 'n') { wp_set_error_msg("wp_recover3d_create: only bc 'n' (zero-normal-flux walls) is implemented"); return WP_ERR_UNSUPPORTED; }
+    if (!check_wavelets(curl_wavelet, div_wavelet)) { wp_set_error_msg("wp_recover3d_create: curl CDF3.7 / div CDF4.6 only"); return WP_ERR_UNSUPPORTED; }
+    wp_recover3d* h = new (std::nothrow) wp_recover3d();
+    if (!h) return WP_ERR_INVALID_ARG;
+    int n[3] = {nx, ny, nz};
+    double hs[3] = {dx, dy, dz};
+    for (int a = 0; a < 3; ++a) {
+        h->n[a] = n[a];
+        h->L[a] = wp_ilog2(n[a]);
+        h->h[a] = hs[a];
+        wp_status st = build_axis_table(&h->tab[a], n[a], hs[a], 0);
+        if (st != WP_OK) { wp_recover3d_destroy(h); return st; }
+    }
+    size_t sz[3] = {(size_t)(nx + 1) * ny * nz, (size_t)nx * (ny + 1) * nz, (size_t)nx * ny * (nz + 1)};
+    for (int a = 0; a < 3; ++a) {
+        cudaError_t e = cudaMalloc((void**)&h->tmp[a], sizeof(float) * sz[a]);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "recover3d temp", __FILE__, __LINE__); wp_recover3d_destroy(h); return WP_ERR_CUDA; }
+    }
+    *out = h;
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_recover3d_destroy(wp_recover3d* h) {
+    if (!h) return WP_OK;
+    for (int a = 0; a < 3; ++a) {
+        if (h->tab[a]) cudaFree(h->tab[a]);
+        if (h->tmp[a]) cudaFree(h->tmp[a]);
+    }
+    delete h;
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_recover3d_project(wp_recover3d* h, float* qx, float* qy, float* qz,
+                                                     const float* xv, const float* yv, const float* zv, void* stream) {
+    if (!h || !qx || !qy || !qz || !xv || !yv || !zv) { wp_set_error_msg("wp_recover3d_project: null pointer"); return WP_ERR_INVALID_ARG; }
+    const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+    if (nz > 65535) return WP_ERR_UNSUPPORTED;
+    dim3 grid(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz);
+    cudaStream_t s = (cudaStream_t)stream;
+    const double bytes = 4.0 * ((double)(nx + 1) * ny * nz * 3 + (double)(nx + 1) * (ny + 1) * nz * 3);
+    WP_KERNEL("project3d", bytes, s,
+              project3d_kernel<<<grid, dim3(32, 8), 0, s>>>(qx, qy, qz, xv, yv, zv, nx, ny, nz, view(h->tab[0], nx),
+                                                            view(h->tab[1], ny), view(h->tab[2], nz)));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_recover3d_run(wp_recover3d* h, float* qx, float* qy, float* qz, const float* xv,
+                                                 const float* yv, const float* zv, void* stream) {
+    if (!h || !qx || !qy || !qz || !xv || !yv || !zv) { wp_set_error_msg("wp_recover3d_run: null pointer"); return WP_ERR_INVALID_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+    const int Lx = h->L[0], Ly = h->L[1], Lz = h->L[2];
+    const int C = WP_ID_CDF3_7, V = WP_ID_CDF4_6;
+    float *tx = h->tmp[0], *ty = h->tmp[1], *tz = h->tmp[2];
+    wp_status st;
+#define WP_T(dst, src, DX, DY, DZ, L, ax, w, bc, f)                                          \
+    if ((st = wp_dwt_axis_launch<float>(dst, src, DX, DY, DZ, L, ax, w, bc, f, s)) != WP_OK) \
+        return st;
+    // forward analysis (cuWaveletPotentialRecover3D.cu:32-42)
+    WP_T(tx, xv, nx + 1, ny, nz, Lx, 'x', V, 'd', 1);
+    WP_T(tx, tx, nx + 1, ny, nz, Ly, 'y', C, 'n', 1);
+    WP_T(tx, tx, nx + 1, ny, nz, Lz, 'z', C, 'n', 1);
+    WP_T(ty, yv, nx, ny + 1, nz, Lx, 'x', C, 'n', 1);
+    WP_T(ty, ty, nx, ny + 1, nz, Ly, 'y', V, 'd', 1);
+    WP_T(ty, ty, nx, ny + 1, nz, Lz, 'z', C, 'n', 1);
+    WP_T(tz, zv, nx, ny, nz + 1, Lx, 'x', C, 'n', 1);
+    WP_T(tz, tz, nx, ny, nz + 1, Ly, 'y', C, 'n', 1);
+    WP_T(tz, tz, nx, ny, nz + 1, Lz, 'z', V, 'd', 1);
+    // local projection (:46)
+    if ((st = wp_recover3d_project(h, qx, qy, qz, tx, ty, tz, stream)) != WP_OK) return st;
+    // inverse synthesis (:50-60)
+    WP_T(qx, qx, nx, ny + 1, nz + 1, Lx, 'x', C, 'n', 0);
+    WP_T(qx, qx, nx, ny + 1, nz + 1, Ly, 'y', V, 'd', 0);
+    WP_T(qx, qx, nx, ny + 1, nz + 1, Lz, 'z', V, 'd', 0);
+    WP_T(qy, qy, nx + 1, ny, nz + 1, Lx, 'x', V, 'd', 0);
+    WP_T(qy, qy, nx + 1, ny, nz + 1, Ly, 'y', C, 'n', 0);
+    WP_T(qy, qy, nx + 1, ny, nz + 1, Lz, 'z', V, 'd', 0);
+    WP_T(qz, qz, nx + 1, ny + 1, nz, Lx, 'x', V, 'd', 0);
+    WP_T(qz, qz, nx + 1, ny + 1, nz, Ly, 'y', V, 'd', 0);
+    WP_T(qz, qz, nx + 1, ny + 1, nz, Lz, 'z', C, 'n', 0);
+#undef WP_T
+    return WP_OK;
+}
+
+struct wp_recover2d {
+    int n[2];
+    int L[2];
+    double h[2];
+    float* tab[2];
+    float* tmp[2];
+};
+
+extern "C" CUWHHD_API wp_status wp_recover2d_create(wp_recover2d** out, int nx, int ny, double dx, double dy, char bc,
+                                                    int curl_wavelet, int div_wavelet) {
+    if (!out) { wp_set_error_msg("wp_recover2d_create: null handle"); return WP_ERR_INVALID_ARG; }
+    *out = nullptr;
+    if (!wp_is_pow2(nx) || !wp_is_pow2(ny) || nx < 4 || ny < 4 || nx > 4096 || ny > 4096 || !(dx > 0) || !(dy > 0)) {
+        wp_set_error_msg("wp_recover2d_create: extents must be powers of two in [4, 4096] and spacings > 0");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (bc != 'n') { wp_set_error_msg("wp_recover2d_create: only bc 'n' (zero-normal-flux walls) is implemented"); return WP_ERR_UNSUPPORTED; }
+    if (!check_wavelets(curl_wavelet, div_wavelet)) { wp_set_error_msg("wp_recover2d_create: curl CDF3.7 / div CDF4.6 only"); return WP_ERR_UNSUPPORTED; }
+    wp_recover2d* h = new (std::nothrow) wp_recover2d();
+    if (!h) return WP_ERR_INVALID_ARG;
+    int n[2] = {nx, ny};
+    double hs[2] = {dx, dy};
+    for (int a = 0; a < 2; ++a) {
+        h->n[a] = n[a];
+        h->L[a] = wp_ilog2(n[a]);
+        h->h[a] = hs[a];
+        wp_status st = build_axis_table(&h->tab[a], n[a], hs[a], 0);
+        if (st != WP_OK) { wp_recover2d_destroy(h); return st; }
+    }
+    size_t sz[2] = {(size_t)(nx + 1) * ny, (size_t)nx * (ny + 1)};
+    for (int a = 0; a < 2; ++a) {
+        cudaError_t e = cudaMalloc((void**)&h->tmp[a], sizeof(float) * sz[a]);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "recover2d temp", __FILE__, __LINE__); wp_recover2d_destroy(h); return WP_ERR_CUDA; }
+    }
+    *out = h;
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_recover2d_destroy(wp_recover2d* h) {
+    if (!h) return WP_OK;
+    for (int a = 0; a < 2; ++a) {
+        if (h->tab[a]) cudaFree(h->tab[a]);
+        if (h->tmp[a]) cudaFree(h->tmp[a]);
+    }
+    delete h;
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_recover2d_project(wp_recover2d* h, float* qz, const float* xv, const float* yv,
+                                                     void* stream) {
+    if (!h || !qz || !xv || !yv) { wp_set_error_msg("wp_recover2d_project: null pointer"); return WP_ERR_INVALID_ARG; }
+    const int nx = h->n[0], ny = h->n[1];
+    dim3 grid(wp_cdiv(ny + 1, 32), wp_cdiv(nx + 1, 8));
+    cudaStream_t s = (cudaStream_t)stream;
+    WP_KERNEL("project2d", 4.0 * ((double)(nx + 1) * ny * 2 + (double)(nx + 1) * (ny + 1)), s,
+              project2d_kernel<<<grid, dim3(32, 8), 0, s>>>(qz, xv, yv, nx, ny, view(h->tab[0], nx), view(h->tab[1], ny)));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_recover2d_run(wp_recover2d* h, float* qz, const float* xv, const float* yv,
+                                                 void* stream) {
+    if (!h || !qz || !xv || !yv) { wp_set_error_msg("wp_recover2d_run: null pointer"); return WP_ERR_INVALID_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nx = h->n[0], ny = h->n[1], Lx = h->L[0], Ly = h->L[1];
+    const int C = WP_ID_CDF3_7, V = WP_ID_CDF4_6;
+    float *tx = h->tmp[0], *ty = h->tmp[1];
+    wp_status st;
+    if ((st = wp_dwt_axis_launch<float>(tx, xv, nx + 1, ny, 1, Lx, 'x', V, 'd', 1, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(tx, tx, nx + 1, ny, 1, Ly, 'y', C, 'n', 1, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(ty, yv, nx, ny + 1, 1, Lx, 'x', C, 'n', 1, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(ty, ty, nx, ny + 1, 1, Ly, 'y', V, 'd', 1, s)) != WP_OK) return st;
+    if ((st = wp_recover2d_project(h, qz, tx, ty, stream)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(qz, qz, nx + 1, ny + 1, 1, Lx, 'x', V, 'd', 0, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(qz, qz, nx + 1, ny + 1, 1, Ly, 'y', V, 'd', 0, s)) != WP_OK) return st;
+    return WP_OK;
+}

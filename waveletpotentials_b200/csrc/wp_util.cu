@@ -1,0 +1,138 @@
+// wp_util.cu -- error reporting and device queries shared by the C ABI.
+#include "wp_common.cuh"
+
+#include <cstdio>
+#include <cstring>
+
+namespace {
+thread_local char g_err[512] = "";
+int g_sms[64] = {0};
+}  // namespace
+
+void wp_set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+    snprintf(g_err, sizeof(g_err), "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+
+void wp_set_error_msg(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+
+int wp_sm_count() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (dev < 64 && g_sms[dev] > 0) return g_sms[dev];
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+    if (dev < 64) g_sms[dev] = sms;
+    return sms;
+}
+
+extern "C" CUWHHD_API const char* wp_last_error(void) { return g_err; }
+
+extern "C" CUWHHD_API int wp_version(void) { return 1; }
+
+// ---------------------------------------------------------------------------------------------
+// Launch accounting and optional per-kernel-class timing with CUDA events recorded on the
+// launching stream.  Counting is always on (one relaxed atomic per launch); event timing only
+// between wp_profile_enable(1) and wp_profile_enable(0).
+#include <atomic>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace {
+struct ProfRec {
+    const char* name;
+    cudaEvent_t a, b;
+    double bytes;
+};
+std::atomic<long long> g_launches{0};
+std::atomic<bool> g_prof_on{false};
+std::mutex g_prof_mu;
+std::vector<ProfRec> g_open;   // indexed by token
+std::vector<ProfRec> g_done;
+std::vector<cudaEvent_t> g_pool;
+
+cudaEvent_t take_event() {
+    if (!g_pool.empty()) {
+        cudaEvent_t e = g_pool.back();
+        g_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct Agg {
+    std::string name;
+    long long launches = 0;
+    double ms = 0.0;
+    double bytes = 0.0;
+};
+std::vector<Agg> g_agg;
+}  // namespace
+
+int wp_prof_start(cudaStream_t s) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (!g_prof_on.load(std::memory_order_relaxed)) return -1;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    ProfRec r{nullptr, take_event(), take_event(), 0.0};
+    cudaEventRecord(r.a, s);
+    g_open.push_back(r);
+    return (int)g_open.size() - 1;
+}
+
+void wp_prof_stop(int tok, const char* name, double bytes, cudaStream_t s) {
+    if (tok < 0) return;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (tok >= (int)g_open.size()) return;
+    ProfRec& r = g_open[tok];
+    r.name = name;
+    r.bytes = bytes;
+    cudaEventRecord(r.b, s);
+}
+
+extern "C" CUWHHD_API void wp_profile_enable(int on) { g_prof_on.store(on != 0); }
+
+extern "C" CUWHHD_API void wp_profile_reset(void) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    for (auto& r : g_open) { g_pool.push_back(r.a); g_pool.push_back(r.b); }
+    g_open.clear();
+    g_agg.clear();
+    g_launches.store(0);
+}
+
+extern "C" CUWHHD_API long long wp_launch_count(void) { return g_launches.load(); }
+
+// Synchronizes the device, folds the recorded events into per-name totals and returns the
+// number of kernel classes; wp_profile_entry(i, ...) reads them.
+extern "C" CUWHHD_API int wp_profile_collect(void) {
+    cudaDeviceSynchronize();
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    for (auto& r : g_open) {
+        float ms = 0.f;
+        if (r.name && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            Agg* a = nullptr;
+            for (auto& x : g_agg) if (x.name == r.name) { a = &x; break; }
+            if (!a) { g_agg.push_back(Agg{r.name}); a = &g_agg.back(); }
+            a->launches += 1;
+            a->ms += ms;
+            a->bytes += r.bytes;
+        }
+        g_pool.push_back(r.a);
+        g_pool.push_back(r.b);
+    }
+    g_open.clear();
+    return (int)g_agg.size();
+}
+
+extern "C" CUWHHD_API int wp_profile_entry(int i, char* name, int name_cap, long long* launches, double* ms,
+                                           double* bytes) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (i < 0 || i >= (int)g_agg.size()) return 1;
+    const Agg& a = g_agg[i];
+    if (name && name_cap > 0) snprintf(name, name_cap, "%s", a.name.c_str());
+    if (launches) *launches = a.launches;
+    if (ms) *ms = a.ms;
+    if (bytes) *bytes = a.bytes;
+    return 0;
+}
