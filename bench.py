@@ -78,15 +78,25 @@ class ClockSampler:
         sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[5 + i]})
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
 
 def make_problem(n, seed):
+    """Seeded inputs (cached in the temp directory: the spectral generator takes ~10 s at 256^3)."""
+    import tempfile
     from waveletpotentials_b200 import fields
     centers, radii = fields.random_spheres(4, 0.05, 0.15, seed + 1000)
+    path = os.path.join(tempfile.gettempdir(), f"wp_bench_fields_{n}_{seed}.npz")
+    if os.path.exists(path):
+        d = np.load(path)
+        return centers, radii, (d["xv"], d["yv"], d["zv"])
     xv, yv, zv = fields.velocity3d((n, n, n), seed, dtype=np.float32)
+    try:
+        np.savez(path, xv=xv, yv=yv, zv=zv)
+    except OSError:
+        pass
     return centers, radii, (xv, yv, zv)
 
 
@@ -244,7 +254,7 @@ def cores():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=25)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)

@@ -189,9 +189,27 @@ CUWHHD_API wp_status wp_max_abs(const float* x, size_t n, double* out, void* str
    cuSolidLevelSet3D.cu:11-27); centers/radii are HOST arrays (3*count, count). */
 CUWHHD_API wp_status wp_sdf_spheres3d(float* sdf, int nx, int ny, int nz, double dx, const double* centers,
                                       const double* radii, int count, void* stream);
+/* Union of axis-aligned boxes (HOST lo/hi arrays, 3*count each) into an existing level set (min);
+   exact box signed distance.  No reference counterpart (the reference builds spheres only); used
+   for the mixed-obstacle configurations. */
+CUWHHD_API wp_status wp_sdf_boxes3d(float* sdf, int nx, int ny, int nz, double dx, const double* lo, const double* hi,
+                                    int count, void* stream);
 /* Face open fractions from a level set (cuGetAx/Ay/Az, cuSolidLevelSet3D.cu:36-90). */
 CUWHHD_API wp_status wp_fractions3d(float* ax, float* ay, float* az, const float* sdf, int nx, int ny, int nz,
                                     double dx, void* stream);
+/* 2D: circle level set (CuSolidLevelSet2D, cuSolidLevelSet2D.cu) and face fractions. */
+CUWHHD_API wp_status wp_sdf_circles2d(float* sdf, int nx, int ny, double dx, const double* centers, const double* radii,
+                                      int count, void* stream);
+CUWHHD_API wp_status wp_fractions2d(float* ax, float* ay, const float* sdf, int nx, int ny, double dx, void* stream);
+
+/* ------------------------------------------------------------- DST-I Poisson ------- */
+typedef struct wp_dst3d wp_dst3d;
+/* Replaces CuDst3D(int3 dim, DTYPE3 dx) (cuDst3D.cu:202-255): Dirichlet Poisson solver by DST-I. */
+CUWHHD_API wp_status wp_dst3d_create(wp_dst3d** h, int nx, int ny, int nz, double dx, double dy, double dz);
+/* Replaces CuDst3D::Solve(dst, f) (cuDst3D.cu:265-341): FP64 device arrays of nx*ny*nz cells,
+   dst may equal f; solves -lap_h p = f with p = 0 outside the grid (scaled by dx*dy as the reference). */
+CUWHHD_API wp_status wp_dst3d_solve(wp_dst3d* h, double* dst, const double* f, void* stream);
+CUWHHD_API wp_status wp_dst3d_destroy(wp_dst3d* h);
 
 #ifdef __cplusplus
 }

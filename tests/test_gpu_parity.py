@@ -281,3 +281,62 @@ def test_projector_end_to_end(wp, oracle):
     oq = oracle.recover3d(*pu, nn, (h,) * 3)
     for o, t in zip(oq, q):
         assert rel(o, N(t)) < TOL32
+
+
+def test_dst3d_matches_oracle(wp, oracle):
+    n = (24, 20, 16)
+    h = (1 / 25, 1 / 21, 1 / 17)
+    rng = np.random.default_rng(21)
+    f = rng.standard_normal((n[2], n[0], n[1]))
+    ref = oracle.dst3d_poisson(f, n, h)
+    dst = wp.CuDst3D(n, h)
+    out = torch.zeros(f.shape, dtype=torch.float64, device="cuda")
+    dst.Solve(out, T(f, torch.float64))
+    assert rel(ref, N(out)) < 1e-12
+    # in place
+    g = T(f, torch.float64)
+    dst.Solve(g, g)
+    assert rel(ref, N(g)) < 1e-12
+
+
+def test_boxes_and_2d_fractions_match_oracle(wp, oracle):
+    n = (32, 24, 16)
+    h = 1 / 32
+    sls = wp.CuSolidLevelSet3D(n, h)
+    sls.InitLsSpheres([[0.3, 0.3, 0.2]], [0.1])
+    sls.AddBoxes([[0.5, 0.1, 0.1]], [[0.8, 0.4, 0.3]])
+    ref = oracle.sdf_boxes3d(oracle.sdf_spheres3d(n, h, [[0.3, 0.3, 0.2]], [0.1]), n, h, [[0.5, 0.1, 0.1]],
+                             [[0.8, 0.4, 0.3]])
+    assert np.max(np.abs(N(sls.ls) - ref)) < 1e-6
+    n2 = (40, 24)
+    s2 = wp.CuSolidLevelSet2D(n2, 1 / 40)
+    s2.InitLsCircles([[0.4, 0.3], [0.7, 0.5]], [0.12, 0.08])
+    x = (np.arange(n2[0]) + 0.5) / 40
+    y = (np.arange(n2[1]) + 0.5) / 40
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    sdf = np.minimum(np.hypot(X - 0.4, Y - 0.3) - 0.12, np.hypot(X - 0.7, Y - 0.5) - 0.08)
+    assert np.max(np.abs(N(s2.ls) - sdf)) < 1e-6
+    ax = torch.zeros((n2[0] + 1, n2[1]), device="cuda")
+    ay = torch.zeros((n2[0], n2[1] + 1), device="cuda")
+    s2.GetFrac(ax, ay)
+    oax, oay = oracle.fractions2d(sdf, n2, 1 / 40)
+    assert np.max(np.abs(N(ax) - oax)) < 1e-5 and np.max(np.abs(N(ay) - oay)) < 1e-5
+
+
+def test_recover2d_and_mg2d_full_config0_size(wp, oracle):
+    """Config 0 size (256^2, no solids): 2D recovery against the oracle and a 2D tolerance solve."""
+    from waveletpotentials_b200 import fields
+    n = (256, 256)
+    h = 1 / 256
+    xv, yv = fields.velocity2d(n, 0)
+    rec = wp.CuWaveletPotentialRecover2D(n, h)
+    qz = torch.zeros((257, 257), device="cuda")
+    rec.Solve(qz, T(xv), T(yv))
+    ref = oracle.recover2d(xv.astype(np.float32), yv.astype(np.float32), n, (h, h))
+    assert rel(ref, N(qz)) < TOL32
+    ax, ay = np.ones((257, 256)), np.ones((256, 257))
+    f = oracle.divergence2d(xv, yv, ax, ay, n, (h, h)).astype(np.float32).astype(np.float64)
+    mg = wp.CuMultigridFrac2D(T(ax), T(ay), n, h)
+    p = torch.zeros(n, device="cuda")
+    rep = mg.SolveTol(p, None, T(f), rel_tol=1e-6, max_cycles=40, precision=wp.PREC_FP32)
+    assert rep["rel_residual"] <= 1e-6

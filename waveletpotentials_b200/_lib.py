@@ -83,6 +83,12 @@ SIGNATURES = {
     "wp_max_abs": (I, [P, S, ctypes.POINTER(D), P]),
     "wp_sdf_spheres3d": (I, [P, I, I, I, D, P, P, I, P]),
     "wp_fractions3d": (I, [P, P, P, P, I, I, I, D, P]),
+    "wp_sdf_boxes3d": (I, [P, I, I, I, D, P, P, I, P]),
+    "wp_sdf_circles2d": (I, [P, I, I, D, P, P, I, P]),
+    "wp_fractions2d": (I, [P, P, P, I, I, D, P]),
+    "wp_dst3d_create": (I, [PP, I, I, I, D, D, D]),
+    "wp_dst3d_solve": (I, [P, P, P, P]),
+    "wp_dst3d_destroy": (I, [P]),
 }
 
 

@@ -19,7 +19,8 @@ from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONS
     MgReport, WPError, check, lib
 
 __all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRecover2D", "CuMultigridFrac3D",
-           "CuMultigridFrac2D", "CuConvergence", "CuGradient", "CuSolidLevelSet3D", "Projector3D", "max_abs",
+           "CuMultigridFrac2D", "CuConvergence", "CuGradient", "CuSolidLevelSet3D", "CuSolidLevelSet2D", "CuDst3D",
+           "Projector3D", "max_abs",
            "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
            "PROLONG_TRILINEAR", "mac_shapes3d", "mac_shapes2d"]
 
@@ -352,6 +353,65 @@ class CuSolidLevelSet3D:
         s = mac_shapes3d(*self.dim)
         check(lib().wp_fractions3d(_ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(az, s["zv"]), _ptr(self.ls), *self.dim,
                                    self.dx, _stream(stream)), "wp_fractions3d")
+
+
+    def AddBoxes(self, lo, hi, stream=None):
+        """Union of axis-aligned boxes into the level set (no reference counterpart)."""
+        import numpy as np
+        l = np.ascontiguousarray(np.reshape(lo, (-1, 3)), dtype=np.float64)
+        u = np.ascontiguousarray(np.reshape(hi, (-1, 3)), dtype=np.float64)
+        check(lib().wp_sdf_boxes3d(_ptr(self.ls), *self.dim, self.dx, l.ctypes.data_as(ctypes.c_void_p),
+                                   u.ctypes.data_as(ctypes.c_void_p), int(l.shape[0]), _stream(stream)),
+              "wp_sdf_boxes3d")
+
+
+class CuSolidLevelSet2D:
+    """CuSolidLevelSet2D: circle level set (positive in fluid) and face open fractions."""
+
+    def __init__(self, dim, dx):
+        self.dim = tuple(int(v) for v in dim)
+        self.dx = float(dx)
+        self.ls = torch.empty(self.dim, device="cuda", dtype=torch.float32)
+
+    def InitLsCircles(self, centers, radii, stream=None):
+        import numpy as np
+        c = np.ascontiguousarray(np.reshape(centers, (-1, 2)), dtype=np.float64)
+        r = np.ascontiguousarray(np.reshape(radii, (-1,)), dtype=np.float64)
+        check(lib().wp_sdf_circles2d(_ptr(self.ls), *self.dim, self.dx, c.ctypes.data_as(ctypes.c_void_p),
+                                     r.ctypes.data_as(ctypes.c_void_p), int(r.size), _stream(stream)),
+              "wp_sdf_circles2d")
+
+    def GetFrac(self, ax, ay, stream=None):
+        s = mac_shapes2d(*self.dim)
+        check(lib().wp_fractions2d(_ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(self.ls), *self.dim, self.dx,
+                                   _stream(stream)), "wp_fractions2d")
+
+
+class CuDst3D:
+    """CuDst3D (cuDst3D.cuh): Dirichlet Poisson solve by DST-I, FP64 tensors of shape (nz, nx, ny)."""
+
+    def __init__(self, dim, dx):
+        self.dim = _dims3(dim)
+        self.dx = _dx3(dx)
+        h = ctypes.c_void_p()
+        check(lib().wp_dst3d_create(ctypes.byref(h), *self.dim, *self.dx), "wp_dst3d_create")
+        self._h = h
+
+    def Solve(self, dst, f, stream=None):
+        nx, ny, nz = self.dim
+        check(lib().wp_dst3d_solve(self._h, _ptr(dst, (nz, nx, ny), torch.float64), _ptr(f, (nz, nx, ny), torch.float64),
+                                   _stream(stream)), "wp_dst3d_solve")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().wp_dst3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Projector3D:

@@ -1,0 +1,170 @@
+// wp_dst.cu -- Dirichlet Poisson solve -lap_h p = f by DST-I along x, y and z, in FP64.
+//
+// Reference behaviour: CuDst3D (cuDst3D.cu:202-341): odd extension into a 2(n+1)-point complex
+// FFT per axis (cuFFT), orthonormal scaling sqrt(2/(n+1)), division by the eigenvalues
+// sum_i (2 - 2 cos(k_i pi / (n_i + 1))) and the factor dx*dy (cuDstProj_dx, :172-200), then the
+// same transforms again (the orthonormal DST-I is its own inverse).
+//
+// B200 design: no FFT library.  Each axis transform is a dense product with the n x n orthonormal
+// DST-I matrix (precomputed once per extent on the host in FP64), applied to a tile of C whole
+// lines staged in shared memory (the same tile geometry as the wavelet passes: coalesced along y,
+// bank-conflict-free column-parallel inner loop).  For the grid sizes of the coarse and gauge
+// solves (n <= a few hundred) the O(n) work per element is cheaper than an FFT's passes.
+#include "wp_common.cuh"
+
+#include <cmath>
+#include <new>
+#include <vector>
+
+namespace {
+
+constexpr int NT = 256;
+
+struct Geom {
+    long s_in, s_out, pstride;
+    int ni;
+    int contiguous;
+};
+
+template <int C>
+__global__ void __launch_bounds__(NT) dst_axis_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                                      const double* __restrict__ M, int N, Geom g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* S = reinterpret_cast<double*>(smem_raw);
+    constexpr int CP = C + 1;
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.x * C;
+    const long obase = (long)blockIdx.y * g.s_out;
+    for (int i = tid; i < C * N; i += NT) {
+        int col, p;
+        if (g.contiguous) { col = i / N; p = i - col * N; }
+        else { col = i % C; p = i / C; }
+        double v = 0.0;
+        if (i0 + col < g.ni) v = src[obase + (long)(i0 + col) * g.s_in + (long)p * g.pstride];
+        S[p * CP + col] = v;
+    }
+    __syncthreads();
+    // out[k][col] = sum_j M[k][j] S[j][col]; lanes span columns, warps span k
+    constexpr int KPER = NT / C;
+    const int col = tid % C, k0 = tid / C;
+    for (int k = k0; k < N; k += KPER) {
+        double acc = 0.0;
+        const double* Mk = M + (long)k * N;
+        for (int j = 0; j < N; ++j) acc = fma(__ldg(Mk + j), S[j * CP + col], acc);
+        if (i0 + col < g.ni) dst[obase + (long)(i0 + col) * g.s_in + (long)k * g.pstride] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(256) dst_eig_kernel(double* __restrict__ p, int nx, int ny, int nz, double scale) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    const double pi = 3.14159265358979323846;
+    const double mu = 2.0 - 2.0 * cos((x + 1) * pi / (nx + 1));
+    const double nu = 2.0 - 2.0 * cos((y + 1) * pi / (ny + 1));
+    const double ku = 2.0 - 2.0 * cos((z + 1) * pi / (nz + 1));
+    p[y + (long)x * ny + (long)z * nx * ny] *= scale / (mu + nu + ku);
+}
+
+template <int C>
+cudaError_t launch_axis(const double* src, double* dst, const double* M, int N, Geom g, int nouter, cudaStream_t s) {
+    const size_t smem = (size_t)N * (C + 1) * sizeof(double);
+    auto k = dst_axis_kernel<C>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int tok = wp_prof_start(s);
+    k<<<dim3((g.ni + C - 1) / C, nouter), NT, smem, s>>>(src, dst, M, N, g);
+    e = cudaGetLastError();
+    wp_prof_stop(tok, "dst_axis", 16.0 * N * (double)g.ni * nouter, s);
+    return e;
+}
+
+cudaError_t apply_axis(const double* src, double* dst, const double* M, int DX, int DY, int DZ, char axis,
+                       cudaStream_t s) {
+    Geom g;
+    int N, nouter;
+    if (axis == 'y') { N = DY; g.s_in = DY; g.ni = DX; g.s_out = (long)DX * DY; nouter = DZ; g.pstride = 1; g.contiguous = 1; }
+    else if (axis == 'x') { N = DX; g.s_in = 1; g.ni = DY; g.s_out = (long)DX * DY; nouter = DZ; g.pstride = DY; g.contiguous = 0; }
+    else { N = DZ; g.s_in = 1; g.ni = DY; g.s_out = DY; nouter = DX; g.pstride = (long)DX * DY; g.contiguous = 0; }
+    int C = 32;
+    while (C > 4 && (size_t)N * (C + 1) * sizeof(double) > 150 * 1024) C >>= 1;
+    if ((size_t)N * (C + 1) * sizeof(double) > 227 * 1024) return cudaErrorInvalidValue;
+    switch (C) {
+        case 32: return launch_axis<32>(src, dst, M, N, g, nouter, s);
+        case 16: return launch_axis<16>(src, dst, M, N, g, nouter, s);
+        case 8: return launch_axis<8>(src, dst, M, N, g, nouter, s);
+        default: return launch_axis<4>(src, dst, M, N, g, nouter, s);
+    }
+}
+
+}  // namespace
+
+struct wp_dst3d {
+    int n[3];
+    double h[3];
+    double* M[3];  // orthonormal DST-I matrices per axis
+    double* tmp;
+};
+
+extern "C" CUWHHD_API wp_status wp_dst3d_create(wp_dst3d** out, int nx, int ny, int nz, double dx, double dy, double dz) {
+    if (!out) { wp_set_error_msg("wp_dst3d_create: null handle"); return WP_ERR_INVALID_ARG; }
+    *out = nullptr;
+    if (nx < 1 || ny < 1 || nz < 1 || nx > 1024 || ny > 1024 || nz > 1024 || nz > 65535 || !(dx > 0) || !(dy > 0) ||
+        !(dz > 0)) {
+        wp_set_error_msg("wp_dst3d_create: extents must be in [1, 1024] and spacings > 0");
+        return WP_ERR_INVALID_ARG;
+    }
+    wp_dst3d* h = new (std::nothrow) wp_dst3d();
+    if (!h) return WP_ERR_INVALID_ARG;
+    const int n[3] = {nx, ny, nz};
+    const double hs[3] = {dx, dy, dz};
+    for (int a = 0; a < 3; ++a) {
+        h->n[a] = n[a];
+        h->h[a] = hs[a];
+        const int m = n[a];
+        std::vector<double> M((size_t)m * m);
+        const double sc = std::sqrt(2.0 / (m + 1));
+        for (int k = 0; k < m; ++k)
+            for (int j = 0; j < m; ++j) M[(size_t)k * m + j] = sc * std::sin(M_PI * (double)(j + 1) * (k + 1) / (m + 1));
+        cudaError_t e = cudaMalloc((void**)&h->M[a], sizeof(double) * M.size());
+        if (e == cudaSuccess) e = cudaMemcpy(h->M[a], M.data(), sizeof(double) * M.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "dst3d create", __FILE__, __LINE__); wp_dst3d_destroy(h); return WP_ERR_CUDA; }
+    }
+    cudaError_t e = cudaMalloc((void**)&h->tmp, sizeof(double) * (size_t)nx * ny * nz);
+    if (e != cudaSuccess) { wp_set_cuda_error(e, "dst3d create", __FILE__, __LINE__); wp_dst3d_destroy(h); return WP_ERR_CUDA; }
+    *out = h;
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_dst3d_solve(wp_dst3d* h, double* dst, const double* f, void* stream) {
+    if (!h || !dst || !f) { wp_set_error_msg("wp_dst3d_solve: null pointer"); return WP_ERR_INVALID_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+    // forward x, y, z; eigen division; inverse z, y, x (ping-pong between dst and tmp)
+    cudaError_t e;
+    if ((e = apply_axis(f, h->tmp, h->M[0], nx, ny, nz, 'x', s)) != cudaSuccess) goto fail;
+    if ((e = apply_axis(h->tmp, dst, h->M[1], nx, ny, nz, 'y', s)) != cudaSuccess) goto fail;
+    if ((e = apply_axis(dst, h->tmp, h->M[2], nx, ny, nz, 'z', s)) != cudaSuccess) goto fail;
+    {
+        const int tok = wp_prof_start(s);
+        dst_eig_kernel<<<dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz), dim3(32, 8), 0, s>>>(h->tmp, nx, ny, nz,
+                                                                                       h->h[0] * h->h[1]);
+        e = cudaGetLastError();
+        wp_prof_stop(tok, "dst_eigen", 16.0 * nx * ny * nz, s);
+        if (e != cudaSuccess) goto fail;
+    }
+    if ((e = apply_axis(h->tmp, dst, h->M[2], nx, ny, nz, 'z', s)) != cudaSuccess) goto fail;
+    if ((e = apply_axis(dst, h->tmp, h->M[1], nx, ny, nz, 'y', s)) != cudaSuccess) goto fail;
+    if ((e = apply_axis(h->tmp, dst, h->M[0], nx, ny, nz, 'x', s)) != cudaSuccess) goto fail;
+    return WP_OK;
+fail:
+    wp_set_cuda_error(e, "dst3d solve", __FILE__, __LINE__);
+    return WP_ERR_CUDA;
+}
+
+extern "C" CUWHHD_API wp_status wp_dst3d_destroy(wp_dst3d* h) {
+    if (!h) return WP_OK;
+    for (int a = 0; a < 3; ++a) if (h->M[a]) cudaFree(h->M[a]);
+    if (h->tmp) cudaFree(h->tmp);
+    delete h;
+    return WP_OK;
+}

@@ -77,6 +77,133 @@ __global__ void __launch_bounds__(256) jacobi_kernel(T* __restrict__ dst, const 
     dst[i] = dg > (T)kEps ? ((T)1 - w) * c + w * (f[i] - od) / dg : (T)0;
 }
 
+// Column walker: the row of cell (x, y, z) for z = z0, z0+1, ... with the z neighbours and the
+// z-face fraction carried in registers, so each v and az value of the column is loaded once;
+// in-plane neighbours come through L1 (they are loaded by the neighbouring threads of the CTA).
+template <typename T, typename TV, bool PROL>
+struct ZCol {
+    const Lvl<T>& L;
+    const TV* __restrict__ v;
+    const TV* __restrict__ vc;
+    int ncx, ncy, x, y, z;
+    long sxy, i, iax, iay, sax, say;
+    T vm, vcur, az_lo, gxl, gxh, gyl, gyh;
+
+    __device__ __forceinline__ T V(long ii, int xx, int yy, int zz) const {
+        T r = (T)v[ii];
+        if (PROL) r += (T)vc[(yy >> 1) + (long)(xx >> 1) * ncy + (long)(zz >> 1) * ncx * ncy];
+        return r;
+    }
+
+    __device__ __forceinline__ ZCol(const Lvl<T>& L_, const TV* v_, const TV* vc_, int ncx_, int ncy_, int x_, int y_,
+                                    int z0)
+        : L(L_), v(v_), vc(vc_), ncx(ncx_), ncy(ncy_), x(x_), y(y_), z(z0) {
+        sxy = (long)L.nx * L.ny;
+        i = y + (long)x * L.ny + z0 * sxy;
+        sax = (long)(L.nx + 1) * L.ny;
+        say = (long)L.nx * (L.ny + 1);
+        iax = y + (long)x * L.ny + z0 * sax;
+        iay = y + (long)x * (L.ny + 1) + z0 * say;
+        vm = z0 > 0 ? V(i - sxy, x, y, z0 - 1) : (T)0;
+        vcur = V(i, x, y, z0);
+        az_lo = z0 > 0 ? (T)L.az[i] : (T)0;
+        gxl = L.glo[0][x];
+        gxh = L.ghi[0][x];
+        gyl = L.glo[1][y];
+        gyh = L.ghi[1][y];
+    }
+
+    // diag, off-diagonal sum and centre value of the current cell; then advances one plane
+    __device__ __forceinline__ void step(T& dg, T& od, T& c) {
+        const int nx = L.nx, ny = L.ny, nz = L.nz;
+        T d = 0, o = 0, cf;
+        if (y > 0) { cf = (T)L.ay[iay] * gyl; d += cf; o -= cf * V(i - 1, x, y - 1, z); }
+        if (y < ny - 1) { cf = (T)L.ay[iay + 1] * gyh; d += cf; o -= cf * V(i + 1, x, y + 1, z); }
+        if (x > 0) { cf = (T)L.ax[iax] * gxl; d += cf; o -= cf * V(i - ny, x - 1, y, z); }
+        if (x < nx - 1) { cf = (T)L.ax[iax + ny] * gxh; d += cf; o -= cf * V(i + ny, x + 1, y, z); }
+        T vp = 0, az_hi = 0;
+        if (z > 0) { cf = az_lo * L.glo[2][z]; d += cf; o -= cf * vm; }
+        if (z < nz - 1) {
+            vp = V(i + sxy, x, y, z + 1);
+            az_hi = (T)L.az[i + sxy];
+            cf = az_hi * L.ghi[2][z];
+            d += cf;
+            o -= cf * vp;
+        }
+        dg = d;
+        od = o;
+        c = vcur;
+        vm = vcur;
+        vcur = vp;
+        az_lo = az_hi;
+        i += sxy;
+        iax += sax;
+        iay += say;
+        ++z;
+    }
+};
+
+template <typename T, bool PROL>
+__global__ void __launch_bounds__(256) jacobi_z_kernel(T* __restrict__ dst, const T* __restrict__ src,
+                                                       const T* __restrict__ f, Lvl<T> L, T w,
+                                                       const T* __restrict__ vc, int ncx, int ncy, int zc) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
+    const int z0 = blockIdx.z * zc, z1 = min(z0 + zc, L.nz);
+    if (y >= L.ny || x >= L.nx || z0 >= z1) return;
+    ZCol<T, T, PROL> col(L, src, vc, ncx, ncy, x, y, z0);
+    for (int z = z0; z < z1; ++z) {
+        const long i = col.i;
+        T dg, od, c;
+        col.step(dg, od, c);
+        dst[i] = dg > (T)kEps ? ((T)1 - w) * c + w * (f[i] - od) / dg : (T)0;
+    }
+}
+
+// Fused residual + restriction: each thread walks one fine column, the 2 x 2 children in (y, x)
+// are combined with a lane shuffle and a shared-memory exchange, the 2 children in z in registers.
+// Coarse value = sum of (dx_x dx_y dx_z / sums) weighted fine residuals (cuRestrict3D.cu:801-970).
+template <typename T>
+__global__ void __launch_bounds__(256) resid_restrict_z_kernel(T* __restrict__ fc, const T* __restrict__ v,
+                                                               const T* __restrict__ f, Lvl<T> L, int ncx, int ncy,
+                                                               int ncz, int czc) {
+    __shared__ T red[8][16];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int y = blockIdx.x * 32 + tx, x = blockIdx.y * 8 + ty;
+    const int cz0 = blockIdx.z * czc, cz1 = min(cz0 + czc, ncz);
+    const bool in = y < L.ny && x < L.nx;
+    T wxy = 0;
+    if (in) {
+        const int y0 = y & ~1, x0 = x & ~1;
+        const double sy = L.d[1][y0] + (y0 + 1 < L.ny ? L.d[1][y0 + 1] : 0.0);
+        const double sx = L.d[0][x0] + (x0 + 1 < L.nx ? L.d[0][x0 + 1] : 0.0);
+        wxy = (T)(L.d[1][y] / sy * (L.d[0][x] / sx));
+    }
+    ZCol<T, T, false> col(L, v, nullptr, 0, 0, in ? x : 0, in ? y : 0, 2 * cz0);
+    for (int cz = cz0; cz < cz1; ++cz) {
+        T acc = 0;
+        const int zb = 2 * cz;
+        const double sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
+        for (int k = 0; k < 2; ++k) {
+            const int z = zb + k;
+            if (z < L.nz && in) {
+                const long i = col.i;
+                T dg, od, c;
+                col.step(dg, od, c);
+                const T r = dg > (T)kEps ? f[i] - (dg * c + od) : (T)0;
+                acc += (T)(L.d[2][z] / sz) * wxy * r;
+            }
+        }
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        if ((tx & 1) == 0) red[ty][tx >> 1] = acc;
+        __syncthreads();
+        if (ty < 4 && tx < 16) {
+            const int cy = blockIdx.x * 16 + tx, cx = blockIdx.y * 4 + ty;
+            if (cy < ncy && cx < ncx) fc[cy + (long)cx * ncy + (long)cz * ncx * ncy] = red[2 * ty][tx] + red[2 * ty + 1][tx];
+        }
+        __syncthreads();
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) prolong_add_kernel(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny,
                                                           int nz, int ncx, int ncy) {
@@ -203,6 +330,36 @@ __global__ void __launch_bounds__(256) defect64_kernel(float* __restrict__ r32, 
 // walls the operator's null space is the constant on the active cells, so a right-hand side stored
 // in FP32 carries an incompatible constant part of FP32 rounding size that floors the residual
 // (about 2e-10 relative at 64^3); the tolerance-driven solve removes that mean in FP64.
+template <typename TP>
+__global__ void __launch_bounds__(256) defect64_z_kernel(float* __restrict__ r32, const TP* __restrict__ p,
+                                                         const float* __restrict__ f, Lvl<double> L, double m,
+                                                         double* __restrict__ acc, int zc) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
+    const int z0 = blockIdx.z * zc, z1 = min(z0 + zc, L.nz);
+    double s2 = 0.0;
+    if (y < L.ny && x < L.nx && z0 < z1) {
+        ZCol<double, TP, false> col(L, p, nullptr, 0, 0, x, y, z0);
+        for (int z = z0; z < z1; ++z) {
+            const long i = col.i;
+            double dg, od, c;
+            col.step(dg, od, c);
+            const double r = dg > kEps ? ((double)f[i] - m) - (dg * c + od) : 0.0;
+            if (r32) r32[i] = (float)r;
+            s2 += r * r;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    __shared__ double red[8];
+    const int lane = threadIdx.x + 32 * threadIdx.y;
+    if ((lane & 31) == 0) red[lane >> 5] = s2;
+    __syncthreads();
+    if (lane == 0) {
+        double t = 0.0;
+        for (int k = 0; k < 8; ++k) t += red[k];
+        atomicAdd(acc, t);
+    }
+}
+
 __global__ void __launch_bounds__(256) active_sum_kernel(const float* __restrict__ f, Lvl<double> L,
                                                          double* __restrict__ acc) {
     const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
@@ -340,6 +497,18 @@ Lvl<double> view<double>(const Level& L) {
 
 dim3 grid_of(int nx, int ny, int nz) { return dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz); }
 
+// z chunk of the column-walking kernels: long columns (register reuse) while keeping >= 4 CTAs
+// per SM in flight
+int zchunk(int nx, int ny, int nz) {
+    const long cols = (long)wp_cdiv(ny, 32) * wp_cdiv(nx, 8);
+    const long want = 4L * wp_sm_count();
+    long nzc = (want + cols - 1) / cols;
+    if (nzc < 1) nzc = 1;
+    if (nzc > nz) nzc = nz;
+    return (int)((nz + nzc - 1) / nzc);
+}
+dim3 grid_z(int nx, int ny, int nz, int zc) { return dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8), wp_cdiv(nz, zc)); }
+
 }  // namespace
 
 struct wp_mgfrac3d {
@@ -455,10 +624,12 @@ struct Bufs<double> {
 template <typename T>
 wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s) {
     const Lvl<T> V = view<T>(L);
-    const dim3 g = grid_of(L.n[0], L.n[1], L.n[2]);
+    const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
+    const dim3 g = grid_z(L.n[0], L.n[1], L.n[2], zc);
     for (int k = 0; k < sweeps; ++k) {
         WP_KERNEL("jacobi", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
-                  jacobi_kernel<T, false><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::t(L), Bufs<T>::v(L), f, V, w, nullptr, 0, 0));
+                  jacobi_z_kernel<T, false><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::t(L), Bufs<T>::v(L), f, V, w, nullptr,
+                                                                      0, 0, zc));
         T* tmp = Bufs<T>::v(L);
         Bufs<T>::v(L) = Bufs<T>::t(L);
         Bufs<T>::t(L) = tmp;
@@ -474,9 +645,14 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
     if (l < h->nl - 1) {
         if ((st = smooth<T>(L, f, nu1, w, s)) != WP_OK) return st;
         Level& C = h->lv[l + 1];
-        WP_KERNEL("resid_restrict", (double)L.cells * (2.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
-                  resid_restrict_kernel<T><<<grid_of(C.n[0], C.n[1], C.n[2]), dim3(32, 8), 0, s>>>(
-                      Bufs<T>::f(C), Bufs<T>::v(L), f, view<T>(L), C.n[0], C.n[1], C.n[2]));
+        {
+            // coarse-z chunk so the fine columns keep >= 4 CTAs per SM busy
+            const int czc = (zchunk(L.n[0], L.n[1], L.n[2]) + 1) / 2;
+            const dim3 gr(wp_cdiv(L.n[1], 32), wp_cdiv(L.n[0], 8), wp_cdiv(C.n[2], czc));
+            WP_KERNEL("resid_restrict", (double)L.cells * (2.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
+                      resid_restrict_z_kernel<T><<<gr, dim3(32, 8), 0, s>>>(Bufs<T>::f(C), Bufs<T>::v(L), f, view<T>(L),
+                                                                           C.n[0], C.n[1], C.n[2], czc));
+        }
         WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(C), 0, sizeof(T) * C.cells, s));
         if ((st = vcycle<T>(h, l + 1, Bufs<T>::f(C), nu1, nu2, w, prolong, s)) != WP_OK) return st;
         if (prolong == WP_PROLONG_TRILINEAR) {
@@ -486,9 +662,10 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
             if ((st = smooth<T>(L, f, nu2, w, s)) != WP_OK) return st;
         } else if (nu2 > 0) {
             // first post-sweep reads v + P vc directly (prolongation fused into the sweep)
+            const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
             WP_KERNEL("jacobi_prolong", (double)L.cells * (3.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
-                      jacobi_kernel<T, true><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::t(L), Bufs<T>::v(L), f, view<T>(L), w,
-                                                                       Bufs<T>::v(C), C.n[0], C.n[1]));
+                      jacobi_z_kernel<T, true><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(
+                          Bufs<T>::t(L), Bufs<T>::v(L), f, view<T>(L), w, Bufs<T>::v(C), C.n[0], C.n[1], zc));
             T* tmp = Bufs<T>::v(L);
             Bufs<T>::v(L) = Bufs<T>::t(L);
             Bufs<T>::t(L) = tmp;
@@ -530,9 +707,10 @@ wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r
                  double* norm_f2, cudaStream_t s) {
     Level& L = h->lv[0];
     WP_CUDA_TRY(cudaMemsetAsync(h->acc, 0, 2 * sizeof(double), s));
+    const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
     WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 16.0 + (r32 ? 4.0 : 0.0)), s,
-              defect64_kernel<TP><<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(r32, p, f, view<double>(L),
-                                                                                         m, h->acc));
+              defect64_z_kernel<TP><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(
+                  r32, p, f, view<double>(L), m, h->acc, zc));
     if (norm_f2) {
         const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
         WP_KERNEL("sumsq", 4.0 * L.cells, s, sumsq_kernel<float><<<b, 256, 0, s>>>(f, L.cells, h->acc + 1));

@@ -148,6 +148,44 @@ __global__ void __launch_bounds__(256) sdf_spheres_kernel(float* __restrict__ sd
     sdf[y + (long)x * ny + (long)z * nx * ny] = best;
 }
 
+// union with axis-aligned boxes: exact box signed distance, min with the existing level set
+struct Box {
+    float lo[3], hi[3];
+};
+
+__global__ void __launch_bounds__(256) sdf_boxes_kernel(float* __restrict__ sdf, int nx, int ny, int nz, float h,
+                                                        const Box* __restrict__ bx, int count) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    const float p[3] = {(x + 0.5f) * h, (y + 0.5f) * h, (z + 0.5f) * h};
+    const long i = y + (long)x * ny + (long)z * nx * ny;
+    float best = sdf[i];
+    for (int b = 0; b < count; ++b) {
+        float out = 0.f, inside = -1e30f;
+        for (int c = 0; c < 3; ++c) {
+            const float ctr = 0.5f * (bx[b].lo[c] + bx[b].hi[c]), half = 0.5f * (bx[b].hi[c] - bx[b].lo[c]);
+            const float q = fabsf(p[c] - ctr) - half;
+            if (q > 0.f) out += q * q;
+            inside = fmaxf(inside, q);
+        }
+        best = fminf(best, sqrtf(out) + fminf(inside, 0.f));
+    }
+    sdf[i] = best;
+}
+
+__global__ void __launch_bounds__(256) sdf_circles_kernel(float* __restrict__ sdf, int nx, int ny, float h,
+                                                          const Sphere* __restrict__ sp, int count) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
+    if (y >= ny || x >= nx) return;
+    const float px = (x + 0.5f) * h, py = (y + 0.5f) * h;
+    float best = 1e30f;
+    for (int s = 0; s < count; ++s) {
+        const float dx = px - sp[s].c[0], dy = py - sp[s].c[1];
+        best = fminf(best, sqrtf(dx * dx + dy * dy) - sp[s].r);
+    }
+    sdf[y + (long)x * ny] = best;
+}
+
 __device__ __forceinline__ float frac_from_ls(float h, float l, float r) {
     const float dif = r - l;
     const float d = sqrtf(fmaxf(h * h - dif * dif, 1e-14f));
@@ -169,6 +207,19 @@ __global__ void __launch_bounds__(256) frac3d_kernel(float* __restrict__ ax, flo
     if (y < ny && x < nx && z <= nz) {
         const int zl = max(z - 1, 0), zr = min(z, nz - 1);
         az[y + (long)x * ny + (long)z * s] = frac_from_ls(h, ls[y + (long)x * ny + zl * s], ls[y + (long)x * ny + zr * s]);
+    }
+}
+
+__global__ void __launch_bounds__(256) frac2d_kernel(float* __restrict__ ax, float* __restrict__ ay,
+                                                     const float* __restrict__ ls, int nx, int ny, float h) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
+    if (y < ny && x <= nx) {
+        const int xl = max(x - 1, 0), xr = min(x, nx - 1);
+        ax[y + (long)x * ny] = frac_from_ls(h, ls[y + (long)xl * ny], ls[y + (long)xr * ny]);
+    }
+    if (y <= ny && x < nx) {
+        const int yl = max(y - 1, 0), yr = min(y, ny - 1);
+        ay[y + (long)x * (ny + 1)] = frac_from_ls(h, ls[yl + (long)x * ny], ls[yr + (long)x * ny]);
     }
 }
 
@@ -299,5 +350,67 @@ extern "C" CUWHHD_API wp_status wp_fractions3d(float* ax, float* ay, float* az, 
     cudaStream_t s = (cudaStream_t)stream;
     WP_KERNEL("fractions", 4.0 * (4.0 * nx * ny * nz), s,
               frac3d_kernel<<<grid, dim3(32, 8), 0, s>>>(ax, ay, az, sdf, nx, ny, nz, (float)dx));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_sdf_boxes3d(float* sdf, int nx, int ny, int nz, double dx, const double* lo,
+                                               const double* hi, int count, void* stream) {
+    if (!sdf || nx <= 0 || ny <= 0 || nz <= 0 || nz > 65535 || count < 0 || count > 4096 ||
+        (count > 0 && (!lo || !hi))) {
+        wp_set_error_msg("wp_sdf_boxes3d: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (count == 0) return WP_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<Box> hb(count);
+    for (int i = 0; i < count; ++i)
+        for (int c = 0; c < 3; ++c) { hb[i].lo[c] = (float)lo[3 * i + c]; hb[i].hi[c] = (float)hi[3 * i + c]; }
+    Box* d = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(Box) * count, s));
+    WP_CUDA_TRY(cudaMemcpyAsync(d, hb.data(), sizeof(Box) * count, cudaMemcpyHostToDevice, s));
+    const int tok = wp_prof_start(s);
+    sdf_boxes_kernel<<<dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz), dim3(32, 8), 0, s>>>(sdf, nx, ny, nz, (float)dx, d, count);
+    cudaError_t e = cudaGetLastError();
+    wp_prof_stop(tok, "sdf_boxes", 8.0 * nx * ny * nz, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFreeAsync(d, s);
+    if (e != cudaSuccess || e2 != cudaSuccess) { wp_set_cuda_error(e != cudaSuccess ? e : e2, "sdf boxes", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_sdf_circles2d(float* sdf, int nx, int ny, double dx, const double* centers,
+                                                 const double* radii, int count, void* stream) {
+    if (!sdf || nx <= 0 || ny <= 0 || count < 0 || count > 4096 || (count > 0 && (!centers || !radii))) {
+        wp_set_error_msg("wp_sdf_circles2d: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<Sphere> hs(count > 0 ? count : 1);
+    for (int i = 0; i < count; ++i) {
+        hs[i].c[0] = (float)centers[2 * i];
+        hs[i].c[1] = (float)centers[2 * i + 1];
+        hs[i].c[2] = 0.f;
+        hs[i].r = (float)radii[i];
+    }
+    Sphere* d = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(Sphere) * hs.size(), s));
+    WP_CUDA_TRY(cudaMemcpyAsync(d, hs.data(), sizeof(Sphere) * hs.size(), cudaMemcpyHostToDevice, s));
+    const int tok = wp_prof_start(s);
+    sdf_circles_kernel<<<dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8)), dim3(32, 8), 0, s>>>(sdf, nx, ny, (float)dx, d, count);
+    cudaError_t e = cudaGetLastError();
+    wp_prof_stop(tok, "sdf_circles", 4.0 * nx * ny, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFreeAsync(d, s);
+    if (e != cudaSuccess || e2 != cudaSuccess) { wp_set_cuda_error(e != cudaSuccess ? e : e2, "sdf circles", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_fractions2d(float* ax, float* ay, const float* sdf, int nx, int ny, double dx,
+                                               void* stream) {
+    if (!ax || !ay || !sdf || nx <= 0 || ny <= 0) { wp_set_error_msg("wp_fractions2d: bad arguments"); return WP_ERR_INVALID_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    WP_KERNEL("fractions2d", 4.0 * 3.0 * nx * ny, s,
+              frac2d_kernel<<<dim3(wp_cdiv(ny + 1, 32), wp_cdiv(nx + 1, 8)), dim3(32, 8), 0, s>>>(ax, ay, sdf, nx, ny,
+                                                                                               (float)dx));
     return WP_OK;
 }
