@@ -172,6 +172,7 @@ CUWHHD_API wp_status wp_mgfrac2d_destroy(wp_mgfrac2d* h);
 CUWHHD_API wp_status wp_divergence_frac3d(float* b, const float* xv, const float* yv, const float* zv, const float* ax,
                                           const float* ay, const float* az, int nx, int ny, int nz, double dx,
                                           double dy, double dz, void* stream);
+/* 2D form (CuConvergence::GetB_2d_frac_vel); ax, ay both NULL means fully open faces. */
 CUWHHD_API wp_status wp_divergence_frac2d(float* b, const float* xv, const float* yv, const float* ax, const float* ay,
                                           int nx, int ny, double dx, double dy, void* stream);
 /* u <- (u - grad p) [* a]: CuGradient::Gradient3D_Frac_P (cuGradient.cu:2520-2540) followed by
@@ -210,6 +211,33 @@ CUWHHD_API wp_status wp_dst3d_create(wp_dst3d** h, int nx, int ny, int nz, doubl
    dst may equal f; solves -lap_h p = f with p = 0 outside the grid (scaled by dx*dy as the reference). */
 CUWHHD_API wp_status wp_dst3d_solve(wp_dst3d* h, double* dst, const double* f, void* stream);
 CUWHHD_API wp_status wp_dst3d_destroy(wp_dst3d* h);
+
+/* ------------------------------------------------------------- batched projection ------- */
+/* No reference counterpart: the reference projects one grid per process.  A batch holds `count`
+   independent grids of uneven sizes (dims[i] = 2 or 3, extents ext[3*i..3*i+2] (z ignored for 2D),
+   uniform spacing dx[i], caller-owned face fractions ax[i], ay[i], az[i] (az may be NULL when all
+   grids are 2D)).  Each grid is projected as the reference test does for one grid
+   (TestLocalProjection.cpp:666-767): b = -div(a u), a mixed-precision multigrid solve, u <- (u -
+   grad p) a, max|div u|, wavelet potential recovery.  wp_batch_plan runs every grid once eagerly
+   (tolerance-driven, params->rel_tol) to fix its number of refinement steps; wp_batch_run then
+   launches the whole batch as ONE CUDA graph whose grids are spread over `nstreams` concurrent
+   branches (the graph is captured on the first run and again whenever the field pointers change). */
+typedef struct wp_batch wp_batch;
+CUWHHD_API wp_status wp_batch_create(wp_batch** h, int count, const int* dims, const int* ext, const double* dx,
+                                     const float* const* ax, const float* const* ay, const float* const* az,
+                                     const wp_mg_params* params, int nstreams);
+/* Synchronous; velocities are read only.  cycles (may be NULL) receives each grid's step count. */
+CUWHHD_API wp_status wp_batch_plan(wp_batch* h, const float* const* xv, const float* const* yv, const float* const* zv,
+                                   int* cycles, void* stream);
+/* Projects every grid in place (xv, yv, zv) and writes the potentials (qx, qy, qz; 2D grids write
+   qz only and may pass NULL in zv/qx/qy).  Asynchronous on `stream`. */
+CUWHHD_API wp_status wp_batch_run(wp_batch* h, float* const* xv, float* const* yv, float* const* zv, float* const* qx,
+                                  float* const* qy, float* const* qz, void* stream);
+/* Per grid: max|div u| after projection and the final FP64 relative residual of the last run;
+   any output may be NULL.  Synchronous. */
+CUWHHD_API wp_status wp_batch_results(wp_batch* h, double* max_abs_div, double* rel_residual, int* cycles,
+                                      void* stream);
+CUWHHD_API wp_status wp_batch_destroy(wp_batch* h);
 
 #ifdef __cplusplus
 }

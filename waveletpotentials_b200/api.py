@@ -20,7 +20,7 @@ from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONS
 
 __all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRecover2D", "CuMultigridFrac3D",
            "CuMultigridFrac2D", "CuConvergence", "CuGradient", "CuSolidLevelSet3D", "CuSolidLevelSet2D", "CuDst3D",
-           "Projector3D", "max_abs",
+           "Projector3D", "Projector2D", "BatchProjector", "max_abs",
            "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
            "PROLONG_TRILINEAR", "mac_shapes3d", "mac_shapes2d"]
 
@@ -446,3 +446,135 @@ class Projector3D:
         rep["max_abs_div"] = max_abs(self.b, stream)
         self.rec.Solve(qx, qy, qz, xv, yv, zv, stream)
         return rep
+
+
+class Projector2D:
+    """2D form of Projector3D (CuMultigridFrac2D + CuWaveletPotentialRecover2D)."""
+
+    def __init__(self, ax, ay, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, stream=None):
+        self.dim = tuple(int(v) for v in dim)
+        self.dx = float(dx)
+        self.ax, self.ay = ax, ay
+        self.mg = CuMultigridFrac2D(ax, ay, self.dim, self.dx, "n", stream)
+        self.rec = CuWaveletPotentialRecover2D(self.dim, self.dx, "n")
+        self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
+                         prolongation=prolongation)
+        s = mac_shapes2d(*self.dim)
+        self.b = torch.empty(s["p"], device="cuda", dtype=torch.float32)
+        self.p = torch.empty(s["p"], device="cuda", dtype=torch.float32)
+
+    def run(self, xv, yv, qz, pre_p=None, stream=None) -> dict:
+        CuConvergence.GetB_2d_frac_vel(self.b, xv, yv, self.ax, self.ay, self.dim, self.dx, stream=stream)
+        rep = self.mg.SolveTol(self.p, pre_p, self.b, raise_on_fail=False, stream=stream, **self.opts)
+        CuGradient.SubtractGradient2D_Frac_P(xv, yv, self.p, self.ax, self.ay, self.dim, self.dx, multiply_frac=True,
+                                             stream=stream)
+        CuConvergence.GetB_2d_frac_vel(self.b, xv, yv, None, None, self.dim, self.dx, stream=stream)
+        rep["max_abs_div"] = max_abs(self.b, stream)
+        self.rec.Solve(qz, xv, yv, stream)
+        return rep
+
+
+def _parray(ptrs):
+    arr = (ctypes.c_void_p * len(ptrs))(*[p.value if isinstance(p, ctypes.c_void_p) else p for p in ptrs])
+    return arr
+
+
+class BatchProjector:
+    """Many independent projections of uneven 2D/3D grids launched as one CUDA graph (wp_batch_*).
+
+    ``grids`` is a list of dicts ``{"dim": (nx, ny[, nz]), "dx": h, "ax": ..., "ay": ...[, "az": ...]}``;
+    a grid is 3D when its ``dim`` has three extents.  ``plan(fields)`` fixes each grid's refinement
+    steps with an eager tolerance-driven solve; ``run(fields, outs)`` projects every grid in place and
+    writes its potential.  ``fields[i]`` is ``(xv, yv, zv)`` (3D) or ``(xv, yv)`` (2D); ``outs[i]`` is
+    ``(qx, qy, qz)`` or ``(qz,)``.
+    """
+
+    def __init__(self, grids, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
+                 prolongation=PROLONG_TRILINEAR, nstreams=8):
+        self.grids = grids
+        self.count = len(grids)
+        dims, ext, dx, ax, ay, az = [], [], [], [], [], []
+        self.shapes = []
+        for g in grids:
+            d = tuple(int(v) for v in g["dim"])
+            if len(d) == 3:
+                s = mac_shapes3d(*d)
+                dims.append(3)
+                ext += list(d)
+                az.append(_ptr(g["az"], s["zv"], name="az").value)
+            else:
+                s = mac_shapes2d(*d)
+                dims.append(2)
+                ext += [d[0], d[1], 1]
+                az.append(None)
+            self.shapes.append(s)
+            dx.append(float(g["dx"]))
+            ax.append(_ptr(g["ax"], s["xv"], name="ax").value)
+            ay.append(_ptr(g["ay"], s["yv"], name="ay").value)
+        self.dims = dims
+        prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), PREC_MIXED,
+                       int(prolongation))
+        h = ctypes.c_void_p()
+        self._keep = ((ctypes.c_int * self.count)(*dims), (ctypes.c_int * (3 * self.count))(*ext),
+                      (ctypes.c_double * self.count)(*dx), _parray(ax), _parray(ay), _parray(az), prm)
+        k = self._keep
+        check(lib().wp_batch_create(ctypes.byref(h), self.count, ctypes.cast(k[0], ctypes.c_void_p),
+                                    ctypes.cast(k[1], ctypes.c_void_p), ctypes.cast(k[2], ctypes.c_void_p),
+                                    ctypes.cast(k[3], ctypes.c_void_p), ctypes.cast(k[4], ctypes.c_void_p),
+                                    ctypes.cast(k[5], ctypes.c_void_p), ctypes.byref(prm), int(nstreams)),
+              "wp_batch_create")
+        self._h = h
+
+    def _fields(self, fields, outs=None):
+        names_in = ("xv", "yv", "zv")
+        cols = [[], [], [], [], [], []]
+        for i, s in enumerate(self.shapes):
+            f = fields[i]
+            d3 = self.dims[i] == 3
+            for a in range(3):
+                cols[a].append(_ptr(f[a], s[names_in[a]], name=names_in[a]).value if (a < 2 or d3) else None)
+            if outs is not None:
+                o = outs[i]
+                if d3:
+                    for a, nm in enumerate(("qx", "qy", "qz")):
+                        cols[3 + a].append(_ptr(o[a], s[nm], name=nm).value)
+                else:
+                    cols[3].append(None)
+                    cols[4].append(None)
+                    cols[5].append(_ptr(o[0], s["qz"], name="qz").value)
+        return [_parray(c) for c in cols]
+
+    def plan(self, fields, stream=None):
+        """Eager tolerance-driven pass; returns the refinement steps of each grid (fields unchanged)."""
+        c = self._fields(fields)
+        cyc = (ctypes.c_int * self.count)()
+        check(lib().wp_batch_plan(self._h, ctypes.cast(c[0], ctypes.c_void_p), ctypes.cast(c[1], ctypes.c_void_p),
+                                  ctypes.cast(c[2], ctypes.c_void_p), ctypes.cast(cyc, ctypes.c_void_p),
+                                  _stream(stream)), "wp_batch_plan")
+        return list(cyc)
+
+    def run(self, fields, outs, stream=None):
+        c = self._fields(fields, outs)
+        self._last = c
+        check(lib().wp_batch_run(self._h, *[ctypes.cast(a, ctypes.c_void_p) for a in c], _stream(stream)),
+              "wp_batch_run")
+
+    def results(self, stream=None) -> dict:
+        m = (ctypes.c_double * self.count)()
+        r = (ctypes.c_double * self.count)()
+        cyc = (ctypes.c_int * self.count)()
+        check(lib().wp_batch_results(self._h, ctypes.cast(m, ctypes.c_void_p), ctypes.cast(r, ctypes.c_void_p),
+                                     ctypes.cast(cyc, ctypes.c_void_p), _stream(stream)), "wp_batch_results")
+        return {"max_abs_div": list(m), "rel_residual": list(r), "cycles": list(cyc)}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().wp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

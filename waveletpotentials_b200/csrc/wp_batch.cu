@@ -1,0 +1,298 @@
+// wp_batch.cu -- many independent projections of uneven sizes (2D and 3D) in one CUDA-graph launch.
+//
+// No reference counterpart (the reference runs one grid per process).  Plan: an eager pass per grid
+// (divergence + tolerance-driven mixed-precision solve) fixes each grid's refinement-step count, then
+// the whole batch -- divergence, fixed-count mixed solve, gradient update, max|div|, wavelet
+// recovery for every grid -- is captured once into a CUDA graph with the grids spread over
+// `nstreams` concurrent branches, and replayed with one cudaGraphLaunch.  Per-grid max|div| and the
+// final FP64 relative residual stay on the device until wp_batch_results() reads them with one copy.
+#include "wp_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
+
+struct wp_mgfrac2d;
+wp_status wp_mg_prepare_mixed(wp_mgfrac3d* h);
+wp_status wp_mg_solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
+                                        cudaStream_t s);
+wp_status wp_mg_solve_tol_internal(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm, wp_mg_report* r,
+                                   cudaStream_t s);
+const double* wp_mg_slots(const wp_mgfrac3d* h);
+wp_mgfrac3d* wp_mg2d_impl(wp_mgfrac2d* h);
+wp_status wp_max_abs_device(const float* x, size_t n, unsigned int* d_out, cudaStream_t s);
+
+namespace {
+
+struct Grid {
+    int dims;
+    int n[3];
+    double h;
+    const float* frac[3];
+    wp_mgfrac3d* mg3 = nullptr;
+    wp_mgfrac2d* mg2 = nullptr;
+    wp_recover3d* rec3 = nullptr;
+    wp_recover2d* rec2 = nullptr;
+    float* b = nullptr;
+    float* p = nullptr;
+    int cycles = 0;
+    long cells() const { return (long)n[0] * n[1] * n[2]; }
+    wp_mgfrac3d* mg() const { return dims == 3 ? mg3 : wp_mg2d_impl(mg2); }
+};
+
+__global__ void gather_results_kernel(double* out, const double* const* slots, const unsigned* maxbits, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const double* a = slots[i];
+    out[2 * i] = (double)__uint_as_float(maxbits[i]);
+    out[2 * i + 1] = a[1] > 0.0 ? sqrt(a[0] / a[1]) : 0.0;
+}
+
+}  // namespace
+
+struct wp_batch {
+    std::vector<Grid> g;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+    wp_mg_params prm;
+    unsigned* d_max = nullptr;       // per grid: max|div| bits
+    const double** d_slots = nullptr; // per grid: pointer to the MG handle's norm slots
+    double* d_out = nullptr;         // per grid: (max|div|, rel residual)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> bound;  // pointers captured into the graph
+    long long graph_launches = 0;    // kernels in one replay of the graph
+    bool planned = false;
+};
+
+namespace {
+
+wp_status project_one(wp_batch* B, int i, float* xv, float* yv, float* zv, float* qx, float* qy, float* qz,
+                      cudaStream_t s) {
+    Grid& G = B->g[i];
+    wp_status st;
+    const double h = G.h;
+    if (G.dims == 3) {
+        if ((st = wp_divergence_frac3d(G.b, xv, yv, zv, G.frac[0], G.frac[1], G.frac[2], G.n[0], G.n[1], G.n[2], h, h,
+                                       h, s)) != WP_OK)
+            return st;
+        if ((st = wp_mg_solve_mixed_fixed_async(G.mg3, G.p, G.b, G.cycles, &B->prm, s)) != WP_OK) return st;
+        if ((st = wp_grad_subtract_frac3d(xv, yv, zv, G.p, G.frac[0], G.frac[1], G.frac[2], G.n[0], G.n[1], G.n[2], h, h,
+                                          h, 1, s)) != WP_OK)
+            return st;
+        if ((st = wp_divergence_frac3d(G.b, xv, yv, zv, nullptr, nullptr, nullptr, G.n[0], G.n[1], G.n[2], h, h, h, s)) !=
+            WP_OK)
+            return st;
+        if ((st = wp_max_abs_device(G.b, G.cells(), B->d_max + i, s)) != WP_OK) return st;
+        return wp_recover3d_run(G.rec3, qx, qy, qz, xv, yv, zv, s);
+    }
+    if ((st = wp_divergence_frac2d(G.b, xv, yv, G.frac[0], G.frac[1], G.n[0], G.n[1], h, h, s)) != WP_OK) return st;
+    if ((st = wp_mg_solve_mixed_fixed_async(wp_mg2d_impl(G.mg2), G.p, G.b, G.cycles, &B->prm, s)) != WP_OK) return st;
+    if ((st = wp_grad_subtract_frac2d(xv, yv, G.p, G.frac[0], G.frac[1], G.n[0], G.n[1], h, h, 1, s)) != WP_OK) return st;
+    if ((st = wp_divergence_frac2d(G.b, xv, yv, nullptr, nullptr, G.n[0], G.n[1], h, h, s)) != WP_OK) return st;
+    if ((st = wp_max_abs_device(G.b, G.cells(), B->d_max + i, s)) != WP_OK) return st;
+    return wp_recover2d_run(G.rec2, qz, xv, yv, s);
+}
+
+void destroy_graph(wp_batch* B) {
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    B->exec = nullptr;
+    B->graph = nullptr;
+    B->bound.clear();
+}
+
+}  // namespace
+
+extern "C" CUWHHD_API wp_status wp_batch_create(wp_batch** out, int count, const int* dims, const int* ext,
+                                                const double* dx, const float* const* ax, const float* const* ay,
+                                                const float* const* az, const wp_mg_params* prm, int nstreams) {
+    if (!out) { wp_set_error_msg("wp_batch_create: null handle"); return WP_ERR_INVALID_ARG; }
+    *out = nullptr;
+    if (count <= 0 || !dims || !ext || !dx || !ax || !ay || !prm || nstreams < 1 || nstreams > 64) {
+        wp_set_error_msg("wp_batch_create: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    wp_batch* B = new (std::nothrow) wp_batch();
+    if (!B) return WP_ERR_INVALID_ARG;
+    B->prm = *prm;
+    B->g.resize(count);
+    wp_status st = WP_OK;
+    for (int i = 0; i < count && st == WP_OK; ++i) {
+        Grid& G = B->g[i];
+        G.dims = dims[i];
+        G.n[0] = ext[3 * i];
+        G.n[1] = ext[3 * i + 1];
+        G.n[2] = dims[i] == 3 ? ext[3 * i + 2] : 1;
+        G.h = dx[i];
+        G.frac[0] = ax[i];
+        G.frac[1] = ay[i];
+        G.frac[2] = dims[i] == 3 && az ? az[i] : nullptr;
+        if (G.dims == 3) {
+            if ((st = wp_mgfrac3d_create(&G.mg3, ax[i], ay[i], G.frac[2], G.n[0], G.n[1], G.n[2], G.h, G.h, G.h, 'n',
+                                         nullptr)) != WP_OK)
+                break;
+            if ((st = wp_recover3d_create(&G.rec3, G.n[0], G.n[1], G.n[2], G.h, G.h, G.h, 'n', WP_CDF3_7, WP_CDF4_6)) !=
+                WP_OK)
+                break;
+        } else if (G.dims == 2) {
+            if ((st = wp_mgfrac2d_create(&G.mg2, ax[i], ay[i], G.n[0], G.n[1], G.h, G.h, 'n', nullptr)) != WP_OK) break;
+            if ((st = wp_recover2d_create(&G.rec2, G.n[0], G.n[1], G.h, G.h, 'n', WP_CDF3_7, WP_CDF4_6)) != WP_OK) break;
+        } else {
+            wp_set_error_msg("wp_batch_create: dims must be 2 or 3");
+            st = WP_ERR_INVALID_ARG;
+            break;
+        }
+        if ((st = wp_mg_prepare_mixed(G.mg())) != WP_OK) break;
+        cudaError_t e = cudaMalloc((void**)&G.b, sizeof(float) * G.cells());
+        if (e == cudaSuccess) e = cudaMalloc((void**)&G.p, sizeof(float) * G.cells());
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "batch alloc", __FILE__, __LINE__); st = WP_ERR_CUDA; }
+    }
+    if (st == WP_OK) {
+        B->streams.resize(nstreams);
+        B->events.resize(nstreams + 1);
+        for (auto& s : B->streams) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        for (auto& e : B->events) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        std::vector<const double*> slots(count);
+        for (int i = 0; i < count; ++i) slots[i] = wp_mg_slots(B->g[i].mg());
+        cudaError_t e = cudaMalloc((void**)&B->d_max, sizeof(unsigned) * count);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_slots, sizeof(double*) * count);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_out, sizeof(double) * 2 * count);
+        if (e == cudaSuccess) e = cudaMemcpy(B->d_slots, slots.data(), sizeof(double*) * count, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "batch alloc", __FILE__, __LINE__); st = WP_ERR_CUDA; }
+    }
+    if (st != WP_OK) { wp_batch_destroy(B); return st; }
+    *out = B;
+    return WP_OK;
+}
+
+// Eager pass: per grid, b = -div(a u) and a tolerance-driven mixed solve; records the refinement
+// steps each grid needs (the velocities are not modified).  Synchronous.
+extern "C" CUWHHD_API wp_status wp_batch_plan(wp_batch* B, const float* const* xv, const float* const* yv,
+                                              const float* const* zv, int* cycles_out, void* stream) {
+    if (!B || !xv || !yv) { wp_set_error_msg("wp_batch_plan: null pointer"); return WP_ERR_INVALID_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    for (size_t i = 0; i < B->g.size(); ++i) {
+        Grid& G = B->g[i];
+        wp_status st;
+        if (G.dims == 3)
+            st = wp_divergence_frac3d(G.b, xv[i], yv[i], zv[i], G.frac[0], G.frac[1], G.frac[2], G.n[0], G.n[1], G.n[2],
+                                      G.h, G.h, G.h, s);
+        else
+            st = wp_divergence_frac2d(G.b, xv[i], yv[i], G.frac[0], G.frac[1], G.n[0], G.n[1], G.h, G.h, s);
+        if (st != WP_OK) return st;
+        wp_mg_params prm = B->prm;
+        prm.precision = WP_PREC_MIXED;
+        wp_mg_report rep;
+        st = wp_mg_solve_tol_internal(G.mg(), G.p, G.b, &prm, &rep, s);
+        if (st != WP_OK && st != WP_ERR_NOT_CONVERGED) return st;
+        G.cycles = rep.cycles;
+        if (cycles_out) cycles_out[i] = rep.cycles;
+    }
+    B->planned = true;
+    destroy_graph(B);
+    return WP_OK;
+}
+
+// Runs the whole batch as one CUDA-graph launch (captured on first use or when the pointer set
+// changes).  2D grids use xv, yv and qz only.
+extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, float* const* yv, float* const* zv,
+                                             float* const* qx, float* const* qy, float* const* qz, void* stream) {
+    if (!B || !xv || !yv || !qz) { wp_set_error_msg("wp_batch_run: null pointer"); return WP_ERR_INVALID_ARG; }
+    if (!B->planned) { wp_set_error_msg("wp_batch_run: call wp_batch_plan first"); return WP_ERR_INVALID_ARG; }
+    const int count = (int)B->g.size();
+    std::vector<const void*> ptrs;
+    for (int i = 0; i < count; ++i) {
+        const bool d3 = B->g[i].dims == 3;
+        if (d3 && (!zv || !qx || !qy || !zv[i] || !qx[i] || !qy[i])) {
+            wp_set_error_msg("wp_batch_run: 3D grid without zv/qx/qy");
+            return WP_ERR_INVALID_ARG;
+        }
+        ptrs.insert(ptrs.end(), {xv[i], yv[i], d3 ? zv[i] : nullptr, d3 ? qx[i] : nullptr, d3 ? qy[i] : nullptr, qz[i]});
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!B->exec || ptrs != B->bound) {
+        destroy_graph(B);
+        cudaStream_t cs = B->streams[0];
+        const long long launches0 = wp_launch_count();
+        WP_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        wp_status st = WP_OK;
+        cudaEventRecord(B->events[0], cs);
+        for (size_t k = 1; k < B->streams.size(); ++k) cudaStreamWaitEvent(B->streams[k], B->events[0], 0);
+        // longest grids first, round-robin over the branches
+        std::vector<int> order(count);
+        for (int i = 0; i < count; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return B->g[a].cells() * (B->g[a].cycles + 2) > B->g[b].cells() * (B->g[b].cycles + 2); });
+        for (int k = 0; k < count && st == WP_OK; ++k) {
+            const int i = order[k];
+            const bool d3 = B->g[i].dims == 3;
+            st = project_one(B, i, xv[i], yv[i], d3 ? zv[i] : nullptr, d3 ? qx[i] : nullptr, d3 ? qy[i] : nullptr, qz[i],
+                             B->streams[k % B->streams.size()]);
+        }
+        for (size_t k = 1; k < B->streams.size(); ++k) {
+            cudaEventRecord(B->events[k], B->streams[k]);
+            cudaStreamWaitEvent(cs, B->events[k], 0);
+        }
+        if (st == WP_OK) {
+            const int tok = wp_prof_start(cs);
+            gather_results_kernel<<<wp_cdiv(count, 128), 128, 0, cs>>>(B->d_out, B->d_slots, B->d_max, count);
+            wp_prof_stop(tok, "batch_gather", 24.0 * count, cs);
+        }
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cs, &graph);
+        if (e != cudaSuccess || st != WP_OK) wp_add_launches(-(wp_launch_count() - launches0));
+        if (st != WP_OK) { if (graph) cudaGraphDestroy(graph); return st; }
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "batch capture", __FILE__, __LINE__); return WP_ERR_CUDA; }
+        B->graph = graph;
+        e = cudaGraphInstantiate(&B->exec, graph, 0);
+        if (e != cudaSuccess) { wp_set_cuda_error(e, "batch instantiate", __FILE__, __LINE__); destroy_graph(B); return WP_ERR_CUDA; }
+        B->bound = ptrs;
+        B->graph_launches = wp_launch_count() - launches0;
+        wp_add_launches(-B->graph_launches);
+    }
+    const int tok = wp_prof_start(s);
+    wp_add_launches(B->graph_launches - 1);
+    const cudaError_t e = cudaGraphLaunch(B->exec, s);
+    wp_prof_stop(tok, "batch_graph", 0.0, s);
+    if (e != cudaSuccess) { wp_set_cuda_error(e, "batch graph launch", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    return WP_OK;
+}
+
+// Per grid (max|div| of the projected field, final FP64 relative residual); synchronous.
+extern "C" CUWHHD_API wp_status wp_batch_results(wp_batch* B, double* max_abs_div, double* rel_residual,
+                                                 int* cycles, void* stream) {
+    if (!B) { wp_set_error_msg("wp_batch_results: null handle"); return WP_ERR_INVALID_ARG; }
+    const int count = (int)B->g.size();
+    std::vector<double> out(2 * count);
+    cudaStream_t s = (cudaStream_t)stream;
+    WP_CUDA_TRY(cudaMemcpyAsync(out.data(), B->d_out, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, s));
+    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int i = 0; i < count; ++i) {
+        if (max_abs_div) max_abs_div[i] = out[2 * i];
+        if (rel_residual) rel_residual[i] = out[2 * i + 1];
+        if (cycles) cycles[i] = B->g[i].cycles;
+    }
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_batch_destroy(wp_batch* B) {
+    if (!B) return WP_OK;
+    destroy_graph(B);
+    for (auto& G : B->g) {
+        if (G.mg3) wp_mgfrac3d_destroy(G.mg3);
+        if (G.mg2) wp_mgfrac2d_destroy(G.mg2);
+        if (G.rec3) wp_recover3d_destroy(G.rec3);
+        if (G.rec2) wp_recover2d_destroy(G.rec2);
+        if (G.b) cudaFree(G.b);
+        if (G.p) cudaFree(G.p);
+    }
+    for (auto& s : B->streams) cudaStreamDestroy(s);
+    for (auto& e : B->events) cudaEventDestroy(e);
+    if (B->d_max) cudaFree(B->d_max);
+    if (B->d_slots) cudaFree((void*)B->d_slots);
+    if (B->d_out) cudaFree(B->d_out);
+    delete B;
+    return WP_OK;
+}

@@ -43,6 +43,11 @@ int wp_sm_count();
 // Launch accounting (always) and per-kernel-class event timing (when enabled): wrap a launch as
 //   WP_KERNEL("name", algorithmic_bytes, stream, kernel<<<g, b, smem, stream>>>(...));
 int wp_prof_start(cudaStream_t s);
+// Launch-count adjustment for work replayed from a CUDA graph (captured launches are counted once at
+// capture time; a replay adds them again).
+void wp_add_launches(long long n);
+// Uploads the wavelet filter tables to the current device (once; synchronous).
+cudaError_t wp_dwt_prepare();
 void wp_prof_stop(int tok, const char* name, double bytes, cudaStream_t s);
 #define WP_KERNEL(name, bytes, stream, ...)                         \
     do {                                                            \
@@ -51,6 +56,14 @@ void wp_prof_stop(int tok, const char* name, double bytes, cudaStream_t s);
         WP_LAUNCH_CHECK();                                          \
         wp_prof_stop(_tok, name, (double)(bytes), stream);          \
     } while (0)
+
+// Raises a kernel's dynamic shared-memory limit once per (kernel, device) (a host-side attribute
+// call, kept out of the launch path so launches can be captured into CUDA graphs).
+cudaError_t wp_set_smem_impl(const void* kernel, size_t bytes);
+template <typename K>
+cudaError_t wp_set_smem(K kernel, size_t bytes) {
+    return wp_set_smem_impl(reinterpret_cast<const void*>(kernel), bytes);
+}
 
 // transform along one axis (wp_dwt.cu); T = float or double
 template <typename T>

@@ -69,7 +69,7 @@ template <int C>
 cudaError_t launch_axis(const double* src, double* dst, const double* M, int N, Geom g, int nouter, cudaStream_t s) {
     const size_t smem = (size_t)N * (C + 1) * sizeof(double);
     auto k = dst_axis_kernel<C>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = wp_set_smem(k, smem);
     if (e != cudaSuccess) return e;
     const int tok = wp_prof_start(s);
     k<<<dim3((g.ni + C - 1) / C, nouter), NT, smem, s>>>(src, dst, M, N, g);

@@ -18,6 +18,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 namespace {
 
@@ -343,11 +344,15 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
 }
 
 bool g_const_ready[64] = {false};
+std::mutex g_const_mu;
 
+// Uploads the filter tables once per device (synchronous copy: run at handle creation, before any
+// stream capture).
 cudaError_t ensure_constants() {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_const_mu);
     if (dev < 64 && g_const_ready[dev]) return cudaSuccess;
     double b37[4][16], b46[4][25];
     memcpy(b37, h_base37, sizeof(b37));
@@ -365,7 +370,7 @@ template <int WAV, bool FWD, typename T, int C>
 cudaError_t launch_one(const T* src, T* dst, int N, int levels, int bcd, TileGeom g, int nouter, cudaStream_t s) {
     const size_t smem = (size_t)(FWD ? 2 : 3) * N * (C + 1) * sizeof(T);
     auto kern = dwt_tile_kernel<WAV, FWD, T, C>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = wp_set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     dim3 grid((g.ni + C - 1) / C, nouter);
     const int tok = wp_prof_start(s);
@@ -438,6 +443,8 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
 template wp_status wp_dwt_axis_launch<float>(float*, const float*, int, int, int, int, char, int, char, int, cudaStream_t);
 template wp_status wp_dwt_axis_launch<double>(double*, const double*, int, int, int, int, char, int, char, int,
                                               cudaStream_t);
+
+cudaError_t wp_dwt_prepare() { return ensure_constants(); }
 
 extern "C" CUWHHD_API wp_status wp_dwt1d(float* dst, const float* src, int dim_x, int dim_y, int dim_z, int levels,
                                          char direction, char bc, int wavelet, int forward, void* stream) {

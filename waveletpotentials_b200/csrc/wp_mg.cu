@@ -333,9 +333,11 @@ __global__ void __launch_bounds__(256) defect64_kernel(float* __restrict__ r32, 
 template <typename TP>
 __global__ void __launch_bounds__(256) defect64_z_kernel(float* __restrict__ r32, const TP* __restrict__ p,
                                                          const float* __restrict__ f, Lvl<double> L, double m,
-                                                         double* __restrict__ acc, int zc) {
+                                                         const double* __restrict__ msum, double* __restrict__ acc,
+                                                         int zc) {
     const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
     const int z0 = blockIdx.z * zc, z1 = min(z0 + zc, L.nz);
+    if (msum) m = msum[0] / fmax(msum[1], 1.0);  // mean of f over the active cells, computed on the device
     double s2 = 0.0;
     if (y < L.ny && x < L.nx && z0 < z1) {
         ZCol<double, TP, false> col(L, p, nullptr, 0, 0, x, y, z0);
@@ -679,7 +681,7 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         const size_t smem = 2 * sizeof(T) * L.cells;
         if (smem <= 200 * 1024) {
             auto k = coarsest_kernel<T>;
-            WP_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            WP_CUDA_TRY(wp_set_smem(k, smem));
             WP_KERNEL("coarsest", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
                       k<<<1, 1024, smem, s>>>(Bufs<T>::v(L), f, view<T>(L), w, h->coarsest_iters));
         } else {
@@ -702,6 +704,24 @@ wp_status active_mean(wp_mgfrac3d* h, const float* f, double* m, cudaStream_t s)
     return WP_OK;
 }
 
+// asynchronous FP64 defect: acc[0] = ||f - m - A p||^2 (msum: device mean slots, or NULL to use m),
+// optionally acc[1] = ||f||^2
+template <typename TP>
+wp_status defect_async(wp_mgfrac3d* h, const TP* p, const float* f, double m, const double* msum, float* r32,
+                       bool with_f2, cudaStream_t s) {
+    Level& L = h->lv[0];
+    WP_CUDA_TRY(cudaMemsetAsync(h->acc, 0, (with_f2 ? 2 : 1) * sizeof(double), s));
+    const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
+    WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 16.0 + (r32 ? 4.0 : 0.0)), s,
+              defect64_z_kernel<TP><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(
+                  r32, p, f, view<double>(L), m, msum, h->acc, zc));
+    if (with_f2) {
+        const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
+        WP_KERNEL("sumsq", 4.0 * L.cells, s, sumsq_kernel<float><<<b, 256, 0, s>>>(f, L.cells, h->acc + 1));
+    }
+    return WP_OK;
+}
+
 template <typename TP>
 wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r32, double* norm_r2,
                  double* norm_f2, cudaStream_t s) {
@@ -710,7 +730,7 @@ wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r
     const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
     WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 16.0 + (r32 ? 4.0 : 0.0)), s,
               defect64_z_kernel<TP><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(
-                  r32, p, f, view<double>(L), m, h->acc, zc));
+                  r32, p, f, view<double>(L), m, nullptr, h->acc, zc));
     if (norm_f2) {
         const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
         WP_KERNEL("sumsq", 4.0 * L.cells, s, sumsq_kernel<float><<<b, 256, 0, s>>>(f, L.cells, h->acc + 1));
@@ -857,6 +877,41 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
     return WP_OK;
 }
 
+// Allocates the mixed-precision work arrays ahead of a graph capture.
+wp_status prepare_mixed(wp_mgfrac3d* h) {
+    const long n = h->lv[0].cells;
+    if (!h->p64) WP_CUDA_TRY(cudaMalloc((void**)&h->p64, sizeof(double) * n));
+    if (!h->r32) WP_CUDA_TRY(cudaMalloc((void**)&h->r32, sizeof(float) * n));
+    return WP_OK;
+}
+
+// `cycles` refinement steps of the mixed solve with no host synchronisation (capturable into a
+// CUDA graph): the active mean of f, the defect norms and ||f||^2 stay in the handle's device
+// slots acc[0..3].
+wp_status solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
+                                  cudaStream_t s) {
+    Level& L = h->lv[0];
+    const long n = L.cells;
+    const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
+    wp_status st;
+    if (!h->p64 || !h->r32) { wp_set_error_msg("mixed solve: work arrays not prepared"); return WP_ERR_INVALID_ARG; }
+    WP_CUDA_TRY(cudaMemsetAsync(h->acc + 2, 0, 2 * sizeof(double), s));
+    WP_KERNEL("active_sum", (double)n * 16.0, s,
+              active_sum_kernel<<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(f, view<double>(L), h->acc + 2));
+    WP_CUDA_TRY(cudaMemsetAsync(h->p64, 0, sizeof(double) * n, s));
+    if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, true, s)) != WP_OK) return st;
+    for (int c = 0; c < cycles; ++c) {
+        WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
+        if ((st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s)) != WP_OK)
+            return st;
+        WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+        if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
+    }
+    h->last64 = 1;
+    WP_KERNEL("convert", 12.0 * n, s, convert_kernel<float, double><<<cb, 256, 0, s>>>(dst, h->p64, n));
+    return WP_OK;
+}
+
 wp_status residual_rel(wp_mgfrac3d* h, const float* v, const float* f, double* rel, cudaStream_t s) {
     if (!h || !v || !f || !rel) { wp_set_error_msg("wp_mgfrac_residual: null pointer"); return WP_ERR_INVALID_ARG; }
     double nr2 = 0.0, nf2 = 0.0;
@@ -946,3 +1001,16 @@ extern "C" CUWHHD_API wp_status wp_mgfrac2d_destroy(wp_mgfrac2d* h) {
     delete h;
     return WP_OK;
 }
+
+// ---- internal hooks used by the batched path (wp_batch.cu)
+wp_status wp_mg_prepare_mixed(wp_mgfrac3d* h) { return prepare_mixed(h); }
+wp_status wp_mg_solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
+                                        cudaStream_t s) {
+    return solve_mixed_fixed_async(h, dst, f, cycles, prm, s);
+}
+wp_status wp_mg_solve_tol_internal(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm, wp_mg_report* r,
+                                   cudaStream_t s) {
+    return solve_tol(h, dst, nullptr, f, prm, r, s);
+}
+const double* wp_mg_slots(const wp_mgfrac3d* h) { return h->acc; }
+wp_mgfrac3d* wp_mg2d_impl(wp_mgfrac2d* h) { return h ? h->impl : nullptr; }

@@ -36,13 +36,17 @@ __global__ void __launch_bounds__(256) div3d_kernel(float* __restrict__ b, const
     b[iz] = -v;
 }
 
+template <bool FRAC>
 __global__ void __launch_bounds__(256) div2d_kernel(float* __restrict__ b, const float* __restrict__ xv,
                                                     const float* __restrict__ yv, const float* __restrict__ ax,
                                                     const float* __restrict__ ay, int nx, int ny, float dxi, float dyi) {
     const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
     if (y >= ny || x >= nx) return;
     const long ix = y + (long)x * ny, iy = y + (long)x * (ny + 1);
-    b[ix] = -((xv[ix + ny] * ax[ix + ny] - xv[ix] * ax[ix]) * dxi + (yv[iy + 1] * ay[iy + 1] - yv[iy] * ay[iy]) * dyi);
+    if (FRAC)
+        b[ix] = -((xv[ix + ny] * ax[ix + ny] - xv[ix] * ax[ix]) * dxi + (yv[iy + 1] * ay[iy + 1] - yv[iy] * ay[iy]) * dyi);
+    else
+        b[ix] = -((xv[ix + ny] - xv[ix]) * dxi + (yv[iy + 1] - yv[iy]) * dyi);
 }
 
 // u <- (u - grad p) [* a] on all faces; grad p = 0 on wall faces and where a <= eps
@@ -248,11 +252,21 @@ extern "C" CUWHHD_API wp_status wp_divergence_frac3d(float* b, const float* xv, 
 
 extern "C" CUWHHD_API wp_status wp_divergence_frac2d(float* b, const float* xv, const float* yv, const float* ax,
                                                      const float* ay, int nx, int ny, double dx, double dy, void* stream) {
-    if (!b || !xv || !yv || !ax || !ay || nx <= 0 || ny <= 0) { wp_set_error_msg("wp_divergence_frac2d: bad arguments"); return WP_ERR_INVALID_ARG; }
+    const bool frac = ax || ay;
+    if (!b || !xv || !yv || (frac && (!ax || !ay)) || nx <= 0 || ny <= 0) {
+        wp_set_error_msg("wp_divergence_frac2d: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
     dim3 grid(wp_cdiv(ny, 32), wp_cdiv(nx, 8));
     cudaStream_t s = (cudaStream_t)stream;
-    WP_KERNEL("divergence2d", 4.0 * (4.0 * (nx + 1) * ny + (double)nx * ny), s,
-              div2d_kernel<<<grid, dim3(32, 8), 0, s>>>(b, xv, yv, ax, ay, nx, ny, (float)(1.0 / dx), (float)(1.0 / dy)));
+    const float dxi = (float)(1.0 / dx), dyi = (float)(1.0 / dy);
+    const double faces = 2.0 * (nx + 1) * ny, cells = (double)nx * ny;
+    if (frac)
+        WP_KERNEL("divergence2d", 4.0 * (2 * faces + cells), s,
+                  div2d_kernel<true><<<grid, dim3(32, 8), 0, s>>>(b, xv, yv, ax, ay, nx, ny, dxi, dyi));
+    else
+        WP_KERNEL("divergence2d", 4.0 * (faces + cells), s,
+                  div2d_kernel<false><<<grid, dim3(32, 8), 0, s>>>(b, xv, yv, ax, ay, nx, ny, dxi, dyi));
     return WP_OK;
 }
 

@@ -174,6 +174,11 @@ extern "C" CUWHHD_API wp_status wp_recover3d_create(wp_recover3d** out, int nx, 
         wp_status st = build_axis_table(&h->tab[a], n[a], hs[a], 0);
         if (st != WP_OK) { wp_recover3d_destroy(h); return st; }
     }
+    if (cudaError_t e = wp_dwt_prepare(); e != cudaSuccess) {
+        wp_set_cuda_error(e, "recover3d filters", __FILE__, __LINE__);
+        wp_recover3d_destroy(h);
+        return WP_ERR_CUDA;
+    }
     size_t sz[3] = {(size_t)(nx + 1) * ny * nz, (size_t)nx * (ny + 1) * nz, (size_t)nx * ny * (nz + 1)};
     for (int a = 0; a < 3; ++a) {
         cudaError_t e = cudaMalloc((void**)&h->tmp[a], sizeof(float) * sz[a]);
@@ -273,6 +278,11 @@ extern "C" CUWHHD_API wp_status wp_recover2d_create(wp_recover2d** out, int nx, 
         h->h[a] = hs[a];
         wp_status st = build_axis_table(&h->tab[a], n[a], hs[a], 0);
         if (st != WP_OK) { wp_recover2d_destroy(h); return st; }
+    }
+    if (cudaError_t e = wp_dwt_prepare(); e != cudaSuccess) {
+        wp_set_cuda_error(e, "recover2d filters", __FILE__, __LINE__);
+        wp_recover2d_destroy(h);
+        return WP_ERR_CUDA;
     }
     size_t sz[2] = {(size_t)(nx + 1) * ny, (size_t)nx * (ny + 1)};
     for (int a = 0; a < 2; ++a) {

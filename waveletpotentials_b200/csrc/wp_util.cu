@@ -71,9 +71,15 @@ struct Agg {
 std::vector<Agg> g_agg;
 }  // namespace
 
+void wp_add_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
 int wp_prof_start(cudaStream_t s) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (!g_prof_on.load(std::memory_order_relaxed)) return -1;
+    // launches captured into a graph are not timed one by one (their events would only fire at
+    // replay); the graph launch is timed as a whole by its owner
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return -1;
     std::lock_guard<std::mutex> lk(g_prof_mu);
     ProfRec r{nullptr, take_event(), take_event(), 0.0};
     cudaEventRecord(r.a, s);
@@ -135,4 +141,22 @@ extern "C" CUWHHD_API int wp_profile_entry(int i, char* name, int name_cap, long
     if (ms) *ms = a.ms;
     if (bytes) *bytes = a.bytes;
     return 0;
+}
+
+#include <map>
+#include <utility>
+
+cudaError_t wp_set_smem_impl(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair(kernel, dev);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) done[key] = bytes;
+    return e;
 }
