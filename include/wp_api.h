@@ -151,6 +151,13 @@ CUWHHD_API wp_status wp_mgfrac3d_residual(wp_mgfrac3d* h, const float* v, const 
    reference iterate is DTYPE). */
 CUWHHD_API wp_status wp_mgfrac3d_iterate64(wp_mgfrac3d* h, double* dst, void* stream);
 CUWHHD_API wp_status wp_mgfrac3d_destroy(wp_mgfrac3d* h);
+/* Tile-shape autotuner (no reference counterpart): times the column-walking stencil kernels of
+   every level (Jacobi sweep, fused residual-restriction, FP64 defect) over candidate z-chunks and
+   keeps the fastest per level; results are independent of the choice.  Synchronous; overwrites
+   the handle's work arrays (not the FP64 iterate).  Choices are cached per device and extents for
+   the process.  wp_mgfrac3d_tiles reports 3 chunks per level (jacobi, restrict, defect). */
+CUWHHD_API wp_status wp_mgfrac3d_autotune(wp_mgfrac3d* h, void* stream);
+CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, int cap, int* levels);
 
 typedef struct wp_mgfrac2d wp_mgfrac2d;
 /* Replaces CuMultigridFrac2D(Ax, Ay, int2 dim, DTYPE2 dx, char bc) (cuMultigridFrac2D.cu:28-111). */

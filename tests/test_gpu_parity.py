@@ -340,3 +340,33 @@ def test_recover2d_and_mg2d_full_config0_size(wp, oracle):
     p = torch.zeros(n, device="cuda")
     rep = mg.SolveTol(p, None, T(f), rel_tol=1e-6, max_cycles=40, precision=wp.PREC_FP32)
     assert rep["rel_residual"] <= 1e-6
+
+
+def test_mg_offset_views_and_autotune_keep_results(wp, oracle):
+    """Right-hand sides that are 4-byte-offset views take the scalar column kernels, aligned ones the
+    128-bit quad kernels, and the autotuner only reshapes grids: all give the same cycles."""
+    nn, h, a, _, f = _sphere_problem(wp, oracle, 32, seed=9)
+    mg = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)
+    fa = T(f)
+    buf = torch.zeros(f.size + 1, device="cuda")
+    buf[1:].copy_(fa.reshape(-1))
+    fo = buf[1:].view(f.shape)  # contiguous, data pointer offset by 4 bytes
+    assert fo.data_ptr() % 16 != 0
+    outs = []
+    for rhs in (fa, fo):
+        dst = torch.zeros(f.shape, device="cuda")
+        rep = mg.SolveTol(dst, None, rhs, rel_tol=0.0, max_cycles=6, precision=wp.PREC_FP32)
+        outs.append((N(dst), rep["history"]))
+    assert rel(outs[0][0], outs[1][0]) < 1e-6
+    np.testing.assert_allclose(outs[0][1], outs[1][1], rtol=1e-4)
+    before = mg.Tiles()
+    mg.Autotune()
+    after = mg.Tiles()
+    assert len(before) == len(after) and all(t[0] >= 1 for t in after)
+    dst = torch.zeros(f.shape, device="cuda")
+    dst0 = torch.zeros(f.shape, device="cuda")
+    mg.Solve(dst, None, fa, n_iters=3, nu1=2, nu2=2, weight=2 / 3)
+    mg2 = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)  # heuristic chunks
+    mg2.Solve(dst0, None, fa, n_iters=3, nu1=2, nu2=2, weight=2 / 3)
+    torch.cuda.synchronize()
+    assert torch.equal(dst, dst0)

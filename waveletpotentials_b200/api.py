@@ -203,6 +203,18 @@ class CuMultigridFrac3D:
             check(st, "wp_mgfrac3d_solve_tol")
         return out
 
+    def Autotune(self, stream=None):
+        """Times the level kernels over candidate z-chunks and keeps the fastest (synchronous)."""
+        check(lib().wp_mgfrac3d_autotune(self._h, _stream(stream)), "wp_mgfrac3d_autotune")
+
+    def Tiles(self):
+        """Per level: (jacobi, restrict, defect) z-chunks in use."""
+        buf = (ctypes.c_int * (3 * 32))()
+        nl = ctypes.c_int()
+        check(lib().wp_mgfrac3d_tiles(self._h, ctypes.cast(buf, ctypes.c_void_p), 96, ctypes.byref(nl)),
+              "wp_mgfrac3d_tiles")
+        return [tuple(buf[3 * l:3 * l + 3]) for l in range(nl.value)]
+
     def Iterate64(self, stream=None):
         """FP64 iterate of the last mixed / FP64 solve, as a numpy array."""
         t = torch.empty(self.cells, device="cuda", dtype=torch.float64)
@@ -421,11 +433,13 @@ class Projector3D:
     """
 
     def __init__(self, ax, ay, az, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, stream=None):
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, autotune=True, stream=None):
         self.dim = _dims3(dim)
         self.dx = _dx3(dx)
         self.ax, self.ay, self.az = ax, ay, az
         self.mg = CuMultigridFrac3D(ax, ay, az, self.dim, self.dx, "n", stream)
+        if autotune:
+            self.mg.Autotune(stream)
         self.rec = CuWaveletPotentialRecover3D(self.dim, self.dx, "n")
         self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
                          prolongation=prolongation)

@@ -145,6 +145,7 @@ extern "C" CUWHHD_API wp_status wp_batch_create(wp_batch** out, int count, const
             break;
         }
         if ((st = wp_mg_prepare_mixed(G.mg())) != WP_OK) break;
+        if ((st = wp_mgfrac3d_autotune(G.mg(), nullptr)) != WP_OK) break;
         cudaError_t e = cudaMalloc((void**)&G.b, sizeof(float) * G.cells());
         if (e == cudaSuccess) e = cudaMalloc((void**)&G.p, sizeof(float) * G.cells());
         if (e != cudaSuccess) { wp_set_cuda_error(e, "batch alloc", __FILE__, __LINE__); st = WP_ERR_CUDA; }

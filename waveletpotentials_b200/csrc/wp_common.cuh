@@ -46,6 +46,7 @@ int wp_prof_start(cudaStream_t s);
 // Launch-count adjustment for work replayed from a CUDA graph (captured launches are counted once at
 // capture time; a replay adds them again).
 void wp_add_launches(long long n);
+bool wp_profile_is_enabled();
 // Uploads the wavelet filter tables to the current device (once; synchronous).
 cudaError_t wp_dwt_prepare();
 void wp_prof_stop(int tok, const char* name, double bytes, cudaStream_t s);

@@ -18,6 +18,10 @@
 #include "wp_common.cuh"
 
 #include <algorithm>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -34,6 +38,7 @@ struct Lvl {
     const float* ax;
     const float* ay;
     const float* az;
+    const float* fyc; // y-face fractions in cell layout: fyc[cell] = ay of the cell's lower y face
     const T* glo[3];  // per-axis factor of the lower face, 0 at the wall
     const T* ghi[3];  // per-axis factor of the upper face, 0 at the wall
     const double* d[3];
@@ -156,6 +161,284 @@ __global__ void __launch_bounds__(256) jacobi_z_kernel(T* __restrict__ dst, cons
         T dg, od, c;
         col.step(dg, od, c);
         dst[i] = dg > (T)kEps ? ((T)1 - w) * c + w * (f[i] - od) / dg : (T)0;
+    }
+}
+
+// ------------------------------------------------------------------ quad kernels
+// The same operator with each thread owning four consecutive cells along y (y0 = 4k; needs
+// ny % 4 == 0): v, f, ax, az and the cell-laid y fractions move as 128-bit loads (two 64-bit-pair
+// loads for FP64), the z neighbours and z-face fractions of the column stay in registers, and the
+// x neighbours come through L1 from the adjacent rows.  Per cell the arithmetic (terms and their
+// order) is that of `row` / ZCol.
+template <typename T>
+struct Q4 {
+    T a[4];
+};
+
+__device__ __forceinline__ Q4<float> ld4(const float* p) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    return {{t.x, t.y, t.z, t.w}};
+}
+__device__ __forceinline__ Q4<double> ld4(const double* p) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    return {{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void st4(float* p, const Q4<float>& v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v.a[0], v.a[1], v.a[2], v.a[3]);
+}
+__device__ __forceinline__ void st4(double* p, const Q4<double>& v) {
+    *reinterpret_cast<double2*>(p) = make_double2(v.a[0], v.a[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(v.a[2], v.a[3]);
+}
+template <typename T, typename S>
+__device__ __forceinline__ Q4<T> cvt4(const Q4<S>& v) {
+    return {{(T)v.a[0], (T)v.a[1], (T)v.a[2], (T)v.a[3]}};
+}
+template <typename T>
+__device__ __forceinline__ Q4<T> zero4() {
+    return {{(T)0, (T)0, (T)0, (T)0}};
+}
+
+// Walker over the quad (x, y0..y0+3) of a column, z = z0, z0+1, ...
+template <typename T, typename TV>
+struct QCol {
+    const Lvl<T>& L;
+    const TV* __restrict__ v;
+    int x, y0, z;
+    long sxy, sax, i, iax;
+    bool xm, xp, ym, yp;
+    T gxl, gxh, gyl[4], gyh[4];
+    Q4<T> vm, vc, azl;
+
+    __device__ __forceinline__ QCol(const Lvl<T>& L_, const TV* v_, int x_, int y0_, int z0)
+        : L(L_), v(v_), x(x_), y0(y0_), z(z0) {
+        sxy = (long)L.nx * L.ny;
+        sax = (long)(L.nx + 1) * L.ny;
+        i = y0 + (long)x * L.ny + z0 * sxy;
+        iax = y0 + (long)x * L.ny + z0 * sax;
+        xm = x > 0;
+        xp = x < L.nx - 1;
+        ym = y0 > 0;
+        yp = y0 + 4 < L.ny;
+        gxl = L.glo[0][x];
+        gxh = L.ghi[0][x];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            gyl[k] = L.glo[1][y0 + k];
+            gyh[k] = L.ghi[1][y0 + k];
+        }
+        vm = z0 > 0 ? cvt4<T>(ld4(v + i - sxy)) : zero4<T>();
+        vc = cvt4<T>(ld4(v + i));
+        azl = z0 > 0 ? cvt4<T>(ld4(L.az + i)) : zero4<T>();
+    }
+
+    __device__ __forceinline__ void step(Q4<T>& dg, Q4<T>& od, Q4<T>& c) {
+        const int ny = L.ny, nz = L.nz;
+        const Q4<float> fyl = ld4(L.fyc + i);
+        const float fyu = yp ? L.fyc[i + 4] : 0.f;
+        const T vym = ym ? (T)v[i - 1] : (T)0;
+        const T vyp = yp ? (T)v[i + 4] : (T)0;
+        const Q4<float> fxl = ld4(L.ax + iax);
+        const Q4<float> fxu = xp ? ld4(L.ax + iax + ny) : zero4<float>();
+        const Q4<T> vxm = xm ? cvt4<T>(ld4(v + i - ny)) : zero4<T>();
+        const Q4<T> vxp = xp ? cvt4<T>(ld4(v + i + ny)) : zero4<T>();
+        Q4<T> vp = zero4<T>(), azu = zero4<T>();
+        const bool zp = z < nz - 1;
+        if (zp) {
+            vp = cvt4<T>(ld4(v + i + sxy));
+            azu = cvt4<T>(ld4(L.az + i + sxy));
+        }
+        const T gzl = L.glo[2][z], gzh = L.ghi[2][z];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = y0 + k;
+            T d = 0, o = 0, cf;
+            if (y > 0) { cf = (T)fyl.a[k] * gyl[k]; d += cf; o -= cf * (k > 0 ? vc.a[k - 1] : vym); }
+            if (y < ny - 1) { cf = (T)(k < 3 ? fyl.a[k + 1] : fyu) * gyh[k]; d += cf; o -= cf * (k < 3 ? vc.a[k + 1] : vyp); }
+            if (xm) { cf = (T)fxl.a[k] * gxl; d += cf; o -= cf * vxm.a[k]; }
+            if (xp) { cf = (T)fxu.a[k] * gxh; d += cf; o -= cf * vxp.a[k]; }
+            if (z > 0) { cf = azl.a[k] * gzl; d += cf; o -= cf * vm.a[k]; }
+            if (zp) { cf = azu.a[k] * gzh; d += cf; o -= cf * vp.a[k]; }
+            dg.a[k] = d;
+            od.a[k] = o;
+            c.a[k] = vc.a[k];
+        }
+        vm = vc;
+        vc = vp;
+        azl = azu;
+        i += sxy;
+        iax += sax;
+        ++z;
+    }
+};
+
+// y-quad index of a thread: q = x * (ny / 4) + yq over one z-plane
+template <typename T>
+__global__ void __launch_bounds__(256) jacobi_q_kernel(T* __restrict__ dst, const T* __restrict__ src,
+                                                       const T* __restrict__ f, Lvl<T> L, T w, int zc) {
+    const int nq = L.ny >> 2;
+    const long q = (long)blockIdx.x * 256 + threadIdx.x;
+    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    if (q >= (long)L.nx * nq || z0 >= z1) return;
+    const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
+    QCol<T, T> col(L, src, x, y0, z0);
+    for (int z = z0; z < z1; ++z) {
+        const long i = col.i;
+        Q4<T> dg, od, c;
+        col.step(dg, od, c);
+        const Q4<T> fv = ld4(f + i);
+        Q4<T> out;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            out.a[k] = dg.a[k] > (T)kEps ? ((T)1 - w) * c.a[k] + w * (fv.a[k] - od.a[k]) / dg.a[k] : (T)0;
+        st4(dst + i, out);
+    }
+}
+
+// Fused residual + restriction on quads: a thread owns the fine rows x0 = 2 cx and x0 + 1 of the
+// quad y0..y0+3 (coarse cells cy = y0/2, y0/2 + 1) and both fine z children of each coarse plane,
+// so every coarse value is summed in registers: ((x0,y) + (x0,y+1)) + ((x0+1,y) + (x0+1,y+1)),
+// each child carrying (0 + w_z0 r_z0) + w_z1 r_z1, the order of resid_restrict_z_kernel.
+template <typename T>
+__global__ void __launch_bounds__(256) resid_restrict_q_kernel(T* __restrict__ fc, const T* __restrict__ v,
+                                                               const T* __restrict__ f, Lvl<T> L, int ncx, int ncy,
+                                                               int ncz, int czc) {
+    const int nq = L.ny >> 2;
+    const long q = (long)blockIdx.x * 256 + threadIdx.x;
+    const int cz0 = blockIdx.y * czc, cz1 = min(cz0 + czc, ncz);
+    if (q >= (long)ncx * nq || cz0 >= cz1) return;
+    const int cx = (int)(q / nq), y0 = (int)(q - (long)cx * nq) * 4;
+    const int x0 = 2 * cx;
+    const bool two = x0 + 1 < L.nx;
+    T wxy[2][4];
+    {
+        const double sx = L.d[0][x0] + (two ? L.d[0][x0 + 1] : 0.0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = y0 + k, yb = y & ~1;
+            const double sy = L.d[1][yb] + (yb + 1 < L.ny ? L.d[1][yb + 1] : 0.0);
+            wxy[0][k] = (T)(L.d[1][y] / sy * (L.d[0][x0] / sx));
+            wxy[1][k] = two ? (T)(L.d[1][y] / sy * (L.d[0][x0 + 1] / sx)) : (T)0;
+        }
+    }
+    QCol<T, T> c0(L, v, x0, y0, 2 * cz0);
+    QCol<T, T> c1(L, v, two ? x0 + 1 : x0, y0, 2 * cz0);
+    for (int cz = cz0; cz < cz1; ++cz) {
+        Q4<T> acc0 = zero4<T>(), acc1 = zero4<T>();
+        const int zb = 2 * cz;
+        const double sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
+        for (int kz = 0; kz < 2; ++kz) {
+            const int z = zb + kz;
+            if (z >= L.nz) break;
+            const T wz = (T)(L.d[2][z] / sz);
+            const long i0 = c0.i, i1 = c1.i;
+            Q4<T> dg, od, c;
+            c0.step(dg, od, c);
+            Q4<T> fv = ld4(f + i0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const T r = dg.a[k] > (T)kEps ? fv.a[k] - (dg.a[k] * c.a[k] + od.a[k]) : (T)0;
+                acc0.a[k] += wz * wxy[0][k] * r;
+            }
+            c1.step(dg, od, c);
+            if (two) {
+                fv = ld4(f + i1);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const T r = dg.a[k] > (T)kEps ? fv.a[k] - (dg.a[k] * c.a[k] + od.a[k]) : (T)0;
+                    acc1.a[k] += wz * wxy[1][k] * r;
+                }
+            }
+        }
+        const long ci = (y0 >> 1) + (long)cx * ncy + (long)cz * ncx * ncy;
+        fc[ci] = (acc0.a[0] + acc0.a[1]) + (acc1.a[0] + acc1.a[1]);
+        fc[ci + 1] = (acc0.a[2] + acc0.a[3]) + (acc1.a[2] + acc1.a[3]);
+    }
+}
+
+// FP64 defect on quads (see defect64_z_kernel)
+template <typename TP>
+__global__ void __launch_bounds__(256) defect64_q_kernel(float* __restrict__ r32, const TP* __restrict__ p,
+                                                         const float* __restrict__ f, Lvl<double> L, double m,
+                                                         const double* __restrict__ msum, double* __restrict__ acc,
+                                                         int zc) {
+    const int nq = L.ny >> 2;
+    const long q = (long)blockIdx.x * 256 + threadIdx.x;
+    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    if (msum) m = msum[0] / fmax(msum[1], 1.0);
+    double s2 = 0.0;
+    if (q < (long)L.nx * nq && z0 < z1) {
+        const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
+        QCol<double, TP> col(L, p, x, y0, z0);
+        for (int z = z0; z < z1; ++z) {
+            const long i = col.i;
+            Q4<double> dg, od, c;
+            col.step(dg, od, c);
+            const Q4<float> fv = ld4(f + i);
+            Q4<float> rr;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double r = dg.a[k] > kEps ? ((double)fv.a[k] - m) - (dg.a[k] * c.a[k] + od.a[k]) : 0.0;
+                rr.a[k] = (float)r;
+                s2 += r * r;
+            }
+            if (r32) st4(r32 + i, rr);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < 8; ++k) t += red[k];
+        atomicAdd(acc, t);
+    }
+}
+
+// trilinear prolongation (prolong_tri_add_kernel) on quads: one 128-bit read-modify-write of v
+template <typename T>
+__global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny,
+                                                            int nz, int ncx, int ncy, int ncz) {
+    const int nq = ny >> 2;
+    const long q = (long)blockIdx.x * 256 + threadIdx.x;
+    const int z = blockIdx.y;
+    if (q >= (long)nx * nq) return;
+    const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
+    const int px = x >> 1, pz = z >> 1;
+    int qx = (x & 1) ? px + 1 : px - 1, qz = (z & 1) ? pz + 1 : pz - 1;
+    if (qx < 0 || qx >= ncx) qx = px;
+    if (qz < 0 || qz >= ncz) qz = pz;
+    const long sc = (long)ncx * ncy;
+    auto C = [&](int xx, int yy, int zz) -> T { return vc[yy + (long)xx * ncy + zz * sc]; };
+    const T a = (T)0.75, b = (T)0.25;
+    const long i = y0 + (long)x * ny + (long)z * nx * ny;
+    Q4<T> out = ld4(v + i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int y = y0 + k, py = y >> 1;
+        int qy = (y & 1) ? py + 1 : py - 1;
+        if (qy < 0 || qy >= ncy) qy = py;
+        T acc;
+        if (ncz == 1 && nz == 1) {
+            acc = a * (a * C(px, py, 0) + b * C(px, qy, 0)) + b * (a * C(qx, py, 0) + b * C(qx, qy, 0));
+        } else {
+            const T lo = a * (a * C(px, py, pz) + b * C(px, qy, pz)) + b * (a * C(qx, py, pz) + b * C(qx, qy, pz));
+            const T hi = a * (a * C(px, py, qz) + b * C(px, qy, qz)) + b * (a * C(qx, py, qz) + b * C(qx, qy, qz));
+            acc = a * lo + b * hi;
+        }
+        out.a[k] += acc;
+    }
+    st4(v + i, out);
+}
+
+// cell layout of the y-face fractions: fyc[y + x ny + z nx ny] = ay[y + x (ny+1) + z nx (ny+1)]
+__global__ void fyc_kernel(float* __restrict__ fyc, const float* __restrict__ ay, int nx, int ny, long cells) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < cells; t += (long)gridDim.x * blockDim.x) {
+        const long row = t / ny;
+        const int y = (int)(t - row * ny);
+        fyc[t] = ay[y + row * (ny + 1)];
     }
 }
 
@@ -459,11 +742,16 @@ struct Level {
     int n[3];
     long cells;
     float* frac[3];   // ax, ay, az (level-owned copies)
+    float* fyc;       // ay re-laid per cell (lower y face), so y-quads of cells load with 128-bit accesses
     double* tab64;    // per axis: glo[n], ghi[n], d[n]
     float* tab32;     // per axis: glo[n], ghi[n]
     float *v, *t, *f; // FP32 work
     double *v64, *t64, *f64;
+    int zc[3];        // z planes per CTA of the column kernels (jacobi, coarse planes of resid_restrict,
+                      // defect64); 0 = heuristic, set by wp_mgfrac3d_autotune
 };
+
+enum { kZcJacobi = 0, kZcRestrict = 1, kZcDefect = 2 };
 
 template <typename T>
 Lvl<T> view(const Level& L);
@@ -471,7 +759,7 @@ template <>
 Lvl<float> view<float>(const Level& L) {
     Lvl<float> o;
     o.nx = L.n[0]; o.ny = L.n[1]; o.nz = L.n[2];
-    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2];
+    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2]; o.fyc = L.fyc;
     long off64 = 0, off32 = 0;
     for (int a = 0; a < 3; ++a) {
         o.glo[a] = L.tab32 + off32;
@@ -486,7 +774,7 @@ template <>
 Lvl<double> view<double>(const Level& L) {
     Lvl<double> o;
     o.nx = L.n[0]; o.ny = L.n[1]; o.nz = L.n[2];
-    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2];
+    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2]; o.fyc = L.fyc;
     long off64 = 0;
     for (int a = 0; a < 3; ++a) {
         o.glo[a] = L.tab64 + off64;
@@ -499,17 +787,89 @@ Lvl<double> view<double>(const Level& L) {
 
 dim3 grid_of(int nx, int ny, int nz) { return dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz); }
 
-// z chunk of the column-walking kernels: long columns (register reuse) while keeping >= 4 CTAs
-// per SM in flight
+// z planes per CTA so the grid holds about eight waves of 5 resident 256-thread CTAs per SM (a
+// single wave leaves a tail that idles most SMs for the last CTAs)
 int zchunk(int nx, int ny, int nz) {
     const long cols = (long)wp_cdiv(ny, 32) * wp_cdiv(nx, 8);
-    const long want = 4L * wp_sm_count();
+    const long want = 40L * wp_sm_count();
     long nzc = (want + cols - 1) / cols;
     if (nzc < 1) nzc = 1;
     if (nzc > nz) nzc = nz;
     return (int)((nz + nzc - 1) / nzc);
 }
 dim3 grid_z(int nx, int ny, int nz, int zc) { return dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8), wp_cdiv(nz, zc)); }
+
+// levels whose y extent is a multiple of 4 run the quad kernels (when every array they read or
+// write with 128-bit accesses is 16-byte aligned: caller-owned arrays may be offset views)
+bool quad_ok(const Level& L) { return L.n[1] % 4 == 0; }
+bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// quad kernels: CTAs of 256 quads; about four waves of 4 resident CTAs per SM by default
+int zchunk_q(int nx, int ny, int nz) {
+    const long per_plane = wp_cdiv((size_t)nx * (ny / 4), 256);
+    const long want = 16L * wp_sm_count();
+    long nzc = (want + per_plane - 1) / per_plane;
+    if (nzc < 1) nzc = 1;
+    if (nzc > nz) nzc = nz;
+    return (int)((nz + nzc - 1) / nzc);
+}
+
+int level_zc(const Level& L, int kind) {
+    if (L.zc[kind] > 0) return L.zc[kind];
+    const int zc = quad_ok(L) ? zchunk_q(L.n[0], L.n[1], L.n[2]) : zchunk(L.n[0], L.n[1], L.n[2]);
+    return kind == kZcRestrict ? (zc + 1) / 2 : zc;
+}
+
+// one weighted-Jacobi sweep dst <- J(src) of level L
+template <typename T>
+void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc, cudaStream_t s) {
+    const Lvl<T> V = view<T>(L);
+    if (quad_ok(L) && al16(dst) && al16(src) && al16(f)) {
+        const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
+        jacobi_q_kernel<T><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
+    } else {
+        jacobi_z_kernel<T, false><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(dst, src, f, V, w, nullptr,
+                                                                                          0, 0, zc);
+    }
+}
+
+// coarse f of C = restriction of the residual f - A v of level L (czc coarse planes per CTA)
+template <typename T>
+void launch_resid_restrict(const Level& L, const Level& C, T* fc, const T* v, const T* f, int czc, cudaStream_t s) {
+    const Lvl<T> V = view<T>(L);
+    if (quad_ok(L) && C.n[1] * 2 == L.n[1] && al16(v) && al16(f)) {
+        const dim3 g(wp_cdiv((size_t)C.n[0] * (L.n[1] / 4), 256), wp_cdiv(C.n[2], czc));
+        resid_restrict_q_kernel<T><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
+    } else {
+        const dim3 g(wp_cdiv(L.n[1], 32), wp_cdiv(L.n[0], 8), wp_cdiv(C.n[2], czc));
+        resid_restrict_z_kernel<T><<<g, dim3(32, 8), 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
+    }
+}
+
+// FP64 defect of the finest level into acc[0] (see defect64_z_kernel)
+template <typename TP>
+void launch_defect64(const Level& L, float* r32, const TP* p, const float* f, double m, const double* msum,
+                     double* acc, int zc, cudaStream_t s) {
+    const Lvl<double> V = view<double>(L);
+    if (quad_ok(L) && al16(r32) && al16(p) && al16(f)) {
+        const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
+        defect64_q_kernel<TP><<<g, 256, 0, s>>>(r32, p, f, V, m, msum, acc, zc);
+    } else {
+        defect64_z_kernel<TP><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(r32, p, f, V, m, msum, acc,
+                                                                                       zc);
+    }
+}
+
+template <typename T>
+void launch_prolong_tri(const Level& L, const Level& C, T* v, const T* vc, cudaStream_t s) {
+    if (quad_ok(L) && al16(v)) {
+        const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), L.n[2]);
+        prolong_tri_q_kernel<T><<<g, 256, 0, s>>>(v, vc, L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2]);
+    } else {
+        prolong_tri_add_kernel<T><<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(v, vc, L.n[0], L.n[1], L.n[2],
+                                                                                         C.n[0], C.n[1], C.n[2]);
+    }
+}
 
 }  // namespace
 
@@ -559,6 +919,10 @@ wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, cons
             }
             if (dims == 2) WP_CUDA_TRY(cudaMemsetAsync(L.frac[2], 0, sizeof(float), s));
         }
+        WP_CUDA_TRY(cudaMalloc((void**)&L.fyc, sizeof(float) * L.cells));
+        WP_KERNEL("fyc", 8.0 * L.cells, s,
+                  fyc_kernel<<<std::min<unsigned>(wp_cdiv(L.cells, 256), 4096), 256, 0, s>>>(L.fyc, L.frac[1], n[0],
+                                                                                             n[1], L.cells));
         // spacing tables; 2D problems have a single z layer with no z faces (tables all zero)
         std::vector<double> t64;
         std::vector<float> t32;
@@ -625,13 +989,10 @@ struct Bufs<double> {
 
 template <typename T>
 wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s) {
-    const Lvl<T> V = view<T>(L);
-    const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
-    const dim3 g = grid_z(L.n[0], L.n[1], L.n[2], zc);
+    const int zc = level_zc(L, kZcJacobi);
     for (int k = 0; k < sweeps; ++k) {
         WP_KERNEL("jacobi", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
-                  jacobi_z_kernel<T, false><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::t(L), Bufs<T>::v(L), f, V, w, nullptr,
-                                                                      0, 0, zc));
+                  launch_jacobi<T>(L, Bufs<T>::t(L), Bufs<T>::v(L), f, w, zc, s));
         T* tmp = Bufs<T>::v(L);
         Bufs<T>::v(L) = Bufs<T>::t(L);
         Bufs<T>::t(L) = tmp;
@@ -649,22 +1010,19 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         Level& C = h->lv[l + 1];
         {
             // coarse-z chunk so the fine columns keep >= 4 CTAs per SM busy
-            const int czc = (zchunk(L.n[0], L.n[1], L.n[2]) + 1) / 2;
-            const dim3 gr(wp_cdiv(L.n[1], 32), wp_cdiv(L.n[0], 8), wp_cdiv(C.n[2], czc));
+            const int czc = level_zc(L, kZcRestrict);
             WP_KERNEL("resid_restrict", (double)L.cells * (2.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
-                      resid_restrict_z_kernel<T><<<gr, dim3(32, 8), 0, s>>>(Bufs<T>::f(C), Bufs<T>::v(L), f, view<T>(L),
-                                                                           C.n[0], C.n[1], C.n[2], czc));
+                      launch_resid_restrict<T>(L, C, Bufs<T>::f(C), Bufs<T>::v(L), f, czc, s));
         }
         WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(C), 0, sizeof(T) * C.cells, s));
         if ((st = vcycle<T>(h, l + 1, Bufs<T>::f(C), nu1, nu2, w, prolong, s)) != WP_OK) return st;
         if (prolong == WP_PROLONG_TRILINEAR) {
             WP_KERNEL("prolong_trilinear", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
-                      prolong_tri_add_kernel<T><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::v(L), Bufs<T>::v(C), L.n[0], L.n[1],
-                                                                         L.n[2], C.n[0], C.n[1], C.n[2]));
+                      launch_prolong_tri<T>(L, C, Bufs<T>::v(L), Bufs<T>::v(C), s));
             if ((st = smooth<T>(L, f, nu2, w, s)) != WP_OK) return st;
         } else if (nu2 > 0) {
             // first post-sweep reads v + P vc directly (prolongation fused into the sweep)
-            const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
+            const int zc = level_zc(L, kZcJacobi);
             WP_KERNEL("jacobi_prolong", (double)L.cells * (3.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
                       jacobi_z_kernel<T, true><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(
                           Bufs<T>::t(L), Bufs<T>::v(L), f, view<T>(L), w, Bufs<T>::v(C), C.n[0], C.n[1], zc));
@@ -711,10 +1069,9 @@ wp_status defect_async(wp_mgfrac3d* h, const TP* p, const float* f, double m, co
                        bool with_f2, cudaStream_t s) {
     Level& L = h->lv[0];
     WP_CUDA_TRY(cudaMemsetAsync(h->acc, 0, (with_f2 ? 2 : 1) * sizeof(double), s));
-    const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
+    const int zc = level_zc(L, kZcDefect);
     WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 16.0 + (r32 ? 4.0 : 0.0)), s,
-              defect64_z_kernel<TP><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(
-                  r32, p, f, view<double>(L), m, msum, h->acc, zc));
+              launch_defect64<TP>(L, r32, p, f, m, msum, h->acc, zc, s));
     if (with_f2) {
         const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
         WP_KERNEL("sumsq", 4.0 * L.cells, s, sumsq_kernel<float><<<b, 256, 0, s>>>(f, L.cells, h->acc + 1));
@@ -727,10 +1084,9 @@ wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r
                  double* norm_f2, cudaStream_t s) {
     Level& L = h->lv[0];
     WP_CUDA_TRY(cudaMemsetAsync(h->acc, 0, 2 * sizeof(double), s));
-    const int zc = zchunk(L.n[0], L.n[1], L.n[2]);
+    const int zc = level_zc(L, kZcDefect);
     WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 16.0 + (r32 ? 4.0 : 0.0)), s,
-              defect64_z_kernel<TP><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(
-                  r32, p, f, view<double>(L), m, nullptr, h->acc, zc));
+              launch_defect64<TP>(L, r32, p, f, m, nullptr, h->acc, zc, s));
     if (norm_f2) {
         const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
         WP_KERNEL("sumsq", 4.0 * L.cells, s, sumsq_kernel<float><<<b, 256, 0, s>>>(f, L.cells, h->acc + 1));
@@ -747,7 +1103,7 @@ void destroy_levels(wp_mgfrac3d* h) {
     for (int l = 0; l < kMaxLevels; ++l) {
         Level& L = h->lv[l];
         for (int a = 0; a < 3; ++a) if (L.frac[a]) cudaFree(L.frac[a]);
-        void* ps[] = {L.tab64, L.tab32, L.v, L.t, L.f, L.v64, L.t64, L.f64};
+        void* ps[] = {L.tab64, L.tab32, L.fyc, L.v, L.t, L.f, L.v64, L.t64, L.f64};
         for (void* p : ps) if (p) cudaFree(p);
     }
     if (h->acc) cudaFree(h->acc);
@@ -1003,6 +1359,104 @@ extern "C" CUWHHD_API wp_status wp_mgfrac2d_destroy(wp_mgfrac2d* h) {
 }
 
 // ---- internal hooks used by the batched path (wp_batch.cu)
+// ------------------------------------------------------------------ tile-shape autotuner
+// Per level, times the column kernels (FP32 Jacobi sweep, fused residual-restriction, FP64 defect)
+// over candidate z-chunks with CUDA events and keeps the fastest.  Results do not depend on the
+// chunk (each cell's arithmetic is the same; only the grid shape changes).  Timings are cached per
+// (device, kernel, extents) for the process, so later handles of the same shapes skip the search.
+namespace {
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_tune_cache;
+
+template <typename F>
+float time_launches(F&& launch, cudaStream_t s, cudaEvent_t a, cudaEvent_t b, int reps) {
+    launch();
+    cudaEventRecord(a, s);
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms / reps;
+}
+
+std::vector<int> zc_candidates(int nplanes) {
+    std::vector<int> c;
+    for (int z = 1; z <= nplanes; z *= 2) c.push_back(z);
+    if (c.empty() || c.back() != nplanes) c.push_back(nplanes);
+    return c;
+}
+
+wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
+    int dev = 0;
+    WP_CUDA_TRY(cudaGetDevice(&dev));
+    cudaEvent_t ea, eb;
+    WP_CUDA_TRY(cudaEventCreate(&ea));
+    WP_CUDA_TRY(cudaEventCreate(&eb));
+    const bool prof = wp_profile_is_enabled();
+    wp_profile_enable(0);
+    const long long launches0 = wp_launch_count();
+    wp_status st = WP_OK;
+    for (int l = 0; l < h->nl && st == WP_OK; ++l) {
+        Level& L = h->lv[l];
+        const int nx = L.n[0], ny = L.n[1], nz = L.n[2];
+        if (nz == 1) { L.zc[0] = L.zc[1] = L.zc[2] = 1; continue; }
+        // scratch contents: zero right-hand side and iterate (the level buffers are work arrays)
+        cudaMemsetAsync(L.v, 0, sizeof(float) * L.cells, s);
+        cudaMemsetAsync(L.f, 0, sizeof(float) * L.cells, s);
+        const int kinds = (l == 0 && h->p64 && h->r32) ? 3 : (l + 1 < h->nl ? 2 : 1);
+        for (int kind = 0; kind < kinds; ++kind) {
+            const auto key = std::make_tuple(dev, kind, nx, ny, nz);
+            {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                auto it = g_tune_cache.find(key);
+                if (it != g_tune_cache.end()) { L.zc[kind] = it->second; continue; }
+            }
+            const Level* C = l + 1 < h->nl ? &h->lv[l + 1] : nullptr;
+            const int planes = kind == kZcRestrict ? (C ? C->n[2] : 1) : nz;
+            float best = 1e30f;
+            int best_zc = level_zc(L, kind);
+            for (int zc : zc_candidates(planes)) {
+                auto launch = [&]() {
+                    if (kind == kZcJacobi) launch_jacobi<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
+                    else if (kind == kZcRestrict) launch_resid_restrict<float>(L, *C, C->f, L.v, L.f, zc, s);
+                    else launch_defect64<double>(L, h->r32, h->p64, L.f, 0.0, nullptr, h->acc, zc, s);
+                };
+                const float ms = time_launches(launch, s, ea, eb, 3);
+                const cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
+                if (ms < best) { best = ms; best_zc = zc; }
+            }
+            if (st != WP_OK) break;
+            L.zc[kind] = best_zc;
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune_cache[key] = best_zc;
+        }
+    }
+    wp_add_launches(-(wp_launch_count() - launches0));
+    wp_profile_enable(prof ? 1 : 0);
+    cudaEventDestroy(ea);
+    cudaEventDestroy(eb);
+    return st;
+}
+
+}  // namespace
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_autotune(wp_mgfrac3d* h, void* stream) {
+    if (!h) { wp_set_error_msg("wp_mgfrac3d_autotune: null handle"); return WP_ERR_INVALID_ARG; }
+    return autotune(h, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, int cap, int* levels) {
+    if (!h || (!zc && cap > 0)) { wp_set_error_msg("wp_mgfrac3d_tiles: null pointer"); return WP_ERR_INVALID_ARG; }
+    if (levels) *levels = h->nl;
+    for (int l = 0; l < h->nl; ++l)
+        for (int k = 0; k < 3; ++k)
+            if (3 * l + k < cap) zc[3 * l + k] = level_zc(h->lv[l], k);
+    return WP_OK;
+}
+
 wp_status wp_mg_prepare_mixed(wp_mgfrac3d* h) { return prepare_mixed(h); }
 wp_status wp_mg_solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
                                         cudaStream_t s) {

@@ -99,6 +99,8 @@ void wp_prof_stop(int tok, const char* name, double bytes, cudaStream_t s) {
 
 extern "C" CUWHHD_API void wp_profile_enable(int on) { g_prof_on.store(on != 0); }
 
+bool wp_profile_is_enabled() { return g_prof_on.load(); }
+
 extern "C" CUWHHD_API void wp_profile_reset(void) {
     std::lock_guard<std::mutex> lk(g_prof_mu);
     for (auto& r : g_open) { g_pool.push_back(r.a); g_pool.push_back(r.b); }
