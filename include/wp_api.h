@@ -219,6 +219,27 @@ CUWHHD_API wp_status wp_dst3d_create(wp_dst3d** h, int nx, int ny, int nz, doubl
 CUWHHD_API wp_status wp_dst3d_solve(wp_dst3d* h, double* dst, const double* f, void* stream);
 CUWHHD_API wp_status wp_dst3d_destroy(wp_dst3d* h);
 
+/* Allocation-free DST-I Poisson solve.  No reference counterpart (CuDst3D allocates its buffers in
+   its constructor).  Same result as wp_dst3d_create + wp_dst3d_solve, but no handle and no device
+   allocation on any call: the three DST-I matrices and the intermediate buffer live in one static
+   device array of 3*64*64 + 64^3 doubles (2.2 MB) inside the library.  For callers that cannot
+   allocate: a solver running under a fixed device-memory budget whose pool is already committed,
+   or a stream-ordered loop next to other streams where cudaFree's implicit device synchronization
+   would stall them.
+   - Limits: every extent <= WP_DST_NOALLOC_MAX_EXTENT and nx*ny*nz <= WP_DST_NOALLOC_MAX_CELLS;
+     larger grids return WP_ERR_INVALID_ARG (use wp_dst3d_create / wp_dst3d_solve).
+   - Nothing in the scratch has to start at zero: every call writes each word it reads.
+   - The first call on each device resolves the scratch address (cudaGetSymbolAddress, with that
+     device current); make that first call an ordinary one, before any stream capture.
+   - The scratch is shared by all calls on a device: two calls that overlap in time (different
+     streams, or different host threads without ordering) race on it and give wrong results.
+     Order them (same stream, or events).
+   dst and f are FP64 device arrays of nx*ny*nz cells in the INDEX3D layout; dst may equal f. */
+#define WP_DST_NOALLOC_MAX_EXTENT 64
+#define WP_DST_NOALLOC_MAX_CELLS (64 * 64 * 64)
+CUWHHD_API wp_status wp_dst3d_solve_noalloc(double* dst, const double* f, int nx, int ny, int nz, double dx,
+                                            double dy, double dz, void* stream);
+
 /* ------------------------------------------------------------- batched projection ------- */
 /* No reference counterpart: the reference projects one grid per process.  A batch holds `count`
    independent grids of uneven sizes (dims[i] = 2 or 3, extents ext[3*i..3*i+2] (z ignored for 2D),

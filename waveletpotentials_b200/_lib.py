@@ -89,6 +89,7 @@ SIGNATURES = {
     "wp_dst3d_create": (I, [PP, I, I, I, D, D, D]),
     "wp_dst3d_solve": (I, [P, P, P, P]),
     "wp_dst3d_destroy": (I, [P]),
+    "wp_dst3d_solve_noalloc": (I, [P, P, I, I, I, D, D, D, P]),
     "wp_mgfrac3d_autotune": (I, [P, P]),
     "wp_mgfrac3d_tiles": (I, [P, P, I, P]),
     "wp_batch_create": (I, [PP, I, P, P, P, P, P, P, P, I]),

@@ -414,6 +414,14 @@ class CuDst3D:
         check(lib().wp_dst3d_solve(self._h, _ptr(dst, (nz, nx, ny), torch.float64), _ptr(f, (nz, nx, ny), torch.float64),
                                    _stream(stream)), "wp_dst3d_solve")
 
+    @staticmethod
+    def SolveNoAlloc(dst, f, dim, dx, stream=None):
+        """Handle-free solve with no device allocation (grids up to 64 per axis, 64^3 cells)."""
+        nx, ny, nz = _dims3(dim)
+        check(lib().wp_dst3d_solve_noalloc(_ptr(dst, (nz, nx, ny), torch.float64),
+                                           _ptr(f, (nz, nx, ny), torch.float64), nx, ny, nz, *_dx3(dx),
+                                           _stream(stream)), "wp_dst3d_solve_noalloc")
+
     def close(self):
         if getattr(self, "_h", None):
             lib().wp_dst3d_destroy(self._h)

@@ -13,6 +13,7 @@
 #include "wp_common.cuh"
 
 #include <cmath>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -167,4 +168,94 @@ extern "C" CUWHHD_API wp_status wp_dst3d_destroy(wp_dst3d* h) {
     if (h->tmp) cudaFree(h->tmp);
     delete h;
     return WP_OK;
+}
+
+// ------------------------------------------------------------------ allocation-free variant
+// Same transforms as wp_dst3d_solve, with the three DST-I matrices and the ping-pong buffer in a
+// file-scope device array instead of handle-owned allocations.  Extents are limited to
+// WP_DST_NOALLOC_MAX_EXTENT per axis and WP_DST_NOALLOC_MAX_CELLS cells in total.
+namespace {
+
+constexpr int kNoAllocMaxN = WP_DST_NOALLOC_MAX_EXTENT;
+constexpr long kNoAllocMaxCells = WP_DST_NOALLOC_MAX_CELLS;
+constexpr long kNoAllocWords = 3L * kNoAllocMaxN * kNoAllocMaxN + kNoAllocMaxCells;
+
+// [M_x | M_y | M_z (kNoAllocMaxN^2 doubles each) | tmp (kNoAllocMaxCells doubles)]
+static __device__ __align__(256) double g_dst_scratch[kNoAllocWords];
+
+double* g_dst_scratch_ptr[64] = {nullptr};
+std::mutex g_dst_scratch_mu;
+
+// M[k][j] = sqrt(2/(m+1)) sin(pi (j+1)(k+1)/(m+1)); the product is reduced modulo 2(m+1) so the
+// sinpi argument is exact.
+__global__ void dst_matrix_kernel(double* __restrict__ M, int m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m * m) return;
+    const int k = i / m, j = i - k * m;
+    const long r = ((long)(j + 1) * (k + 1)) % (2L * (m + 1));
+    M[i] = sqrt(2.0 / (m + 1)) * sinpi((double)r / (m + 1));
+}
+
+// Resolves the scratch address on the current device once (cudaGetSymbolAddress, checked).
+cudaError_t noalloc_scratch(double** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_dst_scratch_mu);
+    if (!g_dst_scratch_ptr[dev]) {
+        double* p = nullptr;
+        e = cudaGetSymbolAddress((void**)&p, g_dst_scratch);
+        if (e != cudaSuccess) return e;
+        g_dst_scratch_ptr[dev] = p;
+    }
+    *out = g_dst_scratch_ptr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" CUWHHD_API wp_status wp_dst3d_solve_noalloc(double* dst, const double* f, int nx, int ny, int nz, double dx,
+                                                       double dy, double dz, void* stream) {
+    if (!dst || !f) { wp_set_error_msg("wp_dst3d_solve_noalloc: null pointer"); return WP_ERR_INVALID_ARG; }
+    if (nx < 1 || ny < 1 || nz < 1 || !(dx > 0) || !(dy > 0) || !(dz > 0)) {
+        wp_set_error_msg("wp_dst3d_solve_noalloc: extents must be >= 1 and spacings > 0");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (nx > kNoAllocMaxN || ny > kNoAllocMaxN || nz > kNoAllocMaxN || (long)nx * ny * nz > kNoAllocMaxCells) {
+        wp_set_error_msg("wp_dst3d_solve_noalloc: grid exceeds the static scratch (at most 64 per axis and 64^3 "
+                         "cells); use wp_dst3d_create/wp_dst3d_solve");
+        return WP_ERR_INVALID_ARG;
+    }
+    double* scratch = nullptr;
+    cudaError_t e = noalloc_scratch(&scratch);
+    if (e != cudaSuccess) { wp_set_cuda_error(e, "dst3d noalloc scratch address", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    cudaStream_t s = (cudaStream_t)stream;
+    double* M[3] = {scratch, scratch + (long)kNoAllocMaxN * kNoAllocMaxN, scratch + 2L * kNoAllocMaxN * kNoAllocMaxN};
+    double* tmp = scratch + 3L * kNoAllocMaxN * kNoAllocMaxN;
+    const int n[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+        const int tok = wp_prof_start(s);
+        dst_matrix_kernel<<<wp_cdiv((size_t)n[a] * n[a], 256), 256, 0, s>>>(M[a], n[a]);
+        e = cudaGetLastError();
+        wp_prof_stop(tok, "dst_matrix", 8.0 * n[a] * n[a], s);
+        if (e != cudaSuccess) goto fail;
+    }
+    if ((e = apply_axis(f, tmp, M[0], nx, ny, nz, 'x', s)) != cudaSuccess) goto fail;
+    if ((e = apply_axis(tmp, dst, M[1], nx, ny, nz, 'y', s)) != cudaSuccess) goto fail;
+    if ((e = apply_axis(dst, tmp, M[2], nx, ny, nz, 'z', s)) != cudaSuccess) goto fail;
+    {
+        const int tok = wp_prof_start(s);
+        dst_eig_kernel<<<dim3(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz), dim3(32, 8), 0, s>>>(tmp, nx, ny, nz, dx * dy);
+        e = cudaGetLastError();
+        wp_prof_stop(tok, "dst_eigen", 16.0 * nx * ny * nz, s);
+        if (e != cudaSuccess) goto fail;
+    }
+    if ((e = apply_axis(tmp, dst, M[2], nx, ny, nz, 'z', s)) != cudaSuccess) goto fail;
+    if ((e = apply_axis(dst, tmp, M[1], nx, ny, nz, 'y', s)) != cudaSuccess) goto fail;
+    if ((e = apply_axis(tmp, dst, M[0], nx, ny, nz, 'x', s)) != cudaSuccess) goto fail;
+    return WP_OK;
+fail:
+    wp_set_cuda_error(e, "dst3d noalloc solve", __FILE__, __LINE__);
+    return WP_ERR_CUDA;
 }
