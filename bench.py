@@ -100,6 +100,29 @@ def make_problem(n, seed):
     return centers, radii, (xv, yv, zv)
 
 
+def max_over_ranks(values, world):
+    """Element-wise max of per-rank timings (device-timed ms) over all ranks; the tensor lives on
+    the current CUDA device under NCCL and on the host under gloo."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([float(v) for v in values], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu().tolist()]
+
+
+def throughput(world, units_per_rank, ms):
+    """Whole-job rate: the units all ranks processed over the slowest rank's device time."""
+    return world * units_per_rank / (ms / 1000.0)
+
+
+def rank_seed(seed, rank):
+    """Each rank projects its own independent seeded problem (weak scaling, no data-path collective)."""
+    return seed + rank
+
+
 # --------------------------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -110,7 +133,7 @@ def run_ours(args, rank, world, local_rank):
     n = args.n
     nn = (n, n, n)
     h = 1.0 / n
-    centers, radii, (xv, yv, zv) = make_problem(n, args.seed + rank)
+    centers, radii, (xv, yv, zv) = make_problem(n, rank_seed(args.seed, rank))
     s = api.mac_shapes3d(*nn)
     sls = api.CuSolidLevelSet3D(nn, h)
     sls.InitLsSpheres(centers, radii)
@@ -156,10 +179,7 @@ def run_ours(args, rank, world, local_rank):
         L.wp_profile_entry(i, name, 64, ctypes.byref(lc), ctypes.byref(t), ctypes.byref(b))
         prof.append({"kernel": name.value.decode(), "launches": lc.value, "ms": t.value, "bytes": b.value})
     prof.sort(key=lambda r: -r["ms"])
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms, = max_over_ranks([ms], world)
 
     # end to end through the public API with host buffers: pinned H2D of the velocity, projection,
     # D2H of the potential q
@@ -189,10 +209,7 @@ def run_ours(args, rank, world, local_rank):
     f1.record(stream)
     torch.cuda.synchronize()
     ems = f0.elapsed_time(f1)
-    if world > 1:
-        t = torch.tensor([ems], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ems = float(t.item())
+    ems, = max_over_ranks([ems], world)
 
     # plain path: FP64 V-cycles throughout to the same tolerance (no mixed precision)
     plain = None
@@ -265,7 +282,7 @@ def run_batch(args, rank, world, local_rank):
     build.build()
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    probs = make_batch(args.batch3d, args.batch2d, args.seed + rank)
+    probs = make_batch(args.batch3d, args.batch2d, rank_seed(args.seed, rank))
     grids, u0, outs = [], [], []
     for d, c, r, u in probs:
         h = 1.0 / d[0]
@@ -304,6 +321,8 @@ def run_batch(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     L = _lib.lib()
+    if world > 1:
+        torch.distributed.barrier()
     torch.cuda.synchronize()
     L.wp_profile_reset()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -355,6 +374,8 @@ def run_batch(args, rank, world, local_rank):
                 d.copy_(src, non_blocking=True)
 
     e2e_step()
+    if world > 1:
+        torch.distributed.barrier()
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ek = max(1, min(args.steps, 5))
@@ -464,16 +485,14 @@ def main():
             torch.cuda.set_device(local_rank)
             torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         ms, ems, ek, h2d, d2h, launches, clocks, info, count = run_batch(args, rank, world, local_rank)
+        ms, ems = max_over_ranks([ms, ems], world)
         if world > 1:
             import torch
-            t = torch.tensor([ms, ems], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms, ems = (float(v) for v in t.tolist())
             torch.distributed.destroy_process_group()
         if rank != 0:
             return
         out = {"metric": "batched projections/s (64 uneven 2D/3D grids per CUDA-graph launch)",
-               "value": world * count * args.steps / (ms / 1000.0), "unit": "projections/s", "n_gpus": world,
+               "value": throughput(world, count * args.steps, ms), "unit": "projections/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 defect/refinement)",
                "data": "synthetic (seeded spectral fields)",
@@ -481,7 +500,7 @@ def main():
                                       f"{{256,512,1024}}^2, 0-4 random spheres each, mixed-precision multigrid to "
                                       f"rel. residual {args.batch_tol:g} + wavelet recovery, one graph per batch",
                           "l2_flush": "inputs larger than L2 (batch working set > 1 GB)"},
-               "e2e": {"value": world * count * ek / (ems / 1000.0), "unit": "projections/s",
+               "e2e": {"value": throughput(world, count * ek, ems), "unit": "projections/s",
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "gpu_launches": launches, "clocks": clocks, "batch": info}
         print(json.dumps(out))
@@ -498,7 +517,7 @@ def main():
         torch.distributed.destroy_process_group()
     if rank != 0:
         return
-    value = world * args.steps / (ms / 1000.0)
+    value = throughput(world, args.steps, ms)
     hbm, peak_kind = peaks()
     top = prof[0] if prof else None
     roof = None
@@ -519,7 +538,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP64 defect/refinement)", "data": "synthetic (seeded spectral fields)",
         "config": workload,
-        "e2e": {"value": world * ek / (ems / 1000.0), "unit": "projections/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": throughput(world, ek, ems), "unit": "projections/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": roof,
