@@ -240,6 +240,24 @@ CUWHHD_API wp_status wp_dst3d_destroy(wp_dst3d* h);
 CUWHHD_API wp_status wp_dst3d_solve_noalloc(double* dst, const double* f, int nx, int ny, int nz, double dx,
                                             double dy, double dz, void* stream);
 
+/* ------------------------------------------------------------- tensor-core convolutions ------- */
+/* No reference counterpart (the reference has no learned component): the 3x3x3 zero-padded
+   convolutions of the warm-start network, on the tcgen05 tensor cores (BF16 operands, FP32
+   accumulation).  Volumes are channels-last BF16 [z][x][y][c] with c in {16, 32, 64}; nx and ny are
+   powers of two.  Weights of input part p are BF16 [27][cout][cin_p], tap = (dz*3 + dx)*3 + dy for
+   the offsets (dz-1, dx-1, dy-1).
+   wp_conv3_forward: out = relu?( conv(x0, w0) [+ conv(x1, w1)] + bias + addend ) and, when mask is
+   given, zero where mask <= 0 (x1/w1, bias, addend, mask may be NULL; bias is FP32 [cout]; addend
+   and mask are BF16 volumes of cout channels).  With the weights transposed and flipped
+   ([26 - tap][cin][cout]) the same call is the input gradient.
+   wp_conv3_wgrad: dw[27][cout][cin] += sum_v gy[v][co] x[v + off(tap)][ci] in FP32 (caller zeroes
+   dw).  Both synchronize the stream to report a pipeline timeout. */
+CUWHHD_API wp_status wp_conv3_forward(void* out, const void* x0, int cin0, const void* w0, const void* x1, int cin1,
+                                      const void* w1, const float* bias, int cout, int nx, int ny, int nz, int relu,
+                                      const void* addend, const void* mask, void* stream);
+CUWHHD_API wp_status wp_conv3_wgrad(float* dw, const void* x, int cin, const void* gy, int cout, int nx, int ny,
+                                    int nz, void* stream);
+
 /* ------------------------------------------------------------- batched projection ------- */
 /* No reference counterpart: the reference projects one grid per process.  A batch holds `count`
    independent grids of uneven sizes (dims[i] = 2 or 3, extents ext[3*i..3*i+2] (z ignored for 2D),

@@ -296,3 +296,51 @@ def rel_l2_multi(refs, gots) -> float:
     num = sum(float(np.sum((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2)) for a, b in zip(refs, gots))
     den = sum(float(np.sum(np.asarray(a, np.float64) ** 2)) for a in refs)
     return float(np.sqrt(num / den)) if den > 0 else float(np.sqrt(num))
+
+
+# ----------------------------------------------------------------------------- warm-start network
+# FP64 restatement of the 3x3x3 zero-padded convolution of the warm-start network (no reference
+# counterpart).  Volumes are channels-last (nz, nx, ny, c); weights (27, cout, cin) with
+# tap = (dz*3 + dx)*3 + dy for offsets (dz-1, dx-1, dy-1).
+
+def bf16_round(a) -> np.ndarray:
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    f = np.ascontiguousarray(a, dtype=np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _shifted(x, dz, dx, dy):
+    """x[z+dz-1, x+dx-1, y+dy-1] with zeros outside (x is (nz, nx, ny, c))."""
+    p = np.pad(x, ((1, 1), (1, 1), (1, 1), (0, 0)))
+    nz, nx, ny = x.shape[:3]
+    return p[dz:dz + nz, dx:dx + nx, dy:dy + ny]
+
+
+def conv3d_forward(x, w, bias=None):
+    x = np.asarray(x, np.float64)
+    w = np.asarray(w, np.float64)
+    out = np.zeros(x.shape[:3] + (w.shape[1],))
+    for t in range(27):
+        dz, dx, dy = t // 9, (t // 3) % 3, t % 3
+        out += np.einsum("zxyc,oc->zxyo", _shifted(x, dz, dx, dy), w[t])
+    if bias is not None:
+        out += np.asarray(bias, np.float64)
+    return out
+
+
+def conv3d_input_grad(gy, w):
+    """d/dx of sum(gy * conv3d_forward(x, w)): the convolution with flipped, transposed weights."""
+    wt = np.transpose(np.asarray(w, np.float64)[::-1], (0, 2, 1))
+    return conv3d_forward(gy, wt)
+
+
+def conv3d_weight_grad(x, gy):
+    x = np.asarray(x, np.float64)
+    gy = np.asarray(gy, np.float64)
+    dw = np.zeros((27, gy.shape[3], x.shape[3]))
+    for t in range(27):
+        dz, dx, dy = t // 9, (t // 3) % 3, t % 3
+        dw[t] = np.einsum("zxyo,zxyc->oc", gy, _shifted(x, dz, dx, dy))
+    return dw

@@ -110,3 +110,20 @@ def test_generated_velocity_has_compatible_divergence(oracle):
     ones = [np.ones_like(a) for a in (xv, yv, zv)]
     b = oracle.divergence3d(xv, yv, zv, *ones, n, (1 / 24,) * 3)
     assert abs(b.sum()) < 1e-8 * np.abs(b).sum()
+
+
+def test_conv_oracle_adjoint_identities(oracle):
+    """<conv(x, w), g> = <x, input_grad(g, w)> = <w, weight_grad(x, g)> for the FP64 convolution."""
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((3, 4, 5, 3))
+    w = rng.standard_normal((27, 2, 3))
+    g = rng.standard_normal((3, 4, 5, 2))
+    a = np.sum(oracle.conv3d_forward(x, w) * g)
+    b = np.sum(x * oracle.conv3d_input_grad(g, w))
+    c = np.sum(w * oracle.conv3d_weight_grad(x, g))
+    assert abs(a - b) < 1e-9 * abs(a) and abs(a - c) < 1e-9 * abs(a)
+    # one tap by hand: the centre tap is a pointwise channel mix
+    wc = np.zeros((27, 2, 3))
+    wc[13] = rng.standard_normal((2, 3))
+    assert np.allclose(oracle.conv3d_forward(x, wc), np.einsum("zxyc,oc->zxyo", x, wc[13]))
+    assert oracle.bf16_round(np.array([1.00390625]))[0] == 1.0

@@ -92,6 +92,8 @@ SIGNATURES = {
     "wp_dst3d_solve_noalloc": (I, [P, P, I, I, I, D, D, D, P]),
     "wp_mgfrac3d_autotune": (I, [P, P]),
     "wp_mgfrac3d_tiles": (I, [P, P, I, P]),
+    "wp_conv3_forward": (I, [P, P, I, P, P, I, P, P, I, I, I, I, I, P, P, P]),
+    "wp_conv3_wgrad": (I, [P, P, I, P, I, I, I, I, P]),
     "wp_batch_create": (I, [PP, I, P, P, P, P, P, P, P, I]),
     "wp_batch_plan": (I, [P, P, P, P, P, P]),
     "wp_batch_run": (I, [P, P, P, P, P, P, P, P]),

@@ -20,7 +20,7 @@ from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONS
 
 __all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRecover2D", "CuMultigridFrac3D",
            "CuMultigridFrac2D", "CuConvergence", "CuGradient", "CuSolidLevelSet3D", "CuSolidLevelSet2D", "CuDst3D",
-           "Projector3D", "Projector2D", "BatchProjector", "max_abs",
+           "Projector3D", "Projector2D", "BatchProjector", "max_abs", "conv3_forward", "conv3_wgrad",
            "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
            "PROLONG_TRILINEAR", "mac_shapes3d", "mac_shapes2d"]
 
@@ -600,3 +600,33 @@ class BatchProjector:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ tensor-core convolutions
+def _bf16(t, name):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.bfloat16 or not t.is_contiguous():
+        raise WPError(1, name, "expected a contiguous CUDA bfloat16 tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def conv3_forward(out, x0, w0, bias=None, x1=None, w1=None, relu=False, addend=None, mask=None, stream=None):
+    """3x3x3 zero-padded convolution on the tensor cores.  x: (nz, nx, ny, cin) bf16 channels-last,
+    w: (27, cout, cin) bf16, bias: (cout,) float32, out: (nz, nx, ny, cout) bf16."""
+    nz, nx, ny, cin0 = x0.shape
+    cout = w0.shape[1]
+    cin1 = x1.shape[3] if x1 is not None else 0
+    check(lib().wp_conv3_forward(_bf16(out, "out"), _bf16(x0, "x0"), cin0, _bf16(w0, "w0"),
+                                 _bf16(x1, "x1") if x1 is not None else None, cin1,
+                                 _bf16(w1, "w1") if w1 is not None else None,
+                                 _ptr(bias, (cout,), name="bias") if bias is not None else None, cout, nx, ny, nz,
+                                 int(bool(relu)), _bf16(addend, "addend") if addend is not None else None,
+                                 _bf16(mask, "mask") if mask is not None else None, _stream(stream)),
+          "wp_conv3_forward")
+
+
+def conv3_wgrad(dw, x, gy, stream=None):
+    """dw (27, cout, cin) float32 += weight gradient of the convolution for input x and output grad gy."""
+    nz, nx, ny, cin = x.shape
+    cout = gy.shape[3]
+    check(lib().wp_conv3_wgrad(_ptr(dw, (27, cout, cin), name="dw"), _bf16(x, "x"), cin, _bf16(gy, "gy"), cout, nx, ny,
+                               nz, _stream(stream)), "wp_conv3_wgrad")
