@@ -155,9 +155,12 @@ CUWHHD_API wp_status wp_mgfrac3d_destroy(wp_mgfrac3d* h);
    every level (Jacobi sweep, fused residual-restriction, FP64 defect) over candidate z-chunks and
    keeps the fastest per level; results are independent of the choice.  Synchronous; overwrites
    the handle's work arrays (not the FP64 iterate).  Choices are cached per device and extents for
-   the process.  wp_mgfrac3d_tiles reports 3 chunks per level (jacobi, restrict, defect). */
+   the process.  Each candidate is timed as the median of single launches, after an L2 flush for
+   levels larger than 16 MB, among chunks that give at least two CTAs per SM (when the level has
+   that many columns).  wp_mgfrac3d_tiles reports 3 chunks per level (jacobi, restrict, defect)
+   and, if ms is not NULL, the tuned median time of each in ms (0 where not tuned). */
 CUWHHD_API wp_status wp_mgfrac3d_autotune(wp_mgfrac3d* h, void* stream);
-CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, int cap, int* levels);
+CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, float* ms, int cap, int* levels);
 
 typedef struct wp_mgfrac2d wp_mgfrac2d;
 /* Replaces CuMultigridFrac2D(Ax, Ay, int2 dim, DTYPE2 dx, char bc) (cuMultigridFrac2D.cu:28-111). */
@@ -257,6 +260,43 @@ CUWHHD_API wp_status wp_conv3_forward(void* out, const void* x0, int cin0, const
                                       const void* addend, const void* mask, void* stream);
 CUWHHD_API wp_status wp_conv3_wgrad(float* dw, const void* x, int cin, const void* gy, int cout, int nx, int ny,
                                     int nz, void* stream);
+
+/* ------------------------------------------------------------- seeded generators ------- */
+/* No reference counterpart.  Gaussian random fields with power spectrum |k|^slope as sums of random
+   Fourier modes 0 < |k| <= kmax (kmax <= 32) over the unit domain, variance scaled to rms^2; modes
+   are drawn on the host from std::mt19937_64(seed), so a seed gives the same field everywhere.
+   wp_random_field3d samples one field at cell indices (x/nx, y/ny, z/nz) into out (nz, nx, ny).
+   wp_velocity3d writes the MAC velocity u = curl(psi) + grad(phi) (psi: three edge fields with
+   psi_slope/psi_rms, phi: a cell field with phi_slope/phi_rms), wall-normal faces zero. */
+CUWHHD_API wp_status wp_random_field3d(float* out, int nx, int ny, int nz, double slope, double rms, int kmax,
+                                       unsigned long long seed, void* stream);
+CUWHHD_API wp_status wp_velocity3d(float* xv, float* yv, float* zv, int nx, int ny, int nz, unsigned long long seed,
+                                   double psi_slope, double psi_rms, double phi_slope, double phi_rms, int kmax,
+                                   void* stream);
+
+/* ------------------------------------------------------------- warm-start network ------- */
+/* No reference counterpart.  A 3-level 3D U-Net (3x3x3 convolutions 16/32/64 channels with ReLU,
+   2x2x2 average pooling, nearest upsampling, concatenated skips, 1x1 head; BF16 weights and
+   activations, FP32 accumulation on the tensor cores) that maps the multigrid right-hand side b
+   and the solid level set sdf (FP32 cell arrays, INDEX3D layout) to a starting guess p for
+   wp_mgfrac3d_solve_tol.  nx, ny: powers of two >= 16; nz a multiple of 4.  The multigrid then
+   runs to the same tolerance, so the guess can only remove cycles (callers fall back to a zero
+   start when the guess's residual exceeds ||b||).
+   wp_unet_train_step: one Adam step (lr) on the loss mean over fluid cells (sdf > 0) of
+   (p/rms(b) - p_target/rms(b) - mean error)^2; *loss (may be NULL) receives the loss before the
+   step (synchronizes).  lr = 0 computes the gradients only.
+   wp_unet_params: parameters (which = 0) or last gradients (which = 1) as one FP32 vector: per
+   convolution its part weights [27][cout][cin_p] then bias, in the order c1a c1b c2a c2b c3a c3b
+   d2a d2b d1a d1b, then the head's 16 weights and bias; host = NULL returns the count only. */
+typedef struct wp_unet wp_unet;
+CUWHHD_API wp_status wp_unet_create(wp_unet** h, int nx, int ny, int nz, unsigned long long seed);
+CUWHHD_API wp_status wp_unet_predict(wp_unet* h, float* p, const float* b, const float* sdf, double h_cell,
+                                     void* stream);
+CUWHHD_API wp_status wp_unet_train_step(wp_unet* h, const float* b, const float* sdf, const float* p_target,
+                                        double h_cell, double lr, double* loss, void* stream);
+CUWHHD_API wp_status wp_unet_params(wp_unet* h, int which, float* host, size_t cap, size_t* count);
+CUWHHD_API wp_status wp_unet_set_params(wp_unet* h, const float* host, size_t count);
+CUWHHD_API wp_status wp_unet_destroy(wp_unet* h);
 
 /* ------------------------------------------------------------- batched projection ------- */
 /* No reference counterpart: the reference projects one grid per process.  A batch holds `count`

@@ -344,3 +344,124 @@ def conv3d_weight_grad(x, gy):
         dz, dx, dy = t // 9, (t // 3) % 3, t % 3
         dw[t] = np.einsum("zxyo,zxyc->oc", gy, _shifted(x, dz, dx, dy))
     return dw
+
+
+# The warm-start U-Net in FP64 (same architecture, parameter order and loss as wp_unet.cu).
+UNET_SPEC = [(16, 0, 16), (16, 0, 16), (16, 0, 32), (32, 0, 32), (32, 0, 64), (64, 0, 64), (32, 64, 32),
+             (32, 0, 32), (16, 32, 16), (16, 0, 16)]
+
+
+def unet_unflatten(vec):
+    vec = np.asarray(vec, np.float64)
+    convs, off = [], 0
+    for cin0, cin1, cout in UNET_SPEC:
+        ws = []
+        for cin in (cin0, cin1):
+            if cin:
+                n = 27 * cout * cin
+                ws.append(vec[off:off + n].reshape(27, cout, cin))
+                off += n
+        b = vec[off:off + cout]
+        off += cout
+        convs.append((ws, b))
+    head = vec[off:off + 17]
+    assert off + 17 == vec.size
+    return convs, head
+
+
+def unet_flatten(convs, head):
+    parts = []
+    for ws, b in convs:
+        parts += [w.ravel() for w in ws] + [np.ravel(b)]
+    parts.append(np.ravel(head))
+    return np.concatenate(parts)
+
+
+def _pool(x):
+    nz, nx, ny, c = x.shape
+    return x.reshape(nz // 2, 2, nx // 2, 2, ny // 2, 2, c).mean(axis=(1, 3, 5))
+
+
+def _up(x):
+    return np.repeat(np.repeat(np.repeat(x, 2, axis=0), 2, axis=1), 2, axis=2)
+
+
+def _up_bwd(g):
+    nz, nx, ny, c = g.shape
+    return g.reshape(nz // 2, 2, nx // 2, 2, ny // 2, 2, c).sum(axis=(1, 3, 5))
+
+
+def unet_forward(vec, b, sdf, hcell):
+    """Returns (p prediction in physical units, cache).  b, sdf: (nz, nx, ny)."""
+    convs, head = unet_unflatten(vec)
+    b = np.asarray(b, np.float64)
+    rms = np.sqrt(np.mean(b * b))
+    x = np.zeros(b.shape + (16,))
+    x[..., 0] = b / rms if rms > 0 else 0.0
+    x[..., 1] = np.clip(np.asarray(sdf, np.float64) / (4.0 * hcell), -1.0, 1.0)
+    relu = lambda v: np.maximum(v, 0.0)
+    def conv(i, *xs):
+        ws, bb = convs[i]
+        return relu(sum(conv3d_forward(xx, w) for xx, w in zip(xs, ws)) + bb)
+    c = {"in": x}
+    c["a1"] = conv(0, x)
+    c["s1"] = conv(1, c["a1"])
+    c["p1"] = _pool(c["s1"])
+    c["a2"] = conv(2, c["p1"])
+    c["s2"] = conv(3, c["a2"])
+    c["p2"] = _pool(c["s2"])
+    c["a3"] = conv(4, c["p2"])
+    c["e3"] = conv(5, c["a3"])
+    c["u2"] = _up(c["e3"])
+    c["a4"] = conv(6, c["s2"], c["u2"])
+    c["e2"] = conv(7, c["a4"])
+    c["u1"] = _up(c["e2"])
+    c["a5"] = conv(8, c["s1"], c["u1"])
+    c["e1"] = conv(9, c["a5"])
+    c["pred"] = c["e1"] @ head[:16] + head[16]
+    c["rms"] = rms
+    return c["pred"] * rms, c
+
+
+def unet_loss_grad(vec, b, sdf, p, hcell):
+    """Loss of wp_unet_train_step and its gradient (flattened in the parameter order)."""
+    convs, head = unet_unflatten(vec)
+    _, c = unet_forward(vec, b, sdf, hcell)
+    fluid = np.asarray(sdf) > 0
+    r = c["pred"] - np.asarray(p, np.float64) / c["rms"]
+    cnt = max(int(fluid.sum()), 1)
+    mu = r[fluid].sum() / cnt
+    rr = np.where(fluid, r - mu, 0.0)
+    loss = float(np.sum(rr * rr) / cnt)
+    g = 2.0 * rr / cnt
+    gconv = [[None for _ in ws] for ws, _ in convs]
+    gbias = [None] * len(convs)
+    ghead = np.concatenate([np.einsum("zxy,zxyc->c", g, c["e1"]), [g.sum()]])
+    mask = lambda gy, y: np.where(y > 0, gy, 0.0)
+
+    def back(i, gy, xs, need):
+        """gy: gradient wrt the (post-ReLU masked) pre-activation; returns input grads of each part."""
+        ws, _ = convs[i]
+        gbias[i] = gy.sum(axis=(0, 1, 2))
+        outs = []
+        for k, (xx, w) in enumerate(zip(xs, ws)):
+            gconv[i][k] = conv3d_weight_grad(xx, gy)
+            outs.append(conv3d_input_grad(gy, w) if need else None)
+        return outs
+    g_e1 = mask(g[..., None] * head[:16], c["e1"])
+    g_a5 = mask(back(9, g_e1, [c["a5"]], True)[0], c["a5"])
+    g_s1p, g_u1 = back(8, g_a5, [c["s1"], c["u1"]], True)
+    g_e2 = mask(_up_bwd(g_u1), c["e2"])
+    g_a4 = mask(back(7, g_e2, [c["a4"]], True)[0], c["a4"])
+    g_s2p, g_u2 = back(6, g_a4, [c["s2"], c["u2"]], True)
+    g_e3 = mask(_up_bwd(g_u2), c["e3"])
+    g_a3 = mask(back(5, g_e3, [c["a3"]], True)[0], c["a3"])
+    g_p2 = back(4, g_a3, [c["p2"]], True)[0]
+    g_s2 = mask(g_s2p + _up(g_p2) / 8.0, c["s2"])
+    g_a2 = mask(back(3, g_s2, [c["a2"]], True)[0], c["a2"])
+    g_p1 = back(2, g_a2, [c["p1"]], True)[0]
+    g_s1 = mask(g_s1p + _up(g_p1) / 8.0, c["s1"])
+    g_a1 = mask(back(1, g_s1, [c["a1"]], True)[0], c["a1"])
+    back(0, g_a1, [c["in"]], False)
+    grads = unet_flatten([(gw, gb) for gw, gb in zip(gconv, gbias)], ghead)
+    return loss, grads

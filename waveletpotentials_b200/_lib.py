@@ -91,9 +91,17 @@ SIGNATURES = {
     "wp_dst3d_destroy": (I, [P]),
     "wp_dst3d_solve_noalloc": (I, [P, P, I, I, I, D, D, D, P]),
     "wp_mgfrac3d_autotune": (I, [P, P]),
-    "wp_mgfrac3d_tiles": (I, [P, P, I, P]),
+    "wp_mgfrac3d_tiles": (I, [P, P, P, I, P]),
     "wp_conv3_forward": (I, [P, P, I, P, P, I, P, P, I, I, I, I, I, P, P, P]),
     "wp_conv3_wgrad": (I, [P, P, I, P, I, I, I, I, P]),
+    "wp_random_field3d": (I, [P, I, I, I, D, D, I, ctypes.c_ulonglong, P]),
+    "wp_velocity3d": (I, [P, P, P, I, I, I, ctypes.c_ulonglong, D, D, D, D, I, P]),
+    "wp_unet_create": (I, [PP, I, I, I, ctypes.c_ulonglong]),
+    "wp_unet_predict": (I, [P, P, P, P, D, P]),
+    "wp_unet_train_step": (I, [P, P, P, P, D, D, P, P]),
+    "wp_unet_params": (I, [P, I, P, S, P]),
+    "wp_unet_set_params": (I, [P, P, S]),
+    "wp_unet_destroy": (I, [P]),
     "wp_batch_create": (I, [PP, I, P, P, P, P, P, P, P, I]),
     "wp_batch_plan": (I, [P, P, P, P, P, P]),
     "wp_batch_run": (I, [P, P, P, P, P, P, P, P]),

@@ -21,6 +21,7 @@ from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONS
 __all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRecover2D", "CuMultigridFrac3D",
            "CuMultigridFrac2D", "CuConvergence", "CuGradient", "CuSolidLevelSet3D", "CuSolidLevelSet2D", "CuDst3D",
            "Projector3D", "Projector2D", "BatchProjector", "max_abs", "conv3_forward", "conv3_wgrad",
+           "random_field3d", "velocity3d_device", "UNetWarmStart",
            "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
            "PROLONG_TRILINEAR", "mac_shapes3d", "mac_shapes2d"]
 
@@ -207,13 +208,17 @@ class CuMultigridFrac3D:
         """Times the level kernels over candidate z-chunks and keeps the fastest (synchronous)."""
         check(lib().wp_mgfrac3d_autotune(self._h, _stream(stream)), "wp_mgfrac3d_autotune")
 
-    def Tiles(self):
-        """Per level: (jacobi, restrict, defect) z-chunks in use."""
+    def Tiles(self, with_times=False):
+        """Per level: (jacobi, restrict, defect) z-chunks in use (and the tuned times in ms)."""
         buf = (ctypes.c_int * (3 * 32))()
+        ms = (ctypes.c_float * (3 * 32))()
         nl = ctypes.c_int()
-        check(lib().wp_mgfrac3d_tiles(self._h, ctypes.cast(buf, ctypes.c_void_p), 96, ctypes.byref(nl)),
-              "wp_mgfrac3d_tiles")
-        return [tuple(buf[3 * l:3 * l + 3]) for l in range(nl.value)]
+        check(lib().wp_mgfrac3d_tiles(self._h, ctypes.cast(buf, ctypes.c_void_p), ctypes.cast(ms, ctypes.c_void_p), 96,
+                                      ctypes.byref(nl)), "wp_mgfrac3d_tiles")
+        zc = [tuple(buf[3 * l:3 * l + 3]) for l in range(nl.value)]
+        if with_times:
+            return zc, [tuple(round(v, 4) for v in ms[3 * l:3 * l + 3]) for l in range(nl.value)]
+        return zc
 
     def Iterate64(self, stream=None):
         """FP64 iterate of the last mixed / FP64 solve, as a numpy array."""
@@ -441,10 +446,14 @@ class Projector3D:
     """
 
     def __init__(self, ax, ay, az, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, autotune=True, stream=None):
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, autotune=True, warm_start=None, sdf=None,
+                 stream=None):
         self.dim = _dims3(dim)
         self.dx = _dx3(dx)
         self.ax, self.ay, self.az = ax, ay, az
+        if warm_start is not None and sdf is None:
+            raise WPError(1, "Projector3D", "a warm start needs the solid level set (sdf)")
+        self.warm_start, self.sdf = warm_start, sdf
         self.mg = CuMultigridFrac3D(ax, ay, az, self.dim, self.dx, "n", stream)
         if autotune:
             self.mg.Autotune(stream)
@@ -460,7 +469,18 @@ class Projector3D:
         """Projects (xv, yv, zv) in place (result a (u - grad p)) and writes the potential q."""
         CuConvergence.GetB_3d_frac_vel(self.b, xv, yv, zv, self.ax, self.ay, self.az, self.dim, self.dx,
                                        stream=stream)
+        warm = None
+        if pre_p is None and self.warm_start is not None:
+            # the network's guess is kept only if it starts below the zero start's residual (1.0);
+            # the multigrid then runs to the same tolerance either way
+            self.warm_start.predict(self.p, self.b, self.sdf, self.dx[0], stream)
+            r0 = self.mg.GetResdualError(self.p, self.b, stream)
+            warm = {"initial_rel_residual": r0, "used": bool(r0 < 1.0)}
+            if warm["used"]:
+                pre_p = self.p
         rep = self.mg.SolveTol(self.p, pre_p, self.b, raise_on_fail=False, stream=stream, **self.opts)
+        if warm is not None:
+            rep["warm_start"] = warm
         CuGradient.SubtractGradient3D_Frac_P(xv, yv, zv, self.p, self.ax, self.ay, self.az, self.dim, self.dx,
                                              multiply_frac=True, stream=stream)
         # -div of the fraction-weighted projected field (open-face divergence of a (u - grad p))
@@ -630,3 +650,71 @@ def conv3_wgrad(dw, x, gy, stream=None):
     cout = gy.shape[3]
     check(lib().wp_conv3_wgrad(_ptr(dw, (27, cout, cin), name="dw"), _bf16(x, "x"), cin, _bf16(gy, "gy"), cout, nx, ny,
                                nz, _stream(stream)), "wp_conv3_wgrad")
+
+
+# ------------------------------------------------------------------ seeded device generators
+def random_field3d(out, slope, rms, kmax=8, seed=0, stream=None):
+    """Gaussian random field (spectrum |k|^slope, |k| <= kmax, variance rms^2) into out (nz, nx, ny)."""
+    nz, nx, ny = out.shape
+    check(lib().wp_random_field3d(_ptr(out), nx, ny, nz, float(slope), float(rms), int(kmax), int(seed),
+                                  _stream(stream)), "wp_random_field3d")
+
+
+def velocity3d_device(xv, yv, zv, dim, seed, psi_slope=-11.0 / 3.0, psi_rms=1.0, phi_slope=-2.0, phi_rms=1.0, kmax=8,
+                      stream=None):
+    """MAC velocity u = curl(psi) + grad(phi) generated on the GPU (wp_velocity3d)."""
+    nx, ny, nz = _dims3(dim)
+    s = mac_shapes3d(nx, ny, nz)
+    check(lib().wp_velocity3d(_ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]), nx, ny, nz, int(seed),
+                              float(psi_slope), float(psi_rms), float(phi_slope), float(phi_rms), int(kmax),
+                              _stream(stream)), "wp_velocity3d")
+
+
+# ------------------------------------------------------------------ warm-start network
+class UNetWarmStart:
+    """The warm-start U-Net (wp_unet_*): predict(p, b, sdf, h) writes a multigrid starting guess,
+    train_step(...) runs one Adam step on the GPU."""
+
+    def __init__(self, dim, seed=0):
+        self.dim = _dims3(dim)
+        h = ctypes.c_void_p()
+        check(lib().wp_unet_create(ctypes.byref(h), *self.dim, int(seed)), "wp_unet_create")
+        self._h = h
+        self.cells = mac_shapes3d(*self.dim)["p"]
+
+    def predict(self, p, b, sdf, hcell, stream=None):
+        c = self.cells
+        check(lib().wp_unet_predict(self._h, _ptr(p, c), _ptr(b, c), _ptr(sdf, c), float(hcell), _stream(stream)),
+              "wp_unet_predict")
+
+    def train_step(self, b, sdf, p_target, hcell, lr, stream=None) -> float:
+        c = self.cells
+        loss = ctypes.c_double()
+        check(lib().wp_unet_train_step(self._h, _ptr(b, c), _ptr(sdf, c), _ptr(p_target, c), float(hcell), float(lr),
+                                       ctypes.byref(loss), _stream(stream)), "wp_unet_train_step")
+        return loss.value
+
+    def params(self, which=0):
+        import numpy as np
+        n = ctypes.c_size_t()
+        check(lib().wp_unet_params(self._h, int(which), None, 0, ctypes.byref(n)), "wp_unet_params")
+        out = np.empty(n.value, np.float32)
+        check(lib().wp_unet_params(self._h, int(which), out.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n)),
+              "wp_unet_params")
+        return out
+
+    def set_params(self, vec):
+        import numpy as np
+        v = np.ascontiguousarray(vec, np.float32)
+        check(lib().wp_unet_set_params(self._h, v.ctypes.data_as(ctypes.c_void_p), v.size), "wp_unet_set_params")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().wp_unet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

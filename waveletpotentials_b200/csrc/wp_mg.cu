@@ -749,6 +749,7 @@ struct Level {
     double *v64, *t64, *f64;
     int zc[3];        // z planes per CTA of the column kernels (jacobi, coarse planes of resid_restrict,
                       // defect64); 0 = heuristic, set by wp_mgfrac3d_autotune
+    float zc_ms[3];   // the autotuner's median time of the chosen chunk (0 = not tuned)
 };
 
 enum { kZcJacobi = 0, kZcRestrict = 1, kZcDefect = 2 };
@@ -1369,16 +1370,34 @@ namespace {
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, int> g_tune_cache;
 
+// median of `reps` single launches, each timed alone; with a flush buffer the L2 is overwritten
+// before every timed launch (a level larger than the L2 meets a cold cache inside a V-cycle)
 template <typename F>
-float time_launches(F&& launch, cudaStream_t s, cudaEvent_t a, cudaEvent_t b, int reps) {
+float time_launches(F&& launch, cudaStream_t s, cudaEvent_t a, cudaEvent_t b, int reps, void* flush,
+                    size_t flush_bytes) {
     launch();
-    cudaEventRecord(a, s);
-    for (int r = 0; r < reps; ++r) launch();
-    cudaEventRecord(b, s);
-    cudaEventSynchronize(b);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
-    return ms / reps;
+    std::vector<float> t;
+    for (int r = 0; r < reps; ++r) {
+        if (flush) cudaMemsetAsync(flush, r & 0xff, flush_bytes, s);
+        cudaEventRecord(a, s);
+        launch();
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        t.push_back(ms);
+    }
+    std::sort(t.begin(), t.end());
+    return t[t.size() / 2];
+}
+
+// CTAs of a column kernel for a z-chunk (to keep candidates that fill the GPU)
+long grid_blocks(const Level& L, const Level* C, int kind, int zc) {
+    const bool q = quad_ok(L) && (kind != kZcRestrict || (C && C->n[1] * 2 == L.n[1]));
+    const int planes = kind == kZcRestrict ? C->n[2] : L.n[2];
+    const long per_plane = q ? (long)wp_cdiv((size_t)(kind == kZcRestrict ? C->n[0] : L.n[0]) * (L.n[1] / 4), 256)
+                             : (long)wp_cdiv(L.n[1], 32) * wp_cdiv(L.n[0], 8);
+    return per_plane * wp_cdiv(planes, zc);
 }
 
 std::vector<int> zc_candidates(int nplanes) {
@@ -1398,6 +1417,14 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
     wp_profile_enable(0);
     const long long launches0 = wp_launch_count();
     wp_status st = WP_OK;
+    // L2 flush buffer (twice the 126 MB L2), only if some level does not fit in the L2 by itself
+    constexpr size_t kFlush = 256u << 20;
+    constexpr long kL2Cells = (16L << 20) / 4;
+    void* flush = nullptr;
+    if (h->lv[0].cells > kL2Cells && cudaMalloc(&flush, kFlush) != cudaSuccess) {
+        cudaGetLastError();
+        flush = nullptr;
+    }
     for (int l = 0; l < h->nl && st == WP_OK; ++l) {
         Level& L = h->lv[l];
         const int nx = L.n[0], ny = L.n[1], nz = L.n[2];
@@ -1417,22 +1444,31 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             const int planes = kind == kZcRestrict ? (C ? C->n[2] : 1) : nz;
             float best = 1e30f;
             int best_zc = level_zc(L, kind);
+            const long most = grid_blocks(L, C, kind, 1);
+            const long floor_blocks = std::min<long>(most, 2L * wp_sm_count());
+            void* fl = L.cells > kL2Cells ? flush : nullptr;
             for (int zc : zc_candidates(planes)) {
+                if (grid_blocks(L, C, kind, zc) < floor_blocks) continue;
                 auto launch = [&]() {
                     if (kind == kZcJacobi) launch_jacobi<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
                     else if (kind == kZcRestrict) launch_resid_restrict<float>(L, *C, C->f, L.v, L.f, zc, s);
                     else launch_defect64<double>(L, h->r32, h->p64, L.f, 0.0, nullptr, h->acc, zc, s);
                 };
-                const float ms = time_launches(launch, s, ea, eb, 3);
+                const float ms = time_launches(launch, s, ea, eb, 5, fl, kFlush);
                 const cudaError_t e = cudaGetLastError();
                 if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
                 if (ms < best) { best = ms; best_zc = zc; }
             }
             if (st != WP_OK) break;
             L.zc[kind] = best_zc;
+            L.zc_ms[kind] = best;
             std::lock_guard<std::mutex> lk(g_tune_mu);
             g_tune_cache[key] = best_zc;
         }
+    }
+    if (flush) {
+        cudaStreamSynchronize(s);
+        cudaFree(flush);
     }
     wp_add_launches(-(wp_launch_count() - launches0));
     wp_profile_enable(prof ? 1 : 0);
@@ -1448,12 +1484,15 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_autotune(wp_mgfrac3d* h, void* strea
     return autotune(h, (cudaStream_t)stream);
 }
 
-extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, int cap, int* levels) {
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, float* ms, int cap, int* levels) {
     if (!h || (!zc && cap > 0)) { wp_set_error_msg("wp_mgfrac3d_tiles: null pointer"); return WP_ERR_INVALID_ARG; }
     if (levels) *levels = h->nl;
     for (int l = 0; l < h->nl; ++l)
         for (int k = 0; k < 3; ++k)
-            if (3 * l + k < cap) zc[3 * l + k] = level_zc(h->lv[l], k);
+            if (3 * l + k < cap) {
+                zc[3 * l + k] = level_zc(h->lv[l], k);
+                if (ms) ms[3 * l + k] = h->lv[l].zc_ms[k];
+            }
     return WP_OK;
 }
 
