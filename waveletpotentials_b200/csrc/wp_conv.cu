@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int q = warp & 3;
         const int m = q * 32 + lane;
         const bool ready = mbar_wait(bar_acc, 0, err);
+        __syncwarp();  // tcgen05.ld is warp-collective
         tc_fence_after();
         float acc[COUT];
 #pragma unroll
@@ -263,6 +264,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int q = warp & 3;
         const int m = q * 32 + lane;
         const bool ready = nk > 0 && mbar_wait(bar_acc, 0, err);
+        __syncwarp();  // tcgen05.ld is warp-collective
         tc_fence_after();
         float acc[COUT];
 #pragma unroll
