@@ -162,11 +162,15 @@ def run_ours(args, rank, world, local_rank):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = []
     with ClockSampler(local_rank) as clk:
+        if args.profile_region:
+            torch.cuda.profiler.start()
         e0.record(stream)
         for _ in range(args.steps):
             reps.append(step())
         e1.record(stream)
         torch.cuda.synchronize()
+        if args.profile_region:
+            torch.cuda.profiler.stop()
     L.wp_profile_enable(0)
     ms = e0.elapsed_time(e1)
     launches = int(L.wp_launch_count())
@@ -327,11 +331,15 @@ def run_batch(args, rank, world, local_rank):
     L.wp_profile_reset()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
+        if args.profile_region:
+            torch.cuda.profiler.start()
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
         torch.cuda.synchronize()
+        if args.profile_region:
+            torch.cuda.profiler.stop()
     ms = e0.elapsed_time(e1)
     launches = int(L.wp_launch_count())
     res = bp.results()
@@ -516,6 +524,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "warmstart"],
                     help="single: one 256^3 projection per step; batch: 64 uneven grids in one graph per step; "
                          "warmstart: train the U-Net, then projections with/without its guess")

@@ -275,8 +275,8 @@ struct QCol {
 
 // y-quad index of a thread: q = x * (ny / 4) + yq over one z-plane
 template <typename T>
-__global__ void __launch_bounds__(256) jacobi_q_kernel(T* __restrict__ dst, const T* __restrict__ src,
-                                                       const T* __restrict__ f, Lvl<T> L, T w, int zc) {
+__device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ f,
+                                              const Lvl<T>& L, T w, int zc) {
     const int nq = L.ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
@@ -296,10 +296,24 @@ __global__ void __launch_bounds__(256) jacobi_q_kernel(T* __restrict__ dst, cons
     }
 }
 
-// Fused residual + restriction on quads: a thread owns the fine rows x0 = 2 cx and x0 + 1 of the
-// quad y0..y0+3 (coarse cells cy = y0/2, y0/2 + 1) and both fine z children of each coarse plane,
-// so every coarse value is summed in registers: ((x0,y) + (x0,y+1)) + ((x0+1,y) + (x0+1,y+1)),
-// each child carrying (0 + w_z0 r_z0) + w_z1 r_z1, the order of resid_restrict_z_kernel.
+// register-allocation variants of the same sweep (the autotuner picks one per level): default
+// limits, and at least 3 or 4 resident 256-thread CTAs per SM
+template <typename T>
+__global__ void __launch_bounds__(256) jacobi_q_kernel(T* __restrict__ dst, const T* __restrict__ src,
+                                                       const T* __restrict__ f, Lvl<T> L, T w, int zc) {
+    jacobi_q_body<T>(dst, src, f, L, w, zc);
+}
+template <typename T, int MINB>
+__global__ void __launch_bounds__(256, MINB) jacobi_q_mb_kernel(T* __restrict__ dst, const T* __restrict__ src,
+                                                                const T* __restrict__ f, Lvl<T> L, T w, int zc) {
+    jacobi_q_body<T>(dst, src, f, L, w, zc);
+}
+
+// Fused residual + restriction on quads: lanes 2k and 2k+1 own the fine rows x0 = 2 cx and x0 + 1 of
+// the quad y0..y0+3 (coarse cells cy = y0/2, y0/2 + 1); each walks both fine z children of every
+// coarse plane and sums its y pairs in registers, and a lane shuffle adds the two rows:
+// ((x0,y) + (x0,y+1)) + ((x0+1,y) + (x0+1,y+1)), each child carrying (0 + w_z0 r_z0) + w_z1 r_z1,
+// the order of resid_restrict_z_kernel.
 template <typename T>
 __global__ void __launch_bounds__(256) resid_restrict_q_kernel(T* __restrict__ fc, const T* __restrict__ v,
                                                                const T* __restrict__ f, Lvl<T> L, int ncx, int ncy,
@@ -307,53 +321,62 @@ __global__ void __launch_bounds__(256) resid_restrict_q_kernel(T* __restrict__ f
     const int nq = L.ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int cz0 = blockIdx.y * czc, cz1 = min(cz0 + czc, ncz);
-    if (q >= (long)ncx * nq || cz0 >= cz1) return;
-    const int cx = (int)(q / nq), y0 = (int)(q - (long)cx * nq) * 4;
+    const long pair = q >> 1;
+    const int xpar = (int)(q & 1);
+    // whole warps stay together for the shuffle; lanes past the grid end only idle along
+    const bool live_pair = pair < (long)ncx * nq && cz0 < cz1;
+    const int cx = live_pair ? (int)(pair / nq) : 0;
+    const int y0 = live_pair ? (int)(pair - (long)cx * nq) * 4 : 0;
     const int x0 = 2 * cx;
     const bool two = x0 + 1 < L.nx;
-    T wxy[2][4];
+    const bool mine = live_pair && (xpar == 0 || two);
+    const int x = mine ? x0 + xpar : x0;
+    T wxy[4];
     {
         const double sx = L.d[0][x0] + (two ? L.d[0][x0 + 1] : 0.0);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int y = y0 + k, yb = y & ~1;
             const double sy = L.d[1][yb] + (yb + 1 < L.ny ? L.d[1][yb + 1] : 0.0);
-            wxy[0][k] = (T)(L.d[1][y] / sy * (L.d[0][x0] / sx));
-            wxy[1][k] = two ? (T)(L.d[1][y] / sy * (L.d[0][x0 + 1] / sx)) : (T)0;
+            wxy[k] = mine ? (T)(L.d[1][y] / sy * (L.d[0][x] / sx)) : (T)0;
         }
     }
-    QCol<T, T> c0(L, v, x0, y0, 2 * cz0);
-    QCol<T, T> c1(L, v, two ? x0 + 1 : x0, y0, 2 * cz0);
-    for (int cz = cz0; cz < cz1; ++cz) {
-        Q4<T> acc0 = zero4<T>(), acc1 = zero4<T>();
-        const int zb = 2 * cz;
-        const double sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
-        for (int kz = 0; kz < 2; ++kz) {
-            const int z = zb + kz;
-            if (z >= L.nz) break;
-            const T wz = (T)(L.d[2][z] / sz);
-            const long i0 = c0.i, i1 = c1.i;
-            Q4<T> dg, od, c;
-            c0.step(dg, od, c);
-            Q4<T> fv = ld4(f + i0);
+    QCol<T, T> col(L, v, x, y0, live_pair ? 2 * cz0 : 0);
+    const int ncz_loop = live_pair ? cz1 - cz0 : 0;
+    // every lane of a warp runs the same number of shuffles: the loop bound is the warp maximum
+    int iters = ncz_loop;
+    for (int o = 16; o > 0; o >>= 1) iters = max(iters, __shfl_xor_sync(0xffffffffu, iters, o));
+    for (int it = 0; it < iters; ++it) {
+        const int cz = cz0 + it;
+        const bool act = it < ncz_loop;
+        Q4<T> acc = zero4<T>();
+        if (act) {
+            const int zb = 2 * cz;
+            const double sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
+            for (int kz = 0; kz < 2; ++kz) {
+                const int z = zb + kz;
+                if (z >= L.nz) break;
+                const T wz = (T)(L.d[2][z] / sz);
+                const long i = col.i;
+                Q4<T> dg, od, c;
+                col.step(dg, od, c);
+                if (mine) {
+                    const Q4<T> fv = ld4(f + i);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const T r = dg.a[k] > (T)kEps ? fv.a[k] - (dg.a[k] * c.a[k] + od.a[k]) : (T)0;
-                acc0.a[k] += wz * wxy[0][k] * r;
-            }
-            c1.step(dg, od, c);
-            if (two) {
-                fv = ld4(f + i1);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const T r = dg.a[k] > (T)kEps ? fv.a[k] - (dg.a[k] * c.a[k] + od.a[k]) : (T)0;
-                    acc1.a[k] += wz * wxy[1][k] * r;
+                    for (int k = 0; k < 4; ++k) {
+                        const T r = dg.a[k] > (T)kEps ? fv.a[k] - (dg.a[k] * c.a[k] + od.a[k]) : (T)0;
+                        acc.a[k] += wz * wxy[k] * r;
+                    }
                 }
             }
         }
-        const long ci = (y0 >> 1) + (long)cx * ncy + (long)cz * ncx * ncy;
-        fc[ci] = (acc0.a[0] + acc0.a[1]) + (acc1.a[0] + acc1.a[1]);
-        fc[ci + 1] = (acc0.a[2] + acc0.a[3]) + (acc1.a[2] + acc1.a[3]);
+        const T ya = acc.a[0] + acc.a[1], yb = acc.a[2] + acc.a[3];
+        const T oa = __shfl_xor_sync(0xffffffffu, ya, 1), ob = __shfl_xor_sync(0xffffffffu, yb, 1);
+        if (act && xpar == 0) {
+            const long ci = (y0 >> 1) + (long)cx * ncy + (long)cz * ncx * ncy;
+            fc[ci] = ya + oa;
+            fc[ci + 1] = yb + ob;
+        }
     }
 }
 
@@ -750,6 +773,7 @@ struct Level {
     int zc[3];        // z planes per CTA of the column kernels (jacobi, coarse planes of resid_restrict,
                       // defect64); 0 = heuristic, set by wp_mgfrac3d_autotune
     float zc_ms[3];   // the autotuner's median time of the chosen chunk (0 = not tuned)
+    int var[3];       // kernel variant per kind (jacobi: 0 = default registers, 1/2 = >= 3/4 CTAs per SM)
 };
 
 enum { kZcJacobi = 0, kZcRestrict = 1, kZcDefect = 2 };
@@ -827,7 +851,10 @@ void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc
     const Lvl<T> V = view<T>(L);
     if (quad_ok(L) && al16(dst) && al16(src) && al16(f)) {
         const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
-        jacobi_q_kernel<T><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
+        const int var = sizeof(T) == 4 ? L.var[kZcJacobi] : 0;
+        if (var == 1) jacobi_q_mb_kernel<T, 3><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
+        else if (var == 2) jacobi_q_mb_kernel<T, 4><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
+        else jacobi_q_kernel<T><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
     } else {
         jacobi_z_kernel<T, false><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(dst, src, f, V, w, nullptr,
                                                                                           0, 0, zc);
@@ -839,7 +866,7 @@ template <typename T>
 void launch_resid_restrict(const Level& L, const Level& C, T* fc, const T* v, const T* f, int czc, cudaStream_t s) {
     const Lvl<T> V = view<T>(L);
     if (quad_ok(L) && C.n[1] * 2 == L.n[1] && al16(v) && al16(f)) {
-        const dim3 g(wp_cdiv((size_t)C.n[0] * (L.n[1] / 4), 256), wp_cdiv(C.n[2], czc));
+        const dim3 g(wp_cdiv((size_t)C.n[0] * (L.n[1] / 4) * 2, 256), wp_cdiv(C.n[2], czc));
         resid_restrict_q_kernel<T><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
     } else {
         const dim3 g(wp_cdiv(L.n[1], 32), wp_cdiv(L.n[0], 8), wp_cdiv(C.n[2], czc));
@@ -1395,7 +1422,7 @@ float time_launches(F&& launch, cudaStream_t s, cudaEvent_t a, cudaEvent_t b, in
 long grid_blocks(const Level& L, const Level* C, int kind, int zc) {
     const bool q = quad_ok(L) && (kind != kZcRestrict || (C && C->n[1] * 2 == L.n[1]));
     const int planes = kind == kZcRestrict ? C->n[2] : L.n[2];
-    const long per_plane = q ? (long)wp_cdiv((size_t)(kind == kZcRestrict ? C->n[0] : L.n[0]) * (L.n[1] / 4), 256)
+    const long per_plane = q ? (long)wp_cdiv((size_t)(kind == kZcRestrict ? 2 * C->n[0] : L.n[0]) * (L.n[1] / 4), 256)
                              : (long)wp_cdiv(L.n[1], 32) * wp_cdiv(L.n[0], 8);
     return per_plane * wp_cdiv(planes, zc);
 }
@@ -1438,32 +1465,41 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
                 auto it = g_tune_cache.find(key);
-                if (it != g_tune_cache.end()) { L.zc[kind] = it->second; continue; }
+                if (it != g_tune_cache.end()) {
+                    L.zc[kind] = it->second % 1000;
+                    L.var[kind] = it->second / 1000;
+                    continue;
+                }
             }
             const Level* C = l + 1 < h->nl ? &h->lv[l + 1] : nullptr;
             const int planes = kind == kZcRestrict ? (C ? C->n[2] : 1) : nz;
             float best = 1e30f;
-            int best_zc = level_zc(L, kind);
+            int best_zc = level_zc(L, kind), best_var = 0;
             const long most = grid_blocks(L, C, kind, 1);
             const long floor_blocks = std::min<long>(most, 2L * wp_sm_count());
             void* fl = L.cells > kL2Cells ? flush : nullptr;
-            for (int zc : zc_candidates(planes)) {
-                if (grid_blocks(L, C, kind, zc) < floor_blocks) continue;
-                auto launch = [&]() {
-                    if (kind == kZcJacobi) launch_jacobi<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
-                    else if (kind == kZcRestrict) launch_resid_restrict<float>(L, *C, C->f, L.v, L.f, zc, s);
-                    else launch_defect64<double>(L, h->r32, h->p64, L.f, 0.0, nullptr, h->acc, zc, s);
-                };
-                const float ms = time_launches(launch, s, ea, eb, 5, fl, kFlush);
-                const cudaError_t e = cudaGetLastError();
-                if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
-                if (ms < best) { best = ms; best_zc = zc; }
+            const int nvar = (kind == kZcJacobi && quad_ok(L)) ? 3 : 1;
+            for (int var = 0; var < nvar && st == WP_OK; ++var) {
+                L.var[kind] = var;
+                for (int zc : zc_candidates(planes)) {
+                    if (grid_blocks(L, C, kind, zc) < floor_blocks) continue;
+                    auto launch = [&]() {
+                        if (kind == kZcJacobi) launch_jacobi<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
+                        else if (kind == kZcRestrict) launch_resid_restrict<float>(L, *C, C->f, L.v, L.f, zc, s);
+                        else launch_defect64<double>(L, h->r32, h->p64, L.f, 0.0, nullptr, h->acc, zc, s);
+                    };
+                    const float ms = time_launches(launch, s, ea, eb, 5, fl, kFlush);
+                    const cudaError_t e = cudaGetLastError();
+                    if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
+                    if (ms < best) { best = ms; best_zc = zc; best_var = var; }
+                }
             }
             if (st != WP_OK) break;
             L.zc[kind] = best_zc;
+            L.var[kind] = best_var;
             L.zc_ms[kind] = best;
             std::lock_guard<std::mutex> lk(g_tune_mu);
-            g_tune_cache[key] = best_zc;
+            g_tune_cache[key] = best_zc + 1000 * best_var;
         }
     }
     if (flush) {
