@@ -220,6 +220,11 @@ class CuMultigridFrac3D:
             return zc, [tuple(round(v, 4) for v in ms[3 * l:3 * l + 3]) for l in range(nl.value)]
         return zc
 
+    def SetTile(self, level, kind, zc, variant=0):
+        """Pins one level's z-chunk and kernel variant (see wp_mgfrac3d_set_tile)."""
+        check(lib().wp_mgfrac3d_set_tile(self._h, int(level), int(kind), int(zc), int(variant)),
+              "wp_mgfrac3d_set_tile")
+
     def Iterate64(self, stream=None):
         """FP64 iterate of the last mixed / FP64 solve, as a numpy array."""
         t = torch.empty(self.cells, device="cuda", dtype=torch.float64)

@@ -309,6 +309,98 @@ __global__ void __launch_bounds__(256, MINB) jacobi_q_mb_kernel(T* __restrict__ 
     jacobi_q_body<T>(dst, src, f, L, w, zc);
 }
 
+// Two weighted-Jacobi sweeps in one pass (temporal blocking along z).  A CTA owns an interior tile
+// of J2_R rows x J2_Q quads and a z-chunk; its 288 threads cover the tile plus a one-row /
+// one-quad halo.  Walking up the chunk, every thread computes the first sweep of its quad at plane z
+// (QCol, as jacobi_q_kernel) into a three-plane shared ring; after a barrier the interior threads
+// compute the second sweep at plane z - 1 from the ring (the same terms in the same order, with the
+// face fractions re-read through L1).  The first sweep runs one plane beyond each end of the chunk,
+// so every second-sweep stencil finds its z neighbours.  Two sweeps then cost one read of v, f and
+// the fractions instead of two.
+constexpr int J2_R = 14, J2_Q = 16;
+constexpr int J2_RH = J2_R + 2, J2_QH = J2_Q + 2;
+constexpr int J2_THREADS = J2_RH * J2_QH;
+constexpr int J2_PITCH = J2_QH * 4 + 4;  // row pitch of the ring (elements); the pad staggers banks
+
+template <typename T>
+__device__ __forceinline__ void jacobi2_body(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ f,
+                                             const Lvl<T>& L, T w, int zc, int nty, T (*s1)[J2_RH][J2_PITCH]) {
+    const int nq = L.ny >> 2;
+    const int tile_x = blockIdx.x / nty, tile_y = blockIdx.x - tile_x * nty;
+    const int hr = threadIdx.x / J2_QH, hq = threadIdx.x - hr * J2_QH;
+    const int x = tile_x * J2_R - 1 + hr, yq = tile_y * J2_Q - 1 + hq;
+    const bool indom = x >= 0 && x < L.nx && yq >= 0 && yq < nq;
+    const bool interior = indom && hr >= 1 && hr <= J2_R && hq >= 1 && hq <= J2_Q;
+    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    const int zs = max(z0 - 1, 0), ze = min(z1, L.nz - 1);
+    const int xc = indom ? x : 0, y0 = indom ? 4 * yq : 0;
+    QCol<T, T> col(L, src, xc, y0, zs);
+    const long sxy = (long)L.nx * L.ny, sax = (long)(L.nx + 1) * L.ny;
+    const int ny = L.ny, nz = L.nz;
+    for (int z = zs; z <= z1; ++z) {
+        if (z <= ze) {
+            Q4<T> v1 = zero4<T>();
+            if (indom) {
+                const long i = col.i;
+                Q4<T> dg, od, c;
+                col.step(dg, od, c);
+                const Q4<T> fv = ld4(f + i);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    v1.a[k] = dg.a[k] > (T)kEps ? ((T)1 - w) * c.a[k] + w * (fv.a[k] - od.a[k]) / dg.a[k] : (T)0;
+            }
+            T* row = &s1[z % 3][hr][hq * 4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) row[k] = v1.a[k];
+        }
+        __syncthreads();
+        const int zz = z - 1;
+        if (interior && zz >= z0 && zz < z1) {
+            const T* cm = &s1[zz % 3][hr][hq * 4];
+            const T* cxm = &s1[zz % 3][hr - 1][hq * 4];
+            const T* cxp = &s1[zz % 3][hr + 1][hq * 4];
+            const T* czm = &s1[(zz + 2) % 3][hr][hq * 4];  // plane zz - 1
+            const T* czp = &s1[(zz + 1) % 3][hr][hq * 4];  // plane zz + 1
+            const long i = y0 + (long)x * ny + zz * sxy;
+            const long iax = y0 + (long)x * ny + zz * sax;
+            const Q4<float> fyl = ld4(L.fyc + i);
+            const bool yp = y0 + 4 < ny;
+            const float fyu = yp ? L.fyc[i + 4] : 0.f;
+            const Q4<float> fxl = ld4(L.ax + iax);
+            const Q4<float> fxu = col.xp ? ld4(L.ax + iax + ny) : zero4<float>();
+            const Q4<T> azl = zz > 0 ? cvt4<T>(ld4(L.az + i)) : zero4<T>();
+            const bool zp = zz < nz - 1;
+            const Q4<T> azu = zp ? cvt4<T>(ld4(L.az + i + sxy)) : zero4<T>();
+            const Q4<T> fv = ld4(f + i);
+            const T gzl = L.glo[2][zz], gzh = L.ghi[2][zz];
+            const T vym = cm[-1], vyp = cm[4];
+            Q4<T> out;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int y = y0 + k;
+                T d = 0, o = 0, cf;
+                if (y > 0) { cf = (T)fyl.a[k] * col.gyl[k]; d += cf; o -= cf * (k > 0 ? cm[k - 1] : vym); }
+                if (y < ny - 1) { cf = (T)(k < 3 ? fyl.a[k + 1] : fyu) * col.gyh[k]; d += cf; o -= cf * (k < 3 ? cm[k + 1] : vyp); }
+                if (col.xm) { cf = (T)fxl.a[k] * col.gxl; d += cf; o -= cf * cxm[k]; }
+                if (col.xp) { cf = (T)fxu.a[k] * col.gxh; d += cf; o -= cf * cxp[k]; }
+                if (zz > 0) { cf = azl.a[k] * gzl; d += cf; o -= cf * czm[k]; }
+                if (zp) { cf = azu.a[k] * gzh; d += cf; o -= cf * czp[k]; }
+                out.a[k] = d > (T)kEps ? ((T)1 - w) * cm[k] + w * (fv.a[k] - o) / d : (T)0;
+            }
+            st4(dst + i, out);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(J2_THREADS, sizeof(T) == 4 ? 2 : 1)
+    jacobi2_q_kernel(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ f, Lvl<T> L, T w, int zc,
+                     int nty) {
+    __shared__ __align__(16) T s1[3][J2_RH][J2_PITCH];
+    jacobi2_body<T>(dst, src, f, L, w, zc, nty, s1);
+}
+
 // Fused residual + restriction on quads: lanes 2k and 2k+1 own the fine rows x0 = 2 cx and x0 + 1 of
 // the quad y0..y0+3 (coarse cells cy = y0/2, y0/2 + 1); each walks both fine z children of every
 // coarse plane and sums its y pairs in registers, and a lane shuffle adds the two rows:
@@ -773,7 +865,8 @@ struct Level {
     int zc[3];        // z planes per CTA of the column kernels (jacobi, coarse planes of resid_restrict,
                       // defect64); 0 = heuristic, set by wp_mgfrac3d_autotune
     float zc_ms[3];   // the autotuner's median time of the chosen chunk (0 = not tuned)
-    int var[3];       // kernel variant per kind (jacobi: 0 = default registers, 1/2 = >= 3/4 CTAs per SM)
+    int var[3];       // kernel variant per kind (jacobi: 0 = default registers, 1/2 = >= 3/4 CTAs per SM,
+                      // 3 = two sweeps per launch)
 };
 
 enum { kZcJacobi = 0, kZcRestrict = 1, kZcDefect = 2 };
@@ -859,6 +952,16 @@ void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc
         jacobi_z_kernel<T, false><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(dst, src, f, V, w, nullptr,
                                                                                           0, 0, zc);
     }
+}
+
+bool jacobi2_ok(const Level& L, const void* f) { return quad_ok(L) && al16(f) && L.n[2] >= 2; }
+
+// two sweeps dst <- J(J(src)) in one pass (jacobi2_q_kernel)
+template <typename T>
+void launch_jacobi2(const Level& L, T* dst, const T* src, const T* f, T w, int zc, cudaStream_t s) {
+    const int nty = (L.n[1] / 4 + J2_Q - 1) / J2_Q, ntx = (L.n[0] + J2_R - 1) / J2_R;
+    jacobi2_q_kernel<T><<<dim3(ntx * nty, wp_cdiv(L.n[2], zc)), J2_THREADS, 0, s>>>(dst, src, f, view<T>(L), w, zc,
+                                                                                   nty);
 }
 
 // coarse f of C = restriction of the residual f - A v of level L (czc coarse planes per CTA)
@@ -1018,9 +1121,18 @@ struct Bufs<double> {
 template <typename T>
 wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s) {
     const int zc = level_zc(L, kZcJacobi);
-    for (int k = 0; k < sweeps; ++k) {
-        WP_KERNEL("jacobi", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
-                  launch_jacobi<T>(L, Bufs<T>::t(L), Bufs<T>::v(L), f, w, zc, s));
+    const bool fused = L.var[kZcJacobi] == 3 && jacobi2_ok(L, f);
+    for (int k = 0; k < sweeps;) {
+        if (fused && sweeps - k >= 2) {
+            // two sweeps, one pass: algorithmic bytes are those of one sweep
+            WP_KERNEL("jacobi2", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
+                      launch_jacobi2<T>(L, Bufs<T>::t(L), Bufs<T>::v(L), f, w, zc, s));
+            k += 2;
+        } else {
+            WP_KERNEL("jacobi", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
+                      launch_jacobi<T>(L, Bufs<T>::t(L), Bufs<T>::v(L), f, w, zc, s));
+            k += 1;
+        }
         T* tmp = Bufs<T>::v(L);
         Bufs<T>::v(L) = Bufs<T>::t(L);
         Bufs<T>::t(L) = tmp;
@@ -1478,17 +1590,24 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             const long most = grid_blocks(L, C, kind, 1);
             const long floor_blocks = std::min<long>(most, 2L * wp_sm_count());
             void* fl = L.cells > kL2Cells ? flush : nullptr;
-            const int nvar = (kind == kZcJacobi && quad_ok(L)) ? 3 : 1;
+            // jacobi variants: 0-2 one sweep per launch (register budgets), 3 two sweeps per launch
+            const int nvar = (kind == kZcJacobi && quad_ok(L)) ? (jacobi2_ok(L, L.f) ? 4 : 3) : 1;
             for (int var = 0; var < nvar && st == WP_OK; ++var) {
                 L.var[kind] = var;
                 for (int zc : zc_candidates(planes)) {
-                    if (grid_blocks(L, C, kind, zc) < floor_blocks) continue;
+                    long blocks = grid_blocks(L, C, kind, zc);
+                    if (var == 3)
+                        blocks = (long)((L.n[1] / 4 + J2_Q - 1) / J2_Q) * ((L.n[0] + J2_R - 1) / J2_R) *
+                                 wp_cdiv(L.n[2], zc);
+                    if (blocks < floor_blocks) continue;
                     auto launch = [&]() {
-                        if (kind == kZcJacobi) launch_jacobi<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
+                        if (kind == kZcJacobi && var == 3) launch_jacobi2<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
+                        else if (kind == kZcJacobi) launch_jacobi<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
                         else if (kind == kZcRestrict) launch_resid_restrict<float>(L, *C, C->f, L.v, L.f, zc, s);
                         else launch_defect64<double>(L, h->r32, h->p64, L.f, 0.0, nullptr, h->acc, zc, s);
                     };
-                    const float ms = time_launches(launch, s, ea, eb, 5, fl, kFlush);
+                    // the fused variant does two sweeps: compare time per sweep
+                    const float ms = time_launches(launch, s, ea, eb, 5, fl, kFlush) / (var == 3 ? 2.f : 1.f);
                     const cudaError_t e = cudaGetLastError();
                     if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
                     if (ms < best) { best = ms; best_zc = zc; best_var = var; }
@@ -1529,6 +1648,21 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc,
                 zc[3 * l + k] = level_zc(h->lv[l], k);
                 if (ms) ms[3 * l + k] = h->lv[l].zc_ms[k];
             }
+    return WP_OK;
+}
+
+// Pins the chunk and kernel variant of one level's column kernel (kind 0 jacobi, 1 restrict,
+// 2 defect); zc <= 0 restores the heuristic.
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant) {
+    if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 3 ||
+        (variant != 0 && kind != kZcJacobi)) {
+        wp_set_error_msg("wp_mgfrac3d_set_tile: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    Level& L = h->lv[level];
+    L.zc[kind] = zc > 0 ? zc : 0;
+    L.var[kind] = variant;
+    L.zc_ms[kind] = 0.f;
     return WP_OK;
 }
 
