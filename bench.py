@@ -237,7 +237,8 @@ def run_ours(args, rank, world, local_rank):
         plain = {"precision": "fp64", "ms_per_projection": pms, "projections_per_s": 1000.0 / pms,
                  "vcycles": preps[-1]["cycles"], "max_abs_div": preps[-1]["max_abs_div"],
                  "rel_residual": preps[-1]["rel_residual"]}
-    return ms, ems, ek, h2d, d2h, launches, prof, reps, clk.summary(), plain
+    tiles = proj.mg.Tiles(with_times=True)
+    return ms, ems, ek, h2d, d2h, launches, prof, reps, clk.summary(), plain, tiles
 
 
 # ------------------------------------------------------------------ batched workload
@@ -448,7 +449,9 @@ def run_warmstart(args, rank, world, local_rank):
                          "max_abs_div": reps[-1]["max_abs_div"], "rel_residual": reps[-1]["rel_residual"]}
             if name == "warm":
                 row[name]["used"] = reps[-1]["warm_start"]["used"]
-                row[name]["initial_rel_residual"] = reps[-1]["warm_start"]["initial_rel_residual"]
+                row[name]["first_cycle_rel_residual"] = reps[-1]["warm_start"]["first_cycle_rel_residual"]
+            else:
+                row[name]["first_cycle_rel_residual"] = reps[-1]["history"][0]
         rows.append(row)
     # network inference alone
     guess = torch.empty(s["p"], device="cuda")
@@ -473,7 +476,10 @@ def run_warmstart(args, rank, world, local_rank):
                           "plain_cycles": float(np.mean([r["plain"]["cycles"] for r in rows])),
                           "warm_cycles": float(np.mean([r["warm"]["cycles"] for r in rows])),
                           "fallback_rate": float(np.mean([0.0 if r["warm"]["used"] else 1.0 for r in rows])),
-                          "initial_rel_residual": float(np.mean([r["warm"]["initial_rel_residual"] for r in rows])),
+                          "first_cycle_rel_residual_warm":
+                              float(np.mean([r["warm"]["first_cycle_rel_residual"] for r in rows])),
+                          "first_cycle_rel_residual_plain":
+                              float(np.mean([r["plain"]["first_cycle_rel_residual"] for r in rows])),
                           "inference_ms": infer_ms, "train_s": train_s, "data_gen_s": gen_s,
                           "loss_first": float(np.mean(losses[:10])), "loss_last": float(np.mean(losses[-50:])),
                           "params": int(net.params(0).size)},
@@ -530,9 +536,9 @@ def main():
                     help="single: one 256^3 projection per step; batch: 64 uneven grids in one graph per step; "
                          "warmstart: train the U-Net, then projections with/without its guess")
     ap.add_argument("--ws-n", type=int, default=128)
-    ap.add_argument("--ws-train", type=int, default=64)
+    ap.add_argument("--ws-train", type=int, default=128)
     ap.add_argument("--ws-eval", type=int, default=8)
-    ap.add_argument("--ws-steps", type=int, default=1500)
+    ap.add_argument("--ws-steps", type=int, default=3000)
     ap.add_argument("--ws-lr", type=float, default=2e-3)
     ap.add_argument("--batch3d", type=int, default=32)
     ap.add_argument("--batch2d", type=int, default=32)
@@ -611,7 +617,7 @@ def main():
         import datetime
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    ms, ems, ek, h2d, d2h, launches, prof, reps, clocks, plain = run_ours(args, rank, world, local_rank)
+    ms, ems, ek, h2d, d2h, launches, prof, reps, clocks, plain, tiles = run_ours(args, rank, world, local_rank)
     if world > 1:
         import torch
         torch.distributed.destroy_process_group()
@@ -648,6 +654,7 @@ def main():
                   "max_abs_div": reps[-1]["max_abs_div"]},
         "plain": plain,
         "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} for r in prof[:8]],
+        "mg_tiles": {"z_chunks_per_level": tiles[0], "variants_per_level": tiles[1], "tuned_ms_per_level": tiles[2]},
     }
     print(json.dumps(out))
 

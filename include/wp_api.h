@@ -157,10 +157,12 @@ CUWHHD_API wp_status wp_mgfrac3d_destroy(wp_mgfrac3d* h);
    the handle's work arrays (not the FP64 iterate).  Choices are cached per device and extents for
    the process.  Each candidate is timed as the median of single launches, after an L2 flush for
    levels larger than 16 MB, among chunks that give at least two CTAs per SM (when the level has
-   that many columns).  wp_mgfrac3d_tiles reports 3 chunks per level (jacobi, restrict, defect)
-   and, if ms is not NULL, the tuned median time of each in ms (0 where not tuned). */
+   that many columns).  wp_mgfrac3d_tiles reports 3 chunks per level (jacobi, restrict, defect),
+   and where not NULL their kernel variants (see wp_mgfrac3d_set_tile) and tuned median time per
+   sweep in ms (0 where not tuned). */
 CUWHHD_API wp_status wp_mgfrac3d_autotune(wp_mgfrac3d* h, void* stream);
-CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, float* ms, int cap, int* levels);
+CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, int* variant, float* ms, int cap,
+                                       int* levels);
 /* Pins one level's choice: kind 0 (Jacobi: variant 0-2 one sweep per launch with default / >= 3 /
    >= 4 CTAs per SM register budgets, 3 two sweeps per launch), 1 (restriction) or 2 (defect), with
    variant 0 for kinds 1-2; zc <= 0 restores the heuristic chunk. */

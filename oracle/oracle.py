@@ -392,7 +392,8 @@ def _up_bwd(g):
 
 
 def unet_forward(vec, b, sdf, hcell):
-    """Returns (p prediction in physical units, cache).  b, sdf: (nz, nx, ny)."""
+    """Returns (p prediction in physical units, cache).  b, sdf: (nz, nx, ny).  The network works on
+    p * tscale / rms(b) with tscale = 4 pi^2 / Lx^2 (Lx = nx h)."""
     convs, head = unet_unflatten(vec)
     b = np.asarray(b, np.float64)
     rms = np.sqrt(np.mean(b * b))
@@ -420,7 +421,8 @@ def unet_forward(vec, b, sdf, hcell):
     c["e1"] = conv(9, c["a5"])
     c["pred"] = c["e1"] @ head[:16] + head[16]
     c["rms"] = rms
-    return c["pred"] * rms, c
+    c["tscale"] = 4.0 * np.pi ** 2 / (b.shape[1] * hcell) ** 2  # 4 pi^2 / Lx^2, Lx = nx h
+    return c["pred"] * rms / c["tscale"], c
 
 
 def unet_loss_grad(vec, b, sdf, p, hcell):
@@ -428,7 +430,7 @@ def unet_loss_grad(vec, b, sdf, p, hcell):
     convs, head = unet_unflatten(vec)
     _, c = unet_forward(vec, b, sdf, hcell)
     fluid = np.asarray(sdf) > 0
-    r = c["pred"] - np.asarray(p, np.float64) / c["rms"]
+    r = c["pred"] - np.asarray(p, np.float64) * c["tscale"] / c["rms"]
     cnt = max(int(fluid.sum()), 1)
     mu = r[fluid].sum() / cnt
     rr = np.where(fluid, r - mu, 0.0)

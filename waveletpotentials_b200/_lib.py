@@ -91,7 +91,7 @@ SIGNATURES = {
     "wp_dst3d_destroy": (I, [P]),
     "wp_dst3d_solve_noalloc": (I, [P, P, I, I, I, D, D, D, P]),
     "wp_mgfrac3d_autotune": (I, [P, P]),
-    "wp_mgfrac3d_tiles": (I, [P, P, P, I, P]),
+    "wp_mgfrac3d_tiles": (I, [P, P, P, P, I, P]),
     "wp_mgfrac3d_set_tile": (I, [P, I, I, I, I]),
     "wp_conv3_forward": (I, [P, P, I, P, P, I, P, P, I, I, I, I, I, P, P, P]),
     "wp_conv3_wgrad": (I, [P, P, I, P, I, I, I, I, P]),

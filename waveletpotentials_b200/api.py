@@ -21,7 +21,7 @@ from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONS
 __all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRecover2D", "CuMultigridFrac3D",
            "CuMultigridFrac2D", "CuConvergence", "CuGradient", "CuSolidLevelSet3D", "CuSolidLevelSet2D", "CuDst3D",
            "Projector3D", "Projector2D", "BatchProjector", "max_abs", "conv3_forward", "conv3_wgrad",
-           "random_field3d", "velocity3d_device", "UNetWarmStart",
+           "random_field3d", "velocity3d_device", "UNetWarmStart", "warm_started_solve",
            "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
            "PROLONG_TRILINEAR", "mac_shapes3d", "mac_shapes2d"]
 
@@ -209,15 +209,18 @@ class CuMultigridFrac3D:
         check(lib().wp_mgfrac3d_autotune(self._h, _stream(stream)), "wp_mgfrac3d_autotune")
 
     def Tiles(self, with_times=False):
-        """Per level: (jacobi, restrict, defect) z-chunks in use (and the tuned times in ms)."""
+        """Per level: (jacobi, restrict, defect) z-chunks in use; with_times adds the kernel variants
+        and the tuned times per sweep in ms."""
         buf = (ctypes.c_int * (3 * 32))()
+        var = (ctypes.c_int * (3 * 32))()
         ms = (ctypes.c_float * (3 * 32))()
         nl = ctypes.c_int()
-        check(lib().wp_mgfrac3d_tiles(self._h, ctypes.cast(buf, ctypes.c_void_p), ctypes.cast(ms, ctypes.c_void_p), 96,
-                                      ctypes.byref(nl)), "wp_mgfrac3d_tiles")
+        check(lib().wp_mgfrac3d_tiles(self._h, ctypes.cast(buf, ctypes.c_void_p), ctypes.cast(var, ctypes.c_void_p),
+                                      ctypes.cast(ms, ctypes.c_void_p), 96, ctypes.byref(nl)), "wp_mgfrac3d_tiles")
         zc = [tuple(buf[3 * l:3 * l + 3]) for l in range(nl.value)]
         if with_times:
-            return zc, [tuple(round(v, 4) for v in ms[3 * l:3 * l + 3]) for l in range(nl.value)]
+            return (zc, [tuple(var[3 * l:3 * l + 3]) for l in range(nl.value)],
+                    [tuple(round(v, 4) for v in ms[3 * l:3 * l + 3]) for l in range(nl.value)])
         return zc
 
     def SetTile(self, level, kind, zc, variant=0):
@@ -444,6 +447,34 @@ class CuDst3D:
             pass
 
 
+WARM_START_ACCEPT = 0.3  # relative residual after one V-cycle below which the network's guess is kept
+
+
+def warm_started_solve(mg, p, b, sdf, hcell, net, opts, stream=None) -> dict:
+    """Multigrid solve to the same tolerance from the network's guess, with the plain solver as
+    fallback: one V-cycle from the guess (its first pre-smoothing removes the guess's grid-scale
+    noise); if the residual is then not below WARM_START_ACCEPT (about one V-cycle's reduction from a
+    zero start) the solve restarts from zero, otherwise it continues from that iterate."""
+    net.predict(p, b, sdf, hcell, stream)
+    one = dict(opts)
+    one["max_cycles"] = 1
+    one["rel_tol"] = 0.0
+    first = mg.SolveTol(p, p, b, raise_on_fail=False, stream=stream, **one)
+    r1 = first["rel_residual"]
+    used = bool(r1 < WARM_START_ACCEPT)
+    if used:
+        rest = dict(opts)
+        rest["max_cycles"] = max(1, opts.get("max_cycles", 60) - 1)
+        rep = mg.SolveTol(p, p, b, raise_on_fail=False, stream=stream, **rest)
+        rep["cycles"] += 1
+        rep["history"] = first["history"] + rep["history"]
+    else:
+        rep = mg.SolveTol(p, None, b, raise_on_fail=False, stream=stream, **opts)
+        rep["cycles"] += 1  # the discarded cycle from the guess
+    rep["warm_start"] = {"first_cycle_rel_residual": r1, "used": used}
+    return rep
+
+
 class Projector3D:
     """One projection of a MAC velocity field (the composition of TestLocalProjection.cpp:666-767):
     b = -div(a u) -> fractional multigrid solve to tolerance -> u <- a (u - grad p) -> max|div| check
@@ -474,18 +505,11 @@ class Projector3D:
         """Projects (xv, yv, zv) in place (result a (u - grad p)) and writes the potential q."""
         CuConvergence.GetB_3d_frac_vel(self.b, xv, yv, zv, self.ax, self.ay, self.az, self.dim, self.dx,
                                        stream=stream)
-        warm = None
         if pre_p is None and self.warm_start is not None:
-            # the network's guess is kept only if it starts below the zero start's residual (1.0);
-            # the multigrid then runs to the same tolerance either way
-            self.warm_start.predict(self.p, self.b, self.sdf, self.dx[0], stream)
-            r0 = self.mg.GetResdualError(self.p, self.b, stream)
-            warm = {"initial_rel_residual": r0, "used": bool(r0 < 1.0)}
-            if warm["used"]:
-                pre_p = self.p
-        rep = self.mg.SolveTol(self.p, pre_p, self.b, raise_on_fail=False, stream=stream, **self.opts)
-        if warm is not None:
-            rep["warm_start"] = warm
+            rep = warm_started_solve(self.mg, self.p, self.b, self.sdf, self.dx[0], self.warm_start, self.opts,
+                                     stream)
+        else:
+            rep = self.mg.SolveTol(self.p, pre_p, self.b, raise_on_fail=False, stream=stream, **self.opts)
         CuGradient.SubtractGradient3D_Frac_P(xv, yv, zv, self.p, self.ax, self.ay, self.az, self.dim, self.dx,
                                              multiply_frac=True, stream=stream)
         # -div of the fraction-weighted projected field (open-face divergence of a (u - grad p))

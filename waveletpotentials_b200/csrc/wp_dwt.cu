@@ -147,11 +147,11 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
 
     // ---- load the tile: C lines of N samples
     if (g.contiguous) {
-        for (int i = tid; i < C * N; i += NT) {
-            int col = i / N, p = i - col * N;
-            T v = T(0);
-            if (i0 + col < g.ni) v = src[obase + (long)(i0 + col) * g.s_in + p];
-            buf[0][p * CP + col] = v;
+        // one warp per line: coalesced along the line, no index division
+        for (int col = tid >> 5; col < C; col += NT / 32) {
+            const bool ok = i0 + col < g.ni;
+            const T* line = src + obase + (long)(ok ? i0 + col : 0) * g.s_in;
+            for (int p = tid & 31; p < N; p += 32) buf[0][p * CP + col] = ok ? line[p] : T(0);
         }
     } else {
         for (int i = tid; i < C * N; i += NT) {
@@ -178,14 +178,24 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
             for (int t = tid; t < C * nch; t += NT) {
                 const int col = t % C, k0 = (t / C) * CH;
                 T A[WIN], Dd[WIN];
+                if (k0 >= 4 && 2 * (k0 + WIN - 4) <= L) {
+                    // interior window: no reflection
+                    const T* base = S + (2 * (k0 - 4)) * CP + col;
 #pragma unroll
-                for (int w = 0; w < WIN; ++w) {
-                    int ai, di; float sa, sd;
-                    fwd_reflect<WAV>(k0 - 4 + w, L, bcd, ai, di, sa, sd);
-                    ai = clampi(ai, 0, lim);
-                    di = clampi(di, 0, lim);
-                    A[w] = T(sa) * S[ai * CP + col];
-                    Dd[w] = T(sd) * S[di * CP + col];
+                    for (int w = 0; w < WIN; ++w) {
+                        A[w] = base[(2 * w) * CP];
+                        Dd[w] = base[(2 * w + 1) * CP];
+                    }
+                } else {
+#pragma unroll
+                    for (int w = 0; w < WIN; ++w) {
+                        int ai, di; float sa, sd;
+                        fwd_reflect<WAV>(k0 - 4 + w, L, bcd, ai, di, sa, sd);
+                        ai = clampi(ai, 0, lim);
+                        di = clampi(di, 0, lim);
+                        A[w] = T(sa) * S[ai * CP + col];
+                        Dd[w] = T(sd) * S[di * CP + col];
+                    }
                 }
                 if (WAV == WP_ID_CDF3_7) {
 #pragma unroll
@@ -260,16 +270,27 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
             for (int t = tid; t < C * nch; t += NT) {
                 const int col = t % C, k0 = (t / C) * CH;
                 T A[WIN], Dd[WIN], SA[WIN], SD[WIN];
+                if (k0 >= 4 && k0 + WIN - 4 <= L) {
+                    // interior window: no reflection
 #pragma unroll
-                for (int w = 0; w < WIN; ++w) {
-                    int ai, di; float sa, sd;
-                    inv_reflect<WAV>(k0 - 4 + w, L, bcd, ai, di, sa, sd);
-                    ai = clampi(ai, 0, NA - 1);
-                    di = clampi(di, 0, L - 1);
-                    A[w] = Sa[ai * CP + col];
-                    Dd[w] = Sd[di * CP + col];
-                    SA[w] = T(sa);
-                    SD[w] = T(sd);
+                    for (int w = 0; w < WIN; ++w) {
+                        A[w] = Sa[(k0 - 4 + w) * CP + col];
+                        Dd[w] = Sd[(k0 - 4 + w) * CP + col];
+                        SA[w] = T(1);
+                        SD[w] = T(1);
+                    }
+                } else {
+#pragma unroll
+                    for (int w = 0; w < WIN; ++w) {
+                        int ai, di; float sa, sd;
+                        inv_reflect<WAV>(k0 - 4 + w, L, bcd, ai, di, sa, sd);
+                        ai = clampi(ai, 0, NA - 1);
+                        di = clampi(di, 0, L - 1);
+                        A[w] = Sa[ai * CP + col];
+                        Dd[w] = Sd[di * CP + col];
+                        SA[w] = T(sa);
+                        SD[w] = T(sd);
+                    }
                 }
                 if (WAV == WP_ID_CDF3_7) {
 #pragma unroll
@@ -325,12 +346,14 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
     // ---- store the tile
     const int basebuf = (levels - 1) & 1;
     if (g.contiguous) {
-        for (int i = tid; i < C * N; i += NT) {
-            int col = i / N, p = i - col * N;
+        for (int col = tid >> 5; col < C; col += NT / 32) {
             if (i0 + col >= g.ni) continue;
-            int b = outbuf;
-            if (b < 0) b = (p < nb) ? basebuf : ((levels - (31 - __clz(p - ext))) & 1);
-            dst[obase + (long)(i0 + col) * g.s_in + p] = buf[b][p * CP + col];
+            T* line = dst + obase + (long)(i0 + col) * g.s_in;
+            for (int p = tid & 31; p < N; p += 32) {
+                int b = outbuf;
+                if (b < 0) b = (p < nb) ? basebuf : ((levels - (31 - __clz(p - ext))) & 1);
+                line[p] = buf[b][p * CP + col];
+            }
         }
     } else {
         for (int i = tid; i < C * N; i += NT) {

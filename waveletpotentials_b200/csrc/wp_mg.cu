@@ -1639,13 +1639,15 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_autotune(wp_mgfrac3d* h, void* strea
     return autotune(h, (cudaStream_t)stream);
 }
 
-extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, float* ms, int cap, int* levels) {
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, int* variant, float* ms, int cap,
+                                                   int* levels) {
     if (!h || (!zc && cap > 0)) { wp_set_error_msg("wp_mgfrac3d_tiles: null pointer"); return WP_ERR_INVALID_ARG; }
     if (levels) *levels = h->nl;
     for (int l = 0; l < h->nl; ++l)
         for (int k = 0; k < 3; ++k)
             if (3 * l + k < cap) {
                 zc[3 * l + k] = level_zc(h->lv[l], k);
+                if (variant) variant[3 * l + k] = h->lv[l].var[k];
                 if (ms) ms[3 * l + k] = h->lv[l].zc_ms[k];
             }
     return WP_OK;

@@ -8,7 +8,7 @@
 //   c2a 16->32, c2b 32->32 = s2 -> avg-pool                                (n/2)^3
 //   c3a 32->64, c3b 64->64 = e3 -> nearest upsample                        (n/4)^3
 //   d2a [s2 | up(e3)] 96->32, d2b 32->32 = e2 -> nearest upsample          (n/2)^3
-//   d1a [s1 | up(e2)] 48->16, d1b 16->16 = e1 -> 1x1 head 16->1 = p / rms(b)
+//   d1a [s1 | up(e2)] 48->16, d1b 16->16 = e1 -> 1x1 head 16->1 = p tscale / rms(b)
 // Every 3x3x3 convolution is followed by ReLU.  Skip concatenations are two input parts of one
 // convolution (wp_conv.cu).  The loss is the mean over fluid cells (sdf > 0) of the squared error
 // after removing the mean error over those cells (a constant offset is free: the multigrid
@@ -163,9 +163,9 @@ __global__ void up_bwd_kernel(bf16* __restrict__ gc, const bf16* __restrict__ gf
     st8(gc + vc * C + cg * 8, acc);
 }
 
-// pred[v] = wh . e1[v] + bh; out (optional) = pred * rms(b)
+// pred[v] = wh . e1[v] + bh; out (optional) = pred * rms(b) / tscale
 __global__ void head_kernel(float* __restrict__ pred, float* __restrict__ out, const bf16* __restrict__ e1,
-                            const float* __restrict__ wh, long n, const double* __restrict__ acc) {
+                            const float* __restrict__ wh, long n, const double* __restrict__ acc, double tscale) {
     const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (i >= n) return;
     float v[16];
@@ -175,15 +175,16 @@ __global__ void head_kernel(float* __restrict__ pred, float* __restrict__ out, c
 #pragma unroll
     for (int c = 0; c < 16; ++c) s += wh[c] * v[c];
     pred[i] = s;
-    if (out) out[i] = (float)(s * sqrt(acc[0] / (double)n));
+    if (out) out[i] = (float)(s * sqrt(acc[0] / (double)n) / tscale);
 }
 
-// pass 1 of the loss: acc[1] += sum over fluid of (pred - t), acc[2] += fluid count; t = p / rms(b)
+// pass 1 of the loss: acc[1] += sum over fluid of (pred - t), acc[2] += fluid count;
+// t = p tscale / rms(b)
 __global__ void loss_mean_kernel(const float* __restrict__ pred, const float* __restrict__ p,
-                                 const float* __restrict__ sdf, long n, double* __restrict__ acc) {
+                                 const float* __restrict__ sdf, long n, double* __restrict__ acc, double tscale) {
     __shared__ double red[8];
     const double ms = acc[0] / (double)n;
-    const double inv = ms > 0.0 ? 1.0 / sqrt(ms) : 0.0;
+    const double inv = ms > 0.0 ? tscale / sqrt(ms) : 0.0;
     double s = 0.0, c = 0.0;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         if (sdf[i] > 0.f) {
@@ -200,10 +201,10 @@ __global__ void loss_mean_kernel(const float* __restrict__ pred, const float* __
 
 // pass 2: g = 2 (r - mean r) / count on fluid cells, acc[3] += (r - mean r)^2 / count
 __global__ void loss_grad_kernel(float* __restrict__ g, const float* __restrict__ pred, const float* __restrict__ p,
-                                 const float* __restrict__ sdf, long n, double* __restrict__ acc) {
+                                 const float* __restrict__ sdf, long n, double* __restrict__ acc, double tscale) {
     __shared__ double red[8];
     const double ms = acc[0] / (double)n;
-    const double inv = ms > 0.0 ? 1.0 / sqrt(ms) : 0.0;
+    const double inv = ms > 0.0 ? tscale / sqrt(ms) : 0.0;
     const double cnt = fmax(acc[2], 1.0), mu = acc[1] / cnt;
     double l = 0.0;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -338,6 +339,13 @@ wp_status refresh_copies(wp_unet* h, cudaStream_t s) {
     return WP_OK;
 }
 
+// the network works on p * tscale / rms(b): tscale = 4 pi^2 / Lx^2 (Lx = nx h, the domain length
+// along x) makes the normalized pressure of a smooth right-hand side O(1)
+double target_scale(const wp_unet* h, double hcell) {
+    const double lx = h->n[0] * hcell;
+    return 4.0 * M_PI * M_PI / (lx * lx);
+}
+
 long vox(const wp_unet* h, int level) {
     return (long)(h->n[0] >> level) * (h->n[1] >> level) * (h->n[2] >> level);
 }
@@ -394,17 +402,19 @@ wp_status forward(wp_unet* h, const float* b, const float* sdf, double hcell, fl
               up_kernel<<<blocks(n0 * 4), 256, 0, s>>>(h->u1, h->e2, 32, nx, ny, nz));
     if ((st = conv_fwd(h, D1A, h->s1, h->u1, h->a5, 0, s)) != WP_OK) return st;
     if ((st = conv_fwd(h, D1B, h->a5, nullptr, h->e1, 0, s)) != WP_OK) return st;
-    WP_KERNEL("unet_head", 40.0 * n0, s, head_kernel<<<blocks(n0), 256, 0, s>>>(h->pred, out, h->e1, h->wh, n0, h->acc));
+    WP_KERNEL("unet_head", 40.0 * n0, s, head_kernel<<<blocks(n0), 256, 0, s>>>(h->pred, out, h->e1, h->wh, n0, h->acc,
+                                                                     target_scale(h, hcell)));
     return WP_OK;
 }
 
-wp_status backward(wp_unet* h, const float* sdf, const float* p, cudaStream_t s) {
+wp_status backward(wp_unet* h, const float* sdf, const float* p, double hcell, cudaStream_t s) {
     const long n0 = vox(h, 0);
     const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
     wp_status st;
     const unsigned rb = std::min<unsigned>(blocks(n0), 4 * wp_sm_count());
-    WP_KERNEL("unet_loss", 12.0 * n0, s, loss_mean_kernel<<<rb, 256, 0, s>>>(h->pred, p, sdf, n0, h->acc));
-    WP_KERNEL("unet_loss", 16.0 * n0, s, loss_grad_kernel<<<rb, 256, 0, s>>>(h->gpred, h->pred, p, sdf, n0, h->acc));
+    WP_KERNEL("unet_loss", 12.0 * n0, s, loss_mean_kernel<<<rb, 256, 0, s>>>(h->pred, p, sdf, n0, h->acc, target_scale(h, hcell)));
+    WP_KERNEL("unet_loss", 16.0 * n0, s, loss_grad_kernel<<<rb, 256, 0, s>>>(h->gpred, h->pred, p, sdf, n0, h->acc,
+                                                                                   target_scale(h, hcell)));
     // zero the gradient accumulators
     for (auto& C : h->c) {
         for (int q = 0; q < C.nparts; ++q) WP_CUDA_TRY(cudaMemsetAsync(C.gw[q], 0, sizeof(float) * C.wsize(q), s));
@@ -591,7 +601,7 @@ extern "C" CUWHHD_API wp_status wp_unet_train_step(wp_unet* h, const float* b, c
     }
     cudaStream_t s = (cudaStream_t)stream;
     wp_status st = forward(h, b, sdf, hcell, nullptr, s);
-    if (st == WP_OK) st = backward(h, sdf, p, s);
+    if (st == WP_OK) st = backward(h, sdf, p, hcell, s);
     if (st == WP_OK && lr > 0) st = adam(h, lr, s);
     if (st != WP_OK) return st;
     if ((st = wp_conv_check_error(s)) != WP_OK) return st;

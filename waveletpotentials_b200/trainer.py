@@ -61,17 +61,17 @@ def evaluate(net: api.UNetWarmStart, samples, tol: float = 1e-6):
     """V-cycles to `tol` from a zero start and from the network's guess (with the fallback rule of
     Projector3D: the guess is used only if its residual is below the zero start's)."""
     out = []
+    opts = dict(rel_tol=tol, max_cycles=60, precision=api.PREC_MIXED)
     for s in samples:
         mg = s["mg"]
         dst = torch.zeros_like(s["b"])
-        plain = mg.SolveTol(dst, None, s["b"], rel_tol=tol, max_cycles=60, precision=api.PREC_MIXED,
-                            raise_on_fail=False)
+        plain = mg.SolveTol(dst, None, s["b"], raise_on_fail=False, **opts)
         guess = torch.empty_like(s["b"])
         net.predict(guess, s["b"], s["sdf"], s["h"])
         r0 = mg.GetResdualError(guess, s["b"])
-        used = r0 < 1.0
-        warm = mg.SolveTol(dst, guess if used else None, s["b"], rel_tol=tol, max_cycles=60,
-                           precision=api.PREC_MIXED, raise_on_fail=False)
+        warm = api.warm_started_solve(mg, dst, s["b"], s["sdf"], s["h"], net, opts)
         out.append({"plain_cycles": plain["cycles"], "warm_cycles": warm["cycles"], "initial_rel_residual": r0,
-                    "used": bool(used), "warm_rel_residual": warm["rel_residual"]})
+                    "plain_first_cycle": plain["history"][0] if plain["history"] else None,
+                    "warm_first_cycle": warm["warm_start"]["first_cycle_rel_residual"],
+                    "used": warm["warm_start"]["used"], "warm_rel_residual": warm["rel_residual"]})
     return out
