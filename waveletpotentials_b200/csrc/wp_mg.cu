@@ -639,6 +639,163 @@ __global__ void __launch_bounds__(256) prolong_tri_add_kernel(T* __restrict__ v,
     v[y + (long)x * ny + (long)z * nx * ny] += acc;
 }
 
+// ------------------------------------------------------------------ fused coarse cycle
+// The V-cycle below a small level (<= kCoarseCells cells) in ONE single-CTA launch: zeroing, sweeps,
+// residual restriction, coarsest sweeps and prolongation of every coarse level, with block barriers
+// between the steps (the data stay in L2).  At these sizes every separate kernel is a few
+// microseconds of launch and ramp for a few thousand cells.  Per cell the arithmetic is that of the
+// separate kernels: `row` for the sweeps, and the restriction sums in the order of
+// resid_restrict_z_kernel: ((x0,y0) + (x0,y1)) + ((x1,y0) + (x1,y1)), each child (0 + w_z0 r) + w_z1 r.
+constexpr int kCoarseMax = 8;
+constexpr int kCoarseCells = 4096;
+
+template <typename T>
+struct CLev {
+    Lvl<T> L;
+    T *v, *t, *f;
+};
+template <typename T>
+struct CPack {
+    CLev<T> lv[kCoarseMax];
+    int n;
+};
+
+template <typename T>
+__device__ __forceinline__ void cc_sweep(const Lvl<T>& L, T* __restrict__ dst, const T* __restrict__ src,
+                                         const T* __restrict__ f, T w) {
+    const int nx = L.nx, ny = L.ny, cells = L.nx * L.ny * L.nz;
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) {
+        const int y = i % ny, x = (i / ny) % nx, z = i / (nx * ny);
+        T dg, od, c;
+        row<T, T, false>(L, src, nullptr, 0, 0, x, y, z, dg, od, c);
+        dst[i] = dg > (T)kEps ? ((T)1 - w) * c + w * (f[i] - od) / dg : (T)0;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void cc_restrict(const Lvl<T>& L, const T* __restrict__ v, const T* __restrict__ f,
+                                            T* __restrict__ fc, int ncx, int ncy, int ncz) {
+    const int ccells = ncx * ncy * ncz;
+    for (int ci = threadIdx.x; ci < ccells; ci += blockDim.x) {
+        const int cy = ci % ncy, cx = (ci / ncy) % ncx, cz = ci / (ncx * ncy);
+        const int x0 = 2 * cx, y0 = 2 * cy, zb = 2 * cz;
+        const double sx = L.d[0][x0] + (x0 + 1 < L.nx ? L.d[0][x0 + 1] : 0.0);
+        const double sy = L.d[1][y0] + (y0 + 1 < L.ny ? L.d[1][y0 + 1] : 0.0);
+        const double sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
+        T tot[2][2] = {{(T)0, (T)0}, {(T)0, (T)0}};
+        for (int xo = 0; xo < 2; ++xo) {
+            const int x = x0 + xo;
+            if (x >= L.nx) break;
+            for (int yo = 0; yo < 2; ++yo) {
+                const int y = y0 + yo;
+                if (y >= L.ny) break;
+                const T wxy = (T)(L.d[1][y] / sy * (L.d[0][x] / sx));
+                T acc = 0;
+                for (int kz = 0; kz < 2; ++kz) {
+                    const int z = zb + kz;
+                    if (z >= L.nz) break;
+                    T dg, od, c;
+                    row<T, T, false>(L, v, nullptr, 0, 0, x, y, z, dg, od, c);
+                    const long i = y + (long)x * L.ny + (long)z * L.nx * L.ny;
+                    const T r = dg > (T)kEps ? f[i] - (dg * c + od) : (T)0;
+                    acc += (T)(L.d[2][z] / sz) * wxy * r;
+                }
+                tot[xo][yo] = acc;
+            }
+        }
+        fc[ci] = (tot[0][0] + tot[0][1]) + (tot[1][0] + tot[1][1]);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void cc_prolong(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny, int nz,
+                                           int ncx, int ncy, int ncz, int prolong) {
+    const int cells = nx * ny * nz;
+    const long sc = (long)ncx * ncy;
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) {
+        const int y = i % ny, x = (i / ny) % nx, z = i / (nx * ny);
+        const int px = x >> 1, py = y >> 1, pz = z >> 1;
+        if (prolong != WP_PROLONG_TRILINEAR) {
+            v[i] += vc[py + (long)px * ncy + pz * sc];
+            continue;
+        }
+        int qx = (x & 1) ? px + 1 : px - 1, qy = (y & 1) ? py + 1 : py - 1, qz = (z & 1) ? pz + 1 : pz - 1;
+        if (qx < 0 || qx >= ncx) qx = px;
+        if (qy < 0 || qy >= ncy) qy = py;
+        if (qz < 0 || qz >= ncz) qz = pz;
+        auto C = [&](int xx, int yy, int zz) -> T { return vc[yy + (long)xx * ncy + zz * sc]; };
+        const T a = (T)0.75, b = (T)0.25;
+        T acc;
+        if (ncz == 1 && nz == 1) {
+            acc = a * (a * C(px, py, 0) + b * C(px, qy, 0)) + b * (a * C(qx, py, 0) + b * C(qx, qy, 0));
+        } else {
+            const T lo = a * (a * C(px, py, pz) + b * C(px, qy, pz)) + b * (a * C(qx, py, pz) + b * C(qx, qy, pz));
+            const T hi = a * (a * C(px, py, qz) + b * C(px, qy, qz)) + b * (a * C(qx, py, qz) + b * C(qx, qy, qz));
+            acc = a * lo + b * hi;
+        }
+        v[i] += acc;
+    }
+}
+
+// V-cycle of the pack's levels; level 0 of the pack has its f and a zeroed v on entry
+template <typename T>
+__global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1, int nu2, T w, int citers,
+                                                            int prolong) {
+    T* v[kCoarseMax];
+    T* t[kCoarseMax];
+    for (int l = 0; l < P.n; ++l) {
+        v[l] = P.lv[l].v;
+        t[l] = P.lv[l].t;
+    }
+    for (int l = 0; l < P.n - 1; ++l) {
+        const Lvl<T>& L = P.lv[l].L;
+        if (l > 0) {
+            const int n = L.nx * L.ny * L.nz;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) v[l][i] = (T)0;
+            __syncthreads();
+        }
+        for (int k = 0; k < nu1; ++k) {
+            cc_sweep<T>(L, t[l], v[l], P.lv[l].f, w);
+            __syncthreads();
+            T* tmp = v[l];
+            v[l] = t[l];
+            t[l] = tmp;
+        }
+        const Lvl<T>& C = P.lv[l + 1].L;
+        cc_restrict<T>(L, v[l], P.lv[l].f, P.lv[l + 1].f, C.nx, C.ny, C.nz);
+        __syncthreads();
+    }
+    {
+        const int l = P.n - 1;
+        const Lvl<T>& L = P.lv[l].L;
+        if (l > 0) {
+            const int n = L.nx * L.ny * L.nz;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) v[l][i] = (T)0;
+            __syncthreads();
+        }
+        for (int k = 0; k < citers; ++k) {
+            cc_sweep<T>(L, t[l], v[l], P.lv[l].f, w);
+            __syncthreads();
+            T* tmp = v[l];
+            v[l] = t[l];
+            t[l] = tmp;
+        }
+    }
+    for (int l = P.n - 2; l >= 0; --l) {
+        const Lvl<T>& L = P.lv[l].L;
+        const Lvl<T>& C = P.lv[l + 1].L;
+        cc_prolong<T>(v[l], v[l + 1], L.nx, L.ny, L.nz, C.nx, C.ny, C.nz, prolong);
+        __syncthreads();
+        for (int k = 0; k < nu2; ++k) {
+            cc_sweep<T>(L, t[l], v[l], P.lv[l].f, w);
+            __syncthreads();
+            T* tmp = v[l];
+            v[l] = t[l];
+            t[l] = tmp;
+        }
+    }
+}
+
 // coarse f = spacing-weighted average of the fine residuals of the (up to 8) children
 template <typename T>
 __global__ void __launch_bounds__(256) resid_restrict_kernel(T* __restrict__ fc, const T* __restrict__ v,
@@ -1145,6 +1302,26 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
     Level& L = h->lv[l];
     const dim3 g = grid_of(L.n[0], L.n[1], L.n[2]);
     wp_status st;
+    if (l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax && f == Bufs<T>::f(L)) {
+        // the rest of the cycle in one launch; the host mirrors the buffer swaps it performs
+        CPack<T> P;
+        P.n = h->nl - l;
+        for (int k = 0; k < P.n; ++k) {
+            Level& Q = h->lv[l + k];
+            P.lv[k].L = view<T>(Q);
+            P.lv[k].v = Bufs<T>::v(Q);
+            P.lv[k].t = Bufs<T>::t(Q);
+            P.lv[k].f = Bufs<T>::f(Q);
+        }
+        WP_KERNEL("coarse_cycle", (double)L.cells * (3.0 * sizeof(T) + 12.0) * (nu1 + nu2 + 2), s,
+                  coarse_cycle_kernel<T><<<1, 1024, 0, s>>>(P, nu1, nu2, w, h->coarsest_iters, prolong));
+        for (int k = 0; k < P.n; ++k) {
+            Level& Q = h->lv[l + k];
+            const int swaps = (k == P.n - 1) ? h->coarsest_iters : nu1 + nu2;
+            if (swaps & 1) std::swap(Bufs<T>::v(Q), Bufs<T>::t(Q));
+        }
+        return WP_OK;
+    }
     if (l < h->nl - 1) {
         if ((st = smooth<T>(L, f, nu1, w, s)) != WP_OK) return st;
         Level& C = h->lv[l + 1];
