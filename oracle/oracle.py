@@ -391,26 +391,31 @@ def _up_bwd(g):
     return g.reshape(nz // 2, 2, nx // 2, 2, ny // 2, 2, c).sum(axis=(1, 3, 5))
 
 
-def unet_forward(vec, b, sdf, hcell):
+def unet_forward(vec, b, sdf, hcell, bf16=False):
     """Returns (p prediction in physical units, cache).  b, sdf: (nz, nx, ny).  The network works on
-    p * tscale / rms(b) with tscale = 4 pi^2 / Lx^2 (Lx = nx h)."""
+    p * tscale / rms(b) with tscale = 4 pi^2 / Lx^2 (Lx = nx h).  bf16=True rounds the weights and
+    every stored activation to BF16 where the GPU network stores them (the arithmetic stays FP64)."""
     convs, head = unet_unflatten(vec)
+    R = bf16_round if bf16 else (lambda a: np.asarray(a, np.float64))
+    if bf16:
+        convs = [([R(w) for w in ws], bb) for ws, bb in convs]
     b = np.asarray(b, np.float64)
     rms = np.sqrt(np.mean(b * b))
     x = np.zeros(b.shape + (16,))
     x[..., 0] = b / rms if rms > 0 else 0.0
     x[..., 1] = np.clip(np.asarray(sdf, np.float64) / (4.0 * hcell), -1.0, 1.0)
+    x = R(x)
     relu = lambda v: np.maximum(v, 0.0)
     def conv(i, *xs):
         ws, bb = convs[i]
-        return relu(sum(conv3d_forward(xx, w) for xx, w in zip(xs, ws)) + bb)
-    c = {"in": x}
+        return R(relu(sum(conv3d_forward(xx, w) for xx, w in zip(xs, ws)) + bb))
+    c = {"in": x, "R": R, "convs": convs}
     c["a1"] = conv(0, x)
     c["s1"] = conv(1, c["a1"])
-    c["p1"] = _pool(c["s1"])
+    c["p1"] = R(_pool(c["s1"]))
     c["a2"] = conv(2, c["p1"])
     c["s2"] = conv(3, c["a2"])
-    c["p2"] = _pool(c["s2"])
+    c["p2"] = R(_pool(c["s2"]))
     c["a3"] = conv(4, c["p2"])
     c["e3"] = conv(5, c["a3"])
     c["u2"] = _up(c["e3"])
@@ -425,10 +430,12 @@ def unet_forward(vec, b, sdf, hcell):
     return c["pred"] * rms / c["tscale"], c
 
 
-def unet_loss_grad(vec, b, sdf, p, hcell):
-    """Loss of wp_unet_train_step and its gradient (flattened in the parameter order)."""
-    convs, head = unet_unflatten(vec)
-    _, c = unet_forward(vec, b, sdf, hcell)
+def unet_loss_grad(vec, b, sdf, p, hcell, bf16=False):
+    """Loss of wp_unet_train_step and its gradient (flattened in the parameter order); bf16=True
+    also rounds the stored gradients to BF16 where the GPU network stores them."""
+    _, head = unet_unflatten(vec)
+    _, c = unet_forward(vec, b, sdf, hcell, bf16)
+    convs, R = c["convs"], c["R"]
     fluid = np.asarray(sdf) > 0
     r = c["pred"] - np.asarray(p, np.float64) * c["tscale"] / c["rms"]
     cnt = max(int(fluid.sum()), 1)
@@ -450,20 +457,20 @@ def unet_loss_grad(vec, b, sdf, p, hcell):
             gconv[i][k] = conv3d_weight_grad(xx, gy)
             outs.append(conv3d_input_grad(gy, w) if need else None)
         return outs
-    g_e1 = mask(g[..., None] * head[:16], c["e1"])
-    g_a5 = mask(back(9, g_e1, [c["a5"]], True)[0], c["a5"])
-    g_s1p, g_u1 = back(8, g_a5, [c["s1"], c["u1"]], True)
-    g_e2 = mask(_up_bwd(g_u1), c["e2"])
-    g_a4 = mask(back(7, g_e2, [c["a4"]], True)[0], c["a4"])
-    g_s2p, g_u2 = back(6, g_a4, [c["s2"], c["u2"]], True)
-    g_e3 = mask(_up_bwd(g_u2), c["e3"])
-    g_a3 = mask(back(5, g_e3, [c["a3"]], True)[0], c["a3"])
-    g_p2 = back(4, g_a3, [c["p2"]], True)[0]
-    g_s2 = mask(g_s2p + _up(g_p2) / 8.0, c["s2"])
-    g_a2 = mask(back(3, g_s2, [c["a2"]], True)[0], c["a2"])
-    g_p1 = back(2, g_a2, [c["p1"]], True)[0]
-    g_s1 = mask(g_s1p + _up(g_p1) / 8.0, c["s1"])
-    g_a1 = mask(back(1, g_s1, [c["a1"]], True)[0], c["a1"])
+    g_e1 = R(mask(g[..., None] * head[:16], c["e1"]))
+    g_a5 = R(mask(back(9, g_e1, [c["a5"]], True)[0], c["a5"]))
+    g_s1p, g_u1 = (R(t) for t in back(8, g_a5, [c["s1"], c["u1"]], True))
+    g_e2 = R(mask(_up_bwd(g_u1), c["e2"]))
+    g_a4 = R(mask(back(7, g_e2, [c["a4"]], True)[0], c["a4"]))
+    g_s2p, g_u2 = (R(t) for t in back(6, g_a4, [c["s2"], c["u2"]], True))
+    g_e3 = R(mask(_up_bwd(g_u2), c["e3"]))
+    g_a3 = R(mask(back(5, g_e3, [c["a3"]], True)[0], c["a3"]))
+    g_p2 = R(back(4, g_a3, [c["p2"]], True)[0])
+    g_s2 = R(mask(g_s2p + _up(g_p2) / 8.0, c["s2"]))
+    g_a2 = R(mask(back(3, g_s2, [c["a2"]], True)[0], c["a2"]))
+    g_p1 = R(back(2, g_a2, [c["p1"]], True)[0])
+    g_s1 = R(mask(g_s1p + _up(g_p1) / 8.0, c["s1"]))
+    g_a1 = R(mask(back(1, g_s1, [c["a1"]], True)[0], c["a1"]))
     back(0, g_a1, [c["in"]], False)
     grads = unet_flatten([(gw, gb) for gw, gb in zip(gconv, gbias)], ghead)
     return loss, grads
