@@ -100,6 +100,14 @@ def make_problem(n, seed):
     return centers, radii, (xv, yv, zv)
 
 
+# DRAM bytes (read + write) per launch of the finest-level kernels, from one ncu capture each of the
+# profiling commands in profiles/ (256^3 workload); algorithmic bytes per launch are 402.7 MB
+# (Jacobi sweep: v, f, three fraction arrays read, v written: 24 B/cell x 16,777,216 cells)
+NCU_TRAFFIC = {
+    ("jacobi_finest", 256): (423194624, "profiles/jacobi_q_256_level0.md (337.2 MB read + 86.0 MB write)"),
+}
+
+
 def max_over_ranks(values, world):
     """Element-wise max of per-rank timings (device-timed ms) over all ranks; the tensor lives on
     the current CUDA device under NCCL and on the host under gloo."""
@@ -629,8 +637,10 @@ def main():
     roof = None
     if top and top["ms"] > 0:
         ach = top["bytes"] / (top["ms"] / 1000.0) / 1e9
+        tr = NCU_TRAFFIC.get((top["kernel"], args.n))
         roof = {"bound": "hbm", "kernel": top["kernel"], "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "peak_kind": peak_kind, "traffic": None,
+                "frac": ach / hbm, "peak_kind": peak_kind, "traffic": tr[0] if tr else None,
+                "traffic_source": tr[1] if tr else None,
                 "avg_launch_us": top["ms"] * 1000.0 / top["launches"],
                 "bytes_per_launch": top["bytes"] / top["launches"]}
     cpu = None

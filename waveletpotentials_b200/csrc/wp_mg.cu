@@ -672,6 +672,20 @@ __device__ __forceinline__ void cc_sweep(const Lvl<T>& L, T* __restrict__ dst, c
     }
 }
 
+// the same sweep by one warp (cells <= 32)
+template <typename T>
+__device__ __forceinline__ void cc_sweep_warp(const Lvl<T>& L, T* __restrict__ dst, const T* __restrict__ src,
+                                              const T* __restrict__ f, T w) {
+    const int nx = L.nx, ny = L.ny, cells = L.nx * L.ny * L.nz;
+    const int i = threadIdx.x;
+    if (i < cells) {
+        const int y = i % ny, x = (i / ny) % nx, z = i / (nx * ny);
+        T dg, od, c;
+        row<T, T, false>(L, src, nullptr, 0, 0, x, y, z, dg, od, c);
+        dst[i] = dg > (T)kEps ? ((T)1 - w) * c + w * (f[i] - od) / dg : (T)0;
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void cc_restrict(const Lvl<T>& L, const T* __restrict__ v, const T* __restrict__ f,
                                             T* __restrict__ fc, int ncx, int ncy, int ncz) {
@@ -773,12 +787,32 @@ __global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1,
             for (int i = threadIdx.x; i < n; i += blockDim.x) v[l][i] = (T)0;
             __syncthreads();
         }
-        for (int k = 0; k < citers; ++k) {
-            cc_sweep<T>(L, t[l], v[l], P.lv[l].f, w);
+        if (L.nx * L.ny * L.nz <= 32) {
+            // a coarsest grid of a few cells: one warp iterates alone (warp barriers only)
+            if (threadIdx.x < 32) {
+                for (int k = 0; k < citers; ++k) {
+                    cc_sweep_warp<T>(L, t[l], v[l], P.lv[l].f, w);
+                    __syncwarp();
+                    T* tmp = v[l];
+                    v[l] = t[l];
+                    t[l] = tmp;
+                }
+            } else {
+                if (citers & 1) {
+                    T* tmp = v[l];
+                    v[l] = t[l];
+                    t[l] = tmp;
+                }
+            }
             __syncthreads();
-            T* tmp = v[l];
-            v[l] = t[l];
-            t[l] = tmp;
+        } else {
+            for (int k = 0; k < citers; ++k) {
+                cc_sweep<T>(L, t[l], v[l], P.lv[l].f, w);
+                __syncthreads();
+                T* tmp = v[l];
+                v[l] = t[l];
+                t[l] = tmp;
+            }
         }
     }
     for (int l = P.n - 2; l >= 0; --l) {
@@ -1275,19 +1309,20 @@ struct Bufs<double> {
     static double*& f(Level& L) { return L.f64; }
 };
 
+// profile names: the finest level is reported apart (it carries the roofline of the cycle)
 template <typename T>
-wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s) {
+wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s, bool finest = false) {
     const int zc = level_zc(L, kZcJacobi);
     // the variant is tuned on the FP32 kernels; FP64 smoothing keeps one sweep per launch
     const bool fused = sizeof(T) == 4 && L.var[kZcJacobi] == 3 && jacobi2_ok(L, f);
     for (int k = 0; k < sweeps;) {
         if (fused && sweeps - k >= 2) {
             // two sweeps, one pass: algorithmic bytes are those of one sweep
-            WP_KERNEL("jacobi2", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
+            WP_KERNEL(finest ? "jacobi2_finest" : "jacobi2", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
                       launch_jacobi2<T>(L, Bufs<T>::t(L), Bufs<T>::v(L), f, w, zc, s));
             k += 2;
         } else {
-            WP_KERNEL("jacobi", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
+            WP_KERNEL(finest ? "jacobi_finest" : "jacobi", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
                       launch_jacobi<T>(L, Bufs<T>::t(L), Bufs<T>::v(L), f, w, zc, s));
             k += 1;
         }
@@ -1324,20 +1359,22 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         return WP_OK;
     }
     if (l < h->nl - 1) {
-        if ((st = smooth<T>(L, f, nu1, w, s)) != WP_OK) return st;
+        if ((st = smooth<T>(L, f, nu1, w, s, l == 0)) != WP_OK) return st;
         Level& C = h->lv[l + 1];
         {
             // coarse-z chunk so the fine columns keep >= 4 CTAs per SM busy
             const int czc = level_zc(L, kZcRestrict);
-            WP_KERNEL("resid_restrict", (double)L.cells * (2.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
+            WP_KERNEL(l == 0 ? "resid_restrict_finest" : "resid_restrict",
+                      (double)L.cells * (2.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
                       launch_resid_restrict<T>(L, C, Bufs<T>::f(C), Bufs<T>::v(L), f, czc, s));
         }
         WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(C), 0, sizeof(T) * C.cells, s));
         if ((st = vcycle<T>(h, l + 1, Bufs<T>::f(C), nu1, nu2, w, prolong, s)) != WP_OK) return st;
         if (prolong == WP_PROLONG_TRILINEAR) {
-            WP_KERNEL("prolong_trilinear", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
+            WP_KERNEL(l == 0 ? "prolong_trilinear_finest" : "prolong_trilinear",
+                      (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
                       launch_prolong_tri<T>(L, C, Bufs<T>::v(L), Bufs<T>::v(C), s));
-            if ((st = smooth<T>(L, f, nu2, w, s)) != WP_OK) return st;
+            if ((st = smooth<T>(L, f, nu2, w, s, l == 0)) != WP_OK) return st;
         } else if (nu2 > 0) {
             // first post-sweep reads v + P vc directly (prolongation fused into the sweep)
             const int zc = level_zc(L, kZcJacobi);
@@ -1347,7 +1384,7 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
             T* tmp = Bufs<T>::v(L);
             Bufs<T>::v(L) = Bufs<T>::t(L);
             Bufs<T>::t(L) = tmp;
-            if ((st = smooth<T>(L, f, nu2 - 1, w, s)) != WP_OK) return st;
+            if ((st = smooth<T>(L, f, nu2 - 1, w, s, l == 0)) != WP_OK) return st;
         } else {
             WP_KERNEL("prolong_constant", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
                       prolong_add_kernel<T><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::v(L), Bufs<T>::v(C), L.n[0], L.n[1],
@@ -1358,8 +1395,9 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         if (smem <= 200 * 1024) {
             auto k = coarsest_kernel<T>;
             WP_CUDA_TRY(wp_set_smem(k, smem));
+            const int nt = (int)std::min<long>(1024, (L.cells + 31) / 32 * 32);
             WP_KERNEL("coarsest", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
-                      k<<<1, 1024, smem, s>>>(Bufs<T>::v(L), f, view<T>(L), w, h->coarsest_iters));
+                      k<<<1, nt, smem, s>>>(Bufs<T>::v(L), f, view<T>(L), w, h->coarsest_iters));
         } else {
             if ((st = smooth<T>(L, f, h->coarsest_iters, w, s)) != WP_OK) return st;
         }
