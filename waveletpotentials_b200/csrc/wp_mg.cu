@@ -16,6 +16,7 @@
 // fused residual+restriction per level (the reference uses 1 + 3 + 3 launches for the latter),
 // a single-CTA coarsest solve, and FP64 defect / norm kernels for the refinement loop.
 #include "wp_common.cuh"
+#include "wp_tc.cuh"
 
 #include <algorithm>
 #include <cstdint>
@@ -399,6 +400,144 @@ __global__ void __launch_bounds__(J2_THREADS, sizeof(T) == 4 ? 2 : 1)
                      int nty) {
     __shared__ __align__(16) T s1[3][J2_RH][J2_PITCH];
     jacobi2_body<T>(dst, src, f, L, w, zc, nty, s1);
+}
+
+// TMA-staged Jacobi sweep.  Persistent CTAs (one per SM) split the (x-tile, z) planes of the level
+// evenly; a tile is R whole x rows (all y).  Per plane a single thread issues contiguous row copies
+// on the TMA engine (cp.async.bulk) into a 4-slot ring: the v rows of the tile and its two x
+// neighbours, and the f, y-face (cell-laid), x-face (R + 1 rows) and z-face rows.  Plane z is
+// computed from the slots of z-1, z and z+1 while z+2 is in flight; after a block barrier the slot of
+// z-1 receives plane z+3.  Compute reads only shared memory (128-bit, conflict-free) and writes the
+// result with 128-bit stores, so the DRAM stream is the copies alone.  Per cell the arithmetic is
+// QCol::step's (same terms, same order).
+constexpr int TS_STAGES = 4;
+constexpr int TS_THREADS = 256;
+
+__host__ __device__ inline int ts_stage_floats(int R, int ny) { return (5 * R + 3) * ny; }
+
+// rows per tile so that four slots fit in 200 KB of shared memory
+inline int ts_rows(int nx, int ny) {
+    int r = ((200 * 1024) / (4 * TS_STAGES * ny) - 3) / 5;
+    return std::max(1, std::min(r, nx));
+}
+
+__global__ void __launch_bounds__(TS_THREADS, 1)
+    jacobi_ts_kernel(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ f,
+                     Lvl<float> L, float w, int R, int* err) {
+    using namespace wptc;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long bars[TS_STAGES];
+    float* sm = reinterpret_cast<float*>(smem_raw);
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const int stg = ts_stage_floats(R, ny);
+    const long sxy = (long)nx * ny, sax = (long)(nx + 1) * ny;
+    const int ntiles = (nx + R - 1) / R;
+    const long W = (long)ntiles * nz;
+    const long u0 = W * blockIdx.x / gridDim.x, u1 = W * (blockIdx.x + 1) / gridDim.x;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < TS_STAGES; ++s) mbar_init(smem_u32(&bars[s]), 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    uint32_t uses[TS_STAGES] = {0, 0, 0, 0};
+    const int nqr = ny >> 2;
+    // slot regions: v (R + 2 rows, row 0 = x0 - 1) | f (R) | ax (R + 1) | fyc (R) | az (R)
+    auto sv = [&](int p) { return sm + (size_t)(p % TS_STAGES) * stg; };
+    auto sf = [&](int p) { return sv(p) + (R + 2) * ny; };
+    auto sa = [&](int p) { return sf(p) + R * ny; };
+    auto sy = [&](int p) { return sa(p) + (R + 1) * ny; };
+    auto sz = [&](int p) { return sy(p) + R * ny; };
+    bool ok = true;
+    long u = u0;
+    while (u < u1 && ok) {
+        const int tile = (int)(u / nz);
+        const int zb = (int)(u - (long)tile * nz);
+        const int ze = (int)min((long)nz, zb + (u1 - u));
+        const int x0 = tile * R, rows = min(R, nx - x0);
+        const int plast = min(ze, nz - 1);
+        auto issue = [&](int p) {
+            const int s = p % TS_STAGES;
+            if (tid == 0) {
+                const uint32_t bar = smem_u32(&bars[s]);
+                const int xv0 = max(x0 - 1, 0), xv1 = min(x0 + rows + 1, nx), xa1 = min(x0 + rows + 1, nx + 1);
+                const uint32_t rb = (uint32_t)ny * 4u;
+                mbar_expect_tx(bar, rb * (uint32_t)((xv1 - xv0) + 3 * rows + (xa1 - x0)));
+                for (int x = xv0; x < xv1; ++x)
+                    bulk_load(smem_u32(sv(p) + (x - x0 + 1) * ny), src + (long)x * ny + p * sxy, rb, bar);
+                for (int r = 0; r < rows; ++r) {
+                    const long g = (long)(x0 + r) * ny + p * sxy;
+                    bulk_load(smem_u32(sf(p) + r * ny), f + g, rb, bar);
+                    bulk_load(smem_u32(sy(p) + r * ny), L.fyc + g, rb, bar);
+                    bulk_load(smem_u32(sz(p) + r * ny), L.az + g, rb, bar);
+                }
+                for (int x = x0; x < xa1; ++x)
+                    bulk_load(smem_u32(sa(p) + (x - x0) * ny), L.ax + (long)x * ny + p * sax, rb, bar);
+            }
+            uses[s] += 1;
+        };
+        auto wait = [&](int p) {
+            return mbar_wait(smem_u32(&bars[p % TS_STAGES]), (uses[p % TS_STAGES] - 1) & 1, err);
+        };
+        for (int p = max(zb - 1, 0); p <= min(plast, zb + 2); ++p) issue(p);
+        if (zb > 0) ok = wait(zb - 1) && ok;
+        ok = wait(zb) && ok;
+        for (int z = zb; z < ze; ++z) {
+            const bool zp = z < nz - 1;
+            if (zp) ok = wait(z + 1) && ok;
+            if (!__syncthreads_and(ok)) {
+                ok = false;
+                break;
+            }
+            const float* vm = sv(z > 0 ? z - 1 : z);
+            const float* vc = sv(z);
+            const float* vp = sv(zp ? z + 1 : z);
+            const float* fz = sf(z);
+            const float* ax = sa(z);
+            const float* fy = sy(z);
+            const float* azl = sz(z);
+            const float* azu = sz(zp ? z + 1 : z);
+            const float gzl = L.glo[2][z], gzh = L.ghi[2][z];
+            for (int q = tid; q < rows * nqr; q += TS_THREADS) {
+                const int r = q / nqr, y0 = (q - r * nqr) * 4;
+                const int x = x0 + r;
+                const int o = r * ny + y0;         // row r of the f / fyc / az / lower-ax regions
+                const int oc = (r + 1) * ny + y0;  // the cell's row in the v region
+                const Q4<float> c = ld4(vc + oc);
+                const Q4<float> vxm = ld4(vc + oc - ny), vxp = ld4(vc + oc + ny);
+                const Q4<float> vzm = ld4(vm + oc), vzp = ld4(vp + oc);
+                const Q4<float> fv = ld4(fz + o);
+                const Q4<float> fyl = ld4(fy + o), fxl = ld4(ax + o), fxu = ld4(ax + o + ny);
+                const Q4<float> al = ld4(azl + o), au = ld4(azu + o);
+                const bool ym = y0 > 0, yp = y0 + 4 < ny, xm = x > 0, xp = x < nx - 1;
+                const float vym = ym ? vc[oc - 1] : 0.f, vyp = yp ? vc[oc + 4] : 0.f;
+                const float fyu = yp ? fy[o + 4] : 0.f;
+                const float gxl = L.glo[0][x], gxh = L.ghi[0][x];
+                Q4<float> out;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int y = y0 + k;
+                    float d = 0.f, od = 0.f, cf;
+                    if (y > 0) { cf = fyl.a[k] * L.glo[1][y]; d += cf; od -= cf * (k > 0 ? c.a[k - 1] : vym); }
+                    if (y < ny - 1) { cf = (k < 3 ? fyl.a[k + 1] : fyu) * L.ghi[1][y]; d += cf; od -= cf * (k < 3 ? c.a[k + 1] : vyp); }
+                    if (xm) { cf = fxl.a[k] * gxl; d += cf; od -= cf * vxm.a[k]; }
+                    if (xp) { cf = fxu.a[k] * gxh; d += cf; od -= cf * vxp.a[k]; }
+                    if (z > 0) { cf = al.a[k] * gzl; d += cf; od -= cf * vzm.a[k]; }
+                    if (zp) { cf = au.a[k] * gzh; d += cf; od -= cf * vzp.a[k]; }
+                    out.a[k] = d > (float)kEps ? (1.f - w) * c.a[k] + w * (fv.a[k] - od) / d : 0.f;
+                }
+                st4(dst + y0 + (long)x * ny + z * sxy, out);
+            }
+            __syncthreads();
+            if (z + 3 <= plast) issue(z + 3);
+        }
+        u += ze - zb;
+    }
+    if (!ok && tid == 0) {
+        // a wait gave up: let the copies still in flight land before the CTA's shared memory goes
+        for (int s = 0; s < TS_STAGES; ++s)
+            if (uses[s]) mbar_wait(smem_u32(&bars[s]), (uses[s] - 1) & 1, err);
+    }
 }
 
 // Fused residual + restriction on quads: lanes 2k and 2k+1 own the fine rows x0 = 2 cx and x0 + 1 of
@@ -1057,7 +1196,8 @@ struct Level {
                       // defect64); 0 = heuristic, set by wp_mgfrac3d_autotune
     float zc_ms[3];   // the autotuner's median time of the chosen chunk (0 = not tuned)
     int var[3];       // kernel variant per kind (jacobi: 0 = default registers, 1/2 = >= 3/4 CTAs per SM,
-                      // 3 = two sweeps per launch)
+                      // 3 = two sweeps per launch, 4 = TMA-staged rows)
+    int* err;         // the handle's device error flag (bounded waits of the TMA-staged kernel)
 };
 
 enum { kZcJacobi = 0, kZcRestrict = 1, kZcDefect = 2 };
@@ -1129,6 +1269,23 @@ int level_zc(const Level& L, int kind) {
     return kind == kZcRestrict ? (zc + 1) / 2 : zc;
 }
 
+bool jacobi2_ok(const Level& L, const void* f) { return quad_ok(L) && al16(f) && L.n[2] >= 2; }
+
+// the TMA-staged sweep: 3D levels with y rows of 16-byte multiples, aligned arrays
+bool jacobi_ts_ok(const Level& L, const void* dst, const void* src, const void* f) {
+    return quad_ok(L) && L.n[2] >= 2 && L.err && al16(dst) && al16(src) && al16(f) &&
+           (size_t)ts_stage_floats(1, L.n[1]) * 4 * TS_STAGES <= 200 * 1024;
+}
+
+void launch_jacobi_ts(const Level& L, float* dst, const float* src, const float* f, float w, cudaStream_t s) {
+    const int R = ts_rows(L.n[0], L.n[1]);
+    const size_t smem = (size_t)ts_stage_floats(R, L.n[1]) * 4 * TS_STAGES;
+    if (wp_set_smem(jacobi_ts_kernel, smem) != cudaSuccess) return;
+    const long W = (long)((L.n[0] + R - 1) / R) * L.n[2];
+    const int grid = (int)std::min<long>(W, wp_sm_count());
+    jacobi_ts_kernel<<<grid, TS_THREADS, smem, s>>>(dst, src, f, view<float>(L), w, R, L.err);
+}
+
 // one weighted-Jacobi sweep dst <- J(src) of level L
 template <typename T>
 void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc, cudaStream_t s) {
@@ -1136,6 +1293,10 @@ void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc
     if (quad_ok(L) && al16(dst) && al16(src) && al16(f)) {
         const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
         const int var = sizeof(T) == 4 ? L.var[kZcJacobi] : 0;
+        if (var == 4 && jacobi_ts_ok(L, dst, src, f)) {
+            launch_jacobi_ts(L, (float*)dst, (const float*)src, (const float*)f, (float)w, s);
+            return;
+        }
         if (var == 1) jacobi_q_mb_kernel<T, 3><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
         else if (var == 2) jacobi_q_mb_kernel<T, 4><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
         else jacobi_q_kernel<T><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
@@ -1145,7 +1306,6 @@ void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc
     }
 }
 
-bool jacobi2_ok(const Level& L, const void* f) { return quad_ok(L) && al16(f) && L.n[2] >= 2; }
 
 // two sweeps dst <- J(J(src)) in one pass (jacobi2_q_kernel)
 template <typename T>
@@ -1483,7 +1643,11 @@ wp_status create_common(wp_mgfrac3d** out, int dims, const float* ax, const floa
     h->coarsest_iters = dims == 3 ? 50 : 10;
     wp_status st = build_hierarchy(h, ax, ay, az, nx, ny, nz, dx, dy, dz, s);
     if (st == WP_OK) {
-        cudaError_t e = cudaMalloc((void**)&h->acc, 4 * sizeof(double));
+        cudaError_t e = cudaMalloc((void**)&h->acc, 4 * sizeof(double) + 16);
+        // the int error flag lives in the 16 bytes after the four FP64 slots
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->acc, 0, 4 * sizeof(double) + 16, s);
+        if (e == cudaSuccess)
+            for (int l = 0; l < h->nl; ++l) h->lv[l].err = reinterpret_cast<int*>(h->acc + 4);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { wp_set_cuda_error(e, "mg create", __FILE__, __LINE__); st = WP_ERR_CUDA; }
     }
@@ -1820,15 +1984,19 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             const long floor_blocks = std::min<long>(most, 2L * wp_sm_count());
             void* fl = L.cells > kL2Cells ? flush : nullptr;
             // jacobi variants: 0-2 one sweep per launch (register budgets), 3 two sweeps per launch
-            const int nvar = (kind == kZcJacobi && quad_ok(L)) ? (jacobi2_ok(L, L.f) ? 4 : 3) : 1;
+            const int nvar = (kind == kZcJacobi && quad_ok(L)) ? 5 : 1;
             for (int var = 0; var < nvar && st == WP_OK; ++var) {
+                if (var == 3 && !jacobi2_ok(L, L.f)) continue;
+                if (var == 4 && !jacobi_ts_ok(L, L.t, L.v, L.f)) continue;
                 L.var[kind] = var;
                 for (int zc : zc_candidates(planes)) {
+                    // the TMA-staged sweep balances its own work over persistent CTAs: one timing
+                    if (var == 4 && zc != 1) continue;
                     long blocks = grid_blocks(L, C, kind, zc);
                     if (var == 3)
                         blocks = (long)((L.n[1] / 4 + J2_Q - 1) / J2_Q) * ((L.n[0] + J2_R - 1) / J2_R) *
                                  wp_cdiv(L.n[2], zc);
-                    if (blocks < floor_blocks) continue;
+                    if (var != 4 && blocks < floor_blocks) continue;
                     auto launch = [&]() {
                         if (kind == kZcJacobi && var == 3) launch_jacobi2<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
                         else if (kind == kZcJacobi) launch_jacobi<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
@@ -1885,7 +2053,7 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc,
 // Pins the chunk and kernel variant of one level's column kernel (kind 0 jacobi, 1 restrict,
 // 2 defect); zc <= 0 restores the heuristic.
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant) {
-    if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 3 ||
+    if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 4 ||
         (variant != 0 && kind != kZcJacobi)) {
         wp_set_error_msg("wp_mgfrac3d_set_tile: bad arguments");
         return WP_ERR_INVALID_ARG;
