@@ -152,6 +152,9 @@ def run_ours(args, rank, world, local_rank):
     q = [torch.zeros(s[k], device=dev) for k in ("qx", "qy", "qz")]
     proj = api.Projector3D(*a, nn, h, rel_tol=args.tol, max_cycles=80, nu1=2, nu2=2, weight=2.0 / 3.0,
                            precision=api.PREC_MIXED, prolongation=api.PROLONG_TRILINEAR)
+    if args.pin_jacobi >= 0:
+        zc = proj.mg.Tiles()[0][0]
+        proj.mg.SetTile(0, 0, zc, args.pin_jacobi)
     stream = torch.cuda.current_stream()
 
     def step():
@@ -538,6 +541,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pin-jacobi", type=int, default=-1,
+                    help="diagnostic: pin the finest-level Jacobi kernel variant (0-4) after autotuning")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "warmstart"],

@@ -890,15 +890,35 @@ __device__ __forceinline__ void cc_prolong(T* __restrict__ v, const T* __restric
     }
 }
 
-// V-cycle of the pack's levels; level 0 of the pack has its f and a zeroed v on entry
+// V-cycle of the pack's levels; level 0 of the pack has its f and a zeroed v on entry.  Every level's
+// v, t and f live in shared memory for the whole cycle (at most kCoarseSmemCells cells in all); the
+// face fractions and tables are read through L1.  On exit the finest pack level's v is written to
+// the global buffer the host will hold as that level's v after mirroring the nu1 + nu2 swaps.
+constexpr int kCoarseSmemCells = 4800;
+
 template <typename T>
 __global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1, int nu2, T w, int citers,
                                                             int prolong) {
+    extern __shared__ __align__(16) unsigned char cc_smem[];
+    T* base = reinterpret_cast<T*>(cc_smem);
     T* v[kCoarseMax];
     T* t[kCoarseMax];
-    for (int l = 0; l < P.n; ++l) {
-        v[l] = P.lv[l].v;
-        t[l] = P.lv[l].t;
+    T* fs[kCoarseMax];
+    {
+        int off = 0;
+        for (int l = 0; l < P.n; ++l) {
+            const int n = P.lv[l].L.nx * P.lv[l].L.ny * P.lv[l].L.nz;
+            v[l] = base + off;
+            t[l] = base + off + n;
+            fs[l] = base + off + 2 * n;
+            off += 3 * n;
+        }
+        const int n0 = P.lv[0].L.nx * P.lv[0].L.ny * P.lv[0].L.nz;
+        for (int i = threadIdx.x; i < n0; i += blockDim.x) {
+            fs[0][i] = P.lv[0].f[i];
+            v[0][i] = (T)0;
+        }
+        __syncthreads();
     }
     for (int l = 0; l < P.n - 1; ++l) {
         const Lvl<T>& L = P.lv[l].L;
@@ -908,14 +928,14 @@ __global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1,
             __syncthreads();
         }
         for (int k = 0; k < nu1; ++k) {
-            cc_sweep<T>(L, t[l], v[l], P.lv[l].f, w);
+            cc_sweep<T>(L, t[l], v[l], fs[l], w);
             __syncthreads();
             T* tmp = v[l];
             v[l] = t[l];
             t[l] = tmp;
         }
         const Lvl<T>& C = P.lv[l + 1].L;
-        cc_restrict<T>(L, v[l], P.lv[l].f, P.lv[l + 1].f, C.nx, C.ny, C.nz);
+        cc_restrict<T>(L, v[l], fs[l], fs[l + 1], C.nx, C.ny, C.nz);
         __syncthreads();
     }
     {
@@ -930,7 +950,7 @@ __global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1,
             // a coarsest grid of a few cells: one warp iterates alone (warp barriers only)
             if (threadIdx.x < 32) {
                 for (int k = 0; k < citers; ++k) {
-                    cc_sweep_warp<T>(L, t[l], v[l], P.lv[l].f, w);
+                    cc_sweep_warp<T>(L, t[l], v[l], fs[l], w);
                     __syncwarp();
                     T* tmp = v[l];
                     v[l] = t[l];
@@ -946,7 +966,7 @@ __global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1,
             __syncthreads();
         } else {
             for (int k = 0; k < citers; ++k) {
-                cc_sweep<T>(L, t[l], v[l], P.lv[l].f, w);
+                cc_sweep<T>(L, t[l], v[l], fs[l], w);
                 __syncthreads();
                 T* tmp = v[l];
                 v[l] = t[l];
@@ -960,13 +980,16 @@ __global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1,
         cc_prolong<T>(v[l], v[l + 1], L.nx, L.ny, L.nz, C.nx, C.ny, C.nz, prolong);
         __syncthreads();
         for (int k = 0; k < nu2; ++k) {
-            cc_sweep<T>(L, t[l], v[l], P.lv[l].f, w);
+            cc_sweep<T>(L, t[l], v[l], fs[l], w);
             __syncthreads();
             T* tmp = v[l];
             v[l] = t[l];
             t[l] = tmp;
         }
     }
+    T* out = ((nu1 + nu2) & 1) ? P.lv[0].t : P.lv[0].v;
+    const int n0 = P.lv[0].L.nx * P.lv[0].L.ny * P.lv[0].L.nz;
+    for (int i = threadIdx.x; i < n0; i += blockDim.x) out[i] = v[0][i];
 }
 
 // coarse f = spacing-weighted average of the fine residuals of the (up to 8) children
@@ -1498,8 +1521,13 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
     Level& L = h->lv[l];
     const dim3 g = grid_of(L.n[0], L.n[1], L.n[2]);
     wp_status st;
-    if (l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax && f == Bufs<T>::f(L)) {
+    long pack_cells = 0;
+    for (int k = l; k < h->nl; ++k) pack_cells += h->lv[k].cells;
+    if (l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax && f == Bufs<T>::f(L) &&
+        pack_cells <= kCoarseSmemCells) {
         // the rest of the cycle in one launch; the host mirrors the buffer swaps it performs
+        const size_t smem_max = 3 * sizeof(T) * (size_t)kCoarseSmemCells;
+        WP_CUDA_TRY(wp_set_smem(coarse_cycle_kernel<T>, smem_max));
         CPack<T> P;
         P.n = h->nl - l;
         for (int k = 0; k < P.n; ++k) {
@@ -1510,7 +1538,8 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
             P.lv[k].f = Bufs<T>::f(Q);
         }
         WP_KERNEL("coarse_cycle", (double)L.cells * (3.0 * sizeof(T) + 12.0) * (nu1 + nu2 + 2), s,
-                  coarse_cycle_kernel<T><<<1, 1024, 0, s>>>(P, nu1, nu2, w, h->coarsest_iters, prolong));
+                  coarse_cycle_kernel<T><<<1, 1024, 3 * sizeof(T) * pack_cells, s>>>(P, nu1, nu2, w,
+                                                                                      h->coarsest_iters, prolong));
         for (int k = 0; k < P.n; ++k) {
             Level& Q = h->lv[l + k];
             const int swaps = (k == P.n - 1) ? h->coarsest_iters : nu1 + nu2;
