@@ -415,13 +415,14 @@ constexpr int TS_THREADS = 256;
 
 __host__ __device__ inline int ts_stage_floats(int R, int ny) { return (5 * R + 3) * ny; }
 
-// rows per tile so that four slots fit in 200 KB of shared memory
+// rows per tile so that four slots fit in 100 KB of shared memory (two CTAs per SM)
 inline int ts_rows(int nx, int ny) {
-    int r = ((200 * 1024) / (4 * TS_STAGES * ny) - 3) / 5;
+    int r = ((100 * 1024) / (4 * TS_STAGES * ny) - 3) / 5;
     return std::max(1, std::min(r, nx));
 }
+inline size_t ts_smem_bytes(int R, int ny) { return ((size_t)ts_stage_floats(R, ny) * TS_STAGES + 2 * ny) * 4; }
 
-__global__ void __launch_bounds__(TS_THREADS, 1)
+__global__ void __launch_bounds__(TS_THREADS, 2)
     jacobi_ts_kernel(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ f,
                      Lvl<float> L, float w, int R, int* err) {
     using namespace wptc;
@@ -434,7 +435,14 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     const int ntiles = (nx + R - 1) / R;
     const long W = (long)ntiles * nz;
     const long u0 = W * blockIdx.x / gridDim.x, u1 = W * (blockIdx.x + 1) / gridDim.x;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // y-face geometry of the level, read once per CTA
+    float* gyl = sm + (size_t)TS_STAGES * stg;
+    float* gyh = gyl + ny;
+    for (int y = tid; y < ny; y += TS_THREADS) {
+        gyl[y] = L.glo[1][y];
+        gyh[y] = L.ghi[1][y];
+    }
     if (tid == 0) {
         for (int s = 0; s < TS_STAGES; ++s) mbar_init(smem_u32(&bars[s]), 1);
         mbar_init_fence();
@@ -456,23 +464,35 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
         const int ze = (int)min((long)nz, zb + (u1 - u));
         const int x0 = tile * R, rows = min(R, nx - x0);
         const int plast = min(ze, nz - 1);
+        // warp 0 issues the plane's row copies, one per lane, after lane 0 posted the byte count
         auto issue = [&](int p) {
             const int s = p % TS_STAGES;
-            if (tid == 0) {
+            if (warp == 0) {
                 const uint32_t bar = smem_u32(&bars[s]);
                 const int xv0 = max(x0 - 1, 0), xv1 = min(x0 + rows + 1, nx), xa1 = min(x0 + rows + 1, nx + 1);
+                const int nv = xv1 - xv0, ncp = nv + 3 * rows + (xa1 - x0);
                 const uint32_t rb = (uint32_t)ny * 4u;
-                mbar_expect_tx(bar, rb * (uint32_t)((xv1 - xv0) + 3 * rows + (xa1 - x0)));
-                for (int x = xv0; x < xv1; ++x)
-                    bulk_load(smem_u32(sv(p) + (x - x0 + 1) * ny), src + (long)x * ny + p * sxy, rb, bar);
-                for (int r = 0; r < rows; ++r) {
-                    const long g = (long)(x0 + r) * ny + p * sxy;
-                    bulk_load(smem_u32(sf(p) + r * ny), f + g, rb, bar);
-                    bulk_load(smem_u32(sy(p) + r * ny), L.fyc + g, rb, bar);
-                    bulk_load(smem_u32(sz(p) + r * ny), L.az + g, rb, bar);
+                if (lane == 0) mbar_expect_tx(bar, rb * (uint32_t)ncp);
+                __syncwarp();
+                for (int j = lane; j < ncp; j += 32) {
+                    const float* g;
+                    float* d;
+                    if (j < nv) {
+                        const int x = xv0 + j;
+                        g = src + (long)x * ny + p * sxy;
+                        d = sv(p) + (x - x0 + 1) * ny;
+                    } else if (j < nv + 3 * rows) {
+                        const int k = (j - nv) / rows, r = (j - nv) - k * rows;
+                        const long o = (long)(x0 + r) * ny + p * sxy;
+                        g = k == 0 ? f + o : k == 1 ? L.fyc + o : L.az + o;
+                        d = (k == 0 ? sf(p) : k == 1 ? sy(p) : sz(p)) + r * ny;
+                    } else {
+                        const int x = x0 + (j - nv - 3 * rows);
+                        g = L.ax + (long)x * ny + p * sax;
+                        d = sa(p) + (x - x0) * ny;
+                    }
+                    bulk_load(smem_u32(d), g, rb, bar);
                 }
-                for (int x = x0; x < xa1; ++x)
-                    bulk_load(smem_u32(sa(p) + (x - x0) * ny), L.ax + (long)x * ny + p * sax, rb, bar);
             }
             uses[s] += 1;
         };
@@ -518,8 +538,8 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
                 for (int k = 0; k < 4; ++k) {
                     const int y = y0 + k;
                     float d = 0.f, od = 0.f, cf;
-                    if (y > 0) { cf = fyl.a[k] * L.glo[1][y]; d += cf; od -= cf * (k > 0 ? c.a[k - 1] : vym); }
-                    if (y < ny - 1) { cf = (k < 3 ? fyl.a[k + 1] : fyu) * L.ghi[1][y]; d += cf; od -= cf * (k < 3 ? c.a[k + 1] : vyp); }
+                    if (y > 0) { cf = fyl.a[k] * gyl[y]; d += cf; od -= cf * (k > 0 ? c.a[k - 1] : vym); }
+                    if (y < ny - 1) { cf = (k < 3 ? fyl.a[k + 1] : fyu) * gyh[y]; d += cf; od -= cf * (k < 3 ? c.a[k + 1] : vyp); }
                     if (xm) { cf = fxl.a[k] * gxl; d += cf; od -= cf * vxm.a[k]; }
                     if (xp) { cf = fxu.a[k] * gxh; d += cf; od -= cf * vxp.a[k]; }
                     if (z > 0) { cf = al.a[k] * gzl; d += cf; od -= cf * vzm.a[k]; }
@@ -1297,15 +1317,15 @@ bool jacobi2_ok(const Level& L, const void* f) { return quad_ok(L) && al16(f) &&
 // the TMA-staged sweep: 3D levels with y rows of 16-byte multiples, aligned arrays
 bool jacobi_ts_ok(const Level& L, const void* dst, const void* src, const void* f) {
     return quad_ok(L) && L.n[2] >= 2 && L.err && al16(dst) && al16(src) && al16(f) &&
-           (size_t)ts_stage_floats(1, L.n[1]) * 4 * TS_STAGES <= 200 * 1024;
+           ts_smem_bytes(1, L.n[1]) <= 110 * 1024;
 }
 
 void launch_jacobi_ts(const Level& L, float* dst, const float* src, const float* f, float w, cudaStream_t s) {
     const int R = ts_rows(L.n[0], L.n[1]);
-    const size_t smem = (size_t)ts_stage_floats(R, L.n[1]) * 4 * TS_STAGES;
+    const size_t smem = ts_smem_bytes(R, L.n[1]);
     if (wp_set_smem(jacobi_ts_kernel, smem) != cudaSuccess) return;
     const long W = (long)((L.n[0] + R - 1) / R) * L.n[2];
-    const int grid = (int)std::min<long>(W, wp_sm_count());
+    const int grid = (int)std::min<long>(W, 2L * wp_sm_count());
     jacobi_ts_kernel<<<grid, TS_THREADS, smem, s>>>(dst, src, f, view<float>(L), w, R, L.err);
 }
 
