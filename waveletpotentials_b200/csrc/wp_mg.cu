@@ -685,24 +685,53 @@ __global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, c
     if (qx < 0 || qx >= ncx) qx = px;
     if (qz < 0 || qz >= ncz) qz = pz;
     const long sc = (long)ncx * ncy;
-    auto C = [&](int xx, int yy, int zz) -> T { return vc[yy + (long)xx * ncy + zz * sc]; };
     const T a = (T)0.75, b = (T)0.25;
     const long i = y0 + (long)x * ny + (long)z * nx * ny;
     Q4<T> out = ld4(v + i);
+    // the quad's coarse y values along one coarse (x, z) row: cy0 - 1, cy0, cy0 + 1, cy0 + 2, with the
+    // wall neighbour repeating the parent (ny % 4 == 0, so ncy = ny / 2 and cy0 = y0 / 2 is even)
+    const int cy0 = y0 >> 1;
+    struct Row4 {
+        T m, a, b, p;
+    };
+    auto row4 = [&](int xx, int zz) -> Row4 {
+        const T* r = vc + cy0 + (long)xx * ncy + zz * sc;
+        Row4 o;
+        o.a = r[0];
+        o.b = r[1];
+        o.m = cy0 > 0 ? r[-1] : o.a;
+        o.p = cy0 + 2 < ncy ? r[2] : o.b;
+        return o;
+    };
+    // parent (P) and neighbour (Q) of cell k of the quad in a row
+    auto PQ = [&](const Row4& r, int k, T& P, T& Q) {
+        if (k == 0) { P = r.a; Q = r.m; }
+        else if (k == 1) { P = r.a; Q = r.b; }
+        else if (k == 2) { P = r.b; Q = r.a; }
+        else { P = r.b; Q = r.p; }
+    };
+    if (ncz == 1 && nz == 1) {
+        const Row4 r0 = row4(px, 0), r1 = row4(qx, 0);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int y = y0 + k, py = y >> 1;
-        int qy = (y & 1) ? py + 1 : py - 1;
-        if (qy < 0 || qy >= ncy) qy = py;
-        T acc;
-        if (ncz == 1 && nz == 1) {
-            acc = a * (a * C(px, py, 0) + b * C(px, qy, 0)) + b * (a * C(qx, py, 0) + b * C(qx, qy, 0));
-        } else {
-            const T lo = a * (a * C(px, py, pz) + b * C(px, qy, pz)) + b * (a * C(qx, py, pz) + b * C(qx, qy, pz));
-            const T hi = a * (a * C(px, py, qz) + b * C(px, qy, qz)) + b * (a * C(qx, py, qz) + b * C(qx, qy, qz));
-            acc = a * lo + b * hi;
+        for (int k = 0; k < 4; ++k) {
+            T P0, Q0, P1, Q1;
+            PQ(r0, k, P0, Q0);
+            PQ(r1, k, P1, Q1);
+            out.a[k] += a * (a * P0 + b * Q0) + b * (a * P1 + b * Q1);
         }
-        out.a[k] += acc;
+    } else {
+        const Row4 r00 = row4(px, pz), r10 = row4(qx, pz), r01 = row4(px, qz), r11 = row4(qx, qz);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            T P00, Q00, P10, Q10, P01, Q01, P11, Q11;
+            PQ(r00, k, P00, Q00);
+            PQ(r10, k, P10, Q10);
+            PQ(r01, k, P01, Q01);
+            PQ(r11, k, P11, Q11);
+            const T lo = a * (a * P00 + b * Q00) + b * (a * P10 + b * Q10);
+            const T hi = a * (a * P01 + b * Q01) + b * (a * P11 + b * Q11);
+            out.a[k] += a * lo + b * hi;
+        }
     }
     st4(v + i, out);
 }
