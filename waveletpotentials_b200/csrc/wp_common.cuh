@@ -47,6 +47,9 @@ int wp_prof_start(cudaStream_t s);
 // capture time; a replay adds them again).
 void wp_add_launches(long long n);
 bool wp_profile_is_enabled();
+template <typename T>
+wp_status wp_dwt_axis_tune(T* buf, int DX, int DY, int DZ, int levels, char axis, int wavelet, char bc, int forward,
+                           cudaStream_t s);
 // Uploads the wavelet filter tables to the current device (once; synchronous).
 cudaError_t wp_dwt_prepare();
 void wp_prof_stop(int tok, const char* name, double bytes, cudaStream_t s);

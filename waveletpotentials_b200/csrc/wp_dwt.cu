@@ -17,8 +17,12 @@
 #include "wp_common.cuh"
 
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
+#include <vector>
 
 namespace {
 
@@ -404,9 +408,25 @@ cudaError_t launch_one(const T* src, T* dst, int N, int levels, int bcd, TileGeo
     return e;
 }
 
+// Tile widths chosen by the autotuner, per (device, wavelet, direction, precision, line length,
+// lines, outer extent, axis kind); a width changes only the grid, never a result.
+std::mutex g_c_mu;
+std::map<std::tuple<int, int, int, int, int, int, int, int>, int> g_c_cache;
+
+std::tuple<int, int, int, int, int, int, int, int> c_key(int wav, bool fwd, int tsize, int N, const TileGeom& g,
+                                                         int nouter) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return std::make_tuple(dev, wav, fwd ? 1 : 0, tsize, N, g.ni, nouter, g.contiguous);
+}
+
+// -1: let launch_c decide (cache, then heuristic); otherwise force this tile width
+thread_local int t_force_c = -1;
+
 template <int WAV, bool FWD, typename T>
 cudaError_t launch_c(const T* src, T* dst, int N, int levels, int bcd, TileGeom g, int nouter, cudaStream_t s) {
-    // widest tile whose staging fits ~100 KB (two CTAs per SM) while keeping >= 2 CTAs per SM busy
+    // widest tile whose staging fits ~100 KB (two CTAs per SM) while keeping >= 2 CTAs per SM busy,
+    // unless the autotuner measured another width for this shape
     const int nbuf = FWD ? 2 : 3;
     int C = 32;
     const long sms = wp_sm_count();
@@ -415,6 +435,13 @@ cudaError_t launch_c(const T* src, T* dst, int N, int levels, int bcd, TileGeom 
         const long ctas = (long)((g.ni + C - 1) / C) * nouter;
         if (smem <= 100 * 1024 && ctas >= 2 * sms) break;
         C >>= 1;
+    }
+    if (t_force_c > 0) {
+        C = t_force_c;
+    } else {
+        std::lock_guard<std::mutex> lk(g_c_mu);
+        auto it = g_c_cache.find(c_key(WAV, FWD, (int)sizeof(T), N, g, nouter));
+        if (it != g_c_cache.end()) C = it->second;
     }
     const size_t smem = (size_t)nbuf * N * (C + 1) * sizeof(T);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
@@ -462,6 +489,59 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
     if (e != cudaSuccess) { wp_set_cuda_error(e, "dwt launch", __FILE__, __LINE__); return WP_ERR_CUDA; }
     return WP_OK;
 }
+
+// Times the pass over the tile widths 4..32 that fit shared memory (median of three single launches,
+// in place on buf) and records the fastest for this shape.  Synchronous; buf's contents are
+// overwritten.
+template <typename T>
+wp_status wp_dwt_axis_tune(T* buf, int DX, int DY, int DZ, int levels, char axis, int wavelet, char bc, int forward,
+                           cudaStream_t s) {
+    const int N = (axis == 'y' || axis == 'Y') ? DY : (axis == 'x' || axis == 'X') ? DX : DZ;
+    cudaEvent_t a, b;
+    WP_CUDA_TRY(cudaEventCreate(&a));
+    WP_CUDA_TRY(cudaEventCreate(&b));
+    float best = 1e30f;
+    int best_c = -1;
+    wp_status st = WP_OK;
+    const int nbuf = forward ? 2 : 3;
+    for (int C = 4; C <= 32 && st == WP_OK; C *= 2) {
+        if ((size_t)nbuf * N * (C + 1) * sizeof(T) > 227 * 1024) break;
+        t_force_c = C;
+        std::vector<float> t;
+        for (int r = 0; r < 4 && st == WP_OK; ++r) {
+            cudaEventRecord(a, s);
+            st = wp_dwt_axis_launch<T>(buf, buf, DX, DY, DZ, levels, axis, wavelet, bc, forward, s);
+            cudaEventRecord(b, s);
+            cudaEventSynchronize(b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (r > 0) t.push_back(ms);
+        }
+        t_force_c = -1;
+        if (st != WP_OK) break;
+        std::sort(t.begin(), t.end());
+        if (t[1] < best) {
+            best = t[1];
+            best_c = C;
+        }
+    }
+    t_force_c = -1;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (st != WP_OK || best_c < 0) return st;
+    TileGeom g;
+    int nouter;
+    switch (axis) {
+        case 'y': case 'Y': g.ni = DX; nouter = DZ; g.contiguous = 1; break;
+        case 'x': case 'X': g.ni = DY; nouter = DZ; g.contiguous = 0; break;
+        default: g.ni = DY; nouter = DX; g.contiguous = 0; break;
+    }
+    const int wav = wavelet == WP_ID_CDF3_7 ? WP_ID_CDF3_7 : WP_ID_CDF4_6;
+    std::lock_guard<std::mutex> lk(g_c_mu);
+    g_c_cache[c_key(wav, forward != 0, (int)sizeof(T), N, g, nouter)] = best_c;
+    return WP_OK;
+}
+template wp_status wp_dwt_axis_tune<float>(float*, int, int, int, int, char, int, char, int, cudaStream_t);
 
 template wp_status wp_dwt_axis_launch<float>(float*, const float*, int, int, int, int, char, int, char, int, cudaStream_t);
 template wp_status wp_dwt_axis_launch<double>(double*, const double*, int, int, int, int, char, int, char, int,

@@ -184,6 +184,31 @@ extern "C" CUWHHD_API wp_status wp_recover3d_create(wp_recover3d** out, int nx, 
         cudaError_t e = cudaMalloc((void**)&h->tmp[a], sizeof(float) * sz[a]);
         if (e != cudaSuccess) { wp_set_cuda_error(e, "recover3d temp", __FILE__, __LINE__); wp_recover3d_destroy(h); return WP_ERR_CUDA; }
     }
+    // tile widths of the 18 passes, measured once per shape for the process (on a scratch array
+    // as large as the largest potential component)
+    {
+        float* scratch = nullptr;
+        const size_t big = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+        if (cudaMalloc((void**)&scratch, sizeof(float) * big) == cudaSuccess) {
+            cudaMemset(scratch, 0, sizeof(float) * big);
+            const int C = WP_ID_CDF3_7, V = WP_ID_CDF4_6;
+            const int Lx = h->L[0], Ly = h->L[1], Lz = h->L[2];
+            struct P { int dx, dy, dz, L; char ax; int w; char bc; int f; };
+            const P passes[18] = {
+                {nx + 1, ny, nz, Lx, 'x', V, 'd', 1}, {nx + 1, ny, nz, Ly, 'y', C, 'n', 1}, {nx + 1, ny, nz, Lz, 'z', C, 'n', 1},
+                {nx, ny + 1, nz, Lx, 'x', C, 'n', 1}, {nx, ny + 1, nz, Ly, 'y', V, 'd', 1}, {nx, ny + 1, nz, Lz, 'z', C, 'n', 1},
+                {nx, ny, nz + 1, Lx, 'x', C, 'n', 1}, {nx, ny, nz + 1, Ly, 'y', C, 'n', 1}, {nx, ny, nz + 1, Lz, 'z', V, 'd', 1},
+                {nx, ny + 1, nz + 1, Lx, 'x', C, 'n', 0}, {nx, ny + 1, nz + 1, Ly, 'y', V, 'd', 0}, {nx, ny + 1, nz + 1, Lz, 'z', V, 'd', 0},
+                {nx + 1, ny, nz + 1, Lx, 'x', V, 'd', 0}, {nx + 1, ny, nz + 1, Ly, 'y', C, 'n', 0}, {nx + 1, ny, nz + 1, Lz, 'z', V, 'd', 0},
+                {nx + 1, ny + 1, nz, Lx, 'x', V, 'd', 0}, {nx + 1, ny + 1, nz, Ly, 'y', V, 'd', 0}, {nx + 1, ny + 1, nz, Lz, 'z', C, 'n', 0}};
+            for (const P& q : passes)
+                if (wp_dwt_axis_tune<float>(scratch, q.dx, q.dy, q.dz, q.L, q.ax, q.w, q.bc, q.f, nullptr) != WP_OK) break;
+            cudaDeviceSynchronize();
+            cudaFree(scratch);
+        } else {
+            cudaGetLastError();
+        }
+    }
     *out = h;
     return WP_OK;
 }
