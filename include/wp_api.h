@@ -110,6 +110,11 @@ CUWHHD_API wp_status wp_recover2d_destroy(wp_recover2d* h);
 /* coarse-to-fine transfer of the V-cycle */
 #define WP_PROLONG_CONSTANT 0  /* the reference's piecewise-constant prolongation (cuProlongate3D.cu:594-617) */
 #define WP_PROLONG_TRILINEAR 1 /* cell-centred trilinear: h-independent convergence for V(2,2), omega 2/3 */
+/* first iterate of the tolerance-driven solve: zero, or a full-multigrid start (the right-hand side
+   restricted to every level, the coarsest solved, then prolongation + one V-cycle per finer level),
+   which costs about two V-cycles of work and counts as one cycle in the report */
+#define WP_START_ZERO 0
+#define WP_START_FMG 1
 
 typedef struct wp_mg_params {
     int max_cycles;   /* cap on V-cycles (or refinement steps) */
@@ -118,6 +123,7 @@ typedef struct wp_mg_params {
     double rel_tol;   /* stop when ||f - A p|| / ||f|| <= rel_tol; <= 0 runs exactly max_cycles */
     int precision;    /* WP_PREC_FP32 | WP_PREC_MIXED | WP_PREC_FP64 */
     int prolongation; /* WP_PROLONG_CONSTANT | WP_PROLONG_TRILINEAR */
+    int start;        /* WP_START_ZERO | WP_START_FMG (ignored when an initial iterate is given) */
 } wp_mg_params;
 
 typedef struct wp_mg_report {

@@ -255,6 +255,27 @@ def test_mg3d_reaches_tolerance_checked_by_oracle(wp, oracle, precision, tol):
     assert orel <= tol * 1.5, (orel, rep)
 
 
+@pytest.mark.parametrize("precision,tol", [("fp32", 1e-6), ("mixed", 1e-10), ("fp64", 1e-10)])
+def test_mg3d_fmg_start_checked_by_oracle(wp, oracle, precision, tol):
+    """The full-multigrid start reaches the same tolerance (checked in FP64 by the oracle) in no more
+    cycles than the zero start; both the batch-style fixed-cycle path and the one-grid path use it."""
+    nn, h, a, _, f = _sphere_problem(wp, oracle, 64, seed=3)
+    mg = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)
+    prec = {"fp32": wp.PREC_FP32, "mixed": wp.PREC_MIXED, "fp64": wp.PREC_FP64}[precision]
+    dz = torch.zeros(f.shape, device="cuda")
+    rz = mg.SolveTol(dz, None, T(f), rel_tol=tol, max_cycles=60, precision=prec)
+    dst = torch.zeros(f.shape, device="cuda")
+    rep = mg.SolveTol(dst, None, T(f), rel_tol=tol, max_cycles=60, precision=prec, start=wp.START_FMG)
+    assert rep["rel_residual"] <= tol and rep["cycles"] <= rz["cycles"], (rep["cycles"], rz["cycles"])
+    assert rep["history"][0] < rz["history"][0]
+    act = active_cells(*a)
+    fc = f.copy()
+    fc[act] -= f[act].mean()
+    sol = N(dst) if precision == "fp32" else mg.Iterate64()
+    _, r = oracle.frac_residual3d(sol, fc, *a, nn, (h,) * 3)
+    assert np.linalg.norm(r) / np.linalg.norm(f) <= tol * 1.5
+
+
 def test_mg_not_converged_is_reported(wp, oracle):
     nn, h, a, _, f = _sphere_problem(wp, oracle, 32)
     mg = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)

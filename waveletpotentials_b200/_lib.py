@@ -19,6 +19,7 @@ CDF4_6 = 7
 CDF3_7 = 11
 PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
 PROLONG_CONSTANT, PROLONG_TRILINEAR = 0, 1
+START_ZERO, START_FMG = 0, 1
 
 
 class WPError(RuntimeError):
@@ -30,7 +31,7 @@ class WPError(RuntimeError):
 class MgParams(ctypes.Structure):
     _fields_ = [("max_cycles", ctypes.c_int), ("nu1", ctypes.c_int), ("nu2", ctypes.c_int),
                 ("omega", ctypes.c_double), ("rel_tol", ctypes.c_double), ("precision", ctypes.c_int),
-                ("prolongation", ctypes.c_int)]
+                ("prolongation", ctypes.c_int), ("start", ctypes.c_int)]
 
 
 class MgReport(ctypes.Structure):

@@ -15,6 +15,7 @@ import ctypes
 import torch
 
 from . import _lib
+from ._lib import START_FMG, START_ZERO  # noqa: F401
 from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONSTANT, PROLONG_TRILINEAR, MgParams, \
     MgReport, WPError, check, lib
 
@@ -23,7 +24,7 @@ __all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRe
            "Projector3D", "Projector2D", "BatchProjector", "max_abs", "conv3_forward", "conv3_wgrad",
            "random_field3d", "velocity3d_device", "UNetWarmStart", "warm_started_solve",
            "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
-           "PROLONG_TRILINEAR", "mac_shapes3d", "mac_shapes2d"]
+           "PROLONG_TRILINEAR", "START_ZERO", "START_FMG", "mac_shapes3d", "mac_shapes2d"]
 
 
 def mac_shapes3d(nx, ny, nz):
@@ -191,10 +192,11 @@ class CuMultigridFrac3D:
                                       int(nu2), float(weight), _stream(stream)), "wp_mgfrac3d_solve")
 
     def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, stream=None) -> dict:
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, start=START_ZERO,
+                 stream=None) -> dict:
         c = self.cells
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), int(precision),
-                       int(prolongation))
+                       int(prolongation), int(start))
         rep = MgReport()
         st = lib().wp_mgfrac3d_solve_tol(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), ctypes.byref(prm),
                                          ctypes.byref(rep), _stream(stream))
@@ -273,10 +275,11 @@ class CuMultigridFrac2D:
                                       int(nu2), float(weight), _stream(stream)), "wp_mgfrac2d_solve")
 
     def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, stream=None) -> dict:
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, start=START_ZERO,
+                 stream=None) -> dict:
         c = self.cells
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), int(precision),
-                       int(prolongation))
+                       int(prolongation), int(start))
         rep = MgReport()
         st = lib().wp_mgfrac2d_solve_tol(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), ctypes.byref(prm),
                                          ctypes.byref(rep), _stream(stream))
@@ -483,7 +486,7 @@ class Projector3D:
 
     def __init__(self, ax, ay, az, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
                  precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, autotune=True, warm_start=None, sdf=None,
-                 stream=None):
+                 start=START_ZERO, stream=None):
         self.dim = _dims3(dim)
         self.dx = _dx3(dx)
         self.ax, self.ay, self.az = ax, ay, az
@@ -495,7 +498,7 @@ class Projector3D:
             self.mg.Autotune(stream)
         self.rec = CuWaveletPotentialRecover3D(self.dim, self.dx, "n")
         self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
-                         prolongation=prolongation)
+                         prolongation=prolongation, start=start)
         s = mac_shapes3d(*self.dim)
         self.shapes = s
         self.b = torch.empty(s["p"], device="cuda", dtype=torch.float32)
@@ -523,14 +526,14 @@ class Projector2D:
     """2D form of Projector3D (CuMultigridFrac2D + CuWaveletPotentialRecover2D)."""
 
     def __init__(self, ax, ay, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, stream=None):
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, start=START_ZERO, stream=None):
         self.dim = tuple(int(v) for v in dim)
         self.dx = float(dx)
         self.ax, self.ay = ax, ay
         self.mg = CuMultigridFrac2D(ax, ay, self.dim, self.dx, "n", stream)
         self.rec = CuWaveletPotentialRecover2D(self.dim, self.dx, "n")
         self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
-                         prolongation=prolongation)
+                         prolongation=prolongation, start=start)
         s = mac_shapes2d(*self.dim)
         self.b = torch.empty(s["p"], device="cuda", dtype=torch.float32)
         self.p = torch.empty(s["p"], device="cuda", dtype=torch.float32)
@@ -562,7 +565,7 @@ class BatchProjector:
     """
 
     def __init__(self, grids, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 prolongation=PROLONG_TRILINEAR, nstreams=8):
+                 prolongation=PROLONG_TRILINEAR, nstreams=8, start=START_ZERO):
         self.grids = grids
         self.count = len(grids)
         dims, ext, dx, ax, ay, az = [], [], [], [], [], []
@@ -585,7 +588,7 @@ class BatchProjector:
             ay.append(_ptr(g["ay"], s["yv"], name="ay").value)
         self.dims = dims
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), PREC_MIXED,
-                       int(prolongation))
+                       int(prolongation), int(start))
         h = ctypes.c_void_p()
         self._keep = ((ctypes.c_int * self.count)(*dims), (ctypes.c_int * (3 * self.count))(*ext),
                       (ctypes.c_double * self.count)(*dx), _parray(ax), _parray(ay), _parray(az), prm)

@@ -1565,15 +1565,18 @@ wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s, bool fin
     return WP_OK;
 }
 
+// One V-cycle at level l from the level's current v (zero_start: v is known to be zero, which lets
+// the single-launch coarse cycle take over below kCoarseCells).
 template <typename T>
-wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int prolong, cudaStream_t s) {
+wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int prolong, cudaStream_t s,
+                 bool zero_start = true) {
     Level& L = h->lv[l];
     const dim3 g = grid_of(L.n[0], L.n[1], L.n[2]);
     wp_status st;
     long pack_cells = 0;
     for (int k = l; k < h->nl; ++k) pack_cells += h->lv[k].cells;
-    if (l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax && f == Bufs<T>::f(L) &&
-        pack_cells <= kCoarseSmemCells) {
+    if (zero_start && l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax &&
+        f == Bufs<T>::f(L) && pack_cells <= kCoarseSmemCells) {
         // the rest of the cycle in one launch; the host mirrors the buffer swaps it performs
         const size_t smem_max = 3 * sizeof(T) * (size_t)kCoarseSmemCells;
         WP_CUDA_TRY(wp_set_smem(coarse_cycle_kernel<T>, smem_max));
@@ -1639,6 +1642,40 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         } else {
             if ((st = smooth<T>(L, f, h->coarsest_iters, w, s)) != WP_OK) return st;
         }
+    }
+    return WP_OK;
+}
+
+// Full-multigrid start: the right-hand side restricted to every level (the residual restriction of
+// a zero iterate), the coarsest level solved from zero, then on each finer level the prolonged
+// coarser solution followed by one V-cycle.  Leaves the finest level's iterate in its v; costs
+// about one V-cycle more than a V-cycle and replaces the first cycles from a zero start.
+template <typename T>
+wp_status fmg_start(wp_mgfrac3d* h, const T* f0, int nu1, int nu2, T w, int prolong, cudaStream_t s) {
+    wp_status st;
+    for (int l = 0; l + 1 < h->nl; ++l) {
+        Level& L = h->lv[l];
+        Level& C = h->lv[l + 1];
+        const T* fl = l == 0 ? f0 : Bufs<T>::f(L);
+        WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(L), 0, sizeof(T) * L.cells, s));
+        WP_KERNEL("fmg_restrict", (double)L.cells * (2.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
+                  launch_resid_restrict<T>(L, C, Bufs<T>::f(C), Bufs<T>::v(L), fl, level_zc(L, kZcRestrict), s));
+    }
+    const int lc = h->nl - 1;
+    WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(h->lv[lc]), 0, sizeof(T) * h->lv[lc].cells, s));
+    if ((st = vcycle<T>(h, lc, lc == 0 ? f0 : Bufs<T>::f(h->lv[lc]), nu1, nu2, w, prolong, s)) != WP_OK) return st;
+    for (int l = lc - 1; l >= 0; --l) {
+        Level& L = h->lv[l];
+        Level& C = h->lv[l + 1];
+        WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(L), 0, sizeof(T) * L.cells, s));
+        if (prolong == WP_PROLONG_TRILINEAR)
+            WP_KERNEL("fmg_prolong", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
+                      launch_prolong_tri<T>(L, C, Bufs<T>::v(L), Bufs<T>::v(C), s));
+        else
+            WP_KERNEL("fmg_prolong", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
+                      prolong_add_kernel<T><<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(
+                          Bufs<T>::v(L), Bufs<T>::v(C), L.n[0], L.n[1], L.n[2], C.n[0], C.n[1]));
+        if ((st = vcycle<T>(h, l, l == 0 ? f0 : Bufs<T>::f(L), nu1, nu2, w, prolong, s, false)) != WP_OK) return st;
     }
     return WP_OK;
 }
@@ -1782,8 +1819,13 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
         if (!(nf2 > 0.0)) nf2 = 1.0;
         double rel = std::sqrt(nr2 / nf2);
         while (!(use_tol && rel <= prm->rel_tol) && r.cycles < prm->max_cycles) {
-            st = f64 ? vcycle<double>(h, 0, L.f64, prm->nu1, prm->nu2, prm->omega, prm->prolongation, s)
-                     : vcycle<float>(h, 0, f, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+            const bool fmg = r.cycles == 0 && !pre_v && prm->start == WP_START_FMG;
+            if (fmg)
+                st = f64 ? fmg_start<double>(h, L.f64, prm->nu1, prm->nu2, prm->omega, prm->prolongation, s)
+                         : fmg_start<float>(h, f, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+            else
+                st = f64 ? vcycle<double>(h, 0, L.f64, prm->nu1, prm->nu2, prm->omega, prm->prolongation, s)
+                         : vcycle<float>(h, 0, f, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
             if (st != WP_OK) return st;
             if (f64) st = defect<double>(h, L.v64, f, m, nullptr, &nr2, nullptr, s);
             else st = defect<float>(h, L.v, f, m, nullptr, &nr2, nullptr, s);
@@ -1806,11 +1848,15 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
         if (!(nf2 > 0.0)) nf2 = 1.0;
         double rel = std::sqrt(nr2 / nf2);
         while (!(use_tol && rel <= prm->rel_tol) && r.cycles < prm->max_cycles) {
-            // one FP32 V-cycle on the FP32 defect from a zero start, FP64 update, FP64 defect
-            WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
-            if ((st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s)) !=
-                WP_OK)
-                return st;
+            // one FP32 V-cycle (the first one a full-multigrid start if asked) on the FP32 defect from a
+            // zero start, FP64 update, FP64 defect
+            if (r.cycles == 0 && !pre_v && prm->start == WP_START_FMG) {
+                st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+            } else {
+                WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
+                st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+            }
+            if (st != WP_OK) return st;
             WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
             if ((st = defect<double>(h, h->p64, f, m, h->r32, &nr2, nullptr, s)) != WP_OK) return st;
             rel = std::sqrt(nr2 / nf2);
@@ -1855,9 +1901,13 @@ wp_status solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, in
     WP_CUDA_TRY(cudaMemsetAsync(h->p64, 0, sizeof(double) * n, s));
     if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, true, s)) != WP_OK) return st;
     for (int c = 0; c < cycles; ++c) {
-        WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
-        if ((st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s)) != WP_OK)
-            return st;
+        if (c == 0 && prm->start == WP_START_FMG) {
+            st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+        } else {
+            WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
+            st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+        }
+        if (st != WP_OK) return st;
         WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
         if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
     }
