@@ -124,6 +124,10 @@ typedef struct wp_mg_params {
     int precision;    /* WP_PREC_FP32 | WP_PREC_MIXED | WP_PREC_FP64 */
     int prolongation; /* WP_PROLONG_CONSTANT | WP_PROLONG_TRILINEAR */
     int start;        /* WP_START_ZERO | WP_START_FMG (ignored when an initial iterate is given) */
+    int host_loop;    /* 0: WP_PREC_MIXED tolerance solves run their cycle loop on the device (a CUDA
+                         graph whose while-node repeats cycle + defect + convergence test, no host
+                         round trip per cycle); 1: the host tests convergence after every cycle.
+                         Both give the same iterates, cycle counts and residual history. */
 } wp_mg_params;
 
 typedef struct wp_mg_report {
@@ -174,6 +178,11 @@ CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, int* varia
    FP32 3D levels only), 1 (restriction) or 2 (defect), with variant 0 for kinds 1-2; zc <= 0
    restores the heuristic chunk. */
 CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant);
+/* Uniform rows of one level (no reference counterpart): the number of (x, z) rows of cells whose
+   interior face fractions are all exactly 1, which the column kernels stream without reading any
+   fraction, and the number of rows (nx nz); counted when the handle is built.  For traffic
+   accounting. */
+CUWHHD_API wp_status wp_mgfrac3d_uniform_rows(const wp_mgfrac3d* h, int level, long long* uniform, long long* rows);
 
 typedef struct wp_mgfrac2d wp_mgfrac2d;
 /* Replaces CuMultigridFrac2D(Ax, Ay, int2 dim, DTYPE2 dx, char bc) (cuMultigridFrac2D.cu:28-111). */

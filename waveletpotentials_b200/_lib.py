@@ -31,7 +31,7 @@ class WPError(RuntimeError):
 class MgParams(ctypes.Structure):
     _fields_ = [("max_cycles", ctypes.c_int), ("nu1", ctypes.c_int), ("nu2", ctypes.c_int),
                 ("omega", ctypes.c_double), ("rel_tol", ctypes.c_double), ("precision", ctypes.c_int),
-                ("prolongation", ctypes.c_int), ("start", ctypes.c_int)]
+                ("prolongation", ctypes.c_int), ("start", ctypes.c_int), ("host_loop", ctypes.c_int)]
 
 
 class MgReport(ctypes.Structure):
@@ -93,6 +93,7 @@ SIGNATURES = {
     "wp_dst3d_solve_noalloc": (I, [P, P, I, I, I, D, D, D, P]),
     "wp_mgfrac3d_autotune": (I, [P, P]),
     "wp_mgfrac3d_tiles": (I, [P, P, P, P, I, P]),
+    "wp_mgfrac3d_uniform_rows": (I, [P, I, P, P]),
     "wp_mgfrac3d_set_tile": (I, [P, I, I, I, I]),
     "wp_conv3_forward": (I, [P, P, I, P, P, I, P, P, I, I, I, I, I, P, P, P]),
     "wp_conv3_wgrad": (I, [P, P, I, P, I, I, I, I, P]),

@@ -11,6 +11,7 @@ raise WPError instead of exiting the process.
 from __future__ import annotations
 
 import ctypes
+import math
 
 import torch
 
@@ -193,10 +194,10 @@ class CuMultigridFrac3D:
 
     def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
                  precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, start=START_ZERO,
-                 stream=None) -> dict:
+                 host_loop=False, stream=None) -> dict:
         c = self.cells
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), int(precision),
-                       int(prolongation), int(start))
+                       int(prolongation), int(start), int(bool(host_loop)))
         rep = MgReport()
         st = lib().wp_mgfrac3d_solve_tol(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), ctypes.byref(prm),
                                          ctypes.byref(rep), _stream(stream))
@@ -205,6 +206,14 @@ class CuMultigridFrac3D:
         if raise_on_fail and st != 0:
             check(st, "wp_mgfrac3d_solve_tol")
         return out
+
+    def UniformRows(self, level=0):
+        """(rows of the level whose face fractions are all 1, rows in all): the rows the column
+        kernels stream without reading fractions."""
+        u, r = ctypes.c_longlong(), ctypes.c_longlong()
+        check(lib().wp_mgfrac3d_uniform_rows(self._h, int(level), ctypes.byref(u), ctypes.byref(r)),
+              "wp_mgfrac3d_uniform_rows")
+        return u.value, r.value
 
     def Autotune(self, stream=None):
         """Times the level kernels over candidate z-chunks and keeps the fastest (synchronous)."""
@@ -276,10 +285,10 @@ class CuMultigridFrac2D:
 
     def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
                  precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, start=START_ZERO,
-                 stream=None) -> dict:
+                 host_loop=False, stream=None) -> dict:
         c = self.cells
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), int(precision),
-                       int(prolongation), int(start))
+                       int(prolongation), int(start), int(bool(host_loop)))
         rep = MgReport()
         st = lib().wp_mgfrac2d_solve_tol(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), ctypes.byref(prm),
                                          ctypes.byref(rep), _stream(stream))
@@ -486,7 +495,7 @@ class Projector3D:
 
     def __init__(self, ax, ay, az, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
                  precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, autotune=True, warm_start=None, sdf=None,
-                 start=START_ZERO, stream=None):
+                 start=START_ZERO, host_loop=False, stream=None):
         self.dim = _dims3(dim)
         self.dx = _dx3(dx)
         self.ax, self.ay, self.az = ax, ay, az
@@ -498,7 +507,7 @@ class Projector3D:
             self.mg.Autotune(stream)
         self.rec = CuWaveletPotentialRecover3D(self.dim, self.dx, "n")
         self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
-                         prolongation=prolongation, start=start)
+                         prolongation=prolongation, start=start, host_loop=host_loop)
         s = mac_shapes3d(*self.dim)
         self.shapes = s
         self.b = torch.empty(s["p"], device="cuda", dtype=torch.float32)
@@ -522,18 +531,76 @@ class Projector3D:
         return rep
 
 
+class HostPipeline3D:
+    """Projections of host-resident velocity fields through one Projector3D, with the transfers
+    overlapped: the pinned host-to-device copy of step k+1 runs on one copy stream and the
+    device-to-host copy of step k-1's potential on another while step k projects on the compute
+    stream (two device buffer sets; the copy engines and the SMs work at the same time).  Each step
+    copies its whole input in and its whole potential out; results are those of Projector3D.run.
+    """
+
+    def __init__(self, projector: "Projector3D", stream=None):
+        self.pr = projector
+        s = projector.shapes
+        self.u = [[torch.empty(s[k], device="cuda") for k in ("xv", "yv", "zv")] for _ in range(2)]
+        self.q = [[torch.empty(s[k], device="cuda") for k in ("qx", "qy", "qz")] for _ in range(2)]
+        self.comp = stream if stream is not None else torch.cuda.Stream()
+        self.s_in, self.s_out = torch.cuda.Stream(), torch.cuda.Stream()
+        ev = lambda: [torch.cuda.Event() for _ in range(2)]
+        self.ev_in, self.ev_done, self.ev_out = ev(), ev(), ev()
+        self.h2d_bytes = sum(4 * math.prod(s[k]) for k in ("xv", "yv", "zv"))
+        self.d2h_bytes = sum(4 * math.prod(s[k]) for k in ("qx", "qy", "qz"))
+
+    def _copy_in(self, k, host_u):
+        b = k % 2
+        with torch.cuda.stream(self.s_in):
+            # buffer b was last projected at step k-2 (the projection writes u in place)
+            self.s_in.wait_event(self.ev_done[b])
+            for d, h in zip(self.u[b], host_u):
+                d.copy_(h, non_blocking=True)
+            self.ev_in[b].record(self.s_in)
+
+    def run(self, host_in, host_out) -> list:
+        """host_in[k] = (xv, yv, zv), host_out[k] = (qx, qy, qz): pinned CPU float32 tensors of the
+        MAC shapes (the same tensors may repeat).  Returns the per-step reports; host_out holds the
+        potentials once the call returns."""
+        n = len(host_in)
+        if len(host_out) != n:
+            raise WPError(1, "HostPipeline3D.run", "host_in and host_out differ in length")
+        for e in self.ev_done + self.ev_out:
+            e.record(self.comp)
+        reps = []
+        if n:
+            self._copy_in(0, host_in[0])
+        for k in range(n):
+            b = k % 2
+            if k + 1 < n:
+                self._copy_in(k + 1, host_in[k + 1])
+            self.comp.wait_event(self.ev_in[b])
+            self.comp.wait_event(self.ev_out[b])  # q[b] was read out at step k-2
+            reps.append(self.pr.run(*self.u[b], *self.q[b], stream=self.comp))
+            self.ev_done[b].record(self.comp)
+            with torch.cuda.stream(self.s_out):
+                self.s_out.wait_event(self.ev_done[b])
+                for h, d in zip(host_out[k], self.q[b]):
+                    h.copy_(d, non_blocking=True)
+                self.ev_out[b].record(self.s_out)
+        self.s_out.synchronize()
+        return reps
+
+
 class Projector2D:
     """2D form of Projector3D (CuMultigridFrac2D + CuWaveletPotentialRecover2D)."""
 
     def __init__(self, ax, ay, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, start=START_ZERO, stream=None):
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, start=START_ZERO, host_loop=False, stream=None):
         self.dim = tuple(int(v) for v in dim)
         self.dx = float(dx)
         self.ax, self.ay = ax, ay
         self.mg = CuMultigridFrac2D(ax, ay, self.dim, self.dx, "n", stream)
         self.rec = CuWaveletPotentialRecover2D(self.dim, self.dx, "n")
         self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
-                         prolongation=prolongation, start=start)
+                         prolongation=prolongation, start=start, host_loop=host_loop)
         s = mac_shapes2d(*self.dim)
         self.b = torch.empty(s["p"], device="cuda", dtype=torch.float32)
         self.p = torch.empty(s["p"], device="cuda", dtype=torch.float32)
@@ -588,7 +655,7 @@ class BatchProjector:
             ay.append(_ptr(g["ay"], s["yv"], name="ay").value)
         self.dims = dims
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), PREC_MIXED,
-                       int(prolongation), int(start))
+                       int(prolongation), int(start), 0)
         h = ctypes.c_void_p()
         self._keep = ((ctypes.c_int * self.count)(*dims), (ctypes.c_int * (3 * self.count))(*ext),
                       (ctypes.c_double * self.count)(*dx), _parray(ax), _parray(ay), _parray(az), prm)

@@ -40,6 +40,8 @@ struct Lvl {
     const float* ay;
     const float* az;
     const float* fyc; // y-face fractions in cell layout: fyc[cell] = ay of the cell's lower y face
+    const unsigned char* uni; // per (x, z) row, at [z nx + x]: 1 when every face fraction the row's
+                              // stencils read (interior faces only) is exactly 1
     const T* glo[3];  // per-axis factor of the lower face, 0 at the wall
     const T* ghi[3];  // per-axis factor of the upper face, 0 at the wall
     const double* d[3];
@@ -209,6 +211,7 @@ struct QCol {
     int x, y0, z;
     long sxy, sax, i, iax;
     bool xm, xp, ym, yp;
+    unsigned char un; // row flag of plane z
     T gxl, gxh, gyl[4], gyh[4];
     Q4<T> vm, vc, azl;
 
@@ -232,23 +235,34 @@ struct QCol {
         vm = z0 > 0 ? cvt4<T>(ld4(v + i - sxy)) : zero4<T>();
         vc = cvt4<T>(ld4(v + i));
         azl = z0 > 0 ? cvt4<T>(ld4(L.az + i)) : zero4<T>();
+        un = z0 < L.nz ? L.uni[(long)z0 * L.nx + x] : 0;
     }
 
     __device__ __forceinline__ void step(Q4<T>& dg, Q4<T>& od, Q4<T>& c) {
         const int ny = L.ny, nz = L.nz;
-        const Q4<float> fyl = ld4(L.fyc + i);
-        const float fyu = yp ? L.fyc[i + 4] : 0.f;
+        const bool zp = z < nz - 1;
+        // a row whose faces are all exactly 1 reads no fractions (the same values, without the traffic)
+        const bool u = un != 0;
+        un = zp ? L.uni[(long)(z + 1) * L.nx + x] : 0;
         const T vym = ym ? (T)v[i - 1] : (T)0;
         const T vyp = yp ? (T)v[i + 4] : (T)0;
-        const Q4<float> fxl = ld4(L.ax + iax);
-        const Q4<float> fxu = xp ? ld4(L.ax + iax + ny) : zero4<float>();
         const Q4<T> vxm = xm ? cvt4<T>(ld4(v + i - ny)) : zero4<T>();
         const Q4<T> vxp = xp ? cvt4<T>(ld4(v + i + ny)) : zero4<T>();
         Q4<T> vp = zero4<T>(), azu = zero4<T>();
-        const bool zp = z < nz - 1;
-        if (zp) {
-            vp = cvt4<T>(ld4(v + i + sxy));
-            azu = cvt4<T>(ld4(L.az + i + sxy));
+        if (zp) vp = cvt4<T>(ld4(v + i + sxy));
+        Q4<float> fyl, fxl, fxu = zero4<float>();
+        float fyu = 0.f;
+        if (u) {
+            fyl = fxl = Q4<float>{{1.f, 1.f, 1.f, 1.f}};
+            if (yp) fyu = 1.f;
+            if (xp) fxu = fxl;
+            if (zp) azu = Q4<T>{{(T)1, (T)1, (T)1, (T)1}};
+        } else {
+            fyl = ld4(L.fyc + i);
+            if (yp) fyu = L.fyc[i + 4];
+            fxl = ld4(L.ax + iax);
+            if (xp) fxu = ld4(L.ax + iax + ny);
+            if (zp) azu = cvt4<T>(ld4(L.az + i + sxy));
         }
         const T gzl = L.glo[2][z], gzh = L.ghi[2][z];
 #pragma unroll
@@ -300,7 +314,7 @@ __device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __re
 // register-allocation variants of the same sweep (the autotuner picks one per level): default
 // limits, and at least 3 or 4 resident 256-thread CTAs per SM
 template <typename T>
-__global__ void __launch_bounds__(256) jacobi_q_kernel(T* __restrict__ dst, const T* __restrict__ src,
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1) jacobi_q_kernel(T* __restrict__ dst, const T* __restrict__ src,
                                                        const T* __restrict__ f, Lvl<T> L, T w, int zc) {
     jacobi_q_body<T>(dst, src, f, L, w, zc);
 }
@@ -633,7 +647,7 @@ __global__ void __launch_bounds__(256) resid_restrict_q_kernel(T* __restrict__ f
 
 // FP64 defect on quads (see defect64_z_kernel)
 template <typename TP>
-__global__ void __launch_bounds__(256) defect64_q_kernel(float* __restrict__ r32, const TP* __restrict__ p,
+__global__ void __launch_bounds__(256, 2) defect64_q_kernel(float* __restrict__ r32, const TP* __restrict__ p,
                                                          const float* __restrict__ f, Lvl<double> L, double m,
                                                          const double* __restrict__ msum, double* __restrict__ acc,
                                                          int zc) {
@@ -742,6 +756,32 @@ __global__ void fyc_kernel(float* __restrict__ fyc, const float* __restrict__ ay
         const long row = t / ny;
         const int y = (int)(t - row * ny);
         fyc[t] = ay[y + row * (ny + 1)];
+    }
+}
+
+// uni[z nx + x] = 1 when every face of row (x, z) that a stencil reads is exactly 1: the lower y
+// faces of y >= 1 (fyc), the x faces x and x + 1 and the z faces z and z + 1 that are interior.  One
+// warp per row.
+__global__ void uniform_rows_kernel(unsigned char* __restrict__ uni, const float* __restrict__ ax,
+                                    const float* __restrict__ fyc, const float* __restrict__ az, int nx, int ny,
+                                    int nz) {
+    const long rows = (long)nx * nz;
+    const int lane = threadIdx.x & 31;
+    for (long r = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; r < rows; r += ((long)gridDim.x * blockDim.x) >> 5) {
+        const int z = (int)(r / nx), x = (int)(r - (long)z * nx);
+        const long i = (long)x * ny + (long)z * nx * ny;
+        const long ia = (long)x * ny + (long)z * (nx + 1) * ny;
+        const long sxy = (long)nx * ny;
+        bool ok = true;
+        for (int y = lane; y < ny; y += 32) {
+            if (y > 0) ok = ok && fyc[i + y] == 1.f;
+            if (x > 0) ok = ok && ax[ia + y] == 1.f;
+            if (x < nx - 1) ok = ok && ax[ia + ny + y] == 1.f;
+            if (z > 0) ok = ok && az[i + y] == 1.f;
+            if (z < nz - 1) ok = ok && az[i + sxy + y] == 1.f;
+        }
+        ok = __all_sync(0xffffffffu, ok);
+        if (lane == 0) uni[r] = ok ? 1 : 0;
     }
 }
 
@@ -1041,6 +1081,283 @@ __global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1,
     for (int i = threadIdx.x; i < n0; i += blockDim.x) out[i] = v[0][i];
 }
 
+// ---- FP32 coarse cycle on precomputed stencils ------------------------------------------------
+// The levels a coarse cycle can hold (cells <= kCoarseCells) keep their stencil per cell, SoA in
+// kCcf arrays of `cells` floats: [0..5] the face coefficients (fraction x spacing factor) in the order
+// row() applies them (y-, y+, x-, x+, z-, z+), 0 where row() skips the face; [6] row()'s diagonal
+// (their sum in that order); [7] the cell's restriction weight (T)(d_z / s_z) * (T)(d_y / s_y *
+// (d_x / s_x)) of resid_restrict.  A sweep then needs no index decomposition, no boundary branches
+// and no global loads: with v padded by one z plane on either side, the six neighbours are
+// i -+ 1, i -+ ny, i -+ nx ny, and a skipped face contributes 0 * (a finite neighbour).
+constexpr int kCcf = 8;
+constexpr size_t kLeanSmemMax = 227 * 1024;
+
+__global__ void cc_coeff_kernel(float* __restrict__ out, Lvl<float> L) {
+    const int nx = L.nx, ny = L.ny, nz = L.nz, cells = nx * ny * nz;
+    const long sxy = (long)nx * ny;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cells; i += gridDim.x * blockDim.x) {
+        const int y = i % ny, x = (i / ny) % nx, z = i / (nx * ny);
+        const long iax = y + (long)x * ny + (long)z * (nx + 1) * ny;
+        const long iay = y + (long)x * (ny + 1) + (long)z * nx * (ny + 1);
+        float c[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float dg = 0.f;
+        if (y > 0) { c[0] = L.ay[iay] * L.glo[1][y]; dg += c[0]; }
+        if (y < ny - 1) { c[1] = L.ay[iay + 1] * L.ghi[1][y]; dg += c[1]; }
+        if (x > 0) { c[2] = L.ax[iax] * L.glo[0][x]; dg += c[2]; }
+        if (x < nx - 1) { c[3] = L.ax[iax + ny] * L.ghi[0][x]; dg += c[3]; }
+        if (z > 0) { c[4] = L.az[i] * L.glo[2][z]; dg += c[4]; }
+        if (z < nz - 1) { c[5] = L.az[i + sxy] * L.ghi[2][z]; dg += c[5]; }
+        const int x0 = x & ~1, y0 = y & ~1, zb = z & ~1;
+        const double sx = L.d[0][x0] + (x0 + 1 < nx ? L.d[0][x0 + 1] : 0.0);
+        const double sy = L.d[1][y0] + (y0 + 1 < ny ? L.d[1][y0 + 1] : 0.0);
+        const double sz = L.d[2][zb] + (zb + 1 < nz ? L.d[2][zb + 1] : 0.0);
+        const float wxy = (float)(L.d[1][y] / sy * (L.d[0][x] / sx));
+        const float wc = (float)(L.d[2][z] / sz) * wxy;
+        for (int k = 0; k < 6; ++k) out[(long)k * cells + i] = c[k];
+        out[6L * cells + i] = dg;
+        out[7L * cells + i] = wc;
+    }
+}
+
+struct LLev {
+    int nx, ny, nz;
+    const float* ccf; // kCcf x cells
+    float *v, *t;     // global v / t (written for the pack's finest level on exit)
+    const float* f;   // global right-hand side (read for the pack's finest level)
+};
+struct LPack {
+    LLev lv[kCoarseMax];
+    int n;
+};
+
+// shared floats a lean pack needs: per level v and t padded by a z plane on both sides, f, stencils
+inline long lean_smem_floats(const LPack& P) {
+    long s = 0;
+    for (int l = 0; l < P.n; ++l) {
+        const long c = (long)P.lv[l].nx * P.lv[l].ny * P.lv[l].nz, p = (long)P.lv[l].nx * P.lv[l].ny;
+        s += 2 * (c + 2 * p) + c + kCcf * c;
+    }
+    return s;
+}
+
+struct LS {
+    int nx, ny, nz, cells, nxy;
+    float *v, *t, *f; // v, t point past their lower padding plane
+    const float* cf;  // kCcf x cells
+};
+
+// off = -(sum of the present c_k * v_neighbour) in row()'s order; returns the centre value
+__device__ __forceinline__ float lean_off(const LS& S, const float* __restrict__ v, int i, float& od) {
+    const float* cf = S.cf;
+    const int n = S.cells;
+    float o = 0.f;
+    o -= cf[i] * v[i - 1];
+    o -= cf[n + i] * v[i + 1];
+    o -= cf[2 * n + i] * v[i - S.ny];
+    o -= cf[3 * n + i] * v[i + S.ny];
+    o -= cf[4 * n + i] * v[i - S.nxy];
+    o -= cf[5 * n + i] * v[i + S.nxy];
+    od = o;
+    return v[i];
+}
+
+__device__ __forceinline__ void lean_sweep(const LS& S, float* __restrict__ dst, const float* __restrict__ src, float w,
+                                           int i0, int step) {
+    for (int i = i0; i < S.cells; i += step) {
+        float od;
+        const float c = lean_off(S, src, i, od);
+        const float dg = S.cf[6 * S.cells + i];
+        dst[i] = dg > (float)kEps ? (1.f - w) * c + w * (S.f[i] - od) / dg : 0.f;
+    }
+}
+
+// (x, y, z) of cell i, and the step that adds `step` to i
+__device__ __forceinline__ void lean_coord(int i, int nx, int ny, int& x, int& y, int& z) {
+    y = i % ny;
+    x = (i / ny) % nx;
+    z = i / (nx * ny);
+}
+__device__ __forceinline__ void lean_advance(int& x, int& y, int& z, int bx, int by, int bz, int nx, int ny) {
+    y += by;
+    if (y >= ny) { y -= ny; ++x; }
+    x += bx;
+    if (x >= nx) { x -= nx; ++z; }
+    z += bz;
+}
+
+// residual of the fine level restricted to the coarse right-hand side (cc_restrict's sums and order)
+__device__ __forceinline__ void lean_restrict(const LS& F, const LS& C) {
+    const int B = blockDim.x;
+    int cx, cy, cz;
+    lean_coord(threadIdx.x, C.nx, C.ny, cx, cy, cz);
+    int bx, by, bz;
+    lean_coord(B, C.nx, C.ny, bx, by, bz);
+    const float* wcf = F.cf + 7L * F.cells;
+    const float* dgf = F.cf + 6L * F.cells;
+    for (int ci = threadIdx.x; ci < C.cells; ci += B) {
+        float tot[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+        for (int xo = 0; xo < 2; ++xo) {
+            const int x = 2 * cx + xo;
+            if (x >= F.nx) break;
+            for (int yo = 0; yo < 2; ++yo) {
+                const int y = 2 * cy + yo;
+                if (y >= F.ny) break;
+                float acc = 0.f;
+                for (int kz = 0; kz < 2; ++kz) {
+                    const int z = 2 * cz + kz;
+                    if (z >= F.nz) break;
+                    const int i = y + x * F.ny + z * F.nxy;
+                    float od;
+                    const float c = lean_off(F, F.v, i, od);
+                    const float dg = dgf[i];
+                    const float r = dg > (float)kEps ? F.f[i] - (dg * c + od) : 0.f;
+                    acc += wcf[i] * r;
+                }
+                tot[xo][yo] = acc;
+            }
+        }
+        C.f[ci] = (tot[0][0] + tot[0][1]) + (tot[1][0] + tot[1][1]);
+        lean_advance(cx, cy, cz, bx, by, bz, C.nx, C.ny);
+    }
+}
+
+// v += P vc (cc_prolong's arithmetic)
+__device__ __forceinline__ void lean_prolong(const LS& F, const LS& C, int prolong) {
+    const int B = blockDim.x;
+    int x, y, z;
+    lean_coord(threadIdx.x, F.nx, F.ny, x, y, z);
+    int bx, by, bz;
+    lean_coord(B, F.nx, F.ny, bx, by, bz);
+    const int ncx = C.nx, ncy = C.ny, ncz = C.nz;
+    const float* vc = C.v;
+    for (int i = threadIdx.x; i < F.cells; i += B) {
+        const int px = x >> 1, py = y >> 1, pz = z >> 1;
+        if (prolong != WP_PROLONG_TRILINEAR) {
+            F.v[i] += vc[py + px * ncy + pz * C.nxy];
+        } else {
+            int qx = (x & 1) ? px + 1 : px - 1, qy = (y & 1) ? py + 1 : py - 1, qz = (z & 1) ? pz + 1 : pz - 1;
+            if (qx < 0 || qx >= ncx) qx = px;
+            if (qy < 0 || qy >= ncy) qy = py;
+            if (qz < 0 || qz >= ncz) qz = pz;
+            auto Cv = [&](int xx, int yy, int zz) -> float { return vc[yy + xx * ncy + zz * C.nxy]; };
+            const float a = 0.75f, b = 0.25f;
+            float acc;
+            if (ncz == 1 && F.nz == 1) {
+                acc = a * (a * Cv(px, py, 0) + b * Cv(px, qy, 0)) + b * (a * Cv(qx, py, 0) + b * Cv(qx, qy, 0));
+            } else {
+                const float lo =
+                    a * (a * Cv(px, py, pz) + b * Cv(px, qy, pz)) + b * (a * Cv(qx, py, pz) + b * Cv(qx, qy, pz));
+                const float hi =
+                    a * (a * Cv(px, py, qz) + b * Cv(px, qy, qz)) + b * (a * Cv(qx, py, qz) + b * Cv(qx, qy, qz));
+                acc = a * lo + b * hi;
+            }
+            F.v[i] += acc;
+        }
+        lean_advance(x, y, z, bx, by, bz, F.nx, F.ny);
+    }
+}
+
+// coarse_cycle_kernel<float> on the precomputed stencils, everything in shared memory: the same
+// cycle, the same arithmetic per cell, the same output buffer
+__global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu1, int nu2, float w, int citers,
+                                                                 int prolong) {
+    extern __shared__ __align__(16) float lean_smem[];
+    LS S[kCoarseMax];
+    {
+        long off = 0;
+        for (int l = 0; l < P.n; ++l) {
+            LS& q = S[l];
+            q.nx = P.lv[l].nx;
+            q.ny = P.lv[l].ny;
+            q.nz = P.lv[l].nz;
+            q.nxy = q.nx * q.ny;
+            q.cells = q.nxy * q.nz;
+            q.v = lean_smem + off + q.nxy;
+            off += q.cells + 2 * q.nxy;
+            q.t = lean_smem + off + q.nxy;
+            off += q.cells + 2 * q.nxy;
+            q.f = lean_smem + off;
+            off += q.cells;
+            float* cf = lean_smem + off;
+            off += (long)kCcf * q.cells;
+            const float* g = P.lv[l].ccf;
+            for (int i = threadIdx.x; i < kCcf * q.cells; i += blockDim.x) cf[i] = g[i];
+            q.cf = cf;
+            // padding planes stay zero; level 0 starts from v = 0 and the global f
+            for (int i = threadIdx.x; i < q.cells + 2 * q.nxy; i += blockDim.x) {
+                q.v[i - q.nxy] = 0.f;
+                q.t[i - q.nxy] = 0.f;
+            }
+            if (l == 0)
+                for (int i = threadIdx.x; i < q.cells; i += blockDim.x) q.f[i] = P.lv[0].f[i];
+        }
+        __syncthreads();
+    }
+    const int tid = threadIdx.x, B = blockDim.x;
+    for (int l = 0; l < P.n - 1; ++l) {
+        LS& L = S[l];
+        if (l > 0) {
+            for (int i = tid; i < L.cells; i += B) L.v[i] = 0.f;
+            __syncthreads();
+        }
+        for (int k = 0; k < nu1; ++k) {
+            lean_sweep(L, L.t, L.v, w, tid, B);
+            __syncthreads();
+            float* tmp = L.v;
+            L.v = L.t;
+            L.t = tmp;
+        }
+        lean_restrict(L, S[l + 1]);
+        __syncthreads();
+    }
+    {
+        LS& L = S[P.n - 1];
+        if (P.n > 1) {
+            for (int i = tid; i < L.cells; i += B) L.v[i] = 0.f;
+            __syncthreads();
+        }
+        if (L.cells <= 32) {
+            // a coarsest grid of a few cells: one warp iterates alone (warp barriers only)
+            if (tid < 32) {
+                for (int k = 0; k < citers; ++k) {
+                    lean_sweep(L, L.t, L.v, w, tid, 32);
+                    __syncwarp();
+                    float* tmp = L.v;
+                    L.v = L.t;
+                    L.t = tmp;
+                }
+            } else if (citers & 1) {
+                float* tmp = L.v;
+                L.v = L.t;
+                L.t = tmp;
+            }
+            __syncthreads();
+        } else {
+            for (int k = 0; k < citers; ++k) {
+                lean_sweep(L, L.t, L.v, w, tid, B);
+                __syncthreads();
+                float* tmp = L.v;
+                L.v = L.t;
+                L.t = tmp;
+            }
+        }
+    }
+    for (int l = P.n - 2; l >= 0; --l) {
+        LS& L = S[l];
+        lean_prolong(L, S[l + 1], prolong);
+        __syncthreads();
+        for (int k = 0; k < nu2; ++k) {
+            lean_sweep(L, L.t, L.v, w, tid, B);
+            __syncthreads();
+            float* tmp = L.v;
+            L.v = L.t;
+            L.t = tmp;
+        }
+    }
+    float* out = ((nu1 + nu2) & 1) ? P.lv[0].t : P.lv[0].v;
+    for (int i = tid; i < S[0].cells; i += B) out[i] = S[0].v[i];
+}
+
 // coarse f = spacing-weighted average of the fine residuals of the (up to 8) children
 template <typename T>
 __global__ void __launch_bounds__(256) resid_restrict_kernel(T* __restrict__ fc, const T* __restrict__ v,
@@ -1260,6 +1577,9 @@ struct Level {
     long cells;
     float* frac[3];   // ax, ay, az (level-owned copies)
     float* fyc;       // ay re-laid per cell (lower y face), so y-quads of cells load with 128-bit accesses
+    unsigned char* uni; // per (x, z) row: all of the row's interior face fractions are exactly 1
+    float* ccf;       // levels of at most kCoarseCells cells: per-cell stencils of the FP32 coarse cycle
+    long long uni_rows; // rows flagged in uni
     double* tab64;    // per axis: glo[n], ghi[n], d[n]
     float* tab32;     // per axis: glo[n], ghi[n]
     float *v, *t, *f; // FP32 work
@@ -1274,13 +1594,20 @@ struct Level {
 
 enum { kZcJacobi = 0, kZcRestrict = 1, kZcDefect = 2 };
 
+// DRAM bytes of the face fractions one column-kernel pass over the level reads: 12 per cell of the
+// rows that are not uniform, and the row flags
+double frac_bytes(const Level& L) {
+    const double rows = (double)L.n[0] * L.n[2];
+    return 12.0 * (rows - (double)L.uni_rows) * L.n[1] + rows;
+}
+
 template <typename T>
 Lvl<T> view(const Level& L);
 template <>
 Lvl<float> view<float>(const Level& L) {
     Lvl<float> o;
     o.nx = L.n[0]; o.ny = L.n[1]; o.nz = L.n[2];
-    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2]; o.fyc = L.fyc;
+    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2]; o.fyc = L.fyc; o.uni = L.uni;
     long off64 = 0, off32 = 0;
     for (int a = 0; a < 3; ++a) {
         o.glo[a] = L.tab32 + off32;
@@ -1295,7 +1622,7 @@ template <>
 Lvl<double> view<double>(const Level& L) {
     Lvl<double> o;
     o.nx = L.n[0]; o.ny = L.n[1]; o.nz = L.n[2];
-    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2]; o.fyc = L.fyc;
+    o.ax = L.frac[0]; o.ay = L.frac[1]; o.az = L.frac[2]; o.fyc = L.fyc; o.uni = L.uni;
     long off64 = 0;
     for (int a = 0; a < 3; ++a) {
         o.glo[a] = L.tab64 + off64;
@@ -1438,6 +1765,17 @@ struct wp_mgfrac3d {
     float* r32;        // FP32 defect (right-hand side of correction cycles)
     const float* fin;  // finest right-hand side of the current solve
     const double* fin64;
+    int tune_gen;      // bumped by every change of a level's tile or kernel variant
+    // device-side cycle loop of the mixed-precision tolerance solve (see solve_mixed_graph)
+    cudaGraph_t loop_graph;
+    cudaGraphExec_t loop_exec;
+    void* loop_state;  // device MgLoop
+    cudaStream_t loop_cap; // private stream the loop is captured on (capture needs a non-default stream)
+    int loop_broken;   // capture or instantiation failed once: the host loop is used from then on
+    const float* loop_f;
+    int loop_key[6];   // nu1, nu2, prolongation, full-multigrid first cycle, tune_gen, device
+    double loop_omega;
+    long long loop_launches[2]; // kernels of the first cycle's graph part and of one loop body
 };
 
 namespace {
@@ -1477,6 +1815,17 @@ wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, cons
         WP_KERNEL("fyc", 8.0 * L.cells, s,
                   fyc_kernel<<<std::min<unsigned>(wp_cdiv(L.cells, 256), 4096), 256, 0, s>>>(L.fyc, L.frac[1], n[0],
                                                                                              n[1], L.cells));
+        WP_CUDA_TRY(cudaMalloc((void**)&L.uni, (size_t)n[0] * n[2]));
+        WP_KERNEL("uniform_rows", 16.0 * L.cells, s,
+                  uniform_rows_kernel<<<std::min<unsigned>(wp_cdiv((long)n[0] * n[2] * 32, 256), 4096), 256, 0, s>>>(
+                      L.uni, L.frac[0], L.fyc, L.frac[2], n[0], n[1], n[2]));
+        {
+            std::vector<unsigned char> u((size_t)n[0] * n[2]);
+            WP_CUDA_TRY(cudaMemcpyAsync(u.data(), L.uni, u.size(), cudaMemcpyDeviceToHost, s));
+            WP_CUDA_TRY(cudaStreamSynchronize(s));
+            L.uni_rows = 0;
+            for (unsigned char b : u) L.uni_rows += b != 0;
+        }
         // spacing tables; 2D problems have a single z layer with no z faces (tables all zero)
         std::vector<double> t64;
         std::vector<float> t32;
@@ -1497,6 +1846,11 @@ wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, cons
         WP_CUDA_TRY(cudaMalloc((void**)&L.tab32, sizeof(float) * t32.size()));
         WP_CUDA_TRY(cudaMemcpy(L.tab64, t64.data(), sizeof(double) * t64.size(), cudaMemcpyHostToDevice));
         WP_CUDA_TRY(cudaMemcpy(L.tab32, t32.data(), sizeof(float) * t32.size(), cudaMemcpyHostToDevice));
+        if (L.cells <= kCoarseCells) {
+            WP_CUDA_TRY(cudaMalloc((void**)&L.ccf, sizeof(float) * kCcf * L.cells));
+            WP_KERNEL("cc_coeff", 40.0 * L.cells, s,
+                      cc_coeff_kernel<<<wp_cdiv(L.cells, 256), 256, 0, s>>>(L.ccf, view<float>(L)));
+        }
         WP_CUDA_TRY(cudaMalloc((void**)&L.v, sizeof(float) * L.cells));
         WP_CUDA_TRY(cudaMalloc((void**)&L.t, sizeof(float) * L.cells));
         WP_CUDA_TRY(cudaMalloc((void**)&L.f, sizeof(float) * L.cells));
@@ -1554,7 +1908,7 @@ wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s, bool fin
                       launch_jacobi2<T>(L, Bufs<T>::t(L), Bufs<T>::v(L), f, w, zc, s));
             k += 2;
         } else {
-            WP_KERNEL(finest ? "jacobi_finest" : "jacobi", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
+            WP_KERNEL(finest ? "jacobi_finest" : "jacobi", (double)L.cells * 3.0 * sizeof(T) + frac_bytes(L), s,
                       launch_jacobi<T>(L, Bufs<T>::t(L), Bufs<T>::v(L), f, w, zc, s));
             k += 1;
         }
@@ -1578,6 +1932,28 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
     if (zero_start && l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax &&
         f == Bufs<T>::f(L) && pack_cells <= kCoarseSmemCells) {
         // the rest of the cycle in one launch; the host mirrors the buffer swaps it performs
+        bool lean = sizeof(T) == 4;
+        LPack Q;
+        Q.n = h->nl - l;
+        for (int k = 0; k < Q.n && lean; ++k) {
+            Level& E = h->lv[l + k];
+            lean = E.ccf != nullptr;
+            Q.lv[k] = {E.n[0], E.n[1], E.n[2], E.ccf, (float*)Bufs<T>::v(E), (float*)Bufs<T>::t(E),
+                       (const float*)Bufs<T>::f(E)};
+        }
+        const size_t lean_bytes = lean ? sizeof(float) * (size_t)lean_smem_floats(Q) : 0;
+        if (lean && lean_bytes <= kLeanSmemMax) {
+            WP_CUDA_TRY(wp_set_smem(coarse_cycle_lean_kernel, kLeanSmemMax));
+            WP_KERNEL("coarse_cycle", (double)L.cells * (3.0 * sizeof(T) + 12.0) * (nu1 + nu2 + 2), s,
+                      coarse_cycle_lean_kernel<<<1, 1024, lean_bytes, s>>>(Q, nu1, nu2, (float)w, h->coarsest_iters,
+                                                                            prolong));
+            for (int k = 0; k < Q.n; ++k) {
+                Level& E = h->lv[l + k];
+                const int swaps = (k == Q.n - 1) ? h->coarsest_iters : nu1 + nu2;
+                if (swaps & 1) std::swap(Bufs<T>::v(E), Bufs<T>::t(E));
+            }
+            return WP_OK;
+        }
         const size_t smem_max = 3 * sizeof(T) * (size_t)kCoarseSmemCells;
         WP_CUDA_TRY(wp_set_smem(coarse_cycle_kernel<T>, smem_max));
         CPack<T> P;
@@ -1606,7 +1982,7 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
             // coarse-z chunk so the fine columns keep >= 4 CTAs per SM busy
             const int czc = level_zc(L, kZcRestrict);
             WP_KERNEL(l == 0 ? "resid_restrict_finest" : "resid_restrict",
-                      (double)L.cells * (2.0 * sizeof(T) + 12.0) + (double)C.cells * sizeof(T), s,
+                      (double)L.cells * 2.0 * sizeof(T) + frac_bytes(L) + (double)C.cells * sizeof(T), s,
                       launch_resid_restrict<T>(L, C, Bufs<T>::f(C), Bufs<T>::v(L), f, czc, s));
         }
         WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(C), 0, sizeof(T) * C.cells, s));
@@ -1701,7 +2077,7 @@ wp_status defect_async(wp_mgfrac3d* h, const TP* p, const float* f, double m, co
     Level& L = h->lv[0];
     WP_CUDA_TRY(cudaMemsetAsync(h->acc, 0, (with_f2 ? 2 : 1) * sizeof(double), s));
     const int zc = level_zc(L, kZcDefect);
-    WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 16.0 + (r32 ? 4.0 : 0.0)), s,
+    WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 4.0 + (r32 ? 4.0 : 0.0)) + frac_bytes(L), s,
               launch_defect64<TP>(L, r32, p, f, m, msum, h->acc, zc, s));
     if (with_f2) {
         const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
@@ -1716,7 +2092,7 @@ wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r
     Level& L = h->lv[0];
     WP_CUDA_TRY(cudaMemsetAsync(h->acc, 0, 2 * sizeof(double), s));
     const int zc = level_zc(L, kZcDefect);
-    WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 16.0 + (r32 ? 4.0 : 0.0)), s,
+    WP_KERNEL("defect64", (double)L.cells * (sizeof(TP) + 4.0 + (r32 ? 4.0 : 0.0)) + frac_bytes(L), s,
               launch_defect64<TP>(L, r32, p, f, m, nullptr, h->acc, zc, s));
     if (norm_f2) {
         const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
@@ -1734,7 +2110,7 @@ void destroy_levels(wp_mgfrac3d* h) {
     for (int l = 0; l < kMaxLevels; ++l) {
         Level& L = h->lv[l];
         for (int a = 0; a < 3; ++a) if (L.frac[a]) cudaFree(L.frac[a]);
-        void* ps[] = {L.tab64, L.tab32, L.fyc, L.v, L.t, L.f, L.v64, L.t64, L.f64};
+        void* ps[] = {L.tab64, L.tab32, L.fyc, L.uni, L.ccf, L.v, L.t, L.f, L.v64, L.t64, L.f64};
         for (void* p : ps) if (p) cudaFree(p);
     }
     if (h->acc) cudaFree(h->acc);
@@ -1782,6 +2158,167 @@ wp_status solve_fixed(wp_mgfrac3d* h, float* dst, const float* pre_v, const floa
         if (st != WP_OK) return st;
     }
     WP_CUDA_TRY(cudaMemcpyAsync(dst, L.v, sizeof(float) * L.cells, cudaMemcpyDeviceToDevice, s));
+    return WP_OK;
+}
+
+// State of the device-side cycle loop: the stopping rule of solve_tol's host loop, evaluated by
+// mg_loop_check_kernel after every defect.
+struct MgLoop {
+    int cycles, max_cycles, use_tol, pad;
+    double tol, rel;
+    double hist[64];
+};
+
+__global__ void mg_loop_init_kernel(MgLoop* st, int max_cycles, int use_tol, double tol) {
+    st->cycles = 0;
+    st->max_cycles = max_cycles;
+    st->use_tol = use_tol;
+    st->tol = tol;
+    st->rel = 0.0;
+}
+
+// rel = sqrt(||r||^2 / ||f||^2) of the defect just computed (acc[0], acc[1]; ||f|| = 0 counts as 1),
+// recorded as in solve_tol; the loop goes on while the tolerance is not met, the cycle cap not
+// reached and rel is finite
+__global__ void mg_loop_check_kernel(MgLoop* st, const double* __restrict__ acc, cudaGraphConditionalHandle hc) {
+    double nf2 = acc[1];
+    if (!(nf2 > 0.0)) nf2 = 1.0;
+    const double rel = sqrt(acc[0] / nf2);
+    const int c = st->cycles;
+    if (c < 64) st->hist[c] = rel;
+    st->cycles = c + 1;
+    st->rel = rel;
+    const bool go = !(st->use_tol && rel <= st->tol) && c + 1 < st->max_cycles && isfinite(rel);
+    cudaGraphSetConditional(hc, go ? 1u : 0u);
+}
+
+void destroy_loop_graph(wp_mgfrac3d* h) {
+    if (h->loop_exec) cudaGraphExecDestroy(h->loop_exec);
+    if (h->loop_graph) cudaGraphDestroy(h->loop_graph);
+    h->loop_exec = nullptr;
+    h->loop_graph = nullptr;
+    h->loop_f = nullptr;
+}
+
+// one refinement step of the mixed solve on the device: FP32 correction cycle on r32 (the first
+// one a full-multigrid start if fmg), FP64 update, FP64 defect with the device mean, loop test
+wp_status mixed_step(wp_mgfrac3d* h, const float* f, const wp_mg_params* prm, bool fmg, cudaGraphConditionalHandle hc,
+                     cudaStream_t s) {
+    Level& L = h->lv[0];
+    const long n = L.cells;
+    const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
+    wp_status st;
+    if (fmg) {
+        st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+    } else {
+        WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
+        st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+    }
+    if (st != WP_OK) return st;
+    WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+    if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
+    WP_KERNEL("mg_loop_check", 0.0, s, mg_loop_check_kernel<<<1, 1, 0, s>>>((MgLoop*)h->loop_state, h->acc, hc));
+    return WP_OK;
+}
+
+// Builds the graph [first step] -> while (go) [step]: the first step is captured into the parent
+// graph, a while-node on the condition the check kernels set follows it, and one step is captured
+// into the node's body.  Every buffer a step reads is written earlier in the same step or is
+// loop-invariant (r32, p64, acc, f), so replaying the body repeats the host loop exactly.
+wp_status build_loop_graph(wp_mgfrac3d* h, const float* f, const wp_mg_params* prm, bool fmg) {
+    destroy_loop_graph(h);
+    if (!h->loop_state) WP_CUDA_TRY(cudaMalloc(&h->loop_state, sizeof(MgLoop)));
+    if (!h->loop_cap) WP_CUDA_TRY(cudaStreamCreateWithFlags(&h->loop_cap, cudaStreamNonBlocking));
+    cudaStream_t s = h->loop_cap;
+    cudaGraph_t g = nullptr;
+    WP_CUDA_TRY(cudaGraphCreate(&g, 0));
+    h->loop_graph = g;
+    cudaGraphConditionalHandle hc;
+    WP_CUDA_TRY(cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault));
+    const long long c0 = wp_launch_count();
+    WP_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    wp_status st = mixed_step(h, f, prm, fmg, hc, s);
+    cudaGraphNode_t cn = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (st == WP_OK) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = hc;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        if (e == cudaSuccess) e = cudaGraphAddNode(&cn, cg, deps, nd, &cp);
+        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &cn, 1, cudaStreamSetCaptureDependencies);
+        if (e == cudaSuccess) {
+            cudaGraph_t out = nullptr;
+            e = cudaStreamEndCapture(s, &out);
+            const long long c1 = wp_launch_count();
+            if (e == cudaSuccess) {
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    st = mixed_step(h, f, prm, false, hc, s);
+                    cudaGraph_t bout = nullptr;
+                    const cudaError_t e2 = cudaStreamEndCapture(s, &bout);
+                    if (st == WP_OK) e = e2;
+                }
+            }
+            h->loop_launches[0] = c1 - c0;
+            h->loop_launches[1] = wp_launch_count() - c1;
+        }
+    }
+    if (e != cudaSuccess || st != WP_OK) {
+        // leave the stream out of capture mode whatever failed
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(s, &junk);
+        }
+        (void)cudaGetLastError();
+    }
+    wp_add_launches(-(wp_launch_count() - c0));
+    if (st != WP_OK) { destroy_loop_graph(h); return st; }
+    if (e != cudaSuccess) { destroy_loop_graph(h); wp_set_cuda_error(e, "multigrid loop capture", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    e = cudaGraphInstantiate(&h->loop_exec, g, 0);
+    if (e != cudaSuccess) { destroy_loop_graph(h); wp_set_cuda_error(e, "multigrid loop instantiate", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    h->loop_f = f;
+    const int key[6] = {prm->nu1, prm->nu2, prm->prolongation, fmg ? 1 : 0, h->tune_gen, dev};
+    memcpy(h->loop_key, key, sizeof(key));
+    h->loop_omega = prm->omega;
+    return WP_OK;
+}
+
+bool loop_graph_ready(const wp_mgfrac3d* h, const float* f, const wp_mg_params* prm, bool fmg) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int key[6] = {prm->nu1, prm->nu2, prm->prolongation, fmg ? 1 : 0, h->tune_gen, dev};
+    return h->loop_exec && h->loop_f == f && memcmp(key, h->loop_key, sizeof(key)) == 0 && h->loop_omega == prm->omega;
+}
+
+// The cycle loop of the mixed tolerance solve as one graph launch (the rest of solve_tol's mixed
+// branch is unchanged): the same steps, stopping rule and report as the host loop, read back once.
+wp_status solve_mixed_graph(wp_mgfrac3d* h, const float* f, const wp_mg_params* prm, bool fmg, wp_mg_report* r,
+                            cudaStream_t s) {
+    if (!loop_graph_ready(h, f, prm, fmg)) {
+        wp_status st = build_loop_graph(h, f, prm, fmg);
+        if (st != WP_OK) return st;
+    }
+    WP_KERNEL("mg_loop_init", 0.0, s,
+              mg_loop_init_kernel<<<1, 1, 0, s>>>((MgLoop*)h->loop_state, prm->max_cycles, prm->rel_tol > 0.0 ? 1 : 0,
+                                                  prm->rel_tol));
+    WP_CUDA_TRY(cudaGraphLaunch(h->loop_exec, s));
+    MgLoop out;
+    WP_CUDA_TRY(cudaMemcpyAsync(&out, h->loop_state, sizeof(out), cudaMemcpyDeviceToHost, s));
+    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    wp_add_launches(h->loop_launches[0] + (long long)(out.cycles > 0 ? out.cycles - 1 : 0) * h->loop_launches[1]);
+    r->cycles = out.cycles;
+    for (int c = 0; c < out.cycles && c < 64; ++c) r->history[c] = out.hist[c];
+    r->rel_residual = out.rel;
     return WP_OK;
 }
 
@@ -1847,7 +2384,23 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
         if ((st = defect<double>(h, h->p64, f, m, h->r32, &nr2, &nf2, s)) != WP_OK) return st;
         if (!(nf2 > 0.0)) nf2 = 1.0;
         double rel = std::sqrt(nr2 / nf2);
-        while (!(use_tol && rel <= prm->rel_tol) && r.cycles < prm->max_cycles) {
+        const bool go = !(use_tol && rel <= prm->rel_tol) && prm->max_cycles > 0;
+        bool on_device = false;
+        if (go && !prm->host_loop && !h->loop_broken && !wp_profile_is_enabled()) {
+            // per-kernel timing events need the host loop; everything else runs the device loop
+            const bool fmg = !pre_v && prm->start == WP_START_FMG;
+            if (!loop_graph_ready(h, f, prm, fmg)) {
+                // a driver without conditional graph nodes, or a failed capture: keep the host loop
+                if (build_loop_graph(h, f, prm, fmg) != WP_OK) h->loop_broken = 1;
+                (void)cudaGetLastError();
+            }
+            if (!h->loop_broken) {
+                if ((st = solve_mixed_graph(h, f, prm, fmg, &r, s)) != WP_OK) return st;
+                rel = r.rel_residual;
+                on_device = true;
+            }
+        }
+        while (!on_device && !(use_tol && rel <= prm->rel_tol) && r.cycles < prm->max_cycles) {
             // one FP32 V-cycle (the first one a full-multigrid start if asked) on the FP32 defect from a
             // zero start, FP64 update, FP64 defect
             if (r.cycles == 0 && !pre_v && prm->start == WP_START_FMG) {
@@ -1957,6 +2510,9 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_iterate64(wp_mgfrac3d* h, double* ds
 
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_destroy(wp_mgfrac3d* h) {
     if (!h) return WP_OK;
+    destroy_loop_graph(h);
+    if (h->loop_state) cudaFree(h->loop_state);
+    if (h->loop_cap) cudaStreamDestroy(h->loop_cap);
     destroy_levels(h);
     delete h;
     return WP_OK;
@@ -2161,6 +2717,7 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
 
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_autotune(wp_mgfrac3d* h, void* stream) {
     if (!h) { wp_set_error_msg("wp_mgfrac3d_autotune: null handle"); return WP_ERR_INVALID_ARG; }
+    ++h->tune_gen;
     return autotune(h, (cudaStream_t)stream);
 }
 
@@ -2190,6 +2747,19 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, 
     L.zc[kind] = zc > 0 ? zc : 0;
     L.var[kind] = variant;
     L.zc_ms[kind] = 0.f;
+    ++h->tune_gen;
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_uniform_rows(const wp_mgfrac3d* h, int level, long long* uniform,
+                                                         long long* rows) {
+    if (!h || level < 0 || level >= h->nl || !uniform || !rows) {
+        wp_set_error_msg("wp_mgfrac3d_uniform_rows: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    const Level& L = h->lv[level];
+    *uniform = L.uni_rows;
+    *rows = (long long)L.n[0] * L.n[2];
     return WP_OK;
 }
 
