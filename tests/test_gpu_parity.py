@@ -409,3 +409,20 @@ def test_mg_jacobi_variants_agree(wp, oracle, variant):
     for o in outs[1:]:
         assert rel(outs[0][0], o[0]) < 1e-6
         np.testing.assert_allclose(outs[0][1], o[1], rtol=1e-4)
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_mg_restrict_variants_agree(wp, oracle, variant):
+    """The register-budget variants of the fused residual-restriction give the default kernel's cycles."""
+    nn, h, a, _, f = _sphere_problem(wp, oracle, 32, seed=13)
+    outs = []
+    for var, zc in ((0, 0), (variant, 1), (variant, 3)):
+        mg = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)
+        for lvl in range(2):
+            mg.SetTile(lvl, 1, zc, var)
+        dst = torch.zeros(f.shape, device="cuda")
+        rep = mg.SolveTol(dst, None, T(f), rel_tol=0.0, max_cycles=4, precision=wp.PREC_FP32)
+        outs.append((N(dst), rep["history"]))
+    for o in outs[1:]:
+        assert rel(outs[0][0], o[0]) < 1e-6
+        np.testing.assert_allclose(outs[0][1], o[1], rtol=1e-4)

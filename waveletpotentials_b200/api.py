@@ -546,8 +546,9 @@ class HostPipeline3D:
         self.q = [[torch.empty(s[k], device="cuda") for k in ("qx", "qy", "qz")] for _ in range(2)]
         self.comp = stream if stream is not None else torch.cuda.Stream()
         self.s_in, self.s_out = torch.cuda.Stream(), torch.cuda.Stream()
-        ev = lambda: [torch.cuda.Event() for _ in range(2)]
-        self.ev_in, self.ev_done, self.ev_out = ev(), ev(), ev()
+        ev = lambda timing=False: [torch.cuda.Event(enable_timing=timing) for _ in range(2)]
+        self.ev_in, self.ev_done, self.ev_out = ev(), ev(), ev(True)
+        self.last_out = None  # event after the last potential copied out by run()
         self.h2d_bytes = sum(4 * math.prod(s[k]) for k in ("xv", "yv", "zv"))
         self.d2h_bytes = sum(4 * math.prod(s[k]) for k in ("qx", "qy", "qz"))
 
@@ -585,6 +586,7 @@ class HostPipeline3D:
                 for h, d in zip(host_out[k], self.q[b]):
                     h.copy_(d, non_blocking=True)
                 self.ev_out[b].record(self.s_out)
+            self.last_out = self.ev_out[b]
         self.s_out.synchronize()
         return reps
 

@@ -268,7 +268,7 @@ extern "C" CUWHHD_API wp_status wp_batch_results(wp_batch* B, double* max_abs_di
     const int count = (int)B->g.size();
     std::vector<double> out(2 * count);
     cudaStream_t s = (cudaStream_t)stream;
-    WP_CUDA_TRY(cudaMemcpyAsync(out.data(), B->d_out, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, s));
+    WP_CUDA_TRY(wp_read_small(out.data(), B->d_out, sizeof(double) * 2 * count, s));
     WP_CUDA_TRY(cudaStreamSynchronize(s));
     for (int i = 0; i < count; ++i) {
         if (max_abs_div) max_abs_div[i] = out[2 * i];

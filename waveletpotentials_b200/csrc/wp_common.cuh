@@ -46,6 +46,10 @@ int wp_prof_start(cudaStream_t s);
 // Launch-count adjustment for work replayed from a CUDA graph (captured launches are counted once at
 // capture time; a replay adds them again).
 void wp_add_launches(long long n);
+// Reads a few bytes of device memory into host memory, ordered on stream s (synchronous).  A kernel
+// stores them into a mapped page-locked buffer, so the readback takes no copy engine and never
+// queues behind a large transfer another stream has in flight.
+cudaError_t wp_read_small(void* host, const void* dev, size_t bytes, cudaStream_t s);
 bool wp_profile_is_enabled();
 template <typename T>
 wp_status wp_dwt_axis_tune(T* buf, int DX, int DY, int DZ, int levels, char axis, int wavelet, char bc, int forward,

@@ -250,34 +250,53 @@ struct QCol {
         const Q4<T> vxp = xp ? cvt4<T>(ld4(v + i + ny)) : zero4<T>();
         Q4<T> vp = zero4<T>(), azu = zero4<T>();
         if (zp) vp = cvt4<T>(ld4(v + i + sxy));
-        Q4<float> fyl, fxl, fxu = zero4<float>();
-        float fyu = 0.f;
-        if (u) {
-            fyl = fxl = Q4<float>{{1.f, 1.f, 1.f, 1.f}};
-            if (yp) fyu = 1.f;
-            if (xp) fxu = fxl;
-            if (zp) azu = Q4<T>{{(T)1, (T)1, (T)1, (T)1}};
-        } else {
-            fyl = ld4(L.fyc + i);
-            if (yp) fyu = L.fyc[i + 4];
-            fxl = ld4(L.ax + iax);
-            if (xp) fxu = ld4(L.ax + iax + ny);
-            if (zp) azu = cvt4<T>(ld4(L.az + i + sxy));
-        }
         const T gzl = L.glo[2][z], gzh = L.ghi[2][z];
+        if (u && xm && xp && z > 0 && zp) {
+            // uniform interior row: each face coefficient is its spacing factor (1 x factor), every
+            // neighbour exists except y ones at the ends of the row
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int y = y0 + k;
-            T d = 0, o = 0, cf;
-            if (y > 0) { cf = (T)fyl.a[k] * gyl[k]; d += cf; o -= cf * (k > 0 ? vc.a[k - 1] : vym); }
-            if (y < ny - 1) { cf = (T)(k < 3 ? fyl.a[k + 1] : fyu) * gyh[k]; d += cf; o -= cf * (k < 3 ? vc.a[k + 1] : vyp); }
-            if (xm) { cf = (T)fxl.a[k] * gxl; d += cf; o -= cf * vxm.a[k]; }
-            if (xp) { cf = (T)fxu.a[k] * gxh; d += cf; o -= cf * vxp.a[k]; }
-            if (z > 0) { cf = azl.a[k] * gzl; d += cf; o -= cf * vm.a[k]; }
-            if (zp) { cf = azu.a[k] * gzh; d += cf; o -= cf * vp.a[k]; }
-            dg.a[k] = d;
-            od.a[k] = o;
-            c.a[k] = vc.a[k];
+            for (int k = 0; k < 4; ++k) {
+                T d = 0, o = 0;
+                if (k > 0 || ym) { d += gyl[k]; o -= gyl[k] * (k > 0 ? vc.a[k - 1] : vym); }
+                if (k < 3 || yp) { d += gyh[k]; o -= gyh[k] * (k < 3 ? vc.a[k + 1] : vyp); }
+                d += gxl; o -= gxl * vxm.a[k];
+                d += gxh; o -= gxh * vxp.a[k];
+                d += gzl; o -= gzl * vm.a[k];
+                d += gzh; o -= gzh * vp.a[k];
+                dg.a[k] = d;
+                od.a[k] = o;
+                c.a[k] = vc.a[k];
+            }
+            azu = Q4<T>{{(T)1, (T)1, (T)1, (T)1}};
+        } else {
+            Q4<float> fyl, fxl, fxu = zero4<float>();
+            float fyu = 0.f;
+            if (u) {
+                fyl = fxl = Q4<float>{{1.f, 1.f, 1.f, 1.f}};
+                if (yp) fyu = 1.f;
+                if (xp) fxu = fxl;
+                if (zp) azu = Q4<T>{{(T)1, (T)1, (T)1, (T)1}};
+            } else {
+                fyl = ld4(L.fyc + i);
+                if (yp) fyu = L.fyc[i + 4];
+                fxl = ld4(L.ax + iax);
+                if (xp) fxu = ld4(L.ax + iax + ny);
+                if (zp) azu = cvt4<T>(ld4(L.az + i + sxy));
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int y = y0 + k;
+                T d = 0, o = 0, cf;
+                if (y > 0) { cf = (T)fyl.a[k] * gyl[k]; d += cf; o -= cf * (k > 0 ? vc.a[k - 1] : vym); }
+                if (y < ny - 1) { cf = (T)(k < 3 ? fyl.a[k + 1] : fyu) * gyh[k]; d += cf; o -= cf * (k < 3 ? vc.a[k + 1] : vyp); }
+                if (xm) { cf = (T)fxl.a[k] * gxl; d += cf; o -= cf * vxm.a[k]; }
+                if (xp) { cf = (T)fxu.a[k] * gxh; d += cf; o -= cf * vxp.a[k]; }
+                if (z > 0) { cf = azl.a[k] * gzl; d += cf; o -= cf * vm.a[k]; }
+                if (zp) { cf = azu.a[k] * gzh; d += cf; o -= cf * vp.a[k]; }
+                dg.a[k] = d;
+                od.a[k] = o;
+                c.a[k] = vc.a[k];
+            }
         }
         vm = vc;
         vc = vp;
@@ -288,10 +307,12 @@ struct QCol {
     }
 };
 
-// y-quad index of a thread: q = x * (ny / 4) + yq over one z-plane
-template <typename T>
+// y-quad index of a thread: q = x * (ny / 4) + yq over one z-plane.  ACC: the swept values are not
+// stored but added to the FP64 iterate p64 (the refinement update fused into the last sweep of a
+// correction cycle, add_correction_kernel's arithmetic).
+template <typename T, bool ACC = false>
 __device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ f,
-                                              const Lvl<T>& L, T w, int zc) {
+                                              const Lvl<T>& L, T w, int zc, double* __restrict__ p64 = nullptr) {
     const int nq = L.ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
@@ -307,21 +328,95 @@ __device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __re
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             out.a[k] = dg.a[k] > (T)kEps ? ((T)1 - w) * c.a[k] + w * (fv.a[k] - od.a[k]) / dg.a[k] : (T)0;
+        if (ACC) {
+            Q4<double> pv = ld4(p64 + i);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) pv.a[k] += (double)out.a[k];
+            st4(p64 + i, pv);
+        } else {
+            st4(dst + i, out);
+        }
+    }
+}
+
+// The first sweep from v = 0: every neighbour and the centre are 0, so the sweep is
+// (1 - w) 0 + w (f - 0) / diag, which reads only f and (outside uniform rows) the fractions for the
+// diagonal -- the same value as jacobi_q_body on a zeroed v, with no v to clear or read.
+template <typename T>
+__global__ void __launch_bounds__(256) jacobi0_q_kernel(T* __restrict__ dst, const T* __restrict__ f, Lvl<T> L, T w,
+                                                        int zc) {
+    const int nq = L.ny >> 2;
+    const long q = (long)blockIdx.x * 256 + threadIdx.x;
+    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    if (q >= (long)L.nx * nq || z0 >= z1) return;
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
+    const long sxy = (long)nx * ny, sax = (long)(nx + 1) * ny;
+    long i = y0 + (long)x * ny + z0 * sxy, iax = y0 + (long)x * ny + z0 * sax;
+    const bool xm = x > 0, xp = x < nx - 1, yp = y0 + 4 < ny;
+    const T gxl = L.glo[0][x], gxh = L.ghi[0][x];
+    T gyl[4], gyh[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        gyl[k] = L.glo[1][y0 + k];
+        gyh[k] = L.ghi[1][y0 + k];
+    }
+    unsigned char un = L.uni[(long)z0 * nx + x];
+    Q4<T> azl = z0 > 0 ? cvt4<T>(ld4(L.az + i)) : zero4<T>();
+    for (int z = z0; z < z1; ++z) {
+        const bool zp = z < nz - 1;
+        const bool u = un != 0;
+        un = zp ? L.uni[(long)(z + 1) * nx + x] : 0;
+        Q4<float> fyl, fxl, fxu = zero4<float>();
+        float fyu = 0.f;
+        Q4<T> azu = zero4<T>();
+        if (u) {
+            fyl = fxl = Q4<float>{{1.f, 1.f, 1.f, 1.f}};
+            if (yp) fyu = 1.f;
+            if (xp) fxu = fxl;
+            if (zp) azu = Q4<T>{{(T)1, (T)1, (T)1, (T)1}};
+        } else {
+            fyl = ld4(L.fyc + i);
+            if (yp) fyu = L.fyc[i + 4];
+            fxl = ld4(L.ax + iax);
+            if (xp) fxu = ld4(L.ax + iax + ny);
+            if (zp) azu = cvt4<T>(ld4(L.az + i + sxy));
+        }
+        const T gzl = L.glo[2][z], gzh = L.ghi[2][z];
+        const Q4<T> fv = ld4(f + i);
+        Q4<T> out;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = y0 + k;
+            T d = 0;
+            if (y > 0) d += (T)fyl.a[k] * gyl[k];
+            if (y < ny - 1) d += (T)(k < 3 ? fyl.a[k + 1] : fyu) * gyh[k];
+            if (xm) d += (T)fxl.a[k] * gxl;
+            if (xp) d += (T)fxu.a[k] * gxh;
+            if (z > 0) d += azl.a[k] * gzl;
+            if (zp) d += azu.a[k] * gzh;
+            out.a[k] = d > (T)kEps ? ((T)1 - w) * (T)0 + w * (fv.a[k] - (T)0) / d : (T)0;
+        }
         st4(dst + i, out);
+        azl = azu;
+        i += sxy;
+        iax += sax;
     }
 }
 
 // register-allocation variants of the same sweep (the autotuner picks one per level): default
 // limits, and at least 3 or 4 resident 256-thread CTAs per SM
-template <typename T>
+template <typename T, bool ACC = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1) jacobi_q_kernel(T* __restrict__ dst, const T* __restrict__ src,
-                                                       const T* __restrict__ f, Lvl<T> L, T w, int zc) {
-    jacobi_q_body<T>(dst, src, f, L, w, zc);
+                                                       const T* __restrict__ f, Lvl<T> L, T w, int zc,
+                                                       double* __restrict__ p64 = nullptr) {
+    jacobi_q_body<T, ACC>(dst, src, f, L, w, zc, p64);
 }
-template <typename T, int MINB>
+template <typename T, int MINB, bool ACC = false>
 __global__ void __launch_bounds__(256, MINB) jacobi_q_mb_kernel(T* __restrict__ dst, const T* __restrict__ src,
-                                                                const T* __restrict__ f, Lvl<T> L, T w, int zc) {
-    jacobi_q_body<T>(dst, src, f, L, w, zc);
+                                                                const T* __restrict__ f, Lvl<T> L, T w, int zc,
+                                                                double* __restrict__ p64 = nullptr) {
+    jacobi_q_body<T, ACC>(dst, src, f, L, w, zc, p64);
 }
 
 // Two weighted-Jacobi sweeps in one pass (temporal blocking along z).  A CTA owns an interior tile
@@ -579,10 +674,11 @@ __global__ void __launch_bounds__(TS_THREADS, 2)
 // coarse plane and sums its y pairs in registers, and a lane shuffle adds the two rows:
 // ((x0,y) + (x0,y+1)) + ((x0+1,y) + (x0+1,y+1)), each child carrying (0 + w_z0 r_z0) + w_z1 r_z1,
 // the order of resid_restrict_z_kernel.
-template <typename T>
-__global__ void __launch_bounds__(256) resid_restrict_q_kernel(T* __restrict__ fc, const T* __restrict__ v,
-                                                               const T* __restrict__ f, Lvl<T> L, int ncx, int ncy,
-                                                               int ncz, int czc) {
+// MINB: register-budget variants as for the Jacobi sweep (1 default, 3 or 4 resident CTAs per SM).
+template <typename T, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) resid_restrict_q_kernel(T* __restrict__ fc, const T* __restrict__ v,
+                                                                     const T* __restrict__ f, Lvl<T> L, int ncx,
+                                                                     int ncy, int ncz, int czc) {
     const int nq = L.ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int cz0 = blockIdx.y * czc, cz1 = min(cz0 + czc, ncz);
@@ -1706,6 +1802,21 @@ void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc
 }
 
 
+// One FP32 sweep of src whose result is added to p64 instead of stored (the level's tuned one-sweep
+// quad kernel); false when the level's kernel has no such form (the caller then stores and adds).
+bool jacobi_acc_ok(const Level& L, const void* src, const void* f, const double* p64) {
+    return quad_ok(L) && al16(src) && al16(f) && al16(p64) && L.var[kZcJacobi] <= 2;
+}
+void launch_jacobi_acc(const Level& L, const float* src, const float* f, float w, int zc, double* p64,
+                       cudaStream_t s) {
+    const int var = L.var[kZcJacobi];
+    const Lvl<float> V = view<float>(L);
+    const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
+    if (var == 1) jacobi_q_mb_kernel<float, 3, true><<<g, 256, 0, s>>>(nullptr, src, f, V, w, zc, p64);
+    else if (var == 2) jacobi_q_mb_kernel<float, 4, true><<<g, 256, 0, s>>>(nullptr, src, f, V, w, zc, p64);
+    else jacobi_q_kernel<float, true><<<g, 256, 0, s>>>(nullptr, src, f, V, w, zc, p64);
+}
+
 // two sweeps dst <- J(J(src)) in one pass (jacobi2_q_kernel)
 template <typename T>
 void launch_jacobi2(const Level& L, T* dst, const T* src, const T* f, T w, int zc, cudaStream_t s) {
@@ -1720,7 +1831,10 @@ void launch_resid_restrict(const Level& L, const Level& C, T* fc, const T* v, co
     const Lvl<T> V = view<T>(L);
     if (quad_ok(L) && C.n[1] * 2 == L.n[1] && al16(v) && al16(f)) {
         const dim3 g(wp_cdiv((size_t)C.n[0] * (L.n[1] / 4) * 2, 256), wp_cdiv(C.n[2], czc));
-        resid_restrict_q_kernel<T><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
+        const int var = sizeof(T) == 4 ? L.var[kZcRestrict] : 0;
+        if (var == 1) resid_restrict_q_kernel<T, 3><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
+        else if (var == 2) resid_restrict_q_kernel<T, 4><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
+        else resid_restrict_q_kernel<T><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
     } else {
         const dim3 g(wp_cdiv(L.n[1], 32), wp_cdiv(L.n[0], 8), wp_cdiv(C.n[2], czc));
         resid_restrict_z_kernel<T><<<g, dim3(32, 8), 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
@@ -1896,12 +2010,25 @@ struct Bufs<double> {
 };
 
 // profile names: the finest level is reported apart (it carries the roofline of the cycle)
+// acc64 (FP32 levels): the last sweep adds its result to acc64 instead of storing it, when the
+// level's kernel allows (*added reports it; the level's v then holds no meaningful values)
 template <typename T>
-wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s, bool finest = false) {
+wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s, bool finest = false, double* acc64 = nullptr,
+                 bool* added = nullptr) {
     const int zc = level_zc(L, kZcJacobi);
     // the variant is tuned on the FP32 kernels; FP64 smoothing keeps one sweep per launch
     const bool fused = sizeof(T) == 4 && L.var[kZcJacobi] == 3 && jacobi2_ok(L, f);
     for (int k = 0; k < sweeps;) {
+        if (sizeof(T) == 4 && acc64 && k == sweeps - 1 && jacobi_acc_ok(L, Bufs<T>::v(L), f, acc64)) {
+            WP_KERNEL(finest ? "jacobi_finest_update" : "jacobi_update",
+                      (double)L.cells * (2.0 * sizeof(T) + 16.0) + frac_bytes(L), s,
+                      launch_jacobi_acc(L, (const float*)Bufs<T>::v(L), (const float*)f, (float)w, zc, acc64, s));
+            *added = true;
+            T* tmp = Bufs<T>::v(L);
+            Bufs<T>::v(L) = Bufs<T>::t(L);
+            Bufs<T>::t(L) = tmp;
+            break;
+        }
         if (fused && sweeps - k >= 2) {
             // two sweeps, one pass: algorithmic bytes are those of one sweep
             WP_KERNEL(finest ? "jacobi2_finest" : "jacobi2", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
@@ -1919,17 +2046,19 @@ wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s, bool fin
     return WP_OK;
 }
 
-// One V-cycle at level l from the level's current v (zero_start: v is known to be zero, which lets
-// the single-launch coarse cycle take over below kCoarseCells).
+// One V-cycle at level l from the level's current v, or (clear_v) from v = 0: then v is neither
+// cleared nor read -- the first sweep is jacobi0_q_kernel where the level's kernel allows, otherwise
+// v is cleared first -- and below kCoarseCells the single-launch coarse cycle takes over.
+// acc64 / added: see smooth (the finest level's last post-sweep adds into acc64 when it can).
 template <typename T>
-wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int prolong, cudaStream_t s,
-                 bool zero_start = true) {
+wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int prolong, cudaStream_t s, bool clear_v,
+                 double* acc64 = nullptr, bool* added = nullptr) {
     Level& L = h->lv[l];
     const dim3 g = grid_of(L.n[0], L.n[1], L.n[2]);
     wp_status st;
     long pack_cells = 0;
     for (int k = l; k < h->nl; ++k) pack_cells += h->lv[k].cells;
-    if (zero_start && l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax &&
+    if (clear_v && l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax &&
         f == Bufs<T>::f(L) && pack_cells <= kCoarseSmemCells) {
         // the rest of the cycle in one launch; the host mirrors the buffer swaps it performs
         bool lean = sizeof(T) == 4;
@@ -1976,7 +2105,21 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         return WP_OK;
     }
     if (l < h->nl - 1) {
-        if ((st = smooth<T>(L, f, nu1, w, s, l == 0)) != WP_OK) return st;
+        int pre = nu1;
+        if (clear_v) {
+            const int var = sizeof(T) == 4 ? L.var[kZcJacobi] : 0;
+            if (nu1 > 0 && quad_ok(L) && al16(Bufs<T>::t(L)) && al16(f) && var <= 2) {
+                const int zc = level_zc(L, kZcJacobi);
+                const dim3 gq(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
+                WP_KERNEL(l == 0 ? "jacobi0_finest" : "jacobi0", (double)L.cells * 2.0 * sizeof(T) + frac_bytes(L), s,
+                          jacobi0_q_kernel<T><<<gq, 256, 0, s>>>(Bufs<T>::t(L), f, view<T>(L), w, zc));
+                std::swap(Bufs<T>::v(L), Bufs<T>::t(L));
+                pre = nu1 - 1;
+            } else {
+                WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(L), 0, sizeof(T) * L.cells, s));
+            }
+        }
+        if ((st = smooth<T>(L, f, pre, w, s, l == 0)) != WP_OK) return st;
         Level& C = h->lv[l + 1];
         {
             // coarse-z chunk so the fine columns keep >= 4 CTAs per SM busy
@@ -1985,13 +2128,12 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
                       (double)L.cells * 2.0 * sizeof(T) + frac_bytes(L) + (double)C.cells * sizeof(T), s,
                       launch_resid_restrict<T>(L, C, Bufs<T>::f(C), Bufs<T>::v(L), f, czc, s));
         }
-        WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(C), 0, sizeof(T) * C.cells, s));
-        if ((st = vcycle<T>(h, l + 1, Bufs<T>::f(C), nu1, nu2, w, prolong, s)) != WP_OK) return st;
+        if ((st = vcycle<T>(h, l + 1, Bufs<T>::f(C), nu1, nu2, w, prolong, s, true)) != WP_OK) return st;
         if (prolong == WP_PROLONG_TRILINEAR) {
             WP_KERNEL(l == 0 ? "prolong_trilinear_finest" : "prolong_trilinear",
                       (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
                       launch_prolong_tri<T>(L, C, Bufs<T>::v(L), Bufs<T>::v(C), s));
-            if ((st = smooth<T>(L, f, nu2, w, s, l == 0)) != WP_OK) return st;
+            if ((st = smooth<T>(L, f, nu2, w, s, l == 0, acc64, added)) != WP_OK) return st;
         } else if (nu2 > 0) {
             // first post-sweep reads v + P vc directly (prolongation fused into the sweep)
             const int zc = level_zc(L, kZcJacobi);
@@ -2001,13 +2143,14 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
             T* tmp = Bufs<T>::v(L);
             Bufs<T>::v(L) = Bufs<T>::t(L);
             Bufs<T>::t(L) = tmp;
-            if ((st = smooth<T>(L, f, nu2 - 1, w, s, l == 0)) != WP_OK) return st;
+            if ((st = smooth<T>(L, f, nu2 - 1, w, s, l == 0, acc64, added)) != WP_OK) return st;
         } else {
             WP_KERNEL("prolong_constant", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
                       prolong_add_kernel<T><<<g, dim3(32, 8), 0, s>>>(Bufs<T>::v(L), Bufs<T>::v(C), L.n[0], L.n[1],
                                                                      L.n[2], C.n[0], C.n[1]));
         }
     } else {
+        if (clear_v) WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(L), 0, sizeof(T) * L.cells, s));
         const size_t smem = 2 * sizeof(T) * L.cells;
         if (smem <= 200 * 1024) {
             auto k = coarsest_kernel<T>;
@@ -2027,7 +2170,8 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
 // coarser solution followed by one V-cycle.  Leaves the finest level's iterate in its v; costs
 // about one V-cycle more than a V-cycle and replaces the first cycles from a zero start.
 template <typename T>
-wp_status fmg_start(wp_mgfrac3d* h, const T* f0, int nu1, int nu2, T w, int prolong, cudaStream_t s) {
+wp_status fmg_start(wp_mgfrac3d* h, const T* f0, int nu1, int nu2, T w, int prolong, cudaStream_t s,
+                    double* acc64 = nullptr, bool* added = nullptr) {
     wp_status st;
     for (int l = 0; l + 1 < h->nl; ++l) {
         Level& L = h->lv[l];
@@ -2038,8 +2182,7 @@ wp_status fmg_start(wp_mgfrac3d* h, const T* f0, int nu1, int nu2, T w, int prol
                   launch_resid_restrict<T>(L, C, Bufs<T>::f(C), Bufs<T>::v(L), fl, level_zc(L, kZcRestrict), s));
     }
     const int lc = h->nl - 1;
-    WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(h->lv[lc]), 0, sizeof(T) * h->lv[lc].cells, s));
-    if ((st = vcycle<T>(h, lc, lc == 0 ? f0 : Bufs<T>::f(h->lv[lc]), nu1, nu2, w, prolong, s)) != WP_OK) return st;
+    if ((st = vcycle<T>(h, lc, lc == 0 ? f0 : Bufs<T>::f(h->lv[lc]), nu1, nu2, w, prolong, s, true)) != WP_OK) return st;
     for (int l = lc - 1; l >= 0; --l) {
         Level& L = h->lv[l];
         Level& C = h->lv[l + 1];
@@ -2051,7 +2194,9 @@ wp_status fmg_start(wp_mgfrac3d* h, const T* f0, int nu1, int nu2, T w, int prol
             WP_KERNEL("fmg_prolong", (double)L.cells * 2.0 * sizeof(T) + (double)C.cells * sizeof(T), s,
                       prolong_add_kernel<T><<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(
                           Bufs<T>::v(L), Bufs<T>::v(C), L.n[0], L.n[1], L.n[2], C.n[0], C.n[1]));
-        if ((st = vcycle<T>(h, l, l == 0 ? f0 : Bufs<T>::f(L), nu1, nu2, w, prolong, s, false)) != WP_OK) return st;
+        if ((st = vcycle<T>(h, l, l == 0 ? f0 : Bufs<T>::f(L), nu1, nu2, w, prolong, s, false, l == 0 ? acc64 : nullptr,
+                            l == 0 ? added : nullptr)) != WP_OK)
+            return st;
     }
     return WP_OK;
 }
@@ -2063,8 +2208,7 @@ wp_status active_mean(wp_mgfrac3d* h, const float* f, double* m, cudaStream_t s)
     WP_KERNEL("active_sum", (double)L.cells * 16.0, s,
               active_sum_kernel<<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(f, view<double>(L), h->acc + 2));
     double hv[2];
-    WP_CUDA_TRY(cudaMemcpyAsync(hv, h->acc + 2, sizeof(hv), cudaMemcpyDeviceToHost, s));
-    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    WP_CUDA_TRY(wp_read_small(hv, h->acc + 2, sizeof(hv), s));
     *m = hv[1] > 0 ? hv[0] / hv[1] : 0.0;
     return WP_OK;
 }
@@ -2099,8 +2243,7 @@ wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r
         WP_KERNEL("sumsq", 4.0 * L.cells, s, sumsq_kernel<float><<<b, 256, 0, s>>>(f, L.cells, h->acc + 1));
     }
     double hv[2];
-    WP_CUDA_TRY(cudaMemcpyAsync(hv, h->acc, sizeof(hv), cudaMemcpyDeviceToHost, s));
-    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    WP_CUDA_TRY(wp_read_small(hv, h->acc, sizeof(hv), s));
     *norm_r2 = hv[0];
     if (norm_f2) *norm_f2 = hv[1];
     return WP_OK;
@@ -2154,7 +2297,7 @@ wp_status solve_fixed(wp_mgfrac3d* h, float* dst, const float* pre_v, const floa
     if (pre_v) WP_CUDA_TRY(cudaMemcpyAsync(L.v, pre_v, sizeof(float) * L.cells, cudaMemcpyDeviceToDevice, s));
     else WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * L.cells, s));
     for (int c = 0; c < n_iters; ++c) {
-        wp_status st = vcycle<float>(h, 0, f, nu1, nu2, (float)weight, WP_PROLONG_CONSTANT, s);
+        wp_status st = vcycle<float>(h, 0, f, nu1, nu2, (float)weight, WP_PROLONG_CONSTANT, s, false);
         if (st != WP_OK) return st;
     }
     WP_CUDA_TRY(cudaMemcpyAsync(dst, L.v, sizeof(float) * L.cells, cudaMemcpyDeviceToDevice, s));
@@ -2208,14 +2351,15 @@ wp_status mixed_step(wp_mgfrac3d* h, const float* f, const wp_mg_params* prm, bo
     const long n = L.cells;
     const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
     wp_status st;
+    bool added = false;
     if (fmg) {
-        st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+        st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, h->p64, &added);
     } else {
-        WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
-        st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+        st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, true, h->p64,
+                           &added);
     }
     if (st != WP_OK) return st;
-    WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+    if (!added) WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
     if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
     WP_KERNEL("mg_loop_check", 0.0, s, mg_loop_check_kernel<<<1, 1, 0, s>>>((MgLoop*)h->loop_state, h->acc, hc));
     return WP_OK;
@@ -2313,8 +2457,7 @@ wp_status solve_mixed_graph(wp_mgfrac3d* h, const float* f, const wp_mg_params* 
                                                   prm->rel_tol));
     WP_CUDA_TRY(cudaGraphLaunch(h->loop_exec, s));
     MgLoop out;
-    WP_CUDA_TRY(cudaMemcpyAsync(&out, h->loop_state, sizeof(out), cudaMemcpyDeviceToHost, s));
-    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    WP_CUDA_TRY(wp_read_small(&out, h->loop_state, sizeof(out), s));
     wp_add_launches(h->loop_launches[0] + (long long)(out.cycles > 0 ? out.cycles - 1 : 0) * h->loop_launches[1]);
     r->cycles = out.cycles;
     for (int c = 0; c < out.cycles && c < 64; ++c) r->history[c] = out.hist[c];
@@ -2361,8 +2504,8 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
                 st = f64 ? fmg_start<double>(h, L.f64, prm->nu1, prm->nu2, prm->omega, prm->prolongation, s)
                          : fmg_start<float>(h, f, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
             else
-                st = f64 ? vcycle<double>(h, 0, L.f64, prm->nu1, prm->nu2, prm->omega, prm->prolongation, s)
-                         : vcycle<float>(h, 0, f, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+                st = f64 ? vcycle<double>(h, 0, L.f64, prm->nu1, prm->nu2, prm->omega, prm->prolongation, s, false)
+                         : vcycle<float>(h, 0, f, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, false);
             if (st != WP_OK) return st;
             if (f64) st = defect<double>(h, L.v64, f, m, nullptr, &nr2, nullptr, s);
             else st = defect<float>(h, L.v, f, m, nullptr, &nr2, nullptr, s);
@@ -2403,14 +2546,17 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
         while (!on_device && !(use_tol && rel <= prm->rel_tol) && r.cycles < prm->max_cycles) {
             // one FP32 V-cycle (the first one a full-multigrid start if asked) on the FP32 defect from a
             // zero start, FP64 update, FP64 defect
+            bool added = false;
             if (r.cycles == 0 && !pre_v && prm->start == WP_START_FMG) {
-                st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+                st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, h->p64,
+                                      &added);
             } else {
-                WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
-                st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+                st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, true,
+                                   h->p64, &added);
             }
             if (st != WP_OK) return st;
-            WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+            if (!added)
+                WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
             if ((st = defect<double>(h, h->p64, f, m, h->r32, &nr2, nullptr, s)) != WP_OK) return st;
             rel = std::sqrt(nr2 / nf2);
             if (r.cycles < 64) r.history[r.cycles] = rel;
@@ -2454,14 +2600,16 @@ wp_status solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, in
     WP_CUDA_TRY(cudaMemsetAsync(h->p64, 0, sizeof(double) * n, s));
     if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, true, s)) != WP_OK) return st;
     for (int c = 0; c < cycles; ++c) {
+        bool added = false;
         if (c == 0 && prm->start == WP_START_FMG) {
-            st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+            st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, h->p64,
+                                  &added);
         } else {
-            WP_CUDA_TRY(cudaMemsetAsync(L.v, 0, sizeof(float) * n, s));
-            st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s);
+            st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, true, h->p64,
+                               &added);
         }
         if (st != WP_OK) return st;
-        WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+        if (!added) WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
         if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
     }
     h->last64 = 1;
@@ -2668,7 +2816,7 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             const long floor_blocks = std::min<long>(most, 2L * wp_sm_count());
             void* fl = L.cells > kL2Cells ? flush : nullptr;
             // jacobi variants: 0-2 one sweep per launch (register budgets), 3 two sweeps per launch
-            const int nvar = (kind == kZcJacobi && quad_ok(L)) ? 5 : 1;
+            const int nvar = !quad_ok(L) ? 1 : kind == kZcJacobi ? 5 : kind == kZcRestrict ? 3 : 1;
             for (int var = 0; var < nvar && st == WP_OK; ++var) {
                 if (var == 3 && !jacobi2_ok(L, L.f)) continue;
                 if (var == 4 && !jacobi_ts_ok(L, L.t, L.v, L.f)) continue;
@@ -2739,7 +2887,7 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc,
 // 2 defect); zc <= 0 restores the heuristic.
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant) {
     if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 4 ||
-        (variant != 0 && kind != kZcJacobi)) {
+        (kind == kZcRestrict && variant > 2) || (kind == kZcDefect && variant != 0)) {
         wp_set_error_msg("wp_mgfrac3d_set_tile: bad arguments");
         return WP_ERR_INVALID_ARG;
     }

@@ -9,6 +9,8 @@
 // All kernels map threadIdx.x to y (the contiguous index) so every access is coalesced.
 #include "wp_common.cuh"
 
+#include <map>
+
 #include <cstring>
 #include <vector>
 
@@ -312,16 +314,18 @@ wp_status wp_max_abs_device(const float* x, size_t n, unsigned int* d_out, cudaS
 extern "C" CUWHHD_API wp_status wp_max_abs(const float* x, size_t n, double* out, void* stream) {
     if ((!x && n) || !out) { wp_set_error_msg("wp_max_abs: null pointer"); return WP_ERR_INVALID_ARG; }
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned int* d = nullptr;
-    WP_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(unsigned int), s));
+    // one device word per (host thread, device), allocated on first use: no allocation per call
+    thread_local std::map<int, unsigned int*> slots;
+    int dev = 0;
+    WP_CUDA_TRY(cudaGetDevice(&dev));
+    unsigned int*& d = slots[dev];
+    if (!d) WP_CUDA_TRY(cudaMalloc((void**)&d, sizeof(unsigned int)));
     wp_status st = wp_max_abs_device(x, n, d, s);
     unsigned int bits = 0;
     if (st == WP_OK) {
-        cudaError_t e = cudaMemcpyAsync(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        const cudaError_t e = wp_read_small(&bits, d, sizeof(bits), s);
         if (e != cudaSuccess) { wp_set_cuda_error(e, "wp_max_abs", __FILE__, __LINE__); st = WP_ERR_CUDA; }
     }
-    cudaFreeAsync(d, s);
     float f;
     memcpy(&f, &bits, sizeof(f));
     *out = (double)f;

@@ -1,6 +1,8 @@
 // wp_util.cu -- error reporting and device queries shared by the C ABI.
 #include "wp_common.cuh"
 
+#include <cstdint>
+
 #include <cstdio>
 #include <cstring>
 
@@ -72,6 +74,54 @@ std::vector<Agg> g_agg;
 }  // namespace
 
 void wp_add_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+__global__ void read_small_kernel(unsigned int* __restrict__ dst, const unsigned int* __restrict__ src, size_t words) {
+    for (size_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+}
+struct SmallBuf {
+    void* host = nullptr; // mapped page-locked staging
+    void* dev = nullptr;  // its device address
+    size_t cap = 0;
+    ~SmallBuf() {
+        if (host) cudaFreeHost(host);
+    }
+};
+}  // namespace
+
+cudaError_t wp_read_small(void* host, const void* dev, size_t bytes, cudaStream_t s) {
+    // one staging buffer per host thread (each call completes before returning), mapped and portable
+    // so that a kernel on any device stores into it: the readback then takes no copy engine, and a
+    // large transfer that another stream has queued on the engines cannot delay it
+    thread_local SmallBuf buf;
+    if (bytes == 0) return cudaSuccess;
+    if (buf.cap < bytes) {
+        if (buf.host) cudaFreeHost(buf.host);
+        buf.host = buf.dev = nullptr;
+        buf.cap = 0;
+        const size_t cap = bytes < 4096 ? 4096 : (bytes + 3) / 4 * 4;
+        if (cudaHostAlloc(&buf.host, cap, cudaHostAllocMapped | cudaHostAllocPortable) == cudaSuccess &&
+            cudaHostGetDevicePointer(&buf.dev, buf.host, 0) == cudaSuccess) {
+            buf.cap = cap;
+        } else {
+            if (buf.host) cudaFreeHost(buf.host);
+            buf.host = buf.dev = nullptr;
+        }
+        (void)cudaGetLastError();
+    }
+    cudaError_t e;
+    if (buf.cap >= bytes && bytes % 4 == 0 && ((uintptr_t)dev & 3u) == 0) {
+        read_small_kernel<<<1, 128, 0, s>>>((unsigned int*)buf.dev, (const unsigned int*)dev, bytes / 4);
+        wp_add_launches(1);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) memcpy(host, buf.host, bytes);
+    } else {
+        e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    return e;
+}
 
 int wp_prof_start(cudaStream_t s) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
