@@ -128,12 +128,18 @@ typedef struct wp_mg_params {
                          graph whose while-node repeats cycle + defect + convergence test, no host
                          round trip per cycle); 1: the host tests convergence after every cycle.
                          Both give the same iterates, cycle counts and residual history. */
+    int inner_cycles; /* WP_PREC_MIXED: FP32 V-cycles per refinement step (0 or 1: one; 2: the
+                         FP32 correction equation is solved with two cycles before the FP64 update
+                         and defect, which halves the FP64 defect passes; the tolerance is then
+                         tested every inner_cycles cycles and history[] holds one entry per step) */
 } wp_mg_params;
 
 typedef struct wp_mg_report {
     int cycles;             /* V-cycles executed */
     double rel_residual;    /* final ||f - A p|| / ||f|| (FP64) */
-    double history[64];     /* per-cycle relative residual (first min(cycles,64)) */
+    double history[64];     /* relative residual after each refinement step (each V-cycle outside
+                               WP_PREC_MIXED with inner_cycles > 1); first min(steps,64) */
+    int steps;              /* entries of history written (= cycles unless inner_cycles > 1) */
 } wp_mg_report;
 
 typedef struct wp_mgfrac3d wp_mgfrac3d;

@@ -97,3 +97,26 @@ def test_uniform_rows_match_oracle_per_cycle(wp, oracle, case):
     dst32 = torch.zeros(f.shape, device="cuda")
     rep32 = mg.SolveTol(dst32, None, T(f), rel_tol=0.0, max_cycles=6, precision=wp.PREC_FP32)
     np.testing.assert_allclose(rep32["history"][:4], ohist[:4], rtol=1e-3)
+
+
+@pytest.mark.parametrize("start", [0, 1])
+def test_inner_cycles_reach_tolerance_on_both_loops(wp, oracle, start):
+    """Two FP32 V-cycles per refinement step: the oracle's FP64 residual meets the tolerance, the
+    cycle count is even and within two of the one-cycle schedule's, the history has one entry per
+    step, and the device and host loops agree."""
+    nn, h, a, _, f = _sphere_problem(wp, oracle, 64, seed=23)
+    mg = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)
+    tf = T(f)
+    one = _solve(wp, mg, tf, False, rel_tol=1e-10, max_cycles=60, start=start)
+    dev = _solve(wp, mg, tf, False, rel_tol=1e-10, max_cycles=60, start=start, inner_cycles=2)
+    host = _solve(wp, mg, tf, True, rel_tol=1e-10, max_cycles=60, start=start, inner_cycles=2)
+    _same(dev, host)
+    rep = dev[0]
+    assert rep["status"] == "WP_OK" and rep["cycles"] % 2 == 0 and len(rep["history"]) == rep["cycles"] // 2
+    assert one[0]["cycles"] <= rep["cycles"] <= one[0]["cycles"] + 2
+    from test_gpu_parity import active_cells
+    act = active_cells(*a)
+    fc = f.copy()
+    fc[act] -= f[act].mean()
+    _, r = oracle.frac_residual3d(dev[2], fc, *a, nn, (h,) * 3)
+    assert np.linalg.norm(r) / np.linalg.norm(f) <= 1.5e-10

@@ -31,11 +31,13 @@ class WPError(RuntimeError):
 class MgParams(ctypes.Structure):
     _fields_ = [("max_cycles", ctypes.c_int), ("nu1", ctypes.c_int), ("nu2", ctypes.c_int),
                 ("omega", ctypes.c_double), ("rel_tol", ctypes.c_double), ("precision", ctypes.c_int),
-                ("prolongation", ctypes.c_int), ("start", ctypes.c_int), ("host_loop", ctypes.c_int)]
+                ("prolongation", ctypes.c_int), ("start", ctypes.c_int), ("host_loop", ctypes.c_int),
+                ("inner_cycles", ctypes.c_int)]
 
 
 class MgReport(ctypes.Structure):
-    _fields_ = [("cycles", ctypes.c_int), ("rel_residual", ctypes.c_double), ("history", ctypes.c_double * 64)]
+    _fields_ = [("cycles", ctypes.c_int), ("rel_residual", ctypes.c_double), ("history", ctypes.c_double * 64),
+                ("steps", ctypes.c_int)]
 
 
 _lib = None

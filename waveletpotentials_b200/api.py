@@ -169,7 +169,7 @@ class CuWaveletPotentialRecover2D:
 
 
 def _report(r: MgReport) -> dict:
-    return {"cycles": r.cycles, "rel_residual": r.rel_residual, "history": list(r.history[:min(r.cycles, 64)])}
+    return {"cycles": r.cycles, "rel_residual": r.rel_residual, "history": list(r.history[:min(r.steps, 64)])}
 
 
 class CuMultigridFrac3D:
@@ -194,10 +194,10 @@ class CuMultigridFrac3D:
 
     def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
                  precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, start=START_ZERO,
-                 host_loop=False, stream=None) -> dict:
+                 host_loop=False, inner_cycles=1, stream=None) -> dict:
         c = self.cells
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), int(precision),
-                       int(prolongation), int(start), int(bool(host_loop)))
+                       int(prolongation), int(start), int(bool(host_loop)), int(inner_cycles))
         rep = MgReport()
         st = lib().wp_mgfrac3d_solve_tol(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), ctypes.byref(prm),
                                          ctypes.byref(rep), _stream(stream))
@@ -285,10 +285,10 @@ class CuMultigridFrac2D:
 
     def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
                  precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, start=START_ZERO,
-                 host_loop=False, stream=None) -> dict:
+                 host_loop=False, inner_cycles=1, stream=None) -> dict:
         c = self.cells
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), int(precision),
-                       int(prolongation), int(start), int(bool(host_loop)))
+                       int(prolongation), int(start), int(bool(host_loop)), int(inner_cycles))
         rep = MgReport()
         st = lib().wp_mgfrac2d_solve_tol(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), ctypes.byref(prm),
                                          ctypes.byref(rep), _stream(stream))
@@ -495,7 +495,8 @@ class Projector3D:
 
     def __init__(self, ax, ay, az, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
                  precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, autotune=True, warm_start=None, sdf=None,
-                 start=START_ZERO, host_loop=False, stream=None):
+                 start=START_ZERO, host_loop=False, inner_cycles=1,
+                 stream=None):
         self.dim = _dims3(dim)
         self.dx = _dx3(dx)
         self.ax, self.ay, self.az = ax, ay, az
@@ -507,7 +508,7 @@ class Projector3D:
             self.mg.Autotune(stream)
         self.rec = CuWaveletPotentialRecover3D(self.dim, self.dx, "n")
         self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
-                         prolongation=prolongation, start=start, host_loop=host_loop)
+                         prolongation=prolongation, start=start, host_loop=host_loop, inner_cycles=inner_cycles)
         s = mac_shapes3d(*self.dim)
         self.shapes = s
         self.b = torch.empty(s["p"], device="cuda", dtype=torch.float32)
@@ -595,14 +596,15 @@ class Projector2D:
     """2D form of Projector3D (CuMultigridFrac2D + CuWaveletPotentialRecover2D)."""
 
     def __init__(self, ax, ay, dim, dx, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, start=START_ZERO, host_loop=False, stream=None):
+                 precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, start=START_ZERO, host_loop=False, inner_cycles=1,
+                 stream=None):
         self.dim = tuple(int(v) for v in dim)
         self.dx = float(dx)
         self.ax, self.ay = ax, ay
         self.mg = CuMultigridFrac2D(ax, ay, self.dim, self.dx, "n", stream)
         self.rec = CuWaveletPotentialRecover2D(self.dim, self.dx, "n")
         self.opts = dict(rel_tol=rel_tol, max_cycles=max_cycles, nu1=nu1, nu2=nu2, weight=weight, precision=precision,
-                         prolongation=prolongation, start=start, host_loop=host_loop)
+                         prolongation=prolongation, start=start, host_loop=host_loop, inner_cycles=inner_cycles)
         s = mac_shapes2d(*self.dim)
         self.b = torch.empty(s["p"], device="cuda", dtype=torch.float32)
         self.p = torch.empty(s["p"], device="cuda", dtype=torch.float32)

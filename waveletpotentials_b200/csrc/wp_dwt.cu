@@ -137,6 +137,18 @@ struct TileGeom {
     int contiguous; // 1: lines are contiguous (y axis)
 };
 
+// Reflection tables: for every level, the (index, sign) of each pair a boundary window reads,
+// k = -4 .. nch CH + 3 (entry k + 4), computed once per CTA; a boundary window then costs one table
+// read per tap instead of the reflection rules.  Entries per level: nch CH + 8.
+__host__ __device__ inline int rt_level_entries(int M) { return (M + CH - 1) / CH * CH + 8; }
+__host__ __device__ inline int rt_entries(int N, int levels, bool fwd) {
+    const int ext = N & 1;
+    int e = 0;
+    for (int l = 2; l < levels; ++l) e += rt_level_entries(fwd ? (1 << l) + ext : (1 << l) + ext);
+    return e;
+}
+__host__ __device__ inline size_t rt_offset(size_t buf_bytes) { return (buf_bytes + 15) / 16 * 16; }
+
 template <int WAV, bool FWD, typename T, int C>
 __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src, T* __restrict__ dst, int N,
                                                       int levels, int bcd, TileGeom g) {
@@ -149,20 +161,71 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
     const long obase = (long)blockIdx.y * g.s_out;
     T* buf[3] = {sm, sm + (size_t)N * CP, sm + 2 * (size_t)N * CP};
 
-    // ---- load the tile: C lines of N samples
+    // ---- reflection tables of every level (see rt_entries), ascending level order
+    int4* rt = reinterpret_cast<int4*>(smem_raw + rt_offset((size_t)(FWD ? 2 : 3) * N * CP * sizeof(T)));
+    {
+        int off = 0;
+        for (int l = 2; l < levels; ++l) {
+            const int ne = rt_level_entries((1 << l) + ext);
+            const int L = FWD ? (1 << (l + 1)) : (1 << l);
+            for (int e = tid; e < ne; e += NT) {
+                int ai, di;
+                float sa, sd;
+                if (FWD) {
+                    fwd_reflect<WAV>(e - 4, L, bcd, ai, di, sa, sd);
+                    ai = clampi(ai, 0, L + ext - 1);
+                    di = clampi(di, 0, L + ext - 1);
+                } else {
+                    inv_reflect<WAV>(e - 4, L, bcd, ai, di, sa, sd);
+                    ai = clampi(ai, 0, L + ext - 1);
+                    di = clampi(di, 0, L - 1);
+                }
+                rt[off + e] = make_int4(ai, di, __float_as_int(sa), __float_as_int(sd));
+            }
+            off += ne;
+        }
+    }
+
+    // ---- load the tile: C lines of N samples, LU independent loads in flight per thread (a loop
+    // of single loads, each waited for before the next, left the pass latency bound)
+    constexpr int LU = 8;
     if (g.contiguous) {
         // one warp per line: coalesced along the line, no index division
         for (int col = tid >> 5; col < C; col += NT / 32) {
             const bool ok = i0 + col < g.ni;
             const T* line = src + obase + (long)(ok ? i0 + col : 0) * g.s_in;
-            for (int p = tid & 31; p < N; p += 32) buf[0][p * CP + col] = ok ? line[p] : T(0);
+            for (int p0 = tid & 31; p0 < N; p0 += 32 * LU) {
+                T v[LU];
+#pragma unroll
+                for (int u = 0; u < LU; ++u) {
+                    const int p = p0 + 32 * u;
+                    v[u] = (ok && p < N) ? line[p] : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < LU; ++u) {
+                    const int p = p0 + 32 * u;
+                    if (p < N) buf[0][p * CP + col] = v[u];
+                }
+            }
         }
     } else {
-        for (int i = tid; i < C * N; i += NT) {
-            int col = i % C, p = i / C;
-            T v = T(0);
-            if (i0 + col < g.ni) v = src[obase + (long)(i0 + col) * g.s_in + (long)p * g.pstride];
-            buf[0][p * CP + col] = v;
+        // NT is a multiple of C: a thread keeps its column, positions advance by NT / C
+        const int col = tid % C;
+        const bool ok = i0 + col < g.ni;
+        const T* cs = src + obase + (long)(ok ? i0 + col : 0) * g.s_in;
+        constexpr int PS = NT / C;
+        for (int p0 = tid / C; p0 < N; p0 += PS * LU) {
+            T v[LU];
+#pragma unroll
+            for (int u = 0; u < LU; ++u) {
+                const int p = p0 + PS * u;
+                v[u] = (ok && p < N) ? cs[(long)p * g.pstride] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < LU; ++u) {
+                const int p = p0 + PS * u;
+                if (p < N) buf[0][p * CP + col] = v[u];
+            }
         }
     }
     __syncthreads();
@@ -171,11 +234,14 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
     int outbuf;
     if (FWD) {
         int cur = 0;
+        int rt_off = 0;
+        for (int l = 2; l < levels; ++l) rt_off += rt_level_entries((1 << l) + ext);
         for (int l = levels - 1; l >= 2; --l) {
+            rt_off -= rt_level_entries((1 << l) + ext);
+            const int4* tb = rt + rt_off;
             const int L = 1 << (l + 1);
             const int M = (L >> 1) + ext;
             const int nd = L >> 1;
-            const int lim = L + ext - 1;
             const T* S = buf[cur];
             T* D = buf[cur ^ 1];
             const int nch = (M + CH - 1) / CH;
@@ -193,12 +259,9 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                 } else {
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) {
-                        int ai, di; float sa, sd;
-                        fwd_reflect<WAV>(k0 - 4 + w, L, bcd, ai, di, sa, sd);
-                        ai = clampi(ai, 0, lim);
-                        di = clampi(di, 0, lim);
-                        A[w] = T(sa) * S[ai * CP + col];
-                        Dd[w] = T(sd) * S[di * CP + col];
+                        const int4 e = tb[k0 + w];
+                        A[w] = T(__int_as_float(e.z)) * S[e.x * CP + col];
+                        Dd[w] = T(__int_as_float(e.w)) * S[e.y * CP + col];
                     }
                 }
                 if (WAV == WP_ID_CDF3_7) {
@@ -264,7 +327,10 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
         }
         __syncthreads();
         int cur = 1;
+        int rt_off = 0;
         for (int l = 2; l < levels; ++l) {
+            const int4* tb = rt + rt_off;
+            rt_off += rt_level_entries((1 << l) + ext);
             const int L = 1 << l;
             const int NA = L + ext;
             const T* Sa = buf[cur];
@@ -286,14 +352,11 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                 } else {
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) {
-                        int ai, di; float sa, sd;
-                        inv_reflect<WAV>(k0 - 4 + w, L, bcd, ai, di, sa, sd);
-                        ai = clampi(ai, 0, NA - 1);
-                        di = clampi(di, 0, L - 1);
-                        A[w] = Sa[ai * CP + col];
-                        Dd[w] = Sd[di * CP + col];
-                        SA[w] = T(sa);
-                        SD[w] = T(sd);
+                        const int4 e = tb[k0 + w];
+                        A[w] = Sa[e.x * CP + col];
+                        Dd[w] = Sd[e.y * CP + col];
+                        SA[w] = T(__int_as_float(e.z));
+                        SD[w] = T(__int_as_float(e.w));
                     }
                 }
                 if (WAV == WP_ID_CDF3_7) {
@@ -393,9 +456,14 @@ cudaError_t ensure_constants() {
     return cudaSuccess;
 }
 
+template <typename T>
+size_t dwt_smem(int N, int levels, bool fwd, int C) {
+    return rt_offset((size_t)(fwd ? 2 : 3) * N * (C + 1) * sizeof(T)) + 16 * (size_t)rt_entries(N, levels, fwd);
+}
+
 template <int WAV, bool FWD, typename T, int C>
 cudaError_t launch_one(const T* src, T* dst, int N, int levels, int bcd, TileGeom g, int nouter, cudaStream_t s) {
-    const size_t smem = (size_t)(FWD ? 2 : 3) * N * (C + 1) * sizeof(T);
+    const size_t smem = dwt_smem<T>(N, levels, FWD, C);
     auto kern = dwt_tile_kernel<WAV, FWD, T, C>;
     cudaError_t e = wp_set_smem(kern, smem);
     if (e != cudaSuccess) return e;
@@ -427,11 +495,10 @@ template <int WAV, bool FWD, typename T>
 cudaError_t launch_c(const T* src, T* dst, int N, int levels, int bcd, TileGeom g, int nouter, cudaStream_t s) {
     // widest tile whose staging fits ~100 KB (two CTAs per SM) while keeping >= 2 CTAs per SM busy,
     // unless the autotuner measured another width for this shape
-    const int nbuf = FWD ? 2 : 3;
     int C = 32;
     const long sms = wp_sm_count();
     while (C > 4) {
-        const size_t smem = (size_t)nbuf * N * (C + 1) * sizeof(T);
+        const size_t smem = dwt_smem<T>(N, levels, FWD, C);
         const long ctas = (long)((g.ni + C - 1) / C) * nouter;
         if (smem <= 100 * 1024 && ctas >= 2 * sms) break;
         C >>= 1;
@@ -443,7 +510,7 @@ cudaError_t launch_c(const T* src, T* dst, int N, int levels, int bcd, TileGeom 
         auto it = g_c_cache.find(c_key(WAV, FWD, (int)sizeof(T), N, g, nouter));
         if (it != g_c_cache.end()) C = it->second;
     }
-    const size_t smem = (size_t)nbuf * N * (C + 1) * sizeof(T);
+    const size_t smem = dwt_smem<T>(N, levels, FWD, C);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     switch (C) {
         case 32: return launch_one<WAV, FWD, T, 32>(src, dst, N, levels, bcd, g, nouter, s);
@@ -503,9 +570,8 @@ wp_status wp_dwt_axis_tune(T* buf, int DX, int DY, int DZ, int levels, char axis
     float best = 1e30f;
     int best_c = -1;
     wp_status st = WP_OK;
-    const int nbuf = forward ? 2 : 3;
     for (int C = 4; C <= 32 && st == WP_OK; C *= 2) {
-        if ((size_t)nbuf * N * (C + 1) * sizeof(T) > 227 * 1024) break;
+        if (dwt_smem<T>(N, levels, forward != 0, C) > 227 * 1024) break;
         t_force_c = C;
         std::vector<float> t;
         for (int r = 0; r < 4 && st == WP_OK; ++r) {

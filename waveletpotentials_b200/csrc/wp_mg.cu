@@ -1186,7 +1186,7 @@ __global__ void __launch_bounds__(1024) coarse_cycle_kernel(CPack<T> P, int nu1,
 // and no global loads: with v padded by one z plane on either side, the six neighbours are
 // i -+ 1, i -+ ny, i -+ nx ny, and a skipped face contributes 0 * (a finite neighbour).
 constexpr int kCcf = 8;
-constexpr size_t kLeanSmemMax = 227 * 1024;
+constexpr size_t kLeanSmemMax = 226 * 1024;  // dynamic part; the level descriptors are static shared memory
 
 __global__ void cc_coeff_kernel(float* __restrict__ out, Lvl<float> L) {
     const int nx = L.nx, ny = L.ny, nz = L.nz, cells = nx * ny * nz;
@@ -1354,13 +1354,20 @@ __device__ __forceinline__ void lean_prolong(const LS& F, const LS& C, int prolo
 }
 
 // coarse_cycle_kernel<float> on the precomputed stencils, everything in shared memory: the same
-// cycle, the same arithmetic per cell, the same output buffer
+// cycle, the same arithmetic per cell, the same output buffer.  The pack's stencils are one
+// contiguous global block (the levels of at most kCoarseCells cells are allocated together, in
+// level order), copied with 128-bit loads that keep many requests in flight; the level
+// descriptors live in shared memory (no local-memory arrays), and thread 0 writes back the
+// ping-pong state of a level after its sweeps (every thread swaps its own copy in lockstep).
 __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu1, int nu2, float w, int citers,
                                                                  int prolong) {
     extern __shared__ __align__(16) float lean_smem[];
-    LS S[kCoarseMax];
-    {
-        long off = 0;
+    __shared__ LS S[kCoarseMax];
+    const int tid = threadIdx.x, B = blockDim.x;
+    long cf_floats = 0;
+    for (int l = 0; l < P.n; ++l) cf_floats += (long)kCcf * P.lv[l].nx * P.lv[l].ny * P.lv[l].nz;
+    if (tid == 0) {
+        long cfo = 0, off = cf_floats;
         for (int l = 0; l < P.n; ++l) {
             LS& q = S[l];
             q.nx = P.lv[l].nx;
@@ -1368,30 +1375,45 @@ __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu
             q.nz = P.lv[l].nz;
             q.nxy = q.nx * q.ny;
             q.cells = q.nxy * q.nz;
+            q.cf = lean_smem + cfo;
+            cfo += (long)kCcf * q.cells;
             q.v = lean_smem + off + q.nxy;
             off += q.cells + 2 * q.nxy;
             q.t = lean_smem + off + q.nxy;
             off += q.cells + 2 * q.nxy;
             q.f = lean_smem + off;
             off += q.cells;
-            float* cf = lean_smem + off;
-            off += (long)kCcf * q.cells;
-            const float* g = P.lv[l].ccf;
-            for (int i = threadIdx.x; i < kCcf * q.cells; i += blockDim.x) cf[i] = g[i];
-            q.cf = cf;
-            // padding planes stay zero; level 0 starts from v = 0 and the global f
-            for (int i = threadIdx.x; i < q.cells + 2 * q.nxy; i += blockDim.x) {
-                q.v[i - q.nxy] = 0.f;
-                q.t[i - q.nxy] = 0.f;
-            }
-            if (l == 0)
-                for (int i = threadIdx.x; i < q.cells; i += blockDim.x) q.f[i] = P.lv[0].f[i];
         }
-        __syncthreads();
     }
-    const int tid = threadIdx.x, B = blockDim.x;
+    {
+        // stencils: one flat 128-bit copy (every level's block is a multiple of 16 bytes)
+        const float4* g = reinterpret_cast<const float4*>(P.lv[0].ccf);
+        float4* d = reinterpret_cast<float4*>(lean_smem);
+        const int n4 = (int)(cf_floats / 4);
+        int i = tid;
+        for (; i + 3 * B < n4; i += 4 * B) {
+            const float4 a0 = g[i], a1 = g[i + B], a2 = g[i + 2 * B], a3 = g[i + 3 * B];
+            d[i] = a0;
+            d[i + B] = a1;
+            d[i + 2 * B] = a2;
+            d[i + 3 * B] = a3;
+        }
+        for (; i < n4; i += B) d[i] = g[i];
+    }
+    __syncthreads();
+    for (int l = 0; l < P.n; ++l) {
+        // padding planes stay zero; level 0 starts from v = 0 and the global f
+        const LS q = S[l];
+        for (int i = tid; i < q.cells + 2 * q.nxy; i += B) {
+            q.v[i - q.nxy] = 0.f;
+            q.t[i - q.nxy] = 0.f;
+        }
+        if (l == 0)
+            for (int i = tid; i < q.cells; i += B) q.f[i] = P.lv[0].f[i];
+    }
+    __syncthreads();
     for (int l = 0; l < P.n - 1; ++l) {
-        LS& L = S[l];
+        LS L = S[l];
         if (l > 0) {
             for (int i = tid; i < L.cells; i += B) L.v[i] = 0.f;
             __syncthreads();
@@ -1404,10 +1426,14 @@ __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu
             L.t = tmp;
         }
         lean_restrict(L, S[l + 1]);
+        if (tid == 0) {
+            S[l].v = L.v;
+            S[l].t = L.t;
+        }
         __syncthreads();
     }
     {
-        LS& L = S[P.n - 1];
+        LS L = S[P.n - 1];
         if (P.n > 1) {
             for (int i = tid; i < L.cells; i += B) L.v[i] = 0.f;
             __syncthreads();
@@ -1427,7 +1453,6 @@ __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu
                 L.v = L.t;
                 L.t = tmp;
             }
-            __syncthreads();
         } else {
             for (int k = 0; k < citers; ++k) {
                 lean_sweep(L, L.t, L.v, w, tid, B);
@@ -1437,9 +1462,14 @@ __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu
                 L.t = tmp;
             }
         }
+        if (tid == 0) {
+            S[P.n - 1].v = L.v;
+            S[P.n - 1].t = L.t;
+        }
+        __syncthreads();
     }
     for (int l = P.n - 2; l >= 0; --l) {
-        LS& L = S[l];
+        LS L = S[l];
         lean_prolong(L, S[l + 1], prolong);
         __syncthreads();
         for (int k = 0; k < nu2; ++k) {
@@ -1449,9 +1479,15 @@ __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu
             L.v = L.t;
             L.t = tmp;
         }
+        if (tid == 0) {
+            S[l].v = L.v;
+            S[l].t = L.t;
+        }
+        __syncthreads();
     }
     float* out = ((nu1 + nu2) & 1) ? P.lv[0].t : P.lv[0].v;
-    for (int i = tid; i < S[0].cells; i += B) out[i] = S[0].v[i];
+    const float* v0 = S[0].v;
+    for (int i = tid; i < S[0].cells; i += B) out[i] = v0[i];
 }
 
 // coarse f = spacing-weighted average of the fine residuals of the (up to 8) children
@@ -1879,6 +1915,7 @@ struct wp_mgfrac3d {
     float* r32;        // FP32 defect (right-hand side of correction cycles)
     const float* fin;  // finest right-hand side of the current solve
     const double* fin64;
+    float* ccf_all;    // the coarse levels' stencils (Level::ccf points into it)
     int tune_gen;      // bumped by every change of a level's tile or kernel variant
     // device-side cycle loop of the mixed-precision tolerance solve (see solve_mixed_graph)
     cudaGraph_t loop_graph;
@@ -1887,7 +1924,7 @@ struct wp_mgfrac3d {
     cudaStream_t loop_cap; // private stream the loop is captured on (capture needs a non-default stream)
     int loop_broken;   // capture or instantiation failed once: the host loop is used from then on
     const float* loop_f;
-    int loop_key[6];   // nu1, nu2, prolongation, full-multigrid first cycle, tune_gen, device
+    int loop_key[7];   // nu1, nu2, prolongation, full-multigrid first cycle, tune_gen, device, inner cycles
     double loop_omega;
     long long loop_launches[2]; // kernels of the first cycle's graph part and of one loop body
 };
@@ -1960,11 +1997,6 @@ wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, cons
         WP_CUDA_TRY(cudaMalloc((void**)&L.tab32, sizeof(float) * t32.size()));
         WP_CUDA_TRY(cudaMemcpy(L.tab64, t64.data(), sizeof(double) * t64.size(), cudaMemcpyHostToDevice));
         WP_CUDA_TRY(cudaMemcpy(L.tab32, t32.data(), sizeof(float) * t32.size(), cudaMemcpyHostToDevice));
-        if (L.cells <= kCoarseCells) {
-            WP_CUDA_TRY(cudaMalloc((void**)&L.ccf, sizeof(float) * kCcf * L.cells));
-            WP_KERNEL("cc_coeff", 40.0 * L.cells, s,
-                      cc_coeff_kernel<<<wp_cdiv(L.cells, 256), 256, 0, s>>>(L.ccf, view<float>(L)));
-        }
         WP_CUDA_TRY(cudaMalloc((void**)&L.v, sizeof(float) * L.cells));
         WP_CUDA_TRY(cudaMalloc((void**)&L.t, sizeof(float) * L.cells));
         WP_CUDA_TRY(cudaMalloc((void**)&L.f, sizeof(float) * L.cells));
@@ -1980,6 +2012,23 @@ wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, cons
         }
     }
     h->nl = nl;
+    // per-cell stencils of the levels of at most kCoarseCells cells (a suffix of the hierarchy), in
+    // one block in level order so that any coarse-cycle pack finds its stencils contiguous
+    long cf = 0;
+    for (int l = 0; l < nl; ++l)
+        if (h->lv[l].cells <= kCoarseCells) cf += (long)kCcf * h->lv[l].cells;
+    if (cf > 0) {
+        WP_CUDA_TRY(cudaMalloc((void**)&h->ccf_all, sizeof(float) * cf));
+        long off = 0;
+        for (int l = 0; l < nl; ++l) {
+            Level& L = h->lv[l];
+            if (L.cells > kCoarseCells) continue;
+            L.ccf = h->ccf_all + off;
+            off += (long)kCcf * L.cells;
+            WP_KERNEL("cc_coeff", 40.0 * L.cells, s,
+                      cc_coeff_kernel<<<wp_cdiv(L.cells, 256), 256, 0, s>>>(L.ccf, view<float>(L)));
+        }
+    }
     return WP_OK;
 }
 
@@ -2253,9 +2302,10 @@ void destroy_levels(wp_mgfrac3d* h) {
     for (int l = 0; l < kMaxLevels; ++l) {
         Level& L = h->lv[l];
         for (int a = 0; a < 3; ++a) if (L.frac[a]) cudaFree(L.frac[a]);
-        void* ps[] = {L.tab64, L.tab32, L.fyc, L.uni, L.ccf, L.v, L.t, L.f, L.v64, L.t64, L.f64};
+        void* ps[] = {L.tab64, L.tab32, L.fyc, L.uni, L.v, L.t, L.f, L.v64, L.t64, L.f64};
         for (void* p : ps) if (p) cudaFree(p);
     }
+    if (h->ccf_all) cudaFree(h->ccf_all);
     if (h->acc) cudaFree(h->acc);
     if (h->p64) cudaFree(h->p64);
     if (h->r32) cudaFree(h->r32);
@@ -2304,18 +2354,48 @@ wp_status solve_fixed(wp_mgfrac3d* h, float* dst, const float* pre_v, const floa
     return WP_OK;
 }
 
+int inner_of(const wp_mg_params* prm) { return prm->inner_cycles > 1 ? prm->inner_cycles : 1; }
+
+// The correction of one refinement step of the mixed solve: inner_cycles FP32 V-cycles on
+// A e = r32 (the first from e = 0, or a full-multigrid start), then p64 += e -- fused into the
+// last post-sweep where the level's kernel allows, add_correction_kernel otherwise.
+wp_status mixed_correction(wp_mgfrac3d* h, const wp_mg_params* prm, bool fmg, cudaStream_t s) {
+    Level& L = h->lv[0];
+    const long n = L.cells;
+    const int inner = inner_of(prm);
+    bool added = false;
+    for (int j = 0; j < inner; ++j) {
+        double* acc = j == inner - 1 ? h->p64 : nullptr;
+        bool* ad = j == inner - 1 ? &added : nullptr;
+        wp_status st;
+        if (j == 0 && fmg)
+            st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, acc, ad);
+        else
+            st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, j == 0, acc,
+                               ad);
+        if (st != WP_OK) return st;
+    }
+    if (!added) {
+        const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
+        WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+    }
+    return WP_OK;
+}
+
 // State of the device-side cycle loop: the stopping rule of solve_tol's host loop, evaluated by
-// mg_loop_check_kernel after every defect.
+// mg_loop_check_kernel after every defect (cycles advance by `inner` per refinement step).
 struct MgLoop {
-    int cycles, max_cycles, use_tol, pad;
+    int cycles, max_cycles, use_tol, inner, steps, pad;
     double tol, rel;
     double hist[64];
 };
 
-__global__ void mg_loop_init_kernel(MgLoop* st, int max_cycles, int use_tol, double tol) {
+__global__ void mg_loop_init_kernel(MgLoop* st, int max_cycles, int use_tol, double tol, int inner) {
     st->cycles = 0;
+    st->steps = 0;
     st->max_cycles = max_cycles;
     st->use_tol = use_tol;
+    st->inner = inner;
     st->tol = tol;
     st->rel = 0.0;
 }
@@ -2327,11 +2407,12 @@ __global__ void mg_loop_check_kernel(MgLoop* st, const double* __restrict__ acc,
     double nf2 = acc[1];
     if (!(nf2 > 0.0)) nf2 = 1.0;
     const double rel = sqrt(acc[0] / nf2);
-    const int c = st->cycles;
-    if (c < 64) st->hist[c] = rel;
-    st->cycles = c + 1;
+    const int k = st->steps, c = st->cycles + st->inner;
+    if (k < 64) st->hist[k] = rel;
+    st->steps = k + 1;
+    st->cycles = c;
     st->rel = rel;
-    const bool go = !(st->use_tol && rel <= st->tol) && c + 1 < st->max_cycles && isfinite(rel);
+    const bool go = !(st->use_tol && rel <= st->tol) && c < st->max_cycles && isfinite(rel);
     cudaGraphSetConditional(hc, go ? 1u : 0u);
 }
 
@@ -2347,19 +2428,8 @@ void destroy_loop_graph(wp_mgfrac3d* h) {
 // one a full-multigrid start if fmg), FP64 update, FP64 defect with the device mean, loop test
 wp_status mixed_step(wp_mgfrac3d* h, const float* f, const wp_mg_params* prm, bool fmg, cudaGraphConditionalHandle hc,
                      cudaStream_t s) {
-    Level& L = h->lv[0];
-    const long n = L.cells;
-    const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
     wp_status st;
-    bool added = false;
-    if (fmg) {
-        st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, h->p64, &added);
-    } else {
-        st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, true, h->p64,
-                           &added);
-    }
-    if (st != WP_OK) return st;
-    if (!added) WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+    if ((st = mixed_correction(h, prm, fmg, s)) != WP_OK) return st;
     if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
     WP_KERNEL("mg_loop_check", 0.0, s, mg_loop_check_kernel<<<1, 1, 0, s>>>((MgLoop*)h->loop_state, h->acc, hc));
     return WP_OK;
@@ -2431,7 +2501,7 @@ wp_status build_loop_graph(wp_mgfrac3d* h, const float* f, const wp_mg_params* p
     int dev = 0;
     cudaGetDevice(&dev);
     h->loop_f = f;
-    const int key[6] = {prm->nu1, prm->nu2, prm->prolongation, fmg ? 1 : 0, h->tune_gen, dev};
+    const int key[7] = {prm->nu1, prm->nu2, prm->prolongation, fmg ? 1 : 0, h->tune_gen, dev, inner_of(prm)};
     memcpy(h->loop_key, key, sizeof(key));
     h->loop_omega = prm->omega;
     return WP_OK;
@@ -2440,7 +2510,7 @@ wp_status build_loop_graph(wp_mgfrac3d* h, const float* f, const wp_mg_params* p
 bool loop_graph_ready(const wp_mgfrac3d* h, const float* f, const wp_mg_params* prm, bool fmg) {
     int dev = 0;
     cudaGetDevice(&dev);
-    const int key[6] = {prm->nu1, prm->nu2, prm->prolongation, fmg ? 1 : 0, h->tune_gen, dev};
+    const int key[7] = {prm->nu1, prm->nu2, prm->prolongation, fmg ? 1 : 0, h->tune_gen, dev, inner_of(prm)};
     return h->loop_exec && h->loop_f == f && memcmp(key, h->loop_key, sizeof(key)) == 0 && h->loop_omega == prm->omega;
 }
 
@@ -2454,13 +2524,14 @@ wp_status solve_mixed_graph(wp_mgfrac3d* h, const float* f, const wp_mg_params* 
     }
     WP_KERNEL("mg_loop_init", 0.0, s,
               mg_loop_init_kernel<<<1, 1, 0, s>>>((MgLoop*)h->loop_state, prm->max_cycles, prm->rel_tol > 0.0 ? 1 : 0,
-                                                  prm->rel_tol));
+                                                  prm->rel_tol, inner_of(prm)));
     WP_CUDA_TRY(cudaGraphLaunch(h->loop_exec, s));
     MgLoop out;
     WP_CUDA_TRY(wp_read_small(&out, h->loop_state, sizeof(out), s));
-    wp_add_launches(h->loop_launches[0] + (long long)(out.cycles > 0 ? out.cycles - 1 : 0) * h->loop_launches[1]);
+    wp_add_launches(h->loop_launches[0] + (long long)(out.steps > 0 ? out.steps - 1 : 0) * h->loop_launches[1]);
     r->cycles = out.cycles;
-    for (int c = 0; c < out.cycles && c < 64; ++c) r->history[c] = out.hist[c];
+    r->steps = out.steps;
+    for (int c = 0; c < out.steps && c < 64; ++c) r->history[c] = out.hist[c];
     r->rel_residual = out.rel;
     return WP_OK;
 }
@@ -2512,7 +2583,7 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
             if (st != WP_OK) return st;
             rel = std::sqrt(nr2 / nf2);
             if (r.cycles < 64) r.history[r.cycles] = rel;
-            ++r.cycles;
+            r.steps = ++r.cycles;
             if (!std::isfinite(rel)) break;
         }
         r.rel_residual = rel;
@@ -2543,24 +2614,17 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
                 on_device = true;
             }
         }
+        int steps = 0;
         while (!on_device && !(use_tol && rel <= prm->rel_tol) && r.cycles < prm->max_cycles) {
-            // one FP32 V-cycle (the first one a full-multigrid start if asked) on the FP32 defect from a
-            // zero start, FP64 update, FP64 defect
-            bool added = false;
-            if (r.cycles == 0 && !pre_v && prm->start == WP_START_FMG) {
-                st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, h->p64,
-                                      &added);
-            } else {
-                st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, true,
-                                   h->p64, &added);
-            }
-            if (st != WP_OK) return st;
-            if (!added)
-                WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+            // one refinement step: FP32 correction cycles (the first one a full-multigrid start if
+            // asked) on the FP32 defect, FP64 update, FP64 defect
+            if ((st = mixed_correction(h, prm, r.cycles == 0 && !pre_v && prm->start == WP_START_FMG, s)) != WP_OK)
+                return st;
             if ((st = defect<double>(h, h->p64, f, m, h->r32, &nr2, nullptr, s)) != WP_OK) return st;
             rel = std::sqrt(nr2 / nf2);
-            if (r.cycles < 64) r.history[r.cycles] = rel;
-            ++r.cycles;
+            if (steps < 64) r.history[steps] = rel;
+            r.steps = ++steps;
+            r.cycles += inner_of(prm);
             if (!std::isfinite(rel)) break;
         }
         r.rel_residual = rel;
@@ -2600,16 +2664,7 @@ wp_status solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, in
     WP_CUDA_TRY(cudaMemsetAsync(h->p64, 0, sizeof(double) * n, s));
     if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, true, s)) != WP_OK) return st;
     for (int c = 0; c < cycles; ++c) {
-        bool added = false;
-        if (c == 0 && prm->start == WP_START_FMG) {
-            st = fmg_start<float>(h, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, h->p64,
-                                  &added);
-        } else {
-            st = vcycle<float>(h, 0, h->r32, prm->nu1, prm->nu2, (float)prm->omega, prm->prolongation, s, true, h->p64,
-                               &added);
-        }
-        if (st != WP_OK) return st;
-        if (!added) WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+        if ((st = mixed_correction(h, prm, c == 0 && prm->start == WP_START_FMG, s)) != WP_OK) return st;
         if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
     }
     h->last64 = 1;
