@@ -100,11 +100,12 @@ def make_problem(n, seed):
     return centers, radii, (xv, yv, zv)
 
 
-# DRAM bytes (read + write) per launch of the finest-level kernels, from one ncu capture each of the
-# profiling commands in profiles/ (256^3 workload); algorithmic bytes per launch are 402.7 MB
-# (Jacobi sweep: v, f, three fraction arrays read, v written: 24 B/cell x 16,777,216 cells)
+# DRAM bytes (read + write) per launch of the finest-level Jacobi sweep, from one ncu capture of the
+# profiling command in profiles/jacobi_q_256_level0.md (256^3 workload).  Algorithmic bytes per
+# launch (226.0 MB): 12 B/cell (v and f read, v written) x 16,777,216 cells + 12 B/cell of face
+# fractions for the rows that are not uniform (12.2% of the (x, z) rows) + 1 B per row flag.
 NCU_TRAFFIC = {
-    ("jacobi_finest", 256): (423194624, "profiles/jacobi_q_256_level0.md (337.2 MB read + 86.0 MB write)"),
+    ("jacobi_finest", 256): (222187520, "profiles/jacobi_q_256_level0.md (173.6 MB read + 48.6 MB write)"),
 }
 
 
