@@ -707,7 +707,9 @@ def main():
         "solve": {"vcycles": reps[-1]["cycles"], "rel_residual": reps[-1]["rel_residual"],
                   "max_abs_div": reps[-1]["max_abs_div"]},
         "plain": plain,
-        "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} for r in prof[:8]],
+        # every kernel of the event-instrumented steps (ms and algorithmic bytes summed over psteps)
+        "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} for r in prof],
+        "kernel_ms_per_step": round(sum(r["ms"] for r in prof) / psteps, 4),
         "mg_tiles": {"z_chunks_per_level": tiles[0], "variants_per_level": tiles[1], "tuned_ms_per_level": tiles[2]},
     }
     print(json.dumps(out))

@@ -65,6 +65,38 @@ void wp_prof_stop(int tok, const char* name, double bytes, cudaStream_t s);
         wp_prof_stop(_tok, name, (double)(bytes), stream);          \
     } while (0)
 
+// Programmatic dependent launch.  A kernel that calls wp_pdl_enter() first waits until the grid
+// launched before it on the stream has completed and its memory is visible (griddepcontrol.wait;
+// immediate when there is no programmatic dependency), then lets the grid after it be scheduled
+// (griddepcontrol.launch_dependents) -- that grid's CTAs become resident as this grid's last wave
+// drains, hiding launch latency and tails.  wp_launch_pdl launches with the attribute that allows
+// it (kernel-to-kernel only; on the legacy default stream it launches normally).
+__device__ __forceinline__ void wp_pdl_enter() {
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 900)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" :::);
+#endif
+}
+
+template <typename... KArgs, typename... Args>
+void wp_launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    if (s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
+        kern<<<grid, block, smem, s>>>(static_cast<KArgs>(args)...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 // Raises a kernel's dynamic shared-memory limit once per (kernel, device) (a host-side attribute
 // call, kept out of the launch path so launches can be captured into CUDA graphs).
 cudaError_t wp_set_smem_impl(const void* kernel, size_t bytes);

@@ -313,6 +313,7 @@ struct QCol {
 template <typename T, bool ACC = false>
 __device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ f,
                                               const Lvl<T>& L, T w, int zc, double* __restrict__ p64 = nullptr) {
+    wp_pdl_enter();
     const int nq = L.ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
@@ -345,6 +346,7 @@ __device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __re
 template <typename T>
 __global__ void __launch_bounds__(256) jacobi0_q_kernel(T* __restrict__ dst, const T* __restrict__ f, Lvl<T> L, T w,
                                                         int zc) {
+    wp_pdl_enter();
     const int nq = L.ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
@@ -679,6 +681,7 @@ template <typename T, int MINB = 1>
 __global__ void __launch_bounds__(256, MINB) resid_restrict_q_kernel(T* __restrict__ fc, const T* __restrict__ v,
                                                                      const T* __restrict__ f, Lvl<T> L, int ncx,
                                                                      int ncy, int ncz, int czc) {
+    wp_pdl_enter();
     const int nq = L.ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int cz0 = blockIdx.y * czc, cz1 = min(cz0 + czc, ncz);
@@ -747,6 +750,7 @@ __global__ void __launch_bounds__(256, 2) defect64_q_kernel(float* __restrict__ 
                                                          const float* __restrict__ f, Lvl<double> L, double m,
                                                          const double* __restrict__ msum, double* __restrict__ acc,
                                                          int zc) {
+    wp_pdl_enter();
     const int nq = L.ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
@@ -785,6 +789,7 @@ __global__ void __launch_bounds__(256, 2) defect64_q_kernel(float* __restrict__ 
 template <typename T>
 __global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny,
                                                             int nz, int ncx, int ncy, int ncz) {
+    wp_pdl_enter();
     const int nq = ny >> 2;
     const long q = (long)blockIdx.x * 256 + threadIdx.x;
     const int z = blockIdx.y;
@@ -1361,6 +1366,7 @@ __device__ __forceinline__ void lean_prolong(const LS& F, const LS& C, int prolo
 // ping-pong state of a level after its sweeps (every thread swaps its own copy in lockstep).
 __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu1, int nu2, float w, int citers,
                                                                  int prolong) {
+    wp_pdl_enter();
     extern __shared__ __align__(16) float lean_smem[];
     __shared__ LS S[kCoarseMax];
     const int tid = threadIdx.x, B = blockDim.x;
@@ -1665,6 +1671,7 @@ __global__ void __launch_bounds__(256) sumsq_kernel(const TS* __restrict__ a, lo
 }
 
 __global__ void add_correction_kernel(double* __restrict__ p, const float* __restrict__ e, long n) {
+    wp_pdl_enter();
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] += (double)e[i];
 }
 
@@ -1828,9 +1835,9 @@ void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc
             launch_jacobi_ts(L, (float*)dst, (const float*)src, (const float*)f, (float)w, s);
             return;
         }
-        if (var == 1) jacobi_q_mb_kernel<T, 3><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
-        else if (var == 2) jacobi_q_mb_kernel<T, 4><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
-        else jacobi_q_kernel<T><<<g, 256, 0, s>>>(dst, src, f, V, w, zc);
+        if (var == 1) wp_launch_pdl(jacobi_q_mb_kernel<T, 3>, g, 256, 0, s, dst, src, f, V, w, zc, nullptr);
+        else if (var == 2) wp_launch_pdl(jacobi_q_mb_kernel<T, 4>, g, 256, 0, s, dst, src, f, V, w, zc, nullptr);
+        else wp_launch_pdl(jacobi_q_kernel<T>, g, 256, 0, s, dst, src, f, V, w, zc, nullptr);
     } else {
         jacobi_z_kernel<T, false><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(dst, src, f, V, w, nullptr,
                                                                                           0, 0, zc);
@@ -1848,9 +1855,9 @@ void launch_jacobi_acc(const Level& L, const float* src, const float* f, float w
     const int var = L.var[kZcJacobi];
     const Lvl<float> V = view<float>(L);
     const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
-    if (var == 1) jacobi_q_mb_kernel<float, 3, true><<<g, 256, 0, s>>>(nullptr, src, f, V, w, zc, p64);
-    else if (var == 2) jacobi_q_mb_kernel<float, 4, true><<<g, 256, 0, s>>>(nullptr, src, f, V, w, zc, p64);
-    else jacobi_q_kernel<float, true><<<g, 256, 0, s>>>(nullptr, src, f, V, w, zc, p64);
+    if (var == 1) wp_launch_pdl(jacobi_q_mb_kernel<float, 3, true>, g, 256, 0, s, nullptr, src, f, V, w, zc, p64);
+    else if (var == 2) wp_launch_pdl(jacobi_q_mb_kernel<float, 4, true>, g, 256, 0, s, nullptr, src, f, V, w, zc, p64);
+    else wp_launch_pdl(jacobi_q_kernel<float, true>, g, 256, 0, s, nullptr, src, f, V, w, zc, p64);
 }
 
 // two sweeps dst <- J(J(src)) in one pass (jacobi2_q_kernel)
@@ -1868,9 +1875,10 @@ void launch_resid_restrict(const Level& L, const Level& C, T* fc, const T* v, co
     if (quad_ok(L) && C.n[1] * 2 == L.n[1] && al16(v) && al16(f)) {
         const dim3 g(wp_cdiv((size_t)C.n[0] * (L.n[1] / 4) * 2, 256), wp_cdiv(C.n[2], czc));
         const int var = sizeof(T) == 4 ? L.var[kZcRestrict] : 0;
-        if (var == 1) resid_restrict_q_kernel<T, 3><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
-        else if (var == 2) resid_restrict_q_kernel<T, 4><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
-        else resid_restrict_q_kernel<T><<<g, 256, 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
+        if (var == 1) wp_launch_pdl(resid_restrict_q_kernel<T, 3>, g, 256, 0, s, fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
+        else if (var == 2)
+            wp_launch_pdl(resid_restrict_q_kernel<T, 4>, g, 256, 0, s, fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
+        else wp_launch_pdl(resid_restrict_q_kernel<T>, g, 256, 0, s, fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
     } else {
         const dim3 g(wp_cdiv(L.n[1], 32), wp_cdiv(L.n[0], 8), wp_cdiv(C.n[2], czc));
         resid_restrict_z_kernel<T><<<g, dim3(32, 8), 0, s>>>(fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
@@ -1884,7 +1892,7 @@ void launch_defect64(const Level& L, float* r32, const TP* p, const float* f, do
     const Lvl<double> V = view<double>(L);
     if (quad_ok(L) && al16(r32) && al16(p) && al16(f)) {
         const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
-        defect64_q_kernel<TP><<<g, 256, 0, s>>>(r32, p, f, V, m, msum, acc, zc);
+        wp_launch_pdl(defect64_q_kernel<TP>, g, 256, 0, s, r32, p, f, V, m, msum, acc, zc);
     } else {
         defect64_z_kernel<TP><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(r32, p, f, V, m, msum, acc,
                                                                                        zc);
@@ -1895,7 +1903,7 @@ template <typename T>
 void launch_prolong_tri(const Level& L, const Level& C, T* v, const T* vc, cudaStream_t s) {
     if (quad_ok(L) && al16(v)) {
         const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), L.n[2]);
-        prolong_tri_q_kernel<T><<<g, 256, 0, s>>>(v, vc, L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2]);
+        wp_launch_pdl(prolong_tri_q_kernel<T>, g, 256, 0, s, v, vc, L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2]);
     } else {
         prolong_tri_add_kernel<T><<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(v, vc, L.n[0], L.n[1], L.n[2],
                                                                                          C.n[0], C.n[1], C.n[2]);
@@ -2123,8 +2131,8 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         if (lean && lean_bytes <= kLeanSmemMax) {
             WP_CUDA_TRY(wp_set_smem(coarse_cycle_lean_kernel, kLeanSmemMax));
             WP_KERNEL("coarse_cycle", (double)L.cells * (3.0 * sizeof(T) + 12.0) * (nu1 + nu2 + 2), s,
-                      coarse_cycle_lean_kernel<<<1, 1024, lean_bytes, s>>>(Q, nu1, nu2, (float)w, h->coarsest_iters,
-                                                                            prolong));
+                      wp_launch_pdl(coarse_cycle_lean_kernel, 1, 1024, lean_bytes, s, Q, nu1, nu2, (float)w,
+                                    h->coarsest_iters, prolong));
             for (int k = 0; k < Q.n; ++k) {
                 Level& E = h->lv[l + k];
                 const int swaps = (k == Q.n - 1) ? h->coarsest_iters : nu1 + nu2;
@@ -2161,7 +2169,7 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
                 const int zc = level_zc(L, kZcJacobi);
                 const dim3 gq(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
                 WP_KERNEL(l == 0 ? "jacobi0_finest" : "jacobi0", (double)L.cells * 2.0 * sizeof(T) + frac_bytes(L), s,
-                          jacobi0_q_kernel<T><<<gq, 256, 0, s>>>(Bufs<T>::t(L), f, view<T>(L), w, zc));
+                          wp_launch_pdl(jacobi0_q_kernel<T>, gq, 256, 0, s, Bufs<T>::t(L), f, view<T>(L), w, zc));
                 std::swap(Bufs<T>::v(L), Bufs<T>::t(L));
                 pre = nu1 - 1;
             } else {
@@ -2377,7 +2385,8 @@ wp_status mixed_correction(wp_mgfrac3d* h, const wp_mg_params* prm, bool fmg, cu
     }
     if (!added) {
         const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
-        WP_KERNEL("add_correction", 20.0 * n, s, add_correction_kernel<<<cb, 256, 0, s>>>(h->p64, L.v, n));
+        WP_KERNEL("add_correction", 20.0 * n, s,
+                  wp_launch_pdl(add_correction_kernel, cb, 256, 0, s, h->p64, (const float*)L.v, n));
     }
     return WP_OK;
 }
@@ -2404,6 +2413,7 @@ __global__ void mg_loop_init_kernel(MgLoop* st, int max_cycles, int use_tol, dou
 // recorded as in solve_tol; the loop goes on while the tolerance is not met, the cycle cap not
 // reached and rel is finite
 __global__ void mg_loop_check_kernel(MgLoop* st, const double* __restrict__ acc, cudaGraphConditionalHandle hc) {
+    wp_pdl_enter();
     double nf2 = acc[1];
     if (!(nf2 > 0.0)) nf2 = 1.0;
     const double rel = sqrt(acc[0] / nf2);
@@ -2431,7 +2441,8 @@ wp_status mixed_step(wp_mgfrac3d* h, const float* f, const wp_mg_params* prm, bo
     wp_status st;
     if ((st = mixed_correction(h, prm, fmg, s)) != WP_OK) return st;
     if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
-    WP_KERNEL("mg_loop_check", 0.0, s, mg_loop_check_kernel<<<1, 1, 0, s>>>((MgLoop*)h->loop_state, h->acc, hc));
+    WP_KERNEL("mg_loop_check", 0.0, s,
+              wp_launch_pdl(mg_loop_check_kernel, 1, 1, 0, s, (MgLoop*)h->loop_state, (const double*)h->acc, hc));
     return WP_OK;
 }
 
