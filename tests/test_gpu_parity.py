@@ -393,7 +393,7 @@ def test_mg_offset_views_and_autotune_keep_results(wp, oracle):
     assert rel(N(dst0), N(dst)) < 1e-6
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
 def test_mg_jacobi_variants_agree(wp, oracle, variant):
     """Register-budget variants, the fused two-sweep kernel and the TMA-staged sweep give the same
     cycles as the default one-sweep kernel (up to FP32 contraction order) for every pinned z-chunk."""

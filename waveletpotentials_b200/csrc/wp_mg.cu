@@ -239,6 +239,13 @@ struct QCol {
     }
 
     __device__ __forceinline__ void step(Q4<T>& dg, Q4<T>& od, Q4<T>& c) {
+        Q4<T> vp = zero4<T>();
+        if (z < L.nz - 1) vp = cvt4<T>(ld4(v + i + sxy));
+        step_with(dg, od, c, vp);
+    }
+
+    // one step with the next plane's centre quad vp supplied by the caller (zero above the top)
+    __device__ __forceinline__ void step_with(Q4<T>& dg, Q4<T>& od, Q4<T>& c, const Q4<T> vp) {
         const int ny = L.ny, nz = L.nz;
         const bool zp = z < nz - 1;
         // a row whose faces are all exactly 1 reads no fractions (the same values, without the traffic)
@@ -248,8 +255,7 @@ struct QCol {
         const T vyp = yp ? (T)v[i + 4] : (T)0;
         const Q4<T> vxm = xm ? cvt4<T>(ld4(v + i - ny)) : zero4<T>();
         const Q4<T> vxp = xp ? cvt4<T>(ld4(v + i + ny)) : zero4<T>();
-        Q4<T> vp = zero4<T>(), azu = zero4<T>();
-        if (zp) vp = cvt4<T>(ld4(v + i + sxy));
+        Q4<T> azu = zero4<T>();
         const T gzl = L.glo[2][z], gzh = L.ghi[2][z];
         if (u && xm && xp && z > 0 && zp) {
             // uniform interior row: each face coefficient is its spacing factor (1 x factor), every
@@ -419,6 +425,87 @@ __global__ void __launch_bounds__(256, MINB) jacobi_q_mb_kernel(T* __restrict__ 
                                                                 const T* __restrict__ f, Lvl<T> L, T w, int zc,
                                                                 double* __restrict__ p64 = nullptr) {
     jacobi_q_body<T, ACC>(dst, src, f, L, w, zc, p64);
+}
+
+// The one-sweep quad kernel with its streaming loads issued ahead: every thread keeps a private
+// ring of JP_DEPTH planes in shared memory and fills it with cp.async (16-byte, L2-only) copies of the
+// next planes' centre quad v(z+1) and right-hand side f(z), JP_DEPTH - 1 planes before it uses them,
+// so each warp has several planes of DRAM reads in flight without holding them in registers.  The
+// arithmetic per cell is QCol's (step_with).  No thread reads another's ring slots: no barriers.
+constexpr int JP_DEPTH = 4;
+constexpr size_t jp_smem_bytes(bool acc) { return (size_t)JP_DEPTH * 256 * 16 * (acc ? 4 : 2); }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(wptc::smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// ACC: the swept values are added to the FP64 iterate p64 (jacobi_q_body's ACC form), whose quads
+// stream through the ring as well.
+template <bool ACC = false>
+__global__ void __launch_bounds__(256, 3) jacobi_qp_kernel(float* __restrict__ dst, const float* __restrict__ src,
+                                                           const float* __restrict__ f, Lvl<float> L, float w,
+                                                           int zc, double* __restrict__ p64) {
+    wp_pdl_enter();
+    // dynamic shared memory: ring_v | ring_f (JP_DEPTH x 256 float4 each) | ring_p (ACC: JP_DEPTH x 512 double2)
+    extern __shared__ __align__(16) float4 jp_smem[];
+    float4 (*ring_v)[256] = reinterpret_cast<float4 (*)[256]>(jp_smem);
+    float4 (*ring_f)[256] = reinterpret_cast<float4 (*)[256]>(jp_smem + JP_DEPTH * 256);
+    double2 (*ring_p)[512] = reinterpret_cast<double2 (*)[512]>(jp_smem + 2 * JP_DEPTH * 256);
+    const int tid = threadIdx.x;
+    const int nq = L.ny >> 2;
+    const long q = (long)blockIdx.x * 256 + tid;
+    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    if (q >= (long)L.nx * nq || z0 >= z1) return;
+    const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
+    const long sxy = (long)L.nx * L.ny;
+    const long ibase = y0 + (long)x * L.ny;
+    auto issue = [&](int p) {
+        const int slot = (p - z0) % JP_DEPTH;
+        if (p < z1) {
+            if (p + 1 < L.nz) cp_async16(&ring_v[slot][tid], src + ibase + (long)(p + 1) * sxy);
+            cp_async16(&ring_f[slot][tid], f + ibase + (long)p * sxy);
+            if constexpr (ACC) {
+                cp_async16(&ring_p[slot][2 * tid], p64 + ibase + (long)p * sxy);
+                cp_async16(&ring_p[slot][2 * tid + 1], p64 + ibase + (long)p * sxy + 2);
+            }
+        }
+        cp_async_commit();  // one group per plane (empty past the chunk) keeps the count uniform
+    };
+    for (int p = z0; p < z0 + JP_DEPTH - 1; ++p) issue(p);
+    QCol<float, float> col(L, src, x, y0, z0);
+    for (int z = z0; z < z1; ++z) {
+        issue(z + JP_DEPTH - 1);
+        cp_async_wait<JP_DEPTH - 1>();  // the group of plane z has landed
+        const int slot = (z - z0) % JP_DEPTH;
+        const long i = col.i;
+        Q4<float> vp = zero4<float>();
+        if (z < L.nz - 1) {
+            const float4 t = ring_v[slot][tid];
+            vp = Q4<float>{{t.x, t.y, t.z, t.w}};
+        }
+        const float4 tf = ring_f[slot][tid];
+        const Q4<float> fv{{tf.x, tf.y, tf.z, tf.w}};
+        Q4<float> dg, od, c;
+        col.step_with(dg, od, c, vp);
+        Q4<float> out;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            out.a[k] = dg.a[k] > (float)kEps ? (1.f - w) * c.a[k] + w * (fv.a[k] - od.a[k]) / dg.a[k] : 0.f;
+        if constexpr (ACC) {
+            const double2 a = ring_p[slot][2 * tid], b = ring_p[slot][2 * tid + 1];
+            const Q4<double> pv{{a.x + (double)out.a[0], a.y + (double)out.a[1], b.x + (double)out.a[2],
+                                 b.y + (double)out.a[3]}};
+            st4(p64 + i, pv);
+        } else {
+            st4(dst + i, out);
+        }
+    }
+    cp_async_wait<0>();
 }
 
 // Two weighted-Jacobi sweeps in one pass (temporal blocking along z).  A CTA owns an interior tile
@@ -1727,7 +1814,8 @@ struct Level {
                       // defect64); 0 = heuristic, set by wp_mgfrac3d_autotune
     float zc_ms[3];   // the autotuner's median time of the chosen chunk (0 = not tuned)
     int var[3];       // kernel variant per kind (jacobi: 0 = default registers, 1/2 = >= 3/4 CTAs per SM,
-                      // 3 = two sweeps per launch, 4 = TMA-staged rows)
+                      // 3 = two sweeps per launch, 4 = TMA-staged rows, 5 = cp.async-pipelined planes;
+                      // restrict: 0-2 register budgets)
     int* err;         // the handle's device error flag (bounded waits of the TMA-staged kernel)
 };
 
@@ -1835,6 +1923,12 @@ void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc
             launch_jacobi_ts(L, (float*)dst, (const float*)src, (const float*)f, (float)w, s);
             return;
         }
+        if constexpr (sizeof(T) == 4) {
+            if (var == 5) {
+                wp_launch_pdl(jacobi_qp_kernel<false>, g, 256, jp_smem_bytes(false), s, dst, src, f, V, w, zc, nullptr);
+                return;
+            }
+        }
         if (var == 1) wp_launch_pdl(jacobi_q_mb_kernel<T, 3>, g, 256, 0, s, dst, src, f, V, w, zc, nullptr);
         else if (var == 2) wp_launch_pdl(jacobi_q_mb_kernel<T, 4>, g, 256, 0, s, dst, src, f, V, w, zc, nullptr);
         else wp_launch_pdl(jacobi_q_kernel<T>, g, 256, 0, s, dst, src, f, V, w, zc, nullptr);
@@ -1848,7 +1942,7 @@ void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc
 // One FP32 sweep of src whose result is added to p64 instead of stored (the level's tuned one-sweep
 // quad kernel); false when the level's kernel has no such form (the caller then stores and adds).
 bool jacobi_acc_ok(const Level& L, const void* src, const void* f, const double* p64) {
-    return quad_ok(L) && al16(src) && al16(f) && al16(p64) && L.var[kZcJacobi] <= 2;
+    return quad_ok(L) && al16(src) && al16(f) && al16(p64) && (L.var[kZcJacobi] <= 2 || L.var[kZcJacobi] == 5);
 }
 void launch_jacobi_acc(const Level& L, const float* src, const float* f, float w, int zc, double* p64,
                        cudaStream_t s) {
@@ -1856,7 +1950,12 @@ void launch_jacobi_acc(const Level& L, const float* src, const float* f, float w
     const Lvl<float> V = view<float>(L);
     const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
     if (var == 1) wp_launch_pdl(jacobi_q_mb_kernel<float, 3, true>, g, 256, 0, s, nullptr, src, f, V, w, zc, p64);
-    else if (var == 2) wp_launch_pdl(jacobi_q_mb_kernel<float, 4, true>, g, 256, 0, s, nullptr, src, f, V, w, zc, p64);
+    else if (var == 5) {
+        wp_set_smem(jacobi_qp_kernel<true>, jp_smem_bytes(true));
+        wp_launch_pdl(jacobi_qp_kernel<true>, g, 256, jp_smem_bytes(true), s, nullptr, src, f, V, w, zc, p64);
+    }
+    else if (var == 2)
+        wp_launch_pdl(jacobi_q_mb_kernel<float, 4, true>, g, 256, 0, s, nullptr, src, f, V, w, zc, p64);
     else wp_launch_pdl(jacobi_q_kernel<float, true>, g, 256, 0, s, nullptr, src, f, V, w, zc, p64);
 }
 
@@ -2165,7 +2264,7 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         int pre = nu1;
         if (clear_v) {
             const int var = sizeof(T) == 4 ? L.var[kZcJacobi] : 0;
-            if (nu1 > 0 && quad_ok(L) && al16(Bufs<T>::t(L)) && al16(f) && var <= 2) {
+            if (nu1 > 0 && quad_ok(L) && al16(Bufs<T>::t(L)) && al16(f) && (var <= 2 || var == 5)) {
                 const int zc = level_zc(L, kZcJacobi);
                 const dim3 gq(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
                 WP_KERNEL(l == 0 ? "jacobi0_finest" : "jacobi0", (double)L.cells * 2.0 * sizeof(T) + frac_bytes(L), s,
@@ -2882,7 +2981,7 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             const long floor_blocks = std::min<long>(most, 2L * wp_sm_count());
             void* fl = L.cells > kL2Cells ? flush : nullptr;
             // jacobi variants: 0-2 one sweep per launch (register budgets), 3 two sweeps per launch
-            const int nvar = !quad_ok(L) ? 1 : kind == kZcJacobi ? 5 : kind == kZcRestrict ? 3 : 1;
+            const int nvar = !quad_ok(L) ? 1 : kind == kZcJacobi ? 6 : kind == kZcRestrict ? 3 : 1;
             for (int var = 0; var < nvar && st == WP_OK; ++var) {
                 if (var == 3 && !jacobi2_ok(L, L.f)) continue;
                 if (var == 4 && !jacobi_ts_ok(L, L.t, L.v, L.f)) continue;
@@ -2952,7 +3051,7 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc,
 // Pins the chunk and kernel variant of one level's column kernel (kind 0 jacobi, 1 restrict,
 // 2 defect); zc <= 0 restores the heuristic.
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant) {
-    if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 4 ||
+    if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 5 ||
         (kind == kZcRestrict && variant > 2) || (kind == kZcDefect && variant != 0)) {
         wp_set_error_msg("wp_mgfrac3d_set_tile: bad arguments");
         return WP_ERR_INVALID_ARG;
