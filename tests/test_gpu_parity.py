@@ -411,7 +411,7 @@ def test_mg_jacobi_variants_agree(wp, oracle, variant):
         np.testing.assert_allclose(outs[0][1], o[1], rtol=1e-4)
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_mg_restrict_variants_agree(wp, oracle, variant):
     """The register-budget variants of the fused residual-restriction give the default kernel's cycles."""
     nn, h, a, _, f = _sphere_problem(wp, oracle, 32, seed=13)
@@ -426,3 +426,18 @@ def test_mg_restrict_variants_agree(wp, oracle, variant):
     for o in outs[1:]:
         assert rel(outs[0][0], o[0]) < 1e-6
         np.testing.assert_allclose(outs[0][1], o[1], rtol=1e-4)
+
+
+def test_mg_defect_variants_agree(wp, oracle):
+    """The cp.async-pipelined FP64 defect gives the quad kernel's refinement history and iterate."""
+    nn, h, a, _, f = _sphere_problem(wp, oracle, 32, seed=17)
+    outs = []
+    for var, zc in ((0, 0), (1, 2), (1, 32)):
+        mg = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)
+        mg.SetTile(0, 2, zc, var)
+        dst = torch.zeros(f.shape, device="cuda")
+        rep = mg.SolveTol(dst, None, T(f), rel_tol=0.0, max_cycles=6, precision=wp.PREC_MIXED)
+        outs.append((mg.Iterate64(), rep["history"]))
+    for o in outs[1:]:
+        assert rel(outs[0][0], o[0]) < 1e-12
+        np.testing.assert_allclose(outs[0][1], o[1], rtol=1e-9)

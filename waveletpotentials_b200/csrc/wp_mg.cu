@@ -831,6 +831,103 @@ __global__ void __launch_bounds__(256, MINB) resid_restrict_q_kernel(T* __restri
     }
 }
 
+// resid_restrict_q_kernel with its fine planes' streaming loads (the walker's next centre quad and
+// f) issued JP_DEPTH - 1 planes ahead into a per-thread cp.async ring (as jacobi_qp_kernel); the
+// sums and their order are resid_restrict_q_kernel's.
+__global__ void __launch_bounds__(256, 3) resid_restrict_qp_kernel(float* __restrict__ fc,
+                                                                   const float* __restrict__ v,
+                                                                   const float* __restrict__ f, Lvl<float> L,
+                                                                   int ncx, int ncy, int ncz, int czc) {
+    wp_pdl_enter();
+    extern __shared__ __align__(16) float4 jp_smem[];
+    float4 (*ring_v)[256] = reinterpret_cast<float4 (*)[256]>(jp_smem);
+    float4 (*ring_f)[256] = reinterpret_cast<float4 (*)[256]>(jp_smem + JP_DEPTH * 256);
+    const int tid = threadIdx.x;
+    const int nq = L.ny >> 2;
+    const long q = (long)blockIdx.x * 256 + tid;
+    const int cz0 = blockIdx.y * czc, cz1 = min(cz0 + czc, ncz);
+    const long pair = q >> 1;
+    const int xpar = (int)(q & 1);
+    const bool live_pair = pair < (long)ncx * nq && cz0 < cz1;
+    const int cx = live_pair ? (int)(pair / nq) : 0;
+    const int y0 = live_pair ? (int)(pair - (long)cx * nq) * 4 : 0;
+    const int x0 = 2 * cx;
+    const bool two = x0 + 1 < L.nx;
+    const bool mine = live_pair && (xpar == 0 || two);
+    const int x = mine ? x0 + xpar : x0;
+    float wxy[4];
+    {
+        const double sx = L.d[0][x0] + (two ? L.d[0][x0 + 1] : 0.0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = y0 + k, yb = y & ~1;
+            const double sy = L.d[1][yb] + (yb + 1 < L.ny ? L.d[1][yb + 1] : 0.0);
+            wxy[k] = mine ? (float)(L.d[1][y] / sy * (L.d[0][x] / sx)) : 0.f;
+        }
+    }
+    // fine planes this lane walks: zs .. ze - 1
+    const int zs = 2 * cz0, ze = live_pair ? min(2 * cz1, L.nz) : zs;
+    const long sxy = (long)L.nx * L.ny;
+    const long ibase = y0 + (long)x * L.ny;
+    auto issue = [&](int p) {
+        const int slot = (p - zs) % JP_DEPTH;
+        if (p < ze) {
+            if (p + 1 < L.nz) cp_async16(&ring_v[slot][tid], v + ibase + (long)(p + 1) * sxy);
+            cp_async16(&ring_f[slot][tid], f + ibase + (long)p * sxy);
+        }
+        cp_async_commit();
+    };
+    if (live_pair)
+        for (int p = zs; p < zs + JP_DEPTH - 1; ++p) issue(p);
+    QCol<float, float> col(L, v, x, y0, live_pair ? zs : 0);
+    const int ncz_loop = live_pair ? cz1 - cz0 : 0;
+    int iters = ncz_loop;
+    for (int o = 16; o > 0; o >>= 1) iters = max(iters, __shfl_xor_sync(0xffffffffu, iters, o));
+    for (int it = 0; it < iters; ++it) {
+        const int cz = cz0 + it;
+        const bool act = it < ncz_loop;
+        Q4<float> acc = zero4<float>();
+        if (act) {
+            const int zb = 2 * cz;
+            const double sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
+            for (int kz = 0; kz < 2; ++kz) {
+                const int z = zb + kz;
+                if (z >= L.nz) break;
+                issue(z + JP_DEPTH - 1);
+                cp_async_wait<JP_DEPTH - 1>();
+                const int slot = (z - zs) % JP_DEPTH;
+                const float wz = (float)(L.d[2][z] / sz);
+                const long i = col.i;
+                Q4<float> vp = zero4<float>();
+                if (z < L.nz - 1) {
+                    const float4 t = ring_v[slot][tid];
+                    vp = Q4<float>{{t.x, t.y, t.z, t.w}};
+                }
+                Q4<float> dg, od, c;
+                col.step_with(dg, od, c, vp);
+                (void)i;
+                if (mine) {
+                    const float4 tf = ring_f[slot][tid];
+                    const Q4<float> fv{{tf.x, tf.y, tf.z, tf.w}};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const float r = dg.a[k] > (float)kEps ? fv.a[k] - (dg.a[k] * c.a[k] + od.a[k]) : 0.f;
+                        acc.a[k] += wz * wxy[k] * r;
+                    }
+                }
+            }
+        }
+        const float ya = acc.a[0] + acc.a[1], yb = acc.a[2] + acc.a[3];
+        const float oa = __shfl_xor_sync(0xffffffffu, ya, 1), ob = __shfl_xor_sync(0xffffffffu, yb, 1);
+        if (act && xpar == 0) {
+            const long ci = (y0 >> 1) + (long)cx * ncy + (long)cz * ncx * ncy;
+            fc[ci] = ya + oa;
+            fc[ci + 1] = yb + ob;
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // FP64 defect on quads (see defect64_z_kernel)
 template <typename TP>
 __global__ void __launch_bounds__(256, 2) defect64_q_kernel(float* __restrict__ r32, const TP* __restrict__ p,
@@ -860,6 +957,76 @@ __global__ void __launch_bounds__(256, 2) defect64_q_kernel(float* __restrict__ 
             }
             if (r32) st4(r32 + i, rr);
         }
+    }
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < 8; ++k) t += red[k];
+        atomicAdd(acc, t);
+    }
+}
+
+// defect64_q_kernel<double> with the walker's next centre quad of p (FP64) and f issued JP_DEPTH - 1
+// planes ahead into a per-thread cp.async ring; the same arithmetic and reduction.
+__global__ void __launch_bounds__(256, 2) defect64_qp_kernel(float* __restrict__ r32, const double* __restrict__ p,
+                                                             const float* __restrict__ f, Lvl<double> L, double m,
+                                                             const double* __restrict__ msum,
+                                                             double* __restrict__ acc, int zc) {
+    wp_pdl_enter();
+    // dynamic shared memory: ring_p (JP_DEPTH x 512 double2) | ring_f (JP_DEPTH x 256 float4)
+    extern __shared__ __align__(16) float4 jp_smem[];
+    double2 (*ring_p)[512] = reinterpret_cast<double2 (*)[512]>(jp_smem);
+    float4 (*ring_f)[256] = reinterpret_cast<float4 (*)[256]>(jp_smem + 2 * JP_DEPTH * 256);
+    const int tid = threadIdx.x;
+    const int nq = L.ny >> 2;
+    const long q = (long)blockIdx.x * 256 + tid;
+    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    if (msum) m = msum[0] / fmax(msum[1], 1.0);
+    double s2 = 0.0;
+    if (q < (long)L.nx * nq && z0 < z1) {
+        const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
+        const long sxy = (long)L.nx * L.ny;
+        const long ibase = y0 + (long)x * L.ny;
+        auto issue = [&](int pl) {
+            const int slot = (pl - z0) % JP_DEPTH;
+            if (pl < z1) {
+                if (pl + 1 < L.nz) {
+                    cp_async16(&ring_p[slot][2 * tid], p + ibase + (long)(pl + 1) * sxy);
+                    cp_async16(&ring_p[slot][2 * tid + 1], p + ibase + (long)(pl + 1) * sxy + 2);
+                }
+                cp_async16(&ring_f[slot][tid], f + ibase + (long)pl * sxy);
+            }
+            cp_async_commit();
+        };
+        for (int pl = z0; pl < z0 + JP_DEPTH - 1; ++pl) issue(pl);
+        QCol<double, double> col(L, p, x, y0, z0);
+        for (int z = z0; z < z1; ++z) {
+            issue(z + JP_DEPTH - 1);
+            cp_async_wait<JP_DEPTH - 1>();
+            const int slot = (z - z0) % JP_DEPTH;
+            const long i = col.i;
+            Q4<double> vp = zero4<double>();
+            if (z < L.nz - 1) {
+                const double2 a = ring_p[slot][2 * tid], b = ring_p[slot][2 * tid + 1];
+                vp = Q4<double>{{a.x, a.y, b.x, b.y}};
+            }
+            Q4<double> dg, od, c;
+            col.step_with(dg, od, c, vp);
+            const float4 tf = ring_f[slot][tid];
+            const float fv[4] = {tf.x, tf.y, tf.z, tf.w};
+            Q4<float> rr;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double r = dg.a[k] > kEps ? ((double)fv[k] - m) - (dg.a[k] * c.a[k] + od.a[k]) : 0.0;
+                rr.a[k] = (float)r;
+                s2 += r * r;
+            }
+            if (r32) st4(r32 + i, rr);
+        }
+        cp_async_wait<0>();
     }
     for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
     __shared__ double red[8];
@@ -1729,6 +1896,40 @@ __global__ void __launch_bounds__(256) active_sum_kernel(const float* __restrict
     }
 }
 
+// active_sum_kernel on quads: each thread walks a z-chunk of a quad column with the FP64 walker
+// (the same diagonal as row()), sums f and the count of active cells, one atomic pair per CTA
+__global__ void __launch_bounds__(256) active_sum_q_kernel(const float* __restrict__ f, Lvl<double> L,
+                                                           double* __restrict__ acc, int zc) {
+    const int nq = L.ny >> 2;
+    const long q = (long)blockIdx.x * 256 + threadIdx.x;
+    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    double sf = 0.0, cnt = 0.0;
+    if (q < (long)L.nx * nq && z0 < z1) {
+        const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
+        QCol<double, float> col(L, f, x, y0, z0);
+        for (int z = z0; z < z1; ++z) {
+            Q4<double> dg, od, c;
+            col.step(dg, od, c);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (dg.a[k] > kEps) { sf += c.a[k]; cnt += 1.0; }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sf += __shfl_xor_sync(0xffffffffu, sf, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    }
+    __shared__ double red[2][8];
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = sf; red[1][threadIdx.x >> 5] = cnt; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < 8; ++k) { a += red[0][k]; b += red[1][k]; }
+        atomicAdd(acc, a);
+        atomicAdd(acc + 1, b);
+    }
+}
+
 // FP64 right-hand side of the compatible problem: f - m on active cells, 0 elsewhere
 __global__ void __launch_bounds__(256) rhs64_kernel(double* __restrict__ out, const float* __restrict__ f, Lvl<double> L,
                                                     double m) {
@@ -1974,6 +2175,13 @@ void launch_resid_restrict(const Level& L, const Level& C, T* fc, const T* v, co
     if (quad_ok(L) && C.n[1] * 2 == L.n[1] && al16(v) && al16(f)) {
         const dim3 g(wp_cdiv((size_t)C.n[0] * (L.n[1] / 4) * 2, 256), wp_cdiv(C.n[2], czc));
         const int var = sizeof(T) == 4 ? L.var[kZcRestrict] : 0;
+        if constexpr (sizeof(T) == 4) {
+            if (var == 3) {
+                wp_launch_pdl(resid_restrict_qp_kernel, g, 256, jp_smem_bytes(false), s, fc, v, f, V, C.n[0], C.n[1],
+                              C.n[2], czc);
+                return;
+            }
+        }
         if (var == 1) wp_launch_pdl(resid_restrict_q_kernel<T, 3>, g, 256, 0, s, fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
         else if (var == 2)
             wp_launch_pdl(resid_restrict_q_kernel<T, 4>, g, 256, 0, s, fc, v, f, V, C.n[0], C.n[1], C.n[2], czc);
@@ -1991,6 +2199,14 @@ void launch_defect64(const Level& L, float* r32, const TP* p, const float* f, do
     const Lvl<double> V = view<double>(L);
     if (quad_ok(L) && al16(r32) && al16(p) && al16(f)) {
         const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
+        if constexpr (sizeof(TP) == 8) {
+            if (L.var[kZcDefect] == 1) {
+                wp_set_smem(defect64_qp_kernel, jp_smem_bytes(true) - (size_t)JP_DEPTH * 256 * 16);
+                wp_launch_pdl(defect64_qp_kernel, g, 256, jp_smem_bytes(true) - (size_t)JP_DEPTH * 256 * 16, s, r32,
+                              (const double*)p, f, V, m, msum, acc, zc);
+                return;
+            }
+        }
         wp_launch_pdl(defect64_q_kernel<TP>, g, 256, 0, s, r32, p, f, V, m, msum, acc, zc);
     } else {
         defect64_z_kernel<TP><<<grid_z(L.n[0], L.n[1], L.n[2], zc), dim3(32, 8), 0, s>>>(r32, p, f, V, m, msum, acc,
@@ -2357,12 +2573,22 @@ wp_status fmg_start(wp_mgfrac3d* h, const T* f0, int nu1, int nu2, T w, int prol
     return WP_OK;
 }
 
+// sum and count of f over the active cells of the level into acc[0], acc[1] (asynchronous)
+void launch_active_sum(const Level& L, const float* f, double* acc, cudaStream_t s) {
+    if (quad_ok(L) && al16(f)) {
+        const int zc = std::max(1, std::min(L.n[2], 16));
+        const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
+        active_sum_q_kernel<<<g, 256, 0, s>>>(f, view<double>(L), acc, zc);
+    } else {
+        active_sum_kernel<<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(f, view<double>(L), acc);
+    }
+}
+
 // mean of f over the active cells of the finest level (synchronous)
 wp_status active_mean(wp_mgfrac3d* h, const float* f, double* m, cudaStream_t s) {
     Level& L = h->lv[0];
     WP_CUDA_TRY(cudaMemsetAsync(h->acc + 2, 0, 2 * sizeof(double), s));
-    WP_KERNEL("active_sum", (double)L.cells * 16.0, s,
-              active_sum_kernel<<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(f, view<double>(L), h->acc + 2));
+    WP_KERNEL("active_sum", (double)L.cells * 4.0 + frac_bytes(L), s, launch_active_sum(L, f, h->acc + 2, s));
     double hv[2];
     WP_CUDA_TRY(wp_read_small(hv, h->acc + 2, sizeof(hv), s));
     *m = hv[1] > 0 ? hv[0] / hv[1] : 0.0;
@@ -2769,8 +2995,7 @@ wp_status solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, in
     wp_status st;
     if (!h->p64 || !h->r32) { wp_set_error_msg("mixed solve: work arrays not prepared"); return WP_ERR_INVALID_ARG; }
     WP_CUDA_TRY(cudaMemsetAsync(h->acc + 2, 0, 2 * sizeof(double), s));
-    WP_KERNEL("active_sum", (double)n * 16.0, s,
-              active_sum_kernel<<<grid_of(L.n[0], L.n[1], L.n[2]), dim3(32, 8), 0, s>>>(f, view<double>(L), h->acc + 2));
+    WP_KERNEL("active_sum", (double)n * 4.0 + frac_bytes(L), s, launch_active_sum(L, f, h->acc + 2, s));
     WP_CUDA_TRY(cudaMemsetAsync(h->p64, 0, sizeof(double) * n, s));
     if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, true, s)) != WP_OK) return st;
     for (int c = 0; c < cycles; ++c) {
@@ -2943,6 +3168,8 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
     WP_CUDA_TRY(cudaEventCreate(&ea));
     WP_CUDA_TRY(cudaEventCreate(&eb));
     const bool prof = wp_profile_is_enabled();
+    // the FP64 defect is tuned too (3D): its work arrays are those of the mixed solve
+    if (h->dims == 3 && prepare_mixed(h) != WP_OK) return WP_ERR_CUDA;
     wp_profile_enable(0);
     const long long launches0 = wp_launch_count();
     wp_status st = WP_OK;
@@ -2981,7 +3208,7 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             const long floor_blocks = std::min<long>(most, 2L * wp_sm_count());
             void* fl = L.cells > kL2Cells ? flush : nullptr;
             // jacobi variants: 0-2 one sweep per launch (register budgets), 3 two sweeps per launch
-            const int nvar = !quad_ok(L) ? 1 : kind == kZcJacobi ? 6 : kind == kZcRestrict ? 3 : 1;
+            const int nvar = !quad_ok(L) ? 1 : kind == kZcJacobi ? 6 : kind == kZcRestrict ? 4 : 2;
             for (int var = 0; var < nvar && st == WP_OK; ++var) {
                 if (var == 3 && !jacobi2_ok(L, L.f)) continue;
                 if (var == 4 && !jacobi_ts_ok(L, L.t, L.v, L.f)) continue;
@@ -3052,7 +3279,7 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc,
 // 2 defect); zc <= 0 restores the heuristic.
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant) {
     if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 5 ||
-        (kind == kZcRestrict && variant > 2) || (kind == kZcDefect && variant != 0)) {
+        (kind == kZcRestrict && variant > 3) || (kind == kZcDefect && variant > 1)) {
         wp_set_error_msg("wp_mgfrac3d_set_tile: bad arguments");
         return WP_ERR_INVALID_ARG;
     }
