@@ -393,7 +393,7 @@ def test_mg_offset_views_and_autotune_keep_results(wp, oracle):
     assert rel(N(dst0), N(dst)) < 1e-6
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
 def test_mg_jacobi_variants_agree(wp, oracle, variant):
     """Register-budget variants, the fused two-sweep kernel and the TMA-staged sweep give the same
     cycles as the default one-sweep kernel (up to FP32 contraction order) for every pinned z-chunk."""
@@ -411,7 +411,7 @@ def test_mg_jacobi_variants_agree(wp, oracle, variant):
         np.testing.assert_allclose(outs[0][1], o[1], rtol=1e-4)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 def test_mg_restrict_variants_agree(wp, oracle, variant):
     """The register-budget variants of the fused residual-restriction give the default kernel's cycles."""
     nn, h, a, _, f = _sphere_problem(wp, oracle, 32, seed=13)

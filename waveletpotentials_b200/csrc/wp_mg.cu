@@ -2015,8 +2015,9 @@ struct Level {
                       // defect64); 0 = heuristic, set by wp_mgfrac3d_autotune
     float zc_ms[3];   // the autotuner's median time of the chosen chunk (0 = not tuned)
     int var[3];       // kernel variant per kind (jacobi: 0 = default registers, 1/2 = >= 3/4 CTAs per SM,
-                      // 3 = two sweeps per launch, 4 = TMA-staged rows, 5 = cp.async-pipelined planes;
-                      // restrict: 0-2 register budgets)
+                      // 3 = two sweeps per launch, 4 = TMA-staged rows, 5 = cp.async-pipelined planes,
+                      // 6 = one cell per thread; restrict: 0-2 register budgets, 3 = pipelined,
+                      // 4 = one cell per thread; defect: 0 quads, 1 pipelined)
     int* err;         // the handle's device error flag (bounded waits of the TMA-staged kernel)
 };
 
@@ -2117,9 +2118,10 @@ void launch_jacobi_ts(const Level& L, float* dst, const float* src, const float*
 template <typename T>
 void launch_jacobi(const Level& L, T* dst, const T* src, const T* f, T w, int zc, cudaStream_t s) {
     const Lvl<T> V = view<T>(L);
-    if (quad_ok(L) && al16(dst) && al16(src) && al16(f)) {
+    const int var6 = sizeof(T) == 4 ? L.var[kZcJacobi] : 0;
+    if (quad_ok(L) && al16(dst) && al16(src) && al16(f) && var6 != 6) {
         const dim3 g(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
-        const int var = sizeof(T) == 4 ? L.var[kZcJacobi] : 0;
+        const int var = var6;
         if (var == 4 && jacobi_ts_ok(L, dst, src, f)) {
             launch_jacobi_ts(L, (float*)dst, (const float*)src, (const float*)f, (float)w, s);
             return;
@@ -2172,7 +2174,7 @@ void launch_jacobi2(const Level& L, T* dst, const T* src, const T* f, T w, int z
 template <typename T>
 void launch_resid_restrict(const Level& L, const Level& C, T* fc, const T* v, const T* f, int czc, cudaStream_t s) {
     const Lvl<T> V = view<T>(L);
-    if (quad_ok(L) && C.n[1] * 2 == L.n[1] && al16(v) && al16(f)) {
+    if (quad_ok(L) && C.n[1] * 2 == L.n[1] && al16(v) && al16(f) && (sizeof(T) != 4 || L.var[kZcRestrict] != 4)) {
         const dim3 g(wp_cdiv((size_t)C.n[0] * (L.n[1] / 4) * 2, 256), wp_cdiv(C.n[2], czc));
         const int var = sizeof(T) == 4 ? L.var[kZcRestrict] : 0;
         if constexpr (sizeof(T) == 4) {
@@ -2480,7 +2482,7 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         int pre = nu1;
         if (clear_v) {
             const int var = sizeof(T) == 4 ? L.var[kZcJacobi] : 0;
-            if (nu1 > 0 && quad_ok(L) && al16(Bufs<T>::t(L)) && al16(f) && (var <= 2 || var == 5)) {
+            if (nu1 > 0 && quad_ok(L) && al16(Bufs<T>::t(L)) && al16(f) && var != 3 && var != 4) {
                 const int zc = level_zc(L, kZcJacobi);
                 const dim3 gq(wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256), wp_cdiv(L.n[2], zc));
                 WP_KERNEL(l == 0 ? "jacobi0_finest" : "jacobi0", (double)L.cells * 2.0 * sizeof(T) + frac_bytes(L), s,
@@ -3208,27 +3210,33 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             const long floor_blocks = std::min<long>(most, 2L * wp_sm_count());
             void* fl = L.cells > kL2Cells ? flush : nullptr;
             // jacobi variants: 0-2 one sweep per launch (register budgets), 3 two sweeps per launch
-            const int nvar = !quad_ok(L) ? 1 : kind == kZcJacobi ? 6 : kind == kZcRestrict ? 4 : 2;
+            // jacobi 6 / restrict 4: one cell per thread (scalar column kernels), for levels small
+            // enough that a quad per thread leaves too few threads
+            const int nvar = !quad_ok(L) ? 1 : kind == kZcJacobi ? 7 : kind == kZcRestrict ? 5 : 2;
             for (int var = 0; var < nvar && st == WP_OK; ++var) {
-                if (var == 3 && !jacobi2_ok(L, L.f)) continue;
-                if (var == 4 && !jacobi_ts_ok(L, L.t, L.v, L.f)) continue;
+                const bool two_sweeps = kind == kZcJacobi && var == 3;
+                const bool staged = kind == kZcJacobi && var == 4;
+                if (two_sweeps && !jacobi2_ok(L, L.f)) continue;
+                if (staged && !jacobi_ts_ok(L, L.t, L.v, L.f)) continue;
                 L.var[kind] = var;
                 for (int zc : zc_candidates(planes)) {
                     // the TMA-staged sweep balances its own work over persistent CTAs: one timing
-                    if (var == 4 && zc != 1) continue;
+                    if (staged && zc != 1) continue;
                     long blocks = grid_blocks(L, C, kind, zc);
-                    if (var == 3)
+                    if (two_sweeps)
                         blocks = (long)((L.n[1] / 4 + J2_Q - 1) / J2_Q) * ((L.n[0] + J2_R - 1) / J2_R) *
                                  wp_cdiv(L.n[2], zc);
-                    if (var != 4 && blocks < floor_blocks) continue;
+                    if ((kind == kZcJacobi && var == 6) || (kind == kZcRestrict && var == 4))
+                        blocks = (long)wp_cdiv(L.n[1], 32) * wp_cdiv(L.n[0], 8) * wp_cdiv(planes, zc);
+                    if (!staged && blocks < floor_blocks) continue;
                     auto launch = [&]() {
-                        if (kind == kZcJacobi && var == 3) launch_jacobi2<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
+                        if (two_sweeps) launch_jacobi2<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
                         else if (kind == kZcJacobi) launch_jacobi<float>(L, L.t, L.v, L.f, 0.5f, zc, s);
                         else if (kind == kZcRestrict) launch_resid_restrict<float>(L, *C, C->f, L.v, L.f, zc, s);
                         else launch_defect64<double>(L, h->r32, h->p64, L.f, 0.0, nullptr, h->acc, zc, s);
                     };
                     // the fused variant does two sweeps: compare time per sweep
-                    const float ms = time_launches(launch, s, ea, eb, 5, fl, kFlush) / (var == 3 ? 2.f : 1.f);
+                    const float ms = time_launches(launch, s, ea, eb, 5, fl, kFlush) / (two_sweeps ? 2.f : 1.f);
                     const cudaError_t e = cudaGetLastError();
                     if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
                     if (ms < best) { best = ms; best_zc = zc; best_var = var; }
@@ -3278,8 +3286,8 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc,
 // Pins the chunk and kernel variant of one level's column kernel (kind 0 jacobi, 1 restrict,
 // 2 defect); zc <= 0 restores the heuristic.
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant) {
-    if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 5 ||
-        (kind == kZcRestrict && variant > 3) || (kind == kZcDefect && variant > 1)) {
+    if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 6 ||
+        (kind == kZcRestrict && variant > 4) || (kind == kZcDefect && variant > 1)) {
         wp_set_error_msg("wp_mgfrac3d_set_tile: bad arguments");
         return WP_ERR_INVALID_ARG;
     }
