@@ -183,7 +183,9 @@ CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc, int* varia
    >= 4 CTAs per SM register budgets, 3 two sweeps per launch, 4 TMA-staged rows on persistent CTAs,
    5 the next planes' loads issued ahead with cp.async, 6 one cell per thread; 3-6 FP32 3D levels
    only), 1 (restriction: variant 0-2 the same register budgets, 3 pipelined, 4 one cell per
-   thread) or 2 (FP64 defect: 0 quads, 1 pipelined); zc <= 0 restores the heuristic chunk. */
+   thread) or 2 (FP64 defect: 0 quads, 1 pipelined); zc <= 0 restores the heuristic chunk.  Kind 3
+   (level and zc ignored): the levels below the finest run as one persistent cooperative launch
+   (variant 1, the default where the autotuner finds it faster) or launch by launch (variant 0). */
 CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant);
 /* Uniform rows of one level (no reference counterpart): the number of (x, z) rows of cells whose
    interior face fractions are all exactly 1, which the column kernels stream without reading any

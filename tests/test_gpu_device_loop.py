@@ -120,3 +120,27 @@ def test_inner_cycles_reach_tolerance_on_both_loops(wp, oracle, start):
     fc[act] -= f[act].mean()
     _, r = oracle.frac_residual3d(dev[2], fc, *a, nn, (h,) * 3)
     assert np.linalg.norm(r) / np.linalg.norm(f) <= 1.5e-10
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_persistent_coarse_levels_match_launch_by_launch(wp, oracle, precision):
+    """The levels below the finest run as one cooperative launch (phases with grid barriers) or
+    launch by launch: the same cycles (FP32 contraction order aside), the same tolerance reached,
+    on the device loop and on the host loop."""
+    nn, h, a, _, f = _sphere_problem(wp, oracle, 128, seed=31, spheres=([[0.4, 0.5, 0.45], [0.7, 0.3, 0.6]], [0.18, 0.1]))
+    prec = wp.PREC_FP32 if precision == "fp32" else wp.PREC_MIXED
+    tf = T(f)
+    outs = []
+    for on, host_loop in ((0, False), (1, False), (1, True)):
+        mg = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)
+        mg.SetTile(0, 3, 0, on)
+        dst = torch.zeros(f.shape, device="cuda")
+        kw = dict(rel_tol=0.0, max_cycles=5) if precision == "fp32" else dict(rel_tol=1e-10, max_cycles=60)
+        rep = mg.SolveTol(dst, None, tf, precision=prec, raise_on_fail=False, host_loop=host_loop, **kw)
+        torch.cuda.synchronize()
+        outs.append((rep, N(dst)))
+    for rep, d in outs[1:]:
+        assert rep["status"] == outs[0][0]["status"] and rep["cycles"] == outs[0][0]["cycles"]
+        np.testing.assert_allclose(rep["history"], outs[0][0]["history"], rtol=1e-4 if precision == "fp32" else 1e-6)
+        scale = np.abs(outs[0][1]).max()
+        assert np.abs(d - outs[0][1]).max() <= 1e-4 * scale

@@ -17,6 +17,7 @@ struct wp_mgfrac2d;
 wp_status wp_mg_prepare_mixed(wp_mgfrac3d* h);
 wp_status wp_mg_solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
                                         cudaStream_t s);
+void wp_mg_forbid_persistent(wp_mgfrac3d* h);
 wp_status wp_mg_solve_tol_internal(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm, wp_mg_report* r,
                                    cudaStream_t s);
 const double* wp_mg_slots(const wp_mgfrac3d* h);
@@ -133,11 +134,13 @@ extern "C" CUWHHD_API wp_status wp_batch_create(wp_batch** out, int count, const
             if ((st = wp_mgfrac3d_create(&G.mg3, ax[i], ay[i], G.frac[2], G.n[0], G.n[1], G.n[2], G.h, G.h, G.h, 'n',
                                          nullptr)) != WP_OK)
                 break;
+            wp_mg_forbid_persistent(G.mg3);
             if ((st = wp_recover3d_create(&G.rec3, G.n[0], G.n[1], G.n[2], G.h, G.h, G.h, 'n', WP_CDF3_7, WP_CDF4_6)) !=
                 WP_OK)
                 break;
         } else if (G.dims == 2) {
             if ((st = wp_mgfrac2d_create(&G.mg2, ax[i], ay[i], G.n[0], G.n[1], G.h, G.h, 'n', nullptr)) != WP_OK) break;
+            wp_mg_forbid_persistent(wp_mg2d_impl(G.mg2));
             if ((st = wp_recover2d_create(&G.rec2, G.n[0], G.n[1], G.h, G.h, 'n', WP_CDF3_7, WP_CDF4_6)) != WP_OK) break;
         } else {
             wp_set_error_msg("wp_batch_create: dims must be 2 or 3");

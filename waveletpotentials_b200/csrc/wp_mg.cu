@@ -203,8 +203,36 @@ __device__ __forceinline__ Q4<T> zero4() {
     return {{(T)0, (T)0, (T)0, (T)0}};
 }
 
-// Walker over the quad (x, y0..y0+3) of a column, z = z0, z0+1, ...
-template <typename T, typename TV>
+// Loads of data that another CTA of the same grid may have written earlier in the grid's life (the
+// persistent coarse-level kernel): cache-global (L2) loads, never a possibly stale L1 line or the
+// non-coherent read-only path.  CG = false: ordinary loads.
+template <bool CG>
+__device__ __forceinline__ Q4<float> ldq(const float* p) {
+    if constexpr (CG) {
+        const float4 t = __ldcg(reinterpret_cast<const float4*>(p));
+        return {{t.x, t.y, t.z, t.w}};
+    } else {
+        return ld4(p);
+    }
+}
+template <bool CG>
+__device__ __forceinline__ Q4<double> ldq(const double* p) {
+    if constexpr (CG) {
+        const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldcg(reinterpret_cast<const double2*>(p + 2));
+        return {{a.x, a.y, b.x, b.y}};
+    } else {
+        return ld4(p);
+    }
+}
+template <bool CG, typename V>
+__device__ __forceinline__ V ld1(const V* p) {
+    if constexpr (CG) return __ldcg(p);
+    else return *p;
+}
+
+// Walker over the quad (x, y0..y0+3) of a column, z = z0, z0+1, ...  CG: v through L2 (see ldq).
+template <typename T, typename TV, bool CG = false>
 struct QCol {
     const Lvl<T>& L;
     const TV* __restrict__ v;
@@ -232,15 +260,15 @@ struct QCol {
             gyl[k] = L.glo[1][y0 + k];
             gyh[k] = L.ghi[1][y0 + k];
         }
-        vm = z0 > 0 ? cvt4<T>(ld4(v + i - sxy)) : zero4<T>();
-        vc = cvt4<T>(ld4(v + i));
+        vm = z0 > 0 ? cvt4<T>(ldq<CG>(v + i - sxy)) : zero4<T>();
+        vc = cvt4<T>(ldq<CG>(v + i));
         azl = z0 > 0 ? cvt4<T>(ld4(L.az + i)) : zero4<T>();
         un = z0 < L.nz ? L.uni[(long)z0 * L.nx + x] : 0;
     }
 
     __device__ __forceinline__ void step(Q4<T>& dg, Q4<T>& od, Q4<T>& c) {
         Q4<T> vp = zero4<T>();
-        if (z < L.nz - 1) vp = cvt4<T>(ld4(v + i + sxy));
+        if (z < L.nz - 1) vp = cvt4<T>(ldq<CG>(v + i + sxy));
         step_with(dg, od, c, vp);
     }
 
@@ -251,10 +279,10 @@ struct QCol {
         // a row whose faces are all exactly 1 reads no fractions (the same values, without the traffic)
         const bool u = un != 0;
         un = zp ? L.uni[(long)(z + 1) * L.nx + x] : 0;
-        const T vym = ym ? (T)v[i - 1] : (T)0;
-        const T vyp = yp ? (T)v[i + 4] : (T)0;
-        const Q4<T> vxm = xm ? cvt4<T>(ld4(v + i - ny)) : zero4<T>();
-        const Q4<T> vxp = xp ? cvt4<T>(ld4(v + i + ny)) : zero4<T>();
+        const T vym = ym ? (T)ld1<CG>(v + i - 1) : (T)0;
+        const T vyp = yp ? (T)ld1<CG>(v + i + 4) : (T)0;
+        const Q4<T> vxm = xm ? cvt4<T>(ldq<CG>(v + i - ny)) : zero4<T>();
+        const Q4<T> vxp = xp ? cvt4<T>(ldq<CG>(v + i + ny)) : zero4<T>();
         Q4<T> azu = zero4<T>();
         const T gzl = L.glo[2][z], gzh = L.ghi[2][z];
         if (u && xm && xp && z > 0 && zp) {
@@ -316,21 +344,21 @@ struct QCol {
 // y-quad index of a thread: q = x * (ny / 4) + yq over one z-plane.  ACC: the swept values are not
 // stored but added to the FP64 iterate p64 (the refinement update fused into the last sweep of a
 // correction cycle, add_correction_kernel's arithmetic).
-template <typename T, bool ACC = false>
+template <typename T, bool ACC = false, bool CG = false>
 __device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ f,
-                                              const Lvl<T>& L, T w, int zc, double* __restrict__ p64 = nullptr) {
-    wp_pdl_enter();
+                                              const Lvl<T>& L, T w, int zc, double* __restrict__ p64, int bx, int by,
+                                              int tid) {
     const int nq = L.ny >> 2;
-    const long q = (long)blockIdx.x * 256 + threadIdx.x;
-    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    const long q = (long)bx * 256 + tid;
+    const int z0 = by * zc, z1 = min(z0 + zc, L.nz);
     if (q >= (long)L.nx * nq || z0 >= z1) return;
     const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
-    QCol<T, T> col(L, src, x, y0, z0);
+    QCol<T, T, CG> col(L, src, x, y0, z0);
     for (int z = z0; z < z1; ++z) {
         const long i = col.i;
         Q4<T> dg, od, c;
         col.step(dg, od, c);
-        const Q4<T> fv = ld4(f + i);
+        const Q4<T> fv = ldq<CG>(f + i);
         Q4<T> out;
 #pragma unroll
         for (int k = 0; k < 4; ++k)
@@ -349,13 +377,12 @@ __device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __re
 // The first sweep from v = 0: every neighbour and the centre are 0, so the sweep is
 // (1 - w) 0 + w (f - 0) / diag, which reads only f and (outside uniform rows) the fractions for the
 // diagonal -- the same value as jacobi_q_body on a zeroed v, with no v to clear or read.
-template <typename T>
-__global__ void __launch_bounds__(256) jacobi0_q_kernel(T* __restrict__ dst, const T* __restrict__ f, Lvl<T> L, T w,
-                                                        int zc) {
-    wp_pdl_enter();
+template <typename T, bool CG = false>
+__device__ __forceinline__ void jacobi0_q_body(T* __restrict__ dst, const T* __restrict__ f, const Lvl<T>& L, T w,
+                                               int zc, int bx, int by, int tid) {
     const int nq = L.ny >> 2;
-    const long q = (long)blockIdx.x * 256 + threadIdx.x;
-    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
+    const long q = (long)bx * 256 + tid;
+    const int z0 = by * zc, z1 = min(z0 + zc, L.nz);
     if (q >= (long)L.nx * nq || z0 >= z1) return;
     const int nx = L.nx, ny = L.ny, nz = L.nz;
     const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
@@ -391,7 +418,7 @@ __global__ void __launch_bounds__(256) jacobi0_q_kernel(T* __restrict__ dst, con
             if (zp) azu = cvt4<T>(ld4(L.az + i + sxy));
         }
         const T gzl = L.glo[2][z], gzh = L.ghi[2][z];
-        const Q4<T> fv = ld4(f + i);
+        const Q4<T> fv = ldq<CG>(f + i);
         Q4<T> out;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -412,19 +439,28 @@ __global__ void __launch_bounds__(256) jacobi0_q_kernel(T* __restrict__ dst, con
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) jacobi0_q_kernel(T* __restrict__ dst, const T* __restrict__ f, Lvl<T> L, T w,
+                                                        int zc) {
+    wp_pdl_enter();
+    jacobi0_q_body<T>(dst, f, L, w, zc, blockIdx.x, blockIdx.y, threadIdx.x);
+}
+
 // register-allocation variants of the same sweep (the autotuner picks one per level): default
 // limits, and at least 3 or 4 resident 256-thread CTAs per SM
 template <typename T, bool ACC = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1) jacobi_q_kernel(T* __restrict__ dst, const T* __restrict__ src,
                                                        const T* __restrict__ f, Lvl<T> L, T w, int zc,
                                                        double* __restrict__ p64 = nullptr) {
-    jacobi_q_body<T, ACC>(dst, src, f, L, w, zc, p64);
+    wp_pdl_enter();
+    jacobi_q_body<T, ACC>(dst, src, f, L, w, zc, p64, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 template <typename T, int MINB, bool ACC = false>
 __global__ void __launch_bounds__(256, MINB) jacobi_q_mb_kernel(T* __restrict__ dst, const T* __restrict__ src,
                                                                 const T* __restrict__ f, Lvl<T> L, T w, int zc,
                                                                 double* __restrict__ p64 = nullptr) {
-    jacobi_q_body<T, ACC>(dst, src, f, L, w, zc, p64);
+    wp_pdl_enter();
+    jacobi_q_body<T, ACC>(dst, src, f, L, w, zc, p64, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
 // The one-sweep quad kernel with its streaming loads issued ahead: every thread keeps a private
@@ -763,15 +799,13 @@ __global__ void __launch_bounds__(TS_THREADS, 2)
 // coarse plane and sums its y pairs in registers, and a lane shuffle adds the two rows:
 // ((x0,y) + (x0,y+1)) + ((x0+1,y) + (x0+1,y+1)), each child carrying (0 + w_z0 r_z0) + w_z1 r_z1,
 // the order of resid_restrict_z_kernel.
-// MINB: register-budget variants as for the Jacobi sweep (1 default, 3 or 4 resident CTAs per SM).
-template <typename T, int MINB = 1>
-__global__ void __launch_bounds__(256, MINB) resid_restrict_q_kernel(T* __restrict__ fc, const T* __restrict__ v,
-                                                                     const T* __restrict__ f, Lvl<T> L, int ncx,
-                                                                     int ncy, int ncz, int czc) {
-    wp_pdl_enter();
+template <typename T, bool CG = false>
+__device__ __forceinline__ void resid_restrict_q_body(T* __restrict__ fc, const T* __restrict__ v,
+                                                      const T* __restrict__ f, const Lvl<T>& L, int ncx, int ncy,
+                                                      int ncz, int czc, int bx, int by, int tid) {
     const int nq = L.ny >> 2;
-    const long q = (long)blockIdx.x * 256 + threadIdx.x;
-    const int cz0 = blockIdx.y * czc, cz1 = min(cz0 + czc, ncz);
+    const long q = (long)bx * 256 + tid;
+    const int cz0 = by * czc, cz1 = min(cz0 + czc, ncz);
     const long pair = q >> 1;
     const int xpar = (int)(q & 1);
     // whole warps stay together for the shuffle; lanes past the grid end only idle along
@@ -792,7 +826,7 @@ __global__ void __launch_bounds__(256, MINB) resid_restrict_q_kernel(T* __restri
             wxy[k] = mine ? (T)(L.d[1][y] / sy * (L.d[0][x] / sx)) : (T)0;
         }
     }
-    QCol<T, T> col(L, v, x, y0, live_pair ? 2 * cz0 : 0);
+    QCol<T, T, CG> col(L, v, x, y0, live_pair ? 2 * cz0 : 0);
     const int ncz_loop = live_pair ? cz1 - cz0 : 0;
     // every lane of a warp runs the same number of shuffles: the loop bound is the warp maximum
     int iters = ncz_loop;
@@ -812,7 +846,7 @@ __global__ void __launch_bounds__(256, MINB) resid_restrict_q_kernel(T* __restri
                 Q4<T> dg, od, c;
                 col.step(dg, od, c);
                 if (mine) {
-                    const Q4<T> fv = ld4(f + i);
+                    const Q4<T> fv = ldq<CG>(f + i);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const T r = dg.a[k] > (T)kEps ? fv.a[k] - (dg.a[k] * c.a[k] + od.a[k]) : (T)0;
@@ -829,6 +863,15 @@ __global__ void __launch_bounds__(256, MINB) resid_restrict_q_kernel(T* __restri
             fc[ci + 1] = yb + ob;
         }
     }
+}
+
+// MINB: register-budget variants as for the Jacobi sweep (1 default, 3 or 4 resident CTAs per SM).
+template <typename T, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) resid_restrict_q_kernel(T* __restrict__ fc, const T* __restrict__ v,
+                                                                     const T* __restrict__ f, Lvl<T> L, int ncx,
+                                                                     int ncy, int ncz, int czc) {
+    wp_pdl_enter();
+    resid_restrict_q_body<T>(fc, v, f, L, ncx, ncy, ncz, czc, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
 // resid_restrict_q_kernel with its fine planes' streaming loads (the walker's next centre quad and
@@ -1040,13 +1083,11 @@ __global__ void __launch_bounds__(256, 2) defect64_qp_kernel(float* __restrict__
 }
 
 // trilinear prolongation (prolong_tri_add_kernel) on quads: one 128-bit read-modify-write of v
-template <typename T>
-__global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny,
-                                                            int nz, int ncx, int ncy, int ncz) {
-    wp_pdl_enter();
+template <typename T, bool CG = false>
+__device__ __forceinline__ void prolong_tri_q_body(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny, int nz,
+                                                   int ncx, int ncy, int ncz, int bx, int z, int tid) {
     const int nq = ny >> 2;
-    const long q = (long)blockIdx.x * 256 + threadIdx.x;
-    const int z = blockIdx.y;
+    const long q = (long)bx * 256 + tid;
     if (q >= (long)nx * nq) return;
     const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
     const int px = x >> 1, pz = z >> 1;
@@ -1056,7 +1097,7 @@ __global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, c
     const long sc = (long)ncx * ncy;
     const T a = (T)0.75, b = (T)0.25;
     const long i = y0 + (long)x * ny + (long)z * nx * ny;
-    Q4<T> out = ld4(v + i);
+    Q4<T> out = ldq<CG>(v + i);
     // the quad's coarse y values along one coarse (x, z) row: cy0 - 1, cy0, cy0 + 1, cy0 + 2, with the
     // wall neighbour repeating the parent (ny % 4 == 0, so ncy = ny / 2 and cy0 = y0 / 2 is even)
     const int cy0 = y0 >> 1;
@@ -1066,10 +1107,10 @@ __global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, c
     auto row4 = [&](int xx, int zz) -> Row4 {
         const T* r = vc + cy0 + (long)xx * ncy + zz * sc;
         Row4 o;
-        o.a = r[0];
-        o.b = r[1];
-        o.m = cy0 > 0 ? r[-1] : o.a;
-        o.p = cy0 + 2 < ncy ? r[2] : o.b;
+        o.a = ld1<CG>(r);
+        o.b = ld1<CG>(r + 1);
+        o.m = cy0 > 0 ? ld1<CG>(r - 1) : o.a;
+        o.p = cy0 + 2 < ncy ? ld1<CG>(r + 2) : o.b;
         return o;
     };
     // parent (P) and neighbour (Q) of cell k of the quad in a row
@@ -1103,6 +1144,13 @@ __global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, c
         }
     }
     st4(v + i, out);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, const T* __restrict__ vc, int nx, int ny,
+                                                            int nz, int ncx, int ncy, int ncz) {
+    wp_pdl_enter();
+    prolong_tri_q_body<T>(v, vc, nx, ny, nz, ncx, ncy, ncz, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
 // cell layout of the y-face fractions: fyc[y + x ny + z nx ny] = ay[y + x (ny+1) + z nx (ny+1)]
@@ -1618,10 +1666,10 @@ __device__ __forceinline__ void lean_prolong(const LS& F, const LS& C, int prolo
 // level order), copied with 128-bit loads that keep many requests in flight; the level
 // descriptors live in shared memory (no local-memory arrays), and thread 0 writes back the
 // ping-pong state of a level after its sweeps (every thread swaps its own copy in lockstep).
-__global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu1, int nu2, float w, int citers,
-                                                                 int prolong) {
-    wp_pdl_enter();
-    extern __shared__ __align__(16) float lean_smem[];
+// The body, run by one 1024-thread CTA (also as the coarse phase of mid_cycle_kernel, whose other
+// CTAs wrote the pack's right-hand side in the same grid: hence the L2 load of f).
+__device__ __forceinline__ void lean_cycle(const LPack& P, int nu1, int nu2, float w, int citers, int prolong,
+                                           float* lean_smem) {
     __shared__ LS S[kCoarseMax];
     const int tid = threadIdx.x, B = blockDim.x;
     long cf_floats = 0;
@@ -1669,7 +1717,7 @@ __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu
             q.t[i - q.nxy] = 0.f;
         }
         if (l == 0)
-            for (int i = tid; i < q.cells; i += B) q.f[i] = P.lv[0].f[i];
+            for (int i = tid; i < q.cells; i += B) q.f[i] = __ldcg(P.lv[0].f + i);
     }
     __syncthreads();
     for (int l = 0; l < P.n - 1; ++l) {
@@ -1748,6 +1796,104 @@ __global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu
     float* out = ((nu1 + nu2) & 1) ? P.lv[0].t : P.lv[0].v;
     const float* v0 = S[0].v;
     for (int i = tid; i < S[0].cells; i += B) out[i] = v0[i];
+}
+
+__global__ void __launch_bounds__(1024) coarse_cycle_lean_kernel(LPack P, int nu1, int nu2, float w, int citers,
+                                                                 int prolong) {
+    wp_pdl_enter();
+    extern __shared__ __align__(16) float lean_smem[];
+    lean_cycle(P, nu1, nu2, w, citers, prolong, lean_smem);
+}
+
+// ---- persistent cycle below the finest level --------------------------------------------------
+// Levels 1 .. k of a V-cycle are small (at 256^3: 128^3, 64^3, 32^3), L2-resident and latency bound:
+// as separate launches each sweep costs a launch, a ramp and a tail.  mid_cycle_kernel runs the whole
+// cycle below the finest level in one cooperative launch (one 1024-thread CTA per SM, all resident):
+// a list of phases -- first sweep from zero, sweeps, residual restriction, trilinear prolongation
+// and the single-CTA coarse cycle -- separated by grid barriers.  A phase runs the quad kernels'
+// bodies (the same arithmetic per cell) on virtual 256-thread blocks, four per CTA, with every load
+// of data written earlier in the grid taken through L2 (CG).  The host mirrors the ping-pong swaps and
+// writes each phase's buffers into the list.
+enum { MP_SWEEP0 = 0, MP_SWEEP = 1, MP_RESTRICT = 2, MP_PROLONG = 3, MP_COARSE = 4 };
+constexpr int kMidLevels = 6;
+constexpr int kMidPhases = 48;
+
+struct MidPhase {
+    int type, level, zc, gx, gy;
+    float* dst;        // sweep output / restricted right-hand side / prolongation target
+    const float* src;  // sweep input / fine iterate of the restriction / coarse correction
+    const float* f;    // right-hand side of the level
+};
+struct MidPack {
+    Lvl<float> L[kMidLevels];
+    MidPhase ph[kMidPhases];
+    LPack coarse;
+    int nph, nu1, nu2, citers, prolong;
+    float w;
+    unsigned* bar;  // [arrivals, generation]
+    int* err;
+};
+static_assert(sizeof(MidPack) < 32000, "kernel parameters are limited to 32 KB");
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident): arrivals counted on bar[0], the last
+// one resets it and advances the generation bar[1], the others wait for that (bounded: after
+// kWaitLimitNs the error flag is raised and false returned, and the grid leaves the kernel).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks, int* err) {
+    __syncthreads();
+    int ok = 1;
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) + 1u == nblocks) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const unsigned long long t0 = wptc::globaltimer();
+            while (*gen == g) {
+                if (wptc::globaltimer() - t0 > wptc::kWaitLimitNs) {
+                    atomicOr(err, 2);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
+__global__ void __launch_bounds__(1024, 1) mid_cycle_kernel(MidPack P) {
+    extern __shared__ __align__(16) float lean_smem[];
+    const int sub = threadIdx.x >> 8, tid = threadIdx.x & 255;
+    const int vstep = gridDim.x * 4;
+    for (int k = 0; k < P.nph; ++k) {
+        const MidPhase& ph = P.ph[k];
+        if (ph.type == MP_COARSE) {
+            if (blockIdx.x == 0) lean_cycle(P.coarse, P.nu1, P.nu2, P.w, P.citers, P.prolong, lean_smem);
+        } else {
+            const Lvl<float>& L = P.L[ph.level];
+            const int nv = ph.gx * ph.gy;
+            for (int vb = blockIdx.x * 4 + sub; vb < nv; vb += vstep) {
+                const int bx = vb % ph.gx, by = vb / ph.gx;
+                if (ph.type == MP_SWEEP0) {
+                    jacobi0_q_body<float, true>(ph.dst, ph.f, L, P.w, ph.zc, bx, by, tid);
+                } else if (ph.type == MP_SWEEP) {
+                    jacobi_q_body<float, false, true>(ph.dst, ph.src, ph.f, L, P.w, ph.zc, nullptr, bx, by, tid);
+                } else if (ph.type == MP_RESTRICT) {
+                    const Lvl<float>& C = P.L[ph.level + 1];
+                    resid_restrict_q_body<float, true>(ph.dst, ph.src, ph.f, L, C.nx, C.ny, C.nz, ph.zc, bx, by,
+                                                        tid);
+                } else {
+                    const Lvl<float>& C = P.L[ph.level + 1];
+                    prolong_tri_q_body<float, true>(ph.dst, ph.src, L.nx, L.ny, L.nz, C.nx, C.ny, C.nz, bx, by,
+                                                     tid);
+                }
+            }
+        }
+        if (k + 1 < P.nph && !grid_barrier(P.bar, gridDim.x, P.err)) return;
+    }
 }
 
 // coarse f = spacing-weighted average of the fine residuals of the (up to 8) children
@@ -2235,7 +2381,11 @@ struct wp_mgfrac3d {
     int nl;
     Level lv[kMaxLevels];
     int coarsest_iters;
-    double* acc;       // device reduction slots
+    double* acc;       // device reduction slots; then the int error flag (acc + 4) and the grid
+                       // barrier words of mid_cycle_kernel (8 bytes further)
+    int mid_on;        // run the levels below the finest as one persistent launch (autotuned, default on)
+    int mid_forbid;    // never (handles whose cycles share the GPU with concurrent graph branches)
+    int mid_grid;      // its CTAs (one per SM; 0 = not yet known, -1 = not possible on this device)
     double* p64;       // FP64 iterate for mixed precision
     float* r32;        // FP32 defect (right-hand side of correction cycles)
     const float* fin;  // finest right-hand side of the current solve
@@ -2420,6 +2570,123 @@ wp_status smooth(Level& L, const T* f, int sweeps, T w, cudaStream_t s, bool fin
     return WP_OK;
 }
 
+// The V-cycle below the finest level (from level l1, v = 0) as one mid_cycle_kernel launch when the
+// levels allow it (FP32, trilinear prolongation, nu1 >= 1, quad levels down to a lean coarse pack);
+// sets *done.  The host mirrors every ping-pong swap the phases perform.
+wp_status mid_cycle(wp_mgfrac3d* h, int l1, int nu1, int nu2, float w, int prolong, cudaStream_t s, bool* done) {
+    *done = false;
+    if (!h->mid_on || h->mid_forbid || h->dims != 3 || h->mid_grid < 0 || prolong != WP_PROLONG_TRILINEAR ||
+        nu1 < 1 || l1 < 1)
+        return WP_OK;
+    // the coarse pack starts at the first level the fused coarse cycle takes
+    int lc = -1;
+    for (int l = l1; l < h->nl - 1 && lc < 0; ++l) {
+        long pack = 0;
+        for (int k = l; k < h->nl; ++k) pack += h->lv[k].cells;
+        if (h->lv[l].cells <= kCoarseCells && h->nl - l <= kCoarseMax && pack <= kCoarseSmemCells) lc = l;
+    }
+    if (lc <= l1 || lc - l1 + 1 > kMidLevels) return WP_OK;
+    for (int l = l1; l < lc; ++l) {
+        Level& L = h->lv[l];
+        const Level& C = h->lv[l + 1];
+        if (!quad_ok(L) || C.n[1] * 2 != L.n[1] || !al16(L.v) || !al16(L.t) || !al16(L.f)) return WP_OK;
+    }
+    LPack Q;
+    Q.n = h->nl - lc;
+    for (int k = 0; k < Q.n; ++k) {
+        Level& E = h->lv[lc + k];
+        if (!E.ccf) return WP_OK;
+        Q.lv[k] = {E.n[0], E.n[1], E.n[2], E.ccf, E.v, E.t, E.f};
+    }
+    const size_t lean_bytes = sizeof(float) * (size_t)lean_smem_floats(Q);
+    if (lean_bytes > kLeanSmemMax) return WP_OK;
+    if (h->mid_grid == 0) {
+        int per_sm = 0;
+        if (wp_set_smem(mid_cycle_kernel, kLeanSmemMax) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mid_cycle_kernel, 1024, kLeanSmemMax) !=
+                cudaSuccess ||
+            per_sm < 1) {
+            (void)cudaGetLastError();
+            h->mid_grid = -1;
+            return WP_OK;
+        }
+        h->mid_grid = wp_sm_count();
+    }
+    MidPack P;
+    memset(&P, 0, sizeof(P));
+    for (int l = l1; l <= lc; ++l) P.L[l - l1] = view<float>(h->lv[l]);
+    auto add = [&](int type, int l, float* dst, const float* src, const float* f, int zc, int gx, int gy) {
+        MidPhase& q = P.ph[P.nph++];
+        q.type = type;
+        q.level = l - l1;
+        q.dst = dst;
+        q.src = src;
+        q.f = f;
+        q.zc = zc;
+        q.gx = gx;
+        q.gy = gy;
+    };
+    const int phases = (lc - l1) * (nu1 + 1 + 1 + nu2) + 1;
+    if (phases > kMidPhases) return WP_OK;
+    auto quads = [](const Level& L) { return (int)wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256); };
+    for (int l = l1; l < lc; ++l) {
+        Level& L = h->lv[l];
+        Level& C = h->lv[l + 1];
+        const int zc = 1;  // as many work units as possible: the phases are short
+        add(MP_SWEEP0, l, L.t, nullptr, L.f, zc, quads(L), (int)wp_cdiv(L.n[2], zc));
+        std::swap(L.v, L.t);
+        for (int k = 1; k < nu1; ++k) {
+            add(MP_SWEEP, l, L.t, L.v, L.f, zc, quads(L), (int)wp_cdiv(L.n[2], zc));
+            std::swap(L.v, L.t);
+        }
+        const int czc = 1;
+        add(MP_RESTRICT, l, C.f, L.v, L.f, czc, (int)wp_cdiv((size_t)C.n[0] * (L.n[1] / 4) * 2, 256),
+            (int)wp_cdiv(C.n[2], czc));
+    }
+    add(MP_COARSE, lc, nullptr, nullptr, nullptr, 0, 0, 0);
+    for (int k = 0; k < Q.n; ++k) {
+        Level& E = h->lv[lc + k];
+        const int swaps = (k == Q.n - 1) ? h->coarsest_iters : nu1 + nu2;
+        if (swaps & 1) std::swap(E.v, E.t);
+    }
+    for (int l = lc - 1; l >= l1; --l) {
+        Level& L = h->lv[l];
+        Level& C = h->lv[l + 1];
+        const int zc = 1;
+        add(MP_PROLONG, l, L.v, C.v, nullptr, 0, quads(L), L.n[2]);
+        for (int k = 0; k < nu2; ++k) {
+            add(MP_SWEEP, l, L.t, L.v, L.f, zc, quads(L), (int)wp_cdiv(L.n[2], zc));
+            std::swap(L.v, L.t);
+        }
+    }
+    P.coarse = Q;
+    P.nu1 = nu1;
+    P.nu2 = nu2;
+    P.citers = h->coarsest_iters;
+    P.prolong = prolong;
+    P.w = w;
+    P.err = reinterpret_cast<int*>(h->acc + 4);
+    P.bar = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(h->acc + 4) + 8);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(h->mid_grid);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = lean_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    double bytes = 0.0;
+    for (int l = l1; l < lc; ++l)
+        bytes += (double)h->lv[l].cells * 4.0 * (3.0 * (nu1 + nu2) + 8.0) + 2.0 * frac_bytes(h->lv[l]) * (nu1 + nu2 + 1);
+    // a barrier that gave up in an earlier launch may have left arrivals counted
+    WP_CUDA_TRY(cudaMemsetAsync(P.bar, 0, sizeof(unsigned), s));
+    WP_KERNEL("mid_cycle", bytes, s, cudaLaunchKernelEx(&cfg, mid_cycle_kernel, P));
+    *done = true;
+    return WP_OK;
+}
+
 // One V-cycle at level l from the level's current v, or (clear_v) from v = 0: then v is neither
 // cleared nor read -- the first sweep is jacobi0_q_kernel where the level's kernel allows, otherwise
 // v is cleared first -- and below kCoarseCells the single-launch coarse cycle takes over.
@@ -2430,6 +2697,13 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
     Level& L = h->lv[l];
     const dim3 g = grid_of(L.n[0], L.n[1], L.n[2]);
     wp_status st;
+    if constexpr (sizeof(T) == 4) {
+        if (clear_v && l >= 1) {
+            bool done = false;
+            if ((st = mid_cycle(h, l, nu1, nu2, (float)w, prolong, s, &done)) != WP_OK) return st;
+            if (done) return WP_OK;
+        }
+    }
     long pack_cells = 0;
     for (int k = l; k < h->nl; ++k) pack_cells += h->lv[k].cells;
     if (clear_v && l > 0 && l < h->nl - 1 && L.cells <= kCoarseCells && h->nl - l <= kCoarseMax &&
@@ -2660,6 +2934,7 @@ wp_status create_common(wp_mgfrac3d** out, int dims, const float* ax, const floa
     if (!h) return WP_ERR_INVALID_ARG;
     h->dims = dims;
     h->coarsest_iters = dims == 3 ? 50 : 10;
+    h->mid_on = 1;
     wp_status st = build_hierarchy(h, ax, ay, az, nx, ny, nz, dx, dy, dz, s);
     if (st == WP_OK) {
         cudaError_t e = cudaMalloc((void**)&h->acc, 4 * sizeof(double) + 16);
@@ -3250,6 +3525,24 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
             g_tune_cache[key] = best_zc + 1000 * best_var;
         }
     }
+    // the levels below the finest as one persistent launch, or launch by launch: time a V-cycle from
+    // level 1 both ways (the levels are L2-resident: no flush) and keep the faster
+    if (st == WP_OK && h->dims == 3 && h->nl >= 3 && !h->mid_forbid) {
+        float best = 1e30f;
+        int best_on = 1;
+        for (int on = 1; on >= 0 && st == WP_OK; --on) {
+            h->mid_on = on;
+            Level& L1 = h->lv[1];
+            auto launch = [&]() {
+                vcycle<float>(h, 1, L1.f, 2, 2, 2.f / 3.f, WP_PROLONG_TRILINEAR, s, true);
+            };
+            const float ms = time_launches(launch, s, ea, eb, 5, nullptr, 0);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
+            if (ms < best) { best = ms; best_on = on; }
+        }
+        h->mid_on = best_on;
+    }
     if (flush) {
         cudaStreamSynchronize(s);
         cudaFree(flush);
@@ -3286,6 +3579,12 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_tiles(const wp_mgfrac3d* h, int* zc,
 // Pins the chunk and kernel variant of one level's column kernel (kind 0 jacobi, 1 restrict,
 // 2 defect); zc <= 0 restores the heuristic.
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, int kind, int zc, int variant) {
+    if (h && kind == 3 && (variant == 0 || variant == 1)) {
+        // the levels below the finest: one persistent launch (1) or launch by launch (0)
+        h->mid_on = variant;
+        ++h->tune_gen;
+        return WP_OK;
+    }
     if (!h || level < 0 || level >= h->nl || kind < 0 || kind > 2 || variant < 0 || variant > 6 ||
         (kind == kZcRestrict && variant > 4) || (kind == kZcDefect && variant > 1)) {
         wp_set_error_msg("wp_mgfrac3d_set_tile: bad arguments");
@@ -3312,6 +3611,9 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_uniform_rows(const wp_mgfrac3d* h, i
 }
 
 wp_status wp_mg_prepare_mixed(wp_mgfrac3d* h) { return prepare_mixed(h); }
+// a cooperative launch needs the whole GPU: the batch, whose grids run on concurrent graph branches,
+// keeps every level launch by launch
+void wp_mg_forbid_persistent(wp_mgfrac3d* h) { h->mid_forbid = 1; }
 wp_status wp_mg_solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
                                         cudaStream_t s) {
     return solve_mixed_fixed_async(h, dst, f, cycles, prm, s);
