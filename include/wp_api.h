@@ -253,6 +253,29 @@ CUWHHD_API wp_status wp_dst3d_create(wp_dst3d** h, int nx, int ny, int nz, doubl
 CUWHHD_API wp_status wp_dst3d_solve(wp_dst3d* h, double* dst, const double* f, void* stream);
 CUWHHD_API wp_status wp_dst3d_destroy(wp_dst3d* h);
 
+/* ------------------------------------------------- sweep + DST potential recovery ------- */
+typedef struct wp_sweep3d wp_sweep3d;
+/* Replaces CuParallelSweep3D(int3 dim, DTYPE3 dx, char bc) (cuParallelSweep3D.cu:868-887), the
+   reference's comparison baseline for the wavelet recovery; bc 'n' (others: WP_ERR_UNSUPPORTED).
+   Owns the DST-I solver of the (n-1)^3 interior nodes. */
+CUWHHD_API wp_status wp_sweep3d_create(wp_sweep3d** h, int nx, int ny, int nz, double dx, double dy, double dz,
+                                       char bc);
+/* Replaces CuParallelSweep3D::Solve(qx, qy, qz, xv, yv, zv) (cuParallelSweep3D.cu:939-966): a vector
+   potential with curl q = u for a divergence-free u with no normal flux: qx, qy integrate yv, -xv
+   along z from 0 on z = 0, qz = 0 except the top plane, which takes the x-integral of qx's top
+   plane (then cleared).  q in the edge shapes of wp_recover3d_run. */
+CUWHHD_API wp_status wp_sweep3d_solve(wp_sweep3d* h, float* qx, float* qy, float* qz, const float* xv,
+                                      const float* yv, const float* zv, void* stream);
+/* Replaces CuParallelSweep3D::Project(qx, qy, qz) with bc 'n' = ProjectZero
+   (cuParallelSweep3D.cu:1043-1081, 1316-1326): q -= grad phi with -lap phi = -div q on the interior
+   nodes (DST-I), phi = 0 on the walls, in place. */
+CUWHHD_API wp_status wp_sweep3d_project(wp_sweep3d* h, float* qx, float* qy, float* qz, void* stream);
+CUWHHD_API wp_status wp_sweep3d_destroy(wp_sweep3d* h);
+/* Replaces CuParallelSweep3D(int2, DTYPE2, char)::Solve(qz, xv, yv) with bc 'n'
+   (cuParallelSweep3D.cu:987-1000): qz ((nx+1) x (ny+1)) = 0 on x = 0, -x-integral of yv. */
+CUWHHD_API wp_status wp_sweep2d_solve(float* qz, const float* xv, const float* yv, int nx, int ny, double dx,
+                                      double dy, char bc, void* stream);
+
 /* Allocation-free DST-I Poisson solve.  No reference counterpart (CuDst3D allocates its buffers in
    its constructor).  Same result as wp_dst3d_create + wp_dst3d_solve, but no handle and no device
    allocation on any call: the three DST-I matrices and the intermediate buffer live in one static

@@ -283,6 +283,68 @@ def dst3d_poisson(f, n, d):
     return p
 
 
+# ------------------------------------------------------------ sweep + DST recovery
+def sweep3d_solve(xv, yv, zv, n, d):
+    """CuParallelSweep3D::Solve with bc 'n' (cuParallelSweep3D.cu:939-966): qz = 0; qx, qy start from
+    0 on the z = 0 plane and integrate yv (+dz) and xv (-dz) along z (SweepingQx / SweepingQy,
+    :28-66); then the top plane is made tangential-free: qp = the x-integral of qx's top plane
+    (cuSweepingQ_x, :9-26), qx and qy top planes cleared, qz's top plane gets -qp / dz (CudaMatAdd,
+    cudaMath.cu:110-118).  FP64 sums in the reference's sequential order."""
+    nx, ny, nz = n
+    dx, dy, dz = d
+    xv, yv = _f64(xv), _f64(yv)
+    s = mac_shapes3d(nx, ny, nz)
+    qx, qy, qz = (np.zeros(s[k]) for k in ("qx", "qy", "qz"))
+    for z in range(1, nz + 1):
+        qx[z] = qx[z - 1] + yv[z - 1] * dz
+        qy[z] = qy[z - 1] - xv[z - 1] * dz
+    qp = np.zeros((nx + 1, ny + 1))
+    for x in range(1, nx + 1):
+        qp[x] = qp[x - 1] + qx[nz, x - 1] * dx
+    qx[nz] = 0.0
+    qy[nz] = 0.0
+    qz[nz - 1] += qp * (-1.0 / dz)
+    return qx, qy, qz
+
+
+def sweep3d_project(qx, qy, qz, n, d):
+    """CuParallelSweep3D::ProjectZero (cuParallelSweep3D.cu:1043-1081): b = -div q on the (n-1)^3
+    interior nodes (cuGetB_q_zero_3d, cuConvergence.cu:126-159), the DST-I Poisson solve on them,
+    q -= grad phi with phi = 0 on the boundary nodes (cuGradientMinus3D_zero_Q, cuGradient.cu:2353-2405,
+    including its choice of spacing for the three wall edges)."""
+    nx, ny, nz = n
+    dxi, dyi, dzi = (1.0 / v for v in d)
+    qx, qy, qz = (_f64(a).copy() for a in (qx, qy, qz))
+    b = -((qx[1:nz, 1:nx, 1:ny] - qx[1:nz, 0:nx - 1, 1:ny]) * dxi +
+          (qy[1:nz, 1:nx, 1:ny] - qy[1:nz, 1:nx, 0:ny - 1]) * dyi +
+          (qz[1:nz, 1:nx, 1:ny] - qz[0:nz - 1, 1:nx, 1:ny]) * dzi)
+    P = dst3d_poisson(b, (nx - 1, ny - 1, nz - 1), d)
+    qy[1:nz, 1:nx, 0] -= P[:, :, 0] * dxi
+    qx[1:nz, 0, 1:ny] -= P[:, 0, :] * dyi
+    qz[0, 1:nx, 1:ny] -= P[0, :, :] * dzi
+    gy = -P * dyi
+    gy[:, :, :-1] += P[:, :, 1:] * dyi
+    gx = -P * dxi
+    gx[:, :-1, :] += P[:, 1:, :] * dxi
+    gz = -P * dzi
+    gz[:-1] += P[1:] * dzi
+    qy[1:nz, 1:nx, 1:ny] -= gy
+    qx[1:nz, 1:nx, 1:ny] -= gx
+    qz[1:nz, 1:nx, 1:ny] -= gz
+    return qx, qy, qz
+
+
+def sweep2d_solve(yv, n, d):
+    """CuParallelSweep3D::Solve(qz, xv, yv) with bc 'n' (cuParallelSweep3D.cu:987-1000,
+    SweepingQz_x_0 :106-124): qz = 0 on x = 0, qz[x] = qz[x-1] - yv[x-1] dx."""
+    nx, ny = n
+    yv = _f64(yv)
+    qz = np.zeros((nx + 1, ny + 1))
+    for x in range(1, nx + 1):
+        qz[x] = qz[x - 1] - yv[x - 1] * d[0]
+    return qz
+
+
 # -------------------------------------------------------------------- metrics
 def rel_l2(ref, got) -> float:
     """Relative L2 error, CalculateErrorL2 (Utils.cpp:184-210): sqrt(sum (a-b)^2 / sum a^2)."""

@@ -1,0 +1,75 @@
+"""Sweep + DST potential recovery (CuParallelSweep3D) against the FP64 oracle."""
+import numpy as np
+import pytest
+import torch
+
+from test_oracle_properties import _wall_compatible_potential
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a):
+    return torch.as_tensor(np.asarray(a, dtype=np.float32), device="cuda")
+
+
+def _rel(ref, got):
+    return float(np.abs(np.asarray(got, np.float64) - ref).max() / max(np.abs(ref).max(), 1e-300))
+
+
+@pytest.mark.parametrize("n", [(32, 32, 32), (24, 16, 20), (7, 9, 5)])
+def test_sweep_solve_and_project_match_oracle(wp, oracle, n):
+    d = (1.0 / 32,) * 3
+    s = oracle.mac_shapes3d(*n)
+    u = [a.astype(np.float32).astype(np.float64) for a in oracle.curl3d(*_wall_compatible_potential(s, 5), n, d)]
+    sw = wp.CuParallelSweep3D(n, d, "n")
+    q = [torch.full(s[k], 7.0, device="cuda") for k in ("qx", "qy", "qz")]  # Solve overwrites every entry
+    sw.Solve(*q, *(_t(a) for a in u))
+    torch.cuda.synchronize()
+    ref = oracle.sweep3d_solve(*u, n, d)
+    for r, g in zip(ref, q):
+        assert _rel(r, g.cpu().numpy()) < 2e-6
+    # projection of the same (FP32-stored) potential on both sides
+    q32 = [a.astype(np.float32).astype(np.float64) for a in ref]
+    qg = [_t(a) for a in q32]
+    sw.Project(*qg)
+    torch.cuda.synchronize()
+    refp = oracle.sweep3d_project(*q32, n, d)
+    for r, g in zip(refp, qg):
+        assert _rel(r, g.cpu().numpy()) < 2e-5
+
+
+def test_sweep_recovers_curl_at_128(wp, oracle):
+    """curl q = u after Solve + Project on a 128^3 divergence-free field with no normal flux."""
+    n = (128, 128, 128)
+    d = (1.0 / 128,) * 3
+    s = oracle.mac_shapes3d(*n)
+    u = [a.astype(np.float32).astype(np.float64) for a in oracle.curl3d(*_wall_compatible_potential(s, 9), n, d)]
+    sw = wp.CuParallelSweep3D(n, d, "n")
+    q = [torch.empty(s[k], device="cuda") for k in ("qx", "qy", "qz")]
+    sw.Solve(*q, *(_t(a) for a in u))
+    sw.Project(*q)
+    torch.cuda.synchronize()
+    got = oracle.curl3d(*(t.cpu().numpy().astype(np.float64) for t in q), n, d)
+    assert oracle.rel_l2_multi(u, got) < 1e-5
+    nx, ny, nz = n
+    px, py, pz = (t.cpu().numpy().astype(np.float64) for t in q)
+    div = ((px[1:nz, 1:nx, 1:ny] - px[1:nz, 0:nx - 1, 1:ny]) + (py[1:nz, 1:nx, 1:ny] - py[1:nz, 1:nx, 0:ny - 1]) +
+           (pz[1:nz, 1:nx, 1:ny] - pz[0:nz - 1, 1:nx, 1:ny])) / d[0]
+    assert np.abs(div).max() <= 1e-3 * np.abs(px).max() / d[0]
+
+
+@pytest.mark.parametrize("n", [(32, 48), (257, 33)])
+def test_sweep2d_matches_oracle(wp, oracle, n):
+    d = (1.0 / 64, 1.0 / 64)
+    rng = np.random.default_rng(2)
+    yv = rng.standard_normal((n[0], n[1] + 1)).astype(np.float32).astype(np.float64)
+    xv = np.zeros((n[0] + 1, n[1]))
+    qz = torch.full((n[0] + 1, n[1] + 1), 3.0, device="cuda")
+    wp.CuParallelSweep3D.Solve2D(qz, _t(xv), _t(yv), n, d[0], "n")
+    torch.cuda.synchronize()
+    assert _rel(oracle.sweep2d_solve(yv, n, d), qz.cpu().numpy()) < 2e-6
+
+
+def test_sweep_rejects_other_boundaries(wp):
+    with pytest.raises(wp.WPError):
+        wp.CuParallelSweep3D((8, 8, 8), 1.0 / 8, "d")

@@ -459,6 +459,50 @@ class CuDst3D:
             pass
 
 
+class CuParallelSweep3D:
+    """CuParallelSweep3D (cuParallelSweep3D.cuh): the sweep + DST-I potential recovery, the
+    reference's comparison baseline for the wavelet recovery (bc 'n').  3D: Solve then Project gives
+    a divergence-free vector potential with curl q = u; 2D: Solve2D (qz from the velocity)."""
+
+    def __init__(self, dim, dx, bc="n"):
+        self.dim = _dims3(dim)
+        self.dx = _dx3(dx)
+        h = ctypes.c_void_p()
+        check(lib().wp_sweep3d_create(ctypes.byref(h), *self.dim, *self.dx, _c(bc)), "wp_sweep3d_create")
+        self._h = h
+        self.shapes = mac_shapes3d(*self.dim)
+
+    def Solve(self, qx, qy, qz, xv, yv, zv, stream=None):
+        s = self.shapes
+        check(lib().wp_sweep3d_solve(self._h, _ptr(qx, s["qx"]), _ptr(qy, s["qy"]), _ptr(qz, s["qz"]),
+                                     _ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]), _stream(stream)),
+              "wp_sweep3d_solve")
+
+    def Project(self, qx, qy, qz, stream=None):
+        s = self.shapes
+        check(lib().wp_sweep3d_project(self._h, _ptr(qx, s["qx"]), _ptr(qy, s["qy"]), _ptr(qz, s["qz"]),
+                                       _stream(stream)), "wp_sweep3d_project")
+
+    @staticmethod
+    def Solve2D(qz, xv, yv, dim, dx, bc="n", stream=None):
+        nx, ny = (int(v) for v in dim)
+        d = (float(dx), float(dx)) if not isinstance(dx, (tuple, list)) else (float(dx[0]), float(dx[1]))
+        s = mac_shapes2d(nx, ny)
+        check(lib().wp_sweep2d_solve(_ptr(qz, s["qz"]), _ptr(xv, s["xv"]), _ptr(yv, s["yv"]), nx, ny, *d, _c(bc),
+                                     _stream(stream)), "wp_sweep2d_solve")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().wp_sweep3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 WARM_START_ACCEPT = 0.3  # relative residual after one V-cycle below which the network's guess is kept
 
 
