@@ -275,6 +275,29 @@ def run_ours(args, rank, world, local_rank):
         plain["mixed_" + ("zero" if other == api.START_ZERO else "fmg") + "_start"] = time_variant(
             api.Projector3D(*a, nn, h, start=other, **mixed))
         plain["mixed_host_loop"] = time_variant(api.Projector3D(*a, nn, h, start=start, host_loop=True, **mixed))
+        # the recovery stage alone: the wavelet recovery against the reference's comparison baseline,
+        # sweep + DST-I (CuParallelSweep3D Solve + Project), on the same projected velocity
+        for d, src in zip(u, u0):
+            d.copy_(src)
+        proj.run(*u, *q)
+        sw = api.CuParallelSweep3D(nn, h, "n")
+        qs = [torch.empty_like(t) for t in q]
+
+        def time_rec(fn, k=5):
+            fn()
+            torch.cuda.synchronize()
+            g0.record(stream)
+            for _ in range(k):
+                fn()
+            g1.record(stream)
+            torch.cuda.synchronize()
+            return g0.elapsed_time(g1) / k
+
+        plain["recovery"] = {
+            "wavelet_ms": time_rec(lambda: proj.rec.Solve(*q, *u)),
+            "sweep_dst_ms": time_rec(lambda: (sw.Solve(*qs, *u), sw.Project(*qs))),
+        }
+        sw.close()
     tiles = proj.mg.Tiles(with_times=True)
     return ms, ems, ek, h2d, d2h, launches, prof, reps, clk.summary(), plain, (tiles, psteps, prof_ms)
 
