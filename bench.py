@@ -300,6 +300,22 @@ def run_ours(args, rank, world, local_rank):
             "sweep_dst_ms": time_rec(lambda: (sw.Solve(*qs, *u), sw.Project(*qs))),
         }
         sw.close()
+        # the index-sparse cycle (CuMultigridFrac3D::Solve_index) against the dense reference cycle
+        # (CuMultigridFrac3D::Solve) on a mostly-solid domain of the same extent: balls of fluid
+        # filling 15% of the cells, four V(2,2) cycles, omega 0.8 (the reference's defaults)
+        from waveletpotentials_b200 import fields as wf
+        fl, fa, frng = wf.porous_domain(nn, 0.15, args.seed)
+        tff = torch.as_tensor(frng.standard_normal(fl.shape) * fl, dtype=torch.float32, device=dev)
+        mgp = api.CuMultigridFrac3D(*(torch.as_tensor(x, dtype=torch.float32, device=dev) for x in fa), nn, h)
+        dp = torch.zeros_like(tff)
+        cells, _ = mgp.IndexSizes()
+        plain["index_sparse"] = {
+            "workload": f"{n}^3 cells, {fl.mean():.3f} fluid (balls in a solid block), 4 V(2,2) cycles, omega 0.8",
+            "listed_cells": [int(c) for c in cells],
+            "index_ms_per_cycle": time_rec(lambda: mgp.Solve_index(dp, None, tff, 4, 2, 2, 0.8)) / 4,
+            "dense_ms_per_cycle": time_rec(lambda: mgp.Solve(dp, None, tff, 4, 2, 2, 0.8)) / 4,
+        }
+        mgp.close()
     tiles = proj.mg.Tiles(with_times=True)
     return ms, ems, ek, h2d, d2h, launches, prof, reps, clk.summary(), plain, (tiles, psteps, prof_ms)
 

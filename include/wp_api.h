@@ -152,6 +152,26 @@ CUWHHD_API wp_status wp_mgfrac3d_create(wp_mgfrac3d** h, const float* ax, const 
    exactly n_iters V-cycles in FP32.  pre_v may be NULL (zero start) or equal dst. */
 CUWHHD_API wp_status wp_mgfrac3d_solve(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f, int n_iters,
                                        int nu1, int nu2, double weight, void* stream);
+/* Replaces CuMultigridFrac3D::Solve_index(dst, pre_v, f, n_iters, nu1, nu2, weight)
+   (cuMultigridFrac3D.cu:347-420, index lists InitIndex :189-229, CuBoundSelector::SelectByFrac
+   cuBoundSelector.cu:4-32): n_iters FP32 V-cycles that sweep, restrict and prolong only the cells
+   with a face fraction >= 1e-12 ("listed" cells), for mostly-solid domains.  As the reference:
+   post-smoothing runs nu1 sweeps (nu2 is checked and otherwise unused); unlisted finest cells keep
+   their start value (pre_v, or 0); the cycle descends while the next level lists a cell, then runs
+   the coarsest solve; the residual workspace is shared by all levels and kept by the handle between
+   calls (zero when the lists are built), and the restriction reads it at every child of a listed
+   coarse cell.  The first call builds the lists (synchronous); 3D handles only. */
+CUWHHD_API wp_status wp_mgfrac3d_solve_index(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f,
+                                             int n_iters, int nu1, int nu2, double weight, void* stream);
+/* The same cycle in FP64, the reference's default DTYPE (DoubleUseDefine.h): dst, pre_v and f are
+   double arrays of cells; it has its own residual workspace.  It overwrites the level arrays that
+   hold the FP64 tolerance solve's iterate (wp_mgfrac3d_iterate64 then reports none). */
+CUWHHD_API wp_status wp_mgfrac3d_solve_index64(wp_mgfrac3d* h, double* dst, const double* pre_v, const double* f,
+                                               int n_iters, int nu1, int nu2, double weight, void* stream);
+/* Listed cells (the reference's v_index_size_) and 32-cell row segments per level, first
+   min(cap, levels); builds the lists if needed.  No reference counterpart. */
+CUWHHD_API wp_status wp_mgfrac3d_index_sizes(wp_mgfrac3d* h, long long* cells, long long* segments, int cap,
+                                             int* levels, void* stream);
 /* Tolerance-driven solve with a precision mode; synchronous (reads residual norms on the host).
    Solves the compatible problem A p = f - m, m = mean of f over the active cells (diag > 0), so the
    FP32 rounding of f does not floor the residual; the residual reported is ||f - m - A p|| / ||f||.

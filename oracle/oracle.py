@@ -62,6 +62,7 @@ def lib():
             "or_fractions3d": (None, [p, p, p, p, i, i, i, d]),
             "or_fractions2d": (None, [p, p, p, i, i, d]),
             "or_mgfrac3d_solve": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, i, p]),
+            "or_mgfrac3d_solve_index": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, p, p]),
             "or_mgfrac2d_solve": (i, [p, p, p, p, p, i, i, d, d, i, i, i, d, i, p]),
             "or_frac_residual3d": (d, [p, p, p, p, p, p, i, i, i, d, d, d]),
             "or_frac_residual2d": (d, [p, p, p, p, p, i, i, d, d]),
@@ -250,6 +251,18 @@ def mgfrac3d_solve(f, ax, ay, az, n, d, ncycles, nu1, nu2, omega, p0=None, prolo
                             _p(_f64(ay)), _p(_f64(az)), nx, ny, nz, *d, ncycles, nu1, nu2, omega, prolong,
                             _p(hist))
     return p, hist[:ncycles]
+
+
+def mgfrac3d_solve_index(f, ax, ay, az, n, d, ncycles, nu1, nu2, omega, p0=None):
+    """Index-sparse V-cycles (CuMultigridFrac3D::Solve_index); returns (p, history, listed cells per level)."""
+    nx, ny, nz = n
+    p = np.zeros((nz, nx, ny))
+    hist = np.zeros(max(ncycles, 1))
+    counts = np.zeros(32, dtype=np.int64)
+    nl = lib().or_mgfrac3d_solve_index(_p(p), _p(None if p0 is None else _f64(p0)), _p(_f64(f)), _p(_f64(ax)),
+                                       _p(_f64(ay)), _p(_f64(az)), nx, ny, nz, *d, ncycles, nu1, nu2, omega,
+                                       _p(hist), counts.ctypes.data_as(ctypes.c_void_p))
+    return p, hist[:ncycles], counts[:nl].copy()
 
 
 def mgfrac2d_solve(f, ax, ay, n, d, ncycles, nu1, nu2, omega, p0=None, prolong=PROLONG_CONSTANT):

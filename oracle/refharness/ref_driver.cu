@@ -165,6 +165,50 @@ int main(int argc, char** argv) {
         checkCudaErrors(cudaDeviceSynchronize());
         write_bin("p", from_dev(p, n));
         write_bin("hist", hist);
+    } else if (op == "mg3d_index") {  // nx ny nz dx ncycles nu1 nu2 omega [time_reps]
+        // CuMultigridFrac3D::Solve_index one cycle per call (the residual workspace carries over
+        // between calls, as between the cycles of one call); with time_reps > 0 also the best of
+        // time_reps timed calls of ncycles cycles each, index-sparse and dense, on fresh iterates.
+        int3 dim = make_int3(I(0), I(1), I(2));
+        DTYPE h = (DTYPE)D(3);
+        DTYPE3 dx = make_DTYPE3(h, h, h);
+        int ncycles = I(4), nu1 = I(5), nu2 = I(6);
+        DTYPE w = (DTYPE)D(7);
+        int reps = argc > 12 ? I(8) : 0;
+        size_t n = (size_t)dim.x * dim.y * dim.z;
+        DTYPE* f = to_dev(read_bin("f", n));
+        DTYPE* ax = to_dev(read_bin("ax", (size_t)(dim.x + 1) * dim.y * dim.z));
+        DTYPE* ay = to_dev(read_bin("ay", (size_t)dim.x * (dim.y + 1) * dim.z));
+        DTYPE* az = to_dev(read_bin("az", (size_t)dim.x * dim.y * (dim.z + 1)));
+        DTYPE* p = dev_zeros(n);
+        CuMultigridFrac3D mg(ax, ay, az, dim, dx, 'n');
+        std::vector<double> hist;
+        for (int c = 0; c < ncycles; ++c) {
+            mg.Solve_index(p, c == 0 ? nullptr : p, f, 1, nu1, nu2, w);
+            hist.push_back((double)mg.GetResdualError(p, f));
+        }
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("p", from_dev(p, n));
+        write_bin("hist", hist);
+        if (reps > 0) {
+            cudaEvent_t e0, e1;
+            checkCudaErrors(cudaEventCreate(&e0));
+            checkCudaErrors(cudaEventCreate(&e1));
+            std::vector<double> best = {1e30, 1e30};
+            for (int k = 0; k < 2; ++k)
+                for (int r = 0; r < reps + 1; ++r) {
+                    checkCudaErrors(cudaDeviceSynchronize());
+                    checkCudaErrors(cudaEventRecord(e0));
+                    if (k == 0) mg.Solve_index(p, nullptr, f, ncycles, nu1, nu2, w);
+                    else mg.Solve(p, nullptr, f, ncycles, nu1, nu2, w);
+                    checkCudaErrors(cudaEventRecord(e1));
+                    checkCudaErrors(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    checkCudaErrors(cudaEventElapsedTime(&ms, e0, e1));
+                    if (r > 0 && ms < best[k]) best[k] = ms;  // the first call of each is a warm-up
+                }
+            write_bin("timing", best);
+        }
     } else if (op == "mg2d") {  // nx ny dx ncycles nu1 nu2 omega
         int2 dim = make_int2(I(0), I(1));
         DTYPE h = (DTYPE)D(2);

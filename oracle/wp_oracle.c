@@ -998,11 +998,10 @@ double or_frac_residual3d(double* r, const double* p, const double* f, const dou
     return res;
 }
 
-/* CuMultigridFrac3D ctor (cuMultigridFrac3D.cu:9-134) + Solve (:249-265) */
-int or_mgfrac3d_solve(double* p, const double* p0, const double* f, const double* ax, const double* ay,
-                      const double* az, int nx, int ny, int nz, double dx, double dy, double dz,
-                      int ncycles, int nu1, int nu2, double omega, int prolong, double* history) {
-    mg3_level lv[32];
+/* CuMultigridFrac3D ctor (cuMultigridFrac3D.cu:9-134): the coarse hierarchy (ceil halving until the
+   smallest extent is 1), face fractions coarsened by SolveP1Ax/Ay/Az, spacings summed pairwise */
+static int build_levels3d(mg3_level* lv, const double* ax, const double* ay, const double* az, int nx, int ny,
+                          int nz, double dx, double dy, double dz) {
     int nl = 0;
     int n[3] = {nx, ny, nz};
     int mn = nx < ny ? (nx < nz ? nx : nz) : (ny < nz ? ny : nz);
@@ -1035,23 +1034,176 @@ int or_mgfrac3d_solve(double* p, const double* p0, const double* f, const double
         for (int a = 0; a < 3; ++a) n[a] = half_up(n[a]);
         mn = n[0] < n[1] ? (n[0] < n[2] ? n[0] : n[2]) : (n[1] < n[2] ? n[1] : n[2]);
     }
+    return nl;
+}
+
+static void free_levels3d(mg3_level* lv, int nl) {
+    for (int l = 0; l < nl; ++l) {
+        free(lv[l].v); free(lv[l].f); free(lv[l].ax); free(lv[l].ay); free(lv[l].az);
+        for (int a = 0; a < 3; ++a) free(lv[l].d[a]);
+    }
+}
+
+static double rel_residual_l0(mg3_level* lv, double* r) {
+    const mg3_level* c = &lv[0];
+    long N = (long)c->n[0] * c->n[1] * c->n[2];
+    residual3d(r, c->v, c->f, c->ax, c->ay, c->az, c->n[0], c->n[1], c->n[2], c->d[0], c->d[1], c->d[2]);
+    return sqrt(norm2(r, N)) / sqrt(norm2(c->f, N));
+}
+
+/* CuMultigridFrac3D::Solve (cuMultigridFrac3D.cu:249-265) */
+int or_mgfrac3d_solve(double* p, const double* p0, const double* f, const double* ax, const double* ay,
+                      const double* az, int nx, int ny, int nz, double dx, double dy, double dz,
+                      int ncycles, int nu1, int nu2, double omega, int prolong, double* history) {
+    mg3_level lv[32];
+    int nl = build_levels3d(lv, ax, ay, az, nx, ny, nz, dx, dy, dz);
     long N = (long)nx * ny * nz;
     if (p0) memcpy(lv[0].v, p0, sizeof(double) * N);
     memcpy(lv[0].f, f, sizeof(double) * N);
     double* r = history ? (double*)malloc(sizeof(double) * N) : NULL;
     for (int c = 0; c < ncycles; ++c) {
         vcycle3d(lv, nl, 0, nu1, nu2, omega, prolong);
-        if (history) {
-            residual3d(r, lv[0].v, lv[0].f, lv[0].ax, lv[0].ay, lv[0].az, nx, ny, nz, lv[0].d[0], lv[0].d[1], lv[0].d[2]);
-            history[c] = sqrt(norm2(r, N)) / sqrt(norm2(lv[0].f, N));
-        }
+        if (history) history[c] = rel_residual_l0(lv, r);
     }
     memcpy(p, lv[0].v, sizeof(double) * N);
     free(r);
-    for (int l = 0; l < nl; ++l) {
-        free(lv[l].v); free(lv[l].f); free(lv[l].ax); free(lv[l].ay); free(lv[l].az);
-        for (int a = 0; a < 3; ++a) free(lv[l].d[a]);
+    free_levels3d(lv, nl);
+    return nl;
+}
+
+/* ------------------------------------------- index-sparse fractional multigrid 3D ---- */
+/* CuBoundSelector::SelectByFrac (cuBoundSelector.cu:4-32): a cell takes part in the index-sparse
+   cycle when any of its six face fractions is >= 1e-12 (boundary faces included); InitIndex
+   (cuMultigridFrac3D.cu:189-229) lists those cells per level. */
+static unsigned char* active_cells3d(const mg3_level* c, long* count) {
+    const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+    const long sl = (long)nx * ny;
+    unsigned char* a = (unsigned char*)malloc((size_t)sl * nz);
+    long cnt = 0;
+    for (int z = 0; z < nz; ++z)
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y) {
+                long i = y + (long)x * ny + z * sl;
+                long iax = y + (long)x * ny + (long)z * (nx + 1) * ny, iay = y + (long)x * (ny + 1) + (long)z * nx * (ny + 1);
+                int on = !(c->ax[iax] < EPS12 && c->ax[iax + ny] < EPS12 && c->ay[iay] < EPS12 && c->ay[iay + 1] < EPS12 &&
+                           c->az[i] < EPS12 && c->az[i + sl] < EPS12);
+                a[i] = (unsigned char)on;
+                cnt += on;
+            }
+    *count = cnt;
+    return a;
+}
+
+/* CuWeightedJacobi3D::SolveFrac with an index list (cuWeightedJacobi3D.cu:2821-2897, 2979-3011):
+   the sweep updates the listed cells only; every other cell keeps its value */
+static void jacobi3d_index(mg3_level* c, const unsigned char* act, int sweeps, double w, double* tmp) {
+    const long n = (long)c->n[0] * c->n[1] * c->n[2];
+    for (int s = 0; s < sweeps; ++s) {
+        memcpy(tmp, c->v, sizeof(double) * n);
+#pragma omp parallel for schedule(static)
+        for (int z = 0; z < c->n[2]; ++z)
+            for (int x = 0; x < c->n[0]; ++x)
+                for (int y = 0; y < c->n[1]; ++y) {
+                    long i = y + (long)x * c->n[1] + (long)z * c->n[0] * c->n[1];
+                    if (!act[i]) continue;
+                    double dg, od;
+                    frac_row3d(c->v, c->ax, c->ay, c->az, c->n[0], c->n[1], c->n[2], c->d[0], c->d[1], c->d[2], x, y, z,
+                               &dg, &od);
+                    tmp[i] = dg > EPS12 ? (1.0 - w) * c->v[i] + w * (c->f[i] - od) / dg : 0.0;
+                }
+        memcpy(c->v, tmp, sizeof(double) * n);
     }
+}
+
+/* SolveOneVCycle_index (cuMultigridFrac3D.cu:366-420).  R is the residual workspace shared by all
+   levels (the reference's "mg3d" buffer): the residual kernel (cuWjGetFracRes_3d_n with an index,
+   cuWeightedJacobi3D.cu:3013-3090) writes the listed cells of the level only, and the restriction
+   (cuRestrict3D_p1_dx_whole, cuRestrict3D.cu:1146-1193) reads all children of each listed coarse
+   cell, so an unlisted child contributes whatever R last held at its position (zero until some
+   level wrote there).  Post-smoothing runs nu1 sweeps, as the reference passes nu1 there. */
+static void vcycle3d_index(mg3_level* lv, unsigned char* const* act, const long* cnt, int nl, int l, int nu1,
+                           double w, double* R, double* tmp) {
+    mg3_level* c = &lv[l];
+    const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+    if (l < nl - 1 && cnt[l + 1] > 0) {
+        jacobi3d_index(c, act[l], nu1, w, tmp);
+#pragma omp parallel for schedule(static)
+        for (int z = 0; z < nz; ++z)
+            for (int x = 0; x < nx; ++x)
+                for (int y = 0; y < ny; ++y) {
+                    long i = y + (long)x * ny + (long)z * nx * ny;
+                    if (!act[l][i]) continue;
+                    double dg, od;
+                    frac_row3d(c->v, c->ax, c->ay, c->az, nx, ny, nz, c->d[0], c->d[1], c->d[2], x, y, z, &dg, &od);
+                    R[i] = dg > EPS12 ? c->f[i] - (dg * c->v[i] + od) : 0.0;
+                }
+        mg3_level* k = &lv[l + 1];
+        const int cx = k->n[0], cy = k->n[1], cz = k->n[2];
+#pragma omp parallel for schedule(static)
+        for (int z = 0; z < cz; ++z)
+            for (int x = 0; x < cx; ++x)
+                for (int y = 0; y < cy; ++y) {
+                    long ci = y + (long)x * cy + (long)z * cx * cy;
+                    if (!act[l + 1][ci]) continue;
+                    int xs = 2 * x, ys = 2 * y, zs = 2 * z;
+                    int hx = xs < nx - 1, hy = ys < ny - 1, hz = zs < nz - 1;
+                    double wxl = c->d[0][xs], wyl = c->d[1][ys], wzl = c->d[2][zs];
+                    double wxr = hx ? c->d[0][xs + 1] : 0.0, wyr = hy ? c->d[1][ys + 1] : 0.0, wzr = hz ? c->d[2][zs + 1] : 0.0;
+                    long ox = hx ? ny : 0, oy = hy ? 1 : 0, oz = hz ? (long)nx * ny : 0;
+                    long s0 = ys + (long)xs * ny + (long)zs * nx * ny;
+                    double val = wxl * wyl * wzl * R[s0];
+                    val += wxl * wyr * wzl * R[s0 + oy];
+                    val += wxr * wyl * wzl * R[s0 + ox];
+                    val += wxr * wyr * wzl * R[s0 + oy + ox];
+                    s0 += oz;
+                    val += wxl * wyl * wzr * R[s0];
+                    val += wxl * wyr * wzr * R[s0 + oy];
+                    val += wxr * wyl * wzr * R[s0 + ox];
+                    val += wxr * wyr * wzr * R[s0 + oy + ox];
+                    k->f[ci] = val / ((wxl + wxr) * (wyl + wyr) * (wzl + wzr));
+                }
+        memset(k->v, 0, sizeof(double) * (size_t)cx * cy * cz);
+        vcycle3d_index(lv, act, cnt, nl, l + 1, nu1, w, R, tmp);
+        /* cuProlongate3D_p1_whole_add (cuProlongate3D.cu:619-640): listed cells only */
+        for (int z = 0; z < nz; ++z)
+            for (int x = 0; x < nx; ++x)
+                for (int y = 0; y < ny; ++y) {
+                    long i = y + (long)x * ny + (long)z * nx * ny;
+                    if (act[l][i]) c->v[i] += k->v[y / 2 + (long)(x / 2) * cy + (long)(z / 2) * cx * cy];
+                }
+        jacobi3d_index(c, act[l], nu1, w, tmp);
+    } else {
+        coarsest3d(c->v, c->f, c->ax, c->ay, c->az, nx, ny, nz, c->d[0], c->d[1], c->d[2], w);
+    }
+}
+
+/* CuMultigridFrac3D::Solve_index (cuMultigridFrac3D.cu:347-364) from a fresh residual workspace;
+   counts (may be NULL) receives the listed cells per level.  nu2 is accepted and not used. */
+int or_mgfrac3d_solve_index(double* p, const double* p0, const double* f, const double* ax, const double* ay,
+                            const double* az, int nx, int ny, int nz, double dx, double dy, double dz, int ncycles,
+                            int nu1, int nu2, double omega, double* history, long* counts) {
+    (void)nu2;
+    mg3_level lv[32];
+    int nl = build_levels3d(lv, ax, ay, az, nx, ny, nz, dx, dy, dz);
+    unsigned char* act[32];
+    long cnt[32];
+    for (int l = 0; l < nl; ++l) {
+        act[l] = active_cells3d(&lv[l], &cnt[l]);
+        if (counts) counts[l] = cnt[l];
+    }
+    long N = (long)nx * ny * nz;
+    if (p0) memcpy(lv[0].v, p0, sizeof(double) * N);
+    memcpy(lv[0].f, f, sizeof(double) * N);
+    double* R = (double*)calloc(N, sizeof(double));
+    double* tmp = (double*)malloc(sizeof(double) * N);
+    for (int c = 0; c < ncycles; ++c) {
+        vcycle3d_index(lv, act, cnt, nl, 0, nu1, omega, R, tmp);
+        if (history) history[c] = rel_residual_l0(lv, tmp);
+    }
+    memcpy(p, lv[0].v, sizeof(double) * N);
+    free(R); free(tmp);
+    for (int l = 0; l < nl; ++l) free(act[l]);
+    free_levels3d(lv, nl);
     return nl;
 }
 

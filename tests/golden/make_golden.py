@@ -3,12 +3,14 @@
 Run on a GPU host after ``make -C oracle/refharness`` has built ``oracle/_ref/ref_driver`` from the
 unmodified reference sources (FP64, the reference default):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py --only index   # the index-sparse multigrid cases only
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
 (CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D::ProjectLocal_q_ccc,
 CuDivLocalProject::ProjectSingle, CuWaveletPotentialRecover3D/2D::Solve, CuMultigridFrac3D/2D::Solve,
-CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P, CuSolidLevelSet3D) and stores inputs
+CuMultigridFrac3D::Solve_index, CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P,
+CuSolidLevelSet3D) and stores inputs
 and reference outputs as ``<case>.npz``.  The CPU tests pin the FP64 oracle against these files;
 the GPU tests compare the CUDA kernels with the oracle on the same inputs.
 """
@@ -23,6 +25,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+from waveletpotentials_b200.fields import porous_fractions  # noqa: E402
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 CDF4_6, CDF3_7 = 7, 11
 
@@ -49,9 +54,46 @@ def shapes3(n):
             "qx": (nz + 1, nx, ny + 1), "qy": (nz + 1, nx + 1, ny), "qz": (nz, nx + 1, ny + 1), "p": (nz, nx, ny)}
 
 
+def index_cases(rng):
+    """CuMultigridFrac3D::Solve_index on mostly-solid domains: tubes and a sphere in a non-cubic box,
+    a fluid island whose coarse level lists no cell (the cycle stops at the finest level), and the
+    inside of a sphere (the reference's own fractions, inverted)."""
+    n = (24, 20, 18)
+    nx, ny, nz = n
+    z, x, y = np.meshgrid(np.arange(nz) + 0.5, np.arange(nx) + 0.5, np.arange(ny) + 0.5, indexing="ij")
+    fluid = ((x - 7) ** 2 + (y - 9) ** 2 < 9) | ((z - 5) ** 2 + (y - 13) ** 2 < 6) | \
+            ((x - 16) ** 2 + (y - 6) ** 2 + (z - 11) ** 2 < 20)
+    cases = [("mg3d_index_pores", n, fluid, 40, True, 4, (2, 3), 0.8)]
+    # the cycle stops at the finest level; the reference's coarsest kernel (cuWjFrac3D_kernel_n) holds
+    # at most 512 cells (one CTA of shared memory), so the island case stays at 8^3
+    isl = np.zeros((8, 8, 8), dtype=bool)
+    isl[2:4, 4:6, 2:4] = True
+    cases.append(("mg3d_index_island", (8, 8, 8), isl, 0, False, 3, (2, 2), 0.8))
+    for tag, nn, fl, tiny, cut, cyc, nu, w in cases:
+        ax, ay, az = porous_fractions(fl, rng, tiny, cut)
+        f = rng.standard_normal(fl.shape)
+        out = run("mg3d_index", {"f": f, "ax": ax, "ay": ay, "az": az}, [*nn, 1.0 / nn[0], cyc, nu[0], nu[1], w],
+                  {"p": fl.shape, "hist": (cyc,)})
+        save(tag, n=np.array(nn), h=1.0 / nn[0], f=f, ax=ax, ay=ay, az=az, ncycles=cyc, nu=np.array(nu), omega=w,
+             **out)
+    n3 = 32
+    s = shapes3((n3, n3, n3))
+    fr = run("frac3d", {}, [n3, 1.0 / n3, 0.5, 0.5, 0.45, 0.4], {k: s[k2] for k, k2 in
+                                                                (("ax", "xv"), ("ay", "yv"), ("az", "zv"))})
+    ax, ay, az = (1.0 - fr[k] for k in ("ax", "ay", "az"))
+    f = rng.standard_normal(s["p"])
+    out = run("mg3d_index", {"f": f, "ax": ax, "ay": ay, "az": az}, [n3, n3, n3, 1.0 / n3, 3, 2, 2, 2.0 / 3.0],
+              {"p": s["p"], "hist": (3,)})
+    save("mg3d_index_sphere32", n=np.array([n3] * 3), h=1.0 / n3, f=f, ax=ax, ay=ay, az=az, ncycles=3,
+         nu=np.array([2, 2]), omega=2.0 / 3.0, **out)
+
+
 def main():
     if not os.path.exists(DRIVER):
         sys.exit(f"{DRIVER} missing: run make -C oracle/refharness first (needs nvcc and the reference sources)")
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "index":
+        index_cases(np.random.default_rng(20261204))
+        return
     rng = np.random.default_rng(20261203)
 
     # 1D transforms along every axis, both wavelets, both boundary types, both directions
@@ -168,6 +210,7 @@ def main():
     f2 -= f2.mean()
     out = run("mg2d", {"f": f2, "ax": ax2, "ay": ay2}, [*n2, 1.0 / 32, 5, 5, 5, 0.8], {"p": n2, "hist": (5,)})
     save("mg2d_32", n=np.array(n2), h=1.0 / 32, f=f2, ax=ax2, ay=ay2, ncycles=5, nu=np.array([5, 5]), omega=0.8, **out)
+    index_cases(np.random.default_rng(20261204))
 
 
 if __name__ == "__main__":

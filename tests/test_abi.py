@@ -62,6 +62,8 @@ def test_multigrid_rejects_bad_arguments(L):
     prm = _lib.MgParams(10, 2, 2, 0.8, 1e-6, 7, 1)
     assert L.wp_mgfrac3d_solve_tol(None, dummy, None, dummy, ctypes.byref(prm), None, None) == 1
     assert L.wp_mgfrac2d_solve(None, dummy, None, dummy, 3, 2, 2, 0.8, None) == 1
+    assert L.wp_mgfrac3d_solve_index(None, dummy, None, dummy, 3, 2, 2, 0.8, None) == 1
+    assert L.wp_mgfrac3d_index_sizes(None, None, None, 4, None, None) == 1
 
 
 def test_field_operators_reject_bad_arguments(L):

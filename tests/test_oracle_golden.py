@@ -95,6 +95,35 @@ def test_mg3d_matches_reference_per_cycle(oracle, name):
     assert oracle.rel_l2(p["p"], sol) < 1e-11
 
 
+@pytest.mark.parametrize("name", ["mg3d_index_pores", "mg3d_index_island", "mg3d_index_sphere32"])
+def test_mg3d_index_matches_reference_per_cycle(oracle, name):
+    """CuMultigridFrac3D::Solve_index, one cycle per call: the oracle's index-sparse cycle, including
+    the residual workspace shared by the levels and nu1 post-sweeps, follows the reference build."""
+    p = load_golden(name)
+    n = tuple(int(v) for v in p["n"])
+    h = float(p["h"])
+    sol, hist, counts = oracle.mgfrac3d_solve_index(p["f"], p["ax"], p["ay"], p["az"], n, (h,) * 3,
+                                                    int(p["ncycles"]), int(p["nu"][0]), int(p["nu"][1]),
+                                                    float(p["omega"]))
+    np.testing.assert_allclose(hist, p["hist"], rtol=1e-9)
+    assert oracle.rel_l2(p["p"], sol) < 1e-11
+    assert counts[0] < np.prod(n) and (name != "mg3d_index_island" or counts[1] == 0)
+
+
+def test_mg3d_index_oracle_reduces_to_the_dense_cycle_without_solids(oracle):
+    """Every cell listed: the index-sparse cycle is the reference V-cycle with nu2 = nu1."""
+    n = (12, 10, 8)
+    s = oracle.mac_shapes3d(*n)
+    rng = np.random.default_rng(4)
+    a = [np.ones(s[k]) for k in ("xv", "yv", "zv")]
+    f = rng.standard_normal(s["p"])
+    pi, hi, counts = oracle.mgfrac3d_solve_index(f, *a, n, (0.1,) * 3, 3, 2, 5, 0.8)
+    pd, hd = oracle.mgfrac3d_solve(f, *a, n, (0.1,) * 3, 3, 2, 2, 0.8)
+    assert list(counts) == [int(np.prod(n)), 6 * 5 * 4, 3 * 3 * 2]
+    np.testing.assert_allclose(hi, hd, rtol=1e-13)
+    assert oracle.rel_l2(pd, pi) < 1e-13
+
+
 def test_mg2d_matches_reference_per_cycle(oracle):
     p = load_golden("mg2d_32")
     n = tuple(int(v) for v in p["n"])

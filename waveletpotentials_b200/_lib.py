@@ -70,6 +70,9 @@ SIGNATURES = {
     "wp_recover2d_destroy": (I, [P]),
     "wp_mgfrac3d_create": (I, [PP, P, P, P, I, I, I, D, D, D, C, P]),
     "wp_mgfrac3d_solve": (I, [P, P, P, P, I, I, I, D, P]),
+    "wp_mgfrac3d_solve_index": (I, [P, P, P, P, I, I, I, D, P]),
+    "wp_mgfrac3d_solve_index64": (I, [P, P, P, P, I, I, I, D, P]),
+    "wp_mgfrac3d_index_sizes": (I, [P, P, P, I, P, P]),
     "wp_mgfrac3d_solve_tol": (I, [P, P, P, P, ctypes.POINTER(MgParams), ctypes.POINTER(MgReport), P]),
     "wp_mgfrac3d_residual": (I, [P, P, P, ctypes.POINTER(D), P]),
     "wp_mgfrac3d_iterate64": (I, [P, P, P]),

@@ -192,6 +192,27 @@ class CuMultigridFrac3D:
         check(lib().wp_mgfrac3d_solve(self._h, _ptr(dst, c), _ptr(pre_v, c), _ptr(f, c), int(n_iters), int(nu1),
                                       int(nu2), float(weight), _stream(stream)), "wp_mgfrac3d_solve")
 
+    def Solve_index(self, dst, pre_v, f, n_iters=10, nu1=2, nu2=2, weight=0.8, stream=None):
+        """n_iters index-sparse V-cycles over the cells with a face fraction >= 1e-12
+        (CuMultigridFrac3D::Solve_index, cuMultigridFrac3D.cu:347-420): post-smoothing runs nu1
+        sweeps as in the reference, unlisted cells keep their start value.  FP64 when dst is float64
+        (the reference's default precision; pre_v and f then float64 too), else FP32."""
+        c = self.cells
+        fn = lib().wp_mgfrac3d_solve_index64 if dst.dtype == torch.float64 else lib().wp_mgfrac3d_solve_index
+        dt = torch.float64 if dst.dtype == torch.float64 else torch.float32
+        check(fn(self._h, _ptr(dst, c, dt), _ptr(pre_v, c, dt), _ptr(f, c, dt), int(n_iters), int(nu1), int(nu2),
+                 float(weight), _stream(stream)), "wp_mgfrac3d_solve_index")
+
+    def IndexSizes(self, stream=None):
+        """(listed cells per level, listed 32-cell row segments per level) of the index-sparse cycle."""
+        cells = (ctypes.c_longlong * 32)()
+        segs = (ctypes.c_longlong * 32)()
+        nl = ctypes.c_int()
+        check(lib().wp_mgfrac3d_index_sizes(self._h, ctypes.cast(cells, ctypes.c_void_p),
+                                            ctypes.cast(segs, ctypes.c_void_p), 32, ctypes.byref(nl),
+                                            _stream(stream)), "wp_mgfrac3d_index_sizes")
+        return [cells[k] for k in range(nl.value)], [segs[k] for k in range(nl.value)]
+
     def SolveTol(self, dst, pre_v, f, rel_tol=1e-6, max_cycles=50, nu1=2, nu2=2, weight=2.0 / 3.0,
                  precision=PREC_MIXED, prolongation=PROLONG_TRILINEAR, raise_on_fail=True, start=START_ZERO,
                  host_loop=False, inner_cycles=1, stream=None) -> dict:

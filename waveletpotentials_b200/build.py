@@ -18,7 +18,10 @@ LIB = os.path.join(HERE, "libwp_b200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-         "--expt-relaxed-constexpr", "-rdc=false"]
+         "--expt-relaxed-constexpr", "-rdc=false",
+         # a value-returning function or lambda that can fall off its end is undefined behaviour the
+         # optimiser exploits (a loop before the missing return may never exit): refuse to build it
+         "--diag-error=940", "-Xcompiler", "-Werror=return-type"]
 
 
 def _sources():

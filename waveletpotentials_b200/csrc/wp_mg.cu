@@ -2114,6 +2114,208 @@ __global__ void convert_kernel(TD* __restrict__ d, const TS* __restrict__ s, lon
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) d[i] = (TD)s[i];
 }
 
+// ------------------------------------------------------------------ index-sparse cycle
+// CuMultigridFrac3D::Solve_index (cuMultigridFrac3D.cu:347-420) sweeps, restricts and prolongs only
+// the cells that CuBoundSelector::SelectByFrac (cuBoundSelector.cu:4-32) selects -- those with a
+// face fraction >= 1e-12 -- from per-level index lists built by a prefix sum (InitIndex, :189-229).
+// Here the unit of the list is a segment: 32 consecutive cells along y of one (x, z) row that hold
+// at least one selected cell, with the lane mask of the selected ones.  One warp per segment keeps
+// every load a 128-byte row piece (the y-fastest layout), solid rows cost nothing, and the mask
+// carries the per-cell selection to the kernels.  Segments are stored in memory order.
+constexpr int kIxBlock = 1024;  // segments per CTA of the list build
+
+// bit k of mask[s] = cell y0 + k of segment s is selected (the fractions compared in FP64, as the
+// reference compares them in its DTYPE); cells counts the selected cells
+__global__ void __launch_bounds__(256) index_mask_kernel(unsigned* __restrict__ mask,
+                                                         unsigned long long* __restrict__ cells, Lvl<float> L,
+                                                         int nsy, long nseg) {
+    const long s = ((long)blockIdx.x * 256 + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= nseg) return;  // uniform across the warp
+    const long row = s / nsy;
+    const int x = (int)(row % L.nx), z = (int)(row / L.nx), y = (int)(s - row * nsy) * 32 + lane;
+    bool on = false;
+    if (y < L.ny) {
+        const long sl = (long)L.nx * L.ny, i = y + (long)x * L.ny + z * sl;
+        const long iax = y + (long)x * L.ny + (long)z * (L.nx + 1) * L.ny;
+        const long iay = y + (long)x * (L.ny + 1) + (long)z * L.nx * (L.ny + 1);
+        on = !((double)L.ax[iax] < kEps && (double)L.ax[iax + L.ny] < kEps && (double)L.ay[iay] < kEps &&
+               (double)L.ay[iay + 1] < kEps && (double)L.az[i] < kEps && (double)L.az[i + sl] < kEps);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, on);
+    if (lane == 0) {
+        mask[s] = m;
+        if (m) atomicAdd(cells, (unsigned long long)__popc(m));
+    }
+}
+
+// segments with a selected cell per CTA of kIxBlock segments
+__global__ void __launch_bounds__(kIxBlock) index_count_kernel(const unsigned* __restrict__ mask, long nseg,
+                                                               int* __restrict__ bcount) {
+    const long s = (long)blockIdx.x * kIxBlock + threadIdx.x;
+    const int c = __syncthreads_count(s < nseg && mask[s] != 0u);
+    if (threadIdx.x == 0) bcount[blockIdx.x] = c;
+}
+
+// exclusive scan of the per-CTA counts in place, in one CTA; *total = the listed segments
+__global__ void __launch_bounds__(1024) index_scan_kernel(int* __restrict__ bcount, int nb,
+                                                          long long* __restrict__ total) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x;
+    const int per = (nb + 1023) / 1024;
+    const int b0 = min(t * per, nb), b1 = min(b0 + per, nb);
+    int sum = 0;
+    for (int b = b0; b < b1; ++b) sum += bcount[b];
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const int v = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int run = part[t] - sum;
+    for (int b = b0; b < b1; ++b) {
+        const int c = bcount[b];
+        bcount[b] = run;
+        run += c;
+    }
+    if (t == 1023) *total = part[1023];
+}
+
+// writes the listed segments {x, z, y0, mask} at the scanned offsets, in memory order
+__global__ void __launch_bounds__(kIxBlock) index_scatter_kernel(const unsigned* __restrict__ mask, long nseg,
+                                                                 const int* __restrict__ boff, int4* __restrict__ seg,
+                                                                 int nsy, int nx) {
+    __shared__ int wbase[kIxBlock / 32];
+    const long s = (long)blockIdx.x * kIxBlock + threadIdx.x;
+    const unsigned m = s < nseg ? mask[s] : 0u;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned b = __ballot_sync(0xffffffffu, m != 0u);
+    if (lane == 0) wbase[wid] = __popc(b);
+    __syncthreads();
+    if (wid == 0) {
+        const int own = wbase[lane];
+        int v = own;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        wbase[lane] = v - own;
+    }
+    __syncthreads();
+    if (m) {
+        const long row = s / nsy;
+        const int pos = boff[blockIdx.x] + wbase[wid] + __popc(b & ((1u << lane) - 1u));
+        seg[pos] = make_int4((int)(row % nx), (int)(row / nx), (int)(s - row * nsy) * 32, (int)m);
+    }
+}
+
+// the cell this lane owns: segment (blockIdx.x * 8 + warp), lane k = cell y0 + k; false when the
+// segment does not exist or does not select the cell.  All lanes load the same 16-byte entry.
+__device__ __forceinline__ bool index_cell(const int4* __restrict__ seg, long nseg, int& x, int& y, int& z) {
+    const long s = ((long)blockIdx.x * 256 + threadIdx.x) >> 5;
+    if (s >= nseg) return false;
+    const int4 g = seg[s];
+    const int lane = threadIdx.x & 31;
+    if (!(((unsigned)g.w >> lane) & 1u)) return false;
+    x = g.x;
+    z = g.y;
+    y = g.z + lane;
+    return true;
+}
+
+// cuWjFrac3D_n with an index (cuWeightedJacobi3D.cu:2821-2897): listed cells only; the others keep
+// their value in both buffers
+template <typename T>
+__global__ void __launch_bounds__(256) jacobi_ix_kernel(T* __restrict__ dst, const T* __restrict__ src,
+                                                        const T* __restrict__ f, Lvl<T> L, T w,
+                                                        const int4* __restrict__ seg, long nseg) {
+    wp_pdl_enter();
+    int x, y, z;
+    if (!index_cell(seg, nseg, x, y, z)) return;
+    T dg, od, c;
+    row<T, T, false>(L, src, nullptr, 0, 0, x, y, z, dg, od, c);
+    const long i = y + (long)x * L.ny + (long)z * L.nx * L.ny;
+    dst[i] = dg > (T)kEps ? ((T)1 - w) * c + w * (f[i] - od) / dg : (T)0;
+}
+
+// the first sweep of a coarse level from v = 0 (the reference clears the level, then sweeps): the
+// same value as jacobi_ix_kernel on a zero iterate without reading it
+template <typename T>
+__global__ void __launch_bounds__(256) jacobi0_ix_kernel(T* __restrict__ dst, const T* __restrict__ f, Lvl<T> L,
+                                                         T w, const int4* __restrict__ seg, long nseg) {
+    wp_pdl_enter();
+    int x, y, z;
+    if (!index_cell(seg, nseg, x, y, z)) return;
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const long sxy = (long)nx * ny, i = y + (long)x * ny + (long)z * sxy;
+    const long iax = y + (long)x * ny + (long)z * (nx + 1) * ny, iay = y + (long)x * (ny + 1) + (long)z * nx * (ny + 1);
+    T dg = 0;
+    if (y > 0) dg += (T)L.ay[iay] * L.glo[1][y];
+    if (y < ny - 1) dg += (T)L.ay[iay + 1] * L.ghi[1][y];
+    if (x > 0) dg += (T)L.ax[iax] * L.glo[0][x];
+    if (x < nx - 1) dg += (T)L.ax[iax + ny] * L.ghi[0][x];
+    if (z > 0) dg += (T)L.az[i] * L.glo[2][z];
+    if (z < nz - 1) dg += (T)L.az[i + sxy] * L.ghi[2][z];
+    dst[i] = dg > (T)kEps ? w * f[i] / dg : (T)0;
+}
+
+// cuWjGetFracRes_3d_n with an index (cuWeightedJacobi3D.cu:3013-3090): the residual of the listed
+// cells into the workspace shared by all levels
+template <typename T>
+__global__ void __launch_bounds__(256) resid_ix_kernel(T* __restrict__ r, const T* __restrict__ v,
+                                                       const T* __restrict__ f, Lvl<T> L,
+                                                       const int4* __restrict__ seg, long nseg) {
+    wp_pdl_enter();
+    int x, y, z;
+    if (!index_cell(seg, nseg, x, y, z)) return;
+    T dg, od, c;
+    row<T, T, false>(L, v, nullptr, 0, 0, x, y, z, dg, od, c);
+    const long i = y + (long)x * L.ny + (long)z * L.nx * L.ny;
+    r[i] = dg > (T)kEps ? f[i] - (dg * c + od) : (T)0;
+}
+
+// cuRestrict3D_p1_dx_whole (cuRestrict3D.cu:1146-1193): each listed coarse cell averages the
+// workspace over its (up to 8) children with the fine spacings as weights -- every child, listed
+// or not, as the reference reads them; the term order is the reference's
+template <typename T>
+__global__ void __launch_bounds__(256) restrict_ix_kernel(T* __restrict__ fc, const T* __restrict__ r, Lvl<T> L,
+                                                          int ncx, int ncy, const int4* __restrict__ cseg,
+                                                          long ncseg) {
+    wp_pdl_enter();
+    int cx, cy, cz;
+    if (!index_cell(cseg, ncseg, cx, cy, cz)) return;
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const int xs = 2 * cx, ys = 2 * cy, zs = 2 * cz;
+    const bool hx = xs < nx - 1, hy = ys < ny - 1, hz = zs < nz - 1;
+    const T wxl = (T)L.d[0][xs], wyl = (T)L.d[1][ys], wzl = (T)L.d[2][zs];
+    const T wxr = hx ? (T)L.d[0][xs + 1] : (T)0, wyr = hy ? (T)L.d[1][ys + 1] : (T)0;
+    const T wzr = hz ? (T)L.d[2][zs + 1] : (T)0;
+    const long ox = hx ? ny : 0, oy = hy ? 1 : 0, oz = hz ? (long)nx * ny : 0;
+    long s0 = ys + (long)xs * ny + (long)zs * nx * ny;
+    T val = wxl * wyl * wzl * r[s0];
+    val += wxl * wyr * wzl * r[s0 + oy];
+    val += wxr * wyl * wzl * r[s0 + ox];
+    val += wxr * wyr * wzl * r[s0 + oy + ox];
+    s0 += oz;
+    val += wxl * wyl * wzr * r[s0];
+    val += wxl * wyr * wzr * r[s0 + oy];
+    val += wxr * wyl * wzr * r[s0 + ox];
+    val += wxr * wyr * wzr * r[s0 + oy + ox];
+    fc[cy + (long)cx * ncy + (long)cz * ncx * ncy] = val / ((wxl + wxr) * (wyl + wyr) * (wzl + wzr));
+}
+
+// cuProlongate3D_p1_whole_add (cuProlongate3D.cu:619-640): listed cells add their parent's value
+template <typename T>
+__global__ void __launch_bounds__(256) prolong_ix_kernel(T* __restrict__ v, const T* __restrict__ vc, Lvl<T> L,
+                                                         int ncx, int ncy, const int4* __restrict__ seg, long nseg) {
+    wp_pdl_enter();
+    int x, y, z;
+    if (!index_cell(seg, nseg, x, y, z)) return;
+    v[y + (long)x * L.ny + (long)z * L.nx * L.ny] += vc[(y >> 1) + (long)(x >> 1) * ncy + (long)(z >> 1) * ncx * ncy];
+}
+
 // coarse face fractions: inject even faces along the face's own axis, average the (up to) two
 // children along the two others (cuRestrict3D.cu:972-1145)
 __global__ void coarsen_faces_kernel(float* __restrict__ dst, const float* __restrict__ src, int fnx, int fny, int fnz,
@@ -2165,6 +2367,11 @@ struct Level {
                       // 6 = one cell per thread; restrict: 0-2 register budgets, 3 = pipelined,
                       // 4 = one cell per thread; defect: 0 quads, 1 pipelined)
     int* err;         // the handle's device error flag (bounded waits of the TMA-staged kernel)
+    // index-sparse cycle (built by the first wp_mgfrac3d_solve_index)
+    unsigned* imask;  // per 32-cell segment of a row: the selected cells
+    int4* iseg;       // the listed segments {x, z, y0, mask}, in memory order
+    long long iseg_n; // listed segments
+    long long icells; // selected cells (the reference's index size)
 };
 
 enum { kZcJacobi = 0, kZcRestrict = 1, kZcDefect = 2 };
@@ -2402,6 +2609,9 @@ struct wp_mgfrac3d {
     int loop_key[7];   // nu1, nu2, prolongation, full-multigrid first cycle, tune_gen, device, inner cycles
     double loop_omega;
     long long loop_launches[2]; // kernels of the first cycle's graph part and of one loop body
+    int ix_built;      // the index lists of every level exist
+    float* ix_r;       // residual workspace of the index-sparse cycle, shared by the levels (finest size)
+    double* ix_r64;    // the same for the FP64 cycle
 };
 
 namespace {
@@ -2687,6 +2897,22 @@ wp_status mid_cycle(wp_mgfrac3d* h, int l1, int nu1, int nu2, float w, int prolo
     return WP_OK;
 }
 
+// The coarsest solve (cuWjFrac3D_kernel_n, cuWeightedJacobi3D.cu:1473-1545) from the level's v:
+// in one CTA when the level fits its shared memory, else as ordinary sweeps.
+template <typename T>
+wp_status coarsest_solve(wp_mgfrac3d* h, Level& L, const T* f, T w, cudaStream_t s) {
+    const size_t smem = 2 * sizeof(T) * L.cells;
+    if (smem <= 200 * 1024) {
+        auto k = coarsest_kernel<T>;
+        WP_CUDA_TRY(wp_set_smem(k, smem));
+        const int nt = (int)std::min<long>(1024, (L.cells + 31) / 32 * 32);
+        WP_KERNEL("coarsest", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
+                  k<<<1, nt, smem, s>>>(Bufs<T>::v(L), f, view<T>(L), w, h->coarsest_iters));
+        return WP_OK;
+    }
+    return smooth<T>(L, f, h->coarsest_iters, w, s);
+}
+
 // One V-cycle at level l from the level's current v, or (clear_v) from v = 0: then v is neither
 // cleared nor read -- the first sweep is jacobi0_q_kernel where the level's kernel allows, otherwise
 // v is cleared first -- and below kCoarseCells the single-launch coarse cycle takes over.
@@ -2799,16 +3025,7 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         }
     } else {
         if (clear_v) WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(L), 0, sizeof(T) * L.cells, s));
-        const size_t smem = 2 * sizeof(T) * L.cells;
-        if (smem <= 200 * 1024) {
-            auto k = coarsest_kernel<T>;
-            WP_CUDA_TRY(wp_set_smem(k, smem));
-            const int nt = (int)std::min<long>(1024, (L.cells + 31) / 32 * 32);
-            WP_KERNEL("coarsest", (double)L.cells * (3.0 * sizeof(T) + 12.0), s,
-                      k<<<1, nt, smem, s>>>(Bufs<T>::v(L), f, view<T>(L), w, h->coarsest_iters));
-        } else {
-            if ((st = smooth<T>(L, f, h->coarsest_iters, w, s)) != WP_OK) return st;
-        }
+        if ((st = coarsest_solve<T>(h, L, f, w, s)) != WP_OK) return st;
     }
     return WP_OK;
 }
@@ -2911,13 +3128,15 @@ void destroy_levels(wp_mgfrac3d* h) {
     for (int l = 0; l < kMaxLevels; ++l) {
         Level& L = h->lv[l];
         for (int a = 0; a < 3; ++a) if (L.frac[a]) cudaFree(L.frac[a]);
-        void* ps[] = {L.tab64, L.tab32, L.fyc, L.uni, L.v, L.t, L.f, L.v64, L.t64, L.f64};
+        void* ps[] = {L.tab64, L.tab32, L.fyc, L.uni, L.v, L.t, L.f, L.v64, L.t64, L.f64, L.imask, L.iseg};
         for (void* p : ps) if (p) cudaFree(p);
     }
     if (h->ccf_all) cudaFree(h->ccf_all);
     if (h->acc) cudaFree(h->acc);
     if (h->p64) cudaFree(h->p64);
     if (h->r32) cudaFree(h->r32);
+    if (h->ix_r) cudaFree(h->ix_r);
+    if (h->ix_r64) cudaFree(h->ix_r64);
 }
 
 wp_status create_common(wp_mgfrac3d** out, int dims, const float* ax, const float* ay, const float* az, int nx, int ny,
@@ -2961,6 +3180,170 @@ wp_status solve_fixed(wp_mgfrac3d* h, float* dst, const float* pre_v, const floa
         if (st != WP_OK) return st;
     }
     WP_CUDA_TRY(cudaMemcpyAsync(dst, L.v, sizeof(float) * L.cells, cudaMemcpyDeviceToDevice, s));
+    return WP_OK;
+}
+
+// The index lists of every level (InitIndex, cuMultigridFrac3D.cu:189-229) and the zeroed residual
+// workspace; once per handle, synchronous (the list lengths size the launches).
+wp_status build_index(wp_mgfrac3d* h, cudaStream_t s) {
+    if (h->ix_built) return WP_OK;
+    long maxseg = 0;
+    for (int l = 0; l < h->nl; ++l) {
+        const Level& L = h->lv[l];
+        maxseg = std::max(maxseg, (long)L.n[0] * L.n[2] * (long)wp_cdiv(L.n[1], 32));
+    }
+    const long maxb = (long)wp_cdiv(maxseg, kIxBlock);
+    int* bcount = nullptr;
+    long long* dev = nullptr;  // [0] listed segments, [1] selected cells
+    wp_status st = WP_OK;
+    auto fail = [&](cudaError_t e, int line) {
+        wp_set_cuda_error(e, "index lists", __FILE__, line);
+        st = WP_ERR_CUDA;
+    };
+    cudaError_t e = cudaMalloc((void**)&bcount, sizeof(int) * maxb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&dev, 2 * sizeof(long long));
+    if (e != cudaSuccess) fail(e, __LINE__);
+    for (int l = 0; l < h->nl && st == WP_OK; ++l) {
+        Level& L = h->lv[l];
+        const int nsy = (int)wp_cdiv(L.n[1], 32);
+        const long nseg = (long)L.n[0] * L.n[2] * nsy;
+        const int nb = (int)wp_cdiv(nseg, kIxBlock);
+        if (L.imask) cudaFree(L.imask);
+        if (L.iseg) cudaFree(L.iseg);
+        L.imask = nullptr;
+        L.iseg = nullptr;
+        e = cudaMalloc((void**)&L.imask, sizeof(unsigned) * nseg);
+        if (e == cudaSuccess) e = cudaMemsetAsync(dev, 0, 2 * sizeof(long long), s);
+        if (e != cudaSuccess) { fail(e, __LINE__); break; }
+        WP_KERNEL("index_mask", 12.0 * L.cells, s,
+                  index_mask_kernel<<<(unsigned)wp_cdiv(nseg * 32, 256), 256, 0, s>>>(
+                      L.imask, reinterpret_cast<unsigned long long*>(dev + 1), view<float>(L), nsy, nseg));
+        WP_KERNEL("index_count", 4.0 * nseg, s, index_count_kernel<<<nb, kIxBlock, 0, s>>>(L.imask, nseg, bcount));
+        WP_KERNEL("index_scan", 8.0 * nb, s, index_scan_kernel<<<1, 1024, 0, s>>>(bcount, nb, dev));
+        long long hv[2] = {0, 0};
+        e = cudaMemcpyAsync(hv, dev, sizeof(hv), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { fail(e, __LINE__); break; }
+        L.iseg_n = hv[0];
+        L.icells = hv[1];
+        if (hv[0] > 0) {
+            e = cudaMalloc((void**)&L.iseg, sizeof(int4) * hv[0]);
+            if (e != cudaSuccess) { fail(e, __LINE__); break; }
+            WP_KERNEL("index_scatter", 4.0 * nseg + 16.0 * hv[0], s,
+                      index_scatter_kernel<<<nb, kIxBlock, 0, s>>>(L.imask, nseg, bcount, L.iseg, nsy, L.n[0]));
+        }
+    }
+    if (st == WP_OK) {
+        if (h->ix_r) cudaFree(h->ix_r);
+        h->ix_r = nullptr;
+        e = cudaMalloc((void**)&h->ix_r, sizeof(float) * h->lv[0].cells);
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->ix_r, 0, sizeof(float) * h->lv[0].cells, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) fail(e, __LINE__);
+    }
+    if (bcount) cudaFree(bcount);
+    if (dev) cudaFree(dev);
+    if (st == WP_OK) h->ix_built = 1;
+    return st;
+}
+
+// One index-sparse V-cycle at level l (SolveOneVCycle_index, cuMultigridFrac3D.cu:366-420).  A
+// coarse level enters with v = 0 at every cell: its unlisted cells stay 0 throughout the solve (no
+// index kernel writes them) and its first sweep computes the listed ones from zero.  The cycle goes
+// down while the next level lists a cell, then the coarsest solve runs; post-smoothing runs nu1
+// sweeps, as the reference passes nu1 there.  r: the residual workspace (finest size).
+template <typename T>
+wp_status vcycle_ix(wp_mgfrac3d* h, int l, const T* f, T* r, int nu1, T w, cudaStream_t s) {
+    Level& L = h->lv[l];
+    T*& v = Bufs<T>::v(L);
+    T*& t = Bufs<T>::t(L);
+    if (!(l < h->nl - 1 && h->lv[l + 1].icells > 0)) {
+        if (l > 0) WP_CUDA_TRY(cudaMemsetAsync(v, 0, sizeof(T) * L.cells, s));
+        return coarsest_solve<T>(h, L, f, w, s);
+    }
+    Level& C = h->lv[l + 1];
+    const unsigned gb = (unsigned)wp_cdiv(L.iseg_n, 8), gc = (unsigned)wp_cdiv(C.iseg_n, 8);
+    const double lc = (double)L.icells, ls = (double)L.iseg_n, B = sizeof(T);
+    const int4* seg = L.iseg;
+    const long nseg = (long)L.iseg_n;
+    auto sweeps = [&](bool first_from_zero) -> wp_status {
+        for (int k = 0; k < nu1; ++k) {
+            if (gb > 0) {
+                if (k == 0 && first_from_zero && l > 0)
+                    WP_KERNEL("jacobi0_ix", lc * (2.0 * B + 12.0) + 16.0 * ls, s,
+                              wp_launch_pdl(jacobi0_ix_kernel<T>, gb, 256, 0, s, t, f, view<T>(L), w, seg, nseg));
+                else
+                    WP_KERNEL(l == 0 ? "jacobi_ix_finest" : "jacobi_ix", lc * (3.0 * B + 12.0) + 16.0 * ls, s,
+                              wp_launch_pdl(jacobi_ix_kernel<T>, gb, 256, 0, s, t, (const T*)v, f, view<T>(L), w,
+                                            seg, nseg));
+            }
+            std::swap(v, t);
+        }
+        return WP_OK;
+    };
+    wp_status st;
+    if (l > 0 && nu1 == 0) WP_CUDA_TRY(cudaMemsetAsync(v, 0, sizeof(T) * L.cells, s));
+    if ((st = sweeps(true)) != WP_OK) return st;
+    if (gb > 0)
+        WP_KERNEL(l == 0 ? "resid_ix_finest" : "resid_ix", lc * (3.0 * B + 12.0) + 16.0 * ls, s,
+                  wp_launch_pdl(resid_ix_kernel<T>, gb, 256, 0, s, r, (const T*)v, f, view<T>(L), seg, nseg));
+    // the coarsest solve sweeps every cell of its level: the unlisted ones read a zero right-hand
+    // side (the reference's never-written coarse arrays; they matter where a face fraction is
+    // nonzero but below the selection threshold)
+    if (!(l + 1 < h->nl - 1 && h->lv[l + 2].icells > 0))
+        WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::f(C), 0, sizeof(T) * C.cells, s));
+    if (gc > 0)
+        WP_KERNEL("restrict_ix", (double)C.icells * (9.0 * B) + 16.0 * C.iseg_n, s,
+                  wp_launch_pdl(restrict_ix_kernel<T>, gc, 256, 0, s, Bufs<T>::f(C), (const T*)r, view<T>(L), C.n[0],
+                                C.n[1], (const int4*)C.iseg, (long)C.iseg_n));
+    if ((st = vcycle_ix<T>(h, l + 1, Bufs<T>::f(C), r, nu1, w, s)) != WP_OK) return st;
+    if (gb > 0)
+        WP_KERNEL(l == 0 ? "prolong_ix_finest" : "prolong_ix", lc * (3.0 * B) + 16.0 * ls, s,
+                  wp_launch_pdl(prolong_ix_kernel<T>, gb, 256, 0, s, v, (const T*)Bufs<T>::v(C), view<T>(L), C.n[0],
+                                C.n[1], seg, nseg));
+    return sweeps(false);
+}
+
+// CuMultigridFrac3D::Solve_index (cuMultigridFrac3D.cu:347-364): n_iters index-sparse V-cycles in T.
+// The finest level's unlisted cells keep their start value (pre_v, or 0).
+template <typename T>
+wp_status solve_index(wp_mgfrac3d* h, T* dst, const T* pre_v, const T* f, int n_iters, int nu1, int nu2,
+                      double weight, cudaStream_t s) {
+    if (!h || !dst || !f || n_iters < 0 || nu1 < 0 || nu2 < 0) {
+        wp_set_error_msg("wp_mgfrac3d_solve_index: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (h->dims != 3) {
+        wp_set_error_msg("wp_mgfrac3d_solve_index: the index-sparse cycle is 3D only");
+        return WP_ERR_UNSUPPORTED;
+    }
+    wp_status st = build_index(h, s);
+    if (st != WP_OK) return st;
+    T* r = nullptr;
+    if (sizeof(T) == 4) {
+        r = reinterpret_cast<T*>(h->ix_r);
+    } else {
+        if ((st = ensure_fp64(h)) != WP_OK) return st;
+        if (!h->ix_r64) {
+            WP_CUDA_TRY(cudaMalloc((void**)&h->ix_r64, sizeof(double) * h->lv[0].cells));
+            WP_CUDA_TRY(cudaMemsetAsync(h->ix_r64, 0, sizeof(double) * h->lv[0].cells, s));
+        }
+        r = reinterpret_cast<T*>(h->ix_r64);
+    }
+    Level& L = h->lv[0];
+    T* v = Bufs<T>::v(L);
+    if (pre_v) WP_CUDA_TRY(cudaMemcpyAsync(v, pre_v, sizeof(T) * L.cells, cudaMemcpyDeviceToDevice, s));
+    else WP_CUDA_TRY(cudaMemsetAsync(v, 0, sizeof(T) * L.cells, s));
+    WP_CUDA_TRY(cudaMemcpyAsync(Bufs<T>::t(L), v, sizeof(T) * L.cells, cudaMemcpyDeviceToDevice, s));
+    for (int l = 1; l < h->nl; ++l) {
+        WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::v(h->lv[l]), 0, sizeof(T) * h->lv[l].cells, s));
+        WP_CUDA_TRY(cudaMemsetAsync(Bufs<T>::t(h->lv[l]), 0, sizeof(T) * h->lv[l].cells, s));
+    }
+    for (int c = 0; c < n_iters; ++c)
+        if ((st = vcycle_ix<T>(h, 0, f, r, nu1, (T)weight, s)) != WP_OK) return st;
+    WP_CUDA_TRY(cudaMemcpyAsync(dst, Bufs<T>::v(L), sizeof(T) * L.cells, cudaMemcpyDeviceToDevice, s));
+    // the FP64 level buffers held the last FP64 tolerance solve's iterate: it is gone
+    if (sizeof(T) == 8 && h->last64 == 2) h->last64 = 0;
     return WP_OK;
 }
 
@@ -3304,6 +3687,32 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_create(wp_mgfrac3d** h, const float*
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_solve(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f,
                                                   int n_iters, int nu1, int nu2, double weight, void* stream) {
     return solve_fixed(h, dst, pre_v, f, n_iters, nu1, nu2, weight, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_solve_index(wp_mgfrac3d* h, float* dst, const float* pre_v,
+                                                        const float* f, int n_iters, int nu1, int nu2, double weight,
+                                                        void* stream) {
+    return solve_index<float>(h, dst, pre_v, f, n_iters, nu1, nu2, weight, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_solve_index64(wp_mgfrac3d* h, double* dst, const double* pre_v,
+                                                          const double* f, int n_iters, int nu1, int nu2,
+                                                          double weight, void* stream) {
+    return solve_index<double>(h, dst, pre_v, f, n_iters, nu1, nu2, weight, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_index_sizes(wp_mgfrac3d* h, long long* cells, long long* segments, int cap,
+                                                        int* levels, void* stream) {
+    if (!h || cap < 0) { wp_set_error_msg("wp_mgfrac3d_index_sizes: bad arguments"); return WP_ERR_INVALID_ARG; }
+    if (h->dims != 3) { wp_set_error_msg("wp_mgfrac3d_index_sizes: the index-sparse cycle is 3D only"); return WP_ERR_UNSUPPORTED; }
+    wp_status st = build_index(h, (cudaStream_t)stream);
+    if (st != WP_OK) return st;
+    if (levels) *levels = h->nl;
+    for (int l = 0; l < h->nl && l < cap; ++l) {
+        if (cells) cells[l] = h->lv[l].icells;
+        if (segments) segments[l] = h->lv[l].iseg_n;
+    }
+    return WP_OK;
 }
 
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float* f,

@@ -124,3 +124,41 @@ def sdf_spheres3d(n, centers, radii):
     for c, r in zip(np.reshape(centers, (-1, 3)), np.reshape(radii, (-1,))):
         out = np.minimum(out, np.sqrt((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) - r)
     return out
+
+
+def porous_fractions(fluid, rng, tiny=0, cut=True):
+    """Face fractions of a cell mask (numpy (nz, nx, ny), True = fluid): 1 between two fluid cells, a
+    random value in [0.2, 0.9] between a fluid and a solid cell (0 with cut=False), 0 between two
+    solid cells; a wall face takes its cell's value.  `tiny` faces of solid-solid pairs get 1e-13
+    (below the 1e-12 threshold of the index-sparse cycle's cell selection).  Returns (ax, ay, az)."""
+    m = fluid.astype(np.float64)
+    out = []
+    for axis in (1, 2, 0):  # ax (x faces), ay (y faces), az (z faces)
+        pad = np.concatenate([np.take(m, [0], axis=axis), m, np.take(m, [-1], axis=axis)], axis=axis)
+        lo = np.take(pad, range(0, pad.shape[axis] - 1), axis=axis)
+        hi = np.take(pad, range(1, pad.shape[axis]), axis=axis)
+        part = rng.uniform(0.2, 0.9, lo.shape) if cut else np.zeros(lo.shape)
+        a = np.where((lo > 0) & (hi > 0), 1.0, np.where((lo > 0) | (hi > 0), part, 0.0))
+        if tiny:
+            zero = np.argwhere(a == 0.0)
+            pick = zero[rng.choice(len(zero), size=min(tiny, len(zero)), replace=False)]
+            a[tuple(pick.T)] = 1e-13
+        out.append(a)
+    return out
+
+
+def porous_domain(n, fluid_fraction: float, seed: int, rmin=0.04, rmax=0.1):
+    """A mostly-solid domain for the index-sparse multigrid: balls of fluid (radii uniform in
+    [rmin, rmax] of the extent) dropped until `fluid_fraction` of the cells are fluid, with cut faces
+    of random area where fluid meets solid.  Returns (fluid mask, (ax, ay, az), rng)."""
+    nx, ny, nz = n
+    rng = np.random.default_rng(seed)
+    z, x, y = np.meshgrid(np.arange(nz) + 0.5, np.arange(nx) + 0.5, np.arange(ny) + 0.5, indexing="ij",
+                          sparse=True)
+    fluid = np.zeros((nz, nx, ny), dtype=bool)
+    ext = np.array([nx, ny, nz], dtype=np.float64)
+    while fluid.mean() < fluid_fraction:
+        c = rng.uniform(0, 1, 3) * ext
+        r = rng.uniform(rmin, rmax) * min(n)
+        fluid |= (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 < r * r
+    return fluid, porous_fractions(fluid, rng), rng
