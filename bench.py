@@ -298,6 +298,8 @@ def run_ours(args, rank, world, local_rank):
         plain["recovery"] = {
             "wavelet_ms": time_rec(lambda: proj.rec.Solve(*q, *u)),
             "sweep_dst_ms": time_rec(lambda: (sw.Solve(*qs, *u), sw.Project(*qs))),
+            # CuWaveletPotentialRecover3D::CutCoefficients of the recovered potential at level 2
+            "cut_level2_ms": time_rec(lambda: proj.rec.CutCoefficients(*qs, *q, 2)),
         }
         sw.close()
         # the index-sparse cycle (CuMultigridFrac3D::Solve_index) against the dense reference cycle

@@ -91,6 +91,13 @@ CUWHHD_API wp_status wp_recover3d_run(wp_recover3d* h, float* qx, float* qy, flo
    (cuDivLocalProject3D.cu:5273-5308): coefficient-space projection only. */
 CUWHHD_API wp_status wp_recover3d_project(wp_recover3d* h, float* qx, float* qy, float* qz, const float* xv_lwt,
                                           const float* yv_lwt, const float* zv_lwt, void* stream);
+/* Replaces CuWaveletPotentialRecover3D::CutCoefficients(qx_out, qy_out, qz_out, qx, qy, qz, level)
+   (cuWaveletPotentialRecover3D.cu:123-239): analyses the potential with the recovery's synthesis
+   wavelets, clears the coefficients of every index whose level along some axis is below `level`
+   (with the reference's coupling of the three components), and synthesises the result into the
+   _out arrays (which may alias the inputs).  level in [0, min(log2 n)]: 0 returns the potential. */
+CUWHHD_API wp_status wp_recover3d_cut(wp_recover3d* h, float* qx_out, float* qy_out, float* qz_out, const float* qx,
+                                      const float* qy, const float* qz, int level, void* stream);
 CUWHHD_API wp_status wp_recover3d_destroy(wp_recover3d* h);
 
 /* ---------------------------------------------------------- potential recovery 2D ------- */

@@ -63,6 +63,7 @@ def lib():
             "or_fractions2d": (None, [p, p, p, i, i, d]),
             "or_mgfrac3d_solve": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, i, p]),
             "or_mgfrac3d_solve_index": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, p, p]),
+            "or_cut3d": (i, [p, p, p, i, i, i, i]),
             "or_mgfrac2d_solve": (i, [p, p, p, p, p, i, i, d, d, i, i, i, d, i, p]),
             "or_frac_residual3d": (d, [p, p, p, p, p, p, i, i, i, d, d, d]),
             "or_frac_residual2d": (d, [p, p, p, p, p, i, i, d, d]),
@@ -156,6 +157,14 @@ def recover2d(xv, yv, n, d, bc="n"):
     qz = np.zeros((nx + 1, ny + 1))
     _check(lib().or_recover2d(_p(qz), _p(_f64(xv)), _p(_f64(yv)), nx, ny, *d, bc.encode()), "recover2d")
     return qz
+
+
+def cut3d(qx, qy, qz, n, level):
+    """CuWaveletPotentialRecover3D::CutCoefficients: the potential with its wavelet coefficients
+    below `level` cleared (returns new arrays)."""
+    out = [np.array(_f64(a)) for a in (qx, qy, qz)]
+    _check(lib().or_cut3d(*(_p(a) for a in out), *n, level), "or_cut3d")
+    return tuple(out)
 
 
 def curl3d(qx, qy, qz, n, d):

@@ -125,6 +125,25 @@ int main(int argc, char** argv) {
         write_bin("qx", from_dev(qx, sqx));
         write_bin("qy", from_dev(qy, sqy));
         write_bin("qz", from_dev(qz, sqz));
+    } else if (op == "cut3d") {  // nx ny nz dx level: CuWaveletPotentialRecover3D::CutCoefficients
+        int3 dim = make_int3(I(0), I(1), I(2));
+        DTYPE h = (DTYPE)D(3);
+        DTYPE3 dx = make_DTYPE3(h, h, h);
+        int level = I(4);
+        size_t sqx = (size_t)dim.x * (dim.y + 1) * (dim.z + 1), sqy = (size_t)(dim.x + 1) * dim.y * (dim.z + 1);
+        size_t sqz = (size_t)(dim.x + 1) * (dim.y + 1) * dim.z;
+        DTYPE* qx = to_dev(read_bin("qx", sqx));
+        DTYPE* qy = to_dev(read_bin("qy", sqy));
+        DTYPE* qz = to_dev(read_bin("qz", sqz));
+        DTYPE* ox = dev_zeros(sqx);
+        DTYPE* oy = dev_zeros(sqy);
+        DTYPE* oz = dev_zeros(sqz);
+        CuWaveletPotentialRecover3D rec(dim, dx, 'n', WaveletType::WT_CDF3_7, WaveletType::WT_CDF4_6);
+        rec.CutCoefficients(ox, oy, oz, qx, qy, qz, level);
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("qx", from_dev(ox, sqx));
+        write_bin("qy", from_dev(oy, sqy));
+        write_bin("qz", from_dev(oz, sqz));
     } else if (op == "project2d" || op == "recover2d") {  // nx ny dx
         int2 dim = make_int2(I(0), I(1));
         DTYPE h = (DTYPE)D(2);

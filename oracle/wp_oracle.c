@@ -476,6 +476,63 @@ int or_recover3d(double* qx, double* qy, double* qz, const double* xv, const dou
     return e;
 }
 
+/* CuWaveletPotentialRecover3D::CutCoefficients (cuWaveletPotentialRecover3D.cu:123-239), in place:
+   analysis with the recovery's synthesis wavelets, cuCutCoefs over the (nx+1, ny+1, nz+1) index box
+   (coefficient level j = L - bitlength(max(i - 1, 0)) per axis; a cell with some j below `level`
+   clears qx at (x-1, y, z), qy at (x, y-1, z), qz at (x, y, z-1) with the reference's guards), then
+   synthesis.  Returns 1 for a level outside [0, min L]. */
+int or_cut3d(double* qx, double* qy, double* qz, int nx, int ny, int nz, int level) {
+    int Lx = ilog2(nx), Ly = ilog2(ny), Lz = ilog2(nz);
+    int Lmin = Lx < Ly ? (Lx < Lz ? Lx : Lz) : (Ly < Lz ? Ly : Lz);
+    if (level < 0 || level > Lmin) return 1;
+    char bc = 'n', bcd = 'd';
+    int e = 0;
+    e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Lx, 'x', OR_CDF3_7, bc, 1);
+    e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Ly, 'y', OR_CDF4_6, bcd, 1);
+    e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Lz, 'z', OR_CDF4_6, bcd, 1);
+    e |= or_dwt_axis(qy, nx + 1, ny, nz + 1, Lx, 'x', OR_CDF4_6, bcd, 1);
+    e |= or_dwt_axis(qy, nx + 1, ny, nz + 1, Ly, 'y', OR_CDF3_7, bc, 1);
+    e |= or_dwt_axis(qy, nx + 1, ny, nz + 1, Lz, 'z', OR_CDF4_6, bcd, 1);
+    e |= or_dwt_axis(qz, nx + 1, ny + 1, nz, Lx, 'x', OR_CDF4_6, bcd, 1);
+    e |= or_dwt_axis(qz, nx + 1, ny + 1, nz, Ly, 'y', OR_CDF4_6, bcd, 1);
+    e |= or_dwt_axis(qz, nx + 1, ny + 1, nz, Lz, 'z', OR_CDF3_7, bc, 1);
+    for (int z = 0; z <= nz; ++z)
+        for (int x = 0; x <= nx; ++x)
+            for (int y = 0; y <= ny; ++y) {
+                int jx = Lx - bitlen(x - 1 > 0 ? x - 1 : 0);
+                int jy = Ly - bitlen(y - 1 > 0 ? y - 1 : 0);
+                int jz = Lz - bitlen(z - 1 > 0 ? z - 1 : 0);
+                long iqx = y + (long)(x - 1) * (ny + 1) + (long)z * nx * (ny + 1);
+                long iqy = (y - 1) + (long)x * ny + (long)z * (nx + 1) * ny;
+                long iqz = y + (long)x * (ny + 1) + (long)(z - 1) * (nx + 1) * (ny + 1);
+                if (jx < level) {
+                    qx[iqx] = 0.0;
+                    if (y > 0) qy[iqy] = 0.0;
+                    if (z > 0) qz[iqz] = 0.0;
+                }
+                if (jy < level) {
+                    qy[iqy] = 0.0;
+                    if (x > 0) qx[iqx] = 0.0;
+                    if (z > 0) qz[iqz] = 0.0;
+                }
+                if (jz < level) {
+                    qz[iqz] = 0.0;
+                    if (x > 0) qx[iqx] = 0.0;
+                    if (y > 0) qy[iqy] = 0.0;
+                }
+            }
+    e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Lx, 'x', OR_CDF3_7, bc, 0);
+    e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Ly, 'y', OR_CDF4_6, bcd, 0);
+    e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Lz, 'z', OR_CDF4_6, bcd, 0);
+    e |= or_dwt_axis(qy, nx + 1, ny, nz + 1, Lx, 'x', OR_CDF4_6, bcd, 0);
+    e |= or_dwt_axis(qy, nx + 1, ny, nz + 1, Ly, 'y', OR_CDF3_7, bc, 0);
+    e |= or_dwt_axis(qy, nx + 1, ny, nz + 1, Lz, 'z', OR_CDF4_6, bcd, 0);
+    e |= or_dwt_axis(qz, nx + 1, ny + 1, nz, Lx, 'x', OR_CDF4_6, bcd, 0);
+    e |= or_dwt_axis(qz, nx + 1, ny + 1, nz, Ly, 'y', OR_CDF4_6, bcd, 0);
+    e |= or_dwt_axis(qz, nx + 1, ny + 1, nz, Lz, 'z', OR_CDF3_7, bc, 0);
+    return e;
+}
+
 /* CuWaveletPotentialRecover2D::Solve (cuWaveletPotentialRecover2D.cu:16-36) */
 int or_recover2d(double* qz, const double* xv, const double* yv, int nx, int ny, double dx, double dy, char bc) {
     if (bc != 'n') return 2;

@@ -72,6 +72,9 @@ void or_fractions2d(double* ax, double* ay, const double* sdf, int nx, int ny, d
 int or_mgfrac3d_solve(double* p, const double* p0, const double* f, const double* ax, const double* ay,
                       const double* az, int nx, int ny, int nz, double dx, double dy, double dz,
                       int ncycles, int nu1, int nu2, double omega, int prolong, double* history);
+/* coefficient truncation of a potential, in place (CuWaveletPotentialRecover3D::CutCoefficients,
+   cuWaveletPotentialRecover3D.cu:123-239); 1 for a level outside [0, min log2 n] */
+int or_cut3d(double* qx, double* qy, double* qz, int nx, int ny, int nz, int level);
 /* index-sparse V-cycles (CuMultigridFrac3D::Solve_index, cuMultigridFrac3D.cu:347-420): only cells with
    a face fraction >= 1e-12 are swept, their residuals go to a residual workspace shared by the levels
    (zero at the start) and the restriction reads it for every child; post-smoothing runs nu1 sweeps

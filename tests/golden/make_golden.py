@@ -5,11 +5,12 @@ unmodified reference sources (FP64, the reference default):
 
     python tests/golden/make_golden.py            # every fixture
     python tests/golden/make_golden.py --only index   # the index-sparse multigrid cases only
+    python tests/golden/make_golden.py --only cut     # the coefficient truncation cases only
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
 (CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D::ProjectLocal_q_ccc,
 CuDivLocalProject::ProjectSingle, CuWaveletPotentialRecover3D/2D::Solve, CuMultigridFrac3D/2D::Solve,
-CuMultigridFrac3D::Solve_index, CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P,
+CuMultigridFrac3D::Solve_index, CuWaveletPotentialRecover3D::CutCoefficients, CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P,
 CuSolidLevelSet3D) and stores inputs
 and reference outputs as ``<case>.npz``.  The CPU tests pin the FP64 oracle against these files;
 the GPU tests compare the CUDA kernels with the oracle on the same inputs.
@@ -88,11 +89,40 @@ def index_cases(rng):
          nu=np.array([2, 2]), omega=2.0 / 3.0, **out)
 
 
+def cut_cases(rng):
+    """CuWaveletPotentialRecover3D::CutCoefficients on random potentials whose samples on the walls
+    of the CDF4.6 (Dirichlet-type) axes are zero, at every level from 0 (the identity) to the
+    smallest log2 extent, on a cube and a box."""
+    out = {}
+    for n in ((16, 16, 16), (16, 8, 32)):
+        s = shapes3(n)
+        q = {k: rng.standard_normal(s[k]) for k in ("qx", "qy", "qz")}
+        q["qx"][:, :, [0, -1]] = 0
+        q["qx"][[0, -1]] = 0
+        q["qy"][:, [0, -1], :] = 0
+        q["qy"][[0, -1]] = 0
+        q["qz"][:, [0, -1], :] = 0
+        q["qz"][:, :, [0, -1]] = 0
+        tag = "x".join(str(v) for v in n)
+        out[f"n_{tag}"] = np.array(n)
+        for k in ("qx", "qy", "qz"):
+            out[f"{k}_{tag}"] = q[k]
+        for level in range(int(np.log2(min(n))) + 1):
+            res = run("cut3d", q, [*n, 1.0 / n[0], level], {k: s[k] for k in ("qx", "qy", "qz")})
+            for k in ("qx", "qy", "qz"):
+                out[f"{k}_{tag}_cut{level}"] = res[k]
+    save("cut3d", **out)
+
+
 def main():
     if not os.path.exists(DRIVER):
         sys.exit(f"{DRIVER} missing: run make -C oracle/refharness first (needs nvcc and the reference sources)")
-    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "index":
+    only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
+    if only == "index":
         index_cases(np.random.default_rng(20261204))
+        return
+    if only == "cut":
+        cut_cases(np.random.default_rng(20261205))
         return
     rng = np.random.default_rng(20261203)
 
@@ -211,6 +241,7 @@ def main():
     out = run("mg2d", {"f": f2, "ax": ax2, "ay": ay2}, [*n2, 1.0 / 32, 5, 5, 5, 0.8], {"p": n2, "hist": (5,)})
     save("mg2d_32", n=np.array(n2), h=1.0 / 32, f=f2, ax=ax2, ay=ay2, ncycles=5, nu=np.array([5, 5]), omega=0.8, **out)
     index_cases(np.random.default_rng(20261204))
+    cut_cases(np.random.default_rng(20261205))
 
 
 if __name__ == "__main__":

@@ -124,6 +124,21 @@ def test_mg3d_index_oracle_reduces_to_the_dense_cycle_without_solids(oracle):
     assert oracle.rel_l2(pd, pi) < 1e-13
 
 
+def test_cut3d_matches_reference(oracle):
+    """CuWaveletPotentialRecover3D::CutCoefficients at every level, two shapes."""
+    g = load_golden("cut3d")
+    for key in [k for k in g.files if k.startswith("n_")]:
+        tag = key[2:]
+        n = tuple(int(v) for v in g[key])
+        q = [g[f"{k}_{tag}"] for k in ("qx", "qy", "qz")]
+        for level in range(int(np.log2(min(n))) + 1):
+            out = oracle.cut3d(*q, n, level)
+            for k, o in zip(("qx", "qy", "qz"), out):
+                assert oracle.rel_l2(g[f"{k}_{tag}_cut{level}"], o) < 1e-12, (tag, level, k)
+            if level == 0:
+                assert all(oracle.rel_l2(a, o) < 1e-13 for a, o in zip(q, out))
+
+
 def test_mg2d_matches_reference_per_cycle(oracle):
     p = load_golden("mg2d_32")
     n = tuple(int(v) for v in p["n"])

@@ -63,6 +63,7 @@ SIGNATURES = {
     "wp_recover3d_create": (I, [PP, I, I, I, D, D, D, C, I, I]),
     "wp_recover3d_run": (I, [P, P, P, P, P, P, P, P]),
     "wp_recover3d_project": (I, [P, P, P, P, P, P, P, P]),
+    "wp_recover3d_cut": (I, [P, P, P, P, P, P, P, I, P]),
     "wp_recover3d_destroy": (I, [P]),
     "wp_recover2d_create": (I, [PP, I, I, D, D, C, I, I]),
     "wp_recover2d_run": (I, [P, P, P, P, P]),

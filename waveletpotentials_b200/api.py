@@ -116,6 +116,14 @@ class CuWaveletPotentialRecover3D:
                                      _ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]), _stream(stream)),
               "wp_recover3d_run")
 
+    def CutCoefficients(self, qx_out, qy_out, qz_out, qx, qy, qz, level, stream=None):
+        """Coarse-scale part of a potential (cuWaveletPotentialRecover3D.cu:199-239): the wavelet
+        coefficients below `level` cleared, synthesised back into the _out arrays."""
+        s = self.shapes
+        check(lib().wp_recover3d_cut(self._h, _ptr(qx_out, s["qx"]), _ptr(qy_out, s["qy"]), _ptr(qz_out, s["qz"]),
+                                     _ptr(qx, s["qx"]), _ptr(qy, s["qy"]), _ptr(qz, s["qz"]), int(level),
+                                     _stream(stream)), "wp_recover3d_cut")
+
     def ProjectLocal_q_ccc(self, qx, qy, qz, xv_lwt, yv_lwt, zv_lwt, stream=None):
         s = self.shapes
         check(lib().wp_recover3d_project(self._h, _ptr(qx, s["qx"]), _ptr(qy, s["qy"]), _ptr(qz, s["qz"]),

@@ -17,6 +17,8 @@
 //   CuWaveletPotentialRecover2D::Solve (cuWaveletPotentialRecover2D.cu:16-36).
 #include "wp_common.cuh"
 
+#include <algorithm>
+
 #include <cmath>
 #include <cstdlib>
 #include <new>
@@ -271,6 +273,74 @@ extern "C" CUWHHD_API wp_status wp_recover3d_run(wp_recover3d* h, float* qx, flo
     WP_T(qz, qz, nx + 1, ny + 1, nz, Lx, 'x', V, 'd', 0);
     WP_T(qz, qz, nx + 1, ny + 1, nz, Ly, 'y', V, 'd', 0);
     WP_T(qz, qz, nx + 1, ny + 1, nz, Lz, 'z', C, 'n', 0);
+#undef WP_T
+    return WP_OK;
+}
+
+// CuWaveletPotentialRecover3D::CutCoefficients (cuWaveletPotentialRecover3D.cu:123-239): in the
+// analysed potential, every cell (x, y, z) of the (nx+1, ny+1, nz+1) index box whose coefficient
+// level along some axis a, j_a = L_a - bitlength(max(i_a - 1, 0)), is below `cut` clears the three
+// components there: qx at (x-1, y, z), qy at (x, y-1, z), qz at (x, y, z-1), each where its index
+// exists (the reference's cuCutCoefs, with the same guards).
+__global__ void cut_coefs_kernel(float* __restrict__ qx, float* __restrict__ qy, float* __restrict__ qz, int nx,
+                                 int ny, int nz, int Lx, int Ly, int Lz, int cut) {
+    const int y = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y, z = blockIdx.z;
+    if (y > ny) return;
+    const int jx = Lx - (32 - __clz(max(x - 1, 0)));
+    const int jy = Ly - (32 - __clz(max(y - 1, 0)));
+    const int jz = Lz - (32 - __clz(max(z - 1, 0)));
+    if (jx >= cut && jy >= cut && jz >= cut) return;
+    // with cut <= min(L) a level below the cut needs an index >= 2 along that axis, so the
+    // component shifted along it exists; the other two are guarded as in the reference
+    if (x > 0 || jx < cut) qx[y + (long)(x - 1) * (ny + 1) + (long)z * nx * (ny + 1)] = 0.f;
+    if (y > 0 || jy < cut) qy[(y - 1) + (long)x * ny + (long)z * (nx + 1) * ny] = 0.f;
+    if (z > 0 || jz < cut) qz[y + (long)x * (ny + 1) + (long)(z - 1) * (nx + 1) * (ny + 1)] = 0.f;
+}
+
+extern "C" CUWHHD_API wp_status wp_recover3d_cut(wp_recover3d* h, float* qx_out, float* qy_out, float* qz_out,
+                                                 const float* qx, const float* qy, const float* qz, int level,
+                                                 void* stream) {
+    if (!h || !qx_out || !qy_out || !qz_out || !qx || !qy || !qz) {
+        wp_set_error_msg("wp_recover3d_cut: null pointer");
+        return WP_ERR_INVALID_ARG;
+    }
+    const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+    const int Lx = h->L[0], Ly = h->L[1], Lz = h->L[2];
+    if (level < 0 || level > std::min(Lx, std::min(Ly, Lz))) {
+        wp_set_error_msg("wp_recover3d_cut: level must lie in [0, min(levels)]");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int C = WP_ID_CDF3_7, V = WP_ID_CDF4_6;
+    wp_status st;
+#define WP_T(dst, src, DX, DY, DZ, L, ax, w, bc, f)                                          \
+    if ((st = wp_dwt_axis_launch<float>(dst, src, DX, DY, DZ, L, ax, w, bc, f, s)) != WP_OK) \
+        return st;
+    // analysis of each component with the recovery's synthesis wavelets (:205-215)
+    WP_T(qx_out, qx, nx, ny + 1, nz + 1, Lx, 'x', C, 'n', 1);
+    WP_T(qx_out, qx_out, nx, ny + 1, nz + 1, Ly, 'y', V, 'd', 1);
+    WP_T(qx_out, qx_out, nx, ny + 1, nz + 1, Lz, 'z', V, 'd', 1);
+    WP_T(qy_out, qy, nx + 1, ny, nz + 1, Lx, 'x', V, 'd', 1);
+    WP_T(qy_out, qy_out, nx + 1, ny, nz + 1, Ly, 'y', C, 'n', 1);
+    WP_T(qy_out, qy_out, nx + 1, ny, nz + 1, Lz, 'z', V, 'd', 1);
+    WP_T(qz_out, qz, nx + 1, ny + 1, nz, Lx, 'x', V, 'd', 1);
+    WP_T(qz_out, qz_out, nx + 1, ny + 1, nz, Ly, 'y', V, 'd', 1);
+    WP_T(qz_out, qz_out, nx + 1, ny + 1, nz, Lz, 'z', C, 'n', 1);
+    // the cut (:221-222)
+    const dim3 g((unsigned)wp_cdiv(ny + 1, 128), nx + 1, nz + 1);
+    const double bytes = 4.0 * 3.0 * (double)(nx + 1) * (ny + 1) * (nz + 1);
+    WP_KERNEL("cut_coefs", bytes, s,
+              cut_coefs_kernel<<<g, 128, 0, s>>>(qx_out, qy_out, qz_out, nx, ny, nz, Lx, Ly, Lz, level));
+    // synthesis (:228-238)
+    WP_T(qx_out, qx_out, nx, ny + 1, nz + 1, Lx, 'x', C, 'n', 0);
+    WP_T(qx_out, qx_out, nx, ny + 1, nz + 1, Ly, 'y', V, 'd', 0);
+    WP_T(qx_out, qx_out, nx, ny + 1, nz + 1, Lz, 'z', V, 'd', 0);
+    WP_T(qy_out, qy_out, nx + 1, ny, nz + 1, Lx, 'x', V, 'd', 0);
+    WP_T(qy_out, qy_out, nx + 1, ny, nz + 1, Ly, 'y', C, 'n', 0);
+    WP_T(qy_out, qy_out, nx + 1, ny, nz + 1, Lz, 'z', V, 'd', 0);
+    WP_T(qz_out, qz_out, nx + 1, ny + 1, nz, Lx, 'x', V, 'd', 0);
+    WP_T(qz_out, qz_out, nx + 1, ny + 1, nz, Ly, 'y', V, 'd', 0);
+    WP_T(qz_out, qz_out, nx + 1, ny + 1, nz, Lz, 'z', C, 'n', 0);
 #undef WP_T
     return WP_OK;
 }
