@@ -301,6 +301,13 @@ def run_ours(args, rank, world, local_rank):
             # CuWaveletPotentialRecover3D::CutCoefficients of the recovered potential at level 2
             "cut_level2_ms": time_rec(lambda: proj.rec.CutCoefficients(*qs, *q, 2)),
         }
+        # face fractions of the same spheres' level set by the static CuSolidLevelSet3D::GetFrac
+        # (cut faces sub-sampled 128 x 128) against the two-point formula the projection uses
+        fa = [torch.empty_like(t) for t in a]
+        plain["fractions"] = {
+            "subsampled_ms": time_rec(lambda: sls.GetFrac(*fa, ls=sls.ls, dim=nn, dx=h), k=3),
+            "two_point_ms": time_rec(lambda: sls.GetFrac(*fa), k=3),
+        }
         sw.close()
         # the index-sparse cycle (CuMultigridFrac3D::Solve_index) against the dense reference cycle
         # (CuMultigridFrac3D::Solve) on a mostly-solid domain of the same extent: balls of fluid

@@ -266,6 +266,13 @@ CUWHHD_API wp_status wp_sdf_boxes3d(float* sdf, int nx, int ny, int nz, double d
 /* Face open fractions from a level set (cuGetAx/Ay/Az, cuSolidLevelSet3D.cu:36-90). */
 CUWHHD_API wp_status wp_fractions3d(float* ax, float* ay, float* az, const float* sdf, int nx, int ny, int nz,
                                     double dx, void* stream);
+/* Replaces the static CuSolidLevelSet3D::GetFrac(ax, ay, az, ls, dim, dx) (cuSolidLevelSet3D.cu:356-372,
+   kernels cuGetAx/Ay/Az_divide :164-316): face open fractions of an arbitrary level set (positive in
+   fluid): open where the quadratic interpolant at the face centre exceeds dx, closed at or below
+   -dx, otherwise the share of 128 x 128 sub-face samples where the trilinear interpolant is
+   positive.  FP64 arithmetic; ls FP32.  Extents >= 2 and fewer than 2^30 faces per axis. */
+CUWHHD_API wp_status wp_fractions3d_subsampled(float* ax, float* ay, float* az, const float* ls, int nx, int ny,
+                                               int nz, double dx, void* stream);
 /* 2D: circle level set (CuSolidLevelSet2D, cuSolidLevelSet2D.cu) and face fractions. */
 CUWHHD_API wp_status wp_sdf_circles2d(float* sdf, int nx, int ny, double dx, const double* centers, const double* radii,
                                       int count, void* stream);

@@ -64,6 +64,7 @@ def lib():
             "or_mgfrac3d_solve": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, i, p]),
             "or_mgfrac3d_solve_index": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, p, p]),
             "or_cut3d": (i, [p, p, p, i, i, i, i]),
+            "or_fractions3d_subsampled": (None, [p, p, p, p, i, i, i, d]),
             "or_mgfrac2d_solve": (i, [p, p, p, p, p, i, i, d, d, i, i, i, d, i, p]),
             "or_frac_residual3d": (d, [p, p, p, p, p, p, i, i, i, d, d, d]),
             "or_frac_residual2d": (d, [p, p, p, p, p, i, i, d, d]),
@@ -237,6 +238,15 @@ def fractions3d(sdf, n, dx):
     s = mac_shapes3d(nx, ny, nz)
     ax, ay, az = (np.zeros(s[k]) for k in ("xv", "yv", "zv"))
     lib().or_fractions3d(_p(ax), _p(ay), _p(az), _p(_f64(sdf)), nx, ny, nz, dx)
+    return ax, ay, az
+
+
+def fractions3d_subsampled(ls, n, dx):
+    """CuSolidLevelSet3D::GetFrac(ax, ay, az, ls, dim, dx): cut faces sub-sampled 128 x 128."""
+    nx, ny, nz = n
+    s = mac_shapes3d(nx, ny, nz)
+    ax, ay, az = (np.zeros(s[k]) for k in ("xv", "yv", "zv"))
+    lib().or_fractions3d_subsampled(_p(ax), _p(ay), _p(az), _p(_f64(ls)), nx, ny, nz, dx)
     return ax, ay, az
 
 

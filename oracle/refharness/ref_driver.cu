@@ -144,6 +144,22 @@ int main(int argc, char** argv) {
         write_bin("qx", from_dev(ox, sqx));
         write_bin("qy", from_dev(oy, sqy));
         write_bin("qz", from_dev(oz, sqz));
+    } else if (op == "frac3d_sub") {  // nx ny nz dx: static CuSolidLevelSet3D::GetFrac(ax, ay, az, ls, dim, dx)
+        int3 dim = make_int3(I(0), I(1), I(2));
+        DTYPE h = (DTYPE)D(3);
+        DTYPE3 dx = make_DTYPE3(h, h, h);
+        size_t n = (size_t)dim.x * dim.y * dim.z;
+        size_t sx = (size_t)(dim.x + 1) * dim.y * dim.z, sy = (size_t)dim.x * (dim.y + 1) * dim.z;
+        size_t sz = (size_t)dim.x * dim.y * (dim.z + 1);
+        DTYPE* ls = to_dev(read_bin("ls", n));
+        DTYPE* ax = dev_zeros(sx);
+        DTYPE* ay = dev_zeros(sy);
+        DTYPE* az = dev_zeros(sz);
+        CuSolidLevelSet3D::GetFrac(ax, ay, az, ls, dim, dx);
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("ax", from_dev(ax, sx));
+        write_bin("ay", from_dev(ay, sy));
+        write_bin("az", from_dev(az, sz));
     } else if (op == "project2d" || op == "recover2d") {  // nx ny dx
         int2 dim = make_int2(I(0), I(1));
         DTYPE h = (DTYPE)D(2);

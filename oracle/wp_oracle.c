@@ -783,6 +783,89 @@ void or_fractions2d(double* ax, double* ay, const double* sdf, int nx, int ny, d
         }
 }
 
+/* --------------------------------------------- subsampled face fractions of a level set ---- */
+/* CuSolidLevelSet3D::GetFrac(ax, ay, az, ls, dim, dx) (cuSolidLevelSet3D.cu:356-372) with
+   cuGetAx/Ay/Az_divide (:164-316); InterpolateQuadratic3D (Interpolation.cuh:119-156),
+   InterpolateLinear3D with cuGetIxFx (:16-29, 80-117), CLAMP_L of the double build (:9) */
+static const double OR_CLAMP_L = (double)1e-10f;
+
+static double ls_quadratic3(const double* ls, double x, double y, double z, int nx, int ny, int nz) {
+    int ix = (int)floor(x - 0.5), iy = (int)floor(y - 0.5), iz = (int)floor(z - 0.5);
+    double fx = x - ix, fy = y - iy, fz = z - iz;
+    double wx[3] = {0.5 * (1.5 - fx) * (1.5 - fx), 0.75 - (fx - 1.0) * (fx - 1.0), 0.5 * (fx - 0.5) * (fx - 0.5)};
+    double wy[3] = {0.5 * (1.5 - fy) * (1.5 - fy), 0.75 - (fy - 1.0) * (fy - 1.0), 0.5 * (fy - 0.5) * (fy - 0.5)};
+    double wz[3] = {0.5 * (1.5 - fz) * (1.5 - fz), 0.75 - (fz - 1.0) * (fz - 1.0), 0.5 * (fz - 0.5) * (fz - 0.5)};
+    double r = 0.0;
+    for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                int xx = ix + j < 0 ? 0 : (ix + j > nx - 1 ? nx - 1 : ix + j);
+                int yy = iy + i < 0 ? 0 : (iy + i > ny - 1 ? ny - 1 : iy + i);
+                int zz = iz + k < 0 ? 0 : (iz + k > nz - 1 ? nz - 1 : iz + k);
+                r += wx[j] * wy[i] * wz[k] * ls[yy + (long)xx * ny + (long)zz * nx * ny];
+            }
+    return r;
+}
+
+static void ixfx(int* i, double* f, double x, int n) {
+    if (x < OR_CLAMP_L) x = OR_CLAMP_L;
+    *i = (int)x;
+    if (*i >= n - 1) { *i = n - 2; *f = 1.0; } /* 1.f - CLAMP_L is 1 in float */
+    else *f = x - *i;
+}
+
+static double ls_linear3(const double* ls, double x, double y, double z, int nx, int ny, int nz) {
+    int ix, iy, iz;
+    double fx, fy, fz;
+    ixfx(&ix, &fx, x, nx);
+    ixfx(&iy, &fy, y, ny);
+    ixfx(&iz, &fz, z, nz);
+    double wx0 = 1 - fx, wy0 = 1 - fy, wz0 = 1 - fz;
+    long sl = (long)nx * ny, i0 = iy + (long)ix * ny + iz * sl;
+    double r = ls[i0] * wx0 * wy0 * wz0;
+    r += ls[i0 + 1] * wx0 * fy * wz0;
+    r += ls[i0 + ny] * fx * wy0 * wz0;
+    r += ls[i0 + ny + 1] * fx * fy * wz0;
+    i0 += sl;
+    r += ls[i0] * wx0 * wy0 * fz;
+    r += ls[i0 + 1] * wx0 * fy * fz;
+    r += ls[i0 + ny] * fx * wy0 * fz;
+    r += ls[i0 + ny + 1] * fx * fy * fz;
+    return r;
+}
+
+void or_fractions3d_subsampled(double* ax, double* ay, double* az, const double* ls, int nx, int ny, int nz, double dx) {
+    double inv = 1.0 / dx, dsub = dx / 128, half = 0.5 * dsub;
+    for (int a = 0; a < 3; ++a) {
+        int ex = nx + (a == 0), ey = ny + (a == 1), ez = nz + (a == 2);
+        double* out = a == 0 ? ax : (a == 1 ? ay : az);
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int z = 0; z < ez; ++z)
+            for (int x = 0; x < ex; ++x)
+                for (int y = 0; y < ey; ++y) {
+                    double px = (a == 0 ? (double)x : x + 0.5) * dx, py = (a == 1 ? (double)y : y + 0.5) * dx;
+                    double pz = (a == 2 ? (double)z : z + 0.5) * dx;
+                    double v = ls_quadratic3(ls, px * inv - 0.5, py * inv - 0.5, pz * inv - 0.5, nx, ny, nz);
+                    double res = 0.0;
+                    if (v > dx) {
+                        res = 1.0;
+                    } else if (v > -dx) {
+                        int cnt = 0;
+                        for (int o = 0; o < 128; ++o)
+                            for (int in = 0; in < 128; ++in) {
+                                double qx, qy, qz;
+                                if (a == 0) { qx = x * dx; qy = y * dx + half + in * dsub; qz = z * dx + half + o * dsub; }
+                                else if (a == 1) { qx = x * dx + half + in * dsub; qy = y * dx; qz = z * dx + half + o * dsub; }
+                                else { qx = x * dx + half + o * dsub; qy = y * dx + half + in * dsub; qz = z * dx; }
+                                if (ls_linear3(ls, qx * inv - 0.5, qy * inv - 0.5, qz * inv - 0.5, nx, ny, nz) > 0.0) ++cnt;
+                            }
+                        res = cnt * (1.0 / 16384.0);
+                    }
+                    out[y + (long)x * ey + (long)z * ex * ey] = res < 0.0 ? 0.0 : (res > 1.0 ? 1.0 : res);
+                }
+    }
+}
+
 /* ------------------------------------------------------- fractional multigrid 3D ---- */
 /* cuWjFrac3D_n (cuWeightedJacobi3D.cu:620-695): Neumann walls, cut-cell face weights */
 static inline void frac_row3d(const double* v, const double* ax, const double* ay, const double* az,

@@ -6,11 +6,13 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py            # every fixture
     python tests/golden/make_golden.py --only index   # the index-sparse multigrid cases only
     python tests/golden/make_golden.py --only cut     # the coefficient truncation cases only
+    python tests/golden/make_golden.py --only frac    # the sub-sampled face fraction cases only
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
 (CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D::ProjectLocal_q_ccc,
 CuDivLocalProject::ProjectSingle, CuWaveletPotentialRecover3D/2D::Solve, CuMultigridFrac3D/2D::Solve,
-CuMultigridFrac3D::Solve_index, CuWaveletPotentialRecover3D::CutCoefficients, CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P,
+CuMultigridFrac3D::Solve_index, CuWaveletPotentialRecover3D::CutCoefficients, CuSolidLevelSet3D::GetFrac (static, sub-sampled),
+CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P,
 CuSolidLevelSet3D) and stores inputs
 and reference outputs as ``<case>.npz``.  The CPU tests pin the FP64 oracle against these files;
 the GPU tests compare the CUDA kernels with the oracle on the same inputs.
@@ -114,6 +116,30 @@ def cut_cases(rng):
     save("cut3d", **out)
 
 
+def frac_cases(rng):
+    """The static CuSolidLevelSet3D::GetFrac(ax, ay, az, ls, dim, dx): sub-sampled face fractions of
+    two level sets given as FP32 values -- two overlapping spheres in a box, and a wavy surface."""
+    out = {}
+    for tag, n in (("spheres", (24, 20, 16)), ("wavy", (16, 16, 16))):
+        nx, ny, nz = n
+        h = 1.0 / nx
+        z, x, y = np.meshgrid((np.arange(nz) + 0.5) * h, (np.arange(nx) + 0.5) * h, (np.arange(ny) + 0.5) * h,
+                              indexing="ij")
+        if tag == "spheres":
+            ls = np.minimum(np.sqrt((x - 0.45) ** 2 + (y - 0.4) ** 2 + (z - 0.3) ** 2) - 0.22,
+                            np.sqrt((x - 0.7) ** 2 + (y - 0.55) ** 2 + (z - 0.35) ** 2) - 0.15)
+        else:
+            ls = z - 0.5 - 0.12 * np.sin(2 * np.pi * x * 1.5) * np.cos(2 * np.pi * y) + 0.01 * rng.standard_normal(x.shape)
+        ls = ls.astype(np.float32).astype(np.float64)
+        s = shapes3(n)
+        res = run("frac3d_sub", {"ls": ls}, [nx, ny, nz, h], {"ax": s["xv"], "ay": s["yv"], "az": s["zv"]})
+        out[f"n_{tag}"] = np.array(n)
+        out[f"ls_{tag}"] = ls
+        for k in ("ax", "ay", "az"):
+            out[f"{k}_{tag}"] = res[k]
+    save("frac3d_sub", **out)
+
+
 def main():
     if not os.path.exists(DRIVER):
         sys.exit(f"{DRIVER} missing: run make -C oracle/refharness first (needs nvcc and the reference sources)")
@@ -123,6 +149,9 @@ def main():
         return
     if only == "cut":
         cut_cases(np.random.default_rng(20261205))
+        return
+    if only == "frac":
+        frac_cases(np.random.default_rng(20261206))
         return
     rng = np.random.default_rng(20261203)
 
@@ -242,6 +271,7 @@ def main():
     save("mg2d_32", n=np.array(n2), h=1.0 / 32, f=f2, ax=ax2, ay=ay2, ncycles=5, nu=np.array([5, 5]), omega=0.8, **out)
     index_cases(np.random.default_rng(20261204))
     cut_cases(np.random.default_rng(20261205))
+    frac_cases(np.random.default_rng(20261206))
 
 
 if __name__ == "__main__":

@@ -141,6 +141,20 @@ def test_cut3d_matches_reference(oracle):
                 assert all(oracle.rel_l2(a, o) < 1e-13 for a, o in zip(q, out))
 
 
+def test_subsampled_fractions_match_reference(oracle):
+    """The static CuSolidLevelSet3D::GetFrac: open / closed by the quadratic interpolant at the face
+    centre, cut faces as a count of 128 x 128 trilinear samples (up to a few samples that lie within
+    rounding of the zero level)."""
+    g = load_golden("frac3d_sub")
+    for key in [k for k in g.files if k.startswith("n_")]:
+        tag = key[2:]
+        n = tuple(int(v) for v in g[key])
+        out = oracle.fractions3d_subsampled(g[f"ls_{tag}"], n, 1.0 / n[0])
+        for k, o in zip(("ax", "ay", "az"), out):
+            d = np.abs(o - g[f"{k}_{tag}"])
+            assert d.max() <= 3.0 / 16384 and np.count_nonzero(d) <= 3, (tag, k, d.max(), np.count_nonzero(d))
+
+
 def test_mg2d_matches_reference_per_cycle(oracle):
     p = load_golden("mg2d_32")
     n = tuple(int(v) for v in p["n"])

@@ -90,6 +90,7 @@ SIGNATURES = {
     "wp_max_abs": (I, [P, S, ctypes.POINTER(D), P]),
     "wp_sdf_spheres3d": (I, [P, I, I, I, D, P, P, I, P]),
     "wp_fractions3d": (I, [P, P, P, P, I, I, I, D, P]),
+    "wp_fractions3d_subsampled": (I, [P, P, P, P, I, I, I, D, P]),
     "wp_sdf_boxes3d": (I, [P, I, I, I, D, P, P, I, P]),
     "wp_sdf_circles2d": (I, [P, I, I, D, P, P, I, P]),
     "wp_fractions2d": (I, [P, P, P, I, I, D, P]),

@@ -415,10 +415,20 @@ class CuSolidLevelSet3D:
     def InitLsSphere(self, center, radius, stream=None):
         self.InitLsSpheres([center], [radius], stream)
 
-    def GetFrac(self, ax, ay, az, stream=None):
-        s = mac_shapes3d(*self.dim)
-        check(lib().wp_fractions3d(_ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(az, s["zv"]), _ptr(self.ls), *self.dim,
-                                   self.dx, _stream(stream)), "wp_fractions3d")
+    def GetFrac(self, ax, ay, az, ls=None, dim=None, dx=None, stream=None):
+        """GetFrac(ax, ay, az): fractions of the object's level set from the values at the two cells
+        of each face (cuGetAx/Ay/Az).  GetFrac(ax, ay, az, ls, dim, dx): the reference's static
+        overload for an arbitrary level set, sub-sampling the cut faces (cuGetAx/Ay/Az_divide)."""
+        if ls is None:
+            s = mac_shapes3d(*self.dim)
+            check(lib().wp_fractions3d(_ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(az, s["zv"]), _ptr(self.ls),
+                                       *self.dim, self.dx, _stream(stream)), "wp_fractions3d")
+            return
+        d = _dims3(dim) if dim is not None else self.dim
+        h = float(dx) if dx is not None else self.dx
+        s = mac_shapes3d(*d)
+        check(lib().wp_fractions3d_subsampled(_ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(az, s["zv"]),
+                                              _ptr(ls, s["p"]), *d, h, _stream(stream)), "wp_fractions3d_subsampled")
 
 
     def AddBoxes(self, lo, hi, stream=None):

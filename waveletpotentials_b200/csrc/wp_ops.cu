@@ -371,6 +371,176 @@ extern "C" CUWHHD_API wp_status wp_fractions3d(float* ax, float* ay, float* az, 
     return WP_OK;
 }
 
+// ------------------------------------------------ subsampled face fractions of a level set
+// CuSolidLevelSet3D::GetFrac(ax, ay, az, ls, dim, dx) (cuSolidLevelSet3D.cu:356-372) with the kernels
+// cuGetAx/Ay/Az_divide (:164-316): the level set interpolated quadratically at the face centre
+// (InterpolateQuadratic3D, Interpolation.cuh:119-156) decides open (> dx), closed (<= -dx) or cut;
+// a cut face is the share of 128 x 128 sub-face samples where the trilinear interpolant
+// (InterpolateLinear3D with cuGetIxFx's clamping, Interpolation.cuh:16-29, 80-117) is positive.
+// FP64 arithmetic in the reference's term order (its default build); the level set is FP32.
+// Work split: one thread per face classifies and lists the cut faces; one warp per listed face
+// counts its samples (16 rounds of 32 lanes x 32 samples with ballots).
+namespace {
+constexpr double kClampL = (double)1e-10f;  // CLAMP_L of the double build (Interpolation.cuh:9)
+
+__device__ __forceinline__ double ls_at(const float* __restrict__ ls, int x, int y, int z, int nx, int ny) {
+    return (double)ls[y + (long)x * ny + (long)z * nx * ny];
+}
+
+__device__ double ls_quadratic(const float* __restrict__ ls, double x, double y, double z, int nx, int ny, int nz) {
+    const int ix = (int)floor(x - 0.5), iy = (int)floor(y - 0.5), iz = (int)floor(z - 0.5);
+    const double fx = x - ix, fy = y - iy, fz = z - iz;
+    auto p2 = [](double v) { return v * v; };
+    const double wx[3] = {0.5 * p2(1.5 - fx), 0.75 - p2(fx - 1.0), 0.5 * p2(fx - 0.5)};
+    const double wy[3] = {0.5 * p2(1.5 - fy), 0.75 - p2(fy - 1.0), 0.5 * p2(fy - 0.5)};
+    const double wz[3] = {0.5 * p2(1.5 - fz), 0.75 - p2(fz - 1.0), 0.5 * p2(fz - 0.5)};
+    double r = 0.0;
+    for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                const int xx = min(max(ix + j, 0), nx - 1), yy = min(max(iy + i, 0), ny - 1);
+                const int zz = min(max(iz + k, 0), nz - 1);
+                r += wx[j] * wy[i] * wz[k] * ls_at(ls, xx, yy, zz, nx, ny);
+            }
+    return r;
+}
+
+__device__ __forceinline__ void clamp_index(int& i, double& f, double x, int n) {
+    x = fmax(kClampL, x);
+    i = (int)x;
+    if (i >= n - 1) {
+        i = n - 2;
+        f = 1.0;  // 1.f - CLAMP_L evaluates in float to 1
+    } else {
+        f = x - i;
+    }
+}
+
+__device__ double ls_linear(const float* __restrict__ ls, double x, double y, double z, int nx, int ny, int nz) {
+    int ix, iy, iz;
+    double fx, fy, fz;
+    clamp_index(ix, fx, x, nx);
+    clamp_index(iy, fy, y, ny);
+    clamp_index(iz, fz, z, nz);
+    const double wx0 = 1 - fx, wy0 = 1 - fy, wz0 = 1 - fz;
+    double r = ls_at(ls, ix, iy, iz, nx, ny) * wx0 * wy0 * wz0;
+    r += ls_at(ls, ix, iy + 1, iz, nx, ny) * wx0 * fy * wz0;
+    r += ls_at(ls, ix + 1, iy, iz, nx, ny) * fx * wy0 * wz0;
+    r += ls_at(ls, ix + 1, iy + 1, iz, nx, ny) * fx * fy * wz0;
+    r += ls_at(ls, ix, iy, iz + 1, nx, ny) * wx0 * wy0 * fz;
+    r += ls_at(ls, ix, iy + 1, iz + 1, nx, ny) * wx0 * fy * fz;
+    r += ls_at(ls, ix + 1, iy, iz + 1, nx, ny) * fx * wy0 * fz;
+    r += ls_at(ls, ix + 1, iy + 1, iz + 1, nx, ny) * fx * fy * fz;
+    return r;
+}
+
+// face (axis a, index i of that axis' face array) -> its integer coordinates
+__device__ __forceinline__ void face_coords(int a, long i, int nx, int ny, int& x, int& y, int& z) {
+    const int ex = nx + (a == 0), ey = ny + (a == 1);
+    y = (int)(i % ey);
+    const long xz = i / ey;
+    x = (int)(xz % ex);
+    z = (int)(xz / ex);
+}
+
+__global__ void frac_classify_kernel(float* __restrict__ ax, float* __restrict__ ay, float* __restrict__ az,
+                                     const float* __restrict__ ls, int nx, int ny, int nz, double dx,
+                                     unsigned* __restrict__ work, unsigned* __restrict__ nwork) {
+    const long n0 = (long)(nx + 1) * ny * nz, n1 = (long)nx * (ny + 1) * nz, n2 = (long)nx * ny * (nz + 1);
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n0 + n1 + n2; t += (long)gridDim.x * blockDim.x) {
+        const int a = t < n0 ? 0 : (t < n0 + n1 ? 1 : 2);
+        const long i = t - (a == 0 ? 0 : (a == 1 ? n0 : n0 + n1));
+        int x, y, z;
+        face_coords(a, i, nx, ny, x, y, z);
+        const double inv = 1.0 / dx;
+        const double px = (a == 0 ? (double)x : x + 0.5) * dx, py = (a == 1 ? (double)y : y + 0.5) * dx;
+        const double pz = (a == 2 ? (double)z : z + 0.5) * dx;
+        const double v = ls_quadratic(ls, px * inv - 0.5, py * inv - 0.5, pz * inv - 0.5, nx, ny, nz);
+        float* out = a == 0 ? ax : (a == 1 ? ay : az);
+        if (v > dx) {
+            out[i] = 1.f;
+        } else if (v > -dx) {
+            out[i] = 0.f;
+            work[atomicAdd(nwork, 1u)] = ((unsigned)a << 30) | (unsigned)i;
+        } else {
+            out[i] = 0.f;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) frac_subsample_kernel(float* __restrict__ ax, float* __restrict__ ay,
+                                                             float* __restrict__ az, const float* __restrict__ ls,
+                                                             int nx, int ny, int nz, double dx,
+                                                             const unsigned* __restrict__ work,
+                                                             const unsigned* __restrict__ nwork) {
+    const int lane = threadIdx.x & 31;
+    const unsigned total = *nwork;
+    const unsigned warps = gridDim.x * (blockDim.x >> 5);
+    const double inv = 1.0 / dx, dsub = dx / 128, half = 0.5 * dsub;
+    for (unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < total; w += warps) {
+        const unsigned code = work[w];
+        const int a = (int)(code >> 30);
+        const long i = code & 0x3fffffffu;
+        int x, y, z;
+        face_coords(a, i, nx, ny, x, y, z);
+        // the two in-face axes: u is the reference's inner loop, w its outer loop
+        const double fixed = (a == 0 ? x : (a == 1 ? y : z)) * dx;
+        const double ub = (a == 0 ? y : x) * dx + half;  // ax: i over y, k over z; ay: j over x, k over z;
+        const double wb = (a == 2 ? y : z) * dx + half;  // az: i over y (inner), j over x (outer)
+        int count = 0;
+        for (int s0 = 0; s0 < 128 * 128; s0 += 32) {
+            const int s = s0 + lane;
+            const int outer = s >> 7, inner = s & 127;
+            double px, py, pz;
+            if (a == 0) {
+                px = fixed; py = ub + inner * dsub; pz = wb + outer * dsub;
+            } else if (a == 1) {
+                px = ub + inner * dsub; py = fixed; pz = wb + outer * dsub;
+            } else {
+                px = ub + outer * dsub; py = wb + inner * dsub; pz = fixed;
+            }
+            const double v = ls_linear(ls, px * inv - 0.5, py * inv - 0.5, pz * inv - 0.5, nx, ny, nz);
+            count += __popc(__ballot_sync(0xffffffffu, v > 0.0));
+        }
+        if (lane == 0) {
+            float* out = a == 0 ? ax : (a == 1 ? ay : az);
+            const double r = count * (1.0 / 16384.0);
+            out[i] = (float)fmin(fmax(r, 0.0), 1.0);
+        }
+    }
+}
+}  // namespace
+
+extern "C" CUWHHD_API wp_status wp_fractions3d_subsampled(float* ax, float* ay, float* az, const float* ls, int nx,
+                                                          int ny, int nz, double dx, void* stream) {
+    if (!ax || !ay || !az || !ls || nx < 2 || ny < 2 || nz < 2 || !(dx > 0) ||
+        (double)(nx + 1) * (ny + 1) * (nz + 1) >= (double)(1u << 30)) {
+        wp_set_error_msg("wp_fractions3d_subsampled: bad arguments (extents >= 2, fewer than 2^30 faces per axis, dx > 0)");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const long faces = (long)(nx + 1) * ny * nz + (long)nx * (ny + 1) * nz + (long)nx * ny * (nz + 1);
+    unsigned* buf = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&buf, sizeof(unsigned) * (faces + 1), s));
+    cudaError_t e = cudaMemsetAsync(buf, 0, sizeof(unsigned), s);
+    if (e == cudaSuccess) {
+        const int tok = wp_prof_start(s);
+        const unsigned g = (unsigned)std::min<long>(wp_cdiv(faces, 256), (long)wp_sm_count() * 16);
+        frac_classify_kernel<<<g, 256, 0, s>>>(ax, ay, az, ls, nx, ny, nz, dx, buf + 1, buf);
+        e = cudaGetLastError();
+        wp_prof_stop(tok, "frac_classify", 4.0 * faces + 27.0 * 4.0 * faces, s);
+    }
+    if (e == cudaSuccess) {
+        const int tok = wp_prof_start(s);
+        frac_subsample_kernel<<<wp_sm_count() * 8, 256, 0, s>>>(ax, ay, az, ls, nx, ny, nz, dx, buf + 1, buf);
+        e = cudaGetLastError();
+        wp_prof_stop(tok, "frac_subsample", 0.0, s);
+    }
+    cudaFreeAsync(buf, s);
+    if (e != cudaSuccess) { wp_set_cuda_error(e, "subsampled fractions", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    return WP_OK;
+}
+
 extern "C" CUWHHD_API wp_status wp_sdf_boxes3d(float* sdf, int nx, int ny, int nz, double dx, const double* lo,
                                                const double* hi, int count, void* stream) {
     if (!sdf || nx <= 0 || ny <= 0 || nz <= 0 || nz > 65535 || count < 0 || count > 4096 ||
