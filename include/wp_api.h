@@ -273,6 +273,14 @@ CUWHHD_API wp_status wp_fractions3d(float* ax, float* ay, float* az, const float
    positive.  FP64 arithmetic; ls FP32.  Extents >= 2 and fewer than 2^30 faces per axis. */
 CUWHHD_API wp_status wp_fractions3d_subsampled(float* ax, float* ay, float* az, const float* ls, int nx, int ny,
                                                int nz, double dx, void* stream);
+/* Replace CuFastSweeping::Solve(ls, dim, dx, n_iters) and ReinitLevelSet(ls, dim, dx, n_iters)
+   (cuFastSweeping.cu:215-257, 383-396): n_iters eikonal updates of every cell above -1e-12 from its
+   neighbours (upwind |grad d| = 1, spacing dx on every axis; cells at or below -1e-12 are the fixed
+   sources); Reinit negates, sweeps, negates back and sweeps again, so both sides become distances.
+   Each iteration reads the previous one (the reference updates in place from concurrent threads):
+   one cell of propagation per iteration, the same fixed point. */
+CUWHHD_API wp_status wp_fast_sweep_solve(float* ls, int nx, int ny, int nz, double dx, int n_iters, void* stream);
+CUWHHD_API wp_status wp_fast_sweep_reinit(float* ls, int nx, int ny, int nz, double dx, int n_iters, void* stream);
 /* 2D: circle level set (CuSolidLevelSet2D, cuSolidLevelSet2D.cu) and face fractions. */
 CUWHHD_API wp_status wp_sdf_circles2d(float* sdf, int nx, int ny, double dx, const double* centers, const double* radii,
                                       int count, void* stream);

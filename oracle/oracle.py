@@ -64,6 +64,7 @@ def lib():
             "or_mgfrac3d_solve": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, i, p]),
             "or_mgfrac3d_solve_index": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, p, p]),
             "or_cut3d": (i, [p, p, p, i, i, i, i]),
+            "or_fast_sweep": (None, [p, i, i, i, d, i, i]),
             "or_fractions3d_subsampled": (None, [p, p, p, p, i, i, i, d]),
             "or_mgfrac2d_solve": (i, [p, p, p, p, p, i, i, d, d, i, i, i, d, i, p]),
             "or_frac_residual3d": (d, [p, p, p, p, p, p, i, i, i, d, d, d]),
@@ -248,6 +249,13 @@ def fractions3d_subsampled(ls, n, dx):
     ax, ay, az = (np.zeros(s[k]) for k in ("xv", "yv", "zv"))
     lib().or_fractions3d_subsampled(_p(ax), _p(ay), _p(az), _p(_f64(ls)), nx, ny, nz, dx)
     return ax, ay, az
+
+
+def fast_sweep(ls, n, dx, iters, reinit=False):
+    """CuFastSweeping::Solve (reinit=False) / ReinitLevelSet (True) as Jacobi iterations."""
+    out = np.array(_f64(ls))
+    lib().or_fast_sweep(_p(out), *n, dx, iters, int(bool(reinit)))
+    return out
 
 
 def fractions2d(sdf, n, dx):

@@ -32,6 +32,7 @@
 #include "cuConvergence.cuh"
 #include "cuGradient.cuh"
 #include "cuSolidLevelSet3D.cuh"
+#include "cuFastSweeping.cuh"
 
 static std::string g_in, g_out;
 
@@ -160,6 +161,16 @@ int main(int argc, char** argv) {
         write_bin("ax", from_dev(ax, sx));
         write_bin("ay", from_dev(ay, sy));
         write_bin("az", from_dev(az, sz));
+    } else if (op == "fsweep") {  // nx ny nz dx iters reinit: CuFastSweeping::Solve / ReinitLevelSet
+        int3 dim = make_int3(I(0), I(1), I(2));
+        DTYPE h = (DTYPE)D(3);
+        int iters = I(4), reinit = I(5);
+        size_t n = (size_t)dim.x * dim.y * dim.z;
+        DTYPE* ls = to_dev(read_bin("ls", n));
+        if (reinit) CuFastSweeping::ReinitLevelSet(ls, dim, h, iters);
+        else CuFastSweeping::Solve(ls, dim, h, iters);
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("ls", from_dev(ls, n));
     } else if (op == "project2d" || op == "recover2d") {  // nx ny dx
         int2 dim = make_int2(I(0), I(1));
         DTYPE h = (DTYPE)D(2);

@@ -866,6 +866,58 @@ void or_fractions3d_subsampled(double* ax, double* ay, double* az, const double*
     }
 }
 
+/* -------------------------------------------------------------- fast sweeping ---- */
+/* CuFastSweeping::Solve / ReinitLevelSet (cuFastSweeping.cu:98-140, 215-257, 383-396): Jacobi
+   iterations (each reads the previous iterate) of the upwind eikonal update on cells above -1e-12 */
+static double eikonal3(double mx, double my, double mz, double h) {
+    double m[3] = {mx, my, mz};
+    for (int i = 1; i < 3; ++i)
+        for (int j = 0; j < 3 - i; ++j)
+            if (m[j] > m[j + 1]) { double t = m[j]; m[j] = m[j + 1]; m[j + 1] = t; }
+    double d2 = h * h, r = m[0] + h;
+    if (r > m[1]) {
+        double s = sqrt(-m[0] * m[0] + 2 * m[0] * m[1] - m[1] * m[1] + 2 * d2);
+        r = (m[1] * d2 + m[0] * d2 + d2 * s) / (2 * d2);
+        if (r > m[2]) {
+            double a = sqrt(d2 * (-2 * m[0] * m[0] - 2 * m[1] * m[1] - 2 * m[2] * m[2] + 2 * m[0] * m[1] +
+                                  2 * m[0] * m[2] + 2 * m[1] * m[2]) + 3 * d2 * d2);
+            r = (d2 * d2 * (m[0] + m[1] + m[2]) + h * d2 * a) / (3 * d2 * d2);
+        }
+    }
+    return r;
+}
+
+static void fsweep3(double* ls, int nx, int ny, int nz, double h, int iters) {
+    long n = (long)nx * ny * nz, sl = (long)nx * ny;
+    double* prev = (double*)malloc(sizeof(double) * n);
+    for (int it = 0; it < iters; ++it) {
+        memcpy(prev, ls, sizeof(double) * n);
+#pragma omp parallel for schedule(static)
+        for (int z = 0; z < nz; ++z)
+            for (int x = 0; x < nx; ++x)
+                for (int y = 0; y < ny; ++y) {
+                    long i = y + (long)x * ny + z * sl;
+                    if (!(prev[i] > -1e-12)) continue;
+                    double big = 1e8;
+                    double l = x > 0 ? prev[i - ny] : big, r = x < nx - 1 ? prev[i + ny] : big;
+                    double u = y < ny - 1 ? prev[i + 1] : big, d = y > 0 ? prev[i - 1] : big;
+                    double f = z > 0 ? prev[i - sl] : big, b = z < nz - 1 ? prev[i + sl] : big;
+                    ls[i] = eikonal3(l < r ? l : r, u < d ? u : d, f < b ? f : b, h);
+                }
+    }
+    free(prev);
+}
+
+void or_fast_sweep(double* ls, int nx, int ny, int nz, double dx, int iters, int reinit) {
+    long n = (long)nx * ny * nz;
+    if (reinit) {
+        for (long i = 0; i < n; ++i) ls[i] = -ls[i];
+        fsweep3(ls, nx, ny, nz, dx, iters);
+        for (long i = 0; i < n; ++i) ls[i] = -ls[i];
+    }
+    fsweep3(ls, nx, ny, nz, dx, iters);
+}
+
 /* ------------------------------------------------------- fractional multigrid 3D ---- */
 /* cuWjFrac3D_n (cuWeightedJacobi3D.cu:620-695): Neumann walls, cut-cell face weights */
 static inline void frac_row3d(const double* v, const double* ax, const double* ay, const double* az,

@@ -75,6 +75,8 @@ int or_mgfrac3d_solve(double* p, const double* p0, const double* f, const double
 /* face open fractions of an arbitrary level set with 128 x 128 sub-face samples on cut faces
    (CuSolidLevelSet3D::GetFrac(ax, ay, az, ls, dim, dx), cuSolidLevelSet3D.cu:164-372) */
 void or_fractions3d_subsampled(double* ax, double* ay, double* az, const double* ls, int nx, int ny, int nz, double dx);
+/* eikonal redistancing (CuFastSweeping::Solve, reinit != 0: ReinitLevelSet), in place */
+void or_fast_sweep(double* ls, int nx, int ny, int nz, double dx, int iters, int reinit);
 /* coefficient truncation of a potential, in place (CuWaveletPotentialRecover3D::CutCoefficients,
    cuWaveletPotentialRecover3D.cu:123-239); 1 for a level outside [0, min log2 n] */
 int or_cut3d(double* qx, double* qy, double* qz, int nx, int ny, int nz, int level);

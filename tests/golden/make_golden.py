@@ -7,11 +7,12 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only index   # the index-sparse multigrid cases only
     python tests/golden/make_golden.py --only cut     # the coefficient truncation cases only
     python tests/golden/make_golden.py --only frac    # the sub-sampled face fraction cases only
+    python tests/golden/make_golden.py --only sweep   # the fast sweeping cases only
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
 (CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D::ProjectLocal_q_ccc,
 CuDivLocalProject::ProjectSingle, CuWaveletPotentialRecover3D/2D::Solve, CuMultigridFrac3D/2D::Solve,
-CuMultigridFrac3D::Solve_index, CuWaveletPotentialRecover3D::CutCoefficients, CuSolidLevelSet3D::GetFrac (static, sub-sampled),
+CuMultigridFrac3D::Solve_index, CuWaveletPotentialRecover3D::CutCoefficients, CuSolidLevelSet3D::GetFrac (static, sub-sampled), CuFastSweeping,
 CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P,
 CuSolidLevelSet3D) and stores inputs
 and reference outputs as ``<case>.npz``.  The CPU tests pin the FP64 oracle against these files;
@@ -140,6 +141,23 @@ def frac_cases(rng):
     save("frac3d_sub", **out)
 
 
+def sweep_cases(rng):
+    """CuFastSweeping::ReinitLevelSet on a squeezed, wavy sphere level set and CuFastSweeping::Solve
+    from fixed negative sources with every other cell at +5, both run past convergence (the
+    reference updates in place from concurrent threads, so only its fixed point is reproducible)."""
+    n = (24, 20, 16)
+    nx, ny, nz = n
+    h = 1.0 / nx
+    z, x, y = np.meshgrid((np.arange(nz) + 0.5) * h, (np.arange(nx) + 0.5) * h, (np.arange(ny) + 0.5) * h,
+                          indexing="ij")
+    sdf = np.sqrt((x - 0.5) ** 2 + (y - 0.45) ** 2 + (z - 0.4) ** 2) - 0.25
+    ls1 = (0.6 * sdf + 0.01 * np.sin(9 * x) * np.cos(7 * y)).astype(np.float32).astype(np.float64)
+    ls2 = np.where(sdf < 0, sdf, 5.0).astype(np.float32).astype(np.float64)
+    r1 = run("fsweep", {"ls": ls1}, [nx, ny, nz, h, 80, 1], {"ls": ls1.shape})["ls"]
+    r2 = run("fsweep", {"ls": ls2}, [nx, ny, nz, h, 80, 0], {"ls": ls2.shape})["ls"]
+    save("fsweep", n=np.array(n), h=h, iters=80, ls_reinit=ls1, out_reinit=r1, ls_solve=ls2, out_solve=r2)
+
+
 def main():
     if not os.path.exists(DRIVER):
         sys.exit(f"{DRIVER} missing: run make -C oracle/refharness first (needs nvcc and the reference sources)")
@@ -152,6 +170,9 @@ def main():
         return
     if only == "frac":
         frac_cases(np.random.default_rng(20261206))
+        return
+    if only == "sweep":
+        sweep_cases(np.random.default_rng(20261207))
         return
     rng = np.random.default_rng(20261203)
 
@@ -272,6 +293,7 @@ def main():
     index_cases(np.random.default_rng(20261204))
     cut_cases(np.random.default_rng(20261205))
     frac_cases(np.random.default_rng(20261206))
+    sweep_cases(np.random.default_rng(20261207))
 
 
 if __name__ == "__main__":

@@ -155,6 +155,17 @@ def test_subsampled_fractions_match_reference(oracle):
             assert d.max() <= 3.0 / 16384 and np.count_nonzero(d) <= 3, (tag, k, d.max(), np.count_nonzero(d))
 
 
+def test_fast_sweep_matches_reference_fixed_point(oracle):
+    """CuFastSweeping::ReinitLevelSet and Solve, past convergence: the oracle's Jacobi iterations
+    reach the reference's fixed point."""
+    g = load_golden("fsweep")
+    n = tuple(int(v) for v in g["n"])
+    for mode, reinit in (("reinit", True), ("solve", False)):
+        out = oracle.fast_sweep(g["ls_" + mode], n, float(g["h"]), int(g["iters"]), reinit)
+        ref = g["out_" + mode]
+        assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max(), (mode, np.abs(out - ref).max())
+
+
 def test_mg2d_matches_reference_per_cycle(oracle):
     p = load_golden("mg2d_32")
     n = tuple(int(v) for v in p["n"])

@@ -91,6 +91,8 @@ SIGNATURES = {
     "wp_sdf_spheres3d": (I, [P, I, I, I, D, P, P, I, P]),
     "wp_fractions3d": (I, [P, P, P, P, I, I, I, D, P]),
     "wp_fractions3d_subsampled": (I, [P, P, P, P, I, I, I, D, P]),
+    "wp_fast_sweep_solve": (I, [P, I, I, I, D, I, P]),
+    "wp_fast_sweep_reinit": (I, [P, I, I, I, D, I, P]),
     "wp_sdf_boxes3d": (I, [P, I, I, I, D, P, P, I, P]),
     "wp_sdf_circles2d": (I, [P, I, I, D, P, P, I, P]),
     "wp_fractions2d": (I, [P, P, P, I, I, D, P]),

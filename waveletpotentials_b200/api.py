@@ -441,6 +441,23 @@ class CuSolidLevelSet3D:
               "wp_sdf_boxes3d")
 
 
+class CuFastSweeping:
+    """CuFastSweeping (cuFastSweeping.cu): eikonal redistancing of a level set (torch CUDA float32,
+    shape (DZ, DX, DY)) in place."""
+
+    @staticmethod
+    def Solve(ls, dim, dx, n_iters, stream=None):
+        d = _dims3(dim)
+        check(lib().wp_fast_sweep_solve(_ptr(ls, (d[2], d[0], d[1])), *d, float(dx), int(n_iters), _stream(stream)),
+              "wp_fast_sweep_solve")
+
+    @staticmethod
+    def ReinitLevelSet(ls, dim, dx, n_iters, stream=None):
+        d = _dims3(dim)
+        check(lib().wp_fast_sweep_reinit(_ptr(ls, (d[2], d[0], d[1])), *d, float(dx), int(n_iters),
+                                         _stream(stream)), "wp_fast_sweep_reinit")
+
+
 class CuSolidLevelSet2D:
     """CuSolidLevelSet2D: circle level set (positive in fluid) and face open fractions."""
 

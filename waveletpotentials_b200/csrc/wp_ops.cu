@@ -9,6 +9,7 @@
 // All kernels map threadIdx.x to y (the contiguous index) so every access is coalesced.
 #include "wp_common.cuh"
 
+#include <algorithm>
 #include <map>
 
 #include <cstring>
@@ -539,6 +540,102 @@ extern "C" CUWHHD_API wp_status wp_fractions3d_subsampled(float* ax, float* ay, 
     cudaFreeAsync(buf, s);
     if (e != cudaSuccess) { wp_set_cuda_error(e, "subsampled fractions", __FILE__, __LINE__); return WP_ERR_CUDA; }
     return WP_OK;
+}
+
+// ------------------------------------------------------------ fast sweeping (eikonal)
+// CuFastSweeping::Solve / ReinitLevelSet (cuFastSweeping.cu:215-257, 383-396): a cell whose value
+// is above -1e-12 takes the upwind (Godunov) solution of |grad d| = 1 from the smaller neighbour of
+// each axis (solve_eikonal_nomin, :98-140; a missing neighbour counts 1e8); cells at or below
+// -1e-12 stay fixed and act as the sources.  The reference updates the array in place from
+// concurrently running threads, so its iterates depend on scheduling; here each iteration reads
+// the previous iterate and writes the other buffer (deterministic, one cell of propagation per
+// iteration), which reaches the same fixed point.
+namespace {
+__device__ double eikonal_upwind(double mx, double my, double mz, double h) {
+    double m[3] = {mx, my, mz};
+    for (int i = 1; i < 3; ++i)
+        for (int j = 0; j < 3 - i; ++j)
+            if (m[j] > m[j + 1]) { const double t = m[j]; m[j] = m[j + 1]; m[j + 1] = t; }
+    const double d2 = h * h;
+    double r = m[0] + h;
+    if (r > m[1]) {
+        const double s = sqrt(-m[0] * m[0] + 2 * m[0] * m[1] - m[1] * m[1] + d2 + d2);
+        r = (m[1] * d2 + m[0] * d2 + h * h * s) / (d2 + d2);
+        if (r > m[2]) {
+            const double a = sqrt(-m[0] * m[0] * d2 - m[0] * m[0] * d2 + 2 * m[0] * m[1] * d2 - m[1] * m[1] * d2 -
+                                  m[1] * m[1] * d2 + 2 * m[0] * m[2] * d2 - m[2] * m[2] * d2 - m[2] * m[2] * d2 +
+                                  2 * m[1] * m[2] * d2 + d2 * d2 + d2 * d2 + d2 * d2);
+            r = (m[2] * d2 * d2 + m[1] * d2 * d2 + m[0] * d2 * d2 + h * h * h * a) / (d2 * d2 + d2 * d2 + d2 * d2);
+        }
+    }
+    return r;
+}
+
+__global__ void fsweep_kernel(float* __restrict__ out, const float* __restrict__ in, int nx, int ny, int nz,
+                              double h) {
+    const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    const long sl = (long)nx * ny, i = y + (long)x * ny + z * sl;
+    const double c = in[i];
+    if (!(c > -1e-12)) { out[i] = (float)c; return; }
+    const double big = 1e8;
+    const double l = x > 0 ? in[i - ny] : big, r = x < nx - 1 ? in[i + ny] : big;
+    const double u = y < ny - 1 ? in[i + 1] : big, d = y > 0 ? in[i - 1] : big;
+    const double f = z > 0 ? in[i - sl] : big, b = z < nz - 1 ? in[i + sl] : big;
+    out[i] = (float)eikonal_upwind(fmin(l, r), fmin(u, d), fmin(f, b), h);
+}
+
+__global__ void negate_kernel(float* __restrict__ v, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v[i] = -v[i];
+}
+
+wp_status fsweep_iters(float* ls, float* tmp, int nx, int ny, int nz, double h, int iters, cudaStream_t s) {
+    const dim3 g(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz);
+    const double bytes = 8.0 * nx * ny * nz;
+    float* a = ls;
+    float* b = tmp;
+    for (int k = 0; k < iters; ++k) {
+        WP_KERNEL("fast_sweep", bytes, s, fsweep_kernel<<<g, dim3(32, 8), 0, s>>>(b, a, nx, ny, nz, h));
+        std::swap(a, b);
+    }
+    if (a != ls) WP_CUDA_TRY(cudaMemcpyAsync(ls, a, sizeof(float) * (size_t)nx * ny * nz, cudaMemcpyDeviceToDevice, s));
+    return WP_OK;
+}
+
+wp_status fsweep_entry(float* ls, int nx, int ny, int nz, double dx, int iters, bool reinit, cudaStream_t s) {
+    if (!ls || nx < 1 || ny < 1 || nz < 1 || nz > 65535 || !(dx > 0) || iters < 0) {
+        wp_set_error_msg("wp_fast_sweep: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    const long n = (long)nx * ny * nz;
+    float* tmp = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * n, s));
+    const unsigned gn = (unsigned)std::min<long>(wp_cdiv(n, 256), (long)wp_sm_count() * 16);
+    wp_status st = WP_OK;
+    auto neg = [&]() -> wp_status {
+        WP_KERNEL("negate", 8.0 * n, s, negate_kernel<<<gn, 256, 0, s>>>(ls, n));
+        return WP_OK;
+    };
+    if (reinit) {
+        if ((st = neg()) == WP_OK && (st = fsweep_iters(ls, tmp, nx, ny, nz, dx, iters, s)) == WP_OK &&
+            (st = neg()) == WP_OK)
+            st = fsweep_iters(ls, tmp, nx, ny, nz, dx, iters, s);
+    } else {
+        st = fsweep_iters(ls, tmp, nx, ny, nz, dx, iters, s);
+    }
+    cudaFreeAsync(tmp, s);
+    return st;
+}
+}  // namespace
+
+extern "C" CUWHHD_API wp_status wp_fast_sweep_solve(float* ls, int nx, int ny, int nz, double dx, int n_iters,
+                                                    void* stream) {
+    return fsweep_entry(ls, nx, ny, nz, dx, n_iters, false, (cudaStream_t)stream);
+}
+
+extern "C" CUWHHD_API wp_status wp_fast_sweep_reinit(float* ls, int nx, int ny, int nz, double dx, int n_iters,
+                                                     void* stream) {
+    return fsweep_entry(ls, nx, ny, nz, dx, n_iters, true, (cudaStream_t)stream);
 }
 
 extern "C" CUWHHD_API wp_status wp_sdf_boxes3d(float* sdf, int nx, int ny, int nz, double dx, const double* lo,
