@@ -633,9 +633,10 @@ def main():
                          "(ncu does not profile kernels inside graphs with conditional nodes)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "warmstart"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "warmstart", "index"],
                     help="single: one 256^3 projection per step; batch: 64 uneven grids in one graph per step; "
-                         "warmstart: train the U-Net, then projections with/without its guess")
+                         "warmstart: train the U-Net, then projections with/without its guess; index: four "
+                         "index-sparse V-cycles on a 15%%-fluid domain (profiling aid)")
     ap.add_argument("--ws-n", type=int, default=128)
     ap.add_argument("--ws-train", type=int, default=128)
     ap.add_argument("--ws-eval", type=int, default=8)
@@ -681,6 +682,32 @@ def main():
         print(json.dumps(out))
         return
 
+    if args.workload == "index" and args.impl == "ours":
+        # the index-sparse cycle alone on the mostly-solid domain of plain["index_sparse"]: one
+        # warm call, then one call of four V(2,2) cycles inside the profiler region (for ncu)
+        import torch
+        from waveletpotentials_b200 import api, fields as wf
+        nn = (args.n,) * 3
+        fl, fa, frng = wf.porous_domain(nn, 0.15, args.seed)
+        tff = torch.as_tensor(frng.standard_normal(fl.shape) * fl, dtype=torch.float32, device="cuda")
+        mgp = api.CuMultigridFrac3D(*(torch.as_tensor(x, dtype=torch.float32, device="cuda") for x in fa), nn,
+                                    1.0 / args.n)
+        dp = torch.zeros_like(tff)
+        mgp.Solve_index(dp, None, tff, 4, 2, 2, 0.8)
+        torch.cuda.synchronize()
+        if args.profile_region:
+            torch.cuda.cudart().cudaProfilerStart()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        mgp.Solve_index(dp, None, tff, 4, 2, 2, 0.8)
+        g1.record()
+        torch.cuda.synchronize()
+        if args.profile_region:
+            torch.cuda.cudart().cudaProfilerStop()
+        cells, segs = mgp.IndexSizes()
+        print(json.dumps({"workload": "index", "n": args.n, "fluid": float(fl.mean()), "listed_cells": cells,
+                          "segments": segs, "ms_per_cycle": g0.elapsed_time(g1) / 4}))
+        return
     if args.workload == "warmstart" and args.impl == "ours":
         if rank == 0:
             print(json.dumps(run_warmstart(args, rank, world, local_rank)))

@@ -3297,6 +3297,9 @@ wp_status vcycle_ix(wp_mgfrac3d* h, int l, const T* f, T* r, int nu1, T w, cudaS
                   wp_launch_pdl(restrict_ix_kernel<T>, gc, 256, 0, s, Bufs<T>::f(C), (const T*)r, view<T>(L), C.n[0],
                                 C.n[1], (const int4*)C.iseg, (long)C.iseg_n));
     if ((st = vcycle_ix<T>(h, l + 1, Bufs<T>::f(C), r, nu1, w, s)) != WP_OK) return st;
+    // a separate pass: folding the prolongation into the first post-sweep needs the neighbours'
+    // selection bits and parent values as dependent loads, which measured slower (117 against
+    // 25 + 51 us at 256^3, 15% fluid)
     if (gb > 0)
         WP_KERNEL(l == 0 ? "prolong_ix_finest" : "prolong_ix", lc * (3.0 * B) + 16.0 * ls, s,
                   wp_launch_pdl(prolong_ix_kernel<T>, gb, 256, 0, s, v, (const T*)Bufs<T>::v(C), view<T>(L), C.n[0],
