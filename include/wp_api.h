@@ -40,6 +40,7 @@ typedef enum wp_status {
 } wp_status;
 
 /* wavelet ids: same numeric values as the reference enum WaveletType (WaveletTypes.h:7-27) */
+#define WP_CDF3_5 2  /* same lifting structure as CDF3.7, 5-tap second update (wp_dwt1d only) */
 #define WP_CDF4_6 7
 #define WP_CDF3_7 11
 

@@ -36,6 +36,24 @@ static const double C4_SCL[2] = {2.0 * SQ2, -1.0 / (2.0 * SQ2)};
 static const double C4_SCL_INV[2] = {1.0 / (2.0 * SQ2), -(2.0 * SQ2)};
 
 /* base-level matrices, row-major: cuWaveletCompute.cuh:773-797 (CDF3.7), :846-874 (CDF4.6) */
+/* CDF3.5 (cuWaveletCompute.cuh:15 RSW_Q5_fu_2, :34-45 RSW_QN5_L10 / RSW_iQN5_L10, :60-71 RSW_QD5_L10 /
+   RSW_iQD5_L10); the first update, predict and scaling are CDF3.7's */
+static const double Q5_FU2[5] = {5. / 288, -34. / 288, 128. / 288, 34. / 288, -5. / 288};
+static const double QN5_L10[16] = {0.5, 0.5, 0.5, 0.5, -0.3828125, -0.234375, 0.234375, 0.3828125,
+                                   -0.353553390593274, 0.530330085889911, -0.176776695296637, 0,
+                                   0, 0.176776695296637, -0.530330085889911, 0.353553390593274};
+static const double IQN5_L10[16] = {0.5, -1.0, -1.038563084867742, 0.375650477505353,
+                                    0.5, -0.5, 1.248485410532498, -0.165728151840597,
+                                    0.5, 0.5, 0.165728151840597, -1.248485410532498,
+                                    0.5, 1.0, -0.375650477505353, 1.038563084867742};
+static const double QD5_L10[16] = {0.937499999999999, 1.53125, 1.53125, 0.9375, -1.0, -1.0, 1.0, 1.0,
+                                   -0.707106781186548, 0.530330085889911, -0.176776695296637, 0,
+                                   0, 0.176776695296637, -0.530330085889911, 0.707106781186548};
+static const double IQD5_L10[16] = {0.125, -0.25, -0.894932019939224, 0.187825238752677,
+                                    0.25, -0.25, 0.685009694274468, 0.02209708691208,
+                                    0.25, 0.25, -0.02209708691208, -0.685009694274468,
+                                    0.125, 0.25, -0.187825238752677, 0.894932019939224};
+#define IS_Q3(w) ((w) == OR_CDF3_7 || (w) == OR_CDF3_5)
 static const double QN7_L10[16] = {
     0.500000000000000, 0.500000000000000, 0.500000000000000, 0.500000000000000,
     -0.399902343750000, -0.200195312500000, 0.200195312500000, 0.399902343750000,
@@ -84,11 +102,15 @@ static const double ICD6_L10[25] = {
 /* 'z' is the Dirichlet-with-spacing alias: CDF3.7 treats it as 'd', CDF4.6 as 'n'
    (cuWHHDForward.cu:886-891, :970-975) */
 static char norm_bc(int wavelet, char bc) {
-    if (bc == 'z') return wavelet == OR_CDF3_7 ? 'd' : 'n';
+    if (bc == 'z') return IS_Q3(wavelet) ? 'd' : 'n';
     return bc;
 }
 
 static const double* base_matrix(int wavelet, char bc, int forward) {
+    if (wavelet == OR_CDF3_5) {
+        if (bc == 'n') return forward ? QN5_L10 : IQN5_L10;
+        return forward ? QD5_L10 : IQD5_L10;
+    }
     if (wavelet == OR_CDF3_7) {
         if (bc == 'n') return forward ? QN7_L10 : IQN7_L10;
         return forward ? QD7_L10 : IQD7_L10;
@@ -106,7 +128,7 @@ static const double* base_matrix(int wavelet, char bc, int forward) {
 static void fwd_reflect(int wavelet, char bc, int k, int L, int* ai, int* di, double* sa, double* sd) {
     int a = 2 * k, d = 2 * k + 1;
     double s_a = 1.0, s_d = 1.0;
-    if (wavelet == OR_CDF3_7) {
+    if (IS_Q3(wavelet)) {
         if (a < 0) { a = -1 - a; if (bc == 'd') s_a = -1.0; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bc == 'd') s_a = -1.0; }
         if (d < 0) { d = -1 - d; if (bc == 'd') s_d = -1.0; }
@@ -126,7 +148,7 @@ static void fwd_reflect(int wavelet, char bc, int k, int L, int* ai, int* di, do
 static void inv_reflect(int wavelet, char bc, int k, int L, int* ai, int* di, double* sa, double* sd) {
     int a = k, d = k;
     double s_a = 1.0, s_d = 1.0;
-    if (wavelet == OR_CDF3_7) {
+    if (IS_Q3(wavelet)) {
         if (a < 0) { a = -1 - a; if (bc == 'n') s_d = -1.0; else s_a = -1.0; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bc == 'n') s_d = -1.0; else s_a = -1.0; }
         d = a;
@@ -161,13 +183,15 @@ static void fwd_level(const double* x, int L, int ext, int wavelet, char bc, dou
         D0[IX(k)] = (di >= 0 && di < n_in) ? sd * x[di] : 0.0;
     }
     for (int k = K0; k < K1; ++k) { A1[IX(k)] = 0.0; D1[IX(k)] = 0.0; }
-    if (wavelet == OR_CDF3_7) {
+    if (IS_Q3(wavelet)) {
+        const double* fu2 = wavelet == OR_CDF3_5 ? Q5_FU2 : Q7_FU2;
+        const int hw = wavelet == OR_CDF3_5 ? 2 : 3;
         for (int k = K0 + 1; k < K1; ++k) A1[IX(k)] = A0[IX(k)] + Q5_FU1 * D0[IX(k - 1)];
         for (int k = K0 + 1; k < K1 - 1; ++k)
             D1[IX(k)] = D0[IX(k)] + Q5_FP[0] * A1[IX(k + 1)] + Q5_FP[1] * A1[IX(k)];
         for (int k = 0; k < M; ++k) {
             double s = A1[IX(k)];
-            for (int t = -3; t <= 3; ++t) s += Q7_FU2[3 - t] * D1[IX(k + t)];
+            for (int t = -hw; t <= hw; ++t) s += fu2[hw - t] * D1[IX(k + t)];
             a_out[k] = s * Q5_SCL[0];
         }
         for (int k = 0; k < L / 2; ++k) d_out[k] = D1[IX(k)] * Q5_SCL[1];
@@ -207,14 +231,16 @@ static void inv_level(const double* a, const double* d, int L, int ext, int wave
         D[IX(k)] = (di >= 0 && di < L) ? d[di] : 0.0;
         SA[IX(k)] = sa; SD[IX(k)] = sd;
     }
-    if (wavelet == OR_CDF3_7) {
+    if (IS_Q3(wavelet)) {
+        const double* fu2 = wavelet == OR_CDF3_5 ? Q5_FU2 : Q7_FU2;
+        const int hw = wavelet == OR_CDF3_5 ? 2 : 3;
         for (int k = K0; k < K1; ++k) {
             A[IX(k)] = SA[IX(k)] * A[IX(k)] * Q5_SCL[1];
             D[IX(k)] = SD[IX(k)] * D[IX(k)] * Q5_SCL[0];
         }
         for (int k = K0 + 3; k < K1 - 3; ++k) {
             double s = 0.0;
-            for (int t = -3; t <= 3; ++t) s += Q7_FU2[3 - t] * D[IX(k + t)];
+            for (int t = -hw; t <= hw; ++t) s += fu2[hw - t] * D[IX(k + t)];
             T[IX(k)] = A[IX(k)] - s;
         }
         for (int k = K0 + 3; k < K1 - 4; ++k) D[IX(k)] = D[IX(k)] - (Q5_FP[1] * T[IX(k)] + Q5_FP[0] * T[IX(k + 1)]);
@@ -241,7 +267,7 @@ static void inv_level(const double* a, const double* d, int L, int ext, int wave
 
 /* ----------------------------------------------------------------- full 1D line ---- */
 int or_dwt_line(double* line, int n, int levels, int wavelet, char bc, int forward) {
-    if (wavelet != OR_CDF3_7 && wavelet != OR_CDF4_6) return 2;
+    if (!IS_Q3(wavelet) && wavelet != OR_CDF4_6) return 2;
     bc = norm_bc(wavelet, bc);
     if (bc != 'n' && bc != 'd') return 2;
     int ext = n & 1;

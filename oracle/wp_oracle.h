@@ -19,6 +19,7 @@ extern "C" {
 #endif
 
 /* wavelet identifiers: same numeric values as the reference enum (WaveletTypes.h:7-27) */
+#define OR_CDF3_5 2
 #define OR_CDF4_6 7
 #define OR_CDF3_7 11
 

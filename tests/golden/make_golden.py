@@ -8,6 +8,7 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only cut     # the coefficient truncation cases only
     python tests/golden/make_golden.py --only frac    # the sub-sampled face fraction cases only
     python tests/golden/make_golden.py --only sweep   # the fast sweeping cases only
+    python tests/golden/make_golden.py --only cdf35   # the CDF3.5 transforms only
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
 (CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D::ProjectLocal_q_ccc,
@@ -33,7 +34,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 from waveletpotentials_b200.fields import porous_fractions  # noqa: E402
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
-CDF4_6, CDF3_7 = 7, 11
+CDF3_5, CDF4_6, CDF3_7 = 2, 7, 11
 
 
 def run(op, inputs: dict, params, outputs: dict):
@@ -158,6 +159,32 @@ def sweep_cases(rng):
     save("fsweep", n=np.array(n), h=h, iters=80, ls_reinit=ls1, out_reinit=r1, ls_solve=ls2, out_solve=r2)
 
 
+def cdf35_cases(rng):
+    """CuWHHDForward::Solve1D with CDF3.5 (another wavelet family of the same lifting structure):
+    every axis, both boundary types, both directions, and a 256-point line."""
+    dwt = {}
+    for bc in "nd":
+        for fwd in (1, 0):
+            for axis, (L, other) in {"y": (4, (3, 2)), "x": (5, (4, 3)), "z": (3, (5, 2))}.items():
+                n = 1 << L
+                DX, DY, DZ = {"y": (other[0], n, other[1]), "x": (n, other[0], other[1]),
+                              "z": (other[0], other[1], n)}[axis]
+                a = rng.standard_normal((DZ, DX, DY))
+                out = run("dwt1d", {"a": a}, [DX, DY, DZ, L, axis, bc, CDF3_5, fwd], {"c": (DZ, DX, DY)})
+                key = f"w{CDF3_5}_{bc}_{'f' if fwd else 'i'}_{axis}"
+                dwt[key + "_in"] = a
+                dwt[key + "_out"] = out["c"]
+                dwt[key + "_meta"] = np.array([DX, DY, DZ, L, ord(axis), ord(bc), CDF3_5, fwd])
+        for fwd in (1, 0):
+            a = rng.standard_normal((1, 2, 256))
+            out = run("dwt1d", {"a": a}, [2, 256, 1, 8, "y", bc, CDF3_5, fwd], {"c": (1, 2, 256)})
+            key = f"w{CDF3_5}_{bc}_{'f' if fwd else 'i'}_long"
+            dwt[key + "_in"] = a
+            dwt[key + "_out"] = out["c"]
+            dwt[key + "_meta"] = np.array([2, 256, 1, 8, ord("y"), ord(bc), CDF3_5, fwd])
+    save("dwt1d_cdf35", **dwt)
+
+
 def main():
     if not os.path.exists(DRIVER):
         sys.exit(f"{DRIVER} missing: run make -C oracle/refharness first (needs nvcc and the reference sources)")
@@ -173,6 +200,9 @@ def main():
         return
     if only == "sweep":
         sweep_cases(np.random.default_rng(20261207))
+        return
+    if only == "cdf35":
+        cdf35_cases(np.random.default_rng(20261208))
         return
     rng = np.random.default_rng(20261203)
 
@@ -294,6 +324,7 @@ def main():
     cut_cases(np.random.default_rng(20261205))
     frac_cases(np.random.default_rng(20261206))
     sweep_cases(np.random.default_rng(20261207))
+    cdf35_cases(np.random.default_rng(20261208))
 
 
 if __name__ == "__main__":

@@ -37,7 +37,7 @@ def test_dwt_rejects_bad_shapes(L):
     assert "2^levels" in _lib.last_error()
     assert L.wp_dwt1d(dummy, dummy, 16, 4, 4, 4, _c("w"), _c("n"), _lib.CDF3_7, 1, None) == 1
     assert L.wp_dwt1d(dummy, dummy, 16, 4, 4, 4, _c("x"), _c("q"), _lib.CDF3_7, 1, None) == 1
-    assert L.wp_dwt1d(dummy, dummy, 16, 4, 4, 4, _c("x"), _c("n"), 3, 1, None) == 2  # CDF3.5: other family
+    assert L.wp_dwt1d(dummy, dummy, 16, 4, 4, 4, _c("x"), _c("n"), 3, 1, None) == 2  # CDF2.10: another family
     assert L.wp_dwt1d(None, None, 16, 4, 4, 4, _c("x"), _c("n"), _lib.CDF3_7, 1, None) == 1
 
 

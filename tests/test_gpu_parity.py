@@ -26,8 +26,9 @@ def rel(ref, got):
     return float(np.sqrt(np.sum((ref - got) ** 2) / max(np.sum(ref * ref), 1e-300)))
 
 
-def test_dwt1d_fp32_and_fp64_match_reference(wp):
-    d = load_golden("dwt1d")
+@pytest.mark.parametrize("name", ["dwt1d", "dwt1d_cdf35"])
+def test_dwt1d_fp32_and_fp64_match_reference(wp, name):
+    d = load_golden(name)
     cases = [k[:-5] for k in d.files if k.endswith("_meta")]
     for b in cases:
         DX, DY, DZ, L, ax, bc, wav, fwd = (int(v) for v in d[b + "_meta"])

@@ -6,7 +6,7 @@ import pytest
 from waveletpotentials_b200 import fields
 
 
-@pytest.mark.parametrize("wav,ext", [(11, 0), (7, 1)])
+@pytest.mark.parametrize("wav,ext", [(11, 0), (7, 1), (2, 0)])
 @pytest.mark.parametrize("bc", ["n", "d"])
 @pytest.mark.parametrize("levels", [2, 3, 5, 8])
 def test_perfect_reconstruction(oracle, wav, ext, bc, levels):

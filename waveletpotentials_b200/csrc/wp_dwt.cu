@@ -40,6 +40,18 @@ struct K37 {
                             q6 = 0.003797743055556;
     static constexpr double scl0 = 3.0 / 1.414213562373095048801, scl1 = 1.414213562373095048801 / 3.0;
 };
+// CDF3.5 (cuWaveletCompute.cuh:15 RSW_Q5_fu_2): CDF3.7's first update, predict and scaling with a
+// 5-tap second update, written in CDF3.7's 7-tap form with zero outer taps
+struct K35 : K37 {
+    // q_i weighs the detail at offset 3 - i (RSW_Q5_fu_2[j] weighs offset 2 - j)
+    static constexpr double q0 = 0.0, q1 = 5.0 / 288, q2 = -34.0 / 288, q3 = 128.0 / 288, q4 = 34.0 / 288,
+                            q5 = -5.0 / 288, q6 = 0.0;
+};
+template <int WAV>
+struct K3 : K37 {};
+template <>
+struct K3<WP_ID_CDF3_5> : K35 {};
+__host__ __device__ constexpr bool is_q3(int w) { return w == WP_ID_CDF3_7 || w == WP_ID_CDF3_5; }
 struct K46 {
     static constexpr double fu1_0 = -0.25, fu1_1 = -0.25;
     static constexpr double fp0 = -1.0, fp1 = -1.0;
@@ -51,6 +63,7 @@ struct K46 {
 
 // base-level matrices, row-major, in this order: 37n, 37d, 46n, 46d (forward), then inverses
 __constant__ double c_base37[4][16];
+__constant__ double c_base35[4][16];
 __constant__ double c_base46[4][25];
 
 const double h_base37[4][16] = {
@@ -68,6 +81,16 @@ const double h_base37[4][16] = {
      -0.250000000000000, 0.636672316654294, 0.070434464532254, 0.250000000000000, 0.250000000000000,
      -0.070434464532254, -0.636672316654294, 0.125000000000000, 0.250000000000000, -0.211993927562764,
      0.919100708749311}};
+// CDF3.5 base-level matrices (cuWaveletCompute.cuh:34-45, 60-71): forward n, forward d, inverse n, inverse d
+const double h_base35[4][16] = {
+    {0.5, 0.5, 0.5, 0.5, -0.3828125, -0.234375, 0.234375, 0.3828125, -0.353553390593274, 0.530330085889911,
+     -0.176776695296637, 0, 0, 0.176776695296637, -0.530330085889911, 0.353553390593274},
+    {0.937499999999999, 1.53125, 1.53125, 0.9375, -1.0, -1.0, 1.0, 1.0, -0.707106781186548, 0.530330085889911,
+     -0.176776695296637, 0, 0, 0.176776695296637, -0.530330085889911, 0.707106781186548},
+    {0.5, -1.0, -1.038563084867742, 0.375650477505353, 0.5, -0.5, 1.248485410532498, -0.165728151840597, 0.5, 0.5,
+     0.165728151840597, -1.248485410532498, 0.5, 1.0, -0.375650477505353, 1.038563084867742},
+    {0.125, -0.25, -0.894932019939224, 0.187825238752677, 0.25, -0.25, 0.685009694274468, 0.02209708691208, 0.25,
+     0.25, -0.02209708691208, -0.685009694274468, 0.125, 0.25, -0.187825238752677, 0.894932019939224}};
 const double h_base46[4][25] = {
     {1.851562500000001, 2.097656250000000, 0.500000000000000, -1.097656250000000, -1.351562500000000,
      -1.351562500000000, -1.097656250000000, 0.500000000000000, 2.097656250000000, 1.851562500000001,
@@ -93,7 +116,7 @@ template <int WAV>
 __device__ __forceinline__ void fwd_reflect(int k, int L, int bcd, int& ai, int& di, float& sa, float& sd) {
     int a = 2 * k, d = 2 * k + 1;
     float s_a = 1.f, s_d = 1.f;
-    if (WAV == WP_ID_CDF3_7) {
+    if (is_q3(WAV)) {
         if (a < 0) { a = -1 - a; if (bcd) s_a = -1.f; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bcd) s_a = -1.f; }
         if (d < 0) { d = -1 - d; if (bcd) s_d = -1.f; }
@@ -112,7 +135,7 @@ template <int WAV>
 __device__ __forceinline__ void inv_reflect(int k, int L, int bcd, int& ai, int& di, float& sa, float& sd) {
     int a = k, d = k;
     float s_a = 1.f, s_d = 1.f;
-    if (WAV == WP_ID_CDF3_7) {
+    if (is_q3(WAV)) {
         if (a < 0) { a = -1 - a; if (bcd) s_a = -1.f; else s_d = -1.f; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bcd) s_a = -1.f; else s_d = -1.f; }
         d = a;
@@ -264,7 +287,7 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                         Dd[w] = T(__int_as_float(e.w)) * S[e.y * CP + col];
                     }
                 }
-                if (WAV == WP_ID_CDF3_7) {
+                if (is_q3(WAV)) {
 #pragma unroll
                     for (int w = WIN - 1; w >= 1; --w) A[w] = A[w] + T(K37::fu1) * Dd[w - 1];
 #pragma unroll
@@ -272,9 +295,9 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
 #pragma unroll
                     for (int j = 0; j < CH; ++j) {
                         const int w = j + 4;
-                        T s = A[w] + T(K37::q6) * Dd[w - 3] + T(K37::q5) * Dd[w - 2] + T(K37::q4) * Dd[w - 1] +
-                              T(K37::q3) * Dd[w] + T(K37::q2) * Dd[w + 1] + T(K37::q1) * Dd[w + 2] +
-                              T(K37::q0) * Dd[w + 3];
+                        T s = A[w] + T(K3<WAV>::q6) * Dd[w - 3] + T(K3<WAV>::q5) * Dd[w - 2] + T(K3<WAV>::q4) * Dd[w - 1] +
+                              T(K3<WAV>::q3) * Dd[w] + T(K3<WAV>::q2) * Dd[w + 1] + T(K3<WAV>::q1) * Dd[w + 2] +
+                              T(K3<WAV>::q0) * Dd[w + 3];
                         const int k = k0 + j;
                         if (k < M) D[k * CP + col] = s * T(K37::scl0);
                         if (k < nd) D[(M + k) * CP + col] = Dd[w] * T(K37::scl1);
@@ -300,7 +323,7 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
             cur ^= 1;
         }
         // base level: nb x nb matrix on the remaining approximation coefficients
-        const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[bcd] : c_base46[bcd];
+        const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[bcd] : (WAV == WP_ID_CDF3_5 ? c_base35[bcd] : c_base46[bcd]);
         if (tid < C) {
             T a[5], o[5];
             for (int i = 0; i < nb; ++i) a[i] = buf[cur][i * CP + tid];
@@ -314,7 +337,8 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
         __syncthreads();
         outbuf = -1;  // position dependent, resolved below
     } else {
-        const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[2 + bcd] : c_base46[2 + bcd];
+        const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[2 + bcd]
+                                                  : (WAV == WP_ID_CDF3_5 ? c_base35[2 + bcd] : c_base46[2 + bcd]);
         if (tid < C) {
             T a[5], o[5];
             for (int i = 0; i < nb; ++i) a[i] = buf[0][i * CP + tid];
@@ -359,7 +383,7 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                         SD[w] = T(__int_as_float(e.w));
                     }
                 }
-                if (WAV == WP_ID_CDF3_7) {
+                if (is_q3(WAV)) {
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) {
                         A[w] = SA[w] * A[w] * T(K37::scl1);
@@ -367,9 +391,9 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                     }
 #pragma unroll
                     for (int w = 3; w < WIN - 3; ++w)
-                        A[w] = A[w] - (T(K37::q6) * Dd[w - 3] + T(K37::q5) * Dd[w - 2] + T(K37::q4) * Dd[w - 1] +
-                                       T(K37::q3) * Dd[w] + T(K37::q2) * Dd[w + 1] + T(K37::q1) * Dd[w + 2] +
-                                       T(K37::q0) * Dd[w + 3]);
+                        A[w] = A[w] - (T(K3<WAV>::q6) * Dd[w - 3] + T(K3<WAV>::q5) * Dd[w - 2] + T(K3<WAV>::q4) * Dd[w - 1] +
+                                       T(K3<WAV>::q3) * Dd[w] + T(K3<WAV>::q2) * Dd[w + 1] + T(K3<WAV>::q1) * Dd[w + 2] +
+                                       T(K3<WAV>::q0) * Dd[w + 3]);
 #pragma unroll
                     for (int w = 3; w < WIN - 4; ++w) Dd[w] = Dd[w] - (T(K37::fp1) * A[w] + T(K37::fp0) * A[w + 1]);
 #pragma unroll
@@ -452,6 +476,8 @@ cudaError_t ensure_constants() {
     if (e != cudaSuccess) return e;
     e = cudaMemcpyToSymbol(c_base46, b46, sizeof(b46));
     if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_base35, h_base35, sizeof(h_base35));
+    if (e != cudaSuccess) return e;
     if (dev < 64) g_const_ready[dev] = true;
     return cudaSuccess;
 }
@@ -527,8 +553,8 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
                              char bc, int forward, cudaStream_t stream) {
     if (!dst || DX <= 0 || DY <= 0 || DZ <= 0) { wp_set_error_msg("wp_dwt1d: bad arguments"); return WP_ERR_INVALID_ARG; }
     if (!src) src = dst;
-    if (wavelet != WP_ID_CDF3_7 && wavelet != WP_ID_CDF4_6) { wp_set_error_msg("wp_dwt1d: wavelet must be CDF3.7 or CDF4.6"); return WP_ERR_UNSUPPORTED; }
-    if (bc == 'z') bc = (wavelet == WP_ID_CDF3_7) ? 'd' : 'n';  // cuWHHDForward.cu:886-891, :970-975
+    if (!is_q3(wavelet) && wavelet != WP_ID_CDF4_6) { wp_set_error_msg("wp_dwt1d: wavelet must be CDF3.7, CDF3.5 or CDF4.6"); return WP_ERR_UNSUPPORTED; }
+    if (bc == 'z') bc = is_q3(wavelet) ? 'd' : 'n';  // cuWHHDForward.cu:760-765, 886-891, 970-975
     if (bc != 'n' && bc != 'd') { wp_set_error_msg("wp_dwt1d: bc must be 'n', 'd' or 'z'"); return WP_ERR_INVALID_ARG; }
     TileGeom g;
     int N, nouter;
@@ -550,6 +576,9 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
     if (wavelet == WP_ID_CDF3_7)
         e = forward ? launch_c<WP_ID_CDF3_7, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
                     : launch_c<WP_ID_CDF3_7, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    else if (wavelet == WP_ID_CDF3_5)
+        e = forward ? launch_c<WP_ID_CDF3_5, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF3_5, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
     else
         e = forward ? launch_c<WP_ID_CDF4_6, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
                     : launch_c<WP_ID_CDF4_6, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
@@ -602,7 +631,7 @@ wp_status wp_dwt_axis_tune(T* buf, int DX, int DY, int DZ, int levels, char axis
         case 'x': case 'X': g.ni = DY; nouter = DZ; g.contiguous = 0; break;
         default: g.ni = DY; nouter = DX; g.contiguous = 0; break;
     }
-    const int wav = wavelet == WP_ID_CDF3_7 ? WP_ID_CDF3_7 : WP_ID_CDF4_6;
+    const int wav = is_q3(wavelet) ? wavelet : WP_ID_CDF4_6;
     std::lock_guard<std::mutex> lk(g_c_mu);
     g_c_cache[c_key(wav, forward != 0, (int)sizeof(T), N, g, nouter)] = best_c;
     return WP_OK;
