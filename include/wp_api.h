@@ -282,6 +282,14 @@ CUWHHD_API wp_status wp_fractions3d_subsampled(float* ax, float* ay, float* az, 
    one cell of propagation per iteration, the same fixed point. */
 CUWHHD_API wp_status wp_fast_sweep_solve(float* ls, int nx, int ny, int nz, double dx, int n_iters, void* stream);
 CUWHHD_API wp_status wp_fast_sweep_reinit(float* ls, int nx, int ny, int nz, double dx, int n_iters, void* stream);
+/* Replaces CuFastSweeping::ParticlesToLs(ls, x, dim, n_pars, dx, radius, max_dis, n_iters)
+   (cuFastSweeping.cu:259-349): a level set (negative inside) of balls of `radius` around `count`
+   particles (xyz: device array of count x 3 floats, positions in the domain's units): rough
+   distances at the 8 cells around each particle, then two sign flips each followed by n_iters
+   eikonal sweeps (wp_fast_sweep_solve), then negation.  Cells outside the grid are skipped (the
+   reference writes them). */
+CUWHHD_API wp_status wp_particles_to_ls(float* ls, const float* xyz, int count, int nx, int ny, int nz, double dx,
+                                        double radius, double max_dis, int n_iters, void* stream);
 /* 2D: circle level set (CuSolidLevelSet2D, cuSolidLevelSet2D.cu) and face fractions. */
 CUWHHD_API wp_status wp_sdf_circles2d(float* sdf, int nx, int ny, double dx, const double* centers, const double* radii,
                                       int count, void* stream);

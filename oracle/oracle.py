@@ -65,6 +65,7 @@ def lib():
             "or_mgfrac3d_solve_index": (i, [p, p, p, p, p, p, i, i, i, d, d, d, i, i, i, d, p, p]),
             "or_cut3d": (i, [p, p, p, i, i, i, i]),
             "or_fast_sweep": (None, [p, i, i, i, d, i, i]),
+            "or_particles_to_ls": (None, [p, p, i, i, i, i, d, d, d, i]),
             "or_fractions3d_subsampled": (None, [p, p, p, p, i, i, i, d]),
             "or_mgfrac2d_solve": (i, [p, p, p, p, p, i, i, d, d, i, i, i, d, i, p]),
             "or_frac_residual3d": (d, [p, p, p, p, p, p, i, i, i, d, d, d]),
@@ -255,6 +256,15 @@ def fast_sweep(ls, n, dx, iters, reinit=False):
     """CuFastSweeping::Solve (reinit=False) / ReinitLevelSet (True) as Jacobi iterations."""
     out = np.array(_f64(ls))
     lib().or_fast_sweep(_p(out), *n, dx, iters, int(bool(reinit)))
+    return out
+
+
+def particles_to_ls(xyz, n, dx, radius, max_dis, iters):
+    """CuFastSweeping::ParticlesToLs; xyz (count, 3) positions; returns the level set (DZ, DX, DY)."""
+    nx, ny, nz = n
+    out = np.zeros((nz, nx, ny))
+    pts = _f64(np.reshape(xyz, (-1, 3)))
+    lib().or_particles_to_ls(_p(out), _p(pts), pts.shape[0], nx, ny, nz, dx, radius, max_dis, iters)
     return out
 
 

@@ -78,6 +78,9 @@ int or_mgfrac3d_solve(double* p, const double* p0, const double* f, const double
 void or_fractions3d_subsampled(double* ax, double* ay, double* az, const double* ls, int nx, int ny, int nz, double dx);
 /* eikonal redistancing (CuFastSweeping::Solve, reinit != 0: ReinitLevelSet), in place */
 void or_fast_sweep(double* ls, int nx, int ny, int nz, double dx, int iters, int reinit);
+/* particles to a level set (CuFastSweeping::ParticlesToLs), xyz: count x 3 positions */
+void or_particles_to_ls(double* ls, const double* xyz, int count, int nx, int ny, int nz, double dx, double radius,
+                        double max_dis, int iters);
 /* coefficient truncation of a potential, in place (CuWaveletPotentialRecover3D::CutCoefficients,
    cuWaveletPotentialRecover3D.cu:123-239); 1 for a level outside [0, min log2 n] */
 int or_cut3d(double* qx, double* qy, double* qz, int nx, int ny, int nz, int level);

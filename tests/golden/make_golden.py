@@ -13,7 +13,7 @@ unmodified reference sources (FP64, the reference default):
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
 (CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D::ProjectLocal_q_ccc,
 CuDivLocalProject::ProjectSingle, CuWaveletPotentialRecover3D/2D::Solve, CuMultigridFrac3D/2D::Solve,
-CuMultigridFrac3D::Solve_index, CuWaveletPotentialRecover3D::CutCoefficients, CuSolidLevelSet3D::GetFrac (static, sub-sampled), CuFastSweeping,
+CuMultigridFrac3D::Solve_index, CuWaveletPotentialRecover3D::CutCoefficients, CuSolidLevelSet3D::GetFrac (static, sub-sampled), CuFastSweeping (incl. ParticlesToLs),
 CuConvergence::GetB_3d_frac_vel, CuGradient::Gradient3D_Frac_P,
 CuSolidLevelSet3D) and stores inputs
 and reference outputs as ``<case>.npz``.  The CPU tests pin the FP64 oracle against these files;
@@ -156,7 +156,14 @@ def sweep_cases(rng):
     ls2 = np.where(sdf < 0, sdf, 5.0).astype(np.float32).astype(np.float64)
     r1 = run("fsweep", {"ls": ls1}, [nx, ny, nz, h, 80, 1], {"ls": ls1.shape})["ls"]
     r2 = run("fsweep", {"ls": ls2}, [nx, ny, nz, h, 80, 0], {"ls": ls2.shape})["ls"]
-    save("fsweep", n=np.array(n), h=h, iters=80, ls_reinit=ls1, out_reinit=r1, ls_solve=ls2, out_solve=r2)
+    # CuFastSweeping::ParticlesToLs: a blob of particles well inside the box (the reference does not
+    # bound-check the cells around a particle)
+    pts = (np.array([0.5, 0.45, 0.5]) + 0.12 * rng.standard_normal((60, 3))).clip(0.2, 0.8)
+    pts = pts * np.array([nx, ny, nz]) * h
+    pts = pts.astype(np.float32).astype(np.float64)
+    r3 = run("p2ls", {"xyz": pts}, [nx, ny, nz, h, 0.6 * h, 1.0, 80, len(pts)], {"ls": ls1.shape})["ls"]
+    save("fsweep", n=np.array(n), h=h, iters=80, ls_reinit=ls1, out_reinit=r1, ls_solve=ls2, out_solve=r2,
+         particles=pts, radius=0.6 * h, max_dis=1.0, out_particles=r3)
 
 
 def cdf35_cases(rng):

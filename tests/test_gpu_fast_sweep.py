@@ -35,3 +35,16 @@ def test_fast_sweep_iterates_match_oracle(wp, oracle, iters):
     # FP32 storage between iterations: at most one rounding per iteration, not amplified (the update
     # is monotone and non-expansive)
     assert np.abs(N(t) - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def test_particles_to_ls_matches_reference_fixed_point(wp):
+    g = load_golden("fsweep")
+    n = tuple(int(v) for v in g["n"])
+    ls = torch.empty((n[2], n[0], n[1]), device="cuda")
+    x = T(g["particles"])
+    wp.CuFastSweeping.ParticlesToLs(ls, x, n, float(g["h"]), float(g["radius"]), float(g["max_dis"]),
+                                    int(g["iters"]))
+    torch.cuda.synchronize()
+    ref = g["out_particles"]
+    assert np.abs(N(ls) - ref).max() <= 1e-5 * np.abs(ref).max()
+    assert np.array_equal(N(ls) > 0, ref > 0)

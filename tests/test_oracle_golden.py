@@ -165,6 +165,10 @@ def test_fast_sweep_matches_reference_fixed_point(oracle):
         out = oracle.fast_sweep(g["ls_" + mode], n, float(g["h"]), int(g["iters"]), reinit)
         ref = g["out_" + mode]
         assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max(), (mode, np.abs(out - ref).max())
+    out = oracle.particles_to_ls(g["particles"], n, float(g["h"]), float(g["radius"]), float(g["max_dis"]),
+                                 int(g["iters"]))
+    ref = g["out_particles"]
+    assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max(), np.abs(out - ref).max()
 
 
 def test_mg2d_matches_reference_per_cycle(oracle):

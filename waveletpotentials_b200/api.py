@@ -458,6 +458,19 @@ class CuFastSweeping:
                                          _stream(stream)), "wp_fast_sweep_reinit")
 
 
+def ParticlesToLs(ls, x, dim, dx, radius, max_dis, n_iters, stream=None):
+    """CuFastSweeping::ParticlesToLs: ls (CUDA float32 (DZ, DX, DY)) from particle positions x (CUDA
+    float32 (count, 3))."""
+    d = _dims3(dim)
+    count = int(x.shape[0])
+    check(lib().wp_particles_to_ls(_ptr(ls, (d[2], d[0], d[1])), _ptr(x, (count, 3)), count, *d, float(dx),
+                                   float(radius), float(max_dis), int(n_iters), _stream(stream)),
+          "wp_particles_to_ls")
+
+
+CuFastSweeping.ParticlesToLs = staticmethod(ParticlesToLs)
+
+
 class CuSolidLevelSet2D:
     """CuSolidLevelSet2D: circle level set (positive in fluid) and face open fractions."""
 

@@ -628,6 +628,79 @@ wp_status fsweep_entry(float* ls, int nx, int ny, int nz, double dx, int iters, 
 }
 }  // namespace
 
+// CuFastSweeping::ParticlesToLs (cuFastSweeping.cu:259-349): every cell starts at dx; each particle
+// lowers the 8 cells around it to (distance to the particle) - radius (a float minimum, order
+// independent); then the sign is flipped outside / the inside set to max_dis, swept, flipped back
+// and swept again, and the result negated.  Cells the reference would index outside the grid (a
+// particle within half a cell of a wall) are skipped here.
+namespace {
+__device__ __forceinline__ void atomic_min_float(float* a, float v) {
+    if (v >= 0.f) atomicMin(reinterpret_cast<int*>(a), __float_as_int(v));
+    else atomicMax(reinterpret_cast<unsigned*>(a), __float_as_uint(v));
+}
+
+__global__ void particles_rough_kernel(float* __restrict__ ls, const float* __restrict__ xyz, int count, int nx,
+                                       int ny, int nz, double dx, double radius) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    const double inv = 1.0 / dx;
+    const double x = xyz[3 * p] * inv - 0.5, y = xyz[3 * p + 1] * inv - 0.5, z = xyz[3 * p + 2] * inv - 0.5;
+    const int ix = (int)floor(x), iy = (int)floor(y), iz = (int)floor(z);
+    const double fx = x - ix, fy = y - iy, fz = z - iz;
+    const double wx[2] = {fx * fx, (1.0 - fx) * (1.0 - fx)}, wy[2] = {fy * fy, (1.0 - fy) * (1.0 - fy)};
+    const double wz[2] = {fz * fz, (1.0 - fz) * (1.0 - fz)};
+    for (int k = 0; k < 2; ++k)
+        for (int j = 0; j < 2; ++j)
+            for (int i = 0; i < 2; ++i) {
+                const int cx = ix + j, cy = iy + i, cz = iz + k;
+                if (cx < 0 || cx >= nx || cy < 0 || cy >= ny || cz < 0 || cz >= nz) continue;
+                const double d = sqrt(wx[j] + wy[i] + wz[k]) * dx - radius;
+                atomic_min_float(ls + cy + (long)cx * ny + (long)cz * nx * ny, (float)d);
+            }
+}
+
+__global__ void fill_kernel(float* __restrict__ v, long n, float val) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v[i] = val;
+}
+
+// cuInvLevelSet (cuFastSweeping.cu:302-317): outside (> 0) negated, the rest set to max_dis
+__global__ void inv_ls_kernel(float* __restrict__ v, long n, float max_dis) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        v[i] = v[i] > 0.f ? -v[i] : max_dis;
+}
+}  // namespace
+
+extern "C" CUWHHD_API wp_status wp_particles_to_ls(float* ls, const float* xyz, int count, int nx, int ny, int nz,
+                                                   double dx, double radius, double max_dis, int n_iters,
+                                                   void* stream) {
+    if (!ls || (count > 0 && !xyz) || count < 0 || nx < 1 || ny < 1 || nz < 1 || nz > 65535 || !(dx > 0) ||
+        n_iters < 0) {
+        wp_set_error_msg("wp_particles_to_ls: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const long n = (long)nx * ny * nz;
+    const unsigned gn = (unsigned)std::min<long>(wp_cdiv(n, 256), (long)wp_sm_count() * 16);
+    WP_KERNEL("fill", 4.0 * n, s, fill_kernel<<<gn, 256, 0, s>>>(ls, n, (float)dx));
+    if (count > 0)
+        WP_KERNEL("particles_rough", 12.0 * count, s,
+                  particles_rough_kernel<<<(unsigned)wp_cdiv(count, 256), 256, 0, s>>>(ls, xyz, count, nx, ny, nz, dx,
+                                                                                     radius));
+    float* tmp = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * n, s));
+    wp_status st = WP_OK;
+    auto inv = [&]() -> wp_status {
+        WP_KERNEL("inv_ls", 8.0 * n, s, inv_ls_kernel<<<gn, 256, 0, s>>>(ls, n, (float)max_dis));
+        return WP_OK;
+    };
+    if ((st = inv()) == WP_OK && (st = fsweep_iters(ls, tmp, nx, ny, nz, dx, n_iters, s)) == WP_OK &&
+        (st = inv()) == WP_OK && (st = fsweep_iters(ls, tmp, nx, ny, nz, dx, n_iters, s)) == WP_OK) {
+        WP_KERNEL("negate", 8.0 * n, s, negate_kernel<<<gn, 256, 0, s>>>(ls, n));
+    }
+    cudaFreeAsync(tmp, s);
+    return st;
+}
+
 extern "C" CUWHHD_API wp_status wp_fast_sweep_solve(float* ls, int nx, int ny, int nz, double dx, int n_iters,
                                                     void* stream) {
     return fsweep_entry(ls, nx, ny, nz, dx, n_iters, false, (cudaStream_t)stream);
