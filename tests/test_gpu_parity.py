@@ -366,7 +366,8 @@ def test_recover2d_and_mg2d_full_config0_size(wp, oracle):
 
 def test_mg_offset_views_and_autotune_keep_results(wp, oracle):
     """Right-hand sides that are 4-byte-offset views take the scalar column kernels, aligned ones the
-    128-bit quad kernels, and the autotuner only reshapes grids: all give the same cycles."""
+    128-bit quad kernels (or the fused level-0 cycle), and the autotuner only reshapes grids: all
+    give the same cycles, up to the constant that FP32 rounding adds to a Neumann iterate."""
     nn, h, a, _, f = _sphere_problem(wp, oracle, 32, seed=9)
     mg = wp.CuMultigridFrac3D(*(T(x) for x in a), nn, h)
     fa = T(f)
@@ -379,7 +380,10 @@ def test_mg_offset_views_and_autotune_keep_results(wp, oracle):
         dst = torch.zeros(f.shape, device="cuda")
         rep = mg.SolveTol(dst, None, rhs, rel_tol=0.0, max_cycles=6, precision=wp.PREC_FP32)
         outs.append((N(dst), rep["history"]))
-    assert rel(outs[0][0], outs[1][0]) < 1e-6
+    act = outs[0][0] != 0
+    d = outs[0][0] - outs[1][0]
+    d[act] -= d[act].mean()
+    assert np.sqrt(np.sum(d * d) / np.sum(outs[0][0] ** 2)) < 1e-6
     np.testing.assert_allclose(outs[0][1], outs[1][1], rtol=1e-4)
     before = mg.Tiles()
     mg.Autotune()

@@ -1153,6 +1153,8 @@ __global__ void __launch_bounds__(256) prolong_tri_q_kernel(T* __restrict__ v, c
     prolong_tri_q_body<T>(v, vc, nx, ny, nz, ncx, ncy, ncz, blockIdx.x, blockIdx.y, threadIdx.x);
 }
 
+#include "wp_mg_fused.cuh"
+
 // cell layout of the y-face fractions: fyc[y + x ny + z nx ny] = ay[y + x (ny+1) + z nx (ny+1)]
 __global__ void fyc_kernel(float* __restrict__ fyc, const float* __restrict__ ay, int nx, int ny, long cells) {
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < cells; t += (long)gridDim.x * blockDim.x) {
@@ -2353,6 +2355,10 @@ struct Level {
     float* frac[3];   // ax, ay, az (level-owned copies)
     float* fyc;       // ay re-laid per cell (lower y face), so y-quads of cells load with 128-bit accesses
     unsigned char* uni; // per (x, z) row: all of the row's interior face fractions are exactly 1
+    unsigned char* tuni; // per (plane, tile) of the fused cycle kernels (tile_uni_kernel); levels whose
+                         // extents fit those kernels (fz_level_ok) only
+    int fz_fast;      // every cell's diagonal is positive on a fully open plane with the interior z
+                      // factors: the fused kernels may take their straight-line path
     float* ccf;       // levels of at most kCoarseCells cells: per-cell stencils of the FP32 coarse cycle
     long long uni_rows; // rows flagged in uni
     double* tab64;    // per axis: glo[n], ghi[n], d[n]
@@ -2580,6 +2586,66 @@ void launch_prolong_tri(const Level& L, const Level& C, T* v, const T* vc, cudaS
     }
 }
 
+// levels the fused cycle kernels handle: whole 32 x 32 (x, y) tiles and an even number of planes
+bool fz_level_ok(const int* n) { return n[0] % fz::TX == 0 && n[1] % fz::TY == 0 && n[2] >= 2 && n[2] % 2 == 0; }
+
+// z planes per CTA (even): `want`, or 16.  Chunks of 16 planes (one warm-up pair of planes per
+// eight) keep several waves of CTAs, so the hardware scheduler evens out tiles that cross solids
+// (their planes take the slower general path); at 256^3 with four spheres 16 beat 8, 24-128 and a
+// single wave of one chunk per resident slot.
+int fz_zchunk(const Level& L, int want) {
+    int zc = want > 0 ? want : 16;
+    zc += zc & 1;
+    // a chunk's planes and their pipeline halo fit the kernels' plane table
+    return std::min(std::min(zc, L.n[2] + (L.n[2] & 1)), fz::ZT - 6);
+}
+
+// pre-smoothing + residual restriction of level L into fc (cycle_down_kernel); v0 NULL: from zero.
+// False when a tensor map cannot be made.
+bool launch_cycle_down(const Level& L, float* dst, float* fc, const float* v0, const float* f, float w, int zc,
+                       cudaStream_t s) {
+    CUtensorMap mv, mf;
+    if (!wptc::map_f32_3d(&mf, f, L.n[1], L.n[0], L.n[2], fz::RY, fz::RX)) return false;
+    if (v0 && !wptc::map_f32_3d(&mv, v0, L.n[1], L.n[0], L.n[2], fz::RY, fz::RX + 2)) return false;
+    if (!v0) mv = mf;  // not read
+    const dim3 g((L.n[0] / fz::TX) * (L.n[1] / fz::TY), wp_cdiv(L.n[2], zc));
+    const Lvl<float> V = view<float>(L);
+    const unsigned char* tu = L.tuni;
+    if (v0) {
+        if (wp_set_smem(cycle_down_kernel<false>, fz::smem_bytes) != cudaSuccess) return false;
+        wp_launch_pdl(cycle_down_kernel<false>, g, fz::THREADS, fz::smem_bytes, s, mv, mf, dst, fc, V, tu, w, zc,
+                      L.fz_fast, L.err);
+    } else {
+        if (wp_set_smem(cycle_down_kernel<true>, fz::smem_bytes) != cudaSuccess) return false;
+        wp_launch_pdl(cycle_down_kernel<true>, g, fz::THREADS, fz::smem_bytes, s, mv, mf, dst, fc, V, tu, w, zc,
+                      L.fz_fast, L.err);
+    }
+    return true;
+}
+
+// prolongation of the coarse correction vc + post-smoothing of vin (cycle_up_kernel): into dst, or
+// added to p64 when p64 is given
+bool launch_cycle_up(const Level& L, const Level& C, float* dst, double* p64, const float* vin, const float* vc,
+                     const float* f, float w, int zc, cudaStream_t s) {
+    (void)C;
+    CUtensorMap mv, mf;
+    if (!wptc::map_f32_3d(&mf, f, L.n[1], L.n[0], L.n[2], fz::RY, fz::RX)) return false;
+    if (!wptc::map_f32_3d(&mv, vin, L.n[1], L.n[0], L.n[2], fz::RY, fz::RX + 2)) return false;
+    const dim3 g((L.n[0] / fz::TX) * (L.n[1] / fz::TY), wp_cdiv(L.n[2], zc));
+    const Lvl<float> V = view<float>(L);
+    const unsigned char* tu = L.tuni;
+    if (p64) {
+        if (wp_set_smem(cycle_up_kernel<true>, fz::smem_bytes) != cudaSuccess) return false;
+        wp_launch_pdl(cycle_up_kernel<true>, g, fz::THREADS, fz::smem_bytes, s, mv, mf, (float*)nullptr, p64, vc, V, tu, w,
+                      zc, L.fz_fast, L.err);
+    } else {
+        if (wp_set_smem(cycle_up_kernel<false>, fz::smem_bytes) != cudaSuccess) return false;
+        wp_launch_pdl(cycle_up_kernel<false>, g, fz::THREADS, fz::smem_bytes, s, mv, mf, dst, (double*)nullptr, vc, V, tu,
+                      w, zc, L.fz_fast, L.err);
+    }
+    return true;
+}
+
 }  // namespace
 
 struct wp_mgfrac3d {
@@ -2609,6 +2675,8 @@ struct wp_mgfrac3d {
     int loop_key[7];   // nu1, nu2, prolongation, full-multigrid first cycle, tune_gen, device, inner cycles
     double loop_omega;
     long long loop_launches[2]; // kernels of the first cycle's graph part and of one loop body
+    int fz_on;         // run the V(2,2) FP32 cycle of level 0 as the two fused kernels where it fits
+    int fz_zc;         // their z planes per CTA (0 = heuristic)
     int ix_built;      // the index lists of every level exist
     float* ix_r;       // residual workspace of the index-sparse cycle, shared by the levels (finest size)
     double* ix_r64;    // the same for the FP64 cycle
@@ -2662,6 +2730,22 @@ wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, cons
             L.uni_rows = 0;
             for (unsigned char b : u) L.uni_rows += b != 0;
         }
+        if (dims == 3 && fz_level_ok(n)) {
+            const int ntiles = (n[0] / fz::TX) * (n[1] / fz::TY);
+            WP_CUDA_TRY(cudaMalloc((void**)&L.tuni, (size_t)ntiles * n[2]));
+            Lvl<float> V{};
+            V.nx = n[0]; V.ny = n[1]; V.nz = n[2];
+            V.ax = L.frac[0]; V.ay = L.frac[1]; V.az = L.frac[2]; V.fyc = L.fyc;
+            WP_KERNEL("tile_uniform", 12.0 * L.cells, s,
+                      tile_uni_kernel<<<dim3(ntiles, n[2]), 256, 0, s>>>(L.tuni, V));
+            if (nl == 0) {
+                // the fused kernels' shared-memory limits, set here rather than while a cycle is captured
+                WP_CUDA_TRY(wp_set_smem(cycle_down_kernel<true>, fz::smem_bytes));
+                WP_CUDA_TRY(wp_set_smem(cycle_down_kernel<false>, fz::smem_bytes));
+                WP_CUDA_TRY(wp_set_smem(cycle_up_kernel<true>, fz::smem_bytes));
+                WP_CUDA_TRY(wp_set_smem(cycle_up_kernel<false>, fz::smem_bytes));
+            }
+        }
         // spacing tables; 2D problems have a single z layer with no z faces (tables all zero)
         std::vector<double> t64;
         std::vector<float> t32;
@@ -2677,6 +2761,21 @@ wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, cons
             t64.insert(t64.end(), hd[a].begin(), hd[a].end());
             for (double v : lo) t32.push_back((float)v);
             for (double v : hi) t32.push_back((float)v);
+        }
+        {
+            // smallest diagonal of a fully open cell (the fused kernels' straight-line path divides by
+            // none): the least lower + upper factor per axis, z at the interior reference plane
+            float mn[2] = {0.f, 0.f};
+            for (int a = 0; a < 2; ++a) {
+                const float* lo = t32.data() + 2 * (size_t)(a == 0 ? 0 : n[0]);
+                const float* hi = lo + n[a];
+                mn[a] = lo[0] + hi[0];
+                for (int i = 1; i < n[a]; ++i) mn[a] = std::min(mn[a], lo[i] + hi[i]);
+            }
+            const float* zlo = t32.data() + 2 * (size_t)(n[0] + n[1]);
+            const int zr = n[2] / 2;
+            const float dmin = ((mn[1] + mn[0]) + zlo[zr]) + zlo[n[2] + zr];
+            L.fz_fast = dmin > 1e-10f ? 1 : 0;
         }
         WP_CUDA_TRY(cudaMalloc((void**)&L.tab64, sizeof(double) * t64.size()));
         WP_CUDA_TRY(cudaMalloc((void**)&L.tab32, sizeof(float) * t32.size()));
@@ -2979,6 +3078,33 @@ wp_status vcycle(wp_mgfrac3d* h, int l, const T* f, int nu1, int nu2, T w, int p
         return WP_OK;
     }
     if (l < h->nl - 1) {
+        if constexpr (sizeof(T) == 4) {
+            // level 0's V(2,2) cycle as two fused passes (wp_mg_fused.cuh): pre-smoothing + residual
+            // restriction, then prolongation + post-smoothing (+ the refinement update)
+            Level& C = h->lv[l + 1];
+            if (l == 0 && h->fz_on && L.tuni && h->dims == 3 && prolong == WP_PROLONG_TRILINEAR && nu1 == 2 &&
+                nu2 == 2 && C.n[0] * 2 == L.n[0] && C.n[1] * 2 == L.n[1] && C.n[2] * 2 == L.n[2] && al16(f) &&
+                al16(L.v) && al16(L.t) && wptc::encode_tiled()) {
+                const int zc = fz_zchunk(L, h->fz_zc);
+                const float* v0 = clear_v ? nullptr : L.v;
+                bool okl = true;
+                WP_KERNEL(v0 ? "cycle_down_finest" : "cycle_down0_finest",
+                          (double)L.cells * (v0 ? 12.0 : 8.0) + (double)C.cells * 4.0 + frac_bytes(L), s,
+                          okl = launch_cycle_down(L, L.t, C.f, v0, (const float*)f, (float)w, zc, s));
+                if (!okl) { wp_set_error_msg("fused cycle: no tensor map for the level"); return WP_ERR_CUDA; }
+                std::swap(L.v, L.t);
+                if ((st = vcycle<T>(h, l + 1, Bufs<T>::f(C), nu1, nu2, w, prolong, s, true)) != WP_OK) return st;
+                const bool acc = acc64 != nullptr && added != nullptr && al16(acc64);
+                WP_KERNEL(acc ? "cycle_up_update_finest" : "cycle_up_finest",
+                          (double)L.cells * (acc ? 24.0 : 12.0) + (double)C.cells * 4.0 + frac_bytes(L), s,
+                          okl = launch_cycle_up(L, C, acc ? nullptr : L.t, acc ? acc64 : nullptr, L.v, C.v,
+                                                (const float*)f, (float)w, zc, s));
+                if (!okl) { wp_set_error_msg("fused cycle: no tensor map for the level"); return WP_ERR_CUDA; }
+                if (acc) *added = true;
+                std::swap(L.v, L.t);
+                return WP_OK;
+            }
+        }
         int pre = nu1;
         if (clear_v) {
             const int var = sizeof(T) == 4 ? L.var[kZcJacobi] : 0;
@@ -3128,7 +3254,7 @@ void destroy_levels(wp_mgfrac3d* h) {
     for (int l = 0; l < kMaxLevels; ++l) {
         Level& L = h->lv[l];
         for (int a = 0; a < 3; ++a) if (L.frac[a]) cudaFree(L.frac[a]);
-        void* ps[] = {L.tab64, L.tab32, L.fyc, L.uni, L.v, L.t, L.f, L.v64, L.t64, L.f64, L.imask, L.iseg};
+        void* ps[] = {L.tab64, L.tab32, L.fyc, L.uni, L.tuni, L.v, L.t, L.f, L.v64, L.t64, L.f64, L.imask, L.iseg};
         for (void* p : ps) if (p) cudaFree(p);
     }
     if (h->ccf_all) cudaFree(h->ccf_all);
@@ -3154,6 +3280,7 @@ wp_status create_common(wp_mgfrac3d** out, int dims, const float* ax, const floa
     h->dims = dims;
     h->coarsest_iters = dims == 3 ? 50 : 10;
     h->mid_on = 1;
+    h->fz_on = 1;
     wp_status st = build_hierarchy(h, ax, ay, az, nx, ny, nz, dx, dy, dz, s);
     if (st == WP_OK) {
         cudaError_t e = cudaMalloc((void**)&h->acc, 4 * sizeof(double) + 16);
@@ -3955,6 +4082,25 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
         }
         h->mid_on = best_on;
     }
+    // level 0's V(2,2) cycle as the two fused passes or kernel by kernel: time a whole cycle from
+    // zero both ways (after an L2 flush when level 0 exceeds it); the fused passes only when they
+    // are clearly (5%) faster -- at 256^3 the two measure alike and the one-sweep kernels use the
+    // memory bandwidth better per byte
+    if (st == WP_OK && h->dims == 3 && h->nl >= 2 && h->lv[0].tuni) {
+        Level& L0 = h->lv[0];
+        float ms[2] = {0.f, 0.f};
+        for (int on = 0; on < 2 && st == WP_OK; ++on) {
+            h->fz_on = on;
+            auto launch = [&]() {
+                vcycle<float>(h, 0, L0.f, 2, 2, 2.f / 3.f, WP_PROLONG_TRILINEAR, s, true);
+            };
+            ms[on] = time_launches(launch, s, ea, eb, 5, flush, flush ? kFlush : 0);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
+        }
+        h->fz_on = ms[1] < 0.95f * ms[0] ? 1 : 0;
+        ++h->tune_gen;
+    }
     if (flush) {
         cudaStreamSynchronize(s);
         cudaFree(flush);
@@ -3994,6 +4140,13 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_set_tile(wp_mgfrac3d* h, int level, 
     if (h && kind == 3 && (variant == 0 || variant == 1)) {
         // the levels below the finest: one persistent launch (1) or launch by launch (0)
         h->mid_on = variant;
+        ++h->tune_gen;
+        return WP_OK;
+    }
+    if (h && kind == 4 && (variant == 0 || variant == 1)) {
+        // level 0's V(2,2) cycle: the two fused kernels (1) or one kernel per sweep / transfer (0)
+        h->fz_on = variant;
+        h->fz_zc = zc > 0 ? zc + (zc & 1) : 0;
         ++h->tune_gen;
         return WP_OK;
     }

@@ -154,4 +154,22 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N, int a_mn_maj
            ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
+            "r"(dst),
+        "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+// ---- host side (wp_util.cu)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+// the driver's cuTensorMapEncodeTiled (nullptr when the driver does not provide it)
+EncodeTiledFn encode_tiled();
+// tensor map of an FP32 array with extents (n0 fastest, n1, n2), no swizzle, box (b0, b1, 1); elements
+// outside the array read as zero.  b0 * 4 must be a multiple of 16 and the base 16-byte aligned.
+bool map_f32_3d(CUtensorMap* m, const float* base, int n0, int n1, int n2, int b0, int b1);
+
 }  // namespace wptc

@@ -212,3 +212,34 @@ cudaError_t wp_set_smem_impl(const void* kernel, size_t bytes) {
     if (e == cudaSuccess) done[key] = bytes;
     return e;
 }
+
+// ---------------------------------------------------------------------------------------------
+// TMA tensor maps (the driver entry point is resolved once per process)
+#include "wp_tc.cuh"
+
+namespace wptc {
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+bool map_f32_3d(CUtensorMap* m, const float* base, int n0, int n1, int n2, int b0, int b1) {
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || ((uintptr_t)base & 15u) || (n0 * 4) % 16 || (b0 * 4) % 16) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)n0, (cuuint64_t)n1, (cuuint64_t)n2};
+    const cuuint64_t strides[2] = {(cuuint64_t)n0 * 4, (cuuint64_t)n0 * 4 * n1};
+    const cuuint32_t box[3] = {(cuuint32_t)b0, (cuuint32_t)b1, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+}  // namespace wptc
