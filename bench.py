@@ -100,13 +100,25 @@ def make_problem(n, seed):
     return centers, radii, (xv, yv, zv)
 
 
-# DRAM bytes (read + write) per launch of the finest-level Jacobi sweep, from one ncu capture of the
-# profiling command in profiles/jacobi_q_256_level0.md (256^3 workload).  Algorithmic bytes per
-# launch (226.0 MB): 12 B/cell (v and f read, v written) x 16,777,216 cells + 12 B/cell of face
-# fractions for the rows that are not uniform (12.2% of the (x, z) rows) + 1 B per row flag.
-NCU_TRAFFIC = {
-    ("jacobi_finest", 256): (219095808, "profiles/jacobi_q_256_level0.md (173.6 MB read + 45.5 MB write)"),
-}
+def ncu_traffic(kernel, n):
+    """DRAM bytes (read + write) per launch of `kernel` at n^3 from the ncu captures summarised in
+    profiles/ncu_traffic.json, or (None, reason).  A capture counts only while the CUDA sources are
+    the ones it was taken from (their SHA-256 is stored with it); otherwise the figure is stale."""
+    import hashlib
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None, "no capture"
+    rec = json.load(open(path)).get(f"{kernel}@{n}")
+    if not rec:
+        return None, "no capture of this kernel at this size"
+    h = hashlib.sha256()
+    csrc = os.path.join(ROOT, "waveletpotentials_b200", "csrc")
+    for f in sorted(os.listdir(csrc)):
+        if f.endswith((".cu", ".cuh")):
+            h.update(open(os.path.join(csrc, f), "rb").read())
+    if rec.get("csrc_sha256") != h.hexdigest():
+        return None, "capture predates the current kernel sources"
+    return int(rec["dram_bytes_per_launch"]), rec["source"]
 
 
 def max_over_ranks(values, world):
@@ -210,6 +222,14 @@ def run_ours(args, rank, world, local_rank):
         prof.append({"kernel": name.value.decode(), "launches": lc.value, "ms": t.value, "bytes": b.value})
     prof.sort(key=lambda r: -r["ms"])
     ms, = max_over_ranks([ms], world)
+    # the last step's outputs (every step projects the same input) and the initial divergence, for
+    # the host-side checks against the oracle
+    b0 = torch.empty(s["p"], device=dev)
+    api.CuConvergence.GetB_3d_frac_vel(b0, *u0, *a, nn, h)
+    outputs = {"u": [x.double().cpu().numpy() for x in u], "q": [x.double().cpu().numpy() for x in q],
+               "u0": [np.asarray(x, np.float64) for x in (xv, yv, zv)],
+               "p64": proj.mg.Iterate64(), "a": [x.double().cpu().numpy() for x in a],
+               "max_abs_b0": api.max_abs(b0)}
 
     # end to end through the public API with host buffers: every step copies its pinned host velocity
     # in and its potential q out; HostPipeline3D overlaps those copies with the neighbouring steps'
@@ -326,7 +346,7 @@ def run_ours(args, rank, world, local_rank):
         }
         mgp.close()
     tiles = proj.mg.Tiles(with_times=True)
-    return ms, ems, ek, h2d, d2h, launches, prof, reps, clk.summary(), plain, (tiles, psteps, prof_ms)
+    return ms, ems, ek, h2d, d2h, launches, prof, reps, clk.summary(), plain, (tiles, psteps, prof_ms, outputs)
 
 
 # ------------------------------------------------------------------ batched workload
@@ -575,29 +595,134 @@ def run_warmstart(args, rank, world, local_rank):
     return out
 
 
+# ------------------------------------------------------------------ convolution kernels
+def run_conv(args):
+    """The warm-start network's tensor-core 3x3x3 convolutions (forward and weight gradient) on one
+    channels-last BF16 volume of conv_n^3 x conv_c: CUDA-event time and TFLOP/s
+    (2 * 27 * c * c * n^3 flops); a profiling aid for the tcgen05 kernels."""
+    import torch
+    from waveletpotentials_b200 import api, build
+    build.build()
+    n, c = args.conv_n, args.conv_c
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn((n, n, n, c), device="cuda", generator=g).to(torch.bfloat16)
+    w = (torch.randn((27, c, c), device="cuda", generator=g) * 0.05).to(torch.bfloat16)
+    out = torch.empty_like(x)
+    dw = torch.zeros((27, c, c), device="cuda")
+    for _ in range(3):
+        api.conv3_forward(out, x, w)
+        api.conv3_wgrad(dw, x, out)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    if args.profile_region:
+        torch.cuda.profiler.start()
+    ev[0].record(st)
+    for _ in range(args.conv_reps):
+        api.conv3_forward(out, x, w)
+    ev[1].record(st)
+    for _ in range(args.conv_reps):
+        api.conv3_wgrad(dw, x, out)
+    ev[2].record(st)
+    torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.profiler.stop()
+    fl = 2.0 * 27 * c * c * n ** 3
+    res = {}
+    for name, t in (("conv3_forward", ev[0].elapsed_time(ev[1]) / args.conv_reps),
+                    ("conv3_wgrad", ev[1].elapsed_time(ev[2]) / args.conv_reps)):
+        res[name] = {"ms": t, "tflops": fl / t / 1e9}
+    print(json.dumps({"workload": "conv", "n": n, "c": c, "kernels": res}))
+
+
 # --------------------------------------------------------------------------- CPU arm
-def cpu_sample(n, seed, ncycles):
-    """One bounded sample of the projection on the host cores with the FP64 oracle: the
-    divergence, ONE trilinear V-cycle, the gradient update and the full recovery at n^3; the
-    projection time is extrapolated to `ncycles` V-cycles."""
+def cpu_inputs(n, seed, fractions=None):
+    """The benchmark's inputs on the host in FP64: velocity (the FP32 values), face fractions (the
+    GPU's FP32 ones when given, else the oracle's)."""
     from oracle import oracle as O
     O.build()
     nn = (n, n, n)
     h = 1.0 / n
     centers, radii, (xv, yv, zv) = make_problem(n, seed)
-    sdf = O.sdf_spheres3d(nn, h, centers, radii)
-    ax, ay, az = O.fractions3d(sdf, nn, h)
+    if fractions is None:
+        sdf = O.sdf_spheres3d(nn, h, centers, radii)
+        fractions = O.fractions3d(sdf, nn, h)
+    u = [np.asarray(x, np.float64) for x in (xv, yv, zv)]
+    a = [np.asarray(x, np.float64) for x in fractions]
+    return nn, h, u, a
+
+
+def cpu_projection(n, seed, ncycles, fractions=None):
+    """One whole projection with the FP64 oracle on the host cores (the same composition as a GPU
+    step): divergence, its mean over the active cells removed, ncycles trilinear V(2,2) cycles,
+    omega 2/3, from zero, the gradient update and the wavelet recovery.  Returns the wall times per
+    stage and the fields."""
+    from oracle import oracle as O
+    nn, h, u, a = cpu_inputs(n, seed, fractions)
+    d = (h,) * 3
     t0 = time.perf_counter()
-    f = O.divergence3d(xv, yv, zv, ax, ay, az, nn, (h,) * 3)
+    f = O.divergence3d(*u, *a, nn, d)
+    act = cpu_active(a)
+    f[act] -= f[act].mean()
     t1 = time.perf_counter()
-    p, _ = O.mgfrac3d_solve(f, ax, ay, az, nn, (h,) * 3, 1, 2, 2, 2.0 / 3.0, prolong=O.PROLONG_TRILINEAR)
+    p, hist = O.mgfrac3d_solve(f, *a, nn, d, ncycles, 2, 2, 2.0 / 3.0, prolong=O.PROLONG_TRILINEAR)
     t2 = time.perf_counter()
-    uu = O.grad_subtract3d(xv, yv, zv, p, ax, ay, az, nn, (h,) * 3, True)
-    O.recover3d(*uu, nn, (h,) * 3)
+    uu = O.grad_subtract3d(*u, p, *a, nn, d, True)
     t3 = time.perf_counter()
-    sample_s = t3 - t0
-    proj_s = (t1 - t0) + ncycles * (t2 - t1) + (t3 - t2)
-    return sample_s, proj_s
+    q = O.recover3d(*uu, nn, d)
+    t4 = time.perf_counter()
+    return {"divergence_s": t1 - t0, "mg_s": t2 - t1, "gradient_s": t3 - t2, "recovery_s": t4 - t3,
+            "total_s": t4 - t0, "rel_residual": float(hist[-1]), "p": p, "u": uu, "q": q, "act": act,
+            "f": f, "a": a, "h": h}
+
+
+def cpu_active(a):
+    """cells with at least one open interior face (the Neumann problem's support)"""
+    ax, ay, az = a
+    act = np.zeros((ax.shape[0], ay.shape[1], ax.shape[2]), dtype=bool)
+    act[:, :-1, :] |= ax[:, 1:-1, :] > 0
+    act[:, 1:, :] |= ax[:, 1:-1, :] > 0
+    act[:, :, :-1] |= ay[:, :, 1:-1] > 0
+    act[:, :, 1:] |= ay[:, :, 1:-1] > 0
+    act[:-1] |= az[1:-1] > 0
+    act[1:] |= az[1:-1] > 0
+    return act
+
+
+def cpu_sample(n, seed, ncycles):
+    """A bounded sample of the projection on the host cores with the FP64 oracle: the divergence,
+    ONE trilinear V-cycle, the gradient update and the whole recovery at n^3.  Returns the sample's
+    wall time and the projection time extrapolated to ncycles V-cycles."""
+    from oracle import oracle as O
+    nn, h, u, a = cpu_inputs(n, seed)
+    d = (h,) * 3
+    t0 = time.perf_counter()
+    f = O.divergence3d(*u, *a, nn, d)
+    t1 = time.perf_counter()
+    p, _ = O.mgfrac3d_solve(f, *a, nn, d, 1, 2, 2, 2.0 / 3.0, prolong=O.PROLONG_TRILINEAR)
+    t2 = time.perf_counter()
+    uu = O.grad_subtract3d(*u, p, *a, nn, d, True)
+    O.recover3d(*uu, nn, d)
+    t3 = time.perf_counter()
+    return t3 - t0, (t1 - t0) + ncycles * (t2 - t1) + (t3 - t2)
+
+
+def rel_l2(ref, got):
+    num = sum(float(np.sum((np.asarray(r, np.float64) - np.asarray(g, np.float64)) ** 2)) for r, g in zip(ref, got))
+    den = sum(float(np.sum(np.asarray(r, np.float64) ** 2)) for r in ref)
+    return float(np.sqrt(num / den))
+
+
+def fp32_div_floor(u0, a, u, h):
+    """The size of max|div| that FP32 rounding allows after the projection: the solver's right-hand
+    side is the FP32 divergence of the input u0 (its rounding, 2^-24 x the cell's sum of |a u0| over
+    its faces / h, cannot be projected out) and the projected u is stored in FP32 (2^-24 x its own
+    sum of |face flux| / h); the largest per-cell sum of the two."""
+    def fluxsum(v):
+        vx, vy, vz = (np.abs(np.asarray(x, np.float64)) for x in v)
+        return (vx[:, :-1, :] + vx[:, 1:, :]) + (vy[:, :, :-1] + vy[:, :, 1:]) + (vz[:-1] + vz[1:])
+    au0 = [np.asarray(x, np.float64) * np.asarray(y, np.float64) for x, y in zip(u0, a)]
+    return float(2.0 ** -24 * (fluxsum(au0) + fluxsum(u)).max() / h)
 
 
 def cores():
@@ -633,10 +758,14 @@ def main():
                          "(ncu does not profile kernels inside graphs with conditional nodes)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "warmstart", "index"],
+    ap.add_argument("--conv-n", type=int, default=64)
+    ap.add_argument("--conv-c", type=int, default=32)
+    ap.add_argument("--conv-reps", type=int, default=10)
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "warmstart", "index", "conv"],
                     help="single: one 256^3 projection per step; batch: 64 uneven grids in one graph per step; "
                          "warmstart: train the U-Net, then projections with/without its guess; index: four "
-                         "index-sparse V-cycles on a 15%%-fluid domain (profiling aid)")
+                         "index-sparse V-cycles on a 15%%-fluid domain (profiling aid); conv: the tensor-core "
+                         "convolutions alone (profiling aid)")
     ap.add_argument("--ws-n", type=int, default=128)
     ap.add_argument("--ws-train", type=int, default=128)
     ap.add_argument("--ws-eval", type=int, default=8)
@@ -662,7 +791,9 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        ncyc = 20
+        from oracle import oracle as O
+        O.build()
+        ncyc = 20  # the V-cycles our arm needs for 1e-10 at this configuration
         vals = []
         for i in range(args.warmup + args.steps):
             sample_s, proj_s = cpu_sample(args.n, args.seed, ncyc)
@@ -671,13 +802,14 @@ def main():
         proj_s = float(np.median([v[1] for v in vals]))
         sample_s = float(np.median([v[0] for v in vals]))
         value = 1.0 / proj_s
+        sample = (f"each step: FP64 oracle at {args.n}^3 on {O.threads()} OpenMP threads, divergence + 1 trilinear "
+                  f"V-cycle + gradient + full recovery ({sample_s:.2f} s); value extrapolated to {ncyc} V-cycles")
         out = {"impl": "reference", "metric": metric, "value": value, "unit": "projections/s", "n_gpus": 0,
-               "steps": args.steps, "warmup": args.warmup, "ms_per_step": proj_s * 1000.0, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded spectral fields)",
-               "config": workload,
-               "cpu_baseline": {"value": value, "unit": "projections/s", "cores": cores(), "kind": "port",
-                                "sample": f"FP64 oracle at {args.n}^3: divergence + 1 V-cycle + gradient + full "
-                                          f"recovery ({sample_s:.1f} s), extrapolated to {ncyc} V-cycles"},
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample_s * 1000.0,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (seeded spectral fields)", "config": workload,
+               "cpu_baseline": {"value": value, "unit": "projections/s", "cores": O.threads(), "kind": "port",
+                                "extrapolated": True, "sample": sample},
                "e2e": {"value": value, "unit": "projections/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
         return
@@ -707,6 +839,10 @@ def main():
         cells, segs = mgp.IndexSizes()
         print(json.dumps({"workload": "index", "n": args.n, "fluid": float(fl.mean()), "listed_cells": cells,
                           "segments": segs, "ms_per_cycle": g0.elapsed_time(g1) / 4}))
+        return
+    if args.workload == "conv" and args.impl == "ours":
+        if rank == 0:
+            run_conv(args)
         return
     if args.workload == "warmstart" and args.impl == "ours":
         if rank == 0:
@@ -747,7 +883,7 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     ms, ems, ek, h2d, d2h, launches, prof, reps, clocks, plain, extra = run_ours(args, rank, world, local_rank)
-    tiles, psteps, prof_ms = extra
+    tiles, psteps, prof_ms = extra[:3]
     if world > 1:
         import torch
         torch.distributed.destroy_process_group()
@@ -759,20 +895,54 @@ def main():
     roof = None
     if top and top["ms"] > 0:
         ach = top["bytes"] / (top["ms"] / 1000.0) / 1e9
-        tr = NCU_TRAFFIC.get((top["kernel"], args.n))
+        tr = ncu_traffic(top["kernel"], args.n)
         roof = {"bound": "hbm", "kernel": top["kernel"], "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "measured_over": f"{psteps} further timed steps with CUDA events around every kernel "
                                  f"({prof_ms:.2f} ms per step there)",
-                "frac": ach / hbm, "peak_kind": peak_kind, "traffic": tr[0] if tr else None,
-                "traffic_source": tr[1] if tr else None,
+                "frac": ach / hbm, "peak_kind": peak_kind, "traffic": tr[0], "traffic_source": tr[1],
                 "avg_launch_us": top["ms"] * 1000.0 / top["launches"],
                 "bytes_per_launch": top["bytes"] / top["launches"]}
-    cpu = None
+    cpu = parity = None
+    ncyc = int(reps[-1]["cycles"])
+    gout = extra[3]
+    div = {"max_abs_div": reps[-1]["max_abs_div"], "max_abs_b0": gout["max_abs_b0"],
+           "relative": reps[-1]["max_abs_div"] / gout["max_abs_b0"],
+           "fp32_floor": fp32_div_floor(gout["u0"], gout["a"], gout["u"], 1.0 / args.n),
+           "note": "max|div a(u - grad p)| of the FP32 projected field after the 1e-10 solve; fp32_floor: 2^-24 x the "
+                   "largest per-cell sum of |a u0| (the FP32 right-hand side's rounding) and |u| (the FP32 storage) "
+                   "over the cell's faces / h, what FP32 rounding alone leaves"}
     if not args.no_cpu_baseline:
-        sample_s, proj_s = cpu_sample(args.n, args.seed, int(round(np.mean([r["cycles"] for r in reps]))))
-        cpu = {"value": 1.0 / proj_s, "unit": "projections/s", "cores": cores(), "kind": "port",
-               "sample": f"FP64 oracle at {args.n}^3: divergence + 1 V-cycle + gradient + full recovery "
-                         f"({sample_s:.1f} s), extrapolated to {reps[-1]['cycles']} V-cycles"}
+        from oracle import oracle as O
+        O.build()
+        nthr = O.threads()
+        cp = cpu_projection(args.n, args.seed, ncyc, fractions=gout["a"])
+        O.set_threads(1)
+        s1, p1 = cpu_sample(args.n, args.seed, ncyc)
+        O.set_threads(nthr)
+        cpu = {"value": 1.0 / cp["total_s"], "unit": "projections/s", "cores": nthr, "kind": "port",
+               "extrapolated": False,
+               "sample": f"one whole projection at {args.n}^3 by the FP64 oracle on {nthr} OpenMP threads: divergence, "
+                         f"{ncyc} trilinear V(2,2) cycles, gradient update, wavelet recovery ({cp['total_s']:.1f} s)",
+               "stages_s": {k: round(cp[k], 3) for k in ("divergence_s", "mg_s", "gradient_s", "recovery_s")},
+               "single_thread": {"value": 1.0 / p1, "unit": "projections/s", "cores": 1, "extrapolated": True,
+                                 "sample": f"divergence + 1 V-cycle + gradient + recovery on one thread ({s1:.1f} s), "
+                                           f"extrapolated to {ncyc} V-cycles"}}
+        act = cp["act"]
+
+        def no_mean(x):
+            y = np.array(x, np.float64, copy=True)
+            y[act] -= y[act].mean()
+            y[~act] = 0.0
+            return y
+
+        parity = {"against": f"the FP64 oracle's projection of the same input (the GPU's FP32 face fractions), "
+                             f"{ncyc} FP64 V-cycles of the same method (rel. residual {cp['rel_residual']:.1e})",
+                  "p_rel_l2": rel_l2([no_mean(cp["p"])], [no_mean(gout["p64"])]),
+                  "u_rel_l2": rel_l2(cp["u"], gout["u"]), "q_rel_l2": rel_l2(cp["q"], gout["q"])}
+        ux, uy, uz = cp["u"]
+        hh = cp["h"]
+        odiv = np.abs((ux[:, 1:, :] - ux[:, :-1, :]) / hh + (uy[:, :, 1:] - uy[:, :, :-1]) / hh + (uz[1:] - uz[:-1]) / hh)
+        div["oracle_fp64_max_abs_div"] = float(odiv.max())
     out = {
         "metric": metric, "value": value, "unit": "projections/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -786,6 +956,8 @@ def main():
         "clocks": clocks,
         "solve": {"vcycles": reps[-1]["cycles"], "rel_residual": reps[-1]["rel_residual"],
                   "max_abs_div": reps[-1]["max_abs_div"]},
+        "divergence": div,
+        "parity": parity,
         "plain": plain,
         # every kernel of the event-instrumented steps (ms and algorithmic bytes summed over psteps)
         "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} for r in prof],

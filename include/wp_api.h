@@ -9,7 +9,10 @@
  * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).  Calls are
  * asynchronous on that stream unless they return a host scalar.  Errors come back as wp_status;
  * nothing calls exit().  wp_last_error() gives the message of the last failure on this thread.
- * Handles are independent: one handle per stream/thread, no process-wide mutable state.
+ * Handles are independent: one handle per stream/thread.  Process-wide state is limited to caches
+ * filled once (per-device SM counts, kernel attributes, the autotuner's choices per device and grid
+ * extents, the launch counters and profiler records) and the static scratch of
+ * wp_dst3d_solve_noalloc, whose sharing rules are stated at its declaration.
  *
  * The reference exposes no C ABI (cuWHHD_Export.h only defines an empty CUWHHD_API macro); each
  * declaration below names the reference C++ entry point it replaces.
@@ -194,6 +197,10 @@ CUWHHD_API wp_status wp_mgfrac3d_residual(wp_mgfrac3d* h, const float* v, const 
    WP_ERR_INVALID_ARG if the handle has not run such a solve.  No reference counterpart (the
    reference iterate is DTYPE). */
 CUWHHD_API wp_status wp_mgfrac3d_iterate64(wp_mgfrac3d* h, double* dst, void* stream);
+/* The device address of that FP64 iterate inside the handle (no copy; valid until the handle's
+   next solve or its destruction); WP_ERR_INVALID_ARG if the handle has not run such a solve.  No
+   reference counterpart. */
+CUWHHD_API wp_status wp_mgfrac3d_iterate64_view(wp_mgfrac3d* h, const double** out);
 CUWHHD_API wp_status wp_mgfrac3d_destroy(wp_mgfrac3d* h);
 /* Tile-shape autotuner (no reference counterpart): times the column-walking stencil kernels of
    every level (Jacobi sweep, fused residual-restriction, FP64 defect) over candidate z-chunks and
@@ -249,6 +256,13 @@ CUWHHD_API wp_status wp_divergence_frac2d(float* b, const float* xv, const float
 CUWHHD_API wp_status wp_grad_subtract_frac3d(float* xv, float* yv, float* zv, const float* p, const float* ax,
                                              const float* ay, const float* az, int nx, int ny, int nz, double dx,
                                              double dy, double dz, int multiply_frac, void* stream);
+/* The same update with the FP64 pressure iterate of a WP_PREC_MIXED / WP_PREC_FP64 solve
+   (wp_mgfrac3d_iterate64_view): the gradient and the difference are formed in FP64 and rounded
+   once to the FP32 face value, as the reference's default FP64 build forms them (DoubleUseDefine.h:5,
+   cuGradient.cu:1952-2000).  No reference counterpart as a separate entry point. */
+CUWHHD_API wp_status wp_grad_subtract_frac3d_p64(float* xv, float* yv, float* zv, const double* p, const float* ax,
+                                                 const float* ay, const float* az, int nx, int ny, int nz, double dx,
+                                                 double dy, double dz, int multiply_frac, void* stream);
 CUWHHD_API wp_status wp_grad_subtract_frac2d(float* xv, float* yv, const float* p, const float* ax, const float* ay,
                                              int nx, int ny, double dx, double dy, int multiply_frac, void* stream);
 /* max |x| over n elements, FP64 result to host (CudaFindMaxValue, cudaMath.cu:1269-1280, without
@@ -338,7 +352,9 @@ CUWHHD_API wp_status wp_sweep2d_solve(float* qz, const float* xv, const float* y
      larger grids return WP_ERR_INVALID_ARG (use wp_dst3d_create / wp_dst3d_solve).
    - Nothing in the scratch has to start at zero: every call writes each word it reads.
    - The first call on each device resolves the scratch address (cudaGetSymbolAddress, with that
-     device current); make that first call an ordinary one, before any stream capture.
+     device current); make that first call an ordinary one, before any stream capture.  The address
+     is kept for the rest of the process: after cudaDeviceReset on a device, do not call this entry
+     point on that device again (the cached address belongs to the destroyed context).
    - The scratch is shared by all calls on a device: two calls that overlap in time (different
      streams, or different host threads without ordering) race on it and give wrong results.
      Order them (same stream, or events).

@@ -71,12 +71,24 @@ def lib():
             "or_frac_residual3d": (d, [p, p, p, p, p, p, i, i, i, d, d, d]),
             "or_frac_residual2d": (d, [p, p, p, p, p, i, i, d, d]),
             "or_dst3d_poisson": (None, [p, p, i, i, i, d, d, d]),
+            "or_set_threads": (None, [i]),
+            "or_get_threads": (i, []),
         }
         for name, (res, args) in sig.items():
             fn = getattr(_lib, name)
             fn.restype = res
             fn.argtypes = args
     return _lib
+
+
+def set_threads(n: int) -> None:
+    """OpenMP threads of the oracle's parallel loops."""
+    lib().or_set_threads(int(n))
+
+
+def threads() -> int:
+    """OpenMP threads the oracle's parallel loops use."""
+    return int(lib().or_get_threads())
 
 
 def _p(a: np.ndarray | None):

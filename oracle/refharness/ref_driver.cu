@@ -5,7 +5,8 @@
 // tests/golden/ and to time the reference build.  It calls only the reference's public entry
 // points (CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D,
 // CuDivLocalProject, CuWaveletPotentialRecover3D/2D, CuMultigridFrac3D/2D, CuConvergence,
-// CuGradient, CuSolidLevelSet3D) with the same call sequences as TestLocalProjection.cpp.
+// CuGradient, CuSolidLevelSet3D, CuDst3D, CuParallelSweep3D) with the same call sequences as
+// TestLocalProjection.cpp.
 //
 // Usage: ref_driver <op> <in_dir> <out_dir> [params...]; arrays are raw little-endian float64
 // files <name>.bin in the reference layout (y fastest).
@@ -33,6 +34,8 @@
 #include "cuGradient.cuh"
 #include "cuSolidLevelSet3D.cuh"
 #include "cuFastSweeping.cuh"
+#include "cuDst3D.cuh"
+#include "cuParallelSweep3D.cuh"
 
 static std::string g_in, g_out;
 
@@ -345,6 +348,53 @@ int main(int argc, char** argv) {
         write_bin("ax", from_dev(ax, sf));
         write_bin("ay", from_dev(ay, sf));
         write_bin("az", from_dev(az, sf));
+    } else if (op == "dst3d") {  // nx ny nz dx dy dz: CuDst3D(dim, dx).Solve(p, f)
+        // equal extents only: the constructor sizes its buffer as the largest of the x and z FFT
+        // layouts and a member it never sets (cuDst3D.cu:209-211); with equal extents every layout
+        // has the same size, so the buffer always holds the y pass too
+        int3 dim = make_int3(I(0), I(1), I(2));
+        if (dim.x != dim.y || dim.y != dim.z) { fprintf(stderr, "dst3d: equal extents only\n"); return 2; }
+        DTYPE3 dx = make_DTYPE3((DTYPE)D(3), (DTYPE)D(4), (DTYPE)D(5));
+        size_t nc = (size_t)dim.x * dim.y * dim.z;
+        DTYPE* f = to_dev(read_bin("f", nc));
+        DTYPE* p = dev_zeros(nc);
+        CuDst3D dst(dim, dx);
+        dst.Solve(p, f);
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("p", from_dev(p, nc));
+    } else if (op == "psweep3d") {  // n dx: CuParallelSweep3D(dim, dx, 'n') Solve, then Project
+        // (TestLocalProjection.cpp:719-721); equal extents only (its CuDst3D on the (n-1)^3 nodes)
+        int n = I(0);
+        int3 dim = make_int3(n, n, n);
+        DTYPE h = (DTYPE)D(1);
+        DTYPE3 dx = make_DTYPE3(h, h, h);
+        size_t sf = (size_t)(n + 1) * n * n, sq = (size_t)n * (n + 1) * (n + 1);
+        DTYPE* xv = to_dev(read_bin("xv", sf));
+        DTYPE* yv = to_dev(read_bin("yv", sf));
+        DTYPE* zv = to_dev(read_bin("zv", sf));
+        DTYPE *qx = dev_zeros(sq), *qy = dev_zeros(sq), *qz = dev_zeros(sq);
+        CuParallelSweep3D cups(dim, dx, 'n');
+        cups.Solve(qx, qy, qz, xv, yv, zv);
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("qx_solve", from_dev(qx, sq));
+        write_bin("qy_solve", from_dev(qy, sq));
+        write_bin("qz_solve", from_dev(qz, sq));
+        cups.Project(qx, qy, qz);
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("qx", from_dev(qx, sq));
+        write_bin("qy", from_dev(qy, sq));
+        write_bin("qz", from_dev(qz, sq));
+    } else if (op == "psweep2d") {  // n dx: CuParallelSweep3D(int2 dim, DTYPE2 dx, 'n').Solve(qz, xv, yv)
+        int n = I(0);
+        DTYPE h = (DTYPE)D(1);
+        size_t sf = (size_t)(n + 1) * n, sq = (size_t)(n + 1) * (n + 1);
+        DTYPE* xv = to_dev(read_bin("xv", sf));
+        DTYPE* yv = to_dev(read_bin("yv", sf));
+        DTYPE* qz = dev_zeros(sq);
+        CuParallelSweep3D cups(make_int2(n, n), make_DTYPE2(h, h), 'n');
+        cups.Solve(qz, xv, yv);
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("qz", from_dev(qz, sq));
     } else if (op == "bench3d") {  // n ncycles nu1 nu2 omega reps : one projection per rep, CUDA events
         int n = I(0), ncycles = I(1), nu1 = I(2), nu2 = I(3), reps = I(5);
         DTYPE w = (DTYPE)D(4);
@@ -365,10 +415,12 @@ int main(int argc, char** argv) {
         DTYPE *ddx = to_dev(std::vector<double>(n, 1.0 / n));
         CuMultigridFrac3D mg(ax, ay, az, dim, dx, 'n');
         CuWaveletPotentialRecover3D rec(dim, dx, 'n', WaveletType::WT_CDF3_7, WaveletType::WT_CDF4_6);
-        cudaEvent_t e0, e1;
+        cudaEvent_t e0, e1, es, eg;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        double best = 1e30, total = 0.0, maxdiv = 0.0, relres = 0.0;
+        cudaEventCreate(&es);
+        cudaEventCreate(&eg);
+        double best = 1e30, total = 0.0, maxdiv = 0.0, relres = 0.0, t_solve = 0.0, t_grad = 0.0, t_rec = 0.0;
         for (int r = 0; r < reps + 1; ++r) {
             checkCudaErrors(cudaMemcpy(ux, xv, sizeof(DTYPE) * sf, cudaMemcpyDeviceToDevice));
             checkCudaErrors(cudaMemcpy(uy, yv, sizeof(DTYPE) * sf, cudaMemcpyDeviceToDevice));
@@ -377,6 +429,7 @@ int main(int argc, char** argv) {
             cudaEventRecord(e0);
             CuConvergence::GetInstance()->GetB_3d_frac_vel(f, ux, uy, uz, ax, ay, az, dim, dx, 'n');
             mg.Solve(p, nullptr, f, ncycles, nu1, nu2, w);
+            cudaEventRecord(es);
             CuGradient::GetInstance()->Gradient3D_Frac_P(gx, gy, gz, p, ax, ay, az, dim, ddx, ddx, ddx, dx, 'n');
             CudaMatAdd(ux, gx, (int)sf, -1.f);
             CudaMatAdd(uy, gy, (int)sf, -1.f);
@@ -386,17 +439,29 @@ int main(int argc, char** argv) {
             CudaMatMul(ux, ux, ax, (int)sf);
             CudaMatMul(uy, uy, ay, (int)sf);
             CudaMatMul(uz, uz, az, (int)sf);
+            cudaEventRecord(eg);
             rec.Solve(qx, qy, qz, ux, uy, uz);
             cudaEventRecord(e1);
             checkCudaErrors(cudaEventSynchronize(e1));
-            float ms = 0.f;
+            float ms = 0.f, m0 = 0.f, m1 = 0.f, m2 = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            if (r > 0) { total += ms; if (ms < best) best = ms; }
+            cudaEventElapsedTime(&m0, e0, es);
+            cudaEventElapsedTime(&m1, es, eg);
+            cudaEventElapsedTime(&m2, eg, e1);
+            if (r > 0) {
+                total += ms;
+                if (ms < best) best = ms;
+                t_solve += m0;
+                t_grad += m1;
+                t_rec += m2;
+            }
         }
         relres = (double)mg.GetResdualError(p, f);
         printf("{\"n\": %d, \"ncycles\": %d, \"nu1\": %d, \"nu2\": %d, \"omega\": %g, \"reps\": %d, \"ms_best\": %.4f, "
-               "\"ms_mean\": %.4f, \"rel_residual\": %.3e, \"max_abs_div\": %.3e, \"dtype_bytes\": %d}\n",
-               n, ncycles, nu1, nu2, (double)w, reps, best, total / reps, relres, maxdiv, (int)sizeof(DTYPE));
+               "\"ms_mean\": %.4f, \"ms_divergence_and_solve\": %.4f, \"ms_gradient_update_maxdiv\": %.4f, "
+               "\"ms_recovery\": %.4f, \"rel_residual\": %.3e, \"max_abs_div\": %.3e, \"dtype_bytes\": %d}\n",
+               n, ncycles, nu1, nu2, (double)w, reps, best, total / reps, t_solve / reps, t_grad / reps, t_rec / reps,
+               relres, maxdiv, (int)sizeof(DTYPE));
     } else {
         fprintf(stderr, "unknown op %s\n", op.c_str());
         return 2;

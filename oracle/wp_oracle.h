@@ -107,7 +107,12 @@ void or_jacobi3d(double* dst, const double* src, const double* f, const double* 
 /* Dirichlet Poisson solve -lap_h p = f by DST-I in x, y, z (cuDst3D.cu:172-341) */
 void or_dst3d_poisson(double* p, const double* f, int nx, int ny, int nz, double dx, double dy, double dz);
 
+/* OpenMP threads of the parallel loops: set (n > 0) / query */
+void or_set_threads(int n);
+int or_get_threads(void);
+
 #ifdef __cplusplus
 }
 #endif
+
 #endif

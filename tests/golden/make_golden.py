@@ -9,6 +9,9 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only frac    # the sub-sampled face fraction cases only
     python tests/golden/make_golden.py --only sweep   # the fast sweeping cases only
     python tests/golden/make_golden.py --only cdf35   # the CDF3.5 transforms only
+    python tests/golden/make_golden.py --only dst     # CuDst3D::Solve only
+    python tests/golden/make_golden.py --only psweep  # CuParallelSweep3D Solve / Project only
+    ... [--out DIR]                                   # write the .npz files to DIR instead of here
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
 (CuWHHDForward::Solve1D, CuGetInnerProduct::GenerateIp, CuDivLocalProject3D::ProjectLocal_q_ccc,
@@ -43,13 +46,19 @@ def run(op, inputs: dict, params, outputs: dict):
         for k, v in inputs.items():
             np.ascontiguousarray(v, dtype=np.float64).tofile(os.path.join(tin, k + ".bin"))
         cmd = [DRIVER, op, tin, tout] + [str(p) for p in params]
-        subprocess.run(cmd, check=True, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=600)
+        r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=600, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout[-2000:] + r.stderr[-2000:])
+            raise subprocess.CalledProcessError(r.returncode, cmd)
         return {k: np.fromfile(os.path.join(tout, k + ".bin"), dtype=np.float64).reshape(s)
                 for k, s in outputs.items()}
 
 
+OUT_DIR = HERE
+
+
 def save(name, **arrays):
-    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+    np.savez_compressed(os.path.join(OUT_DIR, name + ".npz"), **arrays)
     print("wrote", name, {k: np.shape(v) for k, v in arrays.items()})
 
 
@@ -192,7 +201,58 @@ def cdf35_cases(rng):
     save("dwt1d_cdf35", **dwt)
 
 
+def dst_cases(rng):
+    """CuDst3D::Solve (the Dirichlet Poisson solve by DST-I along each axis, cuDst3D.cu:265-341) on
+    grids of equal extents (its constructor's buffer sizing is only safe there, cuDst3D.cu:209-211):
+    an even and an odd extent, unequal spacings."""
+    out = {}
+    for tag, n, d in (("15", 15, (1 / 16, 1 / 16, 1 / 16)), ("8", 8, (0.1, 0.07, 0.13))):
+        f = rng.standard_normal((n, n, n))
+        p = run("dst3d", {"f": f}, [n, n, n, *d], {"p": (n, n, n)})["p"]
+        out[f"f_{tag}"], out[f"p_{tag}"], out[f"d_{tag}"] = f, p, np.array(d)
+    save("dst3d", **out)
+
+
+def psweep_cases(rng):
+    """CuParallelSweep3D with bc 'n' (the reference's comparison baseline): Solve then Project on a
+    divergence-free field with no flux through the walls, as TestLocalProjection.cpp:719-721 calls
+    them, at 8^3 and 16^3 (a first 32^3 run in a fresh process left through the reference's CUDA
+    error exit and was not repeated); and the 2D Solve(qz, xv, yv) on a 32^2 field."""
+    from waveletpotentials_b200 import fields
+    out = {}
+    for n in (8, 16):
+        h = 1.0 / n
+        s = shapes3((n, n, n))
+        qx, qy, qz = (rng.standard_normal(s[k]) for k in ("qx", "qy", "qz"))
+        qx[0] = qx[-1] = 0
+        qx[:, :, 0] = qx[:, :, -1] = 0
+        qy[0] = qy[-1] = 0
+        qy[:, 0, :] = qy[:, -1, :] = 0
+        qz[:, 0, :] = qz[:, -1, :] = 0
+        qz[:, :, 0] = qz[:, :, -1] = 0
+        xv, yv, zv = fields.curl3d(qx, qy, qz, (n, n, n), (h, h, h))
+        res = run("psweep3d", {"xv": xv, "yv": yv, "zv": zv}, [n, h],
+                  {"qx_solve": s["qx"], "qy_solve": s["qy"], "qz_solve": s["qz"], "qx": s["qx"], "qy": s["qy"],
+                   "qz": s["qz"]})
+        out[f"xv_{n}"], out[f"yv_{n}"], out[f"zv_{n}"] = xv, yv, zv
+        for k, v in res.items():
+            out[f"{k}_{n}"] = v
+    n = 32
+    h = 1.0 / n
+    psi = rng.standard_normal((n + 1, n + 1))
+    psi[0] = psi[-1] = 0
+    psi[:, 0] = psi[:, -1] = 0
+    xv2, yv2 = fields.curl2d(psi, (n, n), (h, h))
+    out["qz2d"] = run("psweep2d", {"xv": xv2, "yv": yv2}, [n, h], {"qz": (n + 1, n + 1)})["qz"]
+    out["xv2d"], out["yv2d"] = xv2, yv2
+    save("psweep", **out)
+
+
 def main():
+    global OUT_DIR
+    if "--out" in sys.argv:
+        OUT_DIR = sys.argv[sys.argv.index("--out") + 1]
+        os.makedirs(OUT_DIR, exist_ok=True)
     if not os.path.exists(DRIVER):
         sys.exit(f"{DRIVER} missing: run make -C oracle/refharness first (needs nvcc and the reference sources)")
     only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
@@ -210,6 +270,12 @@ def main():
         return
     if only == "cdf35":
         cdf35_cases(np.random.default_rng(20261208))
+        return
+    if only == "dst":
+        dst_cases(np.random.default_rng(20261209))
+        return
+    if only == "psweep":
+        psweep_cases(np.random.default_rng(20261210))
         return
     rng = np.random.default_rng(20261203)
 

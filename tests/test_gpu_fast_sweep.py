@@ -48,3 +48,32 @@ def test_particles_to_ls_matches_reference_fixed_point(wp):
     ref = g["out_particles"]
     assert np.abs(N(ls) - ref).max() <= 1e-5 * np.abs(ref).max()
     assert np.array_equal(N(ls) > 0, ref > 0)
+
+
+def test_particles_to_ls_near_walls_matches_oracle(wp, oracle):
+    """Particles within half a cell of every wall and in the corners: the rough-distance cells
+    that would lie outside the grid are skipped (the reference indexes past the grid there), and
+    the GPU agrees with the oracle's FP64 restatement everywhere, with no write outside the grid
+    (the guard cells around the level set keep their sentinel)."""
+    n = (24, 20, 16)
+    h = 1.0 / 24
+    ext = np.array([n[0] * h, n[1] * h, n[2] * h])
+    e = 0.3 * h
+    pts = [[e, 0.5 * ext[1], 0.5 * ext[2]], [ext[0] - e, 0.4 * ext[1], 0.6 * ext[2]],
+           [0.5 * ext[0], e, 0.3 * ext[2]], [0.3 * ext[0], ext[1] - e, 0.5 * ext[2]],
+           [0.6 * ext[0], 0.5 * ext[1], e], [0.4 * ext[0], 0.6 * ext[1], ext[2] - e],
+           [e, e, e], [ext[0] - e, ext[1] - e, ext[2] - e], [e, ext[1] - e, e], [ext[0] - e, e, ext[2] - e],
+           [0.5 * ext[0], 0.5 * ext[1], 0.5 * ext[2]]]
+    xyz = np.asarray(pts, np.float32).astype(np.float64)
+    radius, max_dis, iters = 1.5 * h, 1.0, 60
+    ref = oracle.particles_to_ls(xyz, n, h, radius, max_dis, iters)
+    cells = n[0] * n[1] * n[2]
+    buf = torch.full((cells + 2 * 4096,), 12345.0, device="cuda")
+    ls = buf[4096:4096 + cells].view(n[2], n[0], n[1])
+    wp.CuFastSweeping.ParticlesToLs(ls, T(xyz), n, h, radius, max_dis, iters)
+    torch.cuda.synchronize()
+    got = N(ls)
+    assert np.all(N(buf[:4096]) == 12345.0) and np.all(N(buf[4096 + cells:]) == 12345.0)
+    assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+    sure = np.abs(ref) > 1e-6 * np.abs(ref).max()
+    assert np.array_equal((got > 0)[sure], (ref > 0)[sure])

@@ -120,7 +120,8 @@ def test_recover2d_matches_reference(wp, name):
 @pytest.mark.parametrize("n", [128, 256])
 def test_recover3d_reproduces_divergence_free_field_at_full_size(wp, n):
     """Size-independent property at the benchmark sizes: curl(recover(u)) == u for a discretely
-    divergence-free u with zero wall-normal flux (the oracle is too slow to run at 256^3)."""
+    divergence-free u with zero wall-normal flux (the field-by-field comparison with the oracle at
+    these sizes is in test_gpu_parity_fullsize.py)."""
     from waveletpotentials_b200 import fields
     rng = np.random.default_rng(n)
     nn = (n, n, n)

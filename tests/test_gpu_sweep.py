@@ -73,3 +73,24 @@ def test_sweep2d_matches_oracle(wp, oracle, n):
 def test_sweep_rejects_other_boundaries(wp):
     with pytest.raises(wp.WPError):
         wp.CuParallelSweep3D((8, 8, 8), 1.0 / 8, "d")
+
+
+@pytest.mark.parametrize("tag", ["15", "8"])
+def test_dst3d_matches_reference(wp, tag):
+    """The GPU's DST-I solve (handle and allocation-free entry points, FP64) against the reference
+    build's CuDst3D::Solve: within the FP32 rounding of the reference's transform constants."""
+    from conftest import load_golden
+    g = load_golden("dst3d")
+    f, p, d = g["f_" + tag], g["p_" + tag], tuple(float(v) for v in g["d_" + tag])
+    n = f.shape[0]
+    tf = torch.as_tensor(f, dtype=torch.float64, device="cuda")
+    out = torch.empty_like(tf)
+    dst = wp.CuDst3D((n, n, n), d)
+    dst.Solve(out, tf)
+    out2 = torch.empty_like(tf)
+    wp.CuDst3D.SolveNoAlloc(out2, tf, (n, n, n), d)
+    torch.cuda.synchronize()
+    for got in (out, out2):
+        g64 = got.cpu().numpy()
+        assert np.linalg.norm(g64 - p) <= 2e-7 * np.linalg.norm(p)
+    dst.close()

@@ -179,3 +179,15 @@ def test_mg2d_matches_reference_per_cycle(oracle):
                                       int(p["nu"][1]), float(p["omega"]))
     np.testing.assert_allclose(hist, p["hist"], rtol=1e-9)
     assert oracle.rel_l2(p["p"], sol) < 1e-11
+
+
+@pytest.mark.parametrize("tag", ["15", "8"])
+def test_dst3d_matches_reference(oracle, tag):
+    """CuDst3D::Solve (cuDst3D.cu:265-341) of the reference build: the oracle's exact DST-I agrees
+    to the FP32 rounding of the reference's transform constants (it forms sqrt(2/(n+1)) and
+    1/(n+1) in single precision even in its FP64 build, cuDst3D.cu:267-269, 314)."""
+    g = load_golden("dst3d")
+    f, p, d = g["f_" + tag], g["p_" + tag], tuple(float(v) for v in g["d_" + tag])
+    n = f.shape[0]
+    got = oracle.dst3d_poisson(f, (n, n, n), d)
+    assert np.linalg.norm(got - p) <= 2e-7 * np.linalg.norm(p)

@@ -77,6 +77,7 @@ SIGNATURES = {
     "wp_mgfrac3d_solve_tol": (I, [P, P, P, P, ctypes.POINTER(MgParams), ctypes.POINTER(MgReport), P]),
     "wp_mgfrac3d_residual": (I, [P, P, P, ctypes.POINTER(D), P]),
     "wp_mgfrac3d_iterate64": (I, [P, P, P]),
+    "wp_mgfrac3d_iterate64_view": (I, [P, P]),
     "wp_mgfrac3d_destroy": (I, [P]),
     "wp_mgfrac2d_create": (I, [PP, P, P, I, I, D, D, C, P]),
     "wp_mgfrac2d_solve": (I, [P, P, P, P, I, I, I, D, P]),
@@ -86,6 +87,7 @@ SIGNATURES = {
     "wp_divergence_frac3d": (I, [P, P, P, P, P, P, P, I, I, I, D, D, D, P]),
     "wp_divergence_frac2d": (I, [P, P, P, P, P, I, I, D, D, P]),
     "wp_grad_subtract_frac3d": (I, [P, P, P, P, P, P, P, I, I, I, D, D, D, I, P]),
+    "wp_grad_subtract_frac3d_p64": (I, [P, P, P, P, P, P, P, I, I, I, D, D, D, I, P]),
     "wp_grad_subtract_frac2d": (I, [P, P, P, P, P, I, I, D, D, I, P]),
     "wp_max_abs": (I, [P, S, ctypes.POINTER(D), P]),
     "wp_sdf_spheres3d": (I, [P, I, I, I, D, P, P, I, P]),

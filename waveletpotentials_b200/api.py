@@ -268,6 +268,12 @@ class CuMultigridFrac3D:
         check(lib().wp_mgfrac3d_set_tile(self._h, int(level), int(kind), int(zc), int(variant)),
               "wp_mgfrac3d_set_tile")
 
+    def Iterate64Ptr(self) -> int:
+        """Device address of the FP64 iterate of the last mixed / FP64 solve (no copy)."""
+        out = ctypes.c_void_p()
+        check(lib().wp_mgfrac3d_iterate64_view(self._h, ctypes.byref(out)), "wp_mgfrac3d_iterate64_view")
+        return int(out.value)
+
     def Iterate64(self, stream=None):
         """FP64 iterate of the last mixed / FP64 solve, as a numpy array."""
         t = torch.empty(self.cells, device="cuda", dtype=torch.float64)
@@ -377,6 +383,18 @@ class CuGradient:
                                             _ptr(ax, s["xv"]), _ptr(ay, s["yv"]), _ptr(az, s["zv"]), nx, ny, nz,
                                             *_dx3(dx), int(bool(multiply_frac)), _stream(stream)),
               "wp_grad_subtract_frac3d")
+
+    @staticmethod
+    def SubtractGradient3D_Frac_P64(xv, yv, zv, p64_ptr, ax, ay, az, dim, dx, multiply_frac=True, stream=None):
+        """The same update with an FP64 pressure given by its device address (the solver's FP64
+        iterate, CuMultigridFrac3D.Iterate64Ptr): formed in FP64, rounded once per face."""
+        nx, ny, nz = _dims3(dim)
+        s = mac_shapes3d(nx, ny, nz)
+        check(lib().wp_grad_subtract_frac3d_p64(_ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]),
+                                                ctypes.c_void_p(int(p64_ptr)), _ptr(ax, s["xv"]), _ptr(ay, s["yv"]),
+                                                _ptr(az, s["zv"]), nx, ny, nz, *_dx3(dx), int(bool(multiply_frac)),
+                                                _stream(stream)),
+              "wp_grad_subtract_frac3d_p64")
 
     @staticmethod
     def SubtractGradient2D_Frac_P(xv, yv, p, ax, ay, dim, dx, multiply_frac=True, stream=None):
@@ -636,8 +654,14 @@ class Projector3D:
                                      stream)
         else:
             rep = self.mg.SolveTol(self.p, pre_p, self.b, raise_on_fail=False, stream=stream, **self.opts)
-        CuGradient.SubtractGradient3D_Frac_P(xv, yv, zv, self.p, self.ax, self.ay, self.az, self.dim, self.dx,
-                                             multiply_frac=True, stream=stream)
+        if self.opts["precision"] != PREC_FP32:
+            # the gradient of the FP64 iterate, formed in FP64 (the FP32 copy's rounding, amplified by
+            # the 1/h of the difference, would dominate the projected field's divergence)
+            CuGradient.SubtractGradient3D_Frac_P64(xv, yv, zv, self.mg.Iterate64Ptr(), self.ax, self.ay, self.az,
+                                                   self.dim, self.dx, multiply_frac=True, stream=stream)
+        else:
+            CuGradient.SubtractGradient3D_Frac_P(xv, yv, zv, self.p, self.ax, self.ay, self.az, self.dim, self.dx,
+                                                 multiply_frac=True, stream=stream)
         # -div of the fraction-weighted projected field (open-face divergence of a (u - grad p))
         CuConvergence.GetB_3d_frac_vel(self.b, xv, yv, zv, None, None, None, self.dim, self.dx, stream=stream)
         rep["max_abs_div"] = max_abs(self.b, stream)

@@ -21,6 +21,7 @@ void wp_mg_forbid_persistent(wp_mgfrac3d* h);
 wp_status wp_mg_solve_tol_internal(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm, wp_mg_report* r,
                                    cudaStream_t s);
 const double* wp_mg_slots(const wp_mgfrac3d* h);
+const double* wp_mg_p64(const wp_mgfrac3d* h);
 wp_mgfrac3d* wp_mg2d_impl(wp_mgfrac2d* h);
 wp_status wp_max_abs_device(const float* x, size_t n, unsigned int* d_out, cudaStream_t s);
 
@@ -79,8 +80,9 @@ wp_status project_one(wp_batch* B, int i, float* xv, float* yv, float* zv, float
                                        h, s)) != WP_OK)
             return st;
         if ((st = wp_mg_solve_mixed_fixed_async(G.mg3, G.p, G.b, G.cycles, &B->prm, s)) != WP_OK) return st;
-        if ((st = wp_grad_subtract_frac3d(xv, yv, zv, G.p, G.frac[0], G.frac[1], G.frac[2], G.n[0], G.n[1], G.n[2], h, h,
-                                          h, 1, s)) != WP_OK)
+        // the gradient of the FP64 iterate, formed in FP64 (as the one-grid projector does)
+        if ((st = wp_grad_subtract_frac3d_p64(xv, yv, zv, wp_mg_p64(G.mg3), G.frac[0], G.frac[1], G.frac[2], G.n[0],
+                                              G.n[1], G.n[2], h, h, h, 1, s)) != WP_OK)
             return st;
         if ((st = wp_divergence_frac3d(G.b, xv, yv, zv, nullptr, nullptr, nullptr, G.n[0], G.n[1], G.n[2], h, h, h, s)) !=
             WP_OK)

@@ -196,7 +196,10 @@ __global__ void dst_matrix_kernel(double* __restrict__ M, int m) {
     M[i] = sqrt(2.0 / (m + 1)) * sinpi((double)r / (m + 1));
 }
 
-// Resolves the scratch address on the current device once (cudaGetSymbolAddress, checked).
+// Resolves the scratch address on the current device once (cudaGetSymbolAddress, checked).  The
+// address stays valid for the life of the device's primary context: after cudaDeviceReset (or any
+// teardown of that context) the cached value is stale, so the entry point is not to be called on
+// that device again in the same process.
 cudaError_t noalloc_scratch(double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

@@ -3862,6 +3862,15 @@ extern "C" CUWHHD_API wp_status wp_mgfrac3d_iterate64(wp_mgfrac3d* h, double* ds
     return WP_OK;
 }
 
+extern "C" CUWHHD_API wp_status wp_mgfrac3d_iterate64_view(wp_mgfrac3d* h, const double** out) {
+    if (!h || !out || h->last64 == 0) {
+        wp_set_error_msg("wp_mgfrac3d_iterate64_view: no FP64 iterate available");
+        return WP_ERR_INVALID_ARG;
+    }
+    *out = h->last64 == 1 ? h->p64 : h->lv[0].v64;
+    return WP_OK;
+}
+
 extern "C" CUWHHD_API wp_status wp_mgfrac3d_destroy(wp_mgfrac3d* h) {
     if (!h) return WP_OK;
     destroy_loop_graph(h);
@@ -4082,24 +4091,37 @@ wp_status autotune(wp_mgfrac3d* h, cudaStream_t s) {
         }
         h->mid_on = best_on;
     }
-    // level 0's V(2,2) cycle as the two fused passes or kernel by kernel: time a whole cycle from
-    // zero both ways (after an L2 flush when level 0 exceeds it); the fused passes only when they
-    // are clearly (5%) faster -- at 256^3 the two measure alike and the one-sweep kernels use the
-    // memory bandwidth better per byte
+    // level 0's V(2,2) cycle as the two fused passes or kernel by kernel: time both ways the pair of
+    // cycles of one refinement step of the mixed solve (a cycle from zero, then one whose last sweep
+    // adds into an FP64 iterate -- here a scratch array, not the handle's), after an L2 flush when
+    // level 0 exceeds it; the fused passes only when they are clearly (5%) faster -- at 256^3 the
+    // two measure alike and the one-sweep kernels use the memory bandwidth better per byte
     if (st == WP_OK && h->dims == 3 && h->nl >= 2 && h->lv[0].tuni) {
         Level& L0 = h->lv[0];
-        float ms[2] = {0.f, 0.f};
-        for (int on = 0; on < 2 && st == WP_OK; ++on) {
-            h->fz_on = on;
-            auto launch = [&]() {
-                vcycle<float>(h, 0, L0.f, 2, 2, 2.f / 3.f, WP_PROLONG_TRILINEAR, s, true);
-            };
-            ms[on] = time_launches(launch, s, ea, eb, 5, flush, flush ? kFlush : 0);
-            const cudaError_t e = cudaGetLastError();
-            if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
+        double* acc = nullptr;
+        if (cudaMalloc((void**)&acc, sizeof(double) * L0.cells) != cudaSuccess) {
+            cudaGetLastError();
+            acc = nullptr;
         }
-        h->fz_on = ms[1] < 0.95f * ms[0] ? 1 : 0;
-        ++h->tune_gen;
+        if (acc) {
+            cudaMemsetAsync(acc, 0, sizeof(double) * L0.cells, s);
+            float ms[2] = {0.f, 0.f};
+            for (int on = 0; on < 2 && st == WP_OK; ++on) {
+                h->fz_on = on;
+                auto launch = [&]() {
+                    vcycle<float>(h, 0, L0.f, 2, 2, 2.f / 3.f, WP_PROLONG_TRILINEAR, s, true);
+                    bool added = false;
+                    vcycle<float>(h, 0, L0.f, 2, 2, 2.f / 3.f, WP_PROLONG_TRILINEAR, s, false, acc, &added);
+                };
+                ms[on] = time_launches(launch, s, ea, eb, 5, flush, flush ? kFlush : 0);
+                const cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess) { wp_set_cuda_error(e, "autotune", __FILE__, __LINE__); st = WP_ERR_CUDA; break; }
+            }
+            cudaStreamSynchronize(s);
+            cudaFree(acc);
+            h->fz_on = ms[1] < 0.95f * ms[0] ? 1 : 0;
+            ++h->tune_gen;
+        }
     }
     if (flush) {
         cudaStreamSynchronize(s);
@@ -4188,4 +4210,6 @@ wp_status wp_mg_solve_tol_internal(wp_mgfrac3d* h, float* dst, const float* f, c
     return solve_tol(h, dst, nullptr, f, prm, r, s);
 }
 const double* wp_mg_slots(const wp_mgfrac3d* h) { return h->acc; }
+// the FP64 iterate of the mixed solve (wp_mg_solve_mixed_fixed_async leaves its result there)
+const double* wp_mg_p64(const wp_mgfrac3d* h) { return h->p64; }
 wp_mgfrac3d* wp_mg2d_impl(wp_mgfrac2d* h) { return h ? h->impl : nullptr; }

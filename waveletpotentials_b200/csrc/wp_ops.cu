@@ -52,43 +52,45 @@ __global__ void __launch_bounds__(256) div2d_kernel(float* __restrict__ b, const
         b[ix] = -((xv[ix + ny] - xv[ix]) * dxi + (yv[iy + 1] - yv[iy]) * dyi);
 }
 
-// u <- (u - grad p) [* a] on all faces; grad p = 0 on wall faces and where a <= eps
+// u <- (u - grad p) [* a] on all faces; grad p = 0 on wall faces and where a <= eps.  TP = double:
+// the pressure is the FP64 iterate and the update is formed in FP64, rounded once when stored.
+template <typename TP>
 __global__ void __launch_bounds__(256) grad3d_kernel(float* __restrict__ xv, float* __restrict__ yv, float* __restrict__ zv,
-                                                     const float* __restrict__ p, const float* __restrict__ ax,
+                                                     const TP* __restrict__ p, const float* __restrict__ ax,
                                                      const float* __restrict__ ay, const float* __restrict__ az,
-                                                     int nx, int ny, int nz, float gx, float gy, float gz, int mul) {
+                                                     int nx, int ny, int nz, TP gx, TP gy, TP gz, int mul) {
     const int y = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
     const long sp = (long)nx * ny;
     // x faces: (x in [0,nx], y in [0,ny), z in [0,nz))
     if (y < ny && x <= nx && z < nz) {
         const long i = y + (long)x * ny + (long)z * (nx + 1) * ny;
         const float a = ax[i];
-        float g = 0.f;
+        TP g = 0;
         if (x > 0 && x < nx && a > kEps) {
             const long ip = y + (long)x * ny + z * sp;
             g = (p[ip] - p[ip - ny]) * gx;
         }
-        float u = xv[i] - g;
-        xv[i] = mul ? u * a : u;
+        const TP u = (TP)xv[i] - g;
+        xv[i] = (float)(mul ? u * (TP)a : u);
     }
     if (y <= ny && x < nx && z < nz) {
         const long i = y + (long)x * (ny + 1) + (long)z * nx * (ny + 1);
         const float a = ay[i];
-        float g = 0.f;
+        TP g = 0;
         if (y > 0 && y < ny && a > kEps) {
             const long ip = y + (long)x * ny + z * sp;
             g = (p[ip] - p[ip - 1]) * gy;
         }
-        float u = yv[i] - g;
-        yv[i] = mul ? u * a : u;
+        const TP u = (TP)yv[i] - g;
+        yv[i] = (float)(mul ? u * (TP)a : u);
     }
     if (y < ny && x < nx && z <= nz) {
         const long i = y + (long)x * ny + (long)z * sp;
         const float a = az[i];
-        float g = 0.f;
+        TP g = 0;
         if (z > 0 && z < nz && a > kEps) g = (p[i] - p[i - sp]) * gz;
-        float u = zv[i] - g;
-        zv[i] = mul ? u * a : u;
+        const TP u = (TP)zv[i] - g;
+        zv[i] = (float)(mul ? u * (TP)a : u);
     }
 }
 
@@ -285,9 +287,26 @@ extern "C" CUWHHD_API wp_status wp_grad_subtract_frac3d(float* xv, float* yv, fl
     cudaStream_t s = (cudaStream_t)stream;
     const double faces = (double)(nx + 1) * ny * nz * 3, cells = (double)nx * ny * nz;
     WP_KERNEL("grad_subtract", 4.0 * (3 * faces + cells), s,
-              grad3d_kernel<<<grid, dim3(32, 8), 0, s>>>(xv, yv, zv, p, ax, ay, az, nx, ny, nz, (float)(2.0 / (dx + dx)),
-                                                         (float)(2.0 / (dy + dy)), (float)(2.0 / (dz + dz)),
-                                                         multiply_frac));
+              grad3d_kernel<float><<<grid, dim3(32, 8), 0, s>>>(xv, yv, zv, p, ax, ay, az, nx, ny, nz,
+                                                                (float)(2.0 / (dx + dx)), (float)(2.0 / (dy + dy)),
+                                                                (float)(2.0 / (dz + dz)), multiply_frac));
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_grad_subtract_frac3d_p64(float* xv, float* yv, float* zv, const double* p,
+                                                            const float* ax, const float* ay, const float* az, int nx,
+                                                            int ny, int nz, double dx, double dy, double dz,
+                                                            int multiply_frac, void* stream) {
+    if (!xv || !yv || !zv || !p || !ax || !ay || !az || nx <= 0 || ny <= 0 || nz <= 0 || nz >= 65535) {
+        wp_set_error_msg("wp_grad_subtract_frac3d_p64: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    dim3 grid(wp_cdiv(ny + 1, 32), wp_cdiv(nx + 1, 8), nz + 1);
+    cudaStream_t s = (cudaStream_t)stream;
+    const double faces = (double)(nx + 1) * ny * nz * 3, cells = (double)nx * ny * nz;
+    WP_KERNEL("grad_subtract", 4.0 * 3 * faces + 8.0 * cells, s,
+              grad3d_kernel<double><<<grid, dim3(32, 8), 0, s>>>(xv, yv, zv, p, ax, ay, az, nx, ny, nz, 2.0 / (dx + dx),
+                                                                 2.0 / (dy + dy), 2.0 / (dz + dz), multiply_frac));
     return WP_OK;
 }
 
@@ -689,14 +708,18 @@ extern "C" CUWHHD_API wp_status wp_particles_to_ls(float* ls, const float* xyz, 
     float* tmp = nullptr;
     WP_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * n, s));
     wp_status st = WP_OK;
+    // every launch reports through a lambda, so a failed one still reaches the scratch release below
     auto inv = [&]() -> wp_status {
         WP_KERNEL("inv_ls", 8.0 * n, s, inv_ls_kernel<<<gn, 256, 0, s>>>(ls, n, (float)max_dis));
         return WP_OK;
     };
-    if ((st = inv()) == WP_OK && (st = fsweep_iters(ls, tmp, nx, ny, nz, dx, n_iters, s)) == WP_OK &&
-        (st = inv()) == WP_OK && (st = fsweep_iters(ls, tmp, nx, ny, nz, dx, n_iters, s)) == WP_OK) {
+    auto negate = [&]() -> wp_status {
         WP_KERNEL("negate", 8.0 * n, s, negate_kernel<<<gn, 256, 0, s>>>(ls, n));
-    }
+        return WP_OK;
+    };
+    if ((st = inv()) == WP_OK && (st = fsweep_iters(ls, tmp, nx, ny, nz, dx, n_iters, s)) == WP_OK &&
+        (st = inv()) == WP_OK && (st = fsweep_iters(ls, tmp, nx, ny, nz, dx, n_iters, s)) == WP_OK)
+        st = negate();
     cudaFreeAsync(tmp, s);
     return st;
 }
