@@ -94,3 +94,37 @@ def test_dst3d_matches_reference(wp, tag):
         g64 = got.cpu().numpy()
         assert np.linalg.norm(g64 - p) <= 2e-7 * np.linalg.norm(p)
     dst.close()
+
+
+@pytest.mark.parametrize("n", [8, 16])
+def test_sweep_recovery_matches_reference(wp, n):
+    """The GPU's sweep + DST recovery (FP32 sweeps, FP64 DST) against the reference build's
+    CuParallelSweep3D Solve and Project on the same divergence-free field (within FP32 rounding of
+    the line integrals and, at 16^3, the reference's single-precision DST constants)."""
+    from conftest import load_golden
+    g = load_golden("psweep")
+    h = 1.0 / n
+    u = [_t(g[f"{k}_{n}"]) for k in ("xv", "yv", "zv")]
+    s = wp.mac_shapes3d(n, n, n)
+    q = [torch.zeros(s[k], device="cuda") for k in ("qx", "qy", "qz")]
+    sw = wp.CuParallelSweep3D((n, n, n), h, "n")
+    sw.Solve(*q, *u)
+    torch.cuda.synchronize()
+    for t, k in zip(q, ("qx", "qy", "qz")):
+        assert _rel(g[f"{k}_solve_{n}"], t.cpu().numpy()) < 2e-6
+    sw.Project(*q)
+    torch.cuda.synchronize()
+    for t, k in zip(q, ("qx", "qy", "qz")):
+        assert _rel(g[f"{k}_{n}"], t.cpu().numpy()) < 1e-5
+    sw.close()
+
+
+def test_sweep2d_matches_reference(wp):
+    """CuParallelSweep3D(int2, DTYPE2, 'n')::Solve(qz, xv, yv) of the reference build."""
+    from conftest import load_golden
+    g = load_golden("psweep")
+    n = 32
+    qz = torch.zeros((n + 1, n + 1), device="cuda")
+    wp.CuParallelSweep3D.Solve2D(qz, _t(g["xv2d"]), _t(g["yv2d"]), (n, n), 1.0 / n)
+    torch.cuda.synchronize()
+    assert _rel(g["qz2d"], qz.cpu().numpy()) < 2e-6

@@ -191,3 +191,32 @@ def test_dst3d_matches_reference(oracle, tag):
     n = f.shape[0]
     got = oracle.dst3d_poisson(f, (n, n, n), d)
     assert np.linalg.norm(got - p) <= 2e-7 * np.linalg.norm(p)
+
+
+@pytest.mark.parametrize("n", [8, 16])
+def test_sweep_recovery_matches_reference(oracle, n):
+    """CuParallelSweep3D with bc 'n' of the reference build (cuParallelSweep3D.cu:939-966 Solve,
+    :1043-1081 ProjectZero): the line sweeps agree exactly; the projection (a DST-I Poisson solve on
+    the (n-1)^3 interior nodes) agrees to the FP32 rounding of the reference's DST constants, which
+    vanishes at n = 8 where sqrt(2/(n-1+1)) = 1/2 is exact in single precision."""
+    g = load_golden("psweep")
+    h = 1.0 / n
+    nn, d = (n, n, n), (h, h, h)
+    u = [g[f"{k}_{n}"] for k in ("xv", "yv", "zv")]
+    qs = oracle.sweep3d_solve(*u, nn, d)
+    for a, k in zip(qs, ("qx", "qy", "qz")):
+        ref = g[f"{k}_solve_{n}"]
+        assert np.abs(a - ref).max() <= 1e-14 * np.abs(ref).max()
+    qp = oracle.sweep3d_project(*qs, nn, d)
+    tol = 1e-13 if n == 8 else 1e-6
+    for a, k in zip(qp, ("qx", "qy", "qz")):
+        ref = g[f"{k}_{n}"]
+        assert np.abs(a - ref).max() <= tol * np.abs(ref).max()
+
+
+def test_sweep2d_matches_reference(oracle):
+    """CuParallelSweep3D(int2, DTYPE2, 'n')::Solve(qz, xv, yv) (cuParallelSweep3D.cu:987-1000)."""
+    g = load_golden("psweep")
+    n = 32
+    qz = oracle.sweep2d_solve(g["yv2d"], (n, n), (1.0 / n, 1.0 / n))
+    assert np.abs(qz - g["qz2d"]).max() <= 1e-14 * np.abs(g["qz2d"]).max()
