@@ -39,7 +39,9 @@ typedef enum wp_status {
     WP_ERR_CUDA = 3,          /* a CUDA runtime call or launch failed */
     WP_ERR_WORKSPACE = 4,     /* caller workspace too small */
     WP_ERR_NOT_CONVERGED = 5, /* solve hit its cycle cap before the tolerance */
-    WP_ERR_NONFINITE = 6      /* NaN/Inf met in the input or residual */
+    WP_ERR_NONFINITE = 6,     /* NaN/Inf met in the input or residual */
+    WP_ERR_DEVICE_WAIT = 7    /* a bounded wait inside a kernel gave up; that call's outputs are invalid,
+                                 the handle stays usable */
 } wp_status;
 
 /* wavelet ids: same numeric values as the reference enum WaveletType (WaveletTypes.h:7-27) */
@@ -54,6 +56,17 @@ typedef enum wp_status {
 
 CUWHHD_API const char* wp_last_error(void);
 CUWHHD_API int wp_version(void);
+
+/* Test-only: arms one withheld arrival for the next launch at `site`, so that one wait in it runs
+   out after limit_seconds (in [1e-6, 2]) and the call returns WP_ERR_DEVICE_WAIT.  One shot.
+   WP_WAIT_SITE_GRID_BARRIER: the last CTA of the persistent below-finest multigrid cycle skips the
+   first grid barrier.  WP_WAIT_SITE_CONV_PIPELINE: the first CTA of the next tensor-core convolution
+   (forward or weight gradient) does not load pipeline step `at`.  site 0 disarms.  Every other wait
+   of that launch keeps its own limit; the kernels still wait for their copies in flight and free
+   their tensor memory before they return.  No reference counterpart. */
+#define WP_WAIT_SITE_GRID_BARRIER 1
+#define WP_WAIT_SITE_CONV_PIPELINE 2
+CUWHHD_API wp_status wp_debug_withhold_wait(int site, int at, double limit_seconds);
 
 /* Instrumentation (no reference counterpart): number of kernels this library has launched since
    the last reset, and optional per-kernel-class timing with CUDA events on the launching stream.
@@ -441,7 +454,9 @@ CUWHHD_API wp_status wp_batch_plan(wp_batch* h, const float* const* xv, const fl
 CUWHHD_API wp_status wp_batch_run(wp_batch* h, float* const* xv, float* const* yv, float* const* zv, float* const* qx,
                                   float* const* qy, float* const* qz, void* stream);
 /* Per grid: max|div u| after projection and the final FP64 relative residual of the last run;
-   any output may be NULL.  Synchronous. */
+   any output may be NULL.  Synchronous.  The replayed step counts are the plan's, so the tolerance
+   is tested again: WP_ERR_NOT_CONVERGED when any grid's residual is above rel_tol (all outputs
+   written; plan again on such inputs), WP_ERR_DEVICE_WAIT when a bounded device wait gave up. */
 CUWHHD_API wp_status wp_batch_results(wp_batch* h, double* max_abs_div, double* rel_residual, int* cycles,
                                       void* stream);
 CUWHHD_API wp_status wp_batch_destroy(wp_batch* h);

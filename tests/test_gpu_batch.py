@@ -134,3 +134,38 @@ def test_batch_rejects_bad_arguments(wp):
            "ay": torch.ones(s["yv"], device="cuda")}
     with pytest.raises(wp.WPError):
         wp.BatchProjector([bad], rel_tol=1e-6)
+
+
+def test_sharded_batch_shares_match_whole_batch(wp):
+    """The batch split by cost into two shares (both built here on one GPU, as two ranks would build
+    theirs): every grid lands in exactly one share, and each share's per-grid results and projected
+    fields equal those of the whole batch run as one."""
+    from waveletpotentials_b200 import sharding
+    tol = 1e-8
+    grids, u = _grids(wp)
+    whole = wp.BatchProjector(grids, rel_tol=tol, max_cycles=40, nstreams=4)
+    cycles = whole.plan(u)
+    fw = [[x.clone() for x in f] for f in u]
+    ow = _outs(wp, grids)
+    whole.run(fw, ow)
+    rw = whole.results()
+    shares = [sharding.ShardedBatch(grids, rank=r, world=2, rel_tol=tol, steps=cycles, max_cycles=40, nstreams=4)
+              for r in range(2)]
+    assert sorted(shares[0].mine + shares[1].mine) == list(range(len(grids)))
+    assert shares[0].owner == shares[1].owner
+    local = {}
+    for sh in shares:
+        fs = [[x.clone() for x in u[i]] for i in sh.mine]
+        os_ = [_outs(wp, [grids[i]])[0] for i in sh.mine]
+        assert sh.plan([u[i] for i in sh.mine]) == [cycles[i] for i in sh.mine]
+        sh.run(fs, os_)
+        local.update(sh.local_results())
+        for k, i in enumerate(sh.mine):
+            for a, b in zip(ow[i], os_[k]):
+                assert rel(N(a), N(b)) < 1e-6, i
+    merged = sharding.gather_results(local, len(grids), 1)
+    for i, m in enumerate(merged):
+        assert m["cycles"] == rw["cycles"][i] and m["over_tol"] is False
+        assert abs(m["rel_residual"] - rw["rel_residual"][i]) <= 1e-2 * rw["rel_residual"][i] + 1e-14
+    for sh in shares:
+        sh.close()

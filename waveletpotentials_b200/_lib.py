@@ -14,7 +14,9 @@ HEADER = os.path.join(HERE, "..", "include", "wp_api.h")
 
 WP_OK = 0
 STATUS = {0: "WP_OK", 1: "WP_ERR_INVALID_ARG", 2: "WP_ERR_UNSUPPORTED", 3: "WP_ERR_CUDA", 4: "WP_ERR_WORKSPACE",
-          5: "WP_ERR_NOT_CONVERGED", 6: "WP_ERR_NONFINITE"}
+          5: "WP_ERR_NOT_CONVERGED", 6: "WP_ERR_NONFINITE", 7: "WP_ERR_DEVICE_WAIT"}
+WP_ERR_NOT_CONVERGED, WP_ERR_NONFINITE, WP_ERR_DEVICE_WAIT = 5, 6, 7
+WAIT_SITE_GRID_BARRIER, WAIT_SITE_CONV_PIPELINE = 1, 2
 CDF4_6 = 7
 CDF3_7 = 11
 PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
@@ -51,6 +53,7 @@ PP = ctypes.POINTER(ctypes.c_void_p)
 SIGNATURES = {
     "wp_last_error": (ctypes.c_char_p, []),
     "wp_version": (I, []),
+    "wp_debug_withhold_wait": (I, [I, I, ctypes.c_double]),
     "wp_profile_enable": (None, [I]),
     "wp_profile_reset": (None, []),
     "wp_launch_count": (ctypes.c_longlong, []),

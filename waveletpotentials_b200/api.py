@@ -17,6 +17,7 @@ import torch
 
 from . import _lib
 from ._lib import START_FMG, START_ZERO  # noqa: F401
+from ._lib import WAIT_SITE_CONV_PIPELINE, WAIT_SITE_GRID_BARRIER  # noqa: F401
 from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONSTANT, PROLONG_TRILINEAR, MgParams, \
     MgReport, WPError, check, lib
 
@@ -776,6 +777,7 @@ class BatchProjector:
                  prolongation=PROLONG_TRILINEAR, nstreams=8, start=START_ZERO):
         self.grids = grids
         self.count = len(grids)
+        self.rel_tol = float(rel_tol)
         dims, ext, dx, ax, ay, az = [], [], [], [], [], []
         self.shapes = []
         for g in grids:
@@ -843,12 +845,21 @@ class BatchProjector:
               "wp_batch_run")
 
     def results(self, stream=None) -> dict:
+        """Per-grid max|div|, relative residual and step count of the last run.  The replay's step
+        counts are the plan's, so the tolerance is tested again: ``over_tol[i]`` is true for a grid
+        whose residual is above ``rel_tol`` and ``status`` is then ``WP_ERR_NOT_CONVERGED`` (plan
+        again on such inputs).  Any other failure raises."""
         m = (ctypes.c_double * self.count)()
         r = (ctypes.c_double * self.count)()
         cyc = (ctypes.c_int * self.count)()
-        check(lib().wp_batch_results(self._h, ctypes.cast(m, ctypes.c_void_p), ctypes.cast(r, ctypes.c_void_p),
-                                     ctypes.cast(cyc, ctypes.c_void_p), _stream(stream)), "wp_batch_results")
-        return {"max_abs_div": list(m), "rel_residual": list(r), "cycles": list(cyc)}
+        st = lib().wp_batch_results(self._h, ctypes.cast(m, ctypes.c_void_p), ctypes.cast(r, ctypes.c_void_p),
+                                    ctypes.cast(cyc, ctypes.c_void_p), _stream(stream))
+        if st != _lib.WP_ERR_NOT_CONVERGED:
+            check(st, "wp_batch_results")
+        rel = list(r)
+        over = [self.rel_tol > 0 and not (x <= self.rel_tol) for x in rel]
+        return {"max_abs_div": list(m), "rel_residual": rel, "cycles": list(cyc), "over_tol": over,
+                "status": _lib.STATUS.get(st, st)}
 
     def close(self):
         if getattr(self, "_h", None):
@@ -860,6 +871,15 @@ class BatchProjector:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ test-only failure injection
+def debug_withhold_wait(site, at=0, limit_s=1e-3):
+    """Test only: the next launch at ``site`` (``WAIT_SITE_GRID_BARRIER``: the persistent
+    below-finest multigrid cycle; ``WAIT_SITE_CONV_PIPELINE``: the tensor-core convolutions) leaves
+    one wait without its arrival, so that wait runs out after ``limit_s`` and the call that launched
+    it reports ``WP_ERR_DEVICE_WAIT``.  One shot; ``site`` 0 disarms (wp_debug_withhold_wait)."""
+    check(lib().wp_debug_withhold_wait(int(site), int(at), float(limit_s)), "wp_debug_withhold_wait")
 
 
 # ------------------------------------------------------------------ tensor-core convolutions

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <new>
 #include <vector>
 
@@ -43,12 +44,15 @@ struct Grid {
     wp_mgfrac3d* mg() const { return dims == 3 ? mg3 : wp_mg2d_impl(mg2); }
 };
 
+// per grid: max|div|, the FP64 relative residual of the last refinement step, and the MG handle's
+// device error flag (the int after its four norm slots; nonzero when a bounded wait gave up)
 __global__ void gather_results_kernel(double* out, const double* const* slots, const unsigned* maxbits, int count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const double* a = slots[i];
-    out[2 * i] = (double)__uint_as_float(maxbits[i]);
-    out[2 * i + 1] = a[1] > 0.0 ? sqrt(a[0] / a[1]) : 0.0;
+    out[3 * i] = (double)__uint_as_float(maxbits[i]);
+    out[3 * i + 1] = a[1] > 0.0 ? sqrt(a[0] / a[1]) : 0.0;
+    out[3 * i + 2] = (double)*reinterpret_cast<const int*>(a + 4);
 }
 
 }  // namespace
@@ -60,7 +64,7 @@ struct wp_batch {
     wp_mg_params prm;
     unsigned* d_max = nullptr;       // per grid: max|div| bits
     const double** d_slots = nullptr; // per grid: pointer to the MG handle's norm slots
-    double* d_out = nullptr;         // per grid: (max|div|, rel residual)
+    double* d_out = nullptr;         // per grid: (max|div|, rel residual, device error flag)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<const void*> bound;  // pointers captured into the graph
@@ -164,7 +168,7 @@ extern "C" CUWHHD_API wp_status wp_batch_create(wp_batch** out, int count, const
         for (int i = 0; i < count; ++i) slots[i] = wp_mg_slots(B->g[i].mg());
         cudaError_t e = cudaMalloc((void**)&B->d_max, sizeof(unsigned) * count);
         if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_slots, sizeof(double*) * count);
-        if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_out, sizeof(double) * 2 * count);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_out, sizeof(double) * 3 * count);
         if (e == cudaSuccess) e = cudaMemcpy(B->d_slots, slots.data(), sizeof(double*) * count, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) { wp_set_cuda_error(e, "batch alloc", __FILE__, __LINE__); st = WP_ERR_CUDA; }
     }
@@ -266,19 +270,42 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
     return WP_OK;
 }
 
-// Per grid (max|div| of the projected field, final FP64 relative residual); synchronous.
+// Per grid (max|div| of the projected field, final FP64 relative residual); synchronous.  The
+// replayed step counts were fixed by the plan, so the tolerance is tested again here: a grid whose
+// residual is above it makes the call return WP_ERR_NOT_CONVERGED (every output still written).
+// A bounded device wait that gave up in any grid's solve takes precedence (WP_ERR_DEVICE_WAIT; its
+// flag is cleared).
 extern "C" CUWHHD_API wp_status wp_batch_results(wp_batch* B, double* max_abs_div, double* rel_residual,
                                                  int* cycles, void* stream) {
     if (!B) { wp_set_error_msg("wp_batch_results: null handle"); return WP_ERR_INVALID_ARG; }
     const int count = (int)B->g.size();
-    std::vector<double> out(2 * count);
+    std::vector<double> out(3 * count);
     cudaStream_t s = (cudaStream_t)stream;
-    WP_CUDA_TRY(wp_read_small(out.data(), B->d_out, sizeof(double) * 2 * count, s));
+    WP_CUDA_TRY(wp_read_small(out.data(), B->d_out, sizeof(double) * 3 * count, s));
     WP_CUDA_TRY(cudaStreamSynchronize(s));
+    int over = 0, waits = 0;
     for (int i = 0; i < count; ++i) {
-        if (max_abs_div) max_abs_div[i] = out[2 * i];
-        if (rel_residual) rel_residual[i] = out[2 * i + 1];
+        if (max_abs_div) max_abs_div[i] = out[3 * i];
+        if (rel_residual) rel_residual[i] = out[3 * i + 1];
         if (cycles) cycles[i] = B->g[i].cycles;
+        if (B->prm.rel_tol > 0.0 && !(out[3 * i + 1] <= B->prm.rel_tol)) ++over;
+        if (out[3 * i + 2] != 0.0) {
+            ++waits;
+            WP_CUDA_TRY(cudaMemsetAsync((void*)(wp_mg_slots(B->g[i].mg()) + 4), 0, sizeof(int), s));
+        }
+    }
+    char msg[160];
+    if (waits) {
+        WP_CUDA_TRY(cudaStreamSynchronize(s));
+        snprintf(msg, sizeof(msg), "wp_batch_results: a bounded device wait gave up in %d grid(s)", waits);
+        wp_set_error_msg(msg);
+        return WP_ERR_DEVICE_WAIT;
+    }
+    if (over) {
+        snprintf(msg, sizeof(msg), "wp_batch_results: %d grid(s) above the relative tolerance %g after replay", over,
+                 B->prm.rel_tol);
+        wp_set_error_msg(msg);
+        return WP_ERR_NOT_CONVERGED;
     }
     return WP_OK;
 }

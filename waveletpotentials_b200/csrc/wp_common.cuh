@@ -37,6 +37,10 @@ static inline bool wp_is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 static inline int wp_half_up(int n) { return (n & 1) ? (n >> 1) + 1 : (n >> 1); }
 static inline unsigned wp_cdiv(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
 
+// Test-only withheld arrival armed by wp_debug_withhold_wait for `site`: true once (then disarmed),
+// with the index of the withheld arrival and the wait limit in nanoseconds; never while s is capturing.
+bool wp_take_withhold(int site, cudaStream_t s, int* at, unsigned long long* limit_ns);
+
 // Number of SMs of the current device (cached per process; 148 on B200).
 int wp_sm_count();
 

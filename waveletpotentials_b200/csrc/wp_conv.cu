@@ -66,13 +66,22 @@ struct TileGeo {
     int yt, xt, nty, ntx;
 };
 
+// After a pipeline wait gave up: waits (bounded) for the tile loads issued but never consumed, steps
+// [consumed, issued) of the ring of full barriers, so that no copy into this CTA's shared memory is
+// in flight when it exits.  The withheld step was never issued.
+__device__ __forceinline__ void drain_copies(uint32_t bar_full, int stages, int consumed, int issued, int withheld,
+                                             int* err) {
+    for (int k = consumed; k < issued; ++k)
+        if (k != withheld && !mbar_wait(bar_full + 8 * (k % stages), (k / stages) & 1, err)) return;
+}
+
 template <int COUT>
 __global__ void __launch_bounds__(kThreads, 1)
     conv3_fwd_kernel(const __grid_constant__ CUtensorMap xm0, const __grid_constant__ CUtensorMap wm0,
                      const __grid_constant__ CUtensorMap xm1, const __grid_constant__ CUtensorMap wm1, int cin0,
                      int cin1, int nparts, __nv_bfloat16* __restrict__ out, const float* __restrict__ bias,
                      const __nv_bfloat16* __restrict__ addend, const __nv_bfloat16* __restrict__ mask, int relu, int nx,
-                     int ny, int nz, TileGeo tg, int* err) {
+                     int ny, int nz, TileGeo tg, int* err, int withhold, unsigned long long lim) {
     constexpr int NCOL = COUT < 32 ? 32 : COUT;
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -82,8 +91,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t bar_empty = bar_full + 8 * kStagesF;
     const uint32_t bar_acc = bar_empty + 8 * kStagesF;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(basep + kStagesF * (kSlotA + kSlotB) + 16 * kStagesF + 8);
+    volatile int* s_consumed = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(tmem_slot + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (blockIdx.x != 0) withhold = -1;
     long t = blockIdx.x;
     const int ty = (int)(t % tg.nty);
     t /= tg.nty;
@@ -109,10 +121,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t tmem = *tmem_slot;
     const int nk = 27 * nparts;
 
+    int issued = 0;
     if (warp == 0 && lane == 0) {
         for (int k = 0; k < nk; ++k) {
             const int s = k % kStagesF;
-            if (!mbar_wait(bar_empty + 8 * s, ((k / kStagesF) & 1) ^ 1, err)) break;
+            if (!mbar_wait(bar_empty + 8 * s, ((k / kStagesF) & 1) ^ 1, err, lim)) break;
+            issued = k + 1;
+            if (k == withhold) continue;
             const int part = k / 27, tap = k % 27;
             const int cin = part ? cin1 : cin0;
             const int dz = tap / 9, dx = (tap / 3) % 3, dy = tap % 3;
@@ -123,10 +138,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp == 1 && lane == 0) {
         constexpr uint32_t idesc = idesc_bf16_f32(128, COUT, 0, 0);
-        bool ok = true;
-        for (int k = 0; k < nk; ++k) {
+        int k = 0;
+        for (; k < nk; ++k) {
             const int s = k % kStagesF;
-            if (!mbar_wait(bar_full + 8 * s, (k / kStagesF) & 1, err)) { ok = false; break; }
+            if (!mbar_wait(bar_full + 8 * s, (k / kStagesF) & 1, err, lim)) break;
             tc_fence_after();
             const int cin = (k / 27) ? cin1 : cin0;
             const uint32_t rowb = (uint32_t)cin * 2, lay = sw_code(cin * 2);
@@ -138,11 +153,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             umma_commit(bar_empty + 8 * s);
         }
-        if (ok) umma_commit(bar_acc);
-    } else if (warp >= 2) {
+        *s_consumed = k;
+        *s_fail = k < nk;
+        umma_commit(bar_acc);  // also on failure: bar_acc then tracks the MMAs already issued
+    }
+    bool ready = false;
+    if (warp >= 2) ready = mbar_wait(bar_acc, 0, err);
+    __syncthreads();
+    if (warp == 0 && lane == 0) drain_copies(bar_full, kStagesF, *s_consumed, issued, withhold, err);
+    if (warp >= 2) {
         const int q = warp & 3;
         const int m = q * 32 + lane;
-        const bool ready = mbar_wait(bar_acc, 0, err);
+        ready = ready && !*s_fail;
         __syncwarp();  // tcgen05.ld is warp-collective
         tc_fence_after();
         float acc[COUT];
@@ -187,7 +209,7 @@ template <int COUT>
 __global__ void __launch_bounds__(kThreads, 1)
     conv3_wgrad_kernel(const __grid_constant__ CUtensorMap xm, const __grid_constant__ CUtensorMap gm, int cin,
                        float* __restrict__ dw, int nx, int ny, int nz, TileGeo tg, long ntiles, int tiles_per_cta,
-                       int* err) {
+                       int* err, int withhold, unsigned long long lim) {
     constexpr int NCOL = COUT < 32 ? 32 : COUT;
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -197,8 +219,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t bar_empty = bar_full + 8 * kStagesW;
     const uint32_t bar_acc = bar_empty + 8 * kStagesW;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(basep + kStagesW * (kSlotWA + kSlotWB) + 16 * kStagesW + 8);
+    volatile int* s_consumed = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(tmem_slot + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (blockIdx.x != 0 || blockIdx.y != 0) withhold = -1;
     const int tpg = 128 / cin;             // taps per CTA (one M tile of 128 rows)
     const int tap0 = blockIdx.x * tpg;
     const int ntap = min(tpg, 27 - tap0);
@@ -222,10 +247,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
+    int issued = 0;
     if (warp == 0 && lane == 0) {
         for (int k = 0; k < nk; ++k) {
             const int s = k % kStagesW;
-            if (!mbar_wait(bar_empty + 8 * s, ((k / kStagesW) & 1) ^ 1, err)) break;
+            if (!mbar_wait(bar_empty + 8 * s, ((k / kStagesW) & 1) ^ 1, err, lim)) break;
+            issued = k + 1;
+            if (k == withhold) continue;
             long t = k0 + k;
             const int ty = (int)(t % tg.nty);
             t /= tg.nty;
@@ -245,10 +273,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         constexpr uint32_t idesc = idesc_bf16_f32(128, COUT, 1, 1);
         const uint32_t rowa = (uint32_t)cin * 2, laya = sw_code(cin * 2);
         constexpr uint32_t rowb = COUT * 2, layb = sw_code(COUT * 2);
-        bool ok = nk > 0;
-        for (int k = 0; k < nk; ++k) {
+        int k = 0;
+        for (; k < nk; ++k) {
             const int s = k % kStagesW;
-            if (!mbar_wait(bar_full + 8 * s, (k / kStagesW) & 1, err)) { ok = false; break; }
+            if (!mbar_wait(bar_full + 8 * s, (k / kStagesW) & 1, err, lim)) break;
             tc_fence_after();
             const uint32_t a = base + s * (kSlotWA + kSlotWB), b = a + kSlotWA;
 #pragma unroll
@@ -259,11 +287,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             umma_commit(bar_empty + 8 * s);
         }
-        if (ok) umma_commit(bar_acc);
-    } else if (warp >= 2) {
+        *s_consumed = k;
+        *s_fail = k < nk || nk <= 0;
+        umma_commit(bar_acc);  // also on failure: bar_acc then tracks the MMAs already issued
+    }
+    bool ready = false;
+    if (warp >= 2) ready = mbar_wait(bar_acc, 0, err);
+    __syncthreads();
+    if (warp == 0 && lane == 0) drain_copies(bar_full, kStagesW, *s_consumed, issued, withhold, err);
+    if (warp >= 2) {
         const int q = warp & 3;
         const int m = q * 32 + lane;
-        const bool ready = nk > 0 && mbar_wait(bar_acc, 0, err);
+        ready = ready && !*s_fail;
         __syncwarp();  // tcgen05.ld is warp-collective
         tc_fence_after();
         float acc[COUT];
@@ -348,12 +383,15 @@ cudaError_t launch_fwd(const CUtensorMap& x0, const CUtensorMap& w0, const CUten
                        const __nv_bfloat16* addend, const __nv_bfloat16* mask, int relu, int nx, int ny, int nz,
                        TileGeo tg, int* err, cudaStream_t s) {
     const size_t smem = 1024 + kStagesF * (kSlotA + kSlotB) + 16 * kStagesF + 32;
+    int wh = -1;
+    unsigned long long lim = wptc::kWaitLimitNs;
+    if (!wp_take_withhold(WP_WAIT_SITE_CONV_PIPELINE, s, &wh, &lim)) wh = -1;
     auto k = conv3_fwd_kernel<COUT>;
     cudaError_t e = wp_set_smem(k, smem);
     if (e != cudaSuccess) return e;
     const long tiles = (long)tg.nty * tg.ntx * nz;
     k<<<(unsigned)tiles, kThreads, smem, s>>>(x0, w0, x1, w1, cin0, cin1, nparts, out, bias, addend, mask, relu, nx, ny,
-                                              nz, tg, err);
+                                              nz, tg, err, wh, lim);
     return cudaGetLastError();
 }
 
@@ -361,6 +399,9 @@ template <int COUT>
 cudaError_t launch_wgrad(const CUtensorMap& xm, const CUtensorMap& gm, int cin, float* dw, int nx, int ny, int nz,
                          TileGeo tg, int* err, cudaStream_t s) {
     const size_t smem = 1024 + kStagesW * (kSlotWA + kSlotWB) + 16 * kStagesW + 32;
+    int wh = -1;
+    unsigned long long lim = wptc::kWaitLimitNs;
+    if (!wp_take_withhold(WP_WAIT_SITE_CONV_PIPELINE, s, &wh, &lim)) wh = -1;
     auto k = conv3_wgrad_kernel<COUT>;
     cudaError_t e = wp_set_smem(k, smem);
     if (e != cudaSuccess) return e;
@@ -371,7 +412,7 @@ cudaError_t launch_wgrad(const CUtensorMap& xm, const CUtensorMap& gm, int cin, 
     if (chunks > ntiles) chunks = ntiles;
     const int per = (int)((ntiles + chunks - 1) / chunks);
     chunks = (ntiles + per - 1) / per;
-    k<<<dim3(groups, (unsigned)chunks), kThreads, smem, s>>>(xm, gm, cin, dw, nx, ny, nz, tg, ntiles, per, err);
+    k<<<dim3(groups, (unsigned)chunks), kThreads, smem, s>>>(xm, gm, cin, dw, nx, ny, nz, tg, ntiles, per, err, wh, lim);
     return cudaGetLastError();
 }
 
@@ -386,8 +427,8 @@ wp_status wp_conv_check_error(cudaStream_t s) {
     WP_CUDA_TRY(cudaStreamSynchronize(s));
     if (h) {
         cudaMemsetAsync(e, 0, sizeof(int), s);
-        wp_set_error_msg("tensor-core convolution: a pipeline wait timed out");
-        return WP_ERR_CUDA;
+        wp_set_error_msg("tensor-core convolution: a pipeline wait gave up; the outputs of the call are invalid");
+        return WP_ERR_DEVICE_WAIT;
     }
     return WP_OK;
 }

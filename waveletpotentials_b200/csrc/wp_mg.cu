@@ -1834,13 +1834,15 @@ struct MidPack {
     float w;
     unsigned* bar;  // [arrivals, generation]
     int* err;
+    int withhold;             // test only: 1 = the last CTA skips the first barrier
+    unsigned long long lim;   // wait limit of the barriers, ns
 };
 static_assert(sizeof(MidPack) < 32000, "kernel parameters are limited to 32 KB");
 
 // Grid-wide barrier of a cooperative launch (all CTAs resident): arrivals counted on bar[0], the last
 // one resets it and advances the generation bar[1], the others wait for that (bounded: after
-// kWaitLimitNs the error flag is raised and false returned, and the grid leaves the kernel).
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks, int* err) {
+// lim ns the error flag is raised and false returned, and the grid leaves the kernel).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks, int* err, unsigned long long lim) {
     __syncthreads();
     int ok = 1;
     if (threadIdx.x == 0) {
@@ -1854,7 +1856,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks, in
         } else {
             const unsigned long long t0 = wptc::globaltimer();
             while (*gen == g) {
-                if (wptc::globaltimer() - t0 > wptc::kWaitLimitNs) {
+                if (wptc::globaltimer() - t0 > lim) {
                     atomicOr(err, 2);
                     ok = 0;
                     break;
@@ -1894,7 +1896,8 @@ __global__ void __launch_bounds__(1024, 1) mid_cycle_kernel(MidPack P) {
                 }
             }
         }
-        if (k + 1 < P.nph && !grid_barrier(P.bar, gridDim.x, P.err)) return;
+        if (k == 0 && P.withhold && blockIdx.x == gridDim.x - 1) return;
+        if (k + 1 < P.nph && !grid_barrier(P.bar, gridDim.x, P.err, P.lim)) return;
     }
 }
 
@@ -2976,6 +2979,9 @@ wp_status mid_cycle(wp_mgfrac3d* h, int l1, int nu1, int nu2, float w, int prolo
     P.w = w;
     P.err = reinterpret_cast<int*>(h->acc + 4);
     P.bar = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(h->acc + 4) + 8);
+    int wh_at = 0;
+    P.lim = wptc::kWaitLimitNs;
+    P.withhold = wp_take_withhold(WP_WAIT_SITE_GRID_BARRIER, s, &wh_at, &P.lim) ? 1 : 0;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(h->mid_grid);
     cfg.blockDim = dim3(1024);
@@ -3231,6 +3237,22 @@ wp_status defect_async(wp_mgfrac3d* h, const TP* p, const float* f, double m, co
     return WP_OK;
 }
 
+// Turns the handle's device error flag (a grid barrier or a pipeline wait that gave up) into a status,
+// clearing it: the call that saw it fails with WP_ERR_DEVICE_WAIT, the handle stays usable.
+wp_status device_wait_status(wp_mgfrac3d* h, int flag, cudaStream_t s) {
+    if (!flag) return WP_OK;
+    WP_CUDA_TRY(cudaMemsetAsync(h->acc + 4, 0, sizeof(int), s));
+    wp_set_error_msg(flag & 2 ? "multigrid: a grid barrier wait gave up; the iterate of this call is invalid"
+                              : "multigrid: a tile pipeline wait gave up; the iterate of this call is invalid");
+    return WP_ERR_DEVICE_WAIT;
+}
+
+wp_status check_device_wait(wp_mgfrac3d* h, cudaStream_t s) {
+    int flag = 0;
+    WP_CUDA_TRY(wp_read_small(&flag, h->acc + 4, sizeof(int), s));
+    return device_wait_status(h, flag, s);
+}
+
 template <typename TP>
 wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r32, double* norm_r2,
                  double* norm_f2, cudaStream_t s) {
@@ -3243,11 +3265,15 @@ wp_status defect(wp_mgfrac3d* h, const TP* p, const float* f, double m, float* r
         const unsigned b = std::min<unsigned>(wp_cdiv(L.cells, 256), wp_sm_count() * 8);
         WP_KERNEL("sumsq", 4.0 * L.cells, s, sumsq_kernel<float><<<b, 256, 0, s>>>(f, L.cells, h->acc + 1));
     }
-    double hv[2];
-    WP_CUDA_TRY(wp_read_small(hv, h->acc, sizeof(hv), s));
-    *norm_r2 = hv[0];
-    if (norm_f2) *norm_f2 = hv[1];
-    return WP_OK;
+    // the two sums and, in the same read, the device error flag that follows the four slots
+    struct {
+        double v[4];
+        int err;
+    } hv;
+    WP_CUDA_TRY(wp_read_small(&hv, h->acc, 4 * sizeof(double) + sizeof(int), s));
+    *norm_r2 = hv.v[0];
+    if (norm_f2) *norm_f2 = hv.v[1];
+    return device_wait_status(h, hv.err, s);
 }
 
 void destroy_levels(wp_mgfrac3d* h) {
@@ -3307,7 +3333,7 @@ wp_status solve_fixed(wp_mgfrac3d* h, float* dst, const float* pre_v, const floa
         if (st != WP_OK) return st;
     }
     WP_CUDA_TRY(cudaMemcpyAsync(dst, L.v, sizeof(float) * L.cells, cudaMemcpyDeviceToDevice, s));
-    return WP_OK;
+    return check_device_wait(h, s);
 }
 
 // The index lists of every level (InitIndex, cuMultigridFrac3D.cu:189-229) and the zeroed residual
@@ -3761,6 +3787,7 @@ wp_status solve_tol(wp_mgfrac3d* h, float* dst, const float* pre_v, const float*
         return WP_ERR_INVALID_ARG;
     }
     if (rep) *rep = r;
+    if ((st = check_device_wait(h, s)) != WP_OK) return st;
     if (!std::isfinite(r.rel_residual)) { wp_set_error_msg("multigrid: non-finite residual"); return WP_ERR_NONFINITE; }
     if (use_tol && r.rel_residual > prm->rel_tol) { wp_set_error_msg("multigrid: cycle cap reached before tolerance"); return WP_ERR_NOT_CONVERGED; }
     return WP_OK;

@@ -53,14 +53,15 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for the phase of the given parity; after kWaitLimitNs sets *err and returns false.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err) {
+// Waits for the phase of the given parity; after limit_ns sets *err and returns false.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err,
+                                          unsigned long long limit_ns = kWaitLimitNs) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = globaltimer();
     for (;;) {
         for (int k = 0; k < 256; ++k)
             if (mbar_try(bar, parity)) return true;
-        if (globaltimer() - t0 > kWaitLimitNs) {
+        if (globaltimer() - t0 > limit_ns) {
             atomicOr(err, 1);
             return false;
         }

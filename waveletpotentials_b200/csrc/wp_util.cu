@@ -32,6 +32,42 @@ extern "C" CUWHHD_API const char* wp_last_error(void) { return g_err; }
 extern "C" CUWHHD_API int wp_version(void) { return 1; }
 
 // ---------------------------------------------------------------------------------------------
+// Test-only withheld arrival: the next launch at the armed site leaves one wait without the arrival
+// it waits for, so that wait runs out after the given limit.  One shot: taking it disarms it; a launch
+// that is being captured into a graph does not take it.
+#include <mutex>
+
+namespace {
+std::mutex g_wh_mu;
+int g_wh_site = 0, g_wh_at = 0;
+unsigned long long g_wh_ns = 0;
+}  // namespace
+
+bool wp_take_withhold(int site, cudaStream_t s, int* at, unsigned long long* limit_ns) {
+    // never into a captured graph: every replay would withhold again
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+    std::lock_guard<std::mutex> lk(g_wh_mu);
+    if (g_wh_site == 0 || g_wh_site != site) return false;
+    *at = g_wh_at;
+    *limit_ns = g_wh_ns;
+    g_wh_site = 0;
+    return true;
+}
+
+extern "C" CUWHHD_API wp_status wp_debug_withhold_wait(int site, int at, double limit_seconds) {
+    if (site < 0 || site > WP_WAIT_SITE_CONV_PIPELINE || at < 0 || !(limit_seconds >= 1e-6 && limit_seconds <= 2.0)) {
+        wp_set_error_msg("wp_debug_withhold_wait: site 0..2, at >= 0, limit in [1e-6, 2] s");
+        return WP_ERR_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_wh_mu);
+    g_wh_site = site;
+    g_wh_at = at;
+    g_wh_ns = (unsigned long long)(limit_seconds * 1e9);
+    return WP_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Launch accounting and optional per-kernel-class timing with CUDA events recorded on the
 // launching stream.  Counting is always on (one relaxed atomic per launch); event timing only
 // between wp_profile_enable(1) and wp_profile_enable(0).
