@@ -26,8 +26,10 @@
 
 namespace {
 
-constexpr int CH = 8;        // coefficient pairs per thread per level
-constexpr int WIN = CH + 8;  // register window (4-pair halo on each side)
+// Coefficient pairs per thread per level: 8, or 9 for CDF4.6, whose lines have 2^L + 1 samples in the
+// recovery: the 2^(L-1) + 1 approximations of the top level then split into 15 chunks (two rounds of
+// a 256-thread tile of 32 columns) instead of 17 (three rounds, the last one eighth full).
+__host__ __device__ constexpr int ch_of(int wav) { return wav == WP_ID_CDF4_6 ? 9 : 8; }
 constexpr int NT = 256;      // threads per CTA
 
 // lifting constants (cuWaveletCompute.cuh:13-23, :139-148)
@@ -163,18 +165,41 @@ struct TileGeom {
 // Reflection tables: for every level, the (index, sign) of each pair a boundary window reads,
 // k = -4 .. nch CH + 3 (entry k + 4), computed once per CTA; a boundary window then costs one table
 // read per tap instead of the reflection rules.  Entries per level: nch CH + 8.
-__host__ __device__ inline int rt_level_entries(int M) { return (M + CH - 1) / CH * CH + 8; }
-__host__ __device__ inline int rt_entries(int N, int levels, bool fwd) {
+__host__ __device__ inline int rt_level_entries(int M, int ch) { return (M + ch - 1) / ch * ch + 8; }
+__host__ __device__ inline int rt_entries(int N, int levels, bool fwd, int ch) {
     const int ext = N & 1;
     int e = 0;
-    for (int l = 2; l < levels; ++l) e += rt_level_entries(fwd ? (1 << l) + ext : (1 << l) + ext);
+    for (int l = 2; l < levels; ++l) e += rt_level_entries(fwd ? (1 << l) + ext : (1 << l) + ext, ch);
     return e;
 }
 __host__ __device__ inline size_t rt_offset(size_t buf_bytes) { return (buf_bytes + 15) / 16 * 16; }
 
+// base-level matrix (nb = 4 or 5) on one column: in[i * pitch] -> out[i * pitch], unrolled so that
+// the coefficients stay in registers
+template <typename T, int NB>
+__device__ __forceinline__ void base_level_n(const double* mat, const T* in, T* out, int pitch) {
+    T a[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) a[i] = in[i * pitch];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        T s = T(0);
+#pragma unroll
+        for (int j = 0; j < NB; ++j) s += T(mat[i * NB + j]) * a[j];
+        out[i * pitch] = s;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void base_level(const double* mat, int nb, const T* in, T* out, int pitch) {
+    if (nb == 5) base_level_n<T, 5>(mat, in, out, pitch);
+    else base_level_n<T, 4>(mat, in, out, pitch);
+}
+
 template <int WAV, bool FWD, typename T, int C>
 __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src, T* __restrict__ dst, int N,
                                                       int levels, int bcd, TileGeom g) {
+    constexpr int CH = ch_of(WAV);
+    constexpr int WIN = CH + 8;  // register window (4-pair halo on each side)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
     constexpr int CP = C + 1;
@@ -182,14 +207,17 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
     const int ext = N & 1;
     const int i0 = blockIdx.x * C;
     const long obase = (long)blockIdx.y * g.s_out;
-    T* buf[3] = {sm, sm + (size_t)N * CP, sm + 2 * (size_t)N * CP};
+    // the three staging buffers, addressed arithmetically (an array of pointers indexed by a run-time
+    // buffer number would live in local memory)
+    const size_t bstride = (size_t)N * CP;
+    auto buf = [sm, bstride](int i) { return sm + (size_t)i * bstride; };
 
     // ---- reflection tables of every level (see rt_entries), ascending level order
     int4* rt = reinterpret_cast<int4*>(smem_raw + rt_offset((size_t)(FWD ? 2 : 3) * N * CP * sizeof(T)));
     {
         int off = 0;
         for (int l = 2; l < levels; ++l) {
-            const int ne = rt_level_entries((1 << l) + ext);
+            const int ne = rt_level_entries((1 << l) + ext, CH);
             const int L = FWD ? (1 << (l + 1)) : (1 << l);
             for (int e = tid; e < ne; e += NT) {
                 int ai, di;
@@ -227,7 +255,7 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
 #pragma unroll
                 for (int u = 0; u < LU; ++u) {
                     const int p = p0 + 32 * u;
-                    if (p < N) buf[0][p * CP + col] = v[u];
+                    if (p < N) buf(0)[p * CP + col] = v[u];
                 }
             }
         }
@@ -247,7 +275,7 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
 #pragma unroll
             for (int u = 0; u < LU; ++u) {
                 const int p = p0 + PS * u;
-                if (p < N) buf[0][p * CP + col] = v[u];
+                if (p < N) buf(0)[p * CP + col] = v[u];
             }
         }
     }
@@ -258,15 +286,15 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
     if (FWD) {
         int cur = 0;
         int rt_off = 0;
-        for (int l = 2; l < levels; ++l) rt_off += rt_level_entries((1 << l) + ext);
+        for (int l = 2; l < levels; ++l) rt_off += rt_level_entries((1 << l) + ext, CH);
         for (int l = levels - 1; l >= 2; --l) {
-            rt_off -= rt_level_entries((1 << l) + ext);
+            rt_off -= rt_level_entries((1 << l) + ext, CH);
             const int4* tb = rt + rt_off;
             const int L = 1 << (l + 1);
             const int M = (L >> 1) + ext;
             const int nd = L >> 1;
-            const T* S = buf[cur];
-            T* D = buf[cur ^ 1];
+            const T* S = buf(cur);
+            T* D = buf(cur ^ 1);
             const int nch = (M + CH - 1) / CH;
             for (int t = tid; t < C * nch; t += NT) {
                 const int col = t % C, k0 = (t / C) * CH;
@@ -324,42 +352,24 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
         }
         // base level: nb x nb matrix on the remaining approximation coefficients
         const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[bcd] : (WAV == WP_ID_CDF3_5 ? c_base35[bcd] : c_base46[bcd]);
-        if (tid < C) {
-            T a[5], o[5];
-            for (int i = 0; i < nb; ++i) a[i] = buf[cur][i * CP + tid];
-            for (int i = 0; i < nb; ++i) {
-                T s = T(0);
-                for (int j = 0; j < nb; ++j) s += T(mat[i * nb + j]) * a[j];
-                o[i] = s;
-            }
-            for (int i = 0; i < nb; ++i) buf[cur ^ 1][i * CP + tid] = o[i];
-        }
+        if (tid < C) base_level<T>(mat, nb, buf(cur) + tid, buf(cur ^ 1) + tid, CP);
         __syncthreads();
         outbuf = -1;  // position dependent, resolved below
     } else {
         const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[2 + bcd]
                                                   : (WAV == WP_ID_CDF3_5 ? c_base35[2 + bcd] : c_base46[2 + bcd]);
-        if (tid < C) {
-            T a[5], o[5];
-            for (int i = 0; i < nb; ++i) a[i] = buf[0][i * CP + tid];
-            for (int i = 0; i < nb; ++i) {
-                T s = T(0);
-                for (int j = 0; j < nb; ++j) s += T(mat[i * nb + j]) * a[j];
-                o[i] = s;
-            }
-            for (int i = 0; i < nb; ++i) buf[1][i * CP + tid] = o[i];
-        }
+        if (tid < C) base_level<T>(mat, nb, buf(0) + tid, buf(1) + tid, CP);
         __syncthreads();
         int cur = 1;
         int rt_off = 0;
         for (int l = 2; l < levels; ++l) {
             const int4* tb = rt + rt_off;
-            rt_off += rt_level_entries((1 << l) + ext);
+            rt_off += rt_level_entries((1 << l) + ext, CH);
             const int L = 1 << l;
             const int NA = L + ext;
-            const T* Sa = buf[cur];
-            const T* Sd = buf[0] + (size_t)NA * CP;
-            T* D = buf[3 - cur];
+            const T* Sa = buf(cur);
+            const T* Sd = buf(0) + (size_t)NA * CP;
+            T* D = buf(3 - cur);
             const int nch = (NA + CH - 1) / CH;
             for (int t = tid; t < C * nch; t += NT) {
                 const int col = t % C, k0 = (t / C) * CH;
@@ -443,7 +453,7 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
             for (int p = tid & 31; p < N; p += 32) {
                 int b = outbuf;
                 if (b < 0) b = (p < nb) ? basebuf : ((levels - (31 - __clz(p - ext))) & 1);
-                line[p] = buf[b][p * CP + col];
+                line[p] = buf(b)[p * CP + col];
             }
         }
     } else {
@@ -452,7 +462,7 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
             if (i0 + col >= g.ni) continue;
             int b = outbuf;
             if (b < 0) b = (p < nb) ? basebuf : ((levels - (31 - __clz(p - ext))) & 1);
-            dst[obase + (long)(i0 + col) * g.s_in + (long)p * g.pstride] = buf[b][p * CP + col];
+            dst[obase + (long)(i0 + col) * g.s_in + (long)p * g.pstride] = buf(b)[p * CP + col];
         }
     }
 }
@@ -483,13 +493,13 @@ cudaError_t ensure_constants() {
 }
 
 template <typename T>
-size_t dwt_smem(int N, int levels, bool fwd, int C) {
-    return rt_offset((size_t)(fwd ? 2 : 3) * N * (C + 1) * sizeof(T)) + 16 * (size_t)rt_entries(N, levels, fwd);
+size_t dwt_smem(int N, int levels, bool fwd, int C, int ch) {
+    return rt_offset((size_t)(fwd ? 2 : 3) * N * (C + 1) * sizeof(T)) + 16 * (size_t)rt_entries(N, levels, fwd, ch);
 }
 
 template <int WAV, bool FWD, typename T, int C>
 cudaError_t launch_one(const T* src, T* dst, int N, int levels, int bcd, TileGeom g, int nouter, cudaStream_t s) {
-    const size_t smem = dwt_smem<T>(N, levels, FWD, C);
+    const size_t smem = dwt_smem<T>(N, levels, FWD, C, ch_of(WAV));
     auto kern = dwt_tile_kernel<WAV, FWD, T, C>;
     cudaError_t e = wp_set_smem(kern, smem);
     if (e != cudaSuccess) return e;
@@ -524,7 +534,7 @@ cudaError_t launch_c(const T* src, T* dst, int N, int levels, int bcd, TileGeom 
     int C = 32;
     const long sms = wp_sm_count();
     while (C > 4) {
-        const size_t smem = dwt_smem<T>(N, levels, FWD, C);
+        const size_t smem = dwt_smem<T>(N, levels, FWD, C, ch_of(WAV));
         const long ctas = (long)((g.ni + C - 1) / C) * nouter;
         if (smem <= 100 * 1024 && ctas >= 2 * sms) break;
         C >>= 1;
@@ -536,7 +546,7 @@ cudaError_t launch_c(const T* src, T* dst, int N, int levels, int bcd, TileGeom 
         auto it = g_c_cache.find(c_key(WAV, FWD, (int)sizeof(T), N, g, nouter));
         if (it != g_c_cache.end()) C = it->second;
     }
-    const size_t smem = dwt_smem<T>(N, levels, FWD, C);
+    const size_t smem = dwt_smem<T>(N, levels, FWD, C, ch_of(WAV));
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     switch (C) {
         case 32: return launch_one<WAV, FWD, T, 32>(src, dst, N, levels, bcd, g, nouter, s);
@@ -600,7 +610,7 @@ wp_status wp_dwt_axis_tune(T* buf, int DX, int DY, int DZ, int levels, char axis
     int best_c = -1;
     wp_status st = WP_OK;
     for (int C = 4; C <= 32 && st == WP_OK; C *= 2) {
-        if (dwt_smem<T>(N, levels, forward != 0, C) > 227 * 1024) break;
+        if (dwt_smem<T>(N, levels, forward != 0, C, ch_of(wavelet)) > 227 * 1024) break;
         t_force_c = C;
         std::vector<float> t;
         for (int r = 0; r < 4 && st == WP_OK; ++r) {
