@@ -103,7 +103,12 @@ def test_device_velocity_generator(wp, oracle):
     assert abs(float(f.std()) - 0.5) < 0.15
 
 
-def test_trained_warm_start_saves_cycles(wp):
+def test_trained_warm_start_learns_and_fallback_bounds_its_cost(wp):
+    """What the trained network does, stated as it is: training on the plain method's solves halves
+    the loss; on held-out 32^3 problems the solve still meets its tolerance; the guess beats a zero
+    start after one V-cycle; and the fallback (judged after that cycle) keeps the cost at most one
+    cycle above the plain method.  The guess does not save cycles here or at 128^3 (the warm-start
+    run summary in profiles/), so no test asserts that it does."""
     from waveletpotentials_b200 import trainer
     dim = (32, 32, 32)
     train = trainer.make_dataset(dim, 12, seed=1)
