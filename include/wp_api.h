@@ -97,7 +97,10 @@ CUWHHD_API wp_status wp_ip_diag(double* out, int dim, int wavelet, char bc);
 typedef struct wp_recover3d wp_recover3d;
 /* Replaces CuWaveletPotentialRecover3D(int3 dim, DTYPE3 dx, char bc, WaveletType curl,
    WaveletType div) (cuWaveletPotentialRecover3D.cuh:11-12, .cu:6-12).  nx,ny,nz powers of two
-   >= 4; bc 'n' (zero-normal-flux walls).  Allocates its own temporaries on the current device. */
+   >= 4; bc 'n' (zero-normal-flux walls) or 'd' (Dirichlet walls: the curl wavelet takes bc 'd', the
+   div wavelet 'n', and the projection is cuProjectLocal_q_3d_nq_ccc, cuDivLocalProject3D.cu:4474-4877;
+   such a handle recovers fields with nonzero wall flux).  Allocates its own temporaries on the
+   current device. */
 CUWHHD_API wp_status wp_recover3d_create(wp_recover3d** h, int nx, int ny, int nz, double dx, double dy, double dz,
                                          char bc, int curl_wavelet, int div_wavelet);
 /* Replaces CuWaveletPotentialRecover3D::Solve(qx,qy,qz,xv,yv,zv) (cuWaveletPotentialRecover3D.cu:16-61):
@@ -112,7 +115,8 @@ CUWHHD_API wp_status wp_recover3d_project(wp_recover3d* h, float* qx, float* qy,
    (cuWaveletPotentialRecover3D.cu:123-239): analyses the potential with the recovery's synthesis
    wavelets, clears the coefficients of every index whose level along some axis is below `level`
    (with the reference's coupling of the three components), and synthesises the result into the
-   _out arrays (which may alias the inputs).  level in [0, min(log2 n)]: 0 returns the potential. */
+   _out arrays (which may alias the inputs).  level in [0, min(log2 n)]: 0 returns the potential.
+   Handles with bc 'n' only (WP_ERR_UNSUPPORTED otherwise). */
 CUWHHD_API wp_status wp_recover3d_cut(wp_recover3d* h, float* qx_out, float* qy_out, float* qz_out, const float* qx,
                                       const float* qy, const float* qz, int level, void* stream);
 CUWHHD_API wp_status wp_recover3d_destroy(wp_recover3d* h);

@@ -48,6 +48,7 @@ def lib():
             "or_dwt_axis": (i, [p, i, i, i, i, c, i, c, i]),
             "or_ip_diag": (i, [p, i, i, c]),
             "or_project3d": (i, [p, p, p, p, p, p, i, i, i, d, d, d]),
+            "or_project3d_nq": (i, [p, p, p, p, p, p, i, i, i, d, d, d]),
             "or_project2d": (i, [p, p, p, i, i, d, d]),
             "or_recover3d": (i, [p, p, p, p, p, p, i, i, i, d, d, d, c]),
             "or_recover2d": (i, [p, p, p, i, i, d, d, c]),
@@ -142,12 +143,14 @@ def mac_shapes2d(nx, ny):
 
 
 # ----------------------------------------------------------------- projection
-def project3d(xv, yv, zv, n, d):
+def project3d(xv, yv, zv, n, d, bc="n"):
+    """The local projection of the recovery; bc: the walls' boundary type ('n': cuProjectLocal_q_3d_dq_ccc,
+    'd': cuProjectLocal_q_3d_nq_ccc)."""
     nx, ny, nz = n
     s = mac_shapes3d(nx, ny, nz)
     qx, qy, qz = (np.zeros(s[k]) for k in ("qx", "qy", "qz"))
-    _check(lib().or_project3d(_p(qx), _p(qy), _p(qz), _p(_f64(xv)), _p(_f64(yv)), _p(_f64(zv)), nx, ny, nz, *d),
-           "project3d")
+    fn = lib().or_project3d if bc == "n" else lib().or_project3d_nq
+    _check(fn(_p(qx), _p(qy), _p(qz), _p(_f64(xv)), _p(_f64(yv)), _p(_f64(zv)), nx, ny, nz, *d), "project3d")
     return qx, qy, qz
 
 

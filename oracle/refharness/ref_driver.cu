@@ -102,9 +102,10 @@ int main(int argc, char** argv) {
         DTYPE* ip = CuGetInnerProduct::GetInstance()->GenerateIp(wt(I(1)), argv[6][0], dim);
         checkCudaErrors(cudaDeviceSynchronize());
         write_bin("ip", from_dev(ip, (size_t)dim * 8));
-    } else if (op == "project3d" || op == "recover3d") {  // nx ny nz dx
+    } else if (op == "project3d" || op == "recover3d") {  // nx ny nz dx [bc]
         int3 dim = make_int3(I(0), I(1), I(2));
         DTYPE h = (DTYPE)D(3);
+        const char wall = argc > 8 ? argv[8][0] : 'n';  // the walls' boundary type
         DTYPE3 dx = make_DTYPE3(h, h, h);
         size_t sxv = (size_t)(dim.x + 1) * dim.y * dim.z, syv = (size_t)dim.x * (dim.y + 1) * dim.z;
         size_t szv = (size_t)dim.x * dim.y * (dim.z + 1);
@@ -119,10 +120,10 @@ int main(int argc, char** argv) {
         int3 levels = make_int3((int)log2(dim.x), (int)log2(dim.y), (int)log2(dim.z));
         if (op == "project3d") {
             int3 dim_ext = make_int3(dim.x + 1, dim.y + 1, dim.z + 1);
-            CuDivLocalProject3D cudlp(dim_ext, levels, dx, WaveletType::WT_CDF4_6, proj_bc('n'));
+            CuDivLocalProject3D cudlp(dim_ext, levels, dx, WaveletType::WT_CDF4_6, proj_bc(wall));
             cudlp.ProjectLocal_q_ccc(qx, qy, qz, xv, yv, zv, levels);
         } else {
-            CuWaveletPotentialRecover3D rec(dim, dx, 'n', WaveletType::WT_CDF3_7, WaveletType::WT_CDF4_6);
+            CuWaveletPotentialRecover3D rec(dim, dx, wall, WaveletType::WT_CDF3_7, WaveletType::WT_CDF4_6);
             rec.Solve(qx, qy, qz, xv, yv, zv);
         }
         checkCudaErrors(cudaDeviceSynchronize());

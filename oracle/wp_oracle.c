@@ -450,6 +450,149 @@ int or_project3d(double* qx, double* qy, double* qz, const double* xv, const dou
     return 0;
 }
 
+/* Local projection with Dirichlet domain walls (the recovery's bc 'd': base wavelet CDF4.6 with bc
+   'n', projection wavelet CDF3.7 with bc 'd'), cuProjectLocal_q_3d_nq_ccc
+   (cuDivLocalProject3D.cu:4474-4877), launched by ProjectLocal_q_ccc (:5271-5308).  Coefficient
+   (x, y, z) in [0, n)^3 with the velocity coefficients X = xv(x+1, y, z), Y = yv(x, y+1, z),
+   Z = zv(x, y, z+1) and, on a wall plane, the wall-side ones X0 = xv(x, y, z), Y0 = yv(x, y, z),
+   Z0 = zv(x, y, z):
+   - interior (x, y, z > 0): q = (s x v) / |s|^2 as for bc 'n';
+   - a wall plane (one index 0): the wall-normal velocity pair is divided by the scale of the other
+     in-plane axis (the reference's cuCalculateP0Val_single, :156-177), which corrects the in-plane
+     velocity by the difference of the two times dx_inv_a / n_a; the remaining
+     component is the one-component ratio weighted by the inner-product tables;
+   - a wall line (two indices 0): two such corrections, the third component 0;
+   - the corner: the base potentials from the wall velocities times the spacings.
+   Every potential entry with an index 0 along one of its own axes is written by exactly one
+   coefficient (the zero entries included), so the result does not depend on the start of q. */
+int or_project3d_nq(double* qx, double* qy, double* qz, const double* xv, const double* yv, const double* zv,
+                    int nx, int ny, int nz, double dx, double dy, double dz) {
+    int Lx = ilog2(nx), Ly = ilog2(ny), Lz = ilog2(nz);
+    if ((1 << Lx) != nx || (1 << Ly) != ny || (1 << Lz) != nz) return 1;
+    double* ipbx = (double*)malloc(sizeof(double) * (nx + 1));
+    double* ipby = (double*)malloc(sizeof(double) * (ny + 1));
+    double* ipbz = (double*)malloc(sizeof(double) * (nz + 1));
+    double* ippx = (double*)malloc(sizeof(double) * nx);
+    double* ippy = (double*)malloc(sizeof(double) * ny);
+    double* ippz = (double*)malloc(sizeof(double) * nz);
+    or_ip_diag(ipbx, nx + 1, OR_CDF4_6, 'n');
+    or_ip_diag(ipby, ny + 1, OR_CDF4_6, 'n');
+    or_ip_diag(ipbz, nz + 1, OR_CDF4_6, 'n');
+    or_ip_diag(ippx, nx, OR_CDF3_7, 'd');
+    or_ip_diag(ippy, ny, OR_CDF3_7, 'd');
+    or_ip_diag(ippz, nz, OR_CDF3_7, 'd');
+    const double dxi = 1.0 / dx, dyi = 1.0 / dy, dzi = 1.0 / dz;
+    /* inverse extent of the domain along each axis, dx_inv / n (the reference's L_inv) */
+    const double lx = dxi / nx, ly = dyi / ny, lz = dzi / nz;
+    const long pqx = (long)nx * (ny + 1), pqy = (long)(nx + 1) * ny, pqz = (long)(nx + 1) * (ny + 1);
+#define QX(X_, Y_, Z_) qx[(Y_) + (long)(X_) * (ny + 1) + (long)(Z_) * pqx]
+#define QY(X_, Y_, Z_) qy[(Y_) + (long)(X_) * ny + (long)(Z_) * pqy]
+#define QZ(X_, Y_, Z_) qz[(Y_) + (long)(X_) * (ny + 1) + (long)(Z_) * pqz]
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < nz; ++z)
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y) {
+                int jx = Lx - bitlen(x) + 1, jy = Ly - bitlen(y) + 1, jz = Lz - bitlen(z) + 1;
+                double sx = 4.0 * dxi / ((double)(1 << jx) + EPS12);
+                double sy = 4.0 * dyi / ((double)(1 << jy) + EPS12);
+                double sz = 4.0 * dzi / ((double)(1 << jz) + EPS12);
+                double ip0x = ippx[x], ip1x = ipbx[x + 1];
+                double ip0y = ippy[y], ip1y = ipby[y + 1];
+                double ip0z = ippz[z], ip1z = ipbz[z + 1];
+                double X = xv[y + (long)(x + 1) * ny + (long)z * (nx + 1) * ny];
+                double Y = yv[(y + 1) + (long)x * (ny + 1) + (long)z * nx * (ny + 1)];
+                double Z = zv[y + (long)x * ny + (long)(z + 1) * nx * ny];
+                double X0 = xv[y + (long)x * ny + (long)z * (nx + 1) * ny];
+                double Y0 = yv[y + (long)x * (ny + 1) + (long)z * nx * (ny + 1)];
+                double Z0 = zv[y + (long)x * ny + (long)z * nx * ny];
+                double b010 = ip0x * ip1y * ip0z, b100 = ip1x * ip0y * ip0z, b001 = ip0x * ip0y * ip1z;
+                double wx = 1.0 / (sy * (sy * b001) + sz * (sz * b010) + EPS12);
+                double wy = 1.0 / (sx * (sx * b001) + sz * (sz * b100) + EPS12);
+                double wz = 1.0 / (sx * (sx * b010) + sy * (sy * b100) + EPS12);
+                double oX = 0.0, oY = 0.0, oZ = 0.0;
+                int zx = x == 0, zy = y == 0, zz = z == 0;
+                if (!zx && !zy && !zz) {
+                    double inv = 1.0 / (sy * sy + sx * sx + sz * sz);
+                    oZ = (sy * X - sx * Y) * inv;
+                    oX = (sz * Y - sy * Z) * inv;
+                    oY = (sx * Z - sz * X) * inv;
+                } else if (zz && !zx && !zy) {  /* wall plane z = 0 */
+                    double t0 = Z0 / sx, t1 = Z / sx;
+                    X += (t1 - t0) * lz;
+                    QX(x, y + 1, 0) = 0.0;
+                    QY(x + 1, y, 0) = t0;
+                    oY = t1;
+                    oZ = (X * (sy * b100) - Y * (sx * b010)) * wz;
+                } else if (zy && !zx && !zz) {  /* wall plane y = 0 */
+                    double t0 = Y0 / sz, t1 = Y / sz;
+                    Z += (t1 - t0) * ly;
+                    QX(x, 0, z + 1) = t0;
+                    QZ(x + 1, 0, z) = 0.0;
+                    oX = t1;
+                    oY = (Z * (sx * b001) - X * (sz * b100)) * wy;
+                } else if (zx && !zy && !zz) {  /* wall plane x = 0 */
+                    double t0 = X0 / sy, t1 = X / sy;
+                    Y += (t1 - t0) * lx;
+                    QZ(0, y + 1, z) = t0;
+                    QY(0, y, z + 1) = 0.0;
+                    oZ = t1;
+                    oX = (Y * (sz * b010) - Z * (sy * b001)) * wx;
+                } else if (!zx && zy && zz) {  /* wall line along x */
+                    double a0 = Z0 / sx, a1 = Z / sx;
+                    double c0 = -Y0 / sx, c1 = -Y / sx;
+                    QY(x + 1, 0, 0) = a0;
+                    QZ(x + 1, 0, 0) = c0;
+                    QX(x, 0, 1) = 0.0;
+                    QX(x, 0, 0) = 0.0;
+                    QX(x, 1, 0) = 0.0;
+                    oY = a1;
+                    oZ = c1;
+                } else if (zx && !zy && zz) {  /* wall line along y */
+                    double a0 = -Z0 / sy, a1 = -Z / sy;
+                    double c0 = X0 / sy, c1 = X / sy;
+                    QX(0, y + 1, 0) = a0;
+                    QZ(0, y + 1, 0) = c0;
+                    QY(0, y, 0) = 0.0;
+                    QY(1, y, 0) = 0.0;
+                    QY(0, y, 1) = 0.0;
+                    oX = a1;
+                    oZ = c1;
+                } else if (zx && zy && !zz) {  /* wall line along z */
+                    double a0 = Y0 / sz, a1 = Y / sz;
+                    double c0 = -X0 / sz, c1 = -X / sz;
+                    QX(0, 0, z + 1) = a0;
+                    QY(0, 0, z + 1) = c0;
+                    QZ(0, 0, z) = 0.0;
+                    QZ(0, 1, z) = 0.0;
+                    QZ(1, 0, z) = 0.0;
+                    oX = a1;
+                    oY = c1;
+                } else {  /* corner */
+                    double x010 = -Z0 / ly, x001 = Y0 / lz, x011 = x010 + Y / lz;
+                    double y001 = -X0 / lz, y101 = -X / lz;
+                    QZ(0, 0, 0) = 0.0;
+                    QZ(1, 0, 0) = 0.0;
+                    QZ(0, 1, 0) = 0.0;
+                    QX(0, 0, 0) = 0.0;
+                    QX(0, 1, 0) = x010;
+                    QX(0, 0, 1) = x001;
+                    QY(0, 0, 0) = 0.0;
+                    QY(1, 0, 0) = 0.0;
+                    QY(0, 0, 1) = y001;
+                    oX = x011;
+                    oY = y101;
+                }
+                QX(x, y + 1, z + 1) = oX;
+                QY(x + 1, y, z + 1) = oY;
+                QZ(x + 1, y + 1, z) = oZ;
+            }
+#undef QX
+#undef QY
+#undef QZ
+    free(ipbx); free(ipby); free(ipbz); free(ippx); free(ippy); free(ippz);
+    return 0;
+}
+
 /* cuProjectLocal_q_single (cuDivLocalProject.cu:765-1045): both passes evaluate the same pointwise
    ratio and the neighbour terms are unused, so qz(x,y) = P for 2<=x<=nx, 2<=y<=ny, else 0. */
 int or_project2d(double* qz, const double* xv, const double* yv, int nx, int ny, double dx, double dy) {
@@ -488,9 +631,11 @@ int or_project2d(double* qz, const double* xv, const double* yv, int nx, int ny,
 /* CuWaveletPotentialRecover3D::Solve (cuWaveletPotentialRecover3D.cu:16-61) */
 int or_recover3d(double* qx, double* qy, double* qz, const double* xv, const double* yv, const double* zv,
                  int nx, int ny, int nz, double dx, double dy, double dz, char bc) {
-    if (bc != 'n') return 2; /* only zero-normal-flux walls (bc 'n') are on the configured path */
+    /* bc: the walls' boundary type (cuWaveletPotentialRecover3D.cu:6-11); the div wavelet takes the
+       other one (proj_bc) and the projection kernel follows it */
+    if (bc != 'n' && bc != 'd') return 2;
     int Lx = ilog2(nx), Ly = ilog2(ny), Lz = ilog2(nz);
-    char bcd = 'd';
+    char bcd = bc == 'n' ? 'd' : 'n';
     size_t sxv = (size_t)(nx + 1) * ny * nz, syv = (size_t)nx * (ny + 1) * nz, szv = (size_t)nx * ny * (nz + 1);
     double* tx = (double*)malloc(sizeof(double) * sxv);
     double* ty = (double*)malloc(sizeof(double) * syv);
@@ -508,7 +653,8 @@ int or_recover3d(double* qx, double* qy, double* qz, const double* xv, const dou
     e |= or_dwt_axis(tz, nx, ny, nz + 1, Lx, 'x', OR_CDF3_7, bc, 1);
     e |= or_dwt_axis(tz, nx, ny, nz + 1, Ly, 'y', OR_CDF3_7, bc, 1);
     e |= or_dwt_axis(tz, nx, ny, nz + 1, Lz, 'z', OR_CDF4_6, bcd, 1);
-    e |= or_project3d(qx, qy, qz, tx, ty, tz, nx, ny, nz, dx, dy, dz);
+    e |= bc == 'n' ? or_project3d(qx, qy, qz, tx, ty, tz, nx, ny, nz, dx, dy, dz)
+                   : or_project3d_nq(qx, qy, qz, tx, ty, tz, nx, ny, nz, dx, dy, dz);
     e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Lx, 'x', OR_CDF3_7, bc, 0);
     e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Ly, 'y', OR_CDF4_6, bcd, 0);
     e |= or_dwt_axis(qx, nx, ny + 1, nz + 1, Lz, 'z', OR_CDF4_6, bcd, 0);

@@ -34,8 +34,12 @@ int or_ip_diag(double* out, int dim, int wavelet, char bc);
 int or_project3d(double* qx, double* qy, double* qz, const double* xv, const double* yv, const double* zv,
                  int nx, int ny, int nz, double dx, double dy, double dz);
 int or_project2d(double* qz, const double* xv, const double* yv, int nx, int ny, double dx, double dy);
+/* the same projection with Dirichlet domain walls (cuProjectLocal_q_3d_nq_ccc) */
+int or_project3d_nq(double* qx, double* qy, double* qz, const double* xv, const double* yv, const double* zv,
+                    int nx, int ny, int nz, double dx, double dy, double dz);
 
-/* full potential recovery: 9 forward passes, projection, 9 inverse passes (3D); 4 + 1 + 2 (2D) */
+/* full potential recovery: 9 forward passes, projection, 9 inverse passes (3D, bc 'n' or 'd');
+   4 + 1 + 2 (2D) */
 int or_recover3d(double* qx, double* qy, double* qz, const double* xv, const double* yv, const double* zv,
                  int nx, int ny, int nz, double dx, double dy, double dz, char bc);
 int or_recover2d(double* qz, const double* xv, const double* yv, int nx, int ny, double dx, double dy, char bc);

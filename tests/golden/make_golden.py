@@ -11,6 +11,7 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only cdf35   # the CDF3.5 transforms only
     python tests/golden/make_golden.py --only dst     # CuDst3D::Solve only
     python tests/golden/make_golden.py --only psweep  # CuParallelSweep3D Solve / Project only
+    python tests/golden/make_golden.py --only domd    # projection and recovery with Dirichlet walls
     ... [--out DIR]                                   # write the .npz files to DIR instead of here
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
@@ -248,6 +249,28 @@ def psweep_cases(rng):
     save("psweep", **out)
 
 
+def domd_cases(rng):
+    """CuDivLocalProject3D::ProjectLocal_q_ccc with the walls' boundary type 'd' (the base wavelet's bc
+    proj_bc('d') = 'n', so cuProjectLocal_q_3d_nq_ccc runs) on random coefficients, and
+    CuWaveletPotentialRecover3D::Solve with bc 'd' on random velocity fields with nonzero wall flux."""
+    out = {}
+    for tag, n3 in (("p16x8x32", (16, 8, 32)), ("p8", (8, 8, 8))):
+        s = shapes3(n3)
+        xv, yv, zv = (rng.standard_normal(s[k]) for k in ("xv", "yv", "zv"))
+        h = 1.0 / n3[0]
+        r = run("project3d", {"xv": xv, "yv": yv, "zv": zv}, [*n3, h, "d"], {k: s[k] for k in ("qx", "qy", "qz")})
+        out.update({f"{tag}_{k}": v for k, v in dict(xv=xv, yv=yv, zv=zv, **r).items()})
+        out[f"{tag}_meta"] = np.array([*n3, h])
+    for tag, n3 in (("r16", (16, 16, 16)), ("r8x16x32", (8, 16, 32))):
+        s = shapes3(n3)
+        xv, yv, zv = (rng.standard_normal(s[k]) for k in ("xv", "yv", "zv"))
+        h = 1.0 / n3[0]
+        r = run("recover3d", {"xv": xv, "yv": yv, "zv": zv}, [*n3, h, "d"], {k: s[k] for k in ("qx", "qy", "qz")})
+        out.update({f"{tag}_{k}": v for k, v in dict(xv=xv, yv=yv, zv=zv, **r).items()})
+        out[f"{tag}_meta"] = np.array([*n3, h])
+    save("domain_d", **out)
+
+
 def main():
     global OUT_DIR
     if "--out" in sys.argv:
@@ -276,6 +299,9 @@ def main():
         return
     if only == "psweep":
         psweep_cases(np.random.default_rng(20261210))
+        return
+    if only == "domd":
+        domd_cases(np.random.default_rng(20261211))
         return
     rng = np.random.default_rng(20261203)
 

@@ -44,8 +44,8 @@ def test_dwt_rejects_bad_shapes(L):
 def test_recover_rejects_unsupported_requests(L):
     h = ctypes.c_void_p()
     assert L.wp_recover3d_create(ctypes.byref(h), 24, 16, 16, 0.1, 0.1, 0.1, _c("n"), 11, 7) == 1
-    assert L.wp_recover3d_create(ctypes.byref(h), 16, 16, 16, 0.1, 0.1, 0.1, _c("d"), 11, 7) == 2
-    assert "bc 'n'" in _lib.last_error()
+    assert L.wp_recover3d_create(ctypes.byref(h), 16, 16, 16, 0.1, 0.1, 0.1, _c("z"), 11, 7) == 2
+    assert "bc must be 'n'" in _lib.last_error()
     assert L.wp_recover3d_create(ctypes.byref(h), 16, 16, 16, 0.1, 0.1, 0.1, _c("n"), 7, 11) == 2
     assert L.wp_recover3d_create(ctypes.byref(h), 16, 16, 16, 0.0, 0.1, 0.1, _c("n"), 11, 7) == 1
     assert L.wp_recover2d_create(ctypes.byref(h), 16, 12, 0.1, 0.1, _c("n"), 11, 7) == 1

@@ -220,3 +220,20 @@ def test_sweep2d_matches_reference(oracle):
     n = 32
     qz = oracle.sweep2d_solve(g["yv2d"], (n, n), (1.0 / n, 1.0 / n))
     assert np.abs(qz - g["qz2d"]).max() <= 1e-14 * np.abs(g["qz2d"]).max()
+
+
+@pytest.mark.parametrize("tag", ["p16x8x32", "p8", "r16", "r8x16x32"])
+def test_domain_d_projection_and_recovery_match_reference(oracle, tag):
+    """Dirichlet domain walls: CuDivLocalProject3D::ProjectLocal_q_ccc with bc_base 'n'
+    (cuProjectLocal_q_3d_nq_ccc, the wall planes, lines and corner included) on random coefficients
+    ("p" cases) and CuWaveletPotentialRecover3D::Solve with bc 'd' on random fields with wall flux
+    ("r" cases), from the reference's FP64 build.  The reference's inner-product tables carry FP32
+    rounding, hence the 1e-7."""
+    d = load_golden("domain_d")
+    nx, ny, nz, h = d[tag + "_meta"]
+    n = (int(nx), int(ny), int(nz))
+    args = (d[tag + "_xv"], d[tag + "_yv"], d[tag + "_zv"], n, (h,) * 3)
+    q = oracle.project3d(*args, bc="d") if tag[0] == "p" else oracle.recover3d(*args, bc="d")
+    for k, got in zip(("qx", "qy", "qz"), q):
+        ref = d[tag + "_" + k]
+        assert np.sqrt(np.sum((ref - got) ** 2) / np.sum(ref * ref)) < 1e-7, (tag, k)

@@ -175,3 +175,23 @@ def test_oracle_sweep2d_curl(oracle):
     qz = oracle.sweep2d_solve(yv, n, d)
     for a, b in zip(oracle.curl2d(qz, n, d), (xv, yv)):
         assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("n", [(8, 8, 8), (16, 8, 32)])
+def test_recovery_with_dirichlet_walls_reproduces_any_divergence_free_field(oracle, n):
+    """bc 'd': u = curl q for an unconstrained potential q (nonzero wall flux) is recovered exactly:
+    curl(recover(u)) == u to rounding.  The zero-flux recovery (bc 'n') does not reproduce such a
+    field: its walls assume no flux."""
+    rng = np.random.default_rng(sum(n))
+    nx, ny, nz = n
+    shp = {"qx": (nz + 1, nx, ny + 1), "qy": (nz + 1, nx + 1, ny), "qz": (nz, nx + 1, ny + 1)}
+    d = (1.0 / nx, 1.3 / ny, 0.7 / nz)
+    q = [fields.spectral_field(shp[k], -11.0 / 3.0, 1.0, rng) for k in ("qx", "qy", "qz")]
+    u = fields.curl3d(*q, n, d)
+    den = sum(np.sum(a * a) for a in u)
+    r = oracle.recover3d(*u, n, d, bc="d")
+    c = fields.curl3d(*r, n, d)
+    assert np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u, c)) / den) < 1e-10
+    r = oracle.recover3d(*u, n, d, bc="n")
+    c = fields.curl3d(*r, n, d)
+    assert np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u, c)) / den) > 1e-2

@@ -92,6 +92,115 @@ __global__ void __launch_bounds__(256) project3d_kernel(float* __restrict__ qx, 
     if (x == 0 && y == 0) qz[z * sqz] = 0.f;
 }
 
+// The projection with Dirichlet domain walls (the recovery's bc 'd'; cuProjectLocal_q_3d_nq_ccc,
+// cuDivLocalProject3D.cu:4474-4877).  Coefficient (x, y, z) as in project3d_kernel; with one index 0 the
+// wall-side velocity coefficients X0 = xv(x, y, z), Y0 = yv(x, y, z), Z0 = zv(x, y, z) enter too:
+//  * interior: q = (s x v) / |s|^2;
+//  * wall plane a = 0: the wall-normal pair (e.g. Z0, Z for z = 0) divided by the scale of the other
+//    in-plane axis gives the two potential entries along the wall, their difference times
+//    l_a = dx_inv_a / n_a corrects the in-plane velocity, and the remaining component is the
+//    one-component ratio weighted by the inner-product tables;
+//  * wall line (two indices 0): two such divided pairs, the third component 0;
+//  * corner: the wall velocities divided by l.
+// Every potential entry with an index 0 along one of its own axes is written by exactly one thread
+// (zeros included), so q needs no clearing.
+__global__ void __launch_bounds__(256) project3d_nq_kernel(float* __restrict__ qx, float* __restrict__ qy,
+                                                           float* __restrict__ qz, const float* __restrict__ xv,
+                                                           const float* __restrict__ yv, const float* __restrict__ zv,
+                                                           int nx, int ny, int nz, AxisTab tx, AxisTab ty, AxisTab tz,
+                                                           float lx, float ly, float lz) {
+    const int y = blockIdx.x * 32 + threadIdx.x;
+    const int x = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (y >= ny || x >= nx) return;
+    const long sxv = (long)(nx + 1) * ny, syv = (long)nx * (ny + 1), szv = (long)nx * ny;
+    const long pqx = (long)nx * (ny + 1), pqy = (long)(nx + 1) * ny, pqz = (long)(nx + 1) * (ny + 1);
+    auto QX = [&](int i, int j, int k) -> float& { return qx[j + (long)i * (ny + 1) + k * pqx]; };
+    auto QY = [&](int i, int j, int k) -> float& { return qy[j + (long)i * ny + k * pqy]; };
+    auto QZ = [&](int i, int j, int k) -> float& { return qz[j + (long)i * (ny + 1) + k * pqz]; };
+    float X = xv[y + (long)(x + 1) * ny + z * sxv];
+    float Y = yv[(y + 1) + (long)x * (ny + 1) + z * syv];
+    float Z = zv[y + (long)x * ny + (z + 1) * szv];
+    const float sx = tx.s[x], sy = ty.s[y], sz = tz.s[z];
+    float oX = 0.f, oY = 0.f, oZ = 0.f;
+    const bool ix = x == 0, iy = y == 0, iz = z == 0;
+    if (!ix && !iy && !iz) {
+        const float inv = 1.f / (sy * sy + sx * sx + sz * sz);
+        oZ = (sy * X - sx * Y) * inv;
+        oX = (sz * Y - sy * Z) * inv;
+        oY = (sx * Z - sz * X) * inv;
+    } else {
+        const float ip0x = tx.ip0[x], ip1x = tx.ip1[x], ip0y = ty.ip0[y], ip1y = ty.ip1[y];
+        const float ip0z = tz.ip0[z], ip1z = tz.ip1[z];
+        const float b010 = ip0x * ip1y * ip0z, b100 = ip1x * ip0y * ip0z, b001 = ip0x * ip0y * ip1z;
+        const float X0 = ix ? xv[y + z * sxv] : 0.f;
+        const float Y0 = iy ? yv[(long)x * (ny + 1) + z * syv] : 0.f;
+        const float Z0 = iz ? zv[y + (long)x * ny] : 0.f;
+        if (iz && !ix && !iy) {  // wall plane z = 0
+            const float t0 = Z0 / sx, t1 = Z / sx;
+            X += (t1 - t0) * lz;
+            QX(x, y + 1, 0) = 0.f;
+            QY(x + 1, y, 0) = t0;
+            oY = t1;
+            oZ = (X * (sy * b100) - Y * (sx * b010)) * (1.f / (sx * (sx * b010) + sy * (sy * b100) + kEps));
+        } else if (iy && !ix && !iz) {  // wall plane y = 0
+            const float t0 = Y0 / sz, t1 = Y / sz;
+            Z += (t1 - t0) * ly;
+            QX(x, 0, z + 1) = t0;
+            QZ(x + 1, 0, z) = 0.f;
+            oX = t1;
+            oY = (Z * (sx * b001) - X * (sz * b100)) * (1.f / (sx * (sx * b001) + sz * (sz * b100) + kEps));
+        } else if (ix && !iy && !iz) {  // wall plane x = 0
+            const float t0 = X0 / sy, t1 = X / sy;
+            Y += (t1 - t0) * lx;
+            QZ(0, y + 1, z) = t0;
+            QY(0, y, z + 1) = 0.f;
+            oZ = t1;
+            oX = (Y * (sz * b010) - Z * (sy * b001)) * (1.f / (sy * (sy * b001) + sz * (sz * b010) + kEps));
+        } else if (!ix && iy && iz) {  // wall line along x
+            QY(x + 1, 0, 0) = Z0 / sx;
+            QZ(x + 1, 0, 0) = -Y0 / sx;
+            QX(x, 0, 1) = 0.f;
+            QX(x, 0, 0) = 0.f;
+            QX(x, 1, 0) = 0.f;
+            oY = Z / sx;
+            oZ = -Y / sx;
+        } else if (ix && !iy && iz) {  // wall line along y
+            QX(0, y + 1, 0) = -Z0 / sy;
+            QZ(0, y + 1, 0) = X0 / sy;
+            QY(0, y, 0) = 0.f;
+            QY(1, y, 0) = 0.f;
+            QY(0, y, 1) = 0.f;
+            oX = -Z / sy;
+            oZ = X / sy;
+        } else if (ix && iy && !iz) {  // wall line along z
+            QX(0, 0, z + 1) = Y0 / sz;
+            QY(0, 0, z + 1) = -X0 / sz;
+            QZ(0, 0, z) = 0.f;
+            QZ(0, 1, z) = 0.f;
+            QZ(1, 0, z) = 0.f;
+            oX = Y / sz;
+            oY = -X / sz;
+        } else {  // corner
+            const float x010 = -Z0 / ly;
+            QZ(0, 0, 0) = 0.f;
+            QZ(1, 0, 0) = 0.f;
+            QZ(0, 1, 0) = 0.f;
+            QX(0, 0, 0) = 0.f;
+            QX(0, 1, 0) = x010;
+            QX(0, 0, 1) = Y0 / lz;
+            QY(0, 0, 0) = 0.f;
+            QY(1, 0, 0) = 0.f;
+            QY(0, 0, 1) = -X0 / lz;
+            oX = x010 + Y / lz;
+            oY = -X / lz;
+        }
+    }
+    QX(x, y + 1, z + 1) = oX;
+    QY(x + 1, y, z + 1) = oY;
+    QZ(x + 1, y + 1, z) = oZ;
+}
+
 __global__ void __launch_bounds__(256) project2d_kernel(float* __restrict__ qz, const float* __restrict__ xv,
                                                         const float* __restrict__ yv, int nx, int ny, AxisTab tx,
                                                         AxisTab ty) {
@@ -111,13 +220,15 @@ __global__ void __launch_bounds__(256) project2d_kernel(float* __restrict__ qz, 
     qz[y + (long)x * (ny + 1)] = out;
 }
 
-// Builds the per-axis table [s | ip0 | ip1] (length 3n floats) on the device.
-wp_status build_axis_table(float** d_tab, int n, double h, cudaStream_t s) {
+// Builds the per-axis table [s | ip0 | ip1] (length 3n floats) on the device.  wall: the walls'
+// boundary type; the projection wavelet CDF3.7 takes it, the base wavelet CDF4.6 the other one
+// (CuDivLocalProject3D's constructor, cuDivLocalProject3D.cu:50-60, with bc = proj_bc(wall)).
+wp_status build_axis_table(float** d_tab, int n, double h, cudaStream_t s, char wall = 'n') {
     const int L = wp_ilog2(n);
     double* d_ip = nullptr;
     WP_CUDA_TRY(cudaMalloc((void**)&d_ip, sizeof(double) * (2 * n + 1)));
-    wp_status st = wp_ip_diag_device(d_ip, n, WP_ID_CDF3_7, 'n', s);
-    if (st == WP_OK) st = wp_ip_diag_device(d_ip + n, n + 1, WP_ID_CDF4_6, 'd', s);
+    wp_status st = wp_ip_diag_device(d_ip, n, WP_ID_CDF3_7, wall, s);
+    if (st == WP_OK) st = wp_ip_diag_device(d_ip + n, n + 1, WP_ID_CDF4_6, wall == 'n' ? 'd' : 'n', s);
     std::vector<double> ip(2 * n + 1);
     if (st == WP_OK) {
         cudaError_t e = cudaMemcpyAsync(ip.data(), d_ip, sizeof(double) * (2 * n + 1), cudaMemcpyDeviceToHost, s);
@@ -132,8 +243,8 @@ wp_status build_axis_table(float** d_tab, int n, double h, cudaStream_t s) {
         for (int v = i; v > 0; v >>= 1) ++bl;
         const int j = L - bl + 1;
         tab[i] = (float)(4.0 / h / ((double)(1 << j) + 1e-12));
-        tab[n + i] = (float)ip[i];          // ip_proj[i]  (CDF3.7 'n', n points)
-        tab[2 * n + i] = (float)ip[n + i + 1];  // ip_base[i+1] (CDF4.6 'd', n+1 points)
+        tab[n + i] = (float)ip[i];              // ip_proj[i]  (CDF3.7, n points)
+        tab[2 * n + i] = (float)ip[n + i + 1];  // ip_base[i+1] (CDF4.6, n+1 points)
     }
     WP_CUDA_TRY(cudaMalloc((void**)d_tab, sizeof(float) * 3 * n));
     WP_CUDA_TRY(cudaMemcpy(*d_tab, tab.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice));
@@ -150,6 +261,7 @@ struct wp_recover3d {
     int n[3];
     int L[3];
     double h[3];
+    char bc, bcd;  // the walls' boundary type and the div wavelet's (the other one)
     float* tab[3];
     float* tmp[3];
 };
@@ -163,17 +275,19 @@ extern "C" CUWHHD_API wp_status wp_recover3d_create(wp_recover3d** out, int nx, 
         wp_set_error_msg("wp_recover3d_create: extents must be powers of two in [4, 4096] and spacings > 0");
         return WP_ERR_INVALID_ARG;
     }
-    if (bc != 'n') { wp_set_error_msg("wp_recover3d_create: only bc 'n' (zero-normal-flux walls) is implemented"); return WP_ERR_UNSUPPORTED; }
+    if (bc != 'n' && bc != 'd') { wp_set_error_msg("wp_recover3d_create: bc must be 'n' (zero-normal-flux walls) or 'd' (Dirichlet walls)"); return WP_ERR_UNSUPPORTED; }
     if (!check_wavelets(curl_wavelet, div_wavelet)) { wp_set_error_msg("wp_recover3d_create: curl CDF3.7 / div CDF4.6 only"); return WP_ERR_UNSUPPORTED; }
     wp_recover3d* h = new (std::nothrow) wp_recover3d();
     if (!h) return WP_ERR_INVALID_ARG;
+    h->bc = bc;
+    h->bcd = bc == 'n' ? 'd' : 'n';
     int n[3] = {nx, ny, nz};
     double hs[3] = {dx, dy, dz};
     for (int a = 0; a < 3; ++a) {
         h->n[a] = n[a];
         h->L[a] = wp_ilog2(n[a]);
         h->h[a] = hs[a];
-        wp_status st = build_axis_table(&h->tab[a], n[a], hs[a], 0);
+        wp_status st = build_axis_table(&h->tab[a], n[a], hs[a], 0, bc);
         if (st != WP_OK) { wp_recover3d_destroy(h); return st; }
     }
     if (cudaError_t e = wp_dwt_prepare(); e != cudaSuccess) {
@@ -195,14 +309,15 @@ extern "C" CUWHHD_API wp_status wp_recover3d_create(wp_recover3d** out, int nx, 
             cudaMemset(scratch, 0, sizeof(float) * big);
             const int C = WP_ID_CDF3_7, V = WP_ID_CDF4_6;
             const int Lx = h->L[0], Ly = h->L[1], Lz = h->L[2];
+            const char b = h->bc, d = h->bcd;
             struct P { int dx, dy, dz, L; char ax; int w; char bc; int f; };
             const P passes[18] = {
-                {nx + 1, ny, nz, Lx, 'x', V, 'd', 1}, {nx + 1, ny, nz, Ly, 'y', C, 'n', 1}, {nx + 1, ny, nz, Lz, 'z', C, 'n', 1},
-                {nx, ny + 1, nz, Lx, 'x', C, 'n', 1}, {nx, ny + 1, nz, Ly, 'y', V, 'd', 1}, {nx, ny + 1, nz, Lz, 'z', C, 'n', 1},
-                {nx, ny, nz + 1, Lx, 'x', C, 'n', 1}, {nx, ny, nz + 1, Ly, 'y', C, 'n', 1}, {nx, ny, nz + 1, Lz, 'z', V, 'd', 1},
-                {nx, ny + 1, nz + 1, Lx, 'x', C, 'n', 0}, {nx, ny + 1, nz + 1, Ly, 'y', V, 'd', 0}, {nx, ny + 1, nz + 1, Lz, 'z', V, 'd', 0},
-                {nx + 1, ny, nz + 1, Lx, 'x', V, 'd', 0}, {nx + 1, ny, nz + 1, Ly, 'y', C, 'n', 0}, {nx + 1, ny, nz + 1, Lz, 'z', V, 'd', 0},
-                {nx + 1, ny + 1, nz, Lx, 'x', V, 'd', 0}, {nx + 1, ny + 1, nz, Ly, 'y', V, 'd', 0}, {nx + 1, ny + 1, nz, Lz, 'z', C, 'n', 0}};
+                {nx + 1, ny, nz, Lx, 'x', V, d, 1}, {nx + 1, ny, nz, Ly, 'y', C, b, 1}, {nx + 1, ny, nz, Lz, 'z', C, b, 1},
+                {nx, ny + 1, nz, Lx, 'x', C, b, 1}, {nx, ny + 1, nz, Ly, 'y', V, d, 1}, {nx, ny + 1, nz, Lz, 'z', C, b, 1},
+                {nx, ny, nz + 1, Lx, 'x', C, b, 1}, {nx, ny, nz + 1, Ly, 'y', C, b, 1}, {nx, ny, nz + 1, Lz, 'z', V, d, 1},
+                {nx, ny + 1, nz + 1, Lx, 'x', C, b, 0}, {nx, ny + 1, nz + 1, Ly, 'y', V, d, 0}, {nx, ny + 1, nz + 1, Lz, 'z', V, d, 0},
+                {nx + 1, ny, nz + 1, Lx, 'x', V, d, 0}, {nx + 1, ny, nz + 1, Ly, 'y', C, b, 0}, {nx + 1, ny, nz + 1, Lz, 'z', V, d, 0},
+                {nx + 1, ny + 1, nz, Lx, 'x', V, d, 0}, {nx + 1, ny + 1, nz, Ly, 'y', V, d, 0}, {nx + 1, ny + 1, nz, Lz, 'z', C, b, 0}};
             for (const P& q : passes)
                 if (wp_dwt_axis_tune<float>(scratch, q.dx, q.dy, q.dz, q.L, q.ax, q.w, q.bc, q.f, nullptr) != WP_OK) break;
             cudaDeviceSynchronize();
@@ -233,6 +348,16 @@ extern "C" CUWHHD_API wp_status wp_recover3d_project(wp_recover3d* h, float* qx,
     dim3 grid(wp_cdiv(ny, 32), wp_cdiv(nx, 8), nz);
     cudaStream_t s = (cudaStream_t)stream;
     const double bytes = 4.0 * ((double)(nx + 1) * ny * nz * 3 + (double)(nx + 1) * (ny + 1) * nz * 3);
+    if (h->bc == 'd') {
+        // the reference's l = dx_inv / n, formed in FP32 as its FP32 build does
+        const float lx = (1.f / (float)h->h[0]) / (float)nx, ly = (1.f / (float)h->h[1]) / (float)ny;
+        const float lz = (1.f / (float)h->h[2]) / (float)nz;
+        WP_KERNEL("project3d", bytes, s,
+                  project3d_nq_kernel<<<grid, dim3(32, 8), 0, s>>>(qx, qy, qz, xv, yv, zv, nx, ny, nz,
+                                                                   view(h->tab[0], nx), view(h->tab[1], ny),
+                                                                   view(h->tab[2], nz), lx, ly, lz));
+        return WP_OK;
+    }
     WP_KERNEL("project3d", bytes, s,
               project3d_kernel<<<grid, dim3(32, 8), 0, s>>>(qx, qy, qz, xv, yv, zv, nx, ny, nz, view(h->tab[0], nx),
                                                             view(h->tab[1], ny), view(h->tab[2], nz)));
@@ -247,32 +372,33 @@ extern "C" CUWHHD_API wp_status wp_recover3d_run(wp_recover3d* h, float* qx, flo
     const int Lx = h->L[0], Ly = h->L[1], Lz = h->L[2];
     const int C = WP_ID_CDF3_7, V = WP_ID_CDF4_6;
     float *tx = h->tmp[0], *ty = h->tmp[1], *tz = h->tmp[2];
+    const char b = h->bc, d = h->bcd;  // curl wavelet: the walls' type; div wavelet: the other
     wp_status st;
 #define WP_T(dst, src, DX, DY, DZ, L, ax, w, bc, f)                                          \
     if ((st = wp_dwt_axis_launch<float>(dst, src, DX, DY, DZ, L, ax, w, bc, f, s)) != WP_OK) \
         return st;
     // forward analysis (cuWaveletPotentialRecover3D.cu:32-42)
-    WP_T(tx, xv, nx + 1, ny, nz, Lx, 'x', V, 'd', 1);
-    WP_T(tx, tx, nx + 1, ny, nz, Ly, 'y', C, 'n', 1);
-    WP_T(tx, tx, nx + 1, ny, nz, Lz, 'z', C, 'n', 1);
-    WP_T(ty, yv, nx, ny + 1, nz, Lx, 'x', C, 'n', 1);
-    WP_T(ty, ty, nx, ny + 1, nz, Ly, 'y', V, 'd', 1);
-    WP_T(ty, ty, nx, ny + 1, nz, Lz, 'z', C, 'n', 1);
-    WP_T(tz, zv, nx, ny, nz + 1, Lx, 'x', C, 'n', 1);
-    WP_T(tz, tz, nx, ny, nz + 1, Ly, 'y', C, 'n', 1);
-    WP_T(tz, tz, nx, ny, nz + 1, Lz, 'z', V, 'd', 1);
+    WP_T(tx, xv, nx + 1, ny, nz, Lx, 'x', V, d, 1);
+    WP_T(tx, tx, nx + 1, ny, nz, Ly, 'y', C, b, 1);
+    WP_T(tx, tx, nx + 1, ny, nz, Lz, 'z', C, b, 1);
+    WP_T(ty, yv, nx, ny + 1, nz, Lx, 'x', C, b, 1);
+    WP_T(ty, ty, nx, ny + 1, nz, Ly, 'y', V, d, 1);
+    WP_T(ty, ty, nx, ny + 1, nz, Lz, 'z', C, b, 1);
+    WP_T(tz, zv, nx, ny, nz + 1, Lx, 'x', C, b, 1);
+    WP_T(tz, tz, nx, ny, nz + 1, Ly, 'y', C, b, 1);
+    WP_T(tz, tz, nx, ny, nz + 1, Lz, 'z', V, d, 1);
     // local projection (:46)
     if ((st = wp_recover3d_project(h, qx, qy, qz, tx, ty, tz, stream)) != WP_OK) return st;
     // inverse synthesis (:50-60)
-    WP_T(qx, qx, nx, ny + 1, nz + 1, Lx, 'x', C, 'n', 0);
-    WP_T(qx, qx, nx, ny + 1, nz + 1, Ly, 'y', V, 'd', 0);
-    WP_T(qx, qx, nx, ny + 1, nz + 1, Lz, 'z', V, 'd', 0);
-    WP_T(qy, qy, nx + 1, ny, nz + 1, Lx, 'x', V, 'd', 0);
-    WP_T(qy, qy, nx + 1, ny, nz + 1, Ly, 'y', C, 'n', 0);
-    WP_T(qy, qy, nx + 1, ny, nz + 1, Lz, 'z', V, 'd', 0);
-    WP_T(qz, qz, nx + 1, ny + 1, nz, Lx, 'x', V, 'd', 0);
-    WP_T(qz, qz, nx + 1, ny + 1, nz, Ly, 'y', V, 'd', 0);
-    WP_T(qz, qz, nx + 1, ny + 1, nz, Lz, 'z', C, 'n', 0);
+    WP_T(qx, qx, nx, ny + 1, nz + 1, Lx, 'x', C, b, 0);
+    WP_T(qx, qx, nx, ny + 1, nz + 1, Ly, 'y', V, d, 0);
+    WP_T(qx, qx, nx, ny + 1, nz + 1, Lz, 'z', V, d, 0);
+    WP_T(qy, qy, nx + 1, ny, nz + 1, Lx, 'x', V, d, 0);
+    WP_T(qy, qy, nx + 1, ny, nz + 1, Ly, 'y', C, b, 0);
+    WP_T(qy, qy, nx + 1, ny, nz + 1, Lz, 'z', V, d, 0);
+    WP_T(qz, qz, nx + 1, ny + 1, nz, Lx, 'x', V, d, 0);
+    WP_T(qz, qz, nx + 1, ny + 1, nz, Ly, 'y', V, d, 0);
+    WP_T(qz, qz, nx + 1, ny + 1, nz, Lz, 'z', C, b, 0);
 #undef WP_T
     return WP_OK;
 }
@@ -303,6 +429,10 @@ extern "C" CUWHHD_API wp_status wp_recover3d_cut(wp_recover3d* h, float* qx_out,
     if (!h || !qx_out || !qy_out || !qz_out || !qx || !qy || !qz) {
         wp_set_error_msg("wp_recover3d_cut: null pointer");
         return WP_ERR_INVALID_ARG;
+    }
+    if (h->bc != 'n') {
+        wp_set_error_msg("wp_recover3d_cut: only handles with bc 'n' (zero-normal-flux walls)");
+        return WP_ERR_UNSUPPORTED;
     }
     const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
     const int Lx = h->L[0], Ly = h->L[1], Lz = h->L[2];
