@@ -46,7 +46,10 @@ typedef enum wp_status {
 
 /* wavelet ids: same numeric values as the reference enum WaveletType (WaveletTypes.h:7-27) */
 #define WP_CDF3_5 2  /* same lifting structure as CDF3.7, 5-tap second update (wp_dwt1d only) */
+#define WP_CDF2_6 5  /* predict + 6-tap update, lines of 2^L + 1 (wp_dwt1d only) */
+#define WP_CDF4_4 6  /* CDF4.6's structure with a 4-tap second update, lines of 2^L + 1 (wp_dwt1d only) */
 #define WP_CDF4_6 7
+#define WP_CDF2_8 10 /* predict + 8-tap update, lines of 2^L + 1 (wp_dwt1d only) */
 #define WP_CDF3_7 11
 
 /* precision modes of the multigrid solve */
@@ -79,7 +82,8 @@ CUWHHD_API int wp_profile_collect(void);
 CUWHHD_API int wp_profile_entry(int i, char* name, int name_cap, long long* launches, double* ms, double* bytes);
 
 /* ------------------------------------------------------------------ 1D transforms ------- */
-/* Full-depth multilevel 1D lifting transform (CDF3.7 / CDF4.6, bc 'n' | 'd' | 'z') along
+/* Full-depth multilevel 1D lifting transform (CDF3.7 / CDF4.6 and the other families the reference
+   registers: CDF3.5, CDF4.4, CDF2.6, CDF2.8; bc 'n' | 'd' | 'z') along
    direction 'x' | 'y' | 'z' of a (dim_x, dim_y, dim_z) array; dst may equal src.
    Replaces CuWHHDForward::Solve1D(dst, src, int3 dim, level, direction, bc, type, is_forward)
    (cuWHHDForward.cuh:20-23, cuWHHDForward.cu:1122-1153). */

@@ -54,6 +54,16 @@ static const double C6_FU2[6] = {0.008544921875000, -0.064697265625000, 0.243652
 #define SQ2 1.41421356237309504880168872420969807856967187537694
 static const double C4_SCL[2] = {2.0 * SQ2, -1.0 / (2.0 * SQ2)};
 static const double C4_SCL_INV[2] = {1.0 / (2.0 * SQ2), -(2.0 * SQ2)};
+/* CDF4.4: CDF4.6's first update, predict and scaling with a 4-tap second update
+   (cuWaveletCompute.cuh:139-148, cuUpdateCdf44_ad :376-390, cuUpdateCdf44_ad_i :753-769) */
+static const double C4_FU2[4] = {-0.03906250, 0.22656250, 0.22656250, -0.03906250};
+/* CDF2.6 / CDF2.8: one predict and one update (cuWaveletCompute.cuh:72-81; cuUpdateCdf26_ad :313-334,
+   cuUpdateCdf26_ad_i :700-717, cuUpdateCdf28_ad :902-924, cuUpdateCdf28_ad_i :966-984) */
+static const double L6_FP[2] = {-0.5, -0.5};
+static const double L6_FU[6] = {0.009765625, -0.076171875, 0.31640625, 0.31640625, -0.076171875, 0.009765625};
+static const double L8_FU[8] = {-0.002136230468750, 0.020446777343750, -0.095397949218750, 0.327087402343750,
+                                0.327087402343750, -0.095397949218750, 0.020446777343750, -0.002136230468750};
+static const double L6_SCL[2] = {SQ2, 1.0 / SQ2};
 
 /* base-level matrices, row-major: cuWaveletCompute.cuh:773-797 (CDF3.7), :846-874 (CDF4.6) */
 /* CDF3.5 (cuWaveletCompute.cuh:15 RSW_Q5_fu_2, :34-45 RSW_QN5_L10 / RSW_iQN5_L10, :60-71 RSW_QD5_L10 /
@@ -119,10 +129,107 @@ static const double ICD6_L10[25] = {
     0.125000000000000, 0.312500000000000, -1.000000000000000, 0.847975710251055, -1.980451414495135,
     0, 0.281250000000000, -0.000000000000000, 0.000000000000000, -0.000000000000000};
 
-/* 'z' is the Dirichlet-with-spacing alias: CDF3.7 treats it as 'd', CDF4.6 as 'n'
-   (cuWHHDForward.cu:886-891, :970-975) */
+/* base-level matrices of CDF4.4 (RSW_CN4_L10 / RSW_iCN4_L10 / RSW_CD4_L10 / RSW_iCD4_L10) and of
+   CDF2.6 / CDF2.8 with bc 'n', 'd' and 'z' (RSW_L{N,D,Z}{6,8}_L10 and their inverses),
+   cuWaveletCompute.cuh:94-137, 150-177, 799-845 */
+static const double CN4_L10[25] = {
+    2.125, 1.6875, 0.5, -0.6875, -1.625,  -1.625, -0.6875, 0.5, 1.6875, 2.125,  1.0, 0, -2.0, 0, 1.0,
+    0.353553390593274, -0.618718433538229, 0.353553390593274, -0.088388347648318, 0,
+    0, -0.088388347648318, 0.353553390593274, -0.618718433538229, 0.353553390593274};
+static const double ICN4_L10[25] = {
+    0.34375, 0.15625, 0.25, 0.773398041922786, -0.066291260736239,
+    0.3125, 0.1875, 0, -1.016465997955662, 0.309359216769115,
+    0.25, 0.25, -0.25, 0.353553390593274, 0.353553390593274,
+    0.1875, 0.3125, 0, 0.309359216769115, -1.016465997955662,
+    0.15625, 0.34375, 0.25, -0.066291260736239, 0.773398041922786};
+static const double CD4_L10[25] = {
+    2.05078125, 0, 0, 0, 0,  0, 0, 0, 0, 2.05078125,
+    0.734375, -0.1484375, -0.46875, -0.1484375, 0.734375,
+    0.353553390593274, -0.441941738241592, 0.353553390593274, -0.088388347648318, 0,
+    0, -0.088388347648318, 0.353553390593274, -0.441941738241592, 0.353553390593274};
+static const double ICD4_L10[25] = {
+    0.125, 0, 0, 0, 0,
+    0.25, 0.125, -1.0, -2.077126169735483, 0.751300955010707,
+    0.21875, 0.21875, -1.5, 0.419844651329513, 0.419844651329513,
+    0.125, 0.25, -1.0, 0.751300955010707, -2.077126169735483,
+    0, 0.125, 0, 0, 0};
+static const double LN6_L10[25] = {
+    0.8671875, 1.265625, 0.5, -0.265625, -0.3671875,  -0.3671875, -0.265625, 0.5, 1.265625, 0.8671875,
+    -0.5, 0, 1.0, 0, -0.5,
+    -0.353553390593274, 0.707106781186547, -0.353553390593274, 0, 0,
+    0, 0, -0.353553390593274, 0.707106781186547, -0.353553390593274};
+static const double ILN6_L10[25] = {
+    0.5, 0, -0.5, -0.894932019939224, 0.187825238752677,
+    0.375, 0.125, 0, 0.789970857106846, -0.082864075920299,
+    0.25, 0.25, 0.5, -0.353553390593274, -0.353553390593274,
+    0.125, 0.375, 0, -0.082864075920299, 0.789970857106846,
+    0, 0.5, -0.5, 0.187825238752677, -0.894932019939224};
+static const double LZ6_L10[25] = {
+    0.8671875, 0.6328125, 0.25, -0.1328125, -0.3671875,  -0.3671875, -0.1328125, 0.25, 0.6328125, 0.8671875,
+    -1.0, 0, 1.0, 0, -1.0,
+    -0.707106781186547, 0.707106781186547, -0.353553390593274, 0, 0,
+    0, 0, -0.353553390593274, 0.707106781186547, -0.707106781186547};
+static const double ILZ6_L10[25] = {
+    0.5, 0, -0.25, -0.447466009969612, 0.093912619376338,
+    0.75, 0.25, 0, 0.789970857106846, -0.082864075920299,
+    0.5, 0.5, 0.5, -0.353553390593274, -0.353553390593274,
+    0.25, 0.75, 0, -0.082864075920299, 0.789970857106846,
+    0, 0.5, -0.25, 0.093912619376338, -0.447466009969612};
+static const double LD6_L10[25] = {
+    2.0, 0, 0, 0, 0,  0, 0, 0, 0, 2.0,
+    -0.69140625, 0.3828125, 0.6171875, 0.3828125, -0.69140625,
+    -0.353553390593274, 0.707106781186547, -0.353553390593274, 0, 0,
+    0, 0, -0.353553390593274, 0.707106781186547, -0.353553390593274};
+static const double ILD6_L10[25] = {
+    0.5, 0, 0, 0, 0,
+    0.375, 0.125, 0.5, 1.143524247700120, -0.270689314672975,
+    0.25, 0.25, 1.0, -0.541378629345950, -0.541378629345950,
+    0.125, 0.375, 0.5, -0.270689314672975, 1.143524247700120,
+    0, 0.5, 0, 0, 0};
+static const double LN8_L10[25] = {
+    0.85009765625, 1.2998046875, 0.5, -0.2998046875, -0.35009765625,
+    -0.35009765625, -0.2998046875, 0.5, 1.2998046875, 0.85009765625,
+    -0.5, 0, 1.0, 0, -0.5,
+    -0.353553390593274, 0.707106781186548, -0.353553390593274, 0, 0,
+    0, 0, -0.353553390593274, 0.707106781186548, -0.353553390593274};
+static const double ILN8_L10[25] = {
+    0.5, 0, -0.5, -0.919100708749311, 0.211993927562764,
+    0.375, 0.125, 0, 0.777886512701802, -0.070779731515255,
+    0.25, 0.25, 0.5, -0.353553390593274, -0.353553390593274,
+    0.125, 0.375, 0, -0.070779731515255, 0.777886512701803,
+    0, 0.5, -0.5, 0.211993927562764, -0.919100708749311};
+static const double LD8_L10[25] = {
+    0.905622728168965, 0, 0, 0, 0,  0, 0, 0, 0, 0.905622728168965,
+    -0.443145751953125, 0.39990234375, 0.60009765625, 0.39990234375, -0.443145751953125,
+    -0.353553390593274, 0.707106781186548, -0.353553390593274, 0, 0,
+    0, 0, -0.353553390593274, 0.707106781186548, -0.353553390593274};
+static const double ILD8_L10[25] = {
+    0.5, 0, 0, 0, 0,
+    0.375, 0.125, 0.5, 1.131439903295076, -0.282773659078019,
+    0.25, 0.25, 1.0, -0.565547318156037, -0.565547318156038,
+    0.125, 0.375, 0.5, -0.282773659078019, 1.131439903295076,
+    0, 0.5, 0, 0, 0};
+static const double LZ8_L10[25] = {
+    0.85009765625, 0.64990234375, 0.25, -0.14990234375, -0.35009765625,
+    -0.35009765625, -0.14990234375, 0.25, 0.64990234375, 0.85009765625,
+    -1.0, 0, 1.0, 0, -1.0,
+    -0.707106781186548, 0.707106781186548, -0.353553390593274, 0, 0,
+    0, 0, -0.353553390593274, 0.707106781186548, -0.707106781186548};
+static const double ILZ8_L10[25] = {
+    0.5, 0, -0.25, -0.459550354374656, 0.105996963781382,
+    0.75, 0.25, 0, 0.777886512701802, -0.070779731515255,
+    0.5, 0.5, 0.5, -0.353553390593274, -0.353553390593274,
+    0.25, 0.75, 0, -0.070779731515255, 0.777886512701803,
+    0, 0.5, -0.25, 0.105996963781382, -0.459550354374656};
+
+#define IS_C4(w) ((w) == OR_CDF4_6 || (w) == OR_CDF4_4)
+#define IS_L2(w) ((w) == OR_CDF2_6 || (w) == OR_CDF2_8)
+
+/* 'z' is the Dirichlet-with-spacing alias: the CDF3.x wavelets treat it as 'd', the CDF4.x ones as
+   'n' (cuWHHDForward.cu:760-765, 886-891, 970-975); CDF2.6 / CDF2.8 have their own 'z' rule
+   (cuWHHDForward.cu:802-828, cuWT_CDF2_6_z) */
 static char norm_bc(int wavelet, char bc) {
-    if (bc == 'z') return IS_Q3(wavelet) ? 'd' : 'n';
+    if (bc == 'z' && !IS_L2(wavelet)) return IS_Q3(wavelet) ? 'd' : 'n';
     return bc;
 }
 
@@ -134,6 +241,20 @@ static const double* base_matrix(int wavelet, char bc, int forward) {
     if (wavelet == OR_CDF3_7) {
         if (bc == 'n') return forward ? QN7_L10 : IQN7_L10;
         return forward ? QD7_L10 : IQD7_L10;
+    }
+    if (wavelet == OR_CDF4_4) {
+        if (bc == 'n') return forward ? CN4_L10 : ICN4_L10;
+        return forward ? CD4_L10 : ICD4_L10;
+    }
+    if (wavelet == OR_CDF2_6) {
+        if (bc == 'n') return forward ? LN6_L10 : ILN6_L10;
+        if (bc == 'z') return forward ? LZ6_L10 : ILZ6_L10;
+        return forward ? LD6_L10 : ILD6_L10;
+    }
+    if (wavelet == OR_CDF2_8) {
+        if (bc == 'n') return forward ? LN8_L10 : ILN8_L10;
+        if (bc == 'z') return forward ? LZ8_L10 : ILZ8_L10;
+        return forward ? LD8_L10 : ILD8_L10;
     }
     if (bc == 'n') return forward ? CN6_L10 : ICN6_L10;
     return forward ? CD6_L10 : ICD6_L10;
@@ -153,11 +274,20 @@ static void fwd_reflect(int wavelet, char bc, int k, int L, int* ai, int* di, do
         else if (a >= L) { a = 2 * L - 1 - a; if (bc == 'd') s_a = -1.0; }
         if (d < 0) { d = -1 - d; if (bc == 'd') s_d = -1.0; }
         else if (d >= L) { d = 2 * L - 1 - d; if (bc == 'd') s_d = -1.0; }
+    } else if (IS_L2(wavelet) && bc == 'd') {
+        /* cuWT_CDF2_6_d (cuWaveletCompute.cuh:271-294): a whole-sample reflection of a with no sign,
+           d reflected separately with a negative sign */
+        if (a < 0) a = -a;
+        else if (a > L) a = 2 * L - a;
+        if (d < 0) { d = -d; s_d = -1.0; }
+        else if (d >= L) { d = 2 * L - d; s_d = -1.0; }
     } else {
         int a_orig = a;
         if (a < 0) { a = -a; d = -d; if (bc == 'd') { s_a = -1.0; s_d = -1.0; } }
         else if (a >= L) { a = 2 * L - a; d = 2 * L - d; if (bc == 'd') { s_a = -1.0; s_d = -1.0; } }
         if (bc == 'd' && a_orig == L) s_a = 1.0;
+        /* cuWT_CDF2_6_z (:296-311): the boundary samples count twice */
+        if (bc == 'z' && (a == 0 || a == L)) s_a = 2.0;
     }
     if (d < 0) d = 0; /* cuWHHDForward.cu:52 clamps the odd index */
     *ai = a; *di = d; *sa = s_a; *sd = s_d;
@@ -172,9 +302,16 @@ static void inv_reflect(int wavelet, char bc, int k, int L, int* ai, int* di, do
         if (a < 0) { a = -1 - a; if (bc == 'n') s_d = -1.0; else s_a = -1.0; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bc == 'n') s_d = -1.0; else s_a = -1.0; }
         d = a;
-    } else if (bc == 'n') {
+    } else if (bc == 'n' || bc == 'z') {
+        /* cuWT_CDF2_6_z_i (:684-699): the sign is 2 at the two boundary indices, read before the
+           reflection */
+        if (bc == 'z' && (a == 0 || a == L)) s_a = 2.0;
         if (a < 0) { a = -a; d = -d - 1; }
         else if (a >= L) { a = 2 * L - a; d = 2 * L - d - 1; }
+    } else if (IS_L2(wavelet)) {
+        /* cuWT_CDF2_6_d_i (:668-683) */
+        if (a < 0) { a = -a; d = -d - 1; s_d = -1.0; }
+        else if (a >= L) { a = 2 * L - a; d = 2 * L - d - 1; s_d = -1.0; }
     } else {
         if (a < 0) { a = -a; d = -d - 1; s_d = -1.0; s_a = -1.0; }
         else if (a >= L) { d = 2 * L - d - 1; s_d = -1.0; }
@@ -203,7 +340,28 @@ static void fwd_level(const double* x, int L, int ext, int wavelet, char bc, dou
         D0[IX(k)] = (di >= 0 && di < n_in) ? sd * x[di] : 0.0;
     }
     for (int k = K0; k < K1; ++k) { A1[IX(k)] = 0.0; D1[IX(k)] = 0.0; }
-    if (IS_Q3(wavelet)) {
+    if (IS_L2(wavelet)) {
+        /* predict with the signed approximations, then the detail's own sign, then the update;
+           the approximation's sign is divided out at the end (cuUpdateCdf26_ad / cuUpdateCdf28_ad) */
+        const double* fu = wavelet == OR_CDF2_6 ? L6_FU : L8_FU;
+        const int nt = wavelet == OR_CDF2_6 ? 6 : 8, lo = nt / 2; /* taps k - lo .. k + lo - 1 */
+        double* SA = D1 + W;
+        double* SD = SA + W;
+        for (int k = K0; k < K1; ++k) {
+            int ai, di; double sa, sd;
+            fwd_reflect(wavelet, bc, k, L, &ai, &di, &sa, &sd);
+            D0[IX(k)] = (di >= 0 && di < n_in) ? x[di] : 0.0; /* the detail's sign comes after the predict */
+            SA[IX(k)] = sa; SD[IX(k)] = sd;
+        }
+        for (int k = K0; k < K1 - 1; ++k)
+            D1[IX(k)] = (D0[IX(k)] + L6_FP[0] * A0[IX(k)] + L6_FP[1] * A0[IX(k + 1)]) * SD[IX(k)];
+        for (int k = 0; k < M; ++k) {
+            double s = A0[IX(k)];
+            for (int t = 0; t < nt; ++t) s += fu[nt - 1 - t] * D1[IX(k - lo + t)];
+            a_out[k] = s * L6_SCL[0] / SA[IX(k)];
+        }
+        for (int k = 0; k < L / 2; ++k) d_out[k] = D1[IX(k)] * L6_SCL[1];
+    } else if (IS_Q3(wavelet)) {
         const double* fu2 = wavelet == OR_CDF3_5 ? Q5_FU2 : Q7_FU2;
         const int hw = wavelet == OR_CDF3_5 ? 2 : 3;
         for (int k = K0 + 1; k < K1; ++k) A1[IX(k)] = A0[IX(k)] + Q5_FU1 * D0[IX(k - 1)];
@@ -222,8 +380,12 @@ static void fwd_level(const double* x, int L, int ext, int wavelet, char bc, dou
             D1[IX(k)] = D0[IX(k)] + C4_FP[1] * A1[IX(k)] + C4_FP[0] * A1[IX(k + 1)];
         for (int k = 0; k < M; ++k) {
             double s = A1[IX(k)];
-            s += C6_FU2[5] * D1[IX(k - 3)] + C6_FU2[4] * D1[IX(k - 2)] + C6_FU2[3] * D1[IX(k - 1)] +
-                 C6_FU2[2] * D1[IX(k)] + C6_FU2[1] * D1[IX(k + 1)] + C6_FU2[0] * D1[IX(k + 2)];
+            if (wavelet == OR_CDF4_4)
+                s += C4_FU2[3] * D1[IX(k - 2)] + C4_FU2[2] * D1[IX(k - 1)] + C4_FU2[1] * D1[IX(k)] +
+                     C4_FU2[0] * D1[IX(k + 1)];
+            else
+                s += C6_FU2[5] * D1[IX(k - 3)] + C6_FU2[4] * D1[IX(k - 2)] + C6_FU2[3] * D1[IX(k - 1)] +
+                     C6_FU2[2] * D1[IX(k)] + C6_FU2[1] * D1[IX(k + 1)] + C6_FU2[0] * D1[IX(k + 2)];
             a_out[k] = s * C4_SCL[0];
         }
         for (int k = 0; k < L / 2; ++k) d_out[k] = D1[IX(k)] * C4_SCL[1];
@@ -251,7 +413,21 @@ static void inv_level(const double* a, const double* d, int L, int ext, int wave
         D[IX(k)] = (di >= 0 && di < L) ? d[di] : 0.0;
         SA[IX(k)] = sa; SD[IX(k)] = sd;
     }
-    if (IS_Q3(wavelet)) {
+    if (IS_L2(wavelet)) {
+        const double* fu = wavelet == OR_CDF2_6 ? L6_FU : L8_FU;
+        const int nt = wavelet == OR_CDF2_6 ? 6 : 8, lo = nt / 2;
+        for (int k = K0; k < K1; ++k) {
+            D[IX(k)] = SD[IX(k)] * D[IX(k)] * L6_SCL[0];
+            A[IX(k)] = SA[IX(k)] * A[IX(k)] * L6_SCL[1];
+        }
+        for (int k = K0 + lo; k < K1 - lo; ++k) {
+            double t = A[IX(k)];
+            for (int j = 0; j < nt; ++j) t -= fu[nt - 1 - j] * D[IX(k - lo + j)];
+            T[IX(k)] = t;
+        }
+        for (int k = 0; k < NA; ++k) x[2 * k] = T[IX(k)] / SA[IX(k)];
+        for (int k = 0; k < L; ++k) x[2 * k + 1] = D[IX(k)] - (L6_FP[1] * T[IX(k)] + L6_FP[0] * T[IX(k + 1)]);
+    } else if (IS_Q3(wavelet)) {
         const double* fu2 = wavelet == OR_CDF3_5 ? Q5_FU2 : Q7_FU2;
         const int hw = wavelet == OR_CDF3_5 ? 2 : 3;
         for (int k = K0; k < K1; ++k) {
@@ -272,8 +448,11 @@ static void inv_level(const double* a, const double* d, int L, int ext, int wave
             A[IX(k)] = SA[IX(k)] * A[IX(k)] * C4_SCL_INV[0];
         }
         for (int k = K0 + 3; k < K1 - 2; ++k) {
-            double s = C6_FU2[5] * D[IX(k - 3)] + C6_FU2[4] * D[IX(k - 2)] + C6_FU2[3] * D[IX(k - 1)] +
-                       C6_FU2[2] * D[IX(k)] + C6_FU2[1] * D[IX(k + 1)] + C6_FU2[0] * D[IX(k + 2)];
+            double s = wavelet == OR_CDF4_4
+                           ? C4_FU2[3] * D[IX(k - 2)] + C4_FU2[2] * D[IX(k - 1)] + C4_FU2[1] * D[IX(k)] +
+                                 C4_FU2[0] * D[IX(k + 1)]
+                           : C6_FU2[5] * D[IX(k - 3)] + C6_FU2[4] * D[IX(k - 2)] + C6_FU2[3] * D[IX(k - 1)] +
+                                 C6_FU2[2] * D[IX(k)] + C6_FU2[1] * D[IX(k + 1)] + C6_FU2[0] * D[IX(k + 2)];
             T[IX(k)] = SA[IX(k)] * (A[IX(k)] - s); /* A3 = sign_a * A2 */
         }
         for (int k = K0; k < K1; ++k) D[IX(k)] = SD[IX(k)] * D[IX(k)]; /* D2 = sign_d * D1 */
@@ -287,11 +466,13 @@ static void inv_level(const double* a, const double* d, int L, int ext, int wave
 
 /* ----------------------------------------------------------------- full 1D line ---- */
 int or_dwt_line(double* line, int n, int levels, int wavelet, char bc, int forward) {
-    if (!IS_Q3(wavelet) && wavelet != OR_CDF4_6) return 2;
+    if (!IS_Q3(wavelet) && !IS_C4(wavelet) && !IS_L2(wavelet)) return 2;
     bc = norm_bc(wavelet, bc);
-    if (bc != 'n' && bc != 'd') return 2;
+    if (bc != 'n' && bc != 'd' && !(bc == 'z' && IS_L2(wavelet))) return 2;
     int ext = n & 1;
     if (levels < 2 || (1 << levels) != n - ext) return 1;
+    /* the CDF4.4 and CDF2.x base matrices act on 5 coefficients: whole-sample lines of 2^L + 1 */
+    if ((wavelet == OR_CDF4_4 || IS_L2(wavelet)) && !ext) return 1;
     int nb = 4 + ext;
     double* buf = (double*)malloc(sizeof(double) * (size_t)(2 * n + 16));
     double* tmp = buf + n + 8;

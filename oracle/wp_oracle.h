@@ -20,7 +20,10 @@ extern "C" {
 
 /* wavelet identifiers: same numeric values as the reference enum (WaveletTypes.h:7-27) */
 #define OR_CDF3_5 2
+#define OR_CDF2_6 5
+#define OR_CDF4_4 6
 #define OR_CDF4_6 7
+#define OR_CDF2_8 10
 #define OR_CDF3_7 11
 
 /* one full-depth 1D transform of a line in place (cuWHHDForward.cu:5-105 forward, :349-464 inverse) */

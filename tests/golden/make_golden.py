@@ -12,6 +12,7 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only dst     # CuDst3D::Solve only
     python tests/golden/make_golden.py --only psweep  # CuParallelSweep3D Solve / Project only
     python tests/golden/make_golden.py --only domd    # projection and recovery with Dirichlet walls
+    python tests/golden/make_golden.py --only families  # CDF2.6 / CDF2.8 / CDF4.4 transforms
     ... [--out DIR]                                   # write the .npz files to DIR instead of here
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
@@ -38,7 +39,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 from waveletpotentials_b200.fields import porous_fractions  # noqa: E402
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
-CDF3_5, CDF4_6, CDF3_7 = 2, 7, 11
+CDF3_5, CDF2_6, CDF4_4, CDF4_6, CDF2_8, CDF3_7 = 2, 5, 6, 7, 10, 11
 
 
 def run(op, inputs: dict, params, outputs: dict):
@@ -202,6 +203,34 @@ def cdf35_cases(rng):
     save("dwt1d_cdf35", **dwt)
 
 
+def families_cases(rng):
+    """CuWHHDForward::Solve1D with the other whole-sample families the reference registers
+    (cuWHHDForward.cu:788-870, 914-956): CDF2.6, CDF2.8 and CDF4.4 on lines of 2^L + 1 samples,
+    every axis, the boundary types 'n', 'd' and 'z' (CDF2.x have a rule of their own for 'z', CDF4.4
+    treats it as 'n'), both directions, and a 257-point line."""
+    dwt = {}
+    for wav in (CDF2_6, CDF2_8, CDF4_4):
+        for bc in "ndz":
+            for fwd in (1, 0):
+                for axis, (L, other) in {"y": (4, (3, 2)), "x": (5, (4, 3)), "z": (3, (5, 2))}.items():
+                    n = (1 << L) + 1
+                    DX, DY, DZ = {"y": (other[0], n, other[1]), "x": (n, other[0], other[1]),
+                                  "z": (other[0], other[1], n)}[axis]
+                    a = rng.standard_normal((DZ, DX, DY))
+                    out = run("dwt1d", {"a": a}, [DX, DY, DZ, L, axis, bc, wav, fwd], {"c": (DZ, DX, DY)})
+                    key = f"w{wav}_{bc}_{'f' if fwd else 'i'}_{axis}"
+                    dwt[key + "_in"] = a
+                    dwt[key + "_out"] = out["c"]
+                    dwt[key + "_meta"] = np.array([DX, DY, DZ, L, ord(axis), ord(bc), wav, fwd])
+                a = rng.standard_normal((1, 2, 257))
+                out = run("dwt1d", {"a": a}, [2, 257, 1, 8, "y", bc, wav, fwd], {"c": (1, 2, 257)})
+                key = f"w{wav}_{bc}_{'f' if fwd else 'i'}_long"
+                dwt[key + "_in"] = a
+                dwt[key + "_out"] = out["c"]
+                dwt[key + "_meta"] = np.array([2, 257, 1, 8, ord("y"), ord(bc), wav, fwd])
+    save("dwt1d_families", **dwt)
+
+
 def dst_cases(rng):
     """CuDst3D::Solve (the Dirichlet Poisson solve by DST-I along each axis, cuDst3D.cu:265-341) on
     grids of equal extents (its constructor's buffer sizing is only safe there, cuDst3D.cu:209-211):
@@ -302,6 +331,9 @@ def main():
         return
     if only == "domd":
         domd_cases(np.random.default_rng(20261211))
+        return
+    if only == "families":
+        families_cases(np.random.default_rng(20261212))
         return
     rng = np.random.default_rng(20261203)
 

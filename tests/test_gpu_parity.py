@@ -26,7 +26,7 @@ def rel(ref, got):
     return float(np.sqrt(np.sum((ref - got) ** 2) / max(np.sum(ref * ref), 1e-300)))
 
 
-@pytest.mark.parametrize("name", ["dwt1d", "dwt1d_cdf35"])
+@pytest.mark.parametrize("name", ["dwt1d", "dwt1d_cdf35", "dwt1d_families"])
 def test_dwt1d_fp32_and_fp64_match_reference(wp, name):
     d = load_golden(name)
     cases = [k[:-5] for k in d.files if k.endswith("_meta")]

@@ -195,3 +195,17 @@ def test_recovery_with_dirichlet_walls_reproduces_any_divergence_free_field(orac
     r = oracle.recover3d(*u, n, d, bc="n")
     c = fields.curl3d(*r, n, d)
     assert np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u, c)) / den) > 1e-2
+
+
+@pytest.mark.parametrize("wav", [5, 10, 6])  # CDF2.6, CDF2.8, CDF4.4
+@pytest.mark.parametrize("bc", ["n", "d", "z"])
+@pytest.mark.parametrize("levels", [2, 3, 5, 8])
+def test_perfect_reconstruction_of_the_whole_sample_families(oracle, wav, bc, levels):
+    """The other families of the 1D transform on lines of 2^L + 1 samples: analysis then synthesis
+    gives the line back (with 'd', the odd extension, on lines that vanish at both ends)."""
+    rng = np.random.default_rng(levels + wav)
+    x = rng.standard_normal((1 << levels) + 1)
+    if bc == "d":
+        x[0] = x[-1] = 0.0
+    c = oracle.dwt_line(x, levels, wav, bc, True)
+    np.testing.assert_allclose(oracle.dwt_line(c, levels, wav, bc, False), x, atol=1e-12)

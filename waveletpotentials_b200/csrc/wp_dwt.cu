@@ -29,11 +29,14 @@ namespace {
 // Coefficient pairs per thread per level: 8, or 9 for CDF4.6, whose lines have 2^L + 1 samples in the
 // recovery: the 2^(L-1) + 1 approximations of the top level then split into 15 chunks (two rounds of
 // a 256-thread tile of 32 columns) instead of 17 (three rounds, the last one eighth full).
-__host__ __device__ constexpr int ch_of(int wav) { return wav == WP_ID_CDF4_6 ? 9 : 8; }
+__host__ __device__ constexpr int ch_of(int wav) {
+    return (wav == WP_ID_CDF4_6 || wav == WP_ID_CDF4_4 || wav == WP_ID_CDF2_6 || wav == WP_ID_CDF2_8) ? 9 : 8;
+}
 constexpr int NT = 256;      // threads per CTA
 
 // lifting constants (cuWaveletCompute.cuh:13-23, :139-148)
 #define WP_SQ2 1.41421356237309504880168872420969807856967187537694
+#define WP_SQ2_D 1.414213562373095048801
 struct K37 {
     static constexpr double fu1 = -1.0 / 3.0;
     static constexpr double fp0 = -3.0 / 8.0, fp1 = -9.0 / 8.0;
@@ -54,6 +57,28 @@ struct K3 : K37 {};
 template <>
 struct K3<WP_ID_CDF3_5> : K35 {};
 __host__ __device__ constexpr bool is_q3(int w) { return w == WP_ID_CDF3_7 || w == WP_ID_CDF3_5; }
+__host__ __device__ constexpr bool is_c4(int w) { return w == WP_ID_CDF4_6 || w == WP_ID_CDF4_4; }
+__host__ __device__ constexpr bool is_l2(int w) { return w == WP_ID_CDF2_6 || w == WP_ID_CDF2_8; }
+// CDF2.6 / CDF2.8 (cuWaveletCompute.cuh:72-81): a predict from the two neighbouring approximations and
+// one update from NT details at offsets -NT/2 .. NT/2 - 1; u[i] weighs offset NT/2 - 1 - i
+template <int WAV>
+struct K2 {
+    static constexpr double fp0 = -0.5, fp1 = -0.5;
+    static constexpr double scl0 = WP_SQ2_D, scl1 = 1.0 / WP_SQ2_D;
+    static constexpr int NTAP = WAV == WP_ID_CDF2_6 ? 6 : 8;
+    __host__ __device__ static constexpr double u(int i) {
+        return WAV == WP_ID_CDF2_6
+                   ? (i == 0 ? 0.009765625 : i == 1 ? -0.076171875 : i == 2 ? 0.31640625 : i == 3 ? 0.31640625
+                      : i == 4 ? -0.076171875 : 0.009765625)
+                   : (i == 0 ? -0.002136230468750 : i == 1 ? 0.020446777343750 : i == 2 ? -0.095397949218750
+                      : i == 3 ? 0.327087402343750 : i == 4 ? 0.327087402343750 : i == 5 ? -0.095397949218750
+                      : i == 6 ? 0.020446777343750 : -0.002136230468750);
+    }
+};
+// CDF4.4's second update (RSW_C4_fu_2): d4_i weighs offset 1 - i
+struct K44 {
+    static constexpr double d0 = -0.03906250, d1 = 0.22656250, d2 = 0.22656250, d3 = -0.03906250;
+};
 struct K46 {
     static constexpr double fu1_0 = -0.25, fu1_1 = -0.25;
     static constexpr double fp0 = -1.0, fp1 = -1.0;
@@ -67,6 +92,10 @@ struct K46 {
 __constant__ double c_base37[4][16];
 __constant__ double c_base35[4][16];
 __constant__ double c_base46[4][25];
+// CDF4.4: forward n, forward d, inverse n, inverse d; CDF2.6 / CDF2.8: forward n, d, z, inverse n, d, z
+__constant__ double c_base44[4][25];
+__constant__ double c_base26[6][25];
+__constant__ double c_base28[6][25];
 
 const double h_base37[4][16] = {
     {0.500000000000000, 0.500000000000000, 0.500000000000000, 0.500000000000000, -0.399902343750000,
@@ -93,6 +122,27 @@ const double h_base35[4][16] = {
      0.165728151840597, -1.248485410532498, 0.5, 1.0, -0.375650477505353, 1.038563084867742},
     {0.125, -0.25, -0.894932019939224, 0.187825238752677, 0.25, -0.25, 0.685009694274468, 0.02209708691208, 0.25,
      0.25, -0.02209708691208, -0.685009694274468, 0.125, 0.25, -0.187825238752677, 0.894932019939224}};
+// base-level matrices of CDF4.4 and CDF2.6 / CDF2.8 (cuWaveletCompute.cuh:94-137, 150-177, 799-845:
+// RSW_CN4_L10, RSW_CD4_L10, RSW_L{N,D,Z}{6,8}_L10 and their inverses)
+const double h_base44[4][25] = {
+    {2.125, 1.6875, 0.5, -0.6875, -1.625, -1.625, -0.6875, 0.5, 1.6875, 2.125, 1.0, 0, -2.0, 0, 1.0, 0.353553390593274, -0.618718433538229, 0.353553390593274, -0.088388347648318, 0, 0, -0.088388347648318, 0.353553390593274, -0.618718433538229, 0.353553390593274},
+    {2.05078125, 0, 0, 0, 0, 0, 0, 0, 0, 2.05078125, 0.734375, -0.1484375, -0.46875, -0.1484375, 0.734375, 0.353553390593274, -0.441941738241592, 0.353553390593274, -0.088388347648318, 0, 0, -0.088388347648318, 0.353553390593274, -0.441941738241592, 0.353553390593274},
+    {0.34375, 0.15625, 0.25, 0.773398041922786, -0.066291260736239, 0.3125, 0.1875, 0, -1.016465997955662, 0.309359216769115, 0.25, 0.25, -0.25, 0.353553390593274, 0.353553390593274, 0.1875, 0.3125, 0, 0.309359216769115, -1.016465997955662, 0.15625, 0.34375, 0.25, -0.066291260736239, 0.773398041922786},
+    {0.125, 0, 0, 0, 0, 0.25, 0.125, -1.0, -2.077126169735483, 0.751300955010707, 0.21875, 0.21875, -1.5, 0.419844651329513, 0.419844651329513, 0.125, 0.25, -1.0, 0.751300955010707, -2.077126169735483, 0, 0.125, 0, 0, 0}};
+const double h_base26[6][25] = {
+    {0.8671875, 1.265625, 0.5, -0.265625, -0.3671875, -0.3671875, -0.265625, 0.5, 1.265625, 0.8671875, -0.5, 0, 1.0, 0, -0.5, -0.353553390593274, 0.707106781186547, -0.353553390593274, 0, 0, 0, 0, -0.353553390593274, 0.707106781186547, -0.353553390593274},
+    {2.0, 0, 0, 0, 0, 0, 0, 0, 0, 2.0, -0.69140625, 0.3828125, 0.6171875, 0.3828125, -0.69140625, -0.353553390593274, 0.707106781186547, -0.353553390593274, 0, 0, 0, 0, -0.353553390593274, 0.707106781186547, -0.353553390593274},
+    {0.8671875, 0.6328125, 0.25, -0.1328125, -0.3671875, -0.3671875, -0.1328125, 0.25, 0.6328125, 0.8671875, -1.0, 0, 1.0, 0, -1.0, -0.707106781186547, 0.707106781186547, -0.353553390593274, 0, 0, 0, 0, -0.353553390593274, 0.707106781186547, -0.707106781186547},
+    {0.5, 0, -0.5, -0.894932019939224, 0.187825238752677, 0.375, 0.125, 0, 0.789970857106846, -0.082864075920299, 0.25, 0.25, 0.5, -0.353553390593274, -0.353553390593274, 0.125, 0.375, 0, -0.082864075920299, 0.789970857106846, 0, 0.5, -0.5, 0.187825238752677, -0.894932019939224},
+    {0.5, 0, 0, 0, 0, 0.375, 0.125, 0.5, 1.143524247700120, -0.270689314672975, 0.25, 0.25, 1.0, -0.541378629345950, -0.541378629345950, 0.125, 0.375, 0.5, -0.270689314672975, 1.143524247700120, 0, 0.5, 0, 0, 0},
+    {0.5, 0, -0.25, -0.447466009969612, 0.093912619376338, 0.75, 0.25, 0, 0.789970857106846, -0.082864075920299, 0.5, 0.5, 0.5, -0.353553390593274, -0.353553390593274, 0.25, 0.75, 0, -0.082864075920299, 0.789970857106846, 0, 0.5, -0.25, 0.093912619376338, -0.447466009969612}};
+const double h_base28[6][25] = {
+    {0.85009765625, 1.2998046875, 0.5, -0.2998046875, -0.35009765625, -0.35009765625, -0.2998046875, 0.5, 1.2998046875, 0.85009765625, -0.5, 0, 1.0, 0, -0.5, -0.353553390593274, 0.707106781186548, -0.353553390593274, 0, 0, 0, 0, -0.353553390593274, 0.707106781186548, -0.353553390593274},
+    {0.905622728168965, 0, 0, 0, 0, 0, 0, 0, 0, 0.905622728168965, -0.443145751953125, 0.39990234375, 0.60009765625, 0.39990234375, -0.443145751953125, -0.353553390593274, 0.707106781186548, -0.353553390593274, 0, 0, 0, 0, -0.353553390593274, 0.707106781186548, -0.353553390593274},
+    {0.85009765625, 0.64990234375, 0.25, -0.14990234375, -0.35009765625, -0.35009765625, -0.14990234375, 0.25, 0.64990234375, 0.85009765625, -1.0, 0, 1.0, 0, -1.0, -0.707106781186548, 0.707106781186548, -0.353553390593274, 0, 0, 0, 0, -0.353553390593274, 0.707106781186548, -0.707106781186548},
+    {0.5, 0, -0.5, -0.919100708749311, 0.211993927562764, 0.375, 0.125, 0, 0.777886512701802, -0.070779731515255, 0.25, 0.25, 0.5, -0.353553390593274, -0.353553390593274, 0.125, 0.375, 0, -0.070779731515255, 0.777886512701803, 0, 0.5, -0.5, 0.211993927562764, -0.919100708749311},
+    {0.5, 0, 0, 0, 0, 0.375, 0.125, 0.5, 1.131439903295076, -0.282773659078019, 0.25, 0.25, 1.0, -0.565547318156037, -0.565547318156038, 0.125, 0.375, 0.5, -0.282773659078019, 1.131439903295076, 0, 0.5, 0, 0, 0},
+    {0.5, 0, -0.25, -0.459550354374656, 0.105996963781382, 0.75, 0.25, 0, 0.777886512701802, -0.070779731515255, 0.5, 0.5, 0.5, -0.353553390593274, -0.353553390593274, 0.25, 0.75, 0, -0.070779731515255, 0.777886512701803, 0, 0.5, -0.25, 0.105996963781382, -0.459550354374656}};
 const double h_base46[4][25] = {
     {1.851562500000001, 2.097656250000000, 0.500000000000000, -1.097656250000000, -1.351562500000000,
      -1.351562500000000, -1.097656250000000, 0.500000000000000, 2.097656250000000, 1.851562500000001,
@@ -123,6 +173,17 @@ __device__ __forceinline__ void fwd_reflect(int k, int L, int bcd, int& ai, int&
         else if (a >= L) { a = 2 * L - 1 - a; if (bcd) s_a = -1.f; }
         if (d < 0) { d = -1 - d; if (bcd) s_d = -1.f; }
         else if (d >= L) { d = 2 * L - 1 - d; if (bcd) s_d = -1.f; }
+    } else if (is_l2(WAV) && bcd == 1) {
+        // cuWT_CDF2_6_d (cuWaveletCompute.cuh:271-294): a reflected without a sign, d with one
+        if (a < 0) a = -a;
+        else if (a > L) a = 2 * L - a;
+        if (d < 0) { d = -d; s_d = -1.f; }
+        else if (d >= L) { d = 2 * L - d; s_d = -1.f; }
+    } else if (is_l2(WAV)) {
+        // cuWT_CDF2_6_n (:255-269) and _z (:296-311, the boundary samples count twice)
+        if (a < 0) { a = -a; d = -d; }
+        else if (a >= L) { a = 2 * L - a; d = 2 * L - d; }
+        if (bcd == 2 && (a == 0 || a == L)) s_a = 2.f;
     } else {
         const int a0 = a;
         if (a < 0) { a = -a; d = -d; if (bcd) { s_a = -1.f; s_d = -1.f; } }
@@ -141,7 +202,13 @@ __device__ __forceinline__ void inv_reflect(int k, int L, int bcd, int& ai, int&
         if (a < 0) { a = -1 - a; if (bcd) s_a = -1.f; else s_d = -1.f; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bcd) s_a = -1.f; else s_d = -1.f; }
         d = a;
-    } else if (!bcd) {
+    } else if (is_l2(WAV) && bcd == 1) {
+        // cuWT_CDF2_6_d_i (cuWaveletCompute.cuh:668-683)
+        if (a < 0) { a = -a; d = -d - 1; s_d = -1.f; }
+        else if (a >= L) { a = 2 * L - a; d = 2 * L - d - 1; s_d = -1.f; }
+    } else if (bcd != 1) {
+        // 'n' (and CDF2.x's 'z', cuWT_CDF2_6_z_i :684-699, sign 2 at the two boundary indices)
+        if (bcd == 2 && (a == 0 || a == L)) s_a = 2.f;
         if (a < 0) { a = -a; d = -d - 1; }
         else if (a >= L) { a = 2 * L - a; d = 2 * L - d - 1; }
     } else {
@@ -299,23 +366,49 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
             for (int t = tid; t < C * nch; t += NT) {
                 const int col = t % C, k0 = (t / C) * CH;
                 T A[WIN], Dd[WIN];
-                if (k0 >= 4 && 2 * (k0 + WIN - 4) <= L) {
-                    // interior window: no reflection
+                // CDF2.x: the detail's reflection sign applies after the predict and the approximation's
+                // is divided out at the end (cuUpdateCdf26_ad), so they are kept apart from the values
+                T SAw[WIN], SDw[WIN];
+                if (k0 >= 4 + (bcd == 2) && 2 * (k0 + WIN - 4) <= L) {
+                    // interior window: no reflection (CDF2.x 'z' weighs the boundary samples twice)
                     const T* base = S + (2 * (k0 - 4)) * CP + col;
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) {
                         A[w] = base[(2 * w) * CP];
                         Dd[w] = base[(2 * w + 1) * CP];
+                        SAw[w] = T(1);
+                        SDw[w] = T(1);
                     }
                 } else {
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) {
                         const int4 e = tb[k0 + w];
                         A[w] = T(__int_as_float(e.z)) * S[e.x * CP + col];
-                        Dd[w] = T(__int_as_float(e.w)) * S[e.y * CP + col];
+                        if (is_l2(WAV)) {
+                            Dd[w] = S[e.y * CP + col];
+                            SAw[w] = T(__int_as_float(e.z));
+                            SDw[w] = T(__int_as_float(e.w));
+                        } else {
+                            Dd[w] = T(__int_as_float(e.w)) * S[e.y * CP + col];
+                        }
                     }
                 }
-                if (is_q3(WAV)) {
+                if (is_l2(WAV)) {
+                    constexpr int NTP = K2<WAV>::NTAP, LO = NTP / 2;
+#pragma unroll
+                    for (int w = 0; w < WIN - 1; ++w)
+                        Dd[w] = (Dd[w] + T(K2<WAV>::fp0) * A[w] + T(K2<WAV>::fp1) * A[w + 1]) * SDw[w];
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4;
+                        T s = A[w];
+#pragma unroll
+                        for (int t = 0; t < NTP; ++t) s = s + T(K2<WAV>::u(NTP - 1 - t)) * Dd[w - LO + t];
+                        const int k = k0 + j;
+                        if (k < M) D[k * CP + col] = s * T(K2<WAV>::scl0) / SAw[w];
+                        if (k < nd) D[(M + k) * CP + col] = Dd[w] * T(K2<WAV>::scl1);
+                    }
+                } else if (is_q3(WAV)) {
 #pragma unroll
                     for (int w = WIN - 1; w >= 1; --w) A[w] = A[w] + T(K37::fu1) * Dd[w - 1];
 #pragma unroll
@@ -339,8 +432,11 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
 #pragma unroll
                     for (int j = 0; j < CH; ++j) {
                         const int w = j + 4;
-                        T s = A[w] + T(K46::c5) * Dd[w - 3] + T(K46::c4) * Dd[w - 2] + T(K46::c3) * Dd[w - 1] +
-                              T(K46::c2) * Dd[w] + T(K46::c1) * Dd[w + 1] + T(K46::c0) * Dd[w + 2];
+                        T s = WAV == WP_ID_CDF4_4
+                                  ? A[w] + T(K44::d3) * Dd[w - 2] + T(K44::d2) * Dd[w - 1] + T(K44::d1) * Dd[w] +
+                                        T(K44::d0) * Dd[w + 1]
+                                  : A[w] + T(K46::c5) * Dd[w - 3] + T(K46::c4) * Dd[w - 2] + T(K46::c3) * Dd[w - 1] +
+                                        T(K46::c2) * Dd[w] + T(K46::c1) * Dd[w + 1] + T(K46::c0) * Dd[w + 2];
                         const int k = k0 + j;
                         if (k < M) D[k * CP + col] = s * T(K46::scl0);
                         if (k < nd) D[(M + k) * CP + col] = Dd[w] * T(K46::scl1);
@@ -351,13 +447,22 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
             cur ^= 1;
         }
         // base level: nb x nb matrix on the remaining approximation coefficients
-        const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[bcd] : (WAV == WP_ID_CDF3_5 ? c_base35[bcd] : c_base46[bcd]);
+        const double* mat = WAV == WP_ID_CDF3_7   ? c_base37[bcd]
+                            : WAV == WP_ID_CDF3_5 ? c_base35[bcd]
+                            : WAV == WP_ID_CDF4_4 ? c_base44[bcd]
+                            : WAV == WP_ID_CDF2_6 ? c_base26[bcd]
+                            : WAV == WP_ID_CDF2_8 ? c_base28[bcd]
+                                                  : c_base46[bcd];
         if (tid < C) base_level<T>(mat, nb, buf(cur) + tid, buf(cur ^ 1) + tid, CP);
         __syncthreads();
         outbuf = -1;  // position dependent, resolved below
     } else {
-        const double* mat = (WAV == WP_ID_CDF3_7) ? c_base37[2 + bcd]
-                                                  : (WAV == WP_ID_CDF3_5 ? c_base35[2 + bcd] : c_base46[2 + bcd]);
+        const double* mat = WAV == WP_ID_CDF3_7   ? c_base37[2 + bcd]
+                            : WAV == WP_ID_CDF3_5 ? c_base35[2 + bcd]
+                            : WAV == WP_ID_CDF4_4 ? c_base44[2 + bcd]
+                            : WAV == WP_ID_CDF2_6 ? c_base26[3 + bcd]
+                            : WAV == WP_ID_CDF2_8 ? c_base28[3 + bcd]
+                                                  : c_base46[2 + bcd];
         if (tid < C) base_level<T>(mat, nb, buf(0) + tid, buf(1) + tid, CP);
         __syncthreads();
         int cur = 1;
@@ -374,7 +479,7 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
             for (int t = tid; t < C * nch; t += NT) {
                 const int col = t % C, k0 = (t / C) * CH;
                 T A[WIN], Dd[WIN], SA[WIN], SD[WIN];
-                if (k0 >= 4 && k0 + WIN - 4 <= L) {
+                if (k0 >= 4 + (bcd == 2) && k0 + WIN - 4 <= L) {
                     // interior window: no reflection
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) {
@@ -393,7 +498,30 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                         SD[w] = T(__int_as_float(e.w));
                     }
                 }
-                if (is_q3(WAV)) {
+                if (is_l2(WAV)) {
+                    // cuUpdateCdf26_ad_i / cuUpdateCdf28_ad_i: scale, undo the update, undo the predict,
+                    // divide out the approximation's sign
+                    constexpr int NTP = K2<WAV>::NTAP, LO = NTP / 2;
+#pragma unroll
+                    for (int w = 0; w < WIN; ++w) {
+                        Dd[w] = SD[w] * Dd[w] * T(K2<WAV>::scl0);
+                        A[w] = SA[w] * A[w] * T(K2<WAV>::scl1);
+                    }
+#pragma unroll
+                    for (int w = LO; w <= WIN - LO; ++w) {
+                        T t = A[w];
+#pragma unroll
+                        for (int i = 0; i < NTP; ++i) t = t - T(K2<WAV>::u(NTP - 1 - i)) * Dd[w - LO + i];
+                        A[w] = t;
+                    }
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4, k = k0 + j;
+                        if (k < NA) D[(2 * k) * CP + col] = A[w] / SA[w];
+                        if (k < L)
+                            D[(2 * k + 1) * CP + col] = Dd[w] - (T(K2<WAV>::fp1) * A[w] + T(K2<WAV>::fp0) * A[w + 1]);
+                    }
+                } else if (is_q3(WAV)) {
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) {
                         A[w] = SA[w] * A[w] * T(K37::scl1);
@@ -421,9 +549,12 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                     }
 #pragma unroll
                     for (int w = 3; w < WIN - 2; ++w)
-                        A[w] = SA[w] * (A[w] - (T(K46::c5) * Dd[w - 3] + T(K46::c4) * Dd[w - 2] +
-                                                T(K46::c3) * Dd[w - 1] + T(K46::c2) * Dd[w] +
-                                                T(K46::c1) * Dd[w + 1] + T(K46::c0) * Dd[w + 2]));
+                        A[w] = SA[w] * (A[w] - (WAV == WP_ID_CDF4_4
+                                                    ? T(K44::d3) * Dd[w - 2] + T(K44::d2) * Dd[w - 1] +
+                                                          T(K44::d1) * Dd[w] + T(K44::d0) * Dd[w + 1]
+                                                    : T(K46::c5) * Dd[w - 3] + T(K46::c4) * Dd[w - 2] +
+                                                          T(K46::c3) * Dd[w - 1] + T(K46::c2) * Dd[w] +
+                                                          T(K46::c1) * Dd[w + 1] + T(K46::c0) * Dd[w + 2]));
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) Dd[w] = SD[w] * Dd[w];
 #pragma unroll
@@ -487,6 +618,12 @@ cudaError_t ensure_constants() {
     e = cudaMemcpyToSymbol(c_base46, b46, sizeof(b46));
     if (e != cudaSuccess) return e;
     e = cudaMemcpyToSymbol(c_base35, h_base35, sizeof(h_base35));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_base44, h_base44, sizeof(h_base44));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_base26, h_base26, sizeof(h_base26));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_base28, h_base28, sizeof(h_base28));
     if (e != cudaSuccess) return e;
     if (dev < 64) g_const_ready[dev] = true;
     return cudaSuccess;
@@ -563,9 +700,14 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
                              char bc, int forward, cudaStream_t stream) {
     if (!dst || DX <= 0 || DY <= 0 || DZ <= 0) { wp_set_error_msg("wp_dwt1d: bad arguments"); return WP_ERR_INVALID_ARG; }
     if (!src) src = dst;
-    if (!is_q3(wavelet) && wavelet != WP_ID_CDF4_6) { wp_set_error_msg("wp_dwt1d: wavelet must be CDF3.7, CDF3.5 or CDF4.6"); return WP_ERR_UNSUPPORTED; }
-    if (bc == 'z') bc = is_q3(wavelet) ? 'd' : 'n';  // cuWHHDForward.cu:760-765, 886-891, 970-975
-    if (bc != 'n' && bc != 'd') { wp_set_error_msg("wp_dwt1d: bc must be 'n', 'd' or 'z'"); return WP_ERR_INVALID_ARG; }
+    if (!is_q3(wavelet) && !is_c4(wavelet) && !is_l2(wavelet)) {
+        wp_set_error_msg("wp_dwt1d: wavelet must be CDF3.5, CDF3.7, CDF4.4, CDF4.6, CDF2.6 or CDF2.8");
+        return WP_ERR_UNSUPPORTED;
+    }
+    // 'z': CDF3.x treat it as 'd', CDF4.x as 'n' (cuWHHDForward.cu:760-765, 843-848, 886-891, 970-975);
+    // CDF2.x have a rule of their own (:802-828, 928-933)
+    if (bc == 'z' && !is_l2(wavelet)) bc = is_q3(wavelet) ? 'd' : 'n';
+    if (bc != 'n' && bc != 'd' && bc != 'z') { wp_set_error_msg("wp_dwt1d: bc must be 'n', 'd' or 'z'"); return WP_ERR_INVALID_ARG; }
     TileGeom g;
     int N, nouter;
     switch (axis) {
@@ -581,7 +723,12 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
     }
     if (nouter > 65535) { wp_set_error_msg("wp_dwt1d: outer extent too large"); return WP_ERR_UNSUPPORTED; }
     WP_CUDA_TRY(ensure_constants());
-    const int bcd = (bc == 'd');
+    if ((wavelet == WP_ID_CDF4_4 || is_l2(wavelet)) && !(N & 1)) {
+        // their base matrices act on five coefficients: whole-sample lines of 2^levels + 1
+        wp_set_error_msg("wp_dwt1d: CDF4.4 and CDF2.x lines have 2^levels + 1 samples");
+        return WP_ERR_INVALID_ARG;
+    }
+    const int bcd = bc == 'd' ? 1 : (bc == 'z' ? 2 : 0);
     cudaError_t e;
     if (wavelet == WP_ID_CDF3_7)
         e = forward ? launch_c<WP_ID_CDF3_7, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
@@ -589,6 +736,15 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
     else if (wavelet == WP_ID_CDF3_5)
         e = forward ? launch_c<WP_ID_CDF3_5, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
                     : launch_c<WP_ID_CDF3_5, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    else if (wavelet == WP_ID_CDF4_4)
+        e = forward ? launch_c<WP_ID_CDF4_4, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF4_4, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    else if (wavelet == WP_ID_CDF2_6)
+        e = forward ? launch_c<WP_ID_CDF2_6, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF2_6, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    else if (wavelet == WP_ID_CDF2_8)
+        e = forward ? launch_c<WP_ID_CDF2_8, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF2_8, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
     else
         e = forward ? launch_c<WP_ID_CDF4_6, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
                     : launch_c<WP_ID_CDF4_6, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
@@ -641,7 +797,7 @@ wp_status wp_dwt_axis_tune(T* buf, int DX, int DY, int DZ, int levels, char axis
         case 'x': case 'X': g.ni = DY; nouter = DZ; g.contiguous = 0; break;
         default: g.ni = DY; nouter = DX; g.contiguous = 0; break;
     }
-    const int wav = is_q3(wavelet) ? wavelet : WP_ID_CDF4_6;
+    const int wav = wavelet;
     std::lock_guard<std::mutex> lk(g_c_mu);
     g_c_cache[c_key(wav, forward != 0, (int)sizeof(T), N, g, nouter)] = best_c;
     return WP_OK;
