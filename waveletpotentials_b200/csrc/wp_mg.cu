@@ -45,6 +45,7 @@ struct Lvl {
     const T* glo[3];  // per-axis factor of the lower face, 0 at the wall
     const T* ghi[3];  // per-axis factor of the upper face, 0 at the wall
     const double* d[3];
+    const float* rwz;  // restriction weight of fine plane z: (float)(d_z / (d_{2k} + d_{2k+1})), formed in FP64
 };
 
 // diag and off-diagonal sum of row (x,y,z) applied to v (optionally plus the prolonged coarse
@@ -837,11 +838,13 @@ __device__ __forceinline__ void resid_restrict_q_body(T* __restrict__ fc, const 
         Q4<T> acc = zero4<T>();
         if (act) {
             const int zb = 2 * cz;
-            const double sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
+            double sz = 0.0;
+            if constexpr (sizeof(T) == 8) sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
             for (int kz = 0; kz < 2; ++kz) {
                 const int z = zb + kz;
                 if (z >= L.nz) break;
-                const T wz = (T)(L.d[2][z] / sz);
+                // FP32: the same FP64 quotient, rounded once, from the level's table
+                const T wz = sizeof(T) == 4 ? (T)L.rwz[z] : (T)(L.d[2][z] / sz);
                 const long i = col.i;
                 Q4<T> dg, od, c;
                 col.step(dg, od, c);
@@ -932,14 +935,13 @@ __global__ void __launch_bounds__(256, 3) resid_restrict_qp_kernel(float* __rest
         Q4<float> acc = zero4<float>();
         if (act) {
             const int zb = 2 * cz;
-            const double sz = L.d[2][zb] + (zb + 1 < L.nz ? L.d[2][zb + 1] : 0.0);
             for (int kz = 0; kz < 2; ++kz) {
                 const int z = zb + kz;
                 if (z >= L.nz) break;
                 issue(z + JP_DEPTH - 1);
                 cp_async_wait<JP_DEPTH - 1>();
                 const int slot = (z - zs) % JP_DEPTH;
-                const float wz = (float)(L.d[2][z] / sz);
+                const float wz = L.rwz[z];  // (float)(d_z / (d_zb + d_zb+1)), formed in FP64
                 const long i = col.i;
                 Q4<float> vp = zero4<float>();
                 if (z < L.nz - 1) {
@@ -2407,6 +2409,7 @@ Lvl<float> view<float>(const Level& L) {
         off32 += 2 * L.n[a];
         off64 += 3 * L.n[a];
     }
+    o.rwz = L.tab32 + off32;
     return o;
 }
 template <>
@@ -2421,6 +2424,7 @@ Lvl<double> view<double>(const Level& L) {
         o.d[a] = L.tab64 + off64 + 2 * L.n[a];
         off64 += 3 * L.n[a];
     }
+    o.rwz = nullptr;  // the FP64 restriction divides in FP64
     return o;
 }
 
@@ -2764,6 +2768,13 @@ wp_status build_hierarchy(wp_mgfrac3d* h, const float* ax, const float* ay, cons
             t64.insert(t64.end(), hd[a].begin(), hd[a].end());
             for (double v : lo) t32.push_back((float)v);
             for (double v : hi) t32.push_back((float)v);
+        }
+        // after the three axes' factors: the z restriction weights (the FP64 quotient the restriction
+        // forms per fine plane, rounded once; the kernels read it instead of dividing)
+        for (int z = 0; z < n[2]; ++z) {
+            const int zb = z & ~1;
+            const double sz = hd[2][zb] + (zb + 1 < n[2] ? hd[2][zb + 1] : 0.0);
+            t32.push_back((float)(hd[2][z] / sz));
         }
         {
             // smallest diagonal of a fully open cell (the fused kernels' straight-line path divides by
