@@ -51,6 +51,9 @@ typedef enum wp_status {
 #define WP_CDF4_6 7
 #define WP_CDF2_8 10 /* predict + 8-tap update, lines of 2^L + 1 (wp_dwt1d only) */
 #define WP_CDF3_7 11
+#define WP_CDF2_0 16 /* CDF2.x's predict alone, lines of 2^L + 1, bc 'n' / 'd' (wp_dwt1d only) */
+#define WP_CDF1_1 17 /* Haar, lines of 2^L, bc 'n' / 'd' (wp_dwt1d only) */
+#define WP_CDF1_7 18 /* Haar predict + 7-tap update, lines of 2^L, bc 'n' / 'd' (wp_dwt1d only) */
 
 /* precision modes of the multigrid solve */
 #define WP_PREC_FP32 0  /* FP32 V-cycles, FP32 iterate; residual norms accumulated in FP64 */

@@ -225,6 +225,59 @@ static const double ILZ8_L10[25] = {
 #define IS_C4(w) ((w) == OR_CDF4_6 || (w) == OR_CDF4_4)
 #define IS_L2(w) ((w) == OR_CDF2_6 || (w) == OR_CDF2_8)
 
+/* The short families (cuWaveletCompute.cuh:1397-1556; registered at cuWHHDForward.cu:998-1080).
+   CDF2.0: CDF2.x's predict alone, no update, the detail's scale negated, CDF2.6's boundary rules
+   (cuUpdateCdf20_ad / _ad_i); CDF1.1: the Haar step, d - a then a + d/2 (cuUpdateCdf11_ad / _ad_i);
+   CDF1.7: the Haar predict and a 7-tap update, CDF3.5's boundary rules (cuUpdateCdf17_ad / _ad_i). */
+#define IS_SHORT(w) ((w) == OR_CDF2_0 || (w) == OR_CDF1_1 || (w) == OR_CDF1_7)
+static const double T1_FP = -1.0, T1_FU = 0.5;
+static const double T1_SCL[2] = {SQ2, 1.0 / SQ2};
+static const double T7_FU[7] = {-0.002441406250000, 0.021484375000000, -0.098144531250000, 0.5,
+                                0.098144531250000, -0.021484375000000, 0.002441406250000};
+static const double T7_SCL[2] = {SQ2, -1.0 / SQ2};
+static const double B20_L10[25] = {
+    2.0, 0, 0, 0, 0,
+    0, 0, 0, 0, 2.0,
+    0.5, 0, -1.0, 0, 0.5,
+    0.353553390593274, -0.707106781186547, 0.353553390593274, 0, 0,
+    0, 0, 0.353553390593274, -0.707106781186547, 0.353553390593274};
+static const double IB20_L10[25] = {
+    0.5, 0, 0, 0, 0,
+    0.375, 0.125, -0.5, -1.414213562373095, 0,
+    0.25, 0.25, -1.0, 0, 0,
+    0.125, 0.375, -0.5, 0, -1.414213562373095,
+    0, 0.5, 0, 0, 0};
+static const double B11_L10[16] = {
+    0.5, 0.5, 0.5, 0.5,
+    -0.5, -0.5, 0.5, 0.5,
+    -0.707106781186548, 0.707106781186548, 0, 0,
+    0, 0, -0.707106781186548, 0.707106781186548};
+static const double IB11_L10[16] = {
+    0.5, -0.5, -0.707106781186547, 0,
+    0.5, -0.5, 0.707106781186547, 0,
+    0.5, 0.5, 0, -0.707106781186547,
+    0.5, 0.5, 0, 0.707106781186547};
+static const double TN7_L10[16] = {
+    0.5, 0.5, 0.5, 0.5,
+    0.691406250000000, 0.308593750000000, -0.308593750000000, -0.691406250000000,
+    0.707106781186548, -0.707106781186548, 0, 0,
+    0, 0, 0.707106781186548, -0.707106781186548};
+static const double ITN7_L10[16] = {
+    0.5, 0.5, 0.571762123850060, -0.135344657336488,
+    0.5, 0.5, -0.842451438523035, -0.135344657336488,
+    0.5, -0.5, 0.135344657336488, 0.842451438523035,
+    0.5, -0.5, 0.135344657336488, -0.571762123850060};
+static const double TD7_L10[16] = {
+    0.308593750000000, 0.691406250000000, 0.691406250000000, 0.308593750000000,
+    0.5, 0.5, -0.5, -0.5,
+    0.707106781186548, -0.707106781186548, 0, 0,
+    0, 0, 0.707106781186548, -0.707106781186548};
+static const double ITD7_L10[16] = {
+    0.5, 0.5, 0.842451438523035, -0.135344657336488,
+    0.5, 0.5, -0.571762123850060, -0.135344657336488,
+    0.5, -0.5, 0.135344657336488, 0.571762123850060,
+    0.5, -0.5, 0.135344657336488, -0.842451438523035};
+
 /* 'z' is the Dirichlet-with-spacing alias: the CDF3.x wavelets treat it as 'd', the CDF4.x ones as
    'n' (cuWHHDForward.cu:760-765, 886-891, 970-975); CDF2.6 / CDF2.8 have their own 'z' rule
    (cuWHHDForward.cu:802-828, cuWT_CDF2_6_z) */
@@ -234,6 +287,12 @@ static char norm_bc(int wavelet, char bc) {
 }
 
 static const double* base_matrix(int wavelet, char bc, int forward) {
+    if (wavelet == OR_CDF2_0) return forward ? B20_L10 : IB20_L10;
+    if (wavelet == OR_CDF1_1) return forward ? B11_L10 : IB11_L10;
+    if (wavelet == OR_CDF1_7) {
+        if (bc == 'n') return forward ? TN7_L10 : ITN7_L10;
+        return forward ? TD7_L10 : ITD7_L10;
+    }
     if (wavelet == OR_CDF3_5) {
         if (bc == 'n') return forward ? QN5_L10 : IQN5_L10;
         return forward ? QD5_L10 : IQD5_L10;
@@ -269,7 +328,7 @@ static const double* base_matrix(int wavelet, char bc, int forward) {
 static void fwd_reflect(int wavelet, char bc, int k, int L, int* ai, int* di, double* sa, double* sd) {
     int a = 2 * k, d = 2 * k + 1;
     double s_a = 1.0, s_d = 1.0;
-    if (IS_Q3(wavelet)) {
+    if (IS_Q3(wavelet) || wavelet == OR_CDF1_1 || wavelet == OR_CDF1_7) {
         if (a < 0) { a = -1 - a; if (bc == 'd') s_a = -1.0; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bc == 'd') s_a = -1.0; }
         if (d < 0) { d = -1 - d; if (bc == 'd') s_d = -1.0; }
@@ -298,7 +357,7 @@ static void fwd_reflect(int wavelet, char bc, int k, int L, int* ai, int* di, do
 static void inv_reflect(int wavelet, char bc, int k, int L, int* ai, int* di, double* sa, double* sd) {
     int a = k, d = k;
     double s_a = 1.0, s_d = 1.0;
-    if (IS_Q3(wavelet)) {
+    if (IS_Q3(wavelet) || wavelet == OR_CDF1_1 || wavelet == OR_CDF1_7) {
         if (a < 0) { a = -1 - a; if (bc == 'n') s_d = -1.0; else s_a = -1.0; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bc == 'n') s_d = -1.0; else s_a = -1.0; }
         d = a;
@@ -340,7 +399,22 @@ static void fwd_level(const double* x, int L, int ext, int wavelet, char bc, dou
         D0[IX(k)] = (di >= 0 && di < n_in) ? sd * x[di] : 0.0;
     }
     for (int k = K0; k < K1; ++k) { A1[IX(k)] = 0.0; D1[IX(k)] = 0.0; }
-    if (IS_L2(wavelet)) {
+    if (wavelet == OR_CDF2_0) {
+        /* the predict on the raw samples (no reflection sign: it reads no sample outside the line) */
+        for (int k = 0; k < L / 2; ++k)
+            d_out[k] = (x[2 * k + 1] + L6_FP[0] * x[2 * k] + L6_FP[1] * x[2 * k + 2]) * -L6_SCL[1];
+        for (int k = 0; k < M; ++k) a_out[k] = x[2 * k] * L6_SCL[0];
+    } else if (wavelet == OR_CDF1_1 || wavelet == OR_CDF1_7) {
+        for (int k = K0; k < K1; ++k) D1[IX(k)] = D0[IX(k)] + T1_FP * A0[IX(k)];
+        for (int k = 0; k < M; ++k) {
+            double s = A0[IX(k)];
+            if (wavelet == OR_CDF1_1) s += T1_FU * D1[IX(k)];
+            else
+                for (int j = -3; j <= 3; ++j) s += T7_FU[3 - j] * D1[IX(k + j)];
+            a_out[k] = s * (wavelet == OR_CDF1_1 ? T1_SCL[0] : T7_SCL[0]);
+        }
+        for (int k = 0; k < L / 2; ++k) d_out[k] = D1[IX(k)] * (wavelet == OR_CDF1_1 ? T1_SCL[1] : T7_SCL[1]);
+    } else if (IS_L2(wavelet)) {
         /* predict with the signed approximations, then the detail's own sign, then the update;
            the approximation's sign is divided out at the end (cuUpdateCdf26_ad / cuUpdateCdf28_ad) */
         const double* fu = wavelet == OR_CDF2_6 ? L6_FU : L8_FU;
@@ -413,7 +487,29 @@ static void inv_level(const double* a, const double* d, int L, int ext, int wave
         D[IX(k)] = (di >= 0 && di < L) ? d[di] : 0.0;
         SA[IX(k)] = sa; SD[IX(k)] = sd;
     }
-    if (IS_L2(wavelet)) {
+    if (wavelet == OR_CDF2_0) {
+        for (int k = 0; k < NA; ++k) x[2 * k] = a[k] * L6_SCL[1];
+        for (int k = 0; k < L; ++k)
+            x[2 * k + 1] = -d[k] * L6_SCL[0] - (L6_FP[1] * x[2 * k] + L6_FP[0] * x[2 * k + 2]);
+    } else if (wavelet == OR_CDF1_1) {
+        for (int k = 0; k < L; ++k) {
+            const double dd = d[k] * T1_SCL[0];
+            const double aa = a[k] * T1_SCL[1] - T1_FU * dd;
+            x[2 * k] = aa;
+            x[2 * k + 1] = dd - T1_FP * aa;
+        }
+    } else if (wavelet == OR_CDF1_7) {
+        for (int k = K0; k < K1; ++k) {
+            D[IX(k)] = SD[IX(k)] * D[IX(k)] / T7_SCL[1];
+            A[IX(k)] = SA[IX(k)] * A[IX(k)] / T7_SCL[0];
+        }
+        for (int k = 0; k < L; ++k) {
+            double t = A[IX(k)];
+            for (int j = -3; j <= 3; ++j) t -= T7_FU[3 - j] * D[IX(k + j)];
+            x[2 * k] = t;
+            x[2 * k + 1] = D[IX(k)] - T1_FP * t;
+        }
+    } else if (IS_L2(wavelet)) {
         const double* fu = wavelet == OR_CDF2_6 ? L6_FU : L8_FU;
         const int nt = wavelet == OR_CDF2_6 ? 6 : 8, lo = nt / 2;
         for (int k = K0; k < K1; ++k) {
@@ -466,13 +562,16 @@ static void inv_level(const double* a, const double* d, int L, int ext, int wave
 
 /* ----------------------------------------------------------------- full 1D line ---- */
 int or_dwt_line(double* line, int n, int levels, int wavelet, char bc, int forward) {
-    if (!IS_Q3(wavelet) && !IS_C4(wavelet) && !IS_L2(wavelet)) return 2;
+    if (!IS_Q3(wavelet) && !IS_C4(wavelet) && !IS_L2(wavelet) && !IS_SHORT(wavelet)) return 2;
+    /* the short families register 'n' and 'd' only (cuWHHDForward.cu:998-1080) */
+    if (IS_SHORT(wavelet) && bc != 'n' && bc != 'd') return 2;
     bc = norm_bc(wavelet, bc);
     if (bc != 'n' && bc != 'd' && !(bc == 'z' && IS_L2(wavelet))) return 2;
     int ext = n & 1;
     if (levels < 2 || (1 << levels) != n - ext) return 1;
     /* the CDF4.4 and CDF2.x base matrices act on 5 coefficients: whole-sample lines of 2^L + 1 */
-    if ((wavelet == OR_CDF4_4 || IS_L2(wavelet)) && !ext) return 1;
+    if ((wavelet == OR_CDF4_4 || IS_L2(wavelet) || wavelet == OR_CDF2_0) && !ext) return 1;
+    if ((wavelet == OR_CDF1_1 || wavelet == OR_CDF1_7) && ext) return 1;
     int nb = 4 + ext;
     double* buf = (double*)malloc(sizeof(double) * (size_t)(2 * n + 16));
     double* tmp = buf + n + 8;

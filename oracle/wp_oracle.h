@@ -25,6 +25,9 @@ extern "C" {
 #define OR_CDF4_6 7
 #define OR_CDF2_8 10
 #define OR_CDF3_7 11
+#define OR_CDF2_0 16
+#define OR_CDF1_1 17
+#define OR_CDF1_7 18
 
 /* one full-depth 1D transform of a line in place (cuWHHDForward.cu:5-105 forward, :349-464 inverse) */
 int or_dwt_line(double* line, int n, int levels, int wavelet, char bc, int forward);

@@ -13,6 +13,7 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only psweep  # CuParallelSweep3D Solve / Project only
     python tests/golden/make_golden.py --only domd    # projection and recovery with Dirichlet walls
     python tests/golden/make_golden.py --only families  # CDF2.6 / CDF2.8 / CDF4.4 transforms
+    python tests/golden/make_golden.py --only short   # CDF2.0 / CDF1.1 / CDF1.7 transforms
     ... [--out DIR]                                   # write the .npz files to DIR instead of here
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
@@ -40,6 +41,7 @@ if ROOT not in sys.path:
 from waveletpotentials_b200.fields import porous_fractions  # noqa: E402
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 CDF3_5, CDF2_6, CDF4_4, CDF4_6, CDF2_8, CDF3_7 = 2, 5, 6, 7, 10, 11
+CDF2_0, CDF1_1, CDF1_7 = 16, 17, 18
 
 
 def run(op, inputs: dict, params, outputs: dict):
@@ -231,6 +233,36 @@ def families_cases(rng):
     save("dwt1d_families", **dwt)
 
 
+def short_cases(rng):
+    """CuWHHDForward::Solve1D with the short families the reference registers (cuWHHDForward.cu:
+    998-1080): CDF2.0 (the CDF2.x predict alone, with CDF2.6's boundary rules, on lines of 2^L + 1)
+    and CDF1.1 / CDF1.7 (a Haar predict and a 1- or 7-tap update, with CDF3.5's boundary rules, on
+    lines of 2^L); every axis, the boundary types 'n' and 'd' (the only ones registered for these
+    three), both directions, and a 256/257-point line."""
+    dwt = {}
+    for wav, ext in ((CDF2_0, 1), (CDF1_1, 0), (CDF1_7, 0)):
+        for bc in "nd":
+            for fwd in (1, 0):
+                for axis, (L, other) in {"y": (4, (3, 2)), "x": (5, (4, 3)), "z": (3, (5, 2))}.items():
+                    n = (1 << L) + ext
+                    DX, DY, DZ = {"y": (other[0], n, other[1]), "x": (n, other[0], other[1]),
+                                  "z": (other[0], other[1], n)}[axis]
+                    a = rng.standard_normal((DZ, DX, DY))
+                    out = run("dwt1d", {"a": a}, [DX, DY, DZ, L, axis, bc, wav, fwd], {"c": (DZ, DX, DY)})
+                    key = f"w{wav}_{bc}_{'f' if fwd else 'i'}_{axis}"
+                    dwt[key + "_in"] = a
+                    dwt[key + "_out"] = out["c"]
+                    dwt[key + "_meta"] = np.array([DX, DY, DZ, L, ord(axis), ord(bc), wav, fwd])
+                n = 256 + ext
+                a = rng.standard_normal((1, 2, n))
+                out = run("dwt1d", {"a": a}, [2, n, 1, 8, "y", bc, wav, fwd], {"c": (1, 2, n)})
+                key = f"w{wav}_{bc}_{'f' if fwd else 'i'}_long"
+                dwt[key + "_in"] = a
+                dwt[key + "_out"] = out["c"]
+                dwt[key + "_meta"] = np.array([2, n, 1, 8, ord("y"), ord(bc), wav, fwd])
+    save("dwt1d_short", **dwt)
+
+
 def dst_cases(rng):
     """CuDst3D::Solve (the Dirichlet Poisson solve by DST-I along each axis, cuDst3D.cu:265-341) on
     grids of equal extents (its constructor's buffer sizing is only safe there, cuDst3D.cu:209-211):
@@ -334,6 +366,9 @@ def main():
         return
     if only == "families":
         families_cases(np.random.default_rng(20261212))
+        return
+    if only == "short":
+        short_cases(np.random.default_rng(20261213))
         return
     rng = np.random.default_rng(20261203)
 

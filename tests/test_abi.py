@@ -39,6 +39,10 @@ def test_dwt_rejects_bad_shapes(L):
     assert L.wp_dwt1d(dummy, dummy, 16, 4, 4, 4, _c("x"), _c("q"), _lib.CDF3_7, 1, None) == 1
     assert L.wp_dwt1d(dummy, dummy, 16, 4, 4, 4, _c("x"), _c("n"), 3, 1, None) == 2  # CDF2.10: another family
     assert L.wp_dwt1d(None, None, 16, 4, 4, 4, _c("x"), _c("n"), _lib.CDF3_7, 1, None) == 1
+    # the short families register 'n' and 'd' only
+    for wav in (_lib.CDF2_0, _lib.CDF1_1, _lib.CDF1_7):
+        assert L.wp_dwt1d(dummy, dummy, 16, 4, 4, 4, _c("x"), _c("z"), wav, 1, None) == 1
+        assert "take bc 'n' or 'd'" in _lib.last_error()
 
 
 def test_recover_rejects_unsupported_requests(L):

@@ -26,7 +26,7 @@ def rel(ref, got):
     return float(np.sqrt(np.sum((ref - got) ** 2) / max(np.sum(ref * ref), 1e-300)))
 
 
-@pytest.mark.parametrize("name", ["dwt1d", "dwt1d_cdf35", "dwt1d_families"])
+@pytest.mark.parametrize("name", ["dwt1d", "dwt1d_cdf35", "dwt1d_families", "dwt1d_short"])
 def test_dwt1d_fp32_and_fp64_match_reference(wp, name):
     d = load_golden(name)
     cases = [k[:-5] for k in d.files if k.endswith("_meta")]
@@ -44,7 +44,9 @@ def test_dwt1d_fp32_and_fp64_match_reference(wp, name):
             assert torch.equal(src, dst), b
 
 
-@pytest.mark.parametrize("wav,ext,bc", [(11, 0, "n"), (11, 0, "d"), (7, 1, "n"), (7, 1, "d")])
+@pytest.mark.parametrize("wav,ext,bc", [(11, 0, "n"), (11, 0, "d"), (7, 1, "n"), (7, 1, "d"),
+                                        (16, 1, "n"), (16, 1, "d"), (17, 0, "n"), (17, 0, "d"),
+                                        (18, 0, "n"), (18, 0, "d")])
 @pytest.mark.parametrize("axis", ["x", "y", "z"])
 def test_dwt_long_lines_against_oracle(wp, oracle, wav, ext, bc, axis):
     """Full 256(+1)-point lines along every axis (the 256^3 line length), both directions."""

@@ -6,7 +6,8 @@ import pytest
 from conftest import load_golden
 
 
-@pytest.mark.parametrize("name,count", [("dwt1d", 28), ("dwt1d_cdf35", 16), ("dwt1d_families", 72)])
+@pytest.mark.parametrize("name,count", [("dwt1d", 28), ("dwt1d_cdf35", 16), ("dwt1d_families", 72),
+                                        ("dwt1d_short", 48)])
 def test_dwt1d_matches_reference(oracle, name, count):
     d = load_golden(name)
     cases = [k[:-5] for k in d.files if k.endswith("_meta")]

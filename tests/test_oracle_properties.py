@@ -209,3 +209,19 @@ def test_perfect_reconstruction_of_the_whole_sample_families(oracle, wav, bc, le
         x[0] = x[-1] = 0.0
     c = oracle.dwt_line(x, levels, wav, bc, True)
     np.testing.assert_allclose(oracle.dwt_line(c, levels, wav, bc, False), x, atol=1e-12)
+
+
+@pytest.mark.parametrize("wav,ext", [(16, 1), (17, 0), (18, 0)])  # CDF2.0, CDF1.1, CDF1.7
+@pytest.mark.parametrize("bc", ["n", "d"])
+@pytest.mark.parametrize("levels", [2, 3, 5, 8])
+def test_perfect_reconstruction_of_the_short_families(oracle, wav, ext, bc, levels):
+    """CDF2.0 (lines of 2^L + 1), CDF1.1 and CDF1.7 (lines of 2^L): analysis then synthesis gives any
+    line back, with either boundary type; 'z' is not registered for them and is refused."""
+    rng = np.random.default_rng(levels + wav)
+    x = rng.standard_normal((1 << levels) + ext)
+    c = oracle.dwt_line(x, levels, wav, bc, True)
+    np.testing.assert_allclose(oracle.dwt_line(c, levels, wav, bc, False), x, atol=1e-12)
+    with pytest.raises(RuntimeError):
+        oracle.dwt_line(x, levels, wav, "z", True)
+    with pytest.raises(RuntimeError):
+        oracle.dwt_line(rng.standard_normal((1 << levels) + 1 - ext), levels, wav, bc, True)

@@ -26,7 +26,8 @@ void wp_set_cuda_error(cudaError_t e, const char* what, const char* file, int li
 void wp_set_error_msg(const char* msg);
 
 // wavelet ids (same values as the reference enum, WaveletTypes.h:7-27)
-enum { WP_ID_CDF3_5 = 2, WP_ID_CDF2_6 = 5, WP_ID_CDF4_4 = 6, WP_ID_CDF4_6 = 7, WP_ID_CDF2_8 = 10, WP_ID_CDF3_7 = 11 };
+enum { WP_ID_CDF3_5 = 2, WP_ID_CDF2_6 = 5, WP_ID_CDF4_4 = 6, WP_ID_CDF4_6 = 7, WP_ID_CDF2_8 = 10, WP_ID_CDF3_7 = 11,
+       WP_ID_CDF2_0 = 16, WP_ID_CDF1_1 = 17, WP_ID_CDF1_7 = 18 };
 
 static inline int wp_ilog2(int n) {
     int l = 0;

@@ -30,7 +30,8 @@ namespace {
 // recovery: the 2^(L-1) + 1 approximations of the top level then split into 15 chunks (two rounds of
 // a 256-thread tile of 32 columns) instead of 17 (three rounds, the last one eighth full).
 __host__ __device__ constexpr int ch_of(int wav) {
-    return (wav == WP_ID_CDF4_6 || wav == WP_ID_CDF4_4 || wav == WP_ID_CDF2_6 || wav == WP_ID_CDF2_8) ? 9 : 8;
+    return (wav == WP_ID_CDF4_6 || wav == WP_ID_CDF4_4 || wav == WP_ID_CDF2_6 || wav == WP_ID_CDF2_8 ||
+            wav == WP_ID_CDF2_0) ? 9 : 8;
 }
 constexpr int NT = 256;      // threads per CTA
 
@@ -75,6 +76,21 @@ struct K2 {
                       : i == 6 ? 0.020446777343750 : -0.002136230468750);
     }
 };
+// The short families (cuWaveletCompute.cuh:6-11, 1397-1556): CDF2.0 is CDF2.x's predict alone with the
+// detail's scale negated; CDF1.1 the Haar step (d - a, then a + d / 2); CDF1.7 the Haar predict and a
+// 7-tap update, t7(i) weighing the detail at offset 3 - i
+__host__ __device__ constexpr bool is_t1(int w) { return w == WP_ID_CDF1_1 || w == WP_ID_CDF1_7; }
+// boundary rules: CDF1.x take CDF3.5's (cuWT_CDF3_5_*), CDF2.0 CDF2.6's (cuWT_CDF2_6_*)
+__host__ __device__ constexpr bool q3_rules(int w) { return is_q3(w) || is_t1(w); }
+__host__ __device__ constexpr bool l2_rules(int w) { return is_l2(w) || w == WP_ID_CDF2_0; }
+struct KT {
+    static constexpr double fp = -1.0, fu = 0.5;
+    static constexpr double scl0 = WP_SQ2_D, scl1 = 1.0 / 1.41421356237309504, scl7_1 = -1.0 / 1.41421356237309504;
+    __host__ __device__ static constexpr double t7(int i) {
+        return i == 0 ? -0.002441406250000 : i == 1 ? 0.021484375000000 : i == 2 ? -0.098144531250000
+             : i == 3 ? 0.5 : i == 4 ? 0.098144531250000 : i == 5 ? -0.021484375000000 : 0.002441406250000;
+    }
+};
 // CDF4.4's second update (RSW_C4_fu_2): d4_i weighs offset 1 - i
 struct K44 {
     static constexpr double d0 = -0.03906250, d1 = 0.22656250, d2 = 0.22656250, d3 = -0.03906250;
@@ -96,6 +112,24 @@ __constant__ double c_base46[4][25];
 __constant__ double c_base44[4][25];
 __constant__ double c_base26[6][25];
 __constant__ double c_base28[6][25];
+// CDF2.0: forward, inverse (one matrix for 'n' and 'd'); CDF1.1: forward, inverse; CDF1.7: forward n, d,
+// inverse n, d
+__constant__ double c_base20[2][25];
+__constant__ double c_base11[2][16];
+__constant__ double c_base17[4][16];
+// RSW_20_L10 / RSW_i20_L10, RSW_11_L10 / RSW_i11_L10, RSW_T{N,D}7_L10 / RSW_iT{N,D}7_L10
+// (cuWaveletCompute.cuh:1398-1411, 1438-1449, 1479-1502)
+const double h_base20[2][25] = {
+    {2.0, 0, 0, 0, 0, 0, 0, 0, 0, 2.0, 0.5, 0, -1.0, 0, 0.5, 0.353553390593274, -0.707106781186547, 0.353553390593274, 0, 0, 0, 0, 0.353553390593274, -0.707106781186547, 0.353553390593274},
+    {0.5, 0, 0, 0, 0, 0.375, 0.125, -0.5, -1.414213562373095, 0, 0.25, 0.25, -1.0, 0, 0, 0.125, 0.375, -0.5, 0, -1.414213562373095, 0, 0.5, 0, 0, 0}};
+const double h_base11[2][16] = {
+    {0.5, 0.5, 0.5, 0.5, -0.5, -0.5, 0.5, 0.5, -0.707106781186548, 0.707106781186548, 0, 0, 0, 0, -0.707106781186548, 0.707106781186548},
+    {0.5, -0.5, -0.707106781186547, 0, 0.5, -0.5, 0.707106781186547, 0, 0.5, 0.5, 0, -0.707106781186547, 0.5, 0.5, 0, 0.707106781186547}};
+const double h_base17[4][16] = {
+    {0.5, 0.5, 0.5, 0.5, 0.69140625, 0.30859375, -0.30859375, -0.69140625, 0.707106781186548, -0.707106781186548, 0, 0, 0, 0, 0.707106781186548, -0.707106781186548},
+    {0.30859375, 0.69140625, 0.69140625, 0.30859375, 0.5, 0.5, -0.5, -0.5, 0.707106781186548, -0.707106781186548, 0, 0, 0, 0, 0.707106781186548, -0.707106781186548},
+    {0.5, 0.5, 0.571762123850060, -0.135344657336488, 0.5, 0.5, -0.842451438523035, -0.135344657336488, 0.5, -0.5, 0.135344657336488, 0.842451438523035, 0.5, -0.5, 0.135344657336488, -0.571762123850060},
+    {0.5, 0.5, 0.842451438523035, -0.135344657336488, 0.5, 0.5, -0.571762123850060, -0.135344657336488, 0.5, -0.5, 0.135344657336488, 0.571762123850060, 0.5, -0.5, 0.135344657336488, -0.842451438523035}};
 
 const double h_base37[4][16] = {
     {0.500000000000000, 0.500000000000000, 0.500000000000000, 0.500000000000000, -0.399902343750000,
@@ -168,18 +202,18 @@ template <int WAV>
 __device__ __forceinline__ void fwd_reflect(int k, int L, int bcd, int& ai, int& di, float& sa, float& sd) {
     int a = 2 * k, d = 2 * k + 1;
     float s_a = 1.f, s_d = 1.f;
-    if (is_q3(WAV)) {
+    if (q3_rules(WAV)) {
         if (a < 0) { a = -1 - a; if (bcd) s_a = -1.f; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bcd) s_a = -1.f; }
         if (d < 0) { d = -1 - d; if (bcd) s_d = -1.f; }
         else if (d >= L) { d = 2 * L - 1 - d; if (bcd) s_d = -1.f; }
-    } else if (is_l2(WAV) && bcd == 1) {
+    } else if (l2_rules(WAV) && bcd == 1) {
         // cuWT_CDF2_6_d (cuWaveletCompute.cuh:271-294): a reflected without a sign, d with one
         if (a < 0) a = -a;
         else if (a > L) a = 2 * L - a;
         if (d < 0) { d = -d; s_d = -1.f; }
         else if (d >= L) { d = 2 * L - d; s_d = -1.f; }
-    } else if (is_l2(WAV)) {
+    } else if (l2_rules(WAV)) {
         // cuWT_CDF2_6_n (:255-269) and _z (:296-311, the boundary samples count twice)
         if (a < 0) { a = -a; d = -d; }
         else if (a >= L) { a = 2 * L - a; d = 2 * L - d; }
@@ -198,11 +232,11 @@ template <int WAV>
 __device__ __forceinline__ void inv_reflect(int k, int L, int bcd, int& ai, int& di, float& sa, float& sd) {
     int a = k, d = k;
     float s_a = 1.f, s_d = 1.f;
-    if (is_q3(WAV)) {
+    if (q3_rules(WAV)) {
         if (a < 0) { a = -1 - a; if (bcd) s_a = -1.f; else s_d = -1.f; }
         else if (a >= L) { a = 2 * L - 1 - a; if (bcd) s_a = -1.f; else s_d = -1.f; }
         d = a;
-    } else if (is_l2(WAV) && bcd == 1) {
+    } else if (l2_rules(WAV) && bcd == 1) {
         // cuWT_CDF2_6_d_i (cuWaveletCompute.cuh:668-683)
         if (a < 0) { a = -a; d = -d - 1; s_d = -1.f; }
         else if (a >= L) { a = 2 * L - a; d = 2 * L - d - 1; s_d = -1.f; }
@@ -383,8 +417,8 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
 #pragma unroll
                     for (int w = 0; w < WIN; ++w) {
                         const int4 e = tb[k0 + w];
-                        A[w] = T(__int_as_float(e.z)) * S[e.x * CP + col];
-                        if (is_l2(WAV)) {
+                        A[w] = (WAV == WP_ID_CDF2_0 ? T(1) : T(__int_as_float(e.z))) * S[e.x * CP + col];
+                        if (l2_rules(WAV)) {
                             Dd[w] = S[e.y * CP + col];
                             SAw[w] = T(__int_as_float(e.z));
                             SDw[w] = T(__int_as_float(e.w));
@@ -393,7 +427,34 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                         }
                     }
                 }
-                if (is_l2(WAV)) {
+                if (WAV == WP_ID_CDF2_0) {
+                    // cuUpdateCdf20_ad: the predict on the samples as read (no sign: at an output pair
+                    // both neighbours lie inside the line), the detail's scale negated
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4, k = k0 + j;
+                        const T dv = Dd[w] + (T(K2<WP_ID_CDF2_6>::fp0) * A[w] + T(K2<WP_ID_CDF2_6>::fp1) * A[w + 1]);
+                        if (k < M) D[k * CP + col] = A[w] * T(K2<WP_ID_CDF2_6>::scl0);
+                        if (k < nd) D[(M + k) * CP + col] = dv * T(-K2<WP_ID_CDF2_6>::scl1);
+                    }
+                } else if (is_t1(WAV)) {
+                    // cuUpdateCdf11_ad / cuUpdateCdf17_ad (signs applied at the load)
+#pragma unroll
+                    for (int w = 0; w < WIN; ++w) Dd[w] = Dd[w] + T(KT::fp) * A[w];
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4, k = k0 + j;
+                        T s = A[w];
+                        if (WAV == WP_ID_CDF1_1) {
+                            s += T(KT::fu) * Dd[w];
+                        } else {
+#pragma unroll
+                            for (int i = 6; i >= 0; --i) s += T(KT::t7(i)) * Dd[w + 3 - i];
+                        }
+                        if (k < M) D[k * CP + col] = s * T(KT::scl0);
+                        if (k < nd) D[(M + k) * CP + col] = Dd[w] * T(WAV == WP_ID_CDF1_1 ? KT::scl1 : KT::scl7_1);
+                    }
+                } else if (is_l2(WAV)) {
                     constexpr int NTP = K2<WAV>::NTAP, LO = NTP / 2;
 #pragma unroll
                     for (int w = 0; w < WIN - 1; ++w)
@@ -448,6 +509,9 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
         }
         // base level: nb x nb matrix on the remaining approximation coefficients
         const double* mat = WAV == WP_ID_CDF3_7   ? c_base37[bcd]
+                            : WAV == WP_ID_CDF2_0 ? c_base20[0]
+                            : WAV == WP_ID_CDF1_1 ? c_base11[0]
+                            : WAV == WP_ID_CDF1_7 ? c_base17[bcd]
                             : WAV == WP_ID_CDF3_5 ? c_base35[bcd]
                             : WAV == WP_ID_CDF4_4 ? c_base44[bcd]
                             : WAV == WP_ID_CDF2_6 ? c_base26[bcd]
@@ -458,6 +522,9 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
         outbuf = -1;  // position dependent, resolved below
     } else {
         const double* mat = WAV == WP_ID_CDF3_7   ? c_base37[2 + bcd]
+                            : WAV == WP_ID_CDF2_0 ? c_base20[1]
+                            : WAV == WP_ID_CDF1_1 ? c_base11[1]
+                            : WAV == WP_ID_CDF1_7 ? c_base17[2 + bcd]
                             : WAV == WP_ID_CDF3_5 ? c_base35[2 + bcd]
                             : WAV == WP_ID_CDF4_4 ? c_base44[2 + bcd]
                             : WAV == WP_ID_CDF2_6 ? c_base26[3 + bcd]
@@ -498,7 +565,47 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
                         SD[w] = T(__int_as_float(e.w));
                     }
                 }
-                if (is_l2(WAV)) {
+                if (WAV == WP_ID_CDF2_0) {
+                    // cuUpdateCdf20_ad_i
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4, k = k0 + j;
+                        const T a0 = SA[w] * A[w] * T(K2<WP_ID_CDF2_6>::scl1);
+                        const T a1 = SA[w + 1] * A[w + 1] * T(K2<WP_ID_CDF2_6>::scl1);
+                        const T dv = -SD[w] * Dd[w] * T(K2<WP_ID_CDF2_6>::scl0);
+                        if (k < NA) D[(2 * k) * CP + col] = a0;
+                        if (k < L)
+                            D[(2 * k + 1) * CP + col] =
+                                dv - (T(K2<WP_ID_CDF2_6>::fp1) * a0 + T(K2<WP_ID_CDF2_6>::fp0) * a1);
+                    }
+                } else if (WAV == WP_ID_CDF1_1) {
+                    // cuUpdateCdf11_ad_i (no sign: the step reads no neighbour)
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4, k = k0 + j;
+                        const T dv = Dd[w] * T(KT::scl0);
+                        const T av = A[w] * T(KT::scl1) - T(KT::fu) * dv;
+                        if (k < NA) D[(2 * k) * CP + col] = av;
+                        if (k < L) D[(2 * k + 1) * CP + col] = dv - T(KT::fp) * av;
+                    }
+                } else if (WAV == WP_ID_CDF1_7) {
+                    // cuUpdateCdf17_ad_i: signed and scaled (by division, as the reference), the update
+                    // undone, then the predict
+#pragma unroll
+                    for (int w = 0; w < WIN; ++w) {
+                        Dd[w] = SD[w] * Dd[w] / T(KT::scl7_1);
+                        A[w] = SA[w] * A[w] / T(KT::scl0);
+                    }
+#pragma unroll
+                    for (int j = 0; j < CH; ++j) {
+                        const int w = j + 4, k = k0 + j;
+                        T av = A[w];
+#pragma unroll
+                        for (int i = 6; i >= 0; --i) av -= T(KT::t7(i)) * Dd[w + 3 - i];
+                        if (k < NA) D[(2 * k) * CP + col] = av;
+                        if (k < L) D[(2 * k + 1) * CP + col] = Dd[w] - T(KT::fp) * av;
+                    }
+                } else if (is_l2(WAV)) {
                     // cuUpdateCdf26_ad_i / cuUpdateCdf28_ad_i: scale, undo the update, undo the predict,
                     // divide out the approximation's sign
                     constexpr int NTP = K2<WAV>::NTAP, LO = NTP / 2;
@@ -625,6 +732,12 @@ cudaError_t ensure_constants() {
     if (e != cudaSuccess) return e;
     e = cudaMemcpyToSymbol(c_base28, h_base28, sizeof(h_base28));
     if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_base20, h_base20, sizeof(h_base20));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_base11, h_base11, sizeof(h_base11));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_base17, h_base17, sizeof(h_base17));
+    if (e != cudaSuccess) return e;
     if (dev < 64) g_const_ready[dev] = true;
     return cudaSuccess;
 }
@@ -700,9 +813,16 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
                              char bc, int forward, cudaStream_t stream) {
     if (!dst || DX <= 0 || DY <= 0 || DZ <= 0) { wp_set_error_msg("wp_dwt1d: bad arguments"); return WP_ERR_INVALID_ARG; }
     if (!src) src = dst;
-    if (!is_q3(wavelet) && !is_c4(wavelet) && !is_l2(wavelet)) {
-        wp_set_error_msg("wp_dwt1d: wavelet must be CDF3.5, CDF3.7, CDF4.4, CDF4.6, CDF2.6 or CDF2.8");
+    const bool shortf = wavelet == WP_ID_CDF2_0 || is_t1(wavelet);
+    if (!is_q3(wavelet) && !is_c4(wavelet) && !is_l2(wavelet) && !shortf) {
+        wp_set_error_msg("wp_dwt1d: wavelet must be CDF3.5, CDF3.7, CDF4.4, CDF4.6, CDF2.6, CDF2.8, CDF2.0, "
+                         "CDF1.1 or CDF1.7");
         return WP_ERR_UNSUPPORTED;
+    }
+    // the short families register 'n' and 'd' only (cuWHHDForward.cu:998-1080)
+    if (shortf && bc != 'n' && bc != 'd') {
+        wp_set_error_msg("wp_dwt1d: CDF2.0, CDF1.1 and CDF1.7 take bc 'n' or 'd'");
+        return WP_ERR_INVALID_ARG;
     }
     // 'z': CDF3.x treat it as 'd', CDF4.x as 'n' (cuWHHDForward.cu:760-765, 843-848, 886-891, 970-975);
     // CDF2.x have a rule of their own (:802-828, 928-933)
@@ -723,9 +843,14 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
     }
     if (nouter > 65535) { wp_set_error_msg("wp_dwt1d: outer extent too large"); return WP_ERR_UNSUPPORTED; }
     WP_CUDA_TRY(ensure_constants());
-    if ((wavelet == WP_ID_CDF4_4 || is_l2(wavelet)) && !(N & 1)) {
+    if ((wavelet == WP_ID_CDF4_4 || l2_rules(wavelet)) && !(N & 1)) {
         // their base matrices act on five coefficients: whole-sample lines of 2^levels + 1
         wp_set_error_msg("wp_dwt1d: CDF4.4 and CDF2.x lines have 2^levels + 1 samples");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (is_t1(wavelet) && (N & 1)) {
+        // their base matrices act on four coefficients
+        wp_set_error_msg("wp_dwt1d: CDF1.x lines have 2^levels samples");
         return WP_ERR_INVALID_ARG;
     }
     const int bcd = bc == 'd' ? 1 : (bc == 'z' ? 2 : 0);
@@ -745,6 +870,15 @@ wp_status wp_dwt_axis_launch(T* dst, const T* src, int DX, int DY, int DZ, int l
     else if (wavelet == WP_ID_CDF2_8)
         e = forward ? launch_c<WP_ID_CDF2_8, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
                     : launch_c<WP_ID_CDF2_8, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    else if (wavelet == WP_ID_CDF2_0)
+        e = forward ? launch_c<WP_ID_CDF2_0, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF2_0, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    else if (wavelet == WP_ID_CDF1_1)
+        e = forward ? launch_c<WP_ID_CDF1_1, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF1_1, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
+    else if (wavelet == WP_ID_CDF1_7)
+        e = forward ? launch_c<WP_ID_CDF1_7, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
+                    : launch_c<WP_ID_CDF1_7, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
     else
         e = forward ? launch_c<WP_ID_CDF4_6, true, T>(src, dst, N, levels, bcd, g, nouter, stream)
                     : launch_c<WP_ID_CDF4_6, false, T>(src, dst, N, levels, bcd, g, nouter, stream);
