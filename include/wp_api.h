@@ -131,7 +131,9 @@ CUWHHD_API wp_status wp_recover3d_destroy(wp_recover3d* h);
 /* ---------------------------------------------------------- potential recovery 2D ------- */
 typedef struct wp_recover2d wp_recover2d;
 /* Replaces CuWaveletPotentialRecover2D(int2 dim, DTYPE2 dx, char bc, curl, div)
-   (cuWaveletPotentialRecover2D.cuh:11-12). */
+   (cuWaveletPotentialRecover2D.cuh:11-12).  bc 'n' (zero-normal-flux walls: cuProjectLocal_q_single)
+   or 'd' (Dirichlet walls: the div wavelet takes 'n' and the projection is cuProjectLocal_q_single_n,
+   cuDivLocalProject.cu:1047-1460). */
 CUWHHD_API wp_status wp_recover2d_create(wp_recover2d** h, int nx, int ny, double dx, double dy, char bc,
                                          int curl_wavelet, int div_wavelet);
 /* Replaces CuWaveletPotentialRecover2D::Solve(qz, xv, yv) (cuWaveletPotentialRecover2D.cu:16-36). */

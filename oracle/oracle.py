@@ -50,6 +50,7 @@ def lib():
             "or_project3d": (i, [p, p, p, p, p, p, i, i, i, d, d, d]),
             "or_project3d_nq": (i, [p, p, p, p, p, p, i, i, i, d, d, d]),
             "or_project2d": (i, [p, p, p, i, i, d, d]),
+            "or_project2d_nq": (i, [p, p, p, i, i, d, d]),
             "or_recover3d": (i, [p, p, p, p, p, p, i, i, i, d, d, d, c]),
             "or_recover2d": (i, [p, p, p, i, i, d, d, c]),
             "or_curl3d": (None, [p, p, p, p, p, p, i, i, i, d, d, d]),
@@ -154,10 +155,13 @@ def project3d(xv, yv, zv, n, d, bc="n"):
     return qx, qy, qz
 
 
-def project2d(xv, yv, n, d):
+def project2d(xv, yv, n, d, bc="n"):
+    """CuDivLocalProject::ProjectSingle for the walls' boundary type bc ('n': cuProjectLocal_q_single,
+    'd': cuProjectLocal_q_single_n)."""
     nx, ny = n
     qz = np.zeros((nx + 1, ny + 1))
-    _check(lib().or_project2d(_p(qz), _p(_f64(xv)), _p(_f64(yv)), nx, ny, *d), "project2d")
+    fn = lib().or_project2d if bc == "n" else lib().or_project2d_nq
+    _check(fn(_p(qz), _p(_f64(xv)), _p(_f64(yv)), nx, ny, *d), "project2d")
     return qz
 
 

@@ -122,6 +122,7 @@ int main(int argc, char** argv) {
             int3 dim_ext = make_int3(dim.x + 1, dim.y + 1, dim.z + 1);
             CuDivLocalProject3D cudlp(dim_ext, levels, dx, WaveletType::WT_CDF4_6, proj_bc(wall));
             cudlp.ProjectLocal_q_ccc(qx, qy, qz, xv, yv, zv, levels);
+            checkCudaErrors(cudaGetLastError());
         } else {
             CuWaveletPotentialRecover3D rec(dim, dx, wall, WaveletType::WT_CDF3_7, WaveletType::WT_CDF4_6);
             rec.Solve(qx, qy, qz, xv, yv, zv);
@@ -185,10 +186,11 @@ int main(int argc, char** argv) {
         CuFastSweeping::ParticlesToLs(ls, reinterpret_cast<DTYPE3*>(x), dim, count, h, radius, max_dis, iters);
         checkCudaErrors(cudaDeviceSynchronize());
         write_bin("ls", from_dev(ls, n));
-    } else if (op == "project2d" || op == "recover2d") {  // nx ny dx
+    } else if (op == "project2d" || op == "recover2d") {  // nx ny dx [bc [dy]]
         int2 dim = make_int2(I(0), I(1));
         DTYPE h = (DTYPE)D(2);
-        DTYPE2 dx = make_DTYPE2(h, h);
+        const char wall = argc > 7 ? argv[7][0] : 'n';  // the walls' boundary type
+        DTYPE2 dx = make_DTYPE2(h, argc > 8 ? (DTYPE)D(4) : h);
         size_t sxv = (size_t)(dim.x + 1) * dim.y, syv = (size_t)dim.x * (dim.y + 1), sqz = (size_t)(dim.x + 1) * (dim.y + 1);
         DTYPE* xv = to_dev(read_bin("xv", sxv));
         DTYPE* yv = to_dev(read_bin("yv", syv));
@@ -196,10 +198,11 @@ int main(int argc, char** argv) {
         int2 levels = make_int2((int)log2(dim.x), (int)log2(dim.y));
         if (op == "project2d") {
             int2 dim_ext = make_int2(dim.x + 1, dim.y + 1);
-            CuDivLocalProject cudlp(dim_ext, levels, dx, WaveletType::WT_CDF4_6, proj_bc('n'));
+            CuDivLocalProject cudlp(dim_ext, levels, dx, WaveletType::WT_CDF4_6, proj_bc(wall));
             cudlp.ProjectSingle(qz, xv, yv);
+            checkCudaErrors(cudaGetLastError());  // ProjectSingle does not check its own launch
         } else {
-            CuWaveletPotentialRecover2D rec(dim, dx, 'n', WaveletType::WT_CDF3_7, WaveletType::WT_CDF4_6);
+            CuWaveletPotentialRecover2D rec(dim, dx, wall, WaveletType::WT_CDF3_7, WaveletType::WT_CDF4_6);
             rec.Solve(qz, xv, yv);
         }
         checkCudaErrors(cudaDeviceSynchronize());

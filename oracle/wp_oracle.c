@@ -907,6 +907,141 @@ int or_project2d(double* qz, const double* xv, const double* yv, int nx, int ny,
     return 0;
 }
 
+/* Off-diagonal entry (0, 1) of the Gram matrix of the synthesis basis (row 3 of the reference's
+   inner-product table at index 0, cuGetInnerProduct.cu:11-77, 92-126): the inner product of the
+   synthesis functions of coefficients 0 and 1. */
+static double ip_gram01(int dim, int wavelet, char bc) {
+    int levels = 0;
+    while ((2 << levels) <= dim) ++levels;
+    double* e0 = (double*)calloc((size_t)dim, sizeof(double));
+    double* e1 = (double*)calloc((size_t)dim, sizeof(double));
+    e0[0] = 1.0;
+    e1[1] = 1.0;
+    or_dwt_line(e0, dim, levels, wavelet, bc, 0);
+    or_dwt_line(e1, dim, levels, wavelet, bc, 0);
+    double s = 0.0;
+    for (int j = 0; j < dim; ++j) s += e0[j] * e1[j];
+    free(e0);
+    free(e1);
+    return s;
+}
+
+/* GetDivL0Matrix (DivL0Matrix.cpp:3-46): the 4 x 4 map of the corner potentials of a 2D
+   Dirichlet-wall projection, chosen by the difference of the two axes' levels.  The reference's entry
+   for a difference of 5 is written with minus signs where the others have commas, so its first value
+   is the sum of the four numbers and the other three are 0; it is evaluated here the same way. */
+static void div_l0_matrix(double* dst, int lx, int ly) {
+    int m = lx < ly ? lx : ly;
+    int mx = lx - m, my = ly - m, k = mx > my ? mx : my;
+    double r[4] = {-0.374999999999990, -0.124999999999991, -0.375000000000009, -0.125000000000009};
+    static const double T[8][4] = {
+        {-0.600000000000000, -0.400000000000000, -0.450000000000000, -0.050000000000000},
+        {-1.058823529411764, -0.941176470588235, -0.485294117647059, -0.014705882352941},
+        {-2.030769230769231, -1.969230769230771, -0.496153846153847, -0.003846153846153},
+        {-4.015564202334636, -3.984435797665360, -0.499027237354084, -0.000972762645915},
+        {0, 0, 0, 0},
+        {-16.003905296558496, -15.996094703441514, -0.499938979741274, -0.000061020258726},
+        {-32.001953005797915, -31.998046994202070, -0.499984742142203, -0.000015257857796},
+        {-64.000976547601056, -63.999023452398980, -0.499996185360941, -0.000003814639067}};
+    if (k == 5) {
+        r[0] = -8.007804878048813 - 7.992195121951190 - 0.499756097560973 - 0.000243902439025;
+        r[1] = r[2] = r[3] = 0.0;
+    } else if (k >= 1 && k <= 8) {
+        for (int i = 0; i < 4; ++i) r[i] = T[k - 1][i];
+    }
+    if (mx < my) {
+        double t = r[0]; r[0] = r[2]; r[2] = t;
+        t = r[1]; r[1] = r[3]; r[3] = t;
+    }
+    const double v[16] = {r[0], r[1], r[2], r[3], -r[0], -r[1], r[3], r[2],
+                          r[1], r[0], -r[2], -r[3], -r[1], -r[0], -r[3], -r[2]};
+    memcpy(dst, v, sizeof(v));
+}
+
+/* 2D local projection with Dirichlet domain walls (the recovery's bc 'd': base wavelet CDF4.6 with
+   bc 'n', projection wavelet CDF3.7 with bc 'd'), cuProjectLocal_q_single_n
+   (cuDivLocalProject.cu:1047-1460), launched by ProjectSingle (:2162-2198).  Entry (x, y) of qz, in
+   [0, nx] x [0, ny], reads X(x, y) = xv(x, y - 1) and Y(x, y) = yv(x - 1, y) (0 outside):
+   - x, y >= 2: the pointwise ratio P of the bc 'n' kernel (both passes, half each);
+   - x in {0, 1}, y >= 2: the 2 x 2 solve of the pass along y, which couples the two wall-side
+     coefficients X(0, y), X(1, y) with Y(1, y) through the base table's entries (0, 0) and (0, 1)
+     at the scale dx_inv / nx;
+   - y in {0, 1}, x >= 2: the same along x;
+   - x, y in {0, 1}: the corner map (div_l0_matrix) of X(0, 1), X(1, 1), Y(1, 0), Y(1, 1). */
+int or_project2d_nq(double* qz, const double* xv, const double* yv, int nx, int ny, double dx, double dy) {
+    int Lx = ilog2(nx), Ly = ilog2(ny);
+    if ((1 << Lx) != nx || (1 << Ly) != ny) return 1;
+    double* pbx = (double*)malloc(sizeof(double) * (nx + 1));
+    double* pby = (double*)malloc(sizeof(double) * (ny + 1));
+    double* ppx = (double*)malloc(sizeof(double) * nx);
+    double* ppy = (double*)malloc(sizeof(double) * ny);
+    or_ip_diag(pbx, nx + 1, OR_CDF4_6, 'n');
+    or_ip_diag(pby, ny + 1, OR_CDF4_6, 'n');
+    or_ip_diag(ppx, nx, OR_CDF3_7, 'd');
+    or_ip_diag(ppy, ny, OR_CDF3_7, 'd');
+    const double gx = ip_gram01(nx + 1, OR_CDF4_6, 'n'), gy = ip_gram01(ny + 1, OR_CDF4_6, 'n');
+    double l0[16];
+    div_l0_matrix(l0, Lx, Ly);
+    const double dxi = 1.0 / dx, dyi = 1.0 / dy;
+#define XV(X_, Y_) ((Y_) > 0 ? xv[((Y_) - 1) + (long)(X_) * ny] : 0.0)
+#define YV(X_, Y_) ((X_) > 0 ? yv[(Y_) + (long)((X_) - 1) * (ny + 1)] : 0.0)
+    for (int x = 0; x <= nx; ++x)
+        for (int y = 0; y <= ny; ++y) {
+            const double sx = 4.0 * dxi / ((double)(1 << (Lx - bitlen(x > 0 ? x - 1 : 0) + 1)) + EPS12);
+            const double sy = 4.0 * dyi / ((double)(1 << (Ly - bitlen(y > 0 ? y - 1 : 0) + 1)) + EPS12);
+            double qy = 0.0, qx = 0.0;
+            if (x >= 2 && y >= 2) {
+                const double ip0x = ppx[x - 1], ip1x = pbx[x], ip0y = ppy[y - 1], ip1y = pby[y];
+                const double X = XV(x, y), Y = YV(x, y);
+                const double m1 = sx * sx * ip0x * ip1y + sy * sy * ip1x * ip0y + EPS12;
+                qy = 0.5 * ((X * sy * ip1x * ip0y - Y * sx * ip0x * ip1y) / m1);
+                const double m2 = sy * sy * ip0y * ip1x + sx * sx * ip1y * ip0x + EPS12;
+                qx = 0.5 * ((X * sy * ip0y * ip1x - Y * sx * ip1y * ip0x) / m2);
+            } else if (y >= 2) {  /* x in {0, 1}: the pass along y */
+                const double se = dxi / nx, ip0x = ppx[0], b00 = pbx[0], b01 = gx;
+                const double ip0y = ppy[y - 1], ip1y = pby[y];
+                const double ye = YV(1, y), x0 = XV(0, y), x1 = XV(1, y);
+                double m0 = se * se * ip0x * ip1y + sy * sy * b00 * ip0y;
+                double m1 = -se * se * ip0x * ip1y + sy * sy * b01 * ip0y;
+                const double dv = m0 * m0 - m1 * m1 + EPS12;
+                m0 /= dv;
+                m1 /= -dv;
+                double f1 = ye * se * ip0x * ip1y;
+                f1 += x0 * sy * b00 * ip0y;
+                f1 += x1 * sy * b01 * ip0y;
+                double f2 = -ye * se * ip0x * ip1y;
+                f2 += x0 * sy * b01 * ip0y;
+                f2 += x1 * sy * b00 * ip0y;
+                qy = x == 0 ? m0 * f1 + m1 * f2 : m1 * f1 + m0 * f2;
+            } else if (x >= 2) {  /* y in {0, 1}: the pass along x */
+                const double se = dyi / ny, ip0y = ppy[0], b00 = pby[0], b01 = gy;
+                const double ip0x = ppx[x - 1], ip1x = pbx[x];
+                const double xe = XV(x, 1), y0 = YV(x, 0), y1 = YV(x, 1);
+                double m0 = sx * sx * ip0x * b00 + se * se * ip1x * ip0y;
+                double m1 = sx * sx * ip0x * b01 - se * se * ip1x * ip0y;
+                const double dv = m0 * m0 - m1 * m1 + EPS12;
+                m0 /= dv;
+                m1 /= -dv;
+                const double a00 = ip0x * b00, a01 = ip0x * b01;
+                double f1 = -xe * se * ip1x * ip0y;
+                f1 -= y0 * sx * a00;
+                f1 -= y1 * sx * a01;
+                double f2 = xe * se * ip1x * ip0y;
+                f2 -= y0 * sx * a01;
+                f2 -= y1 * sx * a00;
+                qx = y == 0 ? m0 * f1 + m1 * f2 : m1 * f1 + m0 * f2;
+            } else {  /* the corner */
+                const double* a = l0 + 4 * (2 * y + x);
+                qx = a[2] * XV(0, 1) + a[3] * XV(1, 1) - a[0] * YV(1, 0) - a[1] * YV(1, 1);
+            }
+            qz[y + (long)x * (ny + 1)] = qx + qy;
+        }
+#undef XV
+#undef YV
+    free(pbx); free(pby); free(ppx); free(ppy);
+    return 0;
+}
+
 /* ----------------------------------------------------------- potential recovery ---- */
 /* CuWaveletPotentialRecover3D::Solve (cuWaveletPotentialRecover3D.cu:16-61) */
 int or_recover3d(double* qx, double* qy, double* qz, const double* xv, const double* yv, const double* zv,
@@ -1007,7 +1142,8 @@ int or_cut3d(double* qx, double* qy, double* qz, int nx, int ny, int nz, int lev
 
 /* CuWaveletPotentialRecover2D::Solve (cuWaveletPotentialRecover2D.cu:16-36) */
 int or_recover2d(double* qz, const double* xv, const double* yv, int nx, int ny, double dx, double dy, char bc) {
-    if (bc != 'n') return 2;
+    if (bc != 'n' && bc != 'd') return 2;
+    const char bcd = bc == 'n' ? 'd' : 'n';
     int Lx = ilog2(nx), Ly = ilog2(ny);
     size_t sxv = (size_t)(nx + 1) * ny, syv = (size_t)nx * (ny + 1);
     double* tx = (double*)malloc(sizeof(double) * sxv);
@@ -1015,13 +1151,13 @@ int or_recover2d(double* qz, const double* xv, const double* yv, int nx, int ny,
     memcpy(tx, xv, sizeof(double) * sxv);
     memcpy(ty, yv, sizeof(double) * syv);
     int e = 0;
-    e |= or_dwt_axis(tx, nx + 1, ny, 1, Lx, 'x', OR_CDF4_6, 'd', 1);
+    e |= or_dwt_axis(tx, nx + 1, ny, 1, Lx, 'x', OR_CDF4_6, bcd, 1);
     e |= or_dwt_axis(tx, nx + 1, ny, 1, Ly, 'y', OR_CDF3_7, bc, 1);
     e |= or_dwt_axis(ty, nx, ny + 1, 1, Lx, 'x', OR_CDF3_7, bc, 1);
-    e |= or_dwt_axis(ty, nx, ny + 1, 1, Ly, 'y', OR_CDF4_6, 'd', 1);
-    e |= or_project2d(qz, tx, ty, nx, ny, dx, dy);
-    e |= or_dwt_axis(qz, nx + 1, ny + 1, 1, Lx, 'x', OR_CDF4_6, 'd', 0);
-    e |= or_dwt_axis(qz, nx + 1, ny + 1, 1, Ly, 'y', OR_CDF4_6, 'd', 0);
+    e |= or_dwt_axis(ty, nx, ny + 1, 1, Ly, 'y', OR_CDF4_6, bcd, 1);
+    e |= bc == 'n' ? or_project2d(qz, tx, ty, nx, ny, dx, dy) : or_project2d_nq(qz, tx, ty, nx, ny, dx, dy);
+    e |= or_dwt_axis(qz, nx + 1, ny + 1, 1, Lx, 'x', OR_CDF4_6, bcd, 0);
+    e |= or_dwt_axis(qz, nx + 1, ny + 1, 1, Ly, 'y', OR_CDF4_6, bcd, 0);
     free(tx); free(ty);
     return e;
 }

@@ -40,6 +40,7 @@ int or_ip_diag(double* out, int dim, int wavelet, char bc);
 int or_project3d(double* qx, double* qy, double* qz, const double* xv, const double* yv, const double* zv,
                  int nx, int ny, int nz, double dx, double dy, double dz);
 int or_project2d(double* qz, const double* xv, const double* yv, int nx, int ny, double dx, double dy);
+int or_project2d_nq(double* qz, const double* xv, const double* yv, int nx, int ny, double dx, double dy);
 /* the same projection with Dirichlet domain walls (cuProjectLocal_q_3d_nq_ccc) */
 int or_project3d_nq(double* qx, double* qy, double* qz, const double* xv, const double* yv, const double* zv,
                     int nx, int ny, int nz, double dx, double dy, double dz);

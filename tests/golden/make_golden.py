@@ -14,6 +14,7 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only domd    # projection and recovery with Dirichlet walls
     python tests/golden/make_golden.py --only families  # CDF2.6 / CDF2.8 / CDF4.4 transforms
     python tests/golden/make_golden.py --only short   # CDF2.0 / CDF1.1 / CDF1.7 transforms
+    python tests/golden/make_golden.py --only domd2d  # 2D projection and recovery with Dirichlet walls
     ... [--out DIR]                                   # write the .npz files to DIR instead of here
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
@@ -40,16 +41,18 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 from waveletpotentials_b200.fields import porous_fractions  # noqa: E402
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+DRIVER32 = os.path.join(ROOT, "oracle", "_ref", "ref_driver_f32")
 CDF3_5, CDF2_6, CDF4_4, CDF4_6, CDF2_8, CDF3_7 = 2, 5, 6, 7, 10, 11
 CDF2_0, CDF1_1, CDF1_7 = 16, 17, 18
 
 
-def run(op, inputs: dict, params, outputs: dict):
-    """inputs: name -> array; outputs: name -> shape. Returns dict of output arrays."""
+def run(op, inputs: dict, params, outputs: dict, driver=None):
+    """inputs: name -> array; outputs: name -> shape. Returns dict of output arrays.  driver: the
+    FP64 build (default) or DRIVER32."""
     with tempfile.TemporaryDirectory() as tin, tempfile.TemporaryDirectory() as tout:
         for k, v in inputs.items():
             np.ascontiguousarray(v, dtype=np.float64).tofile(os.path.join(tin, k + ".bin"))
-        cmd = [DRIVER, op, tin, tout] + [str(p) for p in params]
+        cmd = [driver or DRIVER, op, tin, tout] + [str(p) for p in params]
         r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=600, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout[-2000:] + r.stderr[-2000:])
@@ -332,6 +335,31 @@ def domd_cases(rng):
     save("domain_d", **out)
 
 
+def domd2d_cases(rng):
+    """The 2D counterparts with the walls' boundary type 'd': CuDivLocalProject::ProjectSingle with the
+    base wavelet's bc proj_bc('d') = 'n' (cuProjectLocal_q_single_n runs) on random coefficients, and
+    CuWaveletPotentialRecover2D::Solve with bc 'd' on random fields with nonzero wall flux; square,
+    unequal-level (1, 2 and 5 levels apart: the three branches of GetDivL0Matrix the shapes reach)
+    and unequal-spacing grids.  From the FP32 build: in the FP64 build cuProjectLocal_q_single_n needs
+    72 registers a thread in its 1024-thread blocks, more than an SM holds, so its launch fails
+    (cudaErrorLaunchOutOfResources) and the FP64 reference has no 2D Dirichlet-wall projection."""
+    out = {}
+    for tag, n2, hx, hy in (("p16", (16, 16), 1 / 16, 1 / 16), ("p32x16", (32, 16), 1 / 32, 1 / 16),
+                            ("p16x64", (16, 64), 1 / 16, 1 / 64), ("p8x256", (8, 256), 1 / 8, 1 / 8)):
+        xv, yv = rng.standard_normal((n2[0] + 1, n2[1])), rng.standard_normal((n2[0], n2[1] + 1))
+        r = run("project2d", {"xv": xv, "yv": yv}, [*n2, hx, "d", hy], {"qz": (n2[0] + 1, n2[1] + 1)}, DRIVER32)
+        assert np.any(r["qz"] != 0), tag
+        out.update({f"{tag}_{k}": v for k, v in dict(xv=xv, yv=yv, **r).items()})
+        out[f"{tag}_meta"] = np.array([*n2, hx, hy])
+    for tag, n2, hx, hy in (("r16", (16, 16), 1 / 16, 1 / 16), ("r32x64", (32, 64), 1 / 32, 1 / 48),
+                            ("r8x256", (8, 256), 1 / 8, 1 / 256)):
+        xv, yv = rng.standard_normal((n2[0] + 1, n2[1])), rng.standard_normal((n2[0], n2[1] + 1))
+        r = run("recover2d", {"xv": xv, "yv": yv}, [*n2, hx, "d", hy], {"qz": (n2[0] + 1, n2[1] + 1)}, DRIVER32)
+        out.update({f"{tag}_{k}": v for k, v in dict(xv=xv, yv=yv, **r).items()})
+        out[f"{tag}_meta"] = np.array([*n2, hx, hy])
+    save("domain_d2d", **out)
+
+
 def main():
     global OUT_DIR
     if "--out" in sys.argv:
@@ -369,6 +397,9 @@ def main():
         return
     if only == "short":
         short_cases(np.random.default_rng(20261213))
+        return
+    if only == "domd2d":
+        domd2d_cases(np.random.default_rng(20261214))
         return
     rng = np.random.default_rng(20261203)
 

@@ -73,3 +73,28 @@ def test_domain_d_rejects_truncation(wp):
     q = [torch.zeros(s[k], device="cuda") for k in ("qx", "qy", "qz")]
     with pytest.raises(wp.WPError):
         rec.CutCoefficients(*q, *q, 1)
+
+
+@pytest.mark.parametrize("tag", ["p16", "p32x16", "p16x64", "p8x256", "r16", "r32x64", "r8x256"])
+def test_domain_d2d_matches_reference_and_oracle(wp, oracle, tag):
+    """2D: CuDivLocalProject::ProjectSingle with the Dirichlet-wall kernel (cuProjectLocal_q_single_n)
+    and CuWaveletPotentialRecover2D::Solve with bc 'd', against the reference's FP32 build and the FP64
+    oracle; every entry of qz is written and the inputs are left alone."""
+    d = load_golden("domain_d2d")
+    nx, ny, hx, hy = d[tag + "_meta"]
+    n, h = (int(nx), int(ny)), (float(hx), float(hy))
+    rec = wp.CuWaveletPotentialRecover2D(n, h, bc="d")
+    qz = torch.full((n[0] + 1, n[1] + 1), 7.0, device="cuda")
+    xv, yv = T(d[tag + "_xv"]), T(d[tag + "_yv"])
+    x0, y0 = xv.clone(), yv.clone()
+    args = (d[tag + "_xv"], d[tag + "_yv"], n, h)
+    if tag[0] == "p":
+        rec.ProjectSingle(qz, xv, yv)
+        oq = oracle.project2d(*args, bc="d")
+    else:
+        rec.Solve(qz, xv, yv)
+        oq = oracle.recover2d(*args, bc="d")
+    torch.cuda.synchronize()
+    assert torch.equal(xv, x0) and torch.equal(yv, y0)
+    assert rel(d[tag + "_qz"], N(qz)) < 1e-5, (tag, rel(d[tag + "_qz"], N(qz)))
+    assert rel(oq, N(qz)) < 1e-5, tag

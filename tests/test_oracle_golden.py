@@ -238,3 +238,20 @@ def test_domain_d_projection_and_recovery_match_reference(oracle, tag):
     for k, got in zip(("qx", "qy", "qz"), q):
         ref = d[tag + "_" + k]
         assert np.sqrt(np.sum((ref - got) ** 2) / np.sum(ref * ref)) < 1e-7, (tag, k)
+
+
+@pytest.mark.parametrize("tag", ["p16", "p32x16", "p16x64", "p8x256", "r16", "r32x64", "r8x256"])
+def test_domain_d2d_projection_and_recovery_match_reference(oracle, tag):
+    """2D Dirichlet domain walls: CuDivLocalProject::ProjectSingle with bc_base 'n'
+    (cuProjectLocal_q_single_n: its wall rows' 2 x 2 solves and the GetDivL0Matrix corner, for axes
+    0, 1, 2 and 5 levels apart) on random coefficients ("p" cases) and CuWaveletPotentialRecover2D::Solve
+    with bc 'd' on random fields with wall flux ("r" cases).  From the reference's FP32 build (its FP64
+    build cannot launch this kernel: 72 registers a thread in 1024-thread blocks), hence the 3e-6."""
+    d = load_golden("domain_d2d")
+    nx, ny, hx, hy = d[tag + "_meta"]
+    n, h = (int(nx), int(ny)), (float(hx), float(hy))
+    args = (d[tag + "_xv"], d[tag + "_yv"], n, h)
+    got = oracle.project2d(*args, bc="d") if tag[0] == "p" else oracle.recover2d(*args, bc="d")
+    ref = d[tag + "_qz"]
+    assert np.sqrt(np.sum((ref - got) ** 2) / np.sum(ref * ref)) < 3e-6, tag
+    assert np.max(np.abs(ref - got)) < 1e-6 * max(1.0, np.max(np.abs(ref))), tag

@@ -225,3 +225,23 @@ def test_perfect_reconstruction_of_the_short_families(oracle, wav, ext, bc, leve
         oracle.dwt_line(x, levels, wav, "z", True)
     with pytest.raises(RuntimeError):
         oracle.dwt_line(rng.standard_normal((1 << levels) + 1 - ext), levels, wav, bc, True)
+
+
+@pytest.mark.parametrize("n", [(16, 16), (32, 8), (64, 64)])
+def test_2d_recovery_with_dirichlet_walls_is_close_to_the_field(oracle, n):
+    """The reference's 2D recovery with Dirichlet walls is not an exact inverse of the curl, unlike the
+    3D one: on u = curl q with wall flux, curl(recover(u)) differs from u by a smooth field of relative
+    size ~1e-2 (the wall rows' 2 x 2 solves and the corner map are local approximations).  The zero-flux
+    recovery is off by O(1) on the same field.  (For axes 5 levels apart the reference's corner table
+    has a typo, commas written as minus signs, and the recovery is off by O(1); reproduced as is.)"""
+    nx, ny = n
+    rng = np.random.default_rng(nx + ny)
+    d = (1.0 / nx, 1.3 / ny)
+    qz = fields.spectral_field((nx + 1, ny + 1), -3.0, 1.0, rng)
+    u = fields.curl2d(qz, n, d)
+    den = sum(np.sum(a * a) for a in u)
+    err = {}
+    for bc in "dn":
+        c = fields.curl2d(oracle.recover2d(*u, n, d, bc=bc), n, d)
+        err[bc] = np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u, c)) / den)
+    assert err["d"] < 2e-2 and err["n"] > 0.5, err

@@ -1004,6 +1004,46 @@ wp_status wp_ip_diag_device(double* d_out, int dim, int wavelet, char bc, cudaSt
     return st;
 }
 
+namespace {
+__global__ void unit_pair_kernel(double* m, int dim) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 2 * dim) m[i] = (i == 0 || i == dim + 1) ? 1.0 : 0.0;
+}
+__global__ void dot_pair_kernel(const double* m, double* out, int dim) {
+    double s = 0.0;
+    for (int j = threadIdx.x; j < dim; j += blockDim.x) s += m[j] * m[dim + j];
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = red[0];
+}
+}  // namespace
+
+// Entry (0, 1) of the Gram matrix of the synthesis basis (the inner-product table's row 3 at index
+// 0, cuGetInnerProduct.cu:11-77): synthesise the unit coefficients 0 and 1 in FP64 and take the
+// inner product of the two functions.
+wp_status wp_ip_gram01_device(double* d_out, int dim, int wavelet, char bc, cudaStream_t s) {
+    int levels = 0;
+    while ((2 << levels) <= dim) ++levels;
+    double* m = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&m, sizeof(double) * 2 * (size_t)dim, s));
+    unit_pair_kernel<<<wp_cdiv((size_t)2 * dim, 256), 256, 0, s>>>(m, dim);
+    wp_status st = wp_dwt_axis_launch<double>(m, m, 2, dim, 1, levels, 'y', wavelet, bc, 0, s);
+    if (st == WP_OK) {
+        dot_pair_kernel<<<1, 256, 0, s>>>(m, d_out, dim);
+        if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) {
+            wp_set_cuda_error(e, "gram01", __FILE__, __LINE__);
+            st = WP_ERR_CUDA;
+        }
+    }
+    cudaFreeAsync(m, s);
+    return st;
+}
+
 extern "C" CUWHHD_API wp_status wp_ip_diag(double* out, int dim, int wavelet, char bc) {
     if (!out || dim < 4) { wp_set_error_msg("wp_ip_diag: bad arguments"); return WP_ERR_INVALID_ARG; }
     double* d = nullptr;

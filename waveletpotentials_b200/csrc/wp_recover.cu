@@ -25,6 +25,7 @@
 #include <vector>
 
 wp_status wp_ip_diag_device(double* d_out, int dim, int wavelet, char bc, cudaStream_t s);
+wp_status wp_ip_gram01_device(double* d_out, int dim, int wavelet, char bc, cudaStream_t s);
 
 namespace {
 
@@ -220,18 +221,121 @@ __global__ void __launch_bounds__(256) project2d_kernel(float* __restrict__ qz, 
     qz[y + (long)x * (ny + 1)] = out;
 }
 
+// What the 2D Dirichlet-wall projection reads besides the axis tables: per axis the base table's
+// entries (0, 0) and (0, 1) and the wall scale dx_inv / n, and the corner map of GetDivL0Matrix.
+struct Edge2D {
+    float b00[2], b01[2], se[2];
+    float l0[16];
+};
+
+// cuProjectLocal_q_single_n (cuDivLocalProject.cu:1047-1460), the projection of a 2D recovery with
+// Dirichlet walls, one thread per qz entry (x, y) in [0, nx] x [0, ny] with X(x, y) = xv(x, y - 1),
+// Y(x, y) = yv(x - 1, y) (0 outside): the pointwise ratio for x, y >= 2 (half from each of the
+// reference's two passes); at x in {0, 1} (y >= 2) the pass along y solves a 2 x 2 system that couples
+// X(0, y), X(1, y) and Y(1, y); at y in {0, 1} (x >= 2) the pass along x the same with the axes
+// swapped; the four corner entries are the GetDivL0Matrix map of X(0, 1), X(1, 1), Y(1, 0), Y(1, 1).
+__global__ void __launch_bounds__(256) project2d_nq_kernel(float* __restrict__ qz, const float* __restrict__ xv,
+                                                           const float* __restrict__ yv, int nx, int ny, AxisTab tx,
+                                                           AxisTab ty, Edge2D e) {
+    const int y = blockIdx.x * 32 + threadIdx.x;
+    const int x = blockIdx.y * 8 + threadIdx.y;
+    if (y > ny || x > nx) return;
+    auto X = [&](int a, int b) { return b > 0 ? xv[(b - 1) + (long)a * ny] : 0.f; };
+    auto Y = [&](int a, int b) { return a > 0 ? yv[b + (long)(a - 1) * (ny + 1)] : 0.f; };
+    const float sx = tx.s[x > 0 ? x - 1 : 0], sy = ty.s[y > 0 ? y - 1 : 0];
+    float qx = 0.f, qy = 0.f;
+    if (x >= 2 && y >= 2) {
+        const float ip0x = tx.ip0[x - 1], ip1x = tx.ip1[x - 1], ip0y = ty.ip0[y - 1], ip1y = ty.ip1[y - 1];
+        const float xin = X(x, y), yin = Y(x, y);
+        const float m1 = sx * sx * ip0x * ip1y + sy * sy * ip1x * ip0y + kEps;
+        qy = 0.5f * ((xin * sy * ip1x * ip0y - yin * sx * ip0x * ip1y) / m1);
+        const float m2 = sy * sy * ip0y * ip1x + sx * sx * ip1y * ip0x + kEps;
+        qx = 0.5f * ((xin * sy * ip0y * ip1x - yin * sx * ip1y * ip0x) / m2);
+    } else if (y >= 2) {
+        const float se = e.se[0], ip0x = tx.ip0[0], b00 = e.b00[0], b01 = e.b01[0];
+        const float ip0y = ty.ip0[y - 1], ip1y = ty.ip1[y - 1];
+        const float ye = Y(1, y), x0 = X(0, y), x1 = X(1, y);
+        float m0 = se * se * ip0x * ip1y + sy * sy * b00 * ip0y;
+        float m1 = -se * se * ip0x * ip1y + sy * sy * b01 * ip0y;
+        const float dv = m0 * m0 - m1 * m1 + kEps;
+        m0 /= dv;
+        m1 /= -dv;
+        float f1 = ye * se * ip0x * ip1y;
+        f1 += x0 * sy * b00 * ip0y;
+        f1 += x1 * sy * b01 * ip0y;
+        float f2 = -ye * se * ip0x * ip1y;
+        f2 += x0 * sy * b01 * ip0y;
+        f2 += x1 * sy * b00 * ip0y;
+        qy = x == 0 ? m0 * f1 + m1 * f2 : m1 * f1 + m0 * f2;
+    } else if (x >= 2) {
+        const float se = e.se[1], ip0y = ty.ip0[0], b00 = e.b00[1], b01 = e.b01[1];
+        const float ip0x = tx.ip0[x - 1], ip1x = tx.ip1[x - 1];
+        const float xe = X(x, 1), y0 = Y(x, 0), y1 = Y(x, 1);
+        float m0 = sx * sx * ip0x * b00 + se * se * ip1x * ip0y;
+        float m1 = sx * sx * ip0x * b01 - se * se * ip1x * ip0y;
+        const float dv = m0 * m0 - m1 * m1 + kEps;
+        m0 /= dv;
+        m1 /= -dv;
+        const float a00 = ip0x * b00, a01 = ip0x * b01;
+        float f1 = -xe * se * ip1x * ip0y;
+        f1 -= y0 * sx * a00;
+        f1 -= y1 * sx * a01;
+        float f2 = xe * se * ip1x * ip0y;
+        f2 -= y0 * sx * a01;
+        f2 -= y1 * sx * a00;
+        qx = y == 0 ? m0 * f1 + m1 * f2 : m1 * f1 + m0 * f2;
+    } else {
+        const float* a = e.l0 + 4 * (2 * y + x);
+        qx = a[2] * X(0, 1) + a[3] * X(1, 1) - a[0] * Y(1, 0) - a[1] * Y(1, 1);
+    }
+    qz[y + (long)x * (ny + 1)] = qx + qy;
+}
+
+// GetDivL0Matrix (DivL0Matrix.cpp:3-46), by the difference of the two axes' levels; the reference's
+// entry for a difference of 5 has minus signs where the others have commas, so its first value is the
+// sum of the four numbers and the rest are 0, evaluated here the same way.
+void div_l0_matrix(float* dst, int lx, int ly) {
+    const int m = std::min(lx, ly), mx = lx - m, my = ly - m, k = std::max(mx, my);
+    static const double T[8][4] = {
+        {-0.600000000000000, -0.400000000000000, -0.450000000000000, -0.050000000000000},
+        {-1.058823529411764, -0.941176470588235, -0.485294117647059, -0.014705882352941},
+        {-2.030769230769231, -1.969230769230771, -0.496153846153847, -0.003846153846153},
+        {-4.015564202334636, -3.984435797665360, -0.499027237354084, -0.000972762645915},
+        {0, 0, 0, 0},
+        {-16.003905296558496, -15.996094703441514, -0.499938979741274, -0.000061020258726},
+        {-32.001953005797915, -31.998046994202070, -0.499984742142203, -0.000015257857796},
+        {-64.000976547601056, -63.999023452398980, -0.499996185360941, -0.000003814639067}};
+    double r[4] = {-0.374999999999990, -0.124999999999991, -0.375000000000009, -0.125000000000009};
+    if (k == 5) {
+        r[0] = -8.007804878048813 - 7.992195121951190 - 0.499756097560973 - 0.000243902439025;
+        r[1] = r[2] = r[3] = 0.0;
+    } else if (k >= 1 && k <= 8) {
+        for (int i = 0; i < 4; ++i) r[i] = T[k - 1][i];
+    }
+    if (mx < my) {
+        std::swap(r[0], r[2]);
+        std::swap(r[1], r[3]);
+    }
+    const double v[16] = {r[0], r[1], r[2], r[3], -r[0], -r[1], r[3], r[2],
+                          r[1], r[0], -r[2], -r[3], -r[1], -r[0], -r[3], -r[2]};
+    for (int i = 0; i < 16; ++i) dst[i] = (float)v[i];
+}
+
 // Builds the per-axis table [s | ip0 | ip1] (length 3n floats) on the device.  wall: the walls'
 // boundary type; the projection wavelet CDF3.7 takes it, the base wavelet CDF4.6 the other one
 // (CuDivLocalProject3D's constructor, cuDivLocalProject3D.cu:50-60, with bc = proj_bc(wall)).
-wp_status build_axis_table(float** d_tab, int n, double h, cudaStream_t s, char wall = 'n') {
+// edge (when not null): the base table's entries (0, 0) and (0, 1), which the 2D Dirichlet-wall
+// projection reads at its walls.
+wp_status build_axis_table(float** d_tab, int n, double h, cudaStream_t s, char wall = 'n', float* edge = nullptr) {
     const int L = wp_ilog2(n);
     double* d_ip = nullptr;
-    WP_CUDA_TRY(cudaMalloc((void**)&d_ip, sizeof(double) * (2 * n + 1)));
+    WP_CUDA_TRY(cudaMalloc((void**)&d_ip, sizeof(double) * (2 * n + 2)));
     wp_status st = wp_ip_diag_device(d_ip, n, WP_ID_CDF3_7, wall, s);
     if (st == WP_OK) st = wp_ip_diag_device(d_ip + n, n + 1, WP_ID_CDF4_6, wall == 'n' ? 'd' : 'n', s);
-    std::vector<double> ip(2 * n + 1);
+    if (st == WP_OK && edge) st = wp_ip_gram01_device(d_ip + 2 * n + 1, n + 1, WP_ID_CDF4_6, wall == 'n' ? 'd' : 'n', s);
+    std::vector<double> ip(2 * n + 2);
     if (st == WP_OK) {
-        cudaError_t e = cudaMemcpyAsync(ip.data(), d_ip, sizeof(double) * (2 * n + 1), cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaMemcpyAsync(ip.data(), d_ip, sizeof(double) * (2 * n + 2), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { wp_set_cuda_error(e, "ip table copy", __FILE__, __LINE__); st = WP_ERR_CUDA; }
     }
@@ -245,6 +349,10 @@ wp_status build_axis_table(float** d_tab, int n, double h, cudaStream_t s, char 
         tab[i] = (float)(4.0 / h / ((double)(1 << j) + 1e-12));
         tab[n + i] = (float)ip[i];              // ip_proj[i]  (CDF3.7, n points)
         tab[2 * n + i] = (float)ip[n + i + 1];  // ip_base[i+1] (CDF4.6, n+1 points)
+    }
+    if (edge) {
+        edge[0] = (float)ip[n];          // ip_base[0]
+        edge[1] = (float)ip[2 * n + 1];  // Gram entry (0, 1) of the base wavelet
     }
     WP_CUDA_TRY(cudaMalloc((void**)d_tab, sizeof(float) * 3 * n));
     WP_CUDA_TRY(cudaMemcpy(*d_tab, tab.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice));
@@ -479,6 +587,8 @@ struct wp_recover2d {
     int n[2];
     int L[2];
     double h[2];
+    char bc, bcd;  // the walls' boundary type and the div wavelet's (the other one)
+    Edge2D edge;   // bc 'd': what the projection reads at the walls
     float* tab[2];
     float* tmp[2];
 };
@@ -491,19 +601,29 @@ extern "C" CUWHHD_API wp_status wp_recover2d_create(wp_recover2d** out, int nx, 
         wp_set_error_msg("wp_recover2d_create: extents must be powers of two in [4, 4096] and spacings > 0");
         return WP_ERR_INVALID_ARG;
     }
-    if (bc != 'n') { wp_set_error_msg("wp_recover2d_create: only bc 'n' (zero-normal-flux walls) is implemented"); return WP_ERR_UNSUPPORTED; }
+    if (bc != 'n' && bc != 'd') {
+        wp_set_error_msg("wp_recover2d_create: bc must be 'n' (zero-normal-flux walls) or 'd' (Dirichlet walls)");
+        return WP_ERR_UNSUPPORTED;
+    }
     if (!check_wavelets(curl_wavelet, div_wavelet)) { wp_set_error_msg("wp_recover2d_create: curl CDF3.7 / div CDF4.6 only"); return WP_ERR_UNSUPPORTED; }
     wp_recover2d* h = new (std::nothrow) wp_recover2d();
     if (!h) return WP_ERR_INVALID_ARG;
+    h->bc = bc;
+    h->bcd = bc == 'n' ? 'd' : 'n';
     int n[2] = {nx, ny};
     double hs[2] = {dx, dy};
     for (int a = 0; a < 2; ++a) {
         h->n[a] = n[a];
         h->L[a] = wp_ilog2(n[a]);
         h->h[a] = hs[a];
-        wp_status st = build_axis_table(&h->tab[a], n[a], hs[a], 0);
+        float edge[2] = {0.f, 0.f};
+        wp_status st = build_axis_table(&h->tab[a], n[a], hs[a], 0, bc, bc == 'd' ? edge : nullptr);
         if (st != WP_OK) { wp_recover2d_destroy(h); return st; }
+        h->edge.b00[a] = edge[0];
+        h->edge.b01[a] = edge[1];
+        h->edge.se[a] = (float)(1.0 / hs[a] / n[a]);
     }
+    div_l0_matrix(h->edge.l0, h->L[0], h->L[1]);
     if (cudaError_t e = wp_dwt_prepare(); e != cudaSuccess) {
         wp_set_cuda_error(e, "recover2d filters", __FILE__, __LINE__);
         wp_recover2d_destroy(h);
@@ -534,6 +654,12 @@ extern "C" CUWHHD_API wp_status wp_recover2d_project(wp_recover2d* h, float* qz,
     const int nx = h->n[0], ny = h->n[1];
     dim3 grid(wp_cdiv(ny + 1, 32), wp_cdiv(nx + 1, 8));
     cudaStream_t s = (cudaStream_t)stream;
+    if (h->bc == 'd') {
+        WP_KERNEL("project2d", 4.0 * ((double)(nx + 1) * ny * 2 + (double)(nx + 1) * (ny + 1)), s,
+                  project2d_nq_kernel<<<grid, dim3(32, 8), 0, s>>>(qz, xv, yv, nx, ny, view(h->tab[0], nx),
+                                                                   view(h->tab[1], ny), h->edge));
+        return WP_OK;
+    }
     WP_KERNEL("project2d", 4.0 * ((double)(nx + 1) * ny * 2 + (double)(nx + 1) * (ny + 1)), s,
               project2d_kernel<<<grid, dim3(32, 8), 0, s>>>(qz, xv, yv, nx, ny, view(h->tab[0], nx), view(h->tab[1], ny)));
     return WP_OK;
@@ -547,12 +673,13 @@ extern "C" CUWHHD_API wp_status wp_recover2d_run(wp_recover2d* h, float* qz, con
     const int C = WP_ID_CDF3_7, V = WP_ID_CDF4_6;
     float *tx = h->tmp[0], *ty = h->tmp[1];
     wp_status st;
-    if ((st = wp_dwt_axis_launch<float>(tx, xv, nx + 1, ny, 1, Lx, 'x', V, 'd', 1, s)) != WP_OK) return st;
-    if ((st = wp_dwt_axis_launch<float>(tx, tx, nx + 1, ny, 1, Ly, 'y', C, 'n', 1, s)) != WP_OK) return st;
-    if ((st = wp_dwt_axis_launch<float>(ty, yv, nx, ny + 1, 1, Lx, 'x', C, 'n', 1, s)) != WP_OK) return st;
-    if ((st = wp_dwt_axis_launch<float>(ty, ty, nx, ny + 1, 1, Ly, 'y', V, 'd', 1, s)) != WP_OK) return st;
+    const char b = h->bc, d = h->bcd;
+    if ((st = wp_dwt_axis_launch<float>(tx, xv, nx + 1, ny, 1, Lx, 'x', V, d, 1, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(tx, tx, nx + 1, ny, 1, Ly, 'y', C, b, 1, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(ty, yv, nx, ny + 1, 1, Lx, 'x', C, b, 1, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(ty, ty, nx, ny + 1, 1, Ly, 'y', V, d, 1, s)) != WP_OK) return st;
     if ((st = wp_recover2d_project(h, qz, tx, ty, stream)) != WP_OK) return st;
-    if ((st = wp_dwt_axis_launch<float>(qz, qz, nx + 1, ny + 1, 1, Lx, 'x', V, 'd', 0, s)) != WP_OK) return st;
-    if ((st = wp_dwt_axis_launch<float>(qz, qz, nx + 1, ny + 1, 1, Ly, 'y', V, 'd', 0, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(qz, qz, nx + 1, ny + 1, 1, Lx, 'x', V, d, 0, s)) != WP_OK) return st;
+    if ((st = wp_dwt_axis_launch<float>(qz, qz, nx + 1, ny + 1, 1, Ly, 'y', V, d, 0, s)) != WP_OK) return st;
     return WP_OK;
 }
