@@ -330,6 +330,13 @@ CUWHHD_API wp_status wp_fast_sweep_reinit(float* ls, int nx, int ny, int nz, dou
    reference writes them). */
 CUWHHD_API wp_status wp_particles_to_ls(float* ls, const float* xyz, int count, int nx, int ny, int nz, double dx,
                                         double radius, double max_dis, int n_iters, void* stream);
+/* Replaces CuFastSweeping::ParticlesToLsNarrow(ls, x, dim, n_pars, dx, radius, max_dis, n_iters)
+   (cuFastSweeping.cu:352-385): ls on entry is the start (a narrow band or a previous level set, not
+   filled); the particles' rough distances lower it, then n_iters sweeps, negation, n_iters sweeps.
+   max_dis is unused (as in the reference).  Cells outside the grid are skipped (the reference writes
+   them). */
+CUWHHD_API wp_status wp_particles_to_ls_narrow(float* ls, const float* xyz, int count, int nx, int ny, int nz,
+                                               double dx, double radius, double max_dis, int n_iters, void* stream);
 /* 2D: circle level set (CuSolidLevelSet2D, cuSolidLevelSet2D.cu) and face fractions. */
 CUWHHD_API wp_status wp_sdf_circles2d(float* sdf, int nx, int ny, double dx, const double* centers, const double* radii,
                                       int count, void* stream);

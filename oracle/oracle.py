@@ -68,6 +68,7 @@ def lib():
             "or_cut3d": (i, [p, p, p, i, i, i, i]),
             "or_fast_sweep": (None, [p, i, i, i, d, i, i]),
             "or_particles_to_ls": (None, [p, p, i, i, i, i, d, d, d, i]),
+            "or_particles_to_ls_narrow": (None, [p, p, i, i, i, i, d, d, i]),
             "or_fractions3d_subsampled": (None, [p, p, p, p, i, i, i, d]),
             "or_mgfrac2d_solve": (i, [p, p, p, p, p, i, i, d, d, i, i, i, d, i, p]),
             "or_frac_residual3d": (d, [p, p, p, p, p, p, i, i, i, d, d, d]),
@@ -284,6 +285,15 @@ def particles_to_ls(xyz, n, dx, radius, max_dis, iters):
     out = np.zeros((nz, nx, ny))
     pts = _f64(np.reshape(xyz, (-1, 3)))
     lib().or_particles_to_ls(_p(out), _p(pts), pts.shape[0], nx, ny, nz, dx, radius, max_dis, iters)
+    return out
+
+
+def particles_to_ls_narrow(ls, xyz, n, dx, radius, iters):
+    """CuFastSweeping::ParticlesToLsNarrow; ls (DZ, DX, DY) is the start; returns the new level set."""
+    out = np.array(_f64(ls))
+    pts = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+    nx, ny, nz = n
+    lib().or_particles_to_ls_narrow(_p(out), _p(pts), pts.shape[0], nx, ny, nz, dx, radius, iters)
     return out
 
 

@@ -186,6 +186,16 @@ int main(int argc, char** argv) {
         CuFastSweeping::ParticlesToLs(ls, reinterpret_cast<DTYPE3*>(x), dim, count, h, radius, max_dis, iters);
         checkCudaErrors(cudaDeviceSynchronize());
         write_bin("ls", from_dev(ls, n));
+    } else if (op == "p2ls_narrow") {  // nx ny nz dx radius max_dis iters count: ParticlesToLsNarrow on ls
+        int3 dim = make_int3(I(0), I(1), I(2));
+        DTYPE h = (DTYPE)D(3), radius = (DTYPE)D(4), max_dis = (DTYPE)D(5);
+        int iters = I(6), count = I(7);
+        size_t n = (size_t)dim.x * dim.y * dim.z;
+        DTYPE* x = to_dev(read_bin("xyz", (size_t)count * 3));
+        DTYPE* ls = to_dev(read_bin("ls", n));
+        CuFastSweeping::ParticlesToLsNarrow(ls, reinterpret_cast<DTYPE3*>(x), dim, count, h, radius, max_dis, iters);
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("ls", from_dev(ls, n));
     } else if (op == "project2d" || op == "recover2d") {  // nx ny dx [bc [dy]]
         int2 dim = make_int2(I(0), I(1));
         DTYPE h = (DTYPE)D(2);

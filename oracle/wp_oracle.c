@@ -1544,6 +1544,33 @@ void or_particles_to_ls(double* ls, const double* xyz, int count, int nx, int ny
     for (long i = 0; i < n; ++i) ls[i] = -ls[i];
 }
 
+/* CuFastSweeping::ParticlesToLsNarrow (cuFastSweeping.cu:352-385): ls is the caller's start (not
+   filled); the particles lower it as above, then n_iters sweeps, negation, n_iters sweeps (max_dis
+   is not used); cells outside the grid are skipped */
+void or_particles_to_ls_narrow(double* ls, const double* xyz, int count, int nx, int ny, int nz, double dx,
+                               double radius, int iters) {
+    long n = (long)nx * ny * nz;
+    for (int p = 0; p < count; ++p) {
+        double x = xyz[3 * p] / dx - 0.5, y = xyz[3 * p + 1] / dx - 0.5, z = xyz[3 * p + 2] / dx - 0.5;
+        int ix = (int)floor(x), iy = (int)floor(y), iz = (int)floor(z);
+        double fx = x - ix, fy = y - iy, fz = z - iz;
+        double wx[2] = {fx * fx, (1 - fx) * (1 - fx)}, wy[2] = {fy * fy, (1 - fy) * (1 - fy)};
+        double wz[2] = {fz * fz, (1 - fz) * (1 - fz)};
+        for (int k = 0; k < 2; ++k)
+            for (int j = 0; j < 2; ++j)
+                for (int i = 0; i < 2; ++i) {
+                    int cx = ix + j, cy = iy + i, cz = iz + k;
+                    if (cx < 0 || cx >= nx || cy < 0 || cy >= ny || cz < 0 || cz >= nz) continue;
+                    double d = sqrt(wx[j] + wy[i] + wz[k]) * dx - radius;
+                    long q = cy + (long)cx * ny + (long)cz * nx * ny;
+                    if (d < ls[q]) ls[q] = d;
+                }
+    }
+    fsweep3(ls, nx, ny, nz, dx, iters);
+    for (long i = 0; i < n; ++i) ls[i] = -ls[i];
+    fsweep3(ls, nx, ny, nz, dx, iters);
+}
+
 void or_fast_sweep(double* ls, int nx, int ny, int nz, double dx, int iters, int reinit) {
     long n = (long)nx * ny * nz;
     if (reinit) {

@@ -92,6 +92,8 @@ void or_fast_sweep(double* ls, int nx, int ny, int nz, double dx, int iters, int
 /* particles to a level set (CuFastSweeping::ParticlesToLs), xyz: count x 3 positions */
 void or_particles_to_ls(double* ls, const double* xyz, int count, int nx, int ny, int nz, double dx, double radius,
                         double max_dis, int iters);
+void or_particles_to_ls_narrow(double* ls, const double* xyz, int count, int nx, int ny, int nz, double dx,
+                               double radius, int iters);
 /* coefficient truncation of a potential, in place (CuWaveletPotentialRecover3D::CutCoefficients,
    cuWaveletPotentialRecover3D.cu:123-239); 1 for a level outside [0, min log2 n] */
 int or_cut3d(double* qx, double* qy, double* qz, int nx, int ny, int nz, int level);

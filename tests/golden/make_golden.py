@@ -15,6 +15,7 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only families  # CDF2.6 / CDF2.8 / CDF4.4 transforms
     python tests/golden/make_golden.py --only short   # CDF2.0 / CDF1.1 / CDF1.7 transforms
     python tests/golden/make_golden.py --only domd2d  # 2D projection and recovery with Dirichlet walls
+    python tests/golden/make_golden.py --only narrow  # CuFastSweeping::ParticlesToLsNarrow
     ... [--out DIR]                                   # write the .npz files to DIR instead of here
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
@@ -180,6 +181,30 @@ def sweep_cases(rng):
     r3 = run("p2ls", {"xyz": pts}, [nx, ny, nz, h, 0.6 * h, 1.0, 80, len(pts)], {"ls": ls1.shape})["ls"]
     save("fsweep", n=np.array(n), h=h, iters=80, ls_reinit=ls1, out_reinit=r1, ls_solve=ls2, out_solve=r2,
          particles=pts, radius=0.6 * h, max_dis=1.0, out_particles=r3)
+
+
+def narrow_cases(rng):
+    """CuFastSweeping::ParticlesToLsNarrow (cuFastSweeping.cu:352-385): the caller's level set is the
+    start (no fill), lowered by the particles' rough distances, swept, negated and swept again; from a
+    constant band value and from a wavy sphere level set, past convergence (the reference sweeps in
+    place from concurrent threads, so only its fixed point is reproducible), with the particles well
+    inside the box (the reference does not bound-check the cells around a particle)."""
+    n = (24, 20, 16)
+    nx, ny, nz = n
+    h = 1.0 / nx
+    z, x, y = np.meshgrid((np.arange(nz) + 0.5) * h, (np.arange(nx) + 0.5) * h, (np.arange(ny) + 0.5) * h,
+                          indexing="ij")
+    sdf = np.sqrt((x - 0.45) ** 2 + (y - 0.5) ** 2 + (z - 0.35) ** 2) - 0.2
+    starts = {"band": np.full(sdf.shape, 4 * h), "wavy": 0.8 * sdf + 0.01 * np.sin(8 * x) * np.cos(6 * y)}
+    out = {"n": np.array(n), "h": h, "iters": 80, "radius": 0.6 * h, "max_dis": 1.0}
+    for tag, ls0 in starts.items():
+        pts = (np.array([0.55, 0.5, 0.5]) + 0.1 * rng.standard_normal((50, 3))).clip(0.2, 0.8)
+        pts = (pts * np.array([nx, ny, nz]) * h).astype(np.float32).astype(np.float64)
+        ls0 = ls0.astype(np.float32).astype(np.float64)
+        r = run("p2ls_narrow", {"xyz": pts, "ls": ls0}, [nx, ny, nz, h, 0.6 * h, 1.0, 80, len(pts)],
+                {"ls": ls0.shape})["ls"]
+        out.update({f"{tag}_particles": pts, f"{tag}_ls": ls0, f"{tag}_out": r})
+    save("p2ls_narrow", **out)
 
 
 def cdf35_cases(rng):
@@ -397,6 +422,9 @@ def main():
         return
     if only == "short":
         short_cases(np.random.default_rng(20261213))
+        return
+    if only == "narrow":
+        narrow_cases(np.random.default_rng(20261215))
         return
     if only == "domd2d":
         domd2d_cases(np.random.default_rng(20261214))

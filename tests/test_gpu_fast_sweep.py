@@ -77,3 +77,31 @@ def test_particles_to_ls_near_walls_matches_oracle(wp, oracle):
     assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
     sure = np.abs(ref) > 1e-6 * np.abs(ref).max()
     assert np.array_equal((got > 0)[sure], (ref > 0)[sure])
+
+
+@pytest.mark.parametrize("start", ["band", "wavy"])
+def test_particles_to_ls_narrow_matches_reference_and_oracle(wp, oracle, start):
+    """ParticlesToLsNarrow from the caller's level set: the reference's fixed point (FP32) and, with
+    particles also within half a cell of the walls, the oracle (no write outside the grid)."""
+    g = load_golden("p2ls_narrow")
+    n = tuple(int(v) for v in g["n"])
+    h, radius, iters = float(g["h"]), float(g["radius"]), int(g["iters"])
+    ls = T(g[start + "_ls"]).contiguous()
+    wp.CuFastSweeping.ParticlesToLsNarrow(ls, T(g[start + "_particles"]), n, h, radius, 1.0, iters)
+    torch.cuda.synchronize()
+    ref = g[start + "_out"]
+    assert np.abs(N(ls) - ref).max() <= 1e-5 * np.abs(ref).max()
+    assert np.array_equal(N(ls) > 0, ref > 0)
+    e = 0.3 * h
+    ext = np.array([n[0] * h, n[1] * h, n[2] * h])
+    pts = np.concatenate([g[start + "_particles"], [[e, e, e], [ext[0] - e, 0.5 * ext[1], ext[2] - e]]])
+    xyz = np.asarray(pts, np.float32).astype(np.float64)
+    ref = oracle.particles_to_ls_narrow(g[start + "_ls"], xyz, n, h, radius, iters)
+    cells = n[0] * n[1] * n[2]
+    buf = torch.full((cells + 2 * 4096,), 12345.0, device="cuda")
+    ls = buf[4096:4096 + cells].view(n[2], n[0], n[1])
+    ls.copy_(T(g[start + "_ls"]))
+    wp.CuFastSweeping.ParticlesToLsNarrow(ls, T(xyz), n, h, radius, 1.0, iters)
+    torch.cuda.synchronize()
+    assert np.abs(N(ls) - ref).max() <= 1e-5 * np.abs(ref).max()
+    assert float(buf[:4096].min()) == 12345.0 and float(buf[4096 + cells:].min()) == 12345.0

@@ -172,6 +172,18 @@ def test_fast_sweep_matches_reference_fixed_point(oracle):
     assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max(), np.abs(out - ref).max()
 
 
+@pytest.mark.parametrize("start", ["band", "wavy"])
+def test_particles_to_ls_narrow_matches_reference_fixed_point(oracle, start):
+    """CuFastSweeping::ParticlesToLsNarrow from a constant band and from a wavy level set, past
+    convergence: the oracle reaches the reference's fixed point."""
+    g = load_golden("p2ls_narrow")
+    n = tuple(int(v) for v in g["n"])
+    out = oracle.particles_to_ls_narrow(g[start + "_ls"], g[start + "_particles"], n, float(g["h"]),
+                                        float(g["radius"]), int(g["iters"]))
+    ref = g[start + "_out"]
+    assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max(), np.abs(out - ref).max()
+
+
 def test_mg2d_matches_reference_per_cycle(oracle):
     p = load_golden("mg2d_32")
     n = tuple(int(v) for v in p["n"])

@@ -99,6 +99,7 @@ SIGNATURES = {
     "wp_fast_sweep_solve": (I, [P, I, I, I, D, I, P]),
     "wp_fast_sweep_reinit": (I, [P, I, I, I, D, I, P]),
     "wp_particles_to_ls": (I, [P, P, I, I, I, I, D, D, D, I, P]),
+    "wp_particles_to_ls_narrow": (I, [P, P, I, I, I, I, D, D, D, I, P]),
     "wp_sdf_boxes3d": (I, [P, I, I, I, D, P, P, I, P]),
     "wp_sdf_circles2d": (I, [P, I, I, D, P, P, I, P]),
     "wp_fractions2d": (I, [P, P, P, I, I, D, P]),

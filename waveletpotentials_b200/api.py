@@ -490,6 +490,19 @@ def ParticlesToLs(ls, x, dim, dx, radius, max_dis, n_iters, stream=None):
 CuFastSweeping.ParticlesToLs = staticmethod(ParticlesToLs)
 
 
+def ParticlesToLsNarrow(ls, x, dim, dx, radius, max_dis, n_iters, stream=None):
+    """CuFastSweeping::ParticlesToLsNarrow: ls (CUDA float32 (DZ, DX, DY)) holds the start and receives
+    the level set of the particles x (CUDA float32 (count, 3))."""
+    d = _dims3(dim)
+    count = int(x.shape[0])
+    check(lib().wp_particles_to_ls_narrow(_ptr(ls, (d[2], d[0], d[1])), _ptr(x, (count, 3)), count, *d, float(dx),
+                                          float(radius), float(max_dis), int(n_iters), _stream(stream)),
+          "wp_particles_to_ls_narrow")
+
+
+CuFastSweeping.ParticlesToLsNarrow = staticmethod(ParticlesToLsNarrow)
+
+
 class CuSolidLevelSet2D:
     """CuSolidLevelSet2D: circle level set (positive in fluid) and face open fractions."""
 

@@ -724,6 +724,38 @@ extern "C" CUWHHD_API wp_status wp_particles_to_ls(float* ls, const float* xyz, 
     return st;
 }
 
+// CuFastSweeping::ParticlesToLsNarrow (cuFastSweeping.cu:352-385): the caller's ls is the start (no
+// fill); the particles lower it, then n_iters sweeps, negation (cuInvLevelSet_nb), n_iters sweeps, and
+// no final negation; max_dis is accepted and unused, as in the reference.
+extern "C" CUWHHD_API wp_status wp_particles_to_ls_narrow(float* ls, const float* xyz, int count, int nx, int ny,
+                                                          int nz, double dx, double radius, double max_dis,
+                                                          int n_iters, void* stream) {
+    (void)max_dis;
+    if (!ls || (count > 0 && !xyz) || count < 0 || nx < 1 || ny < 1 || nz < 1 || nz > 65535 || !(dx > 0) ||
+        n_iters < 0) {
+        wp_set_error_msg("wp_particles_to_ls_narrow: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const long n = (long)nx * ny * nz;
+    const unsigned gn = (unsigned)std::min<long>(wp_cdiv(n, 256), (long)wp_sm_count() * 16);
+    if (count > 0)
+        WP_KERNEL("particles_rough", 12.0 * count, s,
+                  particles_rough_kernel<<<(unsigned)wp_cdiv(count, 256), 256, 0, s>>>(ls, xyz, count, nx, ny, nz, dx,
+                                                                                     radius));
+    float* tmp = nullptr;
+    WP_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * n, s));
+    wp_status st = WP_OK;
+    auto negate = [&]() -> wp_status {
+        WP_KERNEL("negate", 8.0 * n, s, negate_kernel<<<gn, 256, 0, s>>>(ls, n));
+        return WP_OK;
+    };
+    if ((st = fsweep_iters(ls, tmp, nx, ny, nz, dx, n_iters, s)) == WP_OK && (st = negate()) == WP_OK)
+        st = fsweep_iters(ls, tmp, nx, ny, nz, dx, n_iters, s);
+    cudaFreeAsync(tmp, s);
+    return st;
+}
+
 extern "C" CUWHHD_API wp_status wp_fast_sweep_solve(float* ls, int nx, int ny, int nz, double dx, int n_iters,
                                                     void* stream) {
     return fsweep_entry(ls, nx, ny, nz, dx, n_iters, false, (cudaStream_t)stream);
