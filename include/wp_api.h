@@ -458,10 +458,12 @@ CUWHHD_API wp_status wp_unet_destroy(wp_unet* h);
    uniform spacing dx[i], caller-owned face fractions ax[i], ay[i], az[i] (az may be NULL when all
    grids are 2D)).  Each grid is projected as the reference test does for one grid
    (TestLocalProjection.cpp:666-767): b = -div(a u), a mixed-precision multigrid solve, u <- (u -
-   grad p) a, max|div u|, wavelet potential recovery.  wp_batch_plan runs every grid once eagerly
-   (tolerance-driven, params->rel_tol) to fix its number of refinement steps; wp_batch_run then
-   launches the whole batch as ONE CUDA graph whose grids are spread over `nstreams` concurrent
-   branches (the graph is captured on the first run and again whenever the field pointers change). */
+   grad p) a, max|div u|, wavelet potential recovery.  wp_batch_run launches the whole batch as ONE
+   CUDA graph whose grids are spread over `nstreams` concurrent branches (the graph is captured on the
+   first run and again whenever the field pointers change); each grid's solve is a device-side loop
+   (a conditional while-node) that stops at params->rel_tol or params->max_cycles on every replay, so
+   the step counts follow the input.  wp_batch_plan (optional) runs every grid once eagerly on a
+   representative input; its step counts order the grids over the branches, costliest first. */
 typedef struct wp_batch wp_batch;
 CUWHHD_API wp_status wp_batch_create(wp_batch** h, int count, const int* dims, const int* ext, const double* dx,
                                      const float* const* ax, const float* const* ay, const float* const* az,
@@ -473,10 +475,10 @@ CUWHHD_API wp_status wp_batch_plan(wp_batch* h, const float* const* xv, const fl
    qz only and may pass NULL in zv/qx/qy).  Asynchronous on `stream`. */
 CUWHHD_API wp_status wp_batch_run(wp_batch* h, float* const* xv, float* const* yv, float* const* zv, float* const* qx,
                                   float* const* qy, float* const* qz, void* stream);
-/* Per grid: max|div u| after projection and the final FP64 relative residual of the last run;
-   any output may be NULL.  Synchronous.  The replayed step counts are the plan's, so the tolerance
-   is tested again: WP_ERR_NOT_CONVERGED when any grid's residual is above rel_tol (all outputs
-   written; plan again on such inputs), WP_ERR_DEVICE_WAIT when a bounded device wait gave up. */
+/* Per grid: max|div u| after projection, the final FP64 relative residual and the V-cycles of the
+   last run; any output may be NULL.  Synchronous.  WP_ERR_NOT_CONVERGED when any grid's residual is
+   above rel_tol (its loop reached max_cycles or a non-finite residual; all outputs written),
+   WP_ERR_DEVICE_WAIT when a bounded device wait gave up. */
 CUWHHD_API wp_status wp_batch_results(wp_batch* h, double* max_abs_div, double* rel_residual, int* cycles,
                                       void* stream);
 CUWHHD_API wp_status wp_batch_destroy(wp_batch* h);

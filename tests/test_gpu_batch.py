@@ -127,8 +127,9 @@ def test_batch_recovery_matches_oracle(wp, oracle):
 def test_batch_rejects_bad_arguments(wp):
     grids, u = _grids(wp)
     bp = wp.BatchProjector(grids[:2], rel_tol=1e-6, nstreams=2)
+    outs = _outs(wp, grids[:2])
     with pytest.raises(wp.WPError):
-        bp.run(u[:2], _outs(wp, grids[:2]))  # run before plan
+        bp.run([[u[0][0], u[0][1], torch.zeros(3, device="cuda")], u[1]], outs)  # a 3D grid's zv of a wrong shape
     s = wp.mac_shapes2d(48, 64)  # 48 is not a power of two: the wavelet recovery rejects it
     bad = {"dim": (48, 64), "dx": 1 / 64, "ax": torch.ones(s["xv"], device="cuda"),
            "ay": torch.ones(s["yv"], device="cuda")}

@@ -843,7 +843,8 @@ class BatchProjector:
         return [_parray(c) for c in cols]
 
     def plan(self, fields, stream=None):
-        """Eager tolerance-driven pass; returns the refinement steps of each grid (fields unchanged)."""
+        """Eager tolerance-driven pass on representative fields; returns each grid's V-cycles (fields
+        unchanged).  Optional: the counts only order the grids over the graph's branches."""
         c = self._fields(fields)
         cyc = (ctypes.c_int * self.count)()
         check(lib().wp_batch_plan(self._h, ctypes.cast(c[0], ctypes.c_void_p), ctypes.cast(c[1], ctypes.c_void_p),
@@ -858,10 +859,10 @@ class BatchProjector:
               "wp_batch_run")
 
     def results(self, stream=None) -> dict:
-        """Per-grid max|div|, relative residual and step count of the last run.  The replay's step
-        counts are the plan's, so the tolerance is tested again: ``over_tol[i]`` is true for a grid
-        whose residual is above ``rel_tol`` and ``status`` is then ``WP_ERR_NOT_CONVERGED`` (plan
-        again on such inputs).  Any other failure raises."""
+        """Per-grid max|div|, relative residual and V-cycles of the last run (each grid's device loop
+        stops at ``rel_tol`` or ``max_cycles``).  ``over_tol[i]`` is true for a grid whose residual is
+        still above ``rel_tol`` and ``status`` is then ``WP_ERR_NOT_CONVERGED``.  Any other failure
+        raises."""
         m = (ctypes.c_double * self.count)()
         r = (ctypes.c_double * self.count)()
         cyc = (ctypes.c_int * self.count)()

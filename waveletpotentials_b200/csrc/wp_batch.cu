@@ -1,11 +1,14 @@
 // wp_batch.cu -- many independent projections of uneven sizes (2D and 3D) in one CUDA-graph launch.
 //
-// No reference counterpart (the reference runs one grid per process).  Plan: an eager pass per grid
-// (divergence + tolerance-driven mixed-precision solve) fixes each grid's refinement-step count, then
-// the whole batch -- divergence, fixed-count mixed solve, gradient update, max|div|, wavelet
-// recovery for every grid -- is captured once into a CUDA graph with the grids spread over
-// `nstreams` concurrent branches, and replayed with one cudaGraphLaunch.  Per-grid max|div| and the
-// final FP64 relative residual stay on the device until wp_batch_results() reads them with one copy.
+// No reference counterpart (the reference runs one grid per process).  The whole batch --
+// divergence, tolerance-driven mixed-precision solve, gradient update, max|div|, wavelet recovery
+// for every grid -- is captured once into a CUDA graph with the grids spread over `nstreams`
+// concurrent branches, and replayed with one cudaGraphLaunch.  Each grid's solve is a device-side
+// loop (a while-node whose body is one refinement step and whose test kernel applies the stopping
+// rule), so every replay runs as many steps as that grid's current input needs.  An optional eager
+// plan pass (wp_batch_plan) measures the step counts of a representative input; they only order the
+// grids over the branches (costliest first).  Per-grid max|div|, the final FP64 relative residual and
+// the V-cycle count stay on the device until wp_batch_results() reads them with one copy.
 #include "wp_common.cuh"
 
 #include <algorithm>
@@ -16,8 +19,9 @@
 
 struct wp_mgfrac2d;
 wp_status wp_mg_prepare_mixed(wp_mgfrac3d* h);
-wp_status wp_mg_solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
-                                        cudaStream_t s);
+wp_status wp_mg_solve_mixed_loop_capture(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm,
+                                         cudaStream_t s, long long* body_launches);
+const void* wp_mg_loop_state(const wp_mgfrac3d* h);
 void wp_mg_forbid_persistent(wp_mgfrac3d* h);
 wp_status wp_mg_solve_tol_internal(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm, wp_mg_report* r,
                                    cudaStream_t s);
@@ -39,20 +43,26 @@ struct Grid {
     wp_recover2d* rec2 = nullptr;
     float* b = nullptr;
     float* p = nullptr;
-    int cycles = 0;
+    int cycles = 0;               // V-cycles of the plan's eager solve (orders the branches)
+    long long body_launches = 0;  // kernels in one pass of the captured loop body
     long cells() const { return (long)n[0] * n[1] * n[2]; }
     wp_mgfrac3d* mg() const { return dims == 3 ? mg3 : wp_mg2d_impl(mg2); }
 };
 
-// per grid: max|div|, the FP64 relative residual of the last refinement step, and the MG handle's
-// device error flag (the int after its four norm slots; nonzero when a bounded wait gave up)
-__global__ void gather_results_kernel(double* out, const double* const* slots, const unsigned* maxbits, int count) {
+constexpr int kOut = 5;  // per-grid results
+// per grid: max|div|, the FP64 relative residual of the last refinement step, the MG handle's device
+// error flag (the int after its four norm slots; nonzero when a bounded wait gave up), and the
+// device loop's V-cycle and refinement-step counts (ints 0 and 4 of its state)
+__global__ void gather_results_kernel(double* out, const double* const* slots, const int* const* loops,
+                                      const unsigned* maxbits, int count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const double* a = slots[i];
-    out[3 * i] = (double)__uint_as_float(maxbits[i]);
-    out[3 * i + 1] = a[1] > 0.0 ? sqrt(a[0] / a[1]) : 0.0;
-    out[3 * i + 2] = (double)*reinterpret_cast<const int*>(a + 4);
+    out[kOut * i] = (double)__uint_as_float(maxbits[i]);
+    out[kOut * i + 1] = a[1] > 0.0 ? sqrt(a[0] / a[1]) : 0.0;
+    out[kOut * i + 2] = (double)*reinterpret_cast<const int*>(a + 4);
+    out[kOut * i + 3] = (double)loops[i][0];
+    out[kOut * i + 4] = (double)loops[i][4];
 }
 
 }  // namespace
@@ -64,12 +74,14 @@ struct wp_batch {
     wp_mg_params prm;
     unsigned* d_max = nullptr;       // per grid: max|div| bits
     const double** d_slots = nullptr; // per grid: pointer to the MG handle's norm slots
-    double* d_out = nullptr;         // per grid: (max|div|, rel residual, device error flag)
+    const int** d_loops = nullptr;   // per grid: pointer to the MG handle's device loop state
+    double* d_out = nullptr;         // per grid: kOut results (see gather_results_kernel)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<const void*> bound;  // pointers captured into the graph
-    long long graph_launches = 0;    // kernels in one replay of the graph
+    long long graph_launches = 0;    // kernels in one replay of the graph outside the loop bodies
     bool planned = false;
+    bool counted = true;             // the last replay's loop-body kernels were added to the count
 };
 
 namespace {
@@ -83,7 +95,7 @@ wp_status project_one(wp_batch* B, int i, float* xv, float* yv, float* zv, float
         if ((st = wp_divergence_frac3d(G.b, xv, yv, zv, G.frac[0], G.frac[1], G.frac[2], G.n[0], G.n[1], G.n[2], h, h,
                                        h, s)) != WP_OK)
             return st;
-        if ((st = wp_mg_solve_mixed_fixed_async(G.mg3, G.p, G.b, G.cycles, &B->prm, s)) != WP_OK) return st;
+        if ((st = wp_mg_solve_mixed_loop_capture(G.mg3, G.p, G.b, &B->prm, s, &G.body_launches)) != WP_OK) return st;
         // the gradient of the FP64 iterate, formed in FP64 (as the one-grid projector does)
         if ((st = wp_grad_subtract_frac3d_p64(xv, yv, zv, wp_mg_p64(G.mg3), G.frac[0], G.frac[1], G.frac[2], G.n[0],
                                               G.n[1], G.n[2], h, h, h, 1, s)) != WP_OK)
@@ -95,7 +107,8 @@ wp_status project_one(wp_batch* B, int i, float* xv, float* yv, float* zv, float
         return wp_recover3d_run(G.rec3, qx, qy, qz, xv, yv, zv, s);
     }
     if ((st = wp_divergence_frac2d(G.b, xv, yv, G.frac[0], G.frac[1], G.n[0], G.n[1], h, h, s)) != WP_OK) return st;
-    if ((st = wp_mg_solve_mixed_fixed_async(wp_mg2d_impl(G.mg2), G.p, G.b, G.cycles, &B->prm, s)) != WP_OK) return st;
+    if ((st = wp_mg_solve_mixed_loop_capture(wp_mg2d_impl(G.mg2), G.p, G.b, &B->prm, s, &G.body_launches)) != WP_OK)
+        return st;
     if ((st = wp_grad_subtract_frac2d(xv, yv, G.p, G.frac[0], G.frac[1], G.n[0], G.n[1], h, h, 1, s)) != WP_OK) return st;
     if ((st = wp_divergence_frac2d(G.b, xv, yv, nullptr, nullptr, G.n[0], G.n[1], h, h, s)) != WP_OK) return st;
     if ((st = wp_max_abs_device(G.b, G.cells(), B->d_max + i, s)) != WP_OK) return st;
@@ -165,11 +178,17 @@ extern "C" CUWHHD_API wp_status wp_batch_create(wp_batch** out, int count, const
         for (auto& s : B->streams) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
         for (auto& e : B->events) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
         std::vector<const double*> slots(count);
-        for (int i = 0; i < count; ++i) slots[i] = wp_mg_slots(B->g[i].mg());
+        std::vector<const int*> loops(count);
+        for (int i = 0; i < count; ++i) {
+            slots[i] = wp_mg_slots(B->g[i].mg());
+            loops[i] = reinterpret_cast<const int*>(wp_mg_loop_state(B->g[i].mg()));
+        }
         cudaError_t e = cudaMalloc((void**)&B->d_max, sizeof(unsigned) * count);
         if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_slots, sizeof(double*) * count);
-        if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_out, sizeof(double) * 3 * count);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_loops, sizeof(int*) * count);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_out, sizeof(double) * kOut * count);
         if (e == cudaSuccess) e = cudaMemcpy(B->d_slots, slots.data(), sizeof(double*) * count, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(B->d_loops, loops.data(), sizeof(int*) * count, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) { wp_set_cuda_error(e, "batch alloc", __FILE__, __LINE__); st = WP_ERR_CUDA; }
     }
     if (st != WP_OK) { wp_batch_destroy(B); return st; }
@@ -177,8 +196,9 @@ extern "C" CUWHHD_API wp_status wp_batch_create(wp_batch** out, int count, const
     return WP_OK;
 }
 
-// Eager pass: per grid, b = -div(a u) and a tolerance-driven mixed solve; records the refinement
-// steps each grid needs (the velocities are not modified).  Synchronous.
+// Eager pass: per grid, b = -div(a u) and a tolerance-driven mixed solve; records the V-cycles each
+// grid needs on this input (the velocities are not modified), which order the grids over the graph's
+// branches.  Optional: without it the grids are ordered by size.  Synchronous.
 extern "C" CUWHHD_API wp_status wp_batch_plan(wp_batch* B, const float* const* xv, const float* const* yv,
                                               const float* const* zv, int* cycles_out, void* stream) {
     if (!B || !xv || !yv) { wp_set_error_msg("wp_batch_plan: null pointer"); return WP_ERR_INVALID_ARG; }
@@ -210,7 +230,6 @@ extern "C" CUWHHD_API wp_status wp_batch_plan(wp_batch* B, const float* const* x
 extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, float* const* yv, float* const* zv,
                                              float* const* qx, float* const* qy, float* const* qz, void* stream) {
     if (!B || !xv || !yv || !qz) { wp_set_error_msg("wp_batch_run: null pointer"); return WP_ERR_INVALID_ARG; }
-    if (!B->planned) { wp_set_error_msg("wp_batch_run: call wp_batch_plan first"); return WP_ERR_INVALID_ARG; }
     const int count = (int)B->g.size();
     std::vector<const void*> ptrs;
     for (int i = 0; i < count; ++i) {
@@ -230,11 +249,12 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
         wp_status st = WP_OK;
         cudaEventRecord(B->events[0], cs);
         for (size_t k = 1; k < B->streams.size(); ++k) cudaStreamWaitEvent(B->streams[k], B->events[0], 0);
-        // longest grids first, round-robin over the branches
+        // costliest grids first (cells x (planned V-cycles + 2), or cells alone without a plan),
+        // round-robin over the branches
         std::vector<int> order(count);
         for (int i = 0; i < count; ++i) order[i] = i;
-        std::stable_sort(order.begin(), order.end(),
-                         [&](int a, int b) { return B->g[a].cells() * (B->g[a].cycles + 2) > B->g[b].cells() * (B->g[b].cycles + 2); });
+        auto cost = [&](int i) { return B->g[i].cells() * (B->planned ? B->g[i].cycles + 2 : 1); };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
         for (int k = 0; k < count && st == WP_OK; ++k) {
             const int i = order[k];
             const bool d3 = B->g[i].dims == 3;
@@ -247,8 +267,9 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
         }
         if (st == WP_OK) {
             const int tok = wp_prof_start(cs);
-            gather_results_kernel<<<wp_cdiv(count, 128), 128, 0, cs>>>(B->d_out, B->d_slots, B->d_max, count);
-            wp_prof_stop(tok, "batch_gather", 24.0 * count, cs);
+            gather_results_kernel<<<wp_cdiv(count, 128), 128, 0, cs>>>(B->d_out, B->d_slots, B->d_loops, B->d_max,
+                                                                       count);
+            wp_prof_stop(tok, "batch_gather", 8.0 * kOut * count, cs);
         }
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(cs, &graph);
@@ -264,36 +285,45 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
     }
     const int tok = wp_prof_start(s);
     wp_add_launches(B->graph_launches - 1);
+    B->counted = false;
     const cudaError_t e = cudaGraphLaunch(B->exec, s);
     wp_prof_stop(tok, "batch_graph", 0.0, s);
     if (e != cudaSuccess) { wp_set_cuda_error(e, "batch graph launch", __FILE__, __LINE__); return WP_ERR_CUDA; }
     return WP_OK;
 }
 
-// Per grid (max|div| of the projected field, final FP64 relative residual); synchronous.  The
-// replayed step counts were fixed by the plan, so the tolerance is tested again here: a grid whose
-// residual is above it makes the call return WP_ERR_NOT_CONVERGED (every output still written).
-// A bounded device wait that gave up in any grid's solve takes precedence (WP_ERR_DEVICE_WAIT; its
-// flag is cleared).
+// Per grid (max|div| of the projected field, final FP64 relative residual, V-cycles of the last
+// replay); synchronous.  Each grid's device loop stops at the tolerance or at max_cycles, so a grid
+// whose residual is still above the tolerance (the cycle cap reached, or a non-finite residual) makes
+// the call return WP_ERR_NOT_CONVERGED (every output still written).  A bounded device wait that gave
+// up in any grid's solve takes precedence (WP_ERR_DEVICE_WAIT; its flag is cleared).
 extern "C" CUWHHD_API wp_status wp_batch_results(wp_batch* B, double* max_abs_div, double* rel_residual,
                                                  int* cycles, void* stream) {
     if (!B) { wp_set_error_msg("wp_batch_results: null handle"); return WP_ERR_INVALID_ARG; }
     const int count = (int)B->g.size();
-    std::vector<double> out(3 * count);
+    std::vector<double> out(kOut * count);
     cudaStream_t s = (cudaStream_t)stream;
-    WP_CUDA_TRY(wp_read_small(out.data(), B->d_out, sizeof(double) * 3 * count, s));
+    WP_CUDA_TRY(wp_read_small(out.data(), B->d_out, sizeof(double) * kOut * count, s));
     WP_CUDA_TRY(cudaStreamSynchronize(s));
     int over = 0, waits = 0;
     for (int i = 0; i < count; ++i) {
-        if (max_abs_div) max_abs_div[i] = out[3 * i];
-        if (rel_residual) rel_residual[i] = out[3 * i + 1];
-        if (cycles) cycles[i] = B->g[i].cycles;
-        if (B->prm.rel_tol > 0.0 && !(out[3 * i + 1] <= B->prm.rel_tol)) ++over;
-        if (out[3 * i + 2] != 0.0) {
+        const double* o = out.data() + kOut * i;
+        if (max_abs_div) max_abs_div[i] = o[0];
+        if (rel_residual) rel_residual[i] = o[1];
+        if (cycles) cycles[i] = (int)o[3];
+        if (B->prm.rel_tol > 0.0 && !(o[1] <= B->prm.rel_tol)) ++over;
+        // the loop bodies of the last replay: their kernels, counted now that the passes are known (a
+        // full-multigrid start runs its first step before the loop, in the counted part of the graph)
+        if (!B->counted) {
+            const long long passes = (long long)o[4] - (B->prm.start == WP_START_FMG ? 1 : 0);
+            wp_add_launches(std::max(passes, 0LL) * B->g[i].body_launches);
+        }
+        if (o[2] != 0.0) {
             ++waits;
             WP_CUDA_TRY(cudaMemsetAsync((void*)(wp_mg_slots(B->g[i].mg()) + 4), 0, sizeof(int), s));
         }
     }
+    B->counted = true;
     char msg[160];
     if (waits) {
         WP_CUDA_TRY(cudaStreamSynchronize(s));
@@ -325,6 +355,7 @@ extern "C" CUWHHD_API wp_status wp_batch_destroy(wp_batch* B) {
     for (auto& e : B->events) cudaEventDestroy(e);
     if (B->d_max) cudaFree(B->d_max);
     if (B->d_slots) cudaFree((void*)B->d_slots);
+    if (B->d_loops) cudaFree((void*)B->d_loops);
     if (B->d_out) cudaFree(B->d_out);
     delete B;
     return WP_OK;

@@ -3809,6 +3809,83 @@ wp_status prepare_mixed(wp_mgfrac3d* h) {
     const long n = h->lv[0].cells;
     if (!h->p64) WP_CUDA_TRY(cudaMalloc((void**)&h->p64, sizeof(double) * n));
     if (!h->r32) WP_CUDA_TRY(cudaMalloc((void**)&h->r32, sizeof(float) * n));
+    if (!h->loop_state) WP_CUDA_TRY(cudaMalloc(&h->loop_state, sizeof(MgLoop)));
+    if (!h->loop_cap) WP_CUDA_TRY(cudaStreamCreateWithFlags(&h->loop_cap, cudaStreamNonBlocking));
+    return WP_OK;
+}
+
+// The loop test before the first step (nothing counted): go while the initial defect misses the
+// tolerance, the cycle cap allows a step and the residual is finite -- solve_tol's host test.
+__global__ void mg_loop_start_kernel(MgLoop* st, const double* __restrict__ acc, cudaGraphConditionalHandle hc) {
+    double nf2 = acc[1];
+    if (!(nf2 > 0.0)) nf2 = 1.0;
+    const double rel = sqrt(acc[0] / nf2);
+    st->rel = rel;
+    const bool go = !(st->use_tol && rel <= st->tol) && st->max_cycles > 0 && isfinite(rel);
+    cudaGraphSetConditional(hc, go ? 1u : 0u);
+}
+
+// The tolerance-driven mixed solve with its cycle loop on the device, emitted into the graph the
+// caller is capturing on s (a batch branch): the initial defect, a test kernel, then a while-node
+// whose body is one refinement step ending in mg_loop_check_kernel, then dst = (float) p64.  Every
+// replay re-runs the stopping rule of solve_tol on the current f, so the step count follows the
+// input.  A full-multigrid start puts the first step before the loop, as the single-grid loop graph
+// does.  *body_launches: kernels in one pass of the loop body.
+wp_status solve_mixed_loop_capture(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm, cudaStream_t s,
+                                   long long* body_launches) {
+    Level& L = h->lv[0];
+    const long n = L.cells;
+    const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
+    wp_status st;
+    if (!h->p64 || !h->r32 || !h->loop_state || !h->loop_cap) {
+        wp_set_error_msg("mixed solve: work arrays not prepared");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t cg = nullptr;
+    WP_CUDA_TRY(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, nullptr, nullptr));
+    if (cs != cudaStreamCaptureStatusActive) {
+        wp_set_error_msg("mixed solve loop: the stream is not capturing");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaGraphConditionalHandle hc;
+    WP_CUDA_TRY(cudaGraphConditionalHandleCreate(&hc, cg, 0, cudaGraphCondAssignDefault));
+    WP_CUDA_TRY(cudaMemsetAsync(h->acc + 2, 0, 2 * sizeof(double), s));
+    WP_KERNEL("active_sum", (double)n * 4.0 + frac_bytes(L), s, launch_active_sum(L, f, h->acc + 2, s));
+    WP_CUDA_TRY(cudaMemsetAsync(h->p64, 0, sizeof(double) * n, s));
+    if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, true, s)) != WP_OK) return st;
+    WP_KERNEL("mg_loop_init", 0.0, s,
+              mg_loop_init_kernel<<<1, 1, 0, s>>>((MgLoop*)h->loop_state, prm->max_cycles, prm->rel_tol > 0.0 ? 1 : 0,
+                                                  prm->rel_tol, inner_of(prm)));
+    if (prm->start == WP_START_FMG) {
+        if ((st = mixed_step(h, f, prm, true, hc, s)) != WP_OK) return st;
+    } else {
+        WP_KERNEL("mg_loop_start", 0.0, s,
+                  mg_loop_start_kernel<<<1, 1, 0, s>>>((MgLoop*)h->loop_state, (const double*)h->acc, hc));
+    }
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    WP_CUDA_TRY(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = hc;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn = nullptr;
+    WP_CUDA_TRY(cudaGraphAddNode(&cn, cg, deps, nd, &cp));
+    WP_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &cn, 1, cudaStreamSetCaptureDependencies));
+    // the body: one refinement step, captured on the handle's private stream into the node's graph
+    const long long c0 = wp_launch_count();
+    WP_CUDA_TRY(cudaStreamBeginCaptureToGraph(h->loop_cap, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+    st = mixed_step(h, f, prm, false, hc, h->loop_cap);
+    cudaGraph_t bout = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->loop_cap, &bout);
+    if (body_launches) *body_launches = wp_launch_count() - c0;
+    wp_add_launches(-(wp_launch_count() - c0));  // counted per pass when the batch reads its results
+    if (st != WP_OK) return st;
+    if (e != cudaSuccess) { wp_set_cuda_error(e, "mixed solve loop body capture", __FILE__, __LINE__); return WP_ERR_CUDA; }
+    h->last64 = 1;
+    WP_KERNEL("convert", 12.0 * n, s, convert_kernel<float, double><<<cb, 256, 0, s>>>(dst, h->p64, n));
     return WP_OK;
 }
 
@@ -4243,6 +4320,12 @@ wp_status wp_mg_solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float*
                                         cudaStream_t s) {
     return solve_mixed_fixed_async(h, dst, f, cycles, prm, s);
 }
+wp_status wp_mg_solve_mixed_loop_capture(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm,
+                                         cudaStream_t s, long long* body_launches) {
+    return solve_mixed_loop_capture(h, dst, f, prm, s, body_launches);
+}
+// the device loop's state (its first int is the V-cycle count of the last solve)
+const void* wp_mg_loop_state(const wp_mgfrac3d* h) { return h->loop_state; }
 wp_status wp_mg_solve_tol_internal(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm, wp_mg_report* r,
                                    cudaStream_t s) {
     return solve_tol(h, dst, nullptr, f, prm, r, s);
