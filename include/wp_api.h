@@ -354,23 +354,28 @@ CUWHHD_API wp_status wp_dst3d_destroy(wp_dst3d* h);
 /* ------------------------------------------------- sweep + DST potential recovery ------- */
 typedef struct wp_sweep3d wp_sweep3d;
 /* Replaces CuParallelSweep3D(int3 dim, DTYPE3 dx, char bc) (cuParallelSweep3D.cu:868-887), the
-   reference's comparison baseline for the wavelet recovery; bc 'n' (others: WP_ERR_UNSUPPORTED).
-   Owns the DST-I solver of the (n-1)^3 interior nodes. */
+   reference's comparison baseline for the wavelet recovery; bc 'n' or 'd' (others:
+   WP_ERR_UNSUPPORTED).  A bc 'n' handle owns the DST-I solver of the (n-1)^3 interior nodes. */
 CUWHHD_API wp_status wp_sweep3d_create(wp_sweep3d** h, int nx, int ny, int nz, double dx, double dy, double dz,
                                        char bc);
 /* Replaces CuParallelSweep3D::Solve(qx, qy, qz, xv, yv, zv) (cuParallelSweep3D.cu:939-966): a vector
    potential with curl q = u for a divergence-free u with no normal flux: qx, qy integrate yv, -xv
    along z from 0 on z = 0, qz = 0 except the top plane, which takes the x-integral of qx's top
-   plane (then cleared).  q in the edge shapes of wp_recover3d_run. */
+   plane (then cleared).  bc 'd' (SetQxQyBoundary, :925-937): qy's z = 0 plane is the x-integral of
+   zv's bottom face, no top-plane step (zv is read only then).  q in the edge shapes of
+   wp_recover3d_run. */
 CUWHHD_API wp_status wp_sweep3d_solve(wp_sweep3d* h, float* qx, float* qy, float* qz, const float* xv,
                                       const float* yv, const float* zv, void* stream);
 /* Replaces CuParallelSweep3D::Project(qx, qy, qz) with bc 'n' = ProjectZero
    (cuParallelSweep3D.cu:1043-1081, 1316-1326): q -= grad phi with -lap phi = -div q on the interior
-   nodes (DST-I), phi = 0 on the walls, in place. */
+   nodes (DST-I), phi = 0 on the walls, in place.  bc 'd' (ProjectD) returns WP_ERR_UNSUPPORTED: the
+   reference's run of it at 16^3 raised an illegal address, so it is not built. */
 CUWHHD_API wp_status wp_sweep3d_project(wp_sweep3d* h, float* qx, float* qy, float* qz, void* stream);
 CUWHHD_API wp_status wp_sweep3d_destroy(wp_sweep3d* h);
-/* Replaces CuParallelSweep3D(int2, DTYPE2, char)::Solve(qz, xv, yv) with bc 'n'
-   (cuParallelSweep3D.cu:987-1000): qz ((nx+1) x (ny+1)) = 0 on x = 0, -x-integral of yv. */
+/* Replaces CuParallelSweep3D(int2, DTYPE2, char)::Solve(qz, xv, yv) (cuParallelSweep3D.cu:986-998):
+   qz ((nx+1) x (ny+1)) = 0 on x = 0 (bc 'n') or, with bc 'd', the y-integral of xv's x = 0 column
+   there (from qz(0, 0) = 0, which the reference leaves as the caller's buffer had it), then the
+   -x-integral of yv. */
 CUWHHD_API wp_status wp_sweep2d_solve(float* qz, const float* xv, const float* yv, int nx, int ny, double dx,
                                       double dy, char bc, void* stream);
 

@@ -363,20 +363,28 @@ def dst3d_poisson(f, n, d):
 
 
 # ------------------------------------------------------------ sweep + DST recovery
-def sweep3d_solve(xv, yv, zv, n, d):
-    """CuParallelSweep3D::Solve with bc 'n' (cuParallelSweep3D.cu:939-966): qz = 0; qx, qy start from
-    0 on the z = 0 plane and integrate yv (+dz) and xv (-dz) along z (SweepingQx / SweepingQy,
-    :28-66); then the top plane is made tangential-free: qp = the x-integral of qx's top plane
-    (cuSweepingQ_x, :9-26), qx and qy top planes cleared, qz's top plane gets -qp / dz (CudaMatAdd,
-    cudaMath.cu:110-118).  FP64 sums in the reference's sequential order."""
+def sweep3d_solve(xv, yv, zv, n, d, bc="n"):
+    """CuParallelSweep3D::Solve (cuParallelSweep3D.cu:939-966): qz = 0; qx, qy start from their z = 0
+    plane and integrate yv (+dz) and xv (-dz) along z (SweepingQx / SweepingQy, :28-66).  bc 'n': the
+    z = 0 planes are 0 and the top plane is then made tangential-free: qp = the x-integral of qx's top
+    plane (cuSweepingQ_x, :9-26), qx and qy top planes cleared, qz's top plane gets -qp / dz
+    (CudaMatAdd, cudaMath.cu:110-118).  bc 'd' (SetQxQyBoundary, :925-937): qx's z = 0 plane is 0 and
+    qy's is the x-integral of zv's bottom face (SweepingQy_x, :68-85), with no top-plane step.  FP64
+    sums in the reference's sequential order."""
     nx, ny, nz = n
     dx, dy, dz = d
     xv, yv = _f64(xv), _f64(yv)
     s = mac_shapes3d(nx, ny, nz)
     qx, qy, qz = (np.zeros(s[k]) for k in ("qx", "qy", "qz"))
+    if bc == "d":
+        zv = _f64(zv)
+        for x in range(1, nx + 1):
+            qy[0, x] = qy[0, x - 1] + zv[0, x - 1] * dx
     for z in range(1, nz + 1):
         qx[z] = qx[z - 1] + yv[z - 1] * dz
         qy[z] = qy[z - 1] - xv[z - 1] * dz
+    if bc == "d":
+        return qx, qy, qz
     qp = np.zeros((nx + 1, ny + 1))
     for x in range(1, nx + 1):
         qp[x] = qp[x - 1] + qx[nz, x - 1] * dx
@@ -413,12 +421,18 @@ def sweep3d_project(qx, qy, qz, n, d):
     return qx, qy, qz
 
 
-def sweep2d_solve(yv, n, d):
-    """CuParallelSweep3D::Solve(qz, xv, yv) with bc 'n' (cuParallelSweep3D.cu:987-1000,
-    SweepingQz_x_0 :106-124): qz = 0 on x = 0, qz[x] = qz[x-1] - yv[x-1] dx."""
+def sweep2d_solve(yv, n, d, bc="n", xv=None):
+    """CuParallelSweep3D::Solve(qz, xv, yv) (cuParallelSweep3D.cu:986-998): bc 'n' (SweepingQz_x_0,
+    :106-124): qz = 0 on x = 0, qz[x] = qz[x-1] - yv[x-1] dx.  bc 'd' (SweepingQz_y, :126-143, then
+    SweepingQz_x, :87-104): the x = 0 column is the y-integral of xv's x = 0 column from qz(0, 0) =
+    0 (the reference leaves that entry as the caller's buffer had it), then the same x-integral."""
     nx, ny = n
     yv = _f64(yv)
     qz = np.zeros((nx + 1, ny + 1))
+    if bc == "d":
+        xv = _f64(xv)
+        for y in range(1, ny + 1):
+            qz[0, y] = qz[0, y - 1] + xv[0, y - 1] * d[1]
     for x in range(1, nx + 1):
         qz[x] = qz[x - 1] - yv[x - 1] * d[0]
     return qz

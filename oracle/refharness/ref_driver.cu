@@ -376,8 +376,12 @@ int main(int argc, char** argv) {
         dst.Solve(p, f);
         checkCudaErrors(cudaDeviceSynchronize());
         write_bin("p", from_dev(p, nc));
-    } else if (op == "psweep3d") {  // n dx: CuParallelSweep3D(dim, dx, 'n') Solve, then Project
-        // (TestLocalProjection.cpp:719-721); equal extents only (its CuDst3D on the (n-1)^3 nodes)
+    } else if (op == "psweep3d") {  // n dx [bc [solve_only]]: CuParallelSweep3D(dim, dx, bc) Solve, then Project
+        // (TestLocalProjection.cpp:719-721); equal extents only (its CuDst3D on the (n-1)^3 nodes).  With
+        // solve_only = 1 Project is not called (its bc 'd' branch, ProjectD, raised an illegal address
+        // at 16^3 and is not run)
+        const char wall = argc > 6 ? argv[6][0] : 'n';
+        const bool solve_only = argc > 7 && atoi(argv[7]) != 0;
         int n = I(0);
         int3 dim = make_int3(n, n, n);
         DTYPE h = (DTYPE)D(1);
@@ -387,25 +391,27 @@ int main(int argc, char** argv) {
         DTYPE* yv = to_dev(read_bin("yv", sf));
         DTYPE* zv = to_dev(read_bin("zv", sf));
         DTYPE *qx = dev_zeros(sq), *qy = dev_zeros(sq), *qz = dev_zeros(sq);
-        CuParallelSweep3D cups(dim, dx, 'n');
+        CuParallelSweep3D cups(dim, dx, wall);
         cups.Solve(qx, qy, qz, xv, yv, zv);
         checkCudaErrors(cudaDeviceSynchronize());
         write_bin("qx_solve", from_dev(qx, sq));
         write_bin("qy_solve", from_dev(qy, sq));
         write_bin("qz_solve", from_dev(qz, sq));
+        if (solve_only) return 0;
         cups.Project(qx, qy, qz);
         checkCudaErrors(cudaDeviceSynchronize());
         write_bin("qx", from_dev(qx, sq));
         write_bin("qy", from_dev(qy, sq));
         write_bin("qz", from_dev(qz, sq));
-    } else if (op == "psweep2d") {  // n dx: CuParallelSweep3D(int2 dim, DTYPE2 dx, 'n').Solve(qz, xv, yv)
+    } else if (op == "psweep2d") {  // n dx [bc]: CuParallelSweep3D(int2 dim, DTYPE2 dx, bc).Solve(qz, xv, yv)
+        const char wall = argc > 6 ? argv[6][0] : 'n';
         int n = I(0);
         DTYPE h = (DTYPE)D(1);
         size_t sf = (size_t)(n + 1) * n, sq = (size_t)(n + 1) * (n + 1);
         DTYPE* xv = to_dev(read_bin("xv", sf));
         DTYPE* yv = to_dev(read_bin("yv", sf));
         DTYPE* qz = dev_zeros(sq);
-        CuParallelSweep3D cups(make_int2(n, n), make_DTYPE2(h, h), 'n');
+        CuParallelSweep3D cups(make_int2(n, n), make_DTYPE2(h, h), wall);
         cups.Solve(qz, xv, yv);
         checkCudaErrors(cudaDeviceSynchronize());
         write_bin("qz", from_dev(qz, sq));

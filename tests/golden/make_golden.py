@@ -16,6 +16,7 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only short   # CDF2.0 / CDF1.1 / CDF1.7 transforms
     python tests/golden/make_golden.py --only domd2d  # 2D projection and recovery with Dirichlet walls
     python tests/golden/make_golden.py --only narrow  # CuFastSweeping::ParticlesToLsNarrow
+    python tests/golden/make_golden.py --only psweep_d  # CuParallelSweep3D with bc 'd'
     ... [--out DIR]                                   # write the .npz files to DIR instead of here
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
@@ -338,6 +339,33 @@ def psweep_cases(rng):
     save("psweep", **out)
 
 
+def psweep_d_cases(rng):
+    """CuParallelSweep3D with bc 'd': Solve alone (the z = 0 plane of qy from the x-integral of zv's
+    bottom face, no top-plane step) on fields with wall flux, at 8^3 and 16^3; and the 2D Solve with
+    bc 'd' (a y-integral of xv along x = 0, then the x-integral of yv) on a 32^2 field.  Project is
+    not called: its bc 'd' branch (ProjectD) raised an illegal address at 16^3 in the first run of
+    this recipe, so it is not run again."""
+    from waveletpotentials_b200 import fields
+    out = {}
+    for n in (8, 16):
+        h = 1.0 / n
+        s = shapes3((n, n, n))
+        qx, qy, qz = (rng.standard_normal(s[k]) for k in ("qx", "qy", "qz"))
+        xv, yv, zv = fields.curl3d(qx, qy, qz, (n, n, n), (h, h, h))
+        res = run("psweep3d", {"xv": xv, "yv": yv, "zv": zv}, [n, h, "d", 1],
+                  {"qx_solve": s["qx"], "qy_solve": s["qy"], "qz_solve": s["qz"]})
+        out[f"xv_{n}"], out[f"yv_{n}"], out[f"zv_{n}"] = xv, yv, zv
+        for k, v in res.items():
+            out[f"{k}_{n}"] = v
+    n = 32
+    h = 1.0 / n
+    psi = rng.standard_normal((n + 1, n + 1))
+    xv2, yv2 = fields.curl2d(psi, (n, n), (h, h))
+    out["qz2d"] = run("psweep2d", {"xv": xv2, "yv": yv2}, [n, h, "d"], {"qz": (n + 1, n + 1)})["qz"]
+    out["xv2d"], out["yv2d"] = xv2, yv2
+    save("psweep_d", **out)
+
+
 def domd_cases(rng):
     """CuDivLocalProject3D::ProjectLocal_q_ccc with the walls' boundary type 'd' (the base wavelet's bc
     proj_bc('d') = 'n', so cuProjectLocal_q_3d_nq_ccc runs) on random coefficients, and
@@ -422,6 +450,9 @@ def main():
         return
     if only == "short":
         short_cases(np.random.default_rng(20261213))
+        return
+    if only == "psweep_d":
+        psweep_d_cases(np.random.default_rng(20261216))
         return
     if only == "narrow":
         narrow_cases(np.random.default_rng(20261215))

@@ -72,7 +72,11 @@ def test_sweep2d_matches_oracle(wp, oracle, n):
 
 def test_sweep_rejects_other_boundaries(wp):
     with pytest.raises(wp.WPError):
-        wp.CuParallelSweep3D((8, 8, 8), 1.0 / 8, "d")
+        wp.CuParallelSweep3D((8, 8, 8), 1.0 / 8, "z")
+    qz = torch.zeros((9, 9), device="cuda")
+    yv = torch.zeros(wp.mac_shapes2d(8, 8)["yv"], device="cuda")
+    with pytest.raises(wp.WPError):
+        wp.CuParallelSweep3D.Solve2D(qz, None, yv, (8, 8), 1.0 / 8, bc="d")  # bc 'd' reads xv
 
 
 @pytest.mark.parametrize("tag", ["15", "8"])
@@ -126,5 +130,29 @@ def test_sweep2d_matches_reference(wp):
     n = 32
     qz = torch.zeros((n + 1, n + 1), device="cuda")
     wp.CuParallelSweep3D.Solve2D(qz, _t(g["xv2d"]), _t(g["yv2d"]), (n, n), 1.0 / n)
+    torch.cuda.synchronize()
+    assert _rel(g["qz2d"], qz.cpu().numpy()) < 2e-6
+
+
+@pytest.mark.parametrize("n", [8, 16])
+def test_sweep_solve_with_dirichlet_walls_matches_reference(wp, n):
+    """bc 'd': CuParallelSweep3D::Solve (qy's z = 0 plane from zv's bottom face) and the 2D Solve
+    against the reference build; Project, the reference's ProjectD, is refused (not built)."""
+    from conftest import load_golden
+    g = load_golden("psweep_d")
+    h = 1.0 / n
+    u = [_t(g[f"{k}_{n}"]) for k in ("xv", "yv", "zv")]
+    s = wp.mac_shapes3d(n, n, n)
+    q = [torch.full(s[k], 7.0, device="cuda") for k in ("qx", "qy", "qz")]
+    sw = wp.CuParallelSweep3D((n, n, n), h, "d")
+    sw.Solve(*q, *u)
+    torch.cuda.synchronize()
+    for t, k in zip(q, ("qx", "qy", "qz")):
+        assert _rel(g[f"{k}_solve_{n}"], t.cpu().numpy()) < 2e-6, k
+    with pytest.raises(wp.WPError):
+        sw.Project(*q)
+    sw.close()
+    qz = torch.full((33, 33), 7.0, device="cuda")
+    wp.CuParallelSweep3D.Solve2D(qz, _t(g["xv2d"]), _t(g["yv2d"]), (32, 32), 1.0 / 32, bc="d")
     torch.cuda.synchronize()
     assert _rel(g["qz2d"], qz.cpu().numpy()) < 2e-6

@@ -235,6 +235,20 @@ def test_sweep2d_matches_reference(oracle):
     assert np.abs(qz - g["qz2d"]).max() <= 1e-14 * np.abs(g["qz2d"]).max()
 
 
+@pytest.mark.parametrize("n", [8, 16])
+def test_sweep_solve_with_dirichlet_walls_matches_reference(oracle, n):
+    """CuParallelSweep3D::Solve with bc 'd' (qy's z = 0 plane from the x-integral of zv's bottom face,
+    no top-plane step) on a field with wall flux, and the 2D Solve with bc 'd': exact sequential sums."""
+    g = load_golden("psweep_d")
+    h = 1.0 / n
+    qs = oracle.sweep3d_solve(*[g[f"{k}_{n}"] for k in ("xv", "yv", "zv")], (n, n, n), (h, h, h), bc="d")
+    for a, k in zip(qs, ("qx", "qy", "qz")):
+        ref = g[f"{k}_solve_{n}"]
+        assert np.abs(a - ref).max() <= 1e-14 * max(np.abs(ref).max(), 1e-300), k
+    qz = oracle.sweep2d_solve(g["yv2d"], (32, 32), (1 / 32, 1 / 32), bc="d", xv=g["xv2d"])
+    assert np.abs(qz - g["qz2d"]).max() <= 1e-14 * np.abs(g["qz2d"]).max()
+
+
 @pytest.mark.parametrize("tag", ["p16x8x32", "p8", "r16", "r8x16x32"])
 def test_domain_d_projection_and_recovery_match_reference(oracle, tag):
     """Dirichlet domain walls: CuDivLocalProject3D::ProjectLocal_q_ccc with bc_base 'n'

@@ -5,10 +5,15 @@
 // integrate yv (+dz) and xv (-dz) along z (SweepingQx / SweepingQy, :28-66); the top plane is then
 // made tangential-free: qp = the x-integral of qx's top plane (cuSweepingQ_x, :9-26), the top planes
 // of qx and qy are cleared and qz's top plane gets -qp / dz (CudaMatAdd, cudaMath.cu:110-118).
+// Solve with bc 'd' (SetQxQyBoundary, :925-937): qx's z = 0 plane is 0, qy's is the x-integral of
+// zv's bottom face (SweepingQy_x, :68-85); the same z integrals; no top-plane step.
 // Project (bc 'n' -> ProjectZero, :1043-1081): b = -div q on the (n-1)^3 interior nodes
 // (cuGetB_q_zero_3d, cuConvergence.cu:126-159), the DST-I Poisson solve, and q -= grad phi with
 // phi = 0 on the boundary nodes (cuGradientMinus3D_zero_Q, cuGradient.cu:2353-2405, with its spacing
-// for the three wall edges).  2D Solve (SweepingQz_x_0, :106-124): qz = -x-integral of yv.
+// for the three wall edges).  Project with bc 'd' (ProjectD, :1084-1098) is not built: the reference's
+// run of it at 16^3 raised an illegal address.  2D Solve (SweepingQz_x_0, :106-124): qz =
+// -x-integral of yv; with bc 'd' (SweepingQz_y then SweepingQz_x, :87-143) the x = 0 column is first
+// the y-integral of xv's x = 0 column.
 //
 // B200 design: the z integrals are column scans, HBM bound (one read of u, one write of q).  A CTA
 // takes 32 consecutive y columns (128-byte rows) and splits z into 8 chunks over its 8 warps: chunk
@@ -134,7 +139,7 @@ extern "C" CUWHHD_API wp_status wp_sweep3d_create(wp_sweep3d** out, int nx, int 
                                                   double dz, char bc) {
     if (!out) { wp_set_error_msg("wp_sweep3d_create: null handle"); return WP_ERR_INVALID_ARG; }
     *out = nullptr;
-    if (bc != 'n') { wp_set_error_msg("wp_sweep3d_create: only bc 'n' is supported"); return WP_ERR_UNSUPPORTED; }
+    if (bc != 'n' && bc != 'd') { wp_set_error_msg("wp_sweep3d_create: bc must be 'n' or 'd'"); return WP_ERR_UNSUPPORTED; }
     if (nx < 2 || ny < 2 || nz < 2 || !(dx > 0) || !(dy > 0) || !(dz > 0)) {
         wp_set_error_msg("wp_sweep3d_create: extents must be >= 2 and spacings > 0");
         return WP_ERR_INVALID_ARG;
@@ -144,8 +149,9 @@ extern "C" CUWHHD_API wp_status wp_sweep3d_create(wp_sweep3d** out, int nx, int 
     h->n[0] = nx; h->n[1] = ny; h->n[2] = nz;
     h->h[0] = dx; h->h[1] = dy; h->h[2] = dz;
     h->bc = bc;
-    wp_status st = wp_dst3d_create(&h->dst, nx - 1, ny - 1, nz - 1, dx, dy, dz);
-    if (st == WP_OK) {
+    // the DST-I gauge projection is the bc 'n' Project's (ProjectZero); bc 'd' handles only solve
+    wp_status st = bc == 'n' ? wp_dst3d_create(&h->dst, nx - 1, ny - 1, nz - 1, dx, dy, dz) : WP_OK;
+    if (st == WP_OK && bc == 'n') {
         const cudaError_t e = cudaMalloc((void**)&h->phi, sizeof(double) * (size_t)(nx - 1) * (ny - 1) * (nz - 1));
         if (e != cudaSuccess) { wp_set_cuda_error(e, "sweep3d create", __FILE__, __LINE__); st = WP_ERR_CUDA; }
     }
@@ -156,20 +162,29 @@ extern "C" CUWHHD_API wp_status wp_sweep3d_create(wp_sweep3d** out, int nx, int 
 
 extern "C" CUWHHD_API wp_status wp_sweep3d_solve(wp_sweep3d* h, float* qx, float* qy, float* qz, const float* xv,
                                                  const float* yv, const float* zv, void* stream) {
-    if (!h || !qx || !qy || !qz || !xv || !yv) { wp_set_error_msg("wp_sweep3d_solve: null pointer"); return WP_ERR_INVALID_ARG; }
-    (void)zv;  // with bc 'n' the z = 0 planes of qx and qy are 0 (the 'd' boundary would sweep zv there)
+    if (!h || !qx || !qy || !qz || !xv || !yv || (h->bc == 'd' && !zv)) {
+        wp_set_error_msg("wp_sweep3d_solve: null pointer");
+        return WP_ERR_INVALID_ARG;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
     const long sqx = (long)nx * (ny + 1), sqy = (long)(nx + 1) * ny, nqz = (long)(nx + 1) * (ny + 1) * nz;
     WP_CUDA_TRY(cudaMemsetAsync(qz, 0, sizeof(float) * nqz, s));
     WP_CUDA_TRY(cudaMemsetAsync(qx, 0, sizeof(float) * sqx, s));
     WP_CUDA_TRY(cudaMemsetAsync(qy, 0, sizeof(float) * sqy, s));
+    if (h->bc == 'd') {
+        // qy's z = 0 plane ((nx+1) rows of ny): row 0 stays 0, row x = x-integral of zv's bottom face
+        WP_KERNEL("sweep_x", 8.0 * nx * ny, s,
+                  sweep_scan_kernel<<<dim3(wp_cdiv(ny, 32), 1), dim3(32, kChunks), 0, s>>>(qy, zv, 1, ny, nx,
+                                                                                         (float)h->h[0]));
+    }
     const float dz = (float)h->h[2];
     WP_KERNEL("sweep_z", 8.0 * sqx * nz, s,
               sweep_scan_kernel<<<dim3(wp_cdiv(ny + 1, 32), nx), dim3(32, kChunks), 0, s>>>(qx, yv, nx, ny + 1, nz, dz));
     WP_KERNEL("sweep_z", 8.0 * sqy * nz, s,
               sweep_scan_kernel<<<dim3(wp_cdiv(ny, 32), nx + 1), dim3(32, kChunks), 0, s>>>(qy, xv, nx + 1, ny, nz,
                                                                                           -dz));
+    if (h->bc == 'd') return WP_OK;
     // bc 'n': qp from qx's top plane into qz's top plane, then the top planes of qx and qy cleared
     WP_KERNEL("sweep_top", 12.0 * (nx + 1) * (ny + 1), s,
               sweep_top_kernel<<<wp_cdiv((long)(ny + 1) * 32, 256), 256, 0, s>>>(qx, qz, nx, ny, nz, (float)h->h[0],
@@ -181,6 +196,10 @@ extern "C" CUWHHD_API wp_status wp_sweep3d_solve(wp_sweep3d* h, float* qx, float
 
 extern "C" CUWHHD_API wp_status wp_sweep3d_project(wp_sweep3d* h, float* qx, float* qy, float* qz, void* stream) {
     if (!h || !qx || !qy || !qz) { wp_set_error_msg("wp_sweep3d_project: null pointer"); return WP_ERR_INVALID_ARG; }
+    if (h->bc != 'n') {
+        wp_set_error_msg("wp_sweep3d_project: bc 'd' (the reference's ProjectD) is not built");
+        return WP_ERR_UNSUPPORTED;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
     const float dxi = (float)(1.0 / h->h[0]), dyi = (float)(1.0 / h->h[1]), dzi = (float)(1.0 / h->h[2]);
@@ -205,13 +224,20 @@ extern "C" CUWHHD_API wp_status wp_sweep3d_destroy(wp_sweep3d* h) {
 
 extern "C" CUWHHD_API wp_status wp_sweep2d_solve(float* qz, const float* xv, const float* yv, int nx, int ny, double dx,
                                                  double dy, char bc, void* stream) {
-    (void)xv;
-    (void)dy;
-    if (!qz || !yv || nx < 1 || ny < 1 || !(dx > 0)) { wp_set_error_msg("wp_sweep2d_solve: bad arguments"); return WP_ERR_INVALID_ARG; }
-    if (bc != 'n') { wp_set_error_msg("wp_sweep2d_solve: only bc 'n' is supported"); return WP_ERR_UNSUPPORTED; }
+    if (!qz || !yv || nx < 1 || ny < 1 || !(dx > 0) || (bc == 'd' && (!xv || !(dy > 0)))) {
+        wp_set_error_msg("wp_sweep2d_solve: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (bc != 'n' && bc != 'd') { wp_set_error_msg("wp_sweep2d_solve: bc must be 'n' or 'd'"); return WP_ERR_UNSUPPORTED; }
     cudaStream_t s = (cudaStream_t)stream;
     // qz (nx+1) x (ny+1): x is the outer index, so the x integral is a scan over "planes" of ny+1 rows
     WP_CUDA_TRY(cudaMemsetAsync(qz, 0, sizeof(float) * (ny + 1), s));
+    if (bc == 'd') {
+        // the x = 0 column: qz(0, y) = qz(0, y - 1) + xv(0, y - 1) dy from qz(0, 0) = 0 (a scan over ny
+        // "planes" of one entry)
+        WP_KERNEL("sweep_y2d", 8.0 * ny, s,
+                  sweep_scan_kernel<<<dim3(1, 1), dim3(32, kChunks), 0, s>>>(qz, xv, 1, 1, ny, (float)dy));
+    }
     WP_KERNEL("sweep_x2d", 8.0 * (double)nx * (ny + 1), s,
               sweep_scan_kernel<<<dim3(wp_cdiv(ny + 1, 32), 1), dim3(32, kChunks), 0, s>>>(qz, yv, 1, ny + 1, nx,
                                                                                          -(float)dx));
