@@ -366,6 +366,13 @@ CUWHHD_API wp_status wp_sweep3d_create(wp_sweep3d** h, int nx, int ny, int nz, d
    wp_recover3d_run. */
 CUWHHD_API wp_status wp_sweep3d_solve(wp_sweep3d* h, float* qx, float* qy, float* qz, const float* xv,
                                       const float* yv, const float* zv, void* stream);
+/* Replaces CuParallelSweep3D::SolveFromMid(qx, qy, qz, xv, yv, zv, int3 mid) (cuParallelSweep3D.cu:967-984):
+   qz = 0, qx's plane mid_z = 0, qy's plane mid_z the x-integral of zv's plane mid_z both ways from 0
+   at row mid_x (the reference leaves that row as the caller's buffer had it), then the z integrals of
+   Solve both ways from plane mid_z.  mid_y is unused (as in the reference). */
+CUWHHD_API wp_status wp_sweep3d_solve_from_mid(wp_sweep3d* h, float* qx, float* qy, float* qz, const float* xv,
+                                               const float* yv, const float* zv, int mid_x, int mid_y, int mid_z,
+                                               void* stream);
 /* Replaces CuParallelSweep3D::Project(qx, qy, qz) with bc 'n' = ProjectZero
    (cuParallelSweep3D.cu:1043-1081, 1316-1326): q -= grad phi with -lap phi = -div q on the interior
    nodes (DST-I), phi = 0 on the walls, in place.  bc 'd' (ProjectD) returns WP_ERR_UNSUPPORTED: the

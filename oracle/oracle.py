@@ -394,6 +394,31 @@ def sweep3d_solve(xv, yv, zv, n, d, bc="n"):
     return qx, qy, qz
 
 
+def sweep3d_solve_from_mid(xv, yv, zv, n, d, mid):
+    """CuParallelSweep3D::SolveFromMid (cuParallelSweep3D.cu:967-984; SweepingQy_x_mid, SweepingQx_mid,
+    SweepingQy_mid, :145-214): qz = 0; qx's plane mid.z is 0; qy's plane mid.z is the x-integral of
+    zv's plane mid.z both ways from 0 at x = mid.x (the reference leaves that row as the caller's
+    buffer had it); then qx, qy integrate yv (+dz), xv (-dz) along z both ways from plane mid.z.
+    mid.y is not used.  FP64 sums in the reference's sequential order."""
+    nx, ny, nz = n
+    dx, dy, dz = d
+    mx, _, mz = mid
+    xv, yv, zv = _f64(xv), _f64(yv), _f64(zv)
+    s = mac_shapes3d(nx, ny, nz)
+    qx, qy, qz = (np.zeros(s[k]) for k in ("qx", "qy", "qz"))
+    for x in range(mx - 1, -1, -1):
+        qy[mz, x] = qy[mz, x + 1] - zv[mz, x] * dx
+    for x in range(mx + 1, nx + 1):
+        qy[mz, x] = qy[mz, x - 1] + zv[mz, x - 1] * dx
+    for z in range(mz - 1, -1, -1):
+        qx[z] = qx[z + 1] - yv[z] * dz
+        qy[z] = qy[z + 1] + xv[z] * dz
+    for z in range(mz + 1, nz + 1):
+        qx[z] = qx[z - 1] + yv[z - 1] * dz
+        qy[z] = qy[z - 1] - xv[z - 1] * dz
+    return qx, qy, qz
+
+
 def sweep3d_project(qx, qy, qz, n, d):
     """CuParallelSweep3D::ProjectZero (cuParallelSweep3D.cu:1043-1081): b = -div q on the (n-1)^3
     interior nodes (cuGetB_q_zero_3d, cuConvergence.cu:126-159), the DST-I Poisson solve on them,

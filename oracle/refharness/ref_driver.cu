@@ -403,6 +403,24 @@ int main(int argc, char** argv) {
         write_bin("qx", from_dev(qx, sq));
         write_bin("qy", from_dev(qy, sq));
         write_bin("qz", from_dev(qz, sq));
+    } else if (op == "psweep3d_mid") {  // n dx mx my mz: CuParallelSweep3D(dim, dx, 'n').SolveFromMid(..., mid)
+        int n = I(0);
+        int3 dim = make_int3(n, n, n);
+        DTYPE h = (DTYPE)D(1);
+        DTYPE3 dx = make_DTYPE3(h, h, h);
+        int3 mid = make_int3(I(2), I(3), I(4));
+        size_t sf = (size_t)(n + 1) * n * n, sq = (size_t)n * (n + 1) * (n + 1);
+        DTYPE* xv = to_dev(read_bin("xv", sf));
+        DTYPE* yv = to_dev(read_bin("yv", sf));
+        DTYPE* zv = to_dev(read_bin("zv", sf));
+        DTYPE *qx = dev_zeros(sq), *qy = dev_zeros(sq), *qz = dev_zeros(sq);
+        CuParallelSweep3D cups(dim, dx, 'n');
+        cups.SolveFromMid(qx, qy, qz, xv, yv, zv, mid);
+        checkCudaErrors(cudaGetLastError());
+        checkCudaErrors(cudaDeviceSynchronize());
+        write_bin("qx", from_dev(qx, sq));
+        write_bin("qy", from_dev(qy, sq));
+        write_bin("qz", from_dev(qz, sq));
     } else if (op == "psweep2d") {  // n dx [bc]: CuParallelSweep3D(int2 dim, DTYPE2 dx, bc).Solve(qz, xv, yv)
         const char wall = argc > 6 ? argv[6][0] : 'n';
         int n = I(0);

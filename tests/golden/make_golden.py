@@ -17,6 +17,7 @@ unmodified reference sources (FP64, the reference default):
     python tests/golden/make_golden.py --only domd2d  # 2D projection and recovery with Dirichlet walls
     python tests/golden/make_golden.py --only narrow  # CuFastSweeping::ParticlesToLsNarrow
     python tests/golden/make_golden.py --only psweep_d  # CuParallelSweep3D with bc 'd'
+    python tests/golden/make_golden.py --only psweep_mid  # CuParallelSweep3D::SolveFromMid
     ... [--out DIR]                                   # write the .npz files to DIR instead of here
 
 Every case draws seeded inputs with numpy, runs the reference entry point through ref_driver
@@ -366,6 +367,24 @@ def psweep_d_cases(rng):
     save("psweep_d", **out)
 
 
+def psweep_mid_cases(rng):
+    """CuParallelSweep3D::SolveFromMid (cuParallelSweep3D.cu:967-984): the z integrals of qx, qy run
+    both ways from the plane mid.z, whose qy is the x-integral of zv both ways from mid.x; at 8^3 and
+    16^3 with interior and zero mid indices, on fields with wall flux."""
+    from waveletpotentials_b200 import fields
+    out = {}
+    for tag, n, mid in (("a8", 8, (4, 2, 3)), ("b16", 16, (7, 8, 11)), ("c8", 8, (0, 0, 0))):
+        h = 1.0 / n
+        s = shapes3((n, n, n))
+        qx, qy, qz = (rng.standard_normal(s[k]) for k in ("qx", "qy", "qz"))
+        xv, yv, zv = fields.curl3d(qx, qy, qz, (n, n, n), (h, h, h))
+        res = run("psweep3d_mid", {"xv": xv, "yv": yv, "zv": zv}, [n, h, *mid],
+                  {"qx": s["qx"], "qy": s["qy"], "qz": s["qz"]})
+        out.update({f"{tag}_{k}": v for k, v in dict(xv=xv, yv=yv, zv=zv, **res).items()})
+        out[f"{tag}_meta"] = np.array([n, *mid])
+    save("psweep_mid", **out)
+
+
 def domd_cases(rng):
     """CuDivLocalProject3D::ProjectLocal_q_ccc with the walls' boundary type 'd' (the base wavelet's bc
     proj_bc('d') = 'n', so cuProjectLocal_q_3d_nq_ccc runs) on random coefficients, and
@@ -450,6 +469,9 @@ def main():
         return
     if only == "short":
         short_cases(np.random.default_rng(20261213))
+        return
+    if only == "psweep_mid":
+        psweep_mid_cases(np.random.default_rng(20261217))
         return
     if only == "psweep_d":
         psweep_d_cases(np.random.default_rng(20261216))

@@ -249,6 +249,19 @@ def test_sweep_solve_with_dirichlet_walls_matches_reference(oracle, n):
     assert np.abs(qz - g["qz2d"]).max() <= 1e-14 * np.abs(g["qz2d"]).max()
 
 
+@pytest.mark.parametrize("tag", ["a8", "b16", "c8"])
+def test_sweep_solve_from_mid_matches_reference(oracle, tag):
+    """CuParallelSweep3D::SolveFromMid from interior and zero mid indices: exact sequential sums."""
+    g = load_golden("psweep_mid")
+    n, mx, my, mz = (int(v) for v in g[tag + "_meta"])
+    h = 1.0 / n
+    q = oracle.sweep3d_solve_from_mid(*[g[f"{tag}_{k}"] for k in ("xv", "yv", "zv")], (n, n, n), (h, h, h),
+                                      (mx, my, mz))
+    for a, k in zip(q, ("qx", "qy", "qz")):
+        ref = g[f"{tag}_{k}"]
+        assert np.abs(a - ref).max() <= 1e-14 * max(np.abs(ref).max(), 1.0), k
+
+
 @pytest.mark.parametrize("tag", ["p16x8x32", "p8", "r16", "r8x16x32"])
 def test_domain_d_projection_and_recovery_match_reference(oracle, tag):
     """Dirichlet domain walls: CuDivLocalProject3D::ProjectLocal_q_ccc with bc_base 'n'

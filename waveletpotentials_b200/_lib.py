@@ -109,6 +109,7 @@ SIGNATURES = {
     "wp_dst3d_solve_noalloc": (I, [P, P, I, I, I, D, D, D, P]),
     "wp_sweep3d_create": (I, [PP, I, I, I, D, D, D, C]),
     "wp_sweep3d_solve": (I, [P, P, P, P, P, P, P, P]),
+    "wp_sweep3d_solve_from_mid": (I, [P, P, P, P, P, P, P, I, I, I, P]),
     "wp_sweep3d_project": (I, [P, P, P, P, P]),
     "wp_sweep3d_destroy": (I, [P]),
     "wp_sweep2d_solve": (I, [P, P, P, I, I, D, D, C, P]),

@@ -579,6 +579,15 @@ class CuParallelSweep3D:
                                      _ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]), _stream(stream)),
               "wp_sweep3d_solve")
 
+    def SolveFromMid(self, qx, qy, qz, xv, yv, zv, mid, stream=None):
+        """CuParallelSweep3D::SolveFromMid: the integrals run both ways from plane mid[2] (and row
+        mid[0] of qy's plane there); mid[1] is unused."""
+        s = self.shapes
+        mx, my, mz = (int(v) for v in mid)
+        check(lib().wp_sweep3d_solve_from_mid(self._h, _ptr(qx, s["qx"]), _ptr(qy, s["qy"]), _ptr(qz, s["qz"]),
+                                              _ptr(xv, s["xv"]), _ptr(yv, s["yv"]), _ptr(zv, s["zv"]), mx, my, mz,
+                                              _stream(stream)), "wp_sweep3d_solve_from_mid")
+
     def Project(self, qx, qy, qz, stream=None):
         s = self.shapes
         check(lib().wp_sweep3d_project(self._h, _ptr(qx, s["qx"]), _ptr(qy, s["qy"]), _ptr(qz, s["qz"]),

@@ -29,28 +29,31 @@ namespace {
 
 constexpr int kChunks = 8;
 
-// out[col + z slice] for z = 1 .. nzin: out[col] (plane 0, kept) + s * sum of in[col + z' slice], z' < z
+// out[col + z so] for z = 1 .. nzin: out[col] (plane 0, kept) + s * sum of in[col + z' si], z' < z.
+// so = si = ncx ncy (0: that default) scans upward; negative strides scan downward from the base plane.
 __global__ void __launch_bounds__(256) sweep_scan_kernel(float* __restrict__ out, const float* __restrict__ in,
-                                                         int ncx, int ncy, int nzin, float s) {
+                                                         int ncx, int ncy, int nzin, float s, long so = 0,
+                                                         long si = 0) {
     __shared__ float part[kChunks][32];
     const int c = threadIdx.x, k = threadIdx.y;
     const int y = blockIdx.x * 32 + c, x = blockIdx.y;
     const bool ok = y < ncy && x < ncx;
-    const long slice = (long)ncx * ncy;
+    if (so == 0) so = (long)ncx * ncy;
+    if (si == 0) si = (long)ncx * ncy;
     const long col = y + (long)x * ncy;
     const int cz = (nzin + kChunks - 1) / kChunks;
     const int z0 = min(k * cz, nzin), z1 = min(z0 + cz, nzin);
     float loc = 0.f;
     if (ok)
-        for (int z = z0; z < z1; ++z) loc += in[col + z * slice] * s;
+        for (int z = z0; z < z1; ++z) loc += in[col + z * si] * s;
     part[k][c] = loc;
     __syncthreads();
     if (ok) {
         float run = out[col];
         for (int j = 0; j < k; ++j) run += part[j][c];
         for (int z = z0; z < z1; ++z) {
-            run += in[col + z * slice] * s;
-            out[col + (z + 1) * slice] = run;
+            run += in[col + z * si] * s;
+            out[col + (z + 1) * so] = run;
         }
     }
 }
@@ -191,6 +194,62 @@ extern "C" CUWHHD_API wp_status wp_sweep3d_solve(wp_sweep3d* h, float* qx, float
                                                                                -1.f / dz));
     WP_CUDA_TRY(cudaMemsetAsync(qx + sqx * nz, 0, sizeof(float) * sqx, s));
     WP_CUDA_TRY(cudaMemsetAsync(qy + sqy * nz, 0, sizeof(float) * sqy, s));
+    return WP_OK;
+}
+
+// CuParallelSweep3D::SolveFromMid (cuParallelSweep3D.cu:967-984): the integrals of Solve run both ways
+// from the plane mid_z (and, for qy's plane there, from the row mid_x); mid_y is unused, as in the
+// reference.  Any bc.
+extern "C" CUWHHD_API wp_status wp_sweep3d_solve_from_mid(wp_sweep3d* h, float* qx, float* qy, float* qz,
+                                                          const float* xv, const float* yv, const float* zv, int mid_x,
+                                                          int mid_y, int mid_z, void* stream) {
+    (void)mid_y;
+    if (!h || !qx || !qy || !qz || !xv || !yv || !zv) {
+        wp_set_error_msg("wp_sweep3d_solve_from_mid: null pointer");
+        return WP_ERR_INVALID_ARG;
+    }
+    const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+    if (mid_x < 0 || mid_x > nx || mid_z < 0 || mid_z > nz) {
+        wp_set_error_msg("wp_sweep3d_solve_from_mid: mid_x must lie in [0, nx] and mid_z in [0, nz]");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const long sqx = (long)nx * (ny + 1), sqy = (long)(nx + 1) * ny, szv = (long)nx * ny;
+    const float dx = (float)h->h[0], dz = (float)h->h[2];
+    WP_CUDA_TRY(cudaMemsetAsync(qz, 0, sizeof(float) * (size_t)(nx + 1) * (ny + 1) * nz, s));
+    WP_CUDA_TRY(cudaMemsetAsync(qx + mid_z * sqx, 0, sizeof(float) * sqx, s));
+    // qy's plane mid_z: rows x of ny, from row mid_x = 0 both ways along x with zv's plane mid_z
+    float* qp = qy + mid_z * sqy;
+    const float* zp = zv + mid_z * szv;
+    WP_CUDA_TRY(cudaMemsetAsync(qp + (long)mid_x * ny, 0, sizeof(float) * ny, s));
+    const dim3 gy(wp_cdiv(ny, 32), 1), blk(32, kChunks);
+    if (mid_x < nx)
+        WP_KERNEL("sweep_x", 8.0 * (nx - mid_x) * ny, s,
+                  sweep_scan_kernel<<<gy, blk, 0, s>>>(qp + (long)mid_x * ny, zp + (long)mid_x * ny, 1, ny, nx - mid_x,
+                                                       dx, ny, ny));
+    if (mid_x > 0)
+        WP_KERNEL("sweep_x", 8.0 * mid_x * ny, s,
+                  sweep_scan_kernel<<<gy, blk, 0, s>>>(qp + (long)mid_x * ny, zp + (long)(mid_x - 1) * ny, 1, ny, mid_x,
+                                                       -dx, -ny, -ny));
+    // z both ways from plane mid_z: qx with +yv dz, qy with -xv dz (signs flip downward)
+    if (mid_z < nz) {
+        WP_KERNEL("sweep_z", 8.0 * sqx * (nz - mid_z), s,
+                  sweep_scan_kernel<<<dim3(wp_cdiv(ny + 1, 32), nx), blk, 0, s>>>(qx + mid_z * sqx, yv + mid_z * sqx, nx,
+                                                                                 ny + 1, nz - mid_z, dz));
+        WP_KERNEL("sweep_z", 8.0 * sqy * (nz - mid_z), s,
+                  sweep_scan_kernel<<<dim3(wp_cdiv(ny, 32), nx + 1), blk, 0, s>>>(qy + mid_z * sqy, xv + mid_z * sqy,
+                                                                                 nx + 1, ny, nz - mid_z, -dz));
+    }
+    if (mid_z > 0) {
+        WP_KERNEL("sweep_z", 8.0 * sqx * mid_z, s,
+                  sweep_scan_kernel<<<dim3(wp_cdiv(ny + 1, 32), nx), blk, 0, s>>>(qx + mid_z * sqx,
+                                                                                 yv + (mid_z - 1) * sqx, nx, ny + 1,
+                                                                                 mid_z, -dz, -sqx, -sqx));
+        WP_KERNEL("sweep_z", 8.0 * sqy * mid_z, s,
+                  sweep_scan_kernel<<<dim3(wp_cdiv(ny, 32), nx + 1), blk, 0, s>>>(qy + mid_z * sqy,
+                                                                                 xv + (mid_z - 1) * sqy, nx + 1, ny,
+                                                                                 mid_z, dz, -sqy, -sqy));
+    }
     return WP_OK;
 }
 
