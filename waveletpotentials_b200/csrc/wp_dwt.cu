@@ -682,25 +682,49 @@ __global__ void __launch_bounds__(NT) dwt_tile_kernel(const T* __restrict__ src,
         outbuf = cur;
     }
 
-    // ---- store the tile
+    // ---- store the tile.  The forward result's position p lives in one buffer per Mallat region
+    // (the base, then detail level l at [2^l + ext, 2^(l+1) + ext)): a thread walks its positions with
+    // a running global pointer and shared index and re-selects the buffer only when p enters the next
+    // region (the inverse result is all in outbuf).
     const int basebuf = (levels - 1) & 1;
+    auto region = [&](int p, int& b, int& next) {
+        if (outbuf >= 0) {
+            b = outbuf;
+            next = N;
+        } else if (p < nb) {
+            b = basebuf;
+            next = nb;
+        } else {
+            const int lg = 31 - __clz(p - ext);
+            b = (levels - lg) & 1;
+            next = (2 << lg) + ext;
+        }
+    };
     if (g.contiguous) {
         for (int col = tid >> 5; col < C; col += NT / 32) {
             if (i0 + col >= g.ni) continue;
             T* line = dst + obase + (long)(i0 + col) * g.s_in;
-            for (int p = tid & 31; p < N; p += 32) {
-                int b = outbuf;
-                if (b < 0) b = (p < nb) ? basebuf : ((levels - (31 - __clz(p - ext))) & 1);
+            int p = tid & 31, b, next;
+            region(p, b, next);
+            for (; p < N; p += 32) {
+                if (p >= next) region(p, b, next);
                 line[p] = buf(b)[p * CP + col];
             }
         }
     } else {
-        for (int i = tid; i < C * N; i += NT) {
-            int col = i % C, p = i / C;
-            if (i0 + col >= g.ni) continue;
-            int b = outbuf;
-            if (b < 0) b = (p < nb) ? basebuf : ((levels - (31 - __clz(p - ext))) & 1);
-            dst[obase + (long)(i0 + col) * g.s_in + (long)p * g.pstride] = buf(b)[p * CP + col];
+        // NT is a multiple of C: a thread keeps its column, positions advance by NT / C
+        constexpr int PS = NT / C;
+        const int col = tid % C;
+        if (i0 + col < g.ni) {
+            int p = tid / C, b, next;
+            T* gp = dst + obase + (long)(i0 + col) * g.s_in + (long)p * g.pstride;
+            const long gstep = (long)PS * g.pstride;
+            int si = p * CP + col;
+            region(p, b, next);
+            for (; p < N; p += PS, gp += gstep, si += PS * CP) {
+                if (p >= next) region(p, b, next);
+                *gp = buf(b)[si];
+            }
         }
     }
 }

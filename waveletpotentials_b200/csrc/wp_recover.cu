@@ -38,19 +38,12 @@ struct AxisTab {
     const float* ip1;
 };
 
-__global__ void __launch_bounds__(256) project3d_kernel(float* __restrict__ qx, float* __restrict__ qy,
-                                                        float* __restrict__ qz, const float* __restrict__ xv,
-                                                        const float* __restrict__ yv, const float* __restrict__ zv,
-                                                        int nx, int ny, int nz, AxisTab tx, AxisTab ty, AxisTab tz) {
-    const int y = blockIdx.x * 32 + threadIdx.x;
-    const int x = blockIdx.y * 8 + threadIdx.y;
-    const int z = blockIdx.z;
-    if (y >= ny || x >= nx) return;
-    const long sxv = (long)(nx + 1) * ny, syv = (long)nx * (ny + 1), szv = (long)nx * ny;
+// project3d_kernel's per-coefficient body: coefficient (x, y, z) with its velocity coefficients
+// already loaded
+__device__ __forceinline__ void project3d_cell(float* __restrict__ qx, float* __restrict__ qy, float* __restrict__ qz,
+                                               int nx, int ny, int x, int y, int z, float xin, float yin, float zin,
+                                               const AxisTab& tx, const AxisTab& ty, const AxisTab& tz) {
     const long sqx = (long)nx * (ny + 1), sqy = (long)(nx + 1) * ny, sqz = (long)(nx + 1) * (ny + 1);
-    const float xin = xv[y + (long)(x + 1) * ny + z * sxv];
-    const float yin = yv[(y + 1) + (long)x * (ny + 1) + z * syv];
-    const float zin = zv[y + (long)x * ny + (z + 1) * szv];
     const float sx = tx.s[x], sy = ty.s[y], sz = tz.s[z];
     float oX = 0.f, oY = 0.f, oZ = 0.f;
     if (x > 0 && y > 0 && z > 0) {
@@ -91,6 +84,33 @@ __global__ void __launch_bounds__(256) project3d_kernel(float* __restrict__ qx, 
     if (y == 0 && z == 0) qx[(long)x * (ny + 1)] = 0.f;
     if (x == 0 && z == 0) qy[y] = 0.f;
     if (x == 0 && y == 0) qz[z * sqz] = 0.f;
+}
+
+// PZ z-planes per thread, their nine velocity loads issued before any arithmetic (one plane per thread
+// left the pass latency bound at ~0.6 of HBM)
+constexpr int PZ = 4;
+__global__ void __launch_bounds__(256) project3d_kernel(float* __restrict__ qx, float* __restrict__ qy,
+                                                        float* __restrict__ qz, const float* __restrict__ xv,
+                                                        const float* __restrict__ yv, const float* __restrict__ zv,
+                                                        int nx, int ny, int nz, AxisTab tx, AxisTab ty, AxisTab tz) {
+    const int y = blockIdx.x * 32 + threadIdx.x;
+    const int x = blockIdx.y * 8 + threadIdx.y;
+    const int z0 = blockIdx.z * PZ;
+    if (y >= ny || x >= nx) return;
+    const long sxv = (long)(nx + 1) * ny, syv = (long)nx * (ny + 1), szv = (long)nx * ny;
+    float xin[PZ], yin[PZ], zin[PZ];
+#pragma unroll
+    for (int j = 0; j < PZ; ++j) {
+        const int z = z0 + j;
+        if (z < nz) {
+            xin[j] = xv[y + (long)(x + 1) * ny + z * sxv];
+            yin[j] = yv[(y + 1) + (long)x * (ny + 1) + z * syv];
+            zin[j] = zv[y + (long)x * ny + (z + 1) * szv];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PZ; ++j)
+        if (z0 + j < nz) project3d_cell(qx, qy, qz, nx, ny, x, y, z0 + j, xin[j], yin[j], zin[j], tx, ty, tz);
 }
 
 // The projection with Dirichlet domain walls (the recovery's bc 'd'; cuProjectLocal_q_3d_nq_ccc,
@@ -466,9 +486,10 @@ extern "C" CUWHHD_API wp_status wp_recover3d_project(wp_recover3d* h, float* qx,
                                                                    view(h->tab[2], nz), lx, ly, lz));
         return WP_OK;
     }
+    const dim3 gridp(wp_cdiv(ny, 32), wp_cdiv(nx, 8), wp_cdiv(nz, PZ));
     WP_KERNEL("project3d", bytes, s,
-              project3d_kernel<<<grid, dim3(32, 8), 0, s>>>(qx, qy, qz, xv, yv, zv, nx, ny, nz, view(h->tab[0], nx),
-                                                            view(h->tab[1], ny), view(h->tab[2], nz)));
+              project3d_kernel<<<gridp, dim3(32, 8), 0, s>>>(qx, qy, qz, xv, yv, zv, nx, ny, nz, view(h->tab[0], nx),
+                                                             view(h->tab[1], ny), view(h->tab[2], nz)));
     return WP_OK;
 }
 
