@@ -64,11 +64,11 @@ def _outs(wp, grids):
     return outs
 
 
-@pytest.mark.parametrize("nstreams,start", [(1, 0), (4, 0), (4, 1)])
-def test_batch_matches_single_grid_path(wp, nstreams, start):
+@pytest.mark.parametrize("nstreams,start,inner", [(1, 0, 1), (4, 0, 1), (4, 1, 1), (4, 0, 3)])
+def test_batch_matches_single_grid_path(wp, nstreams, start, inner):
     tol = 1e-9
     grids, u = _grids(wp)
-    bp = wp.BatchProjector(grids, rel_tol=tol, max_cycles=40, nstreams=nstreams, start=start)
+    bp = wp.BatchProjector(grids, rel_tol=tol, max_cycles=40, nstreams=nstreams, start=start, inner_cycles=inner)
     cycles = bp.plan(u)
     assert all(1 <= c <= 40 for c in cycles)
     for rnd in range(2):  # the second run replays the captured graph on fresh copies of the fields
@@ -81,12 +81,14 @@ def test_batch_matches_single_grid_path(wp, nstreams, start):
             d = g["dim"]
             ref_u = [x.clone() for x in u[i]]
             if len(d) == 3:
-                pr = wp.Projector3D(g["ax"], g["ay"], g["az"], d, g["dx"], rel_tol=tol, max_cycles=40, start=start)
+                pr = wp.Projector3D(g["ax"], g["ay"], g["az"], d, g["dx"], rel_tol=tol, max_cycles=40, start=start,
+                                    inner_cycles=inner)
                 s = wp.mac_shapes3d(*d)
                 ref_q = [torch.zeros(s[k], device="cuda") for k in ("qx", "qy", "qz")]
                 rep = pr.run(*ref_u, *ref_q)
             else:
-                pr = wp.Projector2D(g["ax"], g["ay"], d, g["dx"], rel_tol=tol, max_cycles=40, start=start)
+                pr = wp.Projector2D(g["ax"], g["ay"], d, g["dx"], rel_tol=tol, max_cycles=40, start=start,
+                                    inner_cycles=inner)
                 ref_q = [torch.zeros(wp.mac_shapes2d(*d)["qz"], device="cuda")]
                 rep = pr.run(*ref_u, *ref_q)
             assert rep["cycles"] == cycles[i], (i, rep["cycles"], cycles[i])

@@ -789,14 +789,16 @@ class BatchProjector:
     """Many independent projections of uneven 2D/3D grids launched as one CUDA graph (wp_batch_*).
 
     ``grids`` is a list of dicts ``{"dim": (nx, ny[, nz]), "dx": h, "ax": ..., "ay": ...[, "az": ...]}``;
-    a grid is 3D when its ``dim`` has three extents.  ``plan(fields)`` fixes each grid's refinement
-    steps with an eager tolerance-driven solve; ``run(fields, outs)`` projects every grid in place and
-    writes its potential.  ``fields[i]`` is ``(xv, yv, zv)`` (3D) or ``(xv, yv)`` (2D); ``outs[i]`` is
-    ``(qx, qy, qz)`` or ``(qz,)``.
+    a grid is 3D when its ``dim`` has three extents.  ``run(fields, outs)`` projects every grid in place
+    and writes its potential, each grid's solve a device loop that stops at ``rel_tol`` (or
+    ``max_cycles``) on the current input; ``plan(fields)`` (optional) measures the cycles of a
+    representative input to order the grids over the graph's branches.  ``fields[i]`` is
+    ``(xv, yv, zv)`` (3D) or ``(xv, yv)`` (2D); ``outs[i]`` is ``(qx, qy, qz)`` or ``(qz,)``.
+    ``inner_cycles``: FP32 V-cycles per FP64 refinement step.
     """
 
     def __init__(self, grids, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 prolongation=PROLONG_TRILINEAR, nstreams=8, start=START_ZERO):
+                 prolongation=PROLONG_TRILINEAR, nstreams=8, start=START_ZERO, inner_cycles=1):
         self.grids = grids
         self.count = len(grids)
         self.rel_tol = float(rel_tol)
@@ -820,7 +822,7 @@ class BatchProjector:
             ay.append(_ptr(g["ay"], s["yv"], name="ay").value)
         self.dims = dims
         prm = MgParams(int(max_cycles), int(nu1), int(nu2), float(weight), float(rel_tol), PREC_MIXED,
-                       int(prolongation), int(start), 0)
+                       int(prolongation), int(start), 0, int(inner_cycles))
         h = ctypes.c_void_p()
         self._keep = ((ctypes.c_int * self.count)(*dims), (ctypes.c_int * (3 * self.count))(*ext),
                       (ctypes.c_double * self.count)(*dx), _parray(ax), _parray(ay), _parray(az), prm)

@@ -3889,29 +3889,6 @@ wp_status solve_mixed_loop_capture(wp_mgfrac3d* h, float* dst, const float* f, c
     return WP_OK;
 }
 
-// `cycles` refinement steps of the mixed solve with no host synchronisation (capturable into a
-// CUDA graph): the active mean of f, the defect norms and ||f||^2 stay in the handle's device
-// slots acc[0..3].
-wp_status solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
-                                  cudaStream_t s) {
-    Level& L = h->lv[0];
-    const long n = L.cells;
-    const unsigned cb = std::min<unsigned>(wp_cdiv(n, 256), wp_sm_count() * 8);
-    wp_status st;
-    if (!h->p64 || !h->r32) { wp_set_error_msg("mixed solve: work arrays not prepared"); return WP_ERR_INVALID_ARG; }
-    WP_CUDA_TRY(cudaMemsetAsync(h->acc + 2, 0, 2 * sizeof(double), s));
-    WP_KERNEL("active_sum", (double)n * 4.0 + frac_bytes(L), s, launch_active_sum(L, f, h->acc + 2, s));
-    WP_CUDA_TRY(cudaMemsetAsync(h->p64, 0, sizeof(double) * n, s));
-    if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, true, s)) != WP_OK) return st;
-    for (int c = 0; c < cycles; ++c) {
-        if ((st = mixed_correction(h, prm, c == 0 && prm->start == WP_START_FMG, s)) != WP_OK) return st;
-        if ((st = defect_async<double>(h, h->p64, f, 0.0, h->acc + 2, h->r32, false, s)) != WP_OK) return st;
-    }
-    h->last64 = 1;
-    WP_KERNEL("convert", 12.0 * n, s, convert_kernel<float, double><<<cb, 256, 0, s>>>(dst, h->p64, n));
-    return WP_OK;
-}
-
 wp_status residual_rel(wp_mgfrac3d* h, const float* v, const float* f, double* rel, cudaStream_t s) {
     if (!h || !v || !f || !rel) { wp_set_error_msg("wp_mgfrac_residual: null pointer"); return WP_ERR_INVALID_ARG; }
     double nr2 = 0.0, nf2 = 0.0;
@@ -4316,10 +4293,6 @@ wp_status wp_mg_prepare_mixed(wp_mgfrac3d* h) { return prepare_mixed(h); }
 // a cooperative launch needs the whole GPU: the batch, whose grids run on concurrent graph branches,
 // keeps every level launch by launch
 void wp_mg_forbid_persistent(wp_mgfrac3d* h) { h->mid_forbid = 1; }
-wp_status wp_mg_solve_mixed_fixed_async(wp_mgfrac3d* h, float* dst, const float* f, int cycles, const wp_mg_params* prm,
-                                        cudaStream_t s) {
-    return solve_mixed_fixed_async(h, dst, f, cycles, prm, s);
-}
 wp_status wp_mg_solve_mixed_loop_capture(wp_mgfrac3d* h, float* dst, const float* f, const wp_mg_params* prm,
                                          cudaStream_t s, long long* body_launches) {
     return solve_mixed_loop_capture(h, dst, f, prm, s, body_launches);
@@ -4331,6 +4304,6 @@ wp_status wp_mg_solve_tol_internal(wp_mgfrac3d* h, float* dst, const float* f, c
     return solve_tol(h, dst, nullptr, f, prm, r, s);
 }
 const double* wp_mg_slots(const wp_mgfrac3d* h) { return h->acc; }
-// the FP64 iterate of the mixed solve (wp_mg_solve_mixed_fixed_async leaves its result there)
+// the FP64 iterate of the mixed solve (the batch's device loop leaves its result there)
 const double* wp_mg_p64(const wp_mgfrac3d* h) { return h->p64; }
 wp_mgfrac3d* wp_mg2d_impl(wp_mgfrac2d* h) { return h ? h->impl : nullptr; }
