@@ -106,7 +106,7 @@ def test_device_velocity_generator(wp, oracle):
 def test_trained_warm_start_learns_and_fallback_bounds_its_cost(wp):
     """What the trained network does, stated as it is: training on the plain method's solves halves
     the loss; on held-out 32^3 problems the solve still meets its tolerance; the guess beats a zero
-    start after one V-cycle; and the fallback (judged after that cycle) keeps the cost at most one
+    start after one V-cycle; and the fallback (decided after that cycle) keeps the cost at most one
     cycle above the plain method.  The guess does not save cycles here or at 128^3 (the warm-start
     run summary in profiles/), so no test asserts that it does."""
     from waveletpotentials_b200 import trainer
