@@ -182,3 +182,26 @@ def test_sweep_solve_from_mid_matches_reference(wp, tag):
     with pytest.raises(wp.WPError):
         sw.SolveFromMid(*q, *u, (n + 1, 0, 0))
     sw.close()
+
+
+def test_dirichlet_sweep_and_mid_sweep_reproduce_fields_at_64(wp):
+    """At 64^3, FP32: curl q = u after the bc 'd' solve and after SolveFromMid, for a field with wall flux."""
+    from waveletpotentials_b200 import fields
+    n = 64
+    h = 1.0 / n
+    rng = np.random.default_rng(5)
+    s = wp.mac_shapes3d(n, n, n)
+    q0 = [fields.spectral_field(s[k], -11.0 / 3.0, 1.0, rng) for k in ("qx", "qy", "qz")]
+    u = fields.curl3d(*q0, (n, n, n), (h, h, h))
+    den = sum(np.sum(a * a) for a in u)
+    for bc, mid in (("d", None), ("n", (20, 0, 41))):
+        sw = wp.CuParallelSweep3D((n, n, n), h, bc)
+        q = [torch.zeros(s[k], device="cuda") for k in ("qx", "qy", "qz")]
+        if mid is None:
+            sw.Solve(*q, *[_t(a) for a in u])
+        else:
+            sw.SolveFromMid(*q, *[_t(a) for a in u], mid)
+        torch.cuda.synchronize()
+        c = fields.curl3d(*[t.double().cpu().numpy() for t in q], (n, n, n), (h, h, h))
+        assert np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u, c)) / den) < 1e-5, (bc, mid)
+        sw.close()

@@ -245,3 +245,24 @@ def test_2d_recovery_with_dirichlet_walls_is_close_to_the_field(oracle, n):
         c = fields.curl2d(oracle.recover2d(*u, n, d, bc=bc), n, d)
         err[bc] = np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u, c)) / den)
     assert err["d"] < 2e-2 and err["n"] > 0.5, err
+
+
+@pytest.mark.parametrize("n", [8, 16])
+def test_dirichlet_sweep_and_mid_sweep_reproduce_fields_with_wall_flux(oracle, n):
+    """The sweep solve with bc 'd' (qy's bottom plane from zv) and SolveFromMid give curl q = u for any
+    discretely divergence-free u, wall flux included; the bc 'n' sweep assumes no flux through the
+    walls and does not."""
+    h = 1.0 / n
+    rng = np.random.default_rng(n)
+    s = oracle.mac_shapes3d(n, n, n)
+    q = [fields.spectral_field(s[k], -11.0 / 3.0, 1.0, rng) for k in ("qx", "qy", "qz")]
+    u = fields.curl3d(*q, (n, n, n), (h, h, h))
+    den = sum(np.sum(a * a) for a in u)
+
+    def err(r):
+        c = fields.curl3d(*r, (n, n, n), (h, h, h))
+        return np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u, c)) / den)
+
+    assert err(oracle.sweep3d_solve(*u, (n, n, n), (h, h, h), bc="d")) < 1e-12
+    assert err(oracle.sweep3d_solve_from_mid(*u, (n, n, n), (h, h, h), (n // 2, 1, n // 3))) < 1e-12
+    assert err(oracle.sweep3d_solve(*u, (n, n, n), (h, h, h), bc="n")) > 1e-2
