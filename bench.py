@@ -419,7 +419,9 @@ def run_batch(args, rank, world, local_rank):
             outs.append([torch.zeros(s["qz"], device=dev)])
         u0.append([torch.as_tensor(x, device=dev) for x in u])
     u = [[x.clone() for x in f] for f in u0]
-    bp = api.BatchProjector(grids, rel_tol=args.batch_tol, max_cycles=80, nstreams=args.nstreams)
+    persistent = args.batch_mode == "persistent"
+    bp = api.BatchProjector(grids, rel_tol=args.batch_tol, max_cycles=80, nstreams=args.nstreams,
+                            persistent=persistent, tile_cells=args.batch_tile)
     cycles = bp.plan(u)
     stream = torch.cuda.current_stream()
     count = len(grids)
@@ -458,6 +460,37 @@ def run_batch(args, rank, world, local_rank):
     launches = int(L.wp_launch_count())
     res = bp.results()
     launches += (int(L.wp_launch_count()) - launches) * (args.steps - 1)
+    # persistent mode: where the persistent kernel's CTAs spend their cycles over one more run
+    prof = None
+    if persistent:
+        bp.profile(True)
+        step()
+        torch.cuda.synchronize()
+        pr = bp.profile(False)
+        tot = pr["wait_cycles"] + pr["setup_cycles"] + pr["complete_cycles"] + sum(
+            pr[k]["cycles"] for k in api.BatchProjector.PROFILE_NAMES)
+        prof = {"cta_cycles": tot, "tiles": pr["tiles"],
+                "share": {"waiting_for_work": pr["wait_cycles"] / tot, "setup": pr["setup_cycles"] / tot,
+                          "complete_publish": pr["complete_cycles"] / tot,
+                          **{k: pr[k]["cycles"] / tot for k in api.BatchProjector.PROFILE_NAMES}},
+                "cycles_per_tile": {k: (pr[k]["cycles"] / pr[k]["tiles"] if pr[k]["tiles"] else 0.0)
+                                    for k in api.BatchProjector.PROFILE_NAMES},
+                "tiles_by_type": {k: pr[k]["tiles"] for k in api.BatchProjector.PROFILE_NAMES}}
+    # the other way of running the solves, same grids and inputs, for comparison
+    other = api.BATCH_GRAPH if persistent else api.BATCH_PERSISTENT
+    bp.set_mode(other, args.batch_tile)
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    o0.record(stream)
+    for _ in range(args.steps):
+        step()
+    o1.record(stream)
+    torch.cuda.synchronize()
+    other_ms = o0.elapsed_time(o1) / args.steps
+    ores = bp.results()
+    bp.set_mode(api.BATCH_PERSISTENT if persistent else api.BATCH_GRAPH, args.batch_tile)
     # the same grids projected one after another through the one-grid path (eager launches)
     projs = []
     for g in grids:
@@ -511,9 +544,16 @@ def run_batch(args, rank, world, local_rank):
     cells = sum(int(np.prod(g["dim"])) for g in grids)
     info = {"grids": count, "grids_3d": args.batch3d, "grids_2d": args.batch2d, "cells": cells,
             "cycles_min": min(res["cycles"]), "cycles_max": max(res["cycles"]), "nstreams": args.nstreams,
-            "cycles_per_grid": "device loop per grid (while-node): each replay stops at the tolerance",
-            "graph_ms_per_batch": ms / args.steps, "sequential_eager_ms_per_batch": seq_ms,
-            "graph_speedup_vs_sequential": seq_ms / (ms / args.steps),
+            "mode": args.batch_mode,
+            "solves": ("one persistent kernel over a device work queue of (grid, level, pass) tiles, "
+                       f"{args.batch_tile or 32768} cells per tile" if persistent else
+                       "a device loop of launches per grid (while-node) on the graph's branches"),
+            "cycles_per_grid": "each replay's stopping rule runs on the device: it stops at the tolerance",
+            "ms_per_batch": ms / args.steps, "sequential_eager_ms_per_batch": seq_ms,
+            "speedup_vs_sequential": seq_ms / (ms / args.steps),
+            ("graph_ms_per_batch" if persistent else "persistent_ms_per_batch"): other_ms,
+            "other_mode_same_cycles": ores["cycles"] == res["cycles"],
+            "persistent_profile": prof,
             "max_rel_residual": max(res["rel_residual"]), "max_abs_div": max(res["max_abs_div"])}
     return ms, ems, ek, h2d, d2h, launches, clk.summary(), info, count
 
@@ -782,6 +822,10 @@ def main():
     ap.add_argument("--batch3d", type=int, default=32)
     ap.add_argument("--batch2d", type=int, default=32)
     ap.add_argument("--batch-tol", type=float, default=1e-6)
+    ap.add_argument("--batch-mode", default="graph", choices=["graph", "persistent"],
+                    help="graph: each grid's solve a device loop of launches on a graph branch; persistent: every "
+                         "grid's solve in one persistent kernel over a device work queue")
+    ap.add_argument("--batch-tile", type=int, default=0, help="persistent mode: cells per work-queue tile (0: 32768)")
     ap.add_argument("--nstreams", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -67,11 +67,14 @@ CUWHHD_API int wp_version(void);
    out after limit_seconds (in [1e-6, 2]) and the call returns WP_ERR_DEVICE_WAIT.  One shot.
    WP_WAIT_SITE_GRID_BARRIER: the last CTA of the persistent below-finest multigrid cycle skips the
    first grid barrier.  WP_WAIT_SITE_CONV_PIPELINE: the first CTA of the next tensor-core convolution
-   (forward or weight gradient) does not load pipeline step `at`.  site 0 disarms.  Every other wait
+   (forward or weight gradient) does not load pipeline step `at`.  WP_WAIT_SITE_BATCH_PUBLISH: the
+   next wp_batch_run of a WP_BATCH_PERSISTENT batch does not publish the phase that follows phase `at`
+   of its first grid, so the persistent kernel's CTAs wait for work until the limit.  site 0 disarms.  Every other wait
    of that launch keeps its own limit; the kernels still wait for their copies in flight and free
    their tensor memory before they return.  No reference counterpart. */
 #define WP_WAIT_SITE_GRID_BARRIER 1
 #define WP_WAIT_SITE_CONV_PIPELINE 2
+#define WP_WAIT_SITE_BATCH_PUBLISH 3
 CUWHHD_API wp_status wp_debug_withhold_wait(int site, int at, double limit_seconds);
 
 /* Instrumentation (no reference counterpart): number of kernels this library has launched since
@@ -493,6 +496,32 @@ CUWHHD_API wp_status wp_batch_run(wp_batch* h, float* const* xv, float* const* y
    WP_ERR_DEVICE_WAIT when a bounded device wait gave up. */
 CUWHHD_API wp_status wp_batch_results(wp_batch* h, double* max_abs_div, double* rel_residual, int* cycles,
                                       void* stream);
+/* How wp_batch_run solves the grids.  WP_BATCH_GRAPH: each grid's solve is its own launches on a
+   branch of the graph (a while-node per grid).  WP_BATCH_PERSISTENT: every grid's solve runs in ONE
+   persistent kernel inside the graph (one 1024-thread CTA per SM) that takes (grid, level, pass)
+   tiles from a device work queue: per grid a program of the phases of one refinement step (first
+   sweep from zero, sweeps, residual restriction, the single-CTA coarse cycle, prolongation, the
+   sweep that adds to the FP64 iterate, FP64 defect and stopping rule) repeated until the rule stops
+   it, the grids advancing independently; the divergence, gradient update, max|div u| and recovery
+   of the grids run on the graph's branches before and after it.  Same per-cell arithmetic, same
+   results as WP_BATCH_GRAPH (up to the order of the FP64 norm reductions).  tile_cells: cells per
+   work-queue tile (0 = 32768).  Needs trilinear V(nu1, nu2) cycles with nu1, nu2 >= 1 from a zero
+   start and, per grid, levels whose y extent is a multiple of 4 down to a coarse level of at most
+   4096 cells whose pack fits the CTA's shared memory; WP_ERR_UNSUPPORTED otherwise (the mode stays
+   as it was).  Every wait of the persistent kernel is bounded (WP_ERR_DEVICE_WAIT from
+   wp_batch_results when one gave up). */
+#define WP_BATCH_GRAPH 0
+#define WP_BATCH_PERSISTENT 1
+CUWHHD_API wp_status wp_batch_set_mode(wp_batch* h, int mode, long long tile_cells);
+/* WP_BATCH_PERSISTENT batches: activity counters of the persistent kernel (SM clock cycles summed
+   over the CTAs, thread 0 of each), synchronous.  out[0..cap-1] receives the sums since counting was
+   last enabled: [0] cycles waiting for a free tile, [1] tiles taken, [2] cycles setting up a tile,
+   [3] cycles completing tiles and publishing phases, then for each phase type k = 0..8 (active-cell
+   sum, defect, first sweep, sweep, sweep into the FP64 iterate, restriction, prolongation, coarse
+   cycle, FP32 copy) [4+2k] its tile cycles and [5+2k] its tiles.  enable 1 clears the sums and counts
+   the following runs, 0 stops counting.  WP_ERR_UNSUPPORTED in graph mode. */
+#define WP_BATCH_PROFILE_SLOTS 22
+CUWHHD_API wp_status wp_batch_profile(wp_batch* h, int enable, double* out, int cap, void* stream);
 CUWHHD_API wp_status wp_batch_destroy(wp_batch* h);
 
 #ifdef __cplusplus

@@ -17,7 +17,8 @@ import torch
 
 from . import _lib
 from ._lib import START_FMG, START_ZERO  # noqa: F401
-from ._lib import WAIT_SITE_CONV_PIPELINE, WAIT_SITE_GRID_BARRIER  # noqa: F401
+from ._lib import WAIT_SITE_BATCH_PUBLISH, WAIT_SITE_CONV_PIPELINE, WAIT_SITE_GRID_BARRIER  # noqa: F401
+from ._lib import BATCH_GRAPH, BATCH_PERSISTENT  # noqa: F401
 from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONSTANT, PROLONG_TRILINEAR, MgParams, \
     MgReport, WPError, check, lib
 
@@ -26,7 +27,8 @@ __all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRe
            "Projector3D", "Projector2D", "BatchProjector", "max_abs", "conv3_forward", "conv3_wgrad",
            "random_field3d", "velocity3d_device", "UNetWarmStart", "warm_started_solve",
            "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
-           "PROLONG_TRILINEAR", "START_ZERO", "START_FMG", "mac_shapes3d", "mac_shapes2d"]
+           "PROLONG_TRILINEAR", "START_ZERO", "START_FMG", "mac_shapes3d", "mac_shapes2d", "BATCH_GRAPH",
+           "BATCH_PERSISTENT"]
 
 
 def mac_shapes3d(nx, ny, nz):
@@ -794,11 +796,15 @@ class BatchProjector:
     ``max_cycles``) on the current input; ``plan(fields)`` (optional) measures the cycles of a
     representative input to order the grids over the graph's branches.  ``fields[i]`` is
     ``(xv, yv, zv)`` (3D) or ``(xv, yv)`` (2D); ``outs[i]`` is ``(qx, qy, qz)`` or ``(qz,)``.
-    ``inner_cycles``: FP32 V-cycles per FP64 refinement step.
+    ``inner_cycles``: FP32 V-cycles per FP64 refinement step.  ``persistent``: every grid's solve in
+    one persistent kernel inside the graph that takes (grid, level, pass) tiles from a device work
+    queue (``wp_batch_set_mode(..., WP_BATCH_PERSISTENT, tile_cells)``), instead of a device loop of
+    launches per grid; ``tile_cells`` (0 = the library's default) sets the cells per queue tile.
     """
 
     def __init__(self, grids, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
-                 prolongation=PROLONG_TRILINEAR, nstreams=8, start=START_ZERO, inner_cycles=1):
+                 prolongation=PROLONG_TRILINEAR, nstreams=8, start=START_ZERO, inner_cycles=1,
+                 persistent=False, tile_cells=0):
         self.grids = grids
         self.count = len(grids)
         self.rel_tol = float(rel_tol)
@@ -833,6 +839,29 @@ class BatchProjector:
                                     ctypes.cast(k[5], ctypes.c_void_p), ctypes.byref(prm), int(nstreams)),
               "wp_batch_create")
         self._h = h
+        if persistent:
+            self.set_mode(BATCH_PERSISTENT, tile_cells)
+
+    PROFILE_NAMES = ("init", "defect", "sweep0", "sweep", "sweep_acc", "restrict", "prolong", "coarse", "convert")
+
+    def profile(self, enable, stream=None):
+        """Persistent mode: the persistent kernel's activity counters since counting was last enabled
+        (wp_batch_profile), as a dict of SM cycles summed over the CTAs; ``enable`` True clears them and
+        counts the following runs, False stops."""
+        out = (ctypes.c_double * 22)()
+        check(lib().wp_batch_profile(self._h, 1 if enable else 0, ctypes.cast(out, ctypes.c_void_p), 22,
+                                     _stream(stream)), "wp_batch_profile")
+        v = list(out)
+        d = {"wait_cycles": v[0], "tiles": v[1], "setup_cycles": v[2], "complete_cycles": v[3]}
+        for k, nm in enumerate(self.PROFILE_NAMES):
+            d[nm] = {"cycles": v[4 + 2 * k], "tiles": v[5 + 2 * k]}
+        return d
+
+    def set_mode(self, mode, tile_cells=0):
+        """BATCH_GRAPH or BATCH_PERSISTENT (see the class docstring); raises WPError (the mode
+        unchanged) when a grid's levels do not fit the persistent program."""
+        check(lib().wp_batch_set_mode(self._h, int(mode), int(tile_cells)), "wp_batch_set_mode")
+        self.mode = int(mode)
 
     def _fields(self, fields, outs=None):
         names_in = ("xv", "yv", "zv")

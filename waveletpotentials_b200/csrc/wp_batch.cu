@@ -9,6 +9,9 @@
 // plan pass (wp_batch_plan) measures the step counts of a representative input; they only order the
 // grids over the branches (costliest first).  Per-grid max|div|, the final FP64 relative residual and
 // the V-cycle count stay on the device until wp_batch_results() reads them with one copy.
+// In WP_BATCH_PERSISTENT mode the solves of all grids run instead in one persistent kernel inside the
+// graph (wp_mg.cu, batch_persist_kernel: a device work queue of (grid, level, pass) tiles), between
+// the grids' divergences and their gradient updates and recoveries on the branches.
 #include "wp_common.cuh"
 
 #include <algorithm>
@@ -29,6 +32,14 @@ const double* wp_mg_slots(const wp_mgfrac3d* h);
 const double* wp_mg_p64(const wp_mgfrac3d* h);
 wp_mgfrac3d* wp_mg2d_impl(wp_mgfrac2d* h);
 wp_status wp_max_abs_device(const float* x, size_t n, unsigned int* d_out, cudaStream_t s);
+struct wp_mg_pbatch;
+wp_status wp_mg_pbatch_create(wp_mg_pbatch** out, wp_mgfrac3d* const* hs, float* const* dst, const float* const* f,
+                              int count, const wp_mg_params* prm, long target_cells);
+wp_status wp_mg_pbatch_arm(wp_mg_pbatch* pb, int at, unsigned long long limit_ns, cudaStream_t s);
+wp_status wp_mg_pbatch_launch(wp_mg_pbatch* pb, cudaStream_t s);
+void wp_mg_pbatch_destroy(wp_mg_pbatch* pb);
+wp_status wp_mg_pbatch_profile(wp_mg_pbatch* pb, int enable, unsigned long long* out, cudaStream_t s);
+int wp_mg_pbatch_prof_slots();
 
 namespace {
 
@@ -82,20 +93,30 @@ struct wp_batch {
     long long graph_launches = 0;    // kernels in one replay of the graph outside the loop bodies
     bool planned = false;
     bool counted = true;             // the last replay's loop-body kernels were added to the count
+    int mode = WP_BATCH_GRAPH;
+    long long tile_cells = 0;        // persistent mode: cells per work-queue tile (0 = default)
+    wp_mg_pbatch* pb = nullptr;      // persistent mode: every grid's solve program, in cost order
 };
 
 namespace {
 
-wp_status project_one(wp_batch* B, int i, float* xv, float* yv, float* zv, float* qx, float* qy, float* qz,
-                      cudaStream_t s) {
+// b = -div(a u) of grid i (the solve's right-hand side)
+wp_status divergence_one(wp_batch* B, int i, const float* xv, const float* yv, const float* zv, cudaStream_t s) {
+    Grid& G = B->g[i];
+    const double h = G.h;
+    if (G.dims == 3)
+        return wp_divergence_frac3d(G.b, xv, yv, zv, G.frac[0], G.frac[1], G.frac[2], G.n[0], G.n[1], G.n[2], h, h, h,
+                                    s);
+    return wp_divergence_frac2d(G.b, xv, yv, G.frac[0], G.frac[1], G.n[0], G.n[1], h, h, s);
+}
+
+// after the solve: u <- (u - grad p) a, max|div u|, wavelet potential recovery
+wp_status finish_one(wp_batch* B, int i, float* xv, float* yv, float* zv, float* qx, float* qy, float* qz,
+                     cudaStream_t s) {
     Grid& G = B->g[i];
     wp_status st;
     const double h = G.h;
     if (G.dims == 3) {
-        if ((st = wp_divergence_frac3d(G.b, xv, yv, zv, G.frac[0], G.frac[1], G.frac[2], G.n[0], G.n[1], G.n[2], h, h,
-                                       h, s)) != WP_OK)
-            return st;
-        if ((st = wp_mg_solve_mixed_loop_capture(G.mg3, G.p, G.b, &B->prm, s, &G.body_launches)) != WP_OK) return st;
         // the gradient of the FP64 iterate, formed in FP64 (as the one-grid projector does)
         if ((st = wp_grad_subtract_frac3d_p64(xv, yv, zv, wp_mg_p64(G.mg3), G.frac[0], G.frac[1], G.frac[2], G.n[0],
                                               G.n[1], G.n[2], h, h, h, 1, s)) != WP_OK)
@@ -106,13 +127,46 @@ wp_status project_one(wp_batch* B, int i, float* xv, float* yv, float* zv, float
         if ((st = wp_max_abs_device(G.b, G.cells(), B->d_max + i, s)) != WP_OK) return st;
         return wp_recover3d_run(G.rec3, qx, qy, qz, xv, yv, zv, s);
     }
-    if ((st = wp_divergence_frac2d(G.b, xv, yv, G.frac[0], G.frac[1], G.n[0], G.n[1], h, h, s)) != WP_OK) return st;
-    if ((st = wp_mg_solve_mixed_loop_capture(wp_mg2d_impl(G.mg2), G.p, G.b, &B->prm, s, &G.body_launches)) != WP_OK)
-        return st;
     if ((st = wp_grad_subtract_frac2d(xv, yv, G.p, G.frac[0], G.frac[1], G.n[0], G.n[1], h, h, 1, s)) != WP_OK) return st;
     if ((st = wp_divergence_frac2d(G.b, xv, yv, nullptr, nullptr, G.n[0], G.n[1], h, h, s)) != WP_OK) return st;
     if ((st = wp_max_abs_device(G.b, G.cells(), B->d_max + i, s)) != WP_OK) return st;
     return wp_recover2d_run(G.rec2, qz, xv, yv, s);
+}
+
+// one grid on one branch: divergence, its device-loop solve, the rest
+wp_status project_one(wp_batch* B, int i, float* xv, float* yv, float* zv, float* qx, float* qy, float* qz,
+                      cudaStream_t s) {
+    Grid& G = B->g[i];
+    wp_status st;
+    if ((st = divergence_one(B, i, xv, yv, zv, s)) != WP_OK) return st;
+    if ((st = wp_mg_solve_mixed_loop_capture(G.mg(), G.p, G.b, &B->prm, s, &G.body_launches)) != WP_OK) return st;
+    return finish_one(B, i, xv, yv, zv, qx, qy, qz, s);
+}
+
+// costliest grids first: cells x (planned V-cycles + 2), or cells alone without a plan
+std::vector<int> cost_order(const wp_batch* B) {
+    const int count = (int)B->g.size();
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    auto cost = [&](int i) { return B->g[i].cells() * (B->planned ? B->g[i].cycles + 2 : 1); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    return order;
+}
+
+// the persistent solve of every grid, programs in cost order
+wp_status build_pbatch(wp_batch* B) {
+    if (B->pb) return WP_OK;
+    const std::vector<int> order = cost_order(B);
+    std::vector<wp_mgfrac3d*> hs;
+    std::vector<float*> dst;
+    std::vector<const float*> f;
+    for (int i : order) {
+        hs.push_back(B->g[i].mg());
+        dst.push_back(B->g[i].p);
+        f.push_back(B->g[i].b);
+    }
+    return wp_mg_pbatch_create(&B->pb, hs.data(), dst.data(), f.data(), (int)order.size(), &B->prm,
+                               (long)B->tile_cells);
 }
 
 void destroy_graph(wp_batch* B) {
@@ -222,6 +276,11 @@ extern "C" CUWHHD_API wp_status wp_batch_plan(wp_batch* B, const float* const* x
     }
     B->planned = true;
     destroy_graph(B);
+    // the programs follow the new cost order
+    if (B->pb) {
+        wp_mg_pbatch_destroy(B->pb);
+        B->pb = nullptr;
+    }
     return WP_OK;
 }
 
@@ -243,28 +302,49 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
     cudaStream_t s = (cudaStream_t)stream;
     if (!B->exec || ptrs != B->bound) {
         destroy_graph(B);
+        wp_status pst;
+        if (B->mode == WP_BATCH_PERSISTENT && (pst = build_pbatch(B)) != WP_OK) return pst;
         cudaStream_t cs = B->streams[0];
         const long long launches0 = wp_launch_count();
         WP_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
         wp_status st = WP_OK;
         cudaEventRecord(B->events[0], cs);
         for (size_t k = 1; k < B->streams.size(); ++k) cudaStreamWaitEvent(B->streams[k], B->events[0], 0);
-        // costliest grids first (cells x (planned V-cycles + 2), or cells alone without a plan),
-        // round-robin over the branches
-        std::vector<int> order(count);
-        for (int i = 0; i < count; ++i) order[i] = i;
-        auto cost = [&](int i) { return B->g[i].cells() * (B->planned ? B->g[i].cycles + 2 : 1); };
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
-        for (int k = 0; k < count && st == WP_OK; ++k) {
-            const int i = order[k];
-            const bool d3 = B->g[i].dims == 3;
-            st = project_one(B, i, xv[i], yv[i], d3 ? zv[i] : nullptr, d3 ? qx[i] : nullptr, d3 ? qy[i] : nullptr, qz[i],
-                             B->streams[k % B->streams.size()]);
+        // costliest grids first, round-robin over the branches
+        const std::vector<int> order = cost_order(B);
+        const size_t ns = B->streams.size();
+        auto join = [&]() {
+            for (size_t k = 1; k < ns; ++k) {
+                cudaEventRecord(B->events[k], B->streams[k]);
+                cudaStreamWaitEvent(cs, B->events[k], 0);
+            }
+        };
+        if (B->mode == WP_BATCH_PERSISTENT) {
+            // divergences on the branches, every solve in the persistent kernel, then the rest
+            for (int k = 0; k < count && st == WP_OK; ++k) {
+                const int i = order[k];
+                st = divergence_one(B, i, xv[i], yv[i], B->g[i].dims == 3 ? zv[i] : nullptr, B->streams[k % ns]);
+                B->g[i].body_launches = 0;
+            }
+            join();
+            if (st == WP_OK) st = wp_mg_pbatch_launch(B->pb, cs);
+            cudaEventRecord(B->events[0], cs);
+            for (size_t k = 1; k < ns; ++k) cudaStreamWaitEvent(B->streams[k], B->events[0], 0);
+            for (int k = 0; k < count && st == WP_OK; ++k) {
+                const int i = order[k];
+                const bool d3 = B->g[i].dims == 3;
+                st = finish_one(B, i, xv[i], yv[i], d3 ? zv[i] : nullptr, d3 ? qx[i] : nullptr, d3 ? qy[i] : nullptr,
+                                qz[i], B->streams[k % ns]);
+            }
+        } else {
+            for (int k = 0; k < count && st == WP_OK; ++k) {
+                const int i = order[k];
+                const bool d3 = B->g[i].dims == 3;
+                st = project_one(B, i, xv[i], yv[i], d3 ? zv[i] : nullptr, d3 ? qx[i] : nullptr, d3 ? qy[i] : nullptr,
+                                 qz[i], B->streams[k % ns]);
+            }
         }
-        for (size_t k = 1; k < B->streams.size(); ++k) {
-            cudaEventRecord(B->events[k], B->streams[k]);
-            cudaStreamWaitEvent(cs, B->events[k], 0);
-        }
+        join();
         if (st == WP_OK) {
             const int tok = wp_prof_start(cs);
             gather_results_kernel<<<wp_cdiv(count, 128), 128, 0, cs>>>(B->d_out, B->d_slots, B->d_loops, B->d_max,
@@ -282,6 +362,17 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
         B->bound = ptrs;
         B->graph_launches = wp_launch_count() - launches0;
         wp_add_launches(-B->graph_launches);
+    }
+    if (B->mode == WP_BATCH_PERSISTENT) {
+        // test only: a withheld publication armed for this run (never inside a capture)
+        int at = -1;
+        unsigned long long lim = 0;
+        if (!wp_take_withhold(WP_WAIT_SITE_BATCH_PUBLISH, s, &at, &lim)) {
+            at = -1;
+            lim = 0;
+        }
+        wp_status ast;
+        if ((ast = wp_mg_pbatch_arm(B->pb, at, lim, s)) != WP_OK) return ast;
     }
     const int tok = wp_prof_start(s);
     wp_add_launches(B->graph_launches - 1);
@@ -340,9 +431,50 @@ extern "C" CUWHHD_API wp_status wp_batch_results(wp_batch* B, double* max_abs_di
     return WP_OK;
 }
 
+extern "C" CUWHHD_API wp_status wp_batch_set_mode(wp_batch* B, int mode, long long tile_cells) {
+    if (!B || (mode != WP_BATCH_GRAPH && mode != WP_BATCH_PERSISTENT) || tile_cells < 0 ||
+        tile_cells > (1LL << 30)) {
+        wp_set_error_msg("wp_batch_set_mode: mode WP_BATCH_GRAPH or WP_BATCH_PERSISTENT, 0 <= tile_cells <= 2^30");
+        return WP_ERR_INVALID_ARG;
+    }
+    wp_mg_pbatch* old = B->pb;
+    const long long old_cells = B->tile_cells;
+    B->pb = nullptr;
+    B->tile_cells = tile_cells;
+    if (mode == WP_BATCH_PERSISTENT) {
+        // checked now, so an unsupported batch fails here and keeps its mode
+        const wp_status st = build_pbatch(B);
+        if (st != WP_OK) {
+            B->pb = old;
+            B->tile_cells = old_cells;
+            return st;
+        }
+    }
+    if (old) wp_mg_pbatch_destroy(old);
+    B->mode = mode;
+    destroy_graph(B);
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_batch_profile(wp_batch* B, int enable, double* out, int cap, void* stream) {
+    if (!B || cap < 0 || (cap > 0 && !out)) {
+        wp_set_error_msg("wp_batch_profile: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (B->mode != WP_BATCH_PERSISTENT || !B->pb) {
+        wp_set_error_msg("wp_batch_profile: the batch is not in WP_BATCH_PERSISTENT mode");
+        return WP_ERR_UNSUPPORTED;
+    }
+    std::vector<unsigned long long> v(wp_mg_pbatch_prof_slots(), 0ull);
+    wp_status st = wp_mg_pbatch_profile(B->pb, enable, v.data(), (cudaStream_t)stream);
+    for (int k = 0; k < cap && k < (int)v.size(); ++k) out[k] = (double)v[k];
+    return st;
+}
+
 extern "C" CUWHHD_API wp_status wp_batch_destroy(wp_batch* B) {
     if (!B) return WP_OK;
     destroy_graph(B);
+    if (B->pb) wp_mg_pbatch_destroy(B->pb);
     for (auto& G : B->g) {
         if (G.mg3) wp_mgfrac3d_destroy(G.mg3);
         if (G.mg2) wp_mgfrac2d_destroy(G.mg2);

@@ -365,7 +365,7 @@ __device__ __forceinline__ void jacobi_q_body(T* __restrict__ dst, const T* __re
         for (int k = 0; k < 4; ++k)
             out.a[k] = dg.a[k] > (T)kEps ? ((T)1 - w) * c.a[k] + w * (fv.a[k] - od.a[k]) / dg.a[k] : (T)0;
         if (ACC) {
-            Q4<double> pv = ld4(p64 + i);
+            Q4<double> pv = ldq<CG>(p64 + i);
 #pragma unroll
             for (int k = 0; k < 4; ++k) pv.a[k] += (double)out.a[k];
             st4(p64 + i, pv);
@@ -973,21 +973,19 @@ __global__ void __launch_bounds__(256, 3) resid_restrict_qp_kernel(float* __rest
     cp_async_wait<0>();
 }
 
-// FP64 defect on quads (see defect64_z_kernel)
-template <typename TP>
-__global__ void __launch_bounds__(256, 2) defect64_q_kernel(float* __restrict__ r32, const TP* __restrict__ p,
-                                                         const float* __restrict__ f, Lvl<double> L, double m,
-                                                         const double* __restrict__ msum, double* __restrict__ acc,
-                                                         int zc) {
-    wp_pdl_enter();
+// FP64 defect on quads (see defect64_z_kernel): one thread's column of quads of block (bx, by);
+// returns its share of ||r||^2.  CG: p through L2 (see ldq).
+template <typename TP, bool CG = false>
+__device__ __forceinline__ double defect64_q_body(float* __restrict__ r32, const TP* __restrict__ p,
+                                                  const float* __restrict__ f, const Lvl<double>& L, double m, int zc,
+                                                  int bx, int by, int tid) {
     const int nq = L.ny >> 2;
-    const long q = (long)blockIdx.x * 256 + threadIdx.x;
-    const int z0 = blockIdx.y * zc, z1 = min(z0 + zc, L.nz);
-    if (msum) m = msum[0] / fmax(msum[1], 1.0);
+    const long q = (long)bx * 256 + tid;
+    const int z0 = by * zc, z1 = min(z0 + zc, L.nz);
     double s2 = 0.0;
     if (q < (long)L.nx * nq && z0 < z1) {
         const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
-        QCol<double, TP> col(L, p, x, y0, z0);
+        QCol<double, TP, CG> col(L, p, x, y0, z0);
         for (int z = z0; z < z1; ++z) {
             const long i = col.i;
             Q4<double> dg, od, c;
@@ -1003,6 +1001,17 @@ __global__ void __launch_bounds__(256, 2) defect64_q_kernel(float* __restrict__ 
             if (r32) st4(r32 + i, rr);
         }
     }
+    return s2;
+}
+
+template <typename TP>
+__global__ void __launch_bounds__(256, 2) defect64_q_kernel(float* __restrict__ r32, const TP* __restrict__ p,
+                                                         const float* __restrict__ f, Lvl<double> L, double m,
+                                                         const double* __restrict__ msum, double* __restrict__ acc,
+                                                         int zc) {
+    wp_pdl_enter();
+    if (msum) m = msum[0] / fmax(msum[1], 1.0);
+    double s2 = defect64_q_body<TP>(r32, p, f, L, m, zc, blockIdx.x, blockIdx.y, threadIdx.x);
     for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
     __shared__ double red[8];
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
@@ -1538,11 +1547,12 @@ struct LPack {
 };
 
 // shared floats a lean pack needs: per level v and t padded by a z plane on both sides, f, stencils
-inline long lean_smem_floats(const LPack& P) {
+// (cf_global: the stencils are read from global memory, not staged)
+inline long lean_smem_floats(const LPack& P, bool cf_global = false) {
     long s = 0;
     for (int l = 0; l < P.n; ++l) {
         const long c = (long)P.lv[l].nx * P.lv[l].ny * P.lv[l].nz, p = (long)P.lv[l].nx * P.lv[l].ny;
-        s += 2 * (c + 2 * p) + c + kCcf * c;
+        s += 2 * (c + 2 * p) + c + (cf_global ? 0 : kCcf * c);
     }
     return s;
 }
@@ -1672,12 +1682,16 @@ __device__ __forceinline__ void lean_prolong(const LS& F, const LS& C, int prolo
 // ping-pong state of a level after its sweeps (every thread swaps its own copy in lockstep).
 // The body, run by one 1024-thread CTA (also as the coarse phase of mid_cycle_kernel, whose other
 // CTAs wrote the pack's right-hand side in the same grid: hence the L2 load of f).
+// CFG: the stencils stay in global memory (read through L1) and only v, t, f are staged, for a CTA
+// that keeps its shared memory small (the persistent batch kernel).
+template <bool CFG = false>
 __device__ __forceinline__ void lean_cycle(const LPack& P, int nu1, int nu2, float w, int citers, int prolong,
                                            float* lean_smem) {
     __shared__ LS S[kCoarseMax];
     const int tid = threadIdx.x, B = blockDim.x;
     long cf_floats = 0;
-    for (int l = 0; l < P.n; ++l) cf_floats += (long)kCcf * P.lv[l].nx * P.lv[l].ny * P.lv[l].nz;
+    if (!CFG)
+        for (int l = 0; l < P.n; ++l) cf_floats += (long)kCcf * P.lv[l].nx * P.lv[l].ny * P.lv[l].nz;
     if (tid == 0) {
         long cfo = 0, off = cf_floats;
         for (int l = 0; l < P.n; ++l) {
@@ -1687,7 +1701,7 @@ __device__ __forceinline__ void lean_cycle(const LPack& P, int nu1, int nu2, flo
             q.nz = P.lv[l].nz;
             q.nxy = q.nx * q.ny;
             q.cells = q.nxy * q.nz;
-            q.cf = lean_smem + cfo;
+            q.cf = CFG ? P.lv[l].ccf : lean_smem + cfo;
             cfo += (long)kCcf * q.cells;
             q.v = lean_smem + off + q.nxy;
             off += q.cells + 2 * q.nxy;
@@ -1697,7 +1711,7 @@ __device__ __forceinline__ void lean_cycle(const LPack& P, int nu1, int nu2, flo
             off += q.cells;
         }
     }
-    {
+    if (!CFG) {
         // stencils: one flat 128-bit copy (every level's block is a multiple of 16 bytes)
         const float4* g = reinterpret_cast<const float4*>(P.lv[0].ccf);
         float4* d = reinterpret_cast<float4*>(lean_smem);
@@ -3888,6 +3902,776 @@ wp_status solve_mixed_loop_capture(wp_mgfrac3d* h, float* dst, const float* f, c
     WP_KERNEL("convert", 12.0 * n, s, convert_kernel<float, double><<<cb, 256, 0, s>>>(dst, h->p64, n));
     return WP_OK;
 }
+
+// ---- persistent batched solve ------------------------------------------------------------------
+// The mixed-precision tolerance solves of many grids in one persistent launch: one 1024-thread CTA
+// per SM takes work from a queue until every grid's solve has ended.  Each grid's solve is a
+// program of phases -- the launches of the launch-by-launch path: the active-cell sum with the FP64
+// iterate cleared, the first FP64 defect with the start test, then one refinement step (inner V(nu1,
+// nu2) cycles: first sweep from zero, sweeps, residual restriction, the single-CTA coarse cycle,
+// trilinear prolongation, and the last post-sweep adding to the FP64 iterate), the FP64 defect with
+// the stopping rule, and the FP32 copy of the solution.  The rule sends the program back to the
+// step or on to the copy.  A phase is cut into tiles of the quad kernels' 256-thread blocks, run by
+// the CTA's four 256-thread sub-blocks with every load of data written earlier in the launch taken
+// through L2; the coarse cycle is one tile for the whole CTA.  Per grid one 64-bit word {phase,
+// its tiles, next tile} hands out tiles (atomicAdd); the CTA that completes a phase's last tile
+// applies the stopping rule where the phase has one and publishes the next phase (atomicExch), so
+// grids advance independently and the small levels of one grid run beside the large levels of
+// another.  A CTA only waits for phases whose tiles running CTAs hold: nothing depends on every CTA
+// being resident.  Every wait is bounded (globaltimer); a CTA that gives up raises the error flag of
+// every unfinished grid and the batch's own flag, and the other CTAs leave when they see it.
+// The per-cell arithmetic is that of the quad kernels, so a grid's iterate is the one its own
+// launch-by-launch solve produces, up to the order of the FP64 norm and mean reductions.
+enum { PP_INIT = 0, PP_DEFECT, PP_SWEEP0, PP_SWEEP, PP_SWEEP_ACC, PP_RESTRICT, PP_PROLONG, PP_COARSE, PP_CONVERT };
+enum { PT_NONE = 0, PT_START = 1, PT_STEP = 2 };
+
+struct PPhase {
+    int type, level, zc, gx;
+    int nvb, per, ntiles, test;  // 256-thread blocks, blocks per tile (a multiple of 4), tiles, stopping rule
+    int cnx, cny, cnz, pack;     // coarse level extents (restriction, prolongation); coarse pack index
+    float* dst;
+    const float* src;
+    const float* f;
+};
+
+struct PGrid {
+    Lvl<float> L[kMaxLevels];
+    Lvl<double> L0;        // FP64 view of the finest level
+    const PPhase* ph;
+    const LPack* packs;
+    MgLoop* loop;          // the handle's loop state (cycles, steps, relative residual history)
+    double* acc;           // the handle's slots: ||r||^2, ||f||^2, sum of f over active cells, their count
+    int* err;              // the handle's device error flag
+    double* p64;
+    float* r32;
+    const float* f;        // finest right-hand side
+    float* dst;            // FP32 copy of the solution
+    int nph, loop_pc, end_pc, nu1, nu2, citers, prolong;
+    float w;
+};
+
+struct __align__(64) PState {
+    unsigned long long word;  // [63:48] phase, [47:32] its tiles, [31:0] next tile to hand out
+    int done;                 // tiles of the current phase completed
+    int finished;             // the grid's program has ended
+};
+
+struct PCtl {
+    int withhold;             // test only: >= 0, the completion of this phase of the first grid is not published
+    int prof;                 // 1: thread 0 of every CTA adds its cycles per activity to PArgs::prof
+    unsigned long long lim;   // wait limit, ns
+};
+// PArgs::prof slots: waiting for work, tiles taken, descriptor setup, completion/publication, then per
+// phase type its tile cycles and tiles
+constexpr int kProfSlots = 4 + 2 * 9;
+
+struct PArgs {
+    const PGrid* grids;       // costliest first: the order the CTAs look for work in
+    PState* st;
+    unsigned* fin;            // grids whose program has ended
+    int* err;                 // a CTA gave up waiting: the others leave too
+    const PCtl* ctl;
+    unsigned long long* prof;
+    int count;
+};
+
+__host__ __device__ inline unsigned long long pp_word(int pc, int ntiles, unsigned next) {
+    return ((unsigned long long)(unsigned)pc << 48) | ((unsigned long long)(unsigned)ntiles << 32) | next;
+}
+
+__global__ void pb_init_kernel(PArgs A, int max_cycles, int use_tol, double tol, int inner) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g == 0) {
+        *A.fin = 0u;
+        *A.err = 0;
+    }
+    if (g >= A.count) return;
+    const PGrid& G = A.grids[g];
+    for (int k = 0; k < 4; ++k) G.acc[k] = 0.0;
+    MgLoop* st = G.loop;
+    st->cycles = 0;
+    st->steps = 0;
+    st->max_cycles = max_cycles;
+    st->use_tol = use_tol;
+    st->inner = inner;
+    st->tol = tol;
+    st->rel = 0.0;
+    A.st[g].word = pp_word(0, G.ph[0].ntiles, 0u);
+    A.st[g].done = 0;
+    A.st[g].finished = 0;
+}
+
+// One attempt at a tile of grid k (lane-private): true with (phase, tile) when one was free.
+__device__ __forceinline__ bool pb_take(PState* S, int& pc, int& t) {
+    const unsigned long long o = atomicAdd(&S->word, 1ull);
+    if ((unsigned)(o & 0xffffffffu) >= (unsigned)((o >> 32) & 0xffffu)) return false;
+    pc = (int)(o >> 48);
+    t = (int)(o & 0xffffffffu);
+    return true;
+}
+
+// A tile of some grid's current phase, looked for by the 32 lanes of warp 0 together: first the grid
+// the CTA worked on last (pref), then every grid's word loaded at once, one per lane, and the first
+// grid (in the costliest-first order) with a free tile taken.  Returns the grid or -1.
+__device__ __forceinline__ int pb_grab(const PArgs& A, int pref, int& pc, int& t) {
+    const int lane = threadIdx.x & 31;
+    int got = 0;
+    if (pref >= 0) {
+        if (lane == 0) got = pb_take(A.st + pref, pc, t) ? 1 : 0;
+        if (__shfl_sync(0xffffffffu, got, 0)) {
+            pc = __shfl_sync(0xffffffffu, pc, 0);
+            t = __shfl_sync(0xffffffffu, t, 0);
+            return pref;
+        }
+    }
+    for (int base = 0; base < A.count; base += 32) {
+        const int k = base + lane;
+        bool free = false;
+        if (k < A.count) {
+            const unsigned long long w = *reinterpret_cast<volatile unsigned long long*>(&A.st[k].word);
+            free = (unsigned)(w & 0xffffffffu) < (unsigned)((w >> 32) & 0xffffu);
+        }
+        for (unsigned m = __ballot_sync(0xffffffffu, free); m; m &= m - 1) {
+            const int lead = __ffs(m) - 1;
+            if (lane == lead) got = pb_take(A.st + k, pc, t) ? 1 : 0;
+            if (__shfl_sync(0xffffffffu, got, lead)) {
+                pc = __shfl_sync(0xffffffffu, pc, lead);
+                t = __shfl_sync(0xffffffffu, t, lead);
+                return base + lead;
+            }
+        }
+    }
+    return -1;
+}
+
+// the stopping rule after a defect (mg_loop_start_kernel / mg_loop_check_kernel); true: one more step
+__device__ bool pb_test(const PGrid& G, int test) {
+    double nf2 = __ldcg(G.acc + 1);
+    if (!(nf2 > 0.0)) nf2 = 1.0;
+    const double rel = sqrt(__ldcg(G.acc) / nf2);
+    volatile MgLoop* st = G.loop;
+    st->rel = rel;
+    if (test == PT_START) return !(st->use_tol && rel <= st->tol) && st->max_cycles > 0 && isfinite(rel);
+    const int k = st->steps, c = st->cycles + st->inner;
+    if (k < 64) st->hist[k] = rel;
+    st->steps = k + 1;
+    st->cycles = c;
+    return !(st->use_tol && rel <= st->tol) && c < st->max_cycles && isfinite(rel);
+}
+
+// thread 0, after the CTA finished tile work of (g, pc)
+__device__ void pb_complete(const PArgs& A, int g, int pc) {
+    const PGrid& G = A.grids[g];
+    PState* S = A.st + g;
+    const PPhase& P = G.ph[pc];
+    __threadfence();
+    if (atomicAdd(&S->done, 1) + 1 != P.ntiles) return;
+    atomicExch(&S->done, 0);
+    if (g == 0 && pc == A.ctl->withhold) return;  // test only: the next phase is never published
+    int npc = pc + 1;
+    if (P.test != PT_NONE) npc = pb_test(G, P.test) ? G.loop_pc : G.end_pc;
+    if (npc >= G.nph) {
+        atomicExch(&S->finished, 1);
+        __threadfence();
+        atomicAdd(A.fin, 1u);
+        return;
+    }
+    const PPhase& N = G.ph[npc];
+    if (N.type == PP_DEFECT) atomicExch(reinterpret_cast<unsigned long long*>(G.acc), 0ull);
+    __threadfence();
+    atomicExch(&S->word, pp_word(npc, N.ntiles, 0u));
+}
+
+// a wait ran out: every grid still running reports it, and the other CTAs leave
+__device__ void pb_give_up(const PArgs& A) {
+    atomicOr(A.err, 2);
+    for (int k = 0; k < A.count; ++k)
+        if (*reinterpret_cast<volatile int*>(&A.st[k].finished) == 0) atomicOr(A.grids[k].err, 2);
+}
+
+// sum of v over the CTA's 32 warps, added to *out by thread 0
+__device__ __forceinline__ void pb_cta_sum(double v, double* out, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < 32; ++k) t += red[k];
+        atomicAdd(out, t);
+    }
+    __syncthreads();
+}
+
+// The work of one tile, one function per phase type (each with its own register allocation: the
+// persistent kernel's 1024 threads leave 64 registers a thread).  vb0 .. v1 - 1: the tile's blocks.
+__device__ __noinline__ void pb_sweep0(const PPhase& Ps, const Lvl<float>& Ls, float w, int vb0, int v1, int tid) {
+    const PPhase P = Ps;
+    const Lvl<float> L = Ls;
+    for (int vb = vb0; vb < v1; vb += 4) jacobi0_q_body<float, true>(P.dst, P.f, L, w, P.zc, vb % P.gx, vb / P.gx, tid);
+}
+__device__ __noinline__ void pb_sweep(const PPhase& Ps, const Lvl<float>& Ls, float w, int vb0, int v1, int tid) {
+    const PPhase P = Ps;
+    const Lvl<float> L = Ls;
+    for (int vb = vb0; vb < v1; vb += 4)
+        jacobi_q_body<float, false, true>(P.dst, P.src, P.f, L, w, P.zc, nullptr, vb % P.gx, vb / P.gx, tid);
+}
+__device__ __noinline__ void pb_sweep_acc(const PPhase& Ps, const Lvl<float>& Ls, float w, double* p64, int vb0,
+                                          int v1, int tid) {
+    const PPhase P = Ps;
+    const Lvl<float> L = Ls;
+    for (int vb = vb0; vb < v1; vb += 4)
+        jacobi_q_body<float, true, true>(nullptr, P.src, P.f, L, w, P.zc, p64, vb % P.gx, vb / P.gx, tid);
+}
+__device__ __noinline__ void pb_restrict(const PPhase& Ps, const Lvl<float>& Ls, int vb0, int v1, int tid) {
+    const PPhase P = Ps;
+    const Lvl<float> L = Ls;
+    for (int vb = vb0; vb < v1; vb += 4)
+        resid_restrict_q_body<float, true>(P.dst, P.src, P.f, L, P.cnx, P.cny, P.cnz, P.zc, vb % P.gx, vb / P.gx, tid);
+}
+__device__ __noinline__ void pb_prolong(const PPhase& Ps, const Lvl<float>& Ls, int vb0, int v1, int tid) {
+    const PPhase P = Ps;
+    const Lvl<float> L = Ls;
+    for (int vb = vb0; vb < v1; vb += 4)
+        prolong_tri_q_body<float, true>(P.dst, P.src, L.nx, L.ny, L.nz, P.cnx, P.cny, P.cnz, vb % P.gx, vb / P.gx, tid);
+}
+__device__ __noinline__ void pb_coarse(const LPack& Q, const PGrid& G, float* lean_smem) {
+    lean_cycle<true>(Q, G.nu1, G.nu2, G.w, G.citers, G.prolong, lean_smem);
+}
+// active-cell sum and count of f (active_sum_q_kernel), ||f||^2 (sumsq_kernel), p64 = 0
+__device__ __noinline__ void pb_init(const PPhase& Ps, const Lvl<double>& Ls, const float* f, double* p64, int vb0,
+                                     int v1, int tid, double* out) {
+    const PPhase P = Ps;
+    const Lvl<double> L = Ls;
+    double sf = 0.0, cnt = 0.0, sq = 0.0;
+    const int nq = L.ny >> 2;
+    for (int vb = vb0; vb < v1; vb += 4) {
+        const long q = (long)(vb % P.gx) * 256 + tid;
+        const int z0 = (vb / P.gx) * P.zc, z1 = min(z0 + P.zc, L.nz);
+        if (q >= (long)L.nx * nq || z0 >= z1) continue;
+        const int x = (int)(q / nq), y0 = (int)(q - (long)x * nq) * 4;
+        QCol<double, float> col(L, f, x, y0, z0);
+        for (int z = z0; z < z1; ++z) {
+            const long i = col.i;
+            Q4<double> dg, od, c;
+            col.step(dg, od, c);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (dg.a[k] > kEps) { sf += c.a[k]; cnt += 1.0; }
+                sq += c.a[k] * c.a[k];
+            }
+            st4(p64 + i, zero4<double>());
+        }
+    }
+    out[0] = sf;
+    out[1] = cnt;
+    out[2] = sq;
+}
+__device__ __noinline__ double pb_defect(const PPhase& Ps, const Lvl<double>& Ls, const PGrid& G, double m, int vb0,
+                                         int v1, int tid) {
+    const PPhase P = Ps;
+    const Lvl<double> L = Ls;
+    float* const r32 = G.r32;
+    const double* const p64 = G.p64;
+    const float* const f = G.f;
+    double s2 = 0.0;
+    for (int vb = vb0; vb < v1; vb += 4)
+        s2 += defect64_q_body<double, true>(r32, p64, f, L, m, P.zc, vb % P.gx, vb / P.gx, tid);
+    return s2;
+}
+
+__global__ void __launch_bounds__(1024, 1) batch_persist_kernel(PArgs A) {
+    extern __shared__ __align__(16) float lean_smem[];
+    __shared__ Lvl<float> sL;
+    __shared__ Lvl<double> sD;
+    __shared__ PPhase sP;
+    __shared__ double red[32];
+    __shared__ int job[3];
+    const int sub = threadIdx.x >> 8, tid = threadIdx.x & 255;
+    int last = -1;  // the grid of the CTA's previous tile (warp 0)
+    const bool prof = A.ctl->prof != 0;
+    long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;  // thread 0: cycle stamps of one tile's stages
+    for (;;) {
+        if (threadIdx.x < 32) {
+            int g = -1, pc = 0, t = 0;
+            if (prof && threadIdx.x == 0) c0 = clock64();
+            const unsigned long long t0 = wptc::globaltimer();
+            for (;;) {
+                if (*reinterpret_cast<volatile int*>(A.err) != 0) break;
+                if ((g = pb_grab(A, last, pc, t)) >= 0) break;
+                if (*reinterpret_cast<volatile unsigned*>(A.fin) >= (unsigned)A.count) break;
+                int out = 0;
+                if (threadIdx.x == 0 && wptc::globaltimer() - t0 > A.ctl->lim) {
+                    pb_give_up(A);
+                    out = 1;
+                }
+                if (__shfl_sync(0xffffffffu, out, 0)) break;
+                __nanosleep(128);
+            }
+            last = g;
+            if (threadIdx.x == 0) {
+                if (prof) {
+                    c1 = clock64();
+                    atomicAdd(A.prof + 0, (unsigned long long)(c1 - c0));
+                    if (g >= 0) atomicAdd(A.prof + 1, 1ull);
+                }
+                job[0] = g;
+                job[1] = pc;
+                job[2] = t;
+                __threadfence();
+            }
+        }
+        __syncthreads();
+        const int g = job[0];
+        if (g < 0) return;
+        const int pc = job[1], t = job[2];
+        const PGrid& G = A.grids[g];
+        {
+            const PPhase* gp = G.ph + pc;
+            constexpr int nP = sizeof(PPhase) / 4, nL = sizeof(Lvl<float>) / 4, nD = sizeof(Lvl<double>) / 4;
+            static_assert(nP <= 64 && nL <= 64 && nD <= 64, "descriptor copy: one word per thread");
+            const int lev = gp->level;
+            if (threadIdx.x < nP)
+                reinterpret_cast<unsigned*>(&sP)[threadIdx.x] = reinterpret_cast<const unsigned*>(gp)[threadIdx.x];
+            else if (threadIdx.x >= 64 && threadIdx.x < 64 + nL)
+                reinterpret_cast<unsigned*>(&sL)[threadIdx.x - 64] =
+                    reinterpret_cast<const unsigned*>(&G.L[lev])[threadIdx.x - 64];
+            else if (threadIdx.x >= 128 && threadIdx.x < 128 + nD)
+                reinterpret_cast<unsigned*>(&sD)[threadIdx.x - 128] =
+                    reinterpret_cast<const unsigned*>(&G.L0)[threadIdx.x - 128];
+        }
+        __syncthreads();
+        if (prof && threadIdx.x == 0) c2 = clock64();
+        const int type = sP.type;
+        const int vb0 = sP.per * t + sub, v1 = min(sP.per * (t + 1), sP.nvb);
+        switch (type) {
+            case PP_COARSE: pb_coarse(G.packs[sP.pack], G, lean_smem); break;
+            case PP_INIT: {
+                double o[3];
+                pb_init(sP, sD, G.f, G.p64, vb0, v1, tid, o);
+                pb_cta_sum(o[0], G.acc + 2, red);
+                pb_cta_sum(o[1], G.acc + 3, red);
+                pb_cta_sum(o[2], G.acc + 1, red);
+                break;
+            }
+            case PP_DEFECT: {
+                const double m = __ldcg(G.acc + 2) / fmax(__ldcg(G.acc + 3), 1.0);
+                pb_cta_sum(pb_defect(sP, sD, G, m, vb0, v1, tid), G.acc, red);
+                break;
+            }
+            case PP_CONVERT: {
+                const long n = (long)sL.nx * sL.ny * sL.nz;
+                for (int vb = vb0; vb < v1; vb += 4) {
+                    const long i = (long)vb * 1024 + 4L * tid;
+                    if (i < n) st4(G.dst + i, cvt4<float>(ldq<true>(G.p64 + i)));
+                }
+                break;
+            }
+            case PP_SWEEP0: pb_sweep0(sP, sL, G.w, vb0, v1, tid); break;
+            case PP_SWEEP: pb_sweep(sP, sL, G.w, vb0, v1, tid); break;
+            case PP_SWEEP_ACC: pb_sweep_acc(sP, sL, G.w, G.p64, vb0, v1, tid); break;
+            case PP_RESTRICT: pb_restrict(sP, sL, vb0, v1, tid); break;
+            default: pb_prolong(sP, sL, vb0, v1, tid); break;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (prof) c3 = clock64();
+            pb_complete(A, g, pc);
+            if (prof) {
+                atomicAdd(A.prof + 2, (unsigned long long)(c2 - c1));
+                atomicAdd(A.prof + 3, (unsigned long long)(clock64() - c3));
+                atomicAdd(A.prof + 4 + 2 * type, (unsigned long long)(c3 - c2));
+                atomicAdd(A.prof + 5 + 2 * type, 1ull);
+            }
+        }
+    }
+}
+
+// The tiles of a phase: nvb blocks of cells_vb cells, about `target` cells per tile (a multiple of
+// four blocks, one per sub-block), at least one tile, at most 65535.
+void pp_tiles(PPhase& q, long nvb, long cells_vb, long target) {
+    long per = (target + cells_vb - 1) / cells_vb;
+    per = std::max(4L, (per + 3) / 4 * 4);
+    long nt = (nvb + per - 1) / per;
+    while (nt > 65535) {
+        per *= 2;
+        nt = (nvb + per - 1) / per;
+    }
+    q.nvb = (int)nvb;
+    q.per = (int)per;
+    q.ntiles = (int)std::max(1L, nt);
+}
+
+// One grid's program (PGrid's phases and coarse packs), built by mirroring the buffer swaps of the
+// launch-by-launch cycle on copies of the level pointers (the handle is not changed).
+struct PBuild {
+    wp_mgfrac3d* h;
+    int nu1, nu2, lc;
+    long target;
+    float* v[kMaxLevels];
+    float* t[kMaxLevels];
+    std::vector<PPhase> ph;
+    std::vector<LPack> packs;
+
+    PPhase base(int type, int l) const {
+        PPhase q;
+        memset(&q, 0, sizeof(q));
+        q.type = type;
+        q.level = l;
+        return q;
+    }
+    static int zc_of(const Level& L) { return std::max(1, std::min(L.n[2], 8)); }
+    static long quads(const Level& L) { return (long)wp_cdiv((size_t)L.n[0] * (L.n[1] / 4), 256); }
+    // a finest-level column phase (INIT, DEFECT) on the quad tiling
+    void column(int type, int test) {
+        const Level& L = h->lv[0];
+        PPhase q = base(type, 0);
+        q.zc = zc_of(L);
+        q.gx = (int)quads(L);
+        q.test = test;
+        pp_tiles(q, q.gx * (long)wp_cdiv(L.n[2], q.zc), 1024L * q.zc, target);
+        ph.push_back(q);
+    }
+    void cycle(int l, const float* f, bool clear, bool acc) {
+        if (l == lc) {
+            LPack Q;
+            memset(&Q, 0, sizeof(Q));
+            Q.n = h->nl - lc;
+            for (int k = 0; k < Q.n; ++k) {
+                Level& E = h->lv[lc + k];
+                Q.lv[k] = {E.n[0], E.n[1], E.n[2], E.ccf, v[lc + k], t[lc + k], E.f};
+            }
+            PPhase q = base(PP_COARSE, l);
+            q.pack = (int)packs.size();
+            q.nvb = q.per = q.ntiles = 1;
+            packs.push_back(Q);
+            ph.push_back(q);
+            for (int k = 0; k < Q.n; ++k) {
+                const int swaps = (k == Q.n - 1) ? h->coarsest_iters : nu1 + nu2;
+                if (swaps & 1) std::swap(v[lc + k], t[lc + k]);
+            }
+            return;
+        }
+        const Level& L = h->lv[l];
+        const Level& C = h->lv[l + 1];
+        const int zc = zc_of(L);
+        const long gx = quads(L);
+        auto sweep = [&](int type) {
+            PPhase q = base(type, l);
+            q.zc = zc;
+            q.gx = (int)gx;
+            q.dst = type == PP_SWEEP_ACC ? nullptr : t[l];
+            q.src = v[l];
+            q.f = f;
+            pp_tiles(q, gx * (long)wp_cdiv(L.n[2], zc), 1024L * zc, target);
+            ph.push_back(q);
+            std::swap(v[l], t[l]);
+        };
+        int pre = nu1;
+        if (clear) {
+            sweep(PP_SWEEP0);
+            pre = nu1 - 1;
+        }
+        for (int k = 0; k < pre; ++k) sweep(PP_SWEEP);
+        {
+            const int czc = std::max(1, zc / 2);
+            PPhase q = base(PP_RESTRICT, l);
+            q.zc = czc;
+            q.gx = (int)wp_cdiv((size_t)C.n[0] * (L.n[1] / 4) * 2, 256);
+            q.dst = C.f;
+            q.src = v[l];
+            q.f = f;
+            q.cnx = C.n[0];
+            q.cny = C.n[1];
+            q.cnz = C.n[2];
+            pp_tiles(q, q.gx * (long)wp_cdiv(C.n[2], czc), 2048L * czc, target);
+            ph.push_back(q);
+        }
+        cycle(l + 1, C.f, true, false);
+        {
+            PPhase q = base(PP_PROLONG, l);
+            q.gx = (int)gx;
+            q.dst = v[l];
+            q.src = v[l + 1];
+            q.cnx = C.n[0];
+            q.cny = C.n[1];
+            q.cnz = C.n[2];
+            pp_tiles(q, gx * (long)L.n[2], 1024L, target);
+            ph.push_back(q);
+        }
+        for (int k = 0; k < nu2; ++k) sweep(acc && k == nu2 - 1 ? PP_SWEEP_ACC : PP_SWEEP);
+    }
+};
+
+// Whether handle h can run its mixed solve as a persistent program (quad levels with aligned work
+// arrays down to a lean coarse pack that fits the CTA's shared memory): the pack's first level, its
+// shared bytes, or -1 with a message.
+int persist_plan(wp_mgfrac3d* h, const wp_mg_params* prm, size_t smem_cap, size_t* lean_bytes, const char** why) {
+    *why = nullptr;
+    if (prm->prolongation != WP_PROLONG_TRILINEAR || prm->nu1 < 1 || prm->nu2 < 1 || prm->start == WP_START_FMG) {
+        *why = "the persistent batch runs trilinear V(nu1, nu2) cycles with nu1, nu2 >= 1 from a zero start";
+        return -1;
+    }
+    if (!h->p64 || !h->r32 || !h->loop_state) {
+        *why = "mixed-precision work arrays not prepared";
+        return -1;
+    }
+    int lc = -1;
+    for (int l = 1; l < h->nl - 1 && lc < 0; ++l) {
+        long pack = 0;
+        for (int k = l; k < h->nl; ++k) pack += h->lv[k].cells;
+        if (h->lv[l].cells <= kCoarseCells && h->nl - l <= kCoarseMax && pack <= kCoarseSmemCells) lc = l;
+    }
+    if (lc < 1) {
+        *why = "a grid has no coarse level of at most 4096 cells for the single-CTA coarse cycle";
+        return -1;
+    }
+    for (int l = 0; l < lc; ++l) {
+        const Level& L = h->lv[l];
+        const Level& C = h->lv[l + 1];
+        if (!quad_ok(L) || C.n[1] * 2 != L.n[1] || !al16(L.v) || !al16(L.t) || (l > 0 && !al16(L.f)) ||
+            !al16(h->r32) || !al16(h->p64)) {
+            *why = "a level above the coarse pack has a y extent that is not a multiple of 4 (or is not halved)";
+            return -1;
+        }
+    }
+    LPack Q;
+    Q.n = h->nl - lc;
+    for (int k = 0; k < Q.n; ++k) {
+        const Level& E = h->lv[lc + k];
+        if (!E.ccf) {
+            *why = "a coarse level has no precomputed stencils";
+            return -1;
+        }
+        Q.lv[k] = {E.n[0], E.n[1], E.n[2], E.ccf, E.v, E.t, E.f};
+    }
+    *lean_bytes = sizeof(float) * (size_t)lean_smem_floats(Q, true);
+    if (*lean_bytes > smem_cap) {
+        *why = "a grid's coarse pack does not fit the persistent CTA's shared memory";
+        return -1;
+    }
+    return lc;
+}
+
+// Builds handle h's program into ph / packs and fills its descriptor (device pointers of the
+// program arrays are set by the caller).
+void persist_program(wp_mgfrac3d* h, const wp_mg_params* prm, float* dst, const float* f, long target, int lc,
+                     PGrid* G, std::vector<PPhase>& ph, std::vector<LPack>& packs) {
+    PBuild b;
+    b.h = h;
+    b.nu1 = prm->nu1;
+    b.nu2 = prm->nu2;
+    b.lc = lc;
+    b.target = target;
+    for (int l = 0; l < h->nl; ++l) {
+        b.v[l] = h->lv[l].v;
+        b.t[l] = h->lv[l].t;
+    }
+    b.column(PP_INIT, PT_NONE);
+    b.column(PP_DEFECT, PT_START);
+    const int loop_pc = (int)b.ph.size();
+    const int inner = inner_of(prm);
+    for (int j = 0; j < inner; ++j) b.cycle(0, h->r32, j == 0, j == inner - 1);
+    b.column(PP_DEFECT, PT_STEP);
+    const int end_pc = (int)b.ph.size();
+    {
+        PPhase q = b.base(PP_CONVERT, 0);
+        pp_tiles(q, (long)wp_cdiv(h->lv[0].cells, 1024), 1024L, target);
+        b.ph.push_back(q);
+    }
+    memset(G, 0, sizeof(*G));
+    for (int l = 0; l <= lc; ++l) G->L[l] = view<float>(h->lv[l]);
+    G->L0 = view<double>(h->lv[0]);
+    G->loop = reinterpret_cast<MgLoop*>(h->loop_state);
+    G->acc = h->acc;
+    G->err = reinterpret_cast<int*>(h->acc + 4);
+    G->p64 = h->p64;
+    G->r32 = h->r32;
+    G->f = f;
+    G->dst = dst;
+    G->nph = (int)b.ph.size();
+    G->loop_pc = loop_pc;
+    G->end_pc = end_pc;
+    G->nu1 = prm->nu1;
+    G->nu2 = prm->nu2;
+    G->citers = h->coarsest_iters;
+    G->prolong = prm->prolongation;
+    G->w = (float)prm->omega;
+    ph.swap(b.ph);
+    packs.swap(b.packs);
+}
+
+}  // namespace
+
+// Many handles' mixed solves as one persistent launch (see batch_persist_kernel).
+struct wp_mg_pbatch {
+    int count = 0;
+    PGrid* d_grids = nullptr;
+    PState* d_st = nullptr;
+    unsigned* d_fin = nullptr;  // then the batch's error flag (the int after it)
+    PCtl* d_ctl = nullptr;
+    PCtl ctl{-1, 0, 0};         // the control block's value on the device
+    unsigned long long* d_prof = nullptr;  // kProfSlots counters (see PCtl::prof)
+    std::vector<void*> blobs;   // per grid: phases, then coarse packs
+    size_t smem = 0;
+    int grid = 0;
+    wp_mg_params prm;
+    long target = 0;
+    long long tiles = 0;        // tiles of one pass of every grid's program (report)
+};
+
+namespace {
+
+void pbatch_free(wp_mg_pbatch* pb) {
+    for (void* p : pb->blobs) cudaFree(p);
+    if (pb->d_grids) cudaFree(pb->d_grids);
+    if (pb->d_st) cudaFree(pb->d_st);
+    if (pb->d_fin) cudaFree(pb->d_fin);
+    if (pb->d_ctl) cudaFree(pb->d_ctl);
+    if (pb->d_prof) cudaFree(pb->d_prof);
+    delete pb;
+}
+
+}  // namespace
+
+// Builds the persistent program of every handle (hs[i] solves f[i] into dst[i] and its FP64 iterate;
+// the mixed work arrays prepared).  The CTAs look for work in the order given.  target_cells:
+// cells per tile (0 = 32768).  WP_ERR_UNSUPPORTED when a handle's levels do not fit the program.
+wp_status wp_mg_pbatch_create(wp_mg_pbatch** out, wp_mgfrac3d* const* hs, float* const* dst, const float* const* f,
+                              int count, const wp_mg_params* prm, long target_cells) {
+    *out = nullptr;
+    if (count < 1 || !hs || !dst || !f || !prm) {
+        wp_set_error_msg("persistent batch: bad arguments");
+        return WP_ERR_INVALID_ARG;
+    }
+    cudaFuncAttributes fa;
+    WP_CUDA_TRY(cudaFuncGetAttributes(&fa, batch_persist_kernel));
+    int dev = 0, optin = 0;
+    WP_CUDA_TRY(cudaGetDevice(&dev));
+    WP_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t cap = (size_t)optin > fa.sharedSizeBytes + 1024 ? (size_t)optin - fa.sharedSizeBytes - 1024 : 0;
+    wp_mg_pbatch* pb = new (std::nothrow) wp_mg_pbatch();
+    if (!pb) return WP_ERR_INVALID_ARG;
+    pb->count = count;
+    pb->prm = *prm;
+    pb->target = target_cells > 0 ? target_cells : 32768;
+    std::vector<PGrid> G(count);
+    wp_status st = WP_OK;
+    for (int i = 0; i < count && st == WP_OK; ++i) {
+        size_t lean = 0;
+        const char* why = nullptr;
+        const int lc = persist_plan(hs[i], prm, cap, &lean, &why);
+        if (lc < 0) {
+            wp_set_error_msg(why);
+            st = WP_ERR_UNSUPPORTED;
+            break;
+        }
+        pb->smem = std::max(pb->smem, lean);
+        std::vector<PPhase> ph;
+        std::vector<LPack> packs;
+        persist_program(hs[i], prm, dst[i], f[i], pb->target, lc, &G[i], ph, packs);
+        hs[i]->last64 = 1;  // the FP64 iterate of the last solve is p64
+        for (const PPhase& q : ph) pb->tiles += q.ntiles;
+        const size_t bph = sizeof(PPhase) * ph.size(), bpk = sizeof(LPack) * packs.size();
+        const size_t off = (bph + 255) / 256 * 256;
+        void* blob = nullptr;
+        cudaError_t e = cudaMalloc(&blob, off + bpk + 16);
+        if (e == cudaSuccess) {
+            pb->blobs.push_back(blob);
+            e = cudaMemcpy(blob, ph.data(), bph, cudaMemcpyHostToDevice);
+        }
+        if (e == cudaSuccess && bpk) e = cudaMemcpy((char*)blob + off, packs.data(), bpk, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            wp_set_cuda_error(e, "persistent batch programs", __FILE__, __LINE__);
+            st = WP_ERR_CUDA;
+            break;
+        }
+        G[i].ph = reinterpret_cast<const PPhase*>(blob);
+        G[i].packs = reinterpret_cast<const LPack*>((char*)blob + off);
+    }
+    if (st == WP_OK) {
+        cudaError_t e = cudaMalloc((void**)&pb->d_grids, sizeof(PGrid) * count);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&pb->d_st, sizeof(PState) * count);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&pb->d_fin, 2 * sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&pb->d_ctl, sizeof(PCtl));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&pb->d_prof, sizeof(unsigned long long) * kProfSlots);
+        if (e == cudaSuccess) e = cudaMemset(pb->d_prof, 0, sizeof(unsigned long long) * kProfSlots);
+        if (e == cudaSuccess) e = cudaMemcpy(pb->d_grids, G.data(), sizeof(PGrid) * count, cudaMemcpyHostToDevice);
+        pb->ctl.withhold = -1;
+        pb->ctl.lim = wptc::kWaitLimitNs;
+        if (e == cudaSuccess) e = cudaMemcpy(pb->d_ctl, &pb->ctl, sizeof(PCtl), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(batch_persist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)pb->smem);
+        int per_sm = 0;
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persist_kernel, 1024, pb->smem);
+        if (e != cudaSuccess) {
+            wp_set_cuda_error(e, "persistent batch setup", __FILE__, __LINE__);
+            st = WP_ERR_CUDA;
+        } else if (per_sm < 1) {
+            wp_set_error_msg("persistent batch: a 1024-thread CTA with the coarse pack's shared memory does not fit an SM");
+            st = WP_ERR_UNSUPPORTED;
+        }
+        pb->grid = wp_sm_count();
+    }
+    if (st != WP_OK) {
+        pbatch_free(pb);
+        return st;
+    }
+    *out = pb;
+    return WP_OK;
+}
+
+// Test only: the next launches withhold the publication that follows phase `at` of the first grid
+// (at < 0: none), and every wait of the launch gives up after limit_ns.  Enqueued on s.
+wp_status wp_mg_pbatch_arm(wp_mg_pbatch* pb, int at, unsigned long long limit_ns, cudaStream_t s) {
+    const PCtl c{at, pb->ctl.prof, limit_ns ? limit_ns : wptc::kWaitLimitNs};
+    if (c.withhold == pb->ctl.withhold && c.lim == pb->ctl.lim) return WP_OK;
+    pb->ctl = c;
+    WP_CUDA_TRY(cudaMemcpyAsync(pb->d_ctl, &pb->ctl, sizeof(PCtl), cudaMemcpyHostToDevice, s));
+    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    return WP_OK;
+}
+
+// The persistent kernel's activity counters: enable 1 clears them and switches the counting on for
+// the following launches, 0 switches it off; out (may be NULL) receives the kProfSlots sums so far.
+wp_status wp_mg_pbatch_profile(wp_mg_pbatch* pb, int enable, unsigned long long* out, cudaStream_t s) {
+    WP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (out) WP_CUDA_TRY(cudaMemcpy(out, pb->d_prof, sizeof(unsigned long long) * kProfSlots, cudaMemcpyDeviceToHost));
+    if (enable) WP_CUDA_TRY(cudaMemset(pb->d_prof, 0, sizeof(unsigned long long) * kProfSlots));
+    if ((enable != 0) != (pb->ctl.prof != 0)) {
+        pb->ctl.prof = enable != 0;
+        WP_CUDA_TRY(cudaMemcpy(pb->d_ctl, &pb->ctl, sizeof(PCtl), cudaMemcpyHostToDevice));
+    }
+    return WP_OK;
+}
+int wp_mg_pbatch_prof_slots() { return kProfSlots; }
+
+// The loop state and slots initialised, then the persistent kernel (two launches, capturable).
+wp_status wp_mg_pbatch_launch(wp_mg_pbatch* pb, cudaStream_t s) {
+    PArgs A;
+    A.grids = pb->d_grids;
+    A.st = pb->d_st;
+    A.fin = pb->d_fin;
+    A.err = reinterpret_cast<int*>(pb->d_fin + 1);
+    A.ctl = pb->d_ctl;
+    A.prof = pb->d_prof;
+    A.count = pb->count;
+    const wp_mg_params& p = pb->prm;
+    WP_KERNEL("batch_persist_init", 0.0, s,
+              pb_init_kernel<<<wp_cdiv(pb->count, 128), 128, 0, s>>>(A, p.max_cycles, p.rel_tol > 0.0 ? 1 : 0, p.rel_tol,
+                                                                     inner_of(&p)));
+    WP_KERNEL("batch_persistent", 0.0, s, batch_persist_kernel<<<pb->grid, 1024, pb->smem, s>>>(A));
+    return WP_OK;
+}
+
+long long wp_mg_pbatch_tiles(const wp_mg_pbatch* pb) { return pb->tiles; }
+size_t wp_mg_pbatch_smem(const wp_mg_pbatch* pb) { return pb->smem; }
+
+void wp_mg_pbatch_destroy(wp_mg_pbatch* pb) {
+    if (pb) pbatch_free(pb);
+}
+
+namespace {
 
 wp_status residual_rel(wp_mgfrac3d* h, const float* v, const float* f, double* rel, cudaStream_t s) {
     if (!h || !v || !f || !rel) { wp_set_error_msg("wp_mgfrac_residual: null pointer"); return WP_ERR_INVALID_ARG; }

@@ -56,8 +56,8 @@ bool wp_take_withhold(int site, cudaStream_t s, int* at, unsigned long long* lim
 }
 
 extern "C" CUWHHD_API wp_status wp_debug_withhold_wait(int site, int at, double limit_seconds) {
-    if (site < 0 || site > WP_WAIT_SITE_CONV_PIPELINE || at < 0 || !(limit_seconds >= 1e-6 && limit_seconds <= 2.0)) {
-        wp_set_error_msg("wp_debug_withhold_wait: site 0..2, at >= 0, limit in [1e-6, 2] s");
+    if (site < 0 || site > WP_WAIT_SITE_BATCH_PUBLISH || at < 0 || !(limit_seconds >= 1e-6 && limit_seconds <= 2.0)) {
+        wp_set_error_msg("wp_debug_withhold_wait: site 0..3, at >= 0, limit in [1e-6, 2] s");
         return WP_ERR_INVALID_ARG;
     }
     std::lock_guard<std::mutex> lk(g_wh_mu);
