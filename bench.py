@@ -423,6 +423,7 @@ def run_batch(args, rank, world, local_rank):
     bp = api.BatchProjector(grids, rel_tol=args.batch_tol, max_cycles=80, nstreams=args.nstreams,
                             persistent=persistent, tile_cells=args.batch_tile)
     cycles = bp.plan(u)
+    mode_info = bp.get_mode()
     stream = torch.cuda.current_stream()
     count = len(grids)
 
@@ -479,6 +480,9 @@ def run_batch(args, rank, world, local_rank):
     # the other way of running the solves, same grids and inputs, for comparison
     other = api.BATCH_GRAPH if persistent else api.BATCH_PERSISTENT
     bp.set_mode(other, args.batch_tile)
+    if not persistent:
+        bp.plan(u)  # orders the programs and, with --batch-tile 0, tunes the persistent tile
+    pers_mode = bp.get_mode() if not persistent else None
     for _ in range(2):
         step()
     torch.cuda.synchronize()
@@ -490,7 +494,8 @@ def run_batch(args, rank, world, local_rank):
     torch.cuda.synchronize()
     other_ms = o0.elapsed_time(o1) / args.steps
     ores = bp.results()
-    bp.set_mode(api.BATCH_PERSISTENT if persistent else api.BATCH_GRAPH, args.batch_tile)
+    # back to the timed mode (the persistent tile the plan chose, when it chose one)
+    bp.set_mode(api.BATCH_PERSISTENT if persistent else api.BATCH_GRAPH, mode_info[1] if persistent else 0)
     # the same grids projected one after another through the one-grid path (eager launches)
     projs = []
     for g in grids:
@@ -554,6 +559,9 @@ def run_batch(args, rank, world, local_rank):
             ("graph_ms_per_batch" if persistent else "persistent_ms_per_batch"): other_ms,
             "other_mode_same_cycles": ores["cycles"] == res["cycles"],
             "persistent_profile": prof,
+            "persistent_tile": (pers_mode if pers_mode else mode_info)[1],
+            "persistent_tile_tuning_ms": dict(zip(("16384", "32768", "65536"),
+                                                  (pers_mode if pers_mode else mode_info)[2])),
             "max_rel_residual": max(res["rel_residual"]), "max_abs_div": max(res["max_abs_div"])}
     return ms, ems, ek, h2d, d2h, launches, clk.summary(), info, count
 

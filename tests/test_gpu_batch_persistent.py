@@ -78,6 +78,23 @@ def test_persistent_batch_without_plan_and_mode_switch(wp):
     _same_fields(gu, gq, pu, pq)
 
 
+def test_persistent_tile_is_tuned_by_the_plan(wp):
+    """With tile_cells 0 the plan times the persistent solve with each candidate tile and keeps the
+    fastest; a tile the caller gives is kept as given."""
+    grids, u = _grids(wp)
+    bp = wp.BatchProjector(grids, rel_tol=1e-6, max_cycles=40, nstreams=2, persistent=True)
+    assert bp.get_mode()[0] == wp.BATCH_PERSISTENT
+    bp.plan(u)
+    mode, tile, ms = bp.get_mode()
+    assert mode == wp.BATCH_PERSISTENT and tile in (16384, 32768, 65536), (tile, ms)
+    assert all(t > 0 for t in ms) and ms[(16384, 32768, 65536).index(tile)] == min(ms), ms
+    _, _, res = _run(bp, u, grids, wp)
+    assert res["status"] == "WP_OK"
+    fixed = wp.BatchProjector(grids, rel_tol=1e-6, max_cycles=40, nstreams=2, persistent=True, tile_cells=4096)
+    fixed.plan(u)
+    assert fixed.get_mode()[1] == 4096 and fixed.get_mode()[2] == [0.0, 0.0, 0.0]
+
+
 def test_persistent_batch_cycle_cap(wp):
     grids, u = _grids(wp)
     bp = wp.BatchProjector(grids, rel_tol=1e-12, max_cycles=2, nstreams=2, persistent=True)

@@ -114,7 +114,7 @@ def test_conv_wgrad_wait_gives_up_and_next_call_matches(wp):
 
 def test_withhold_is_one_shot_and_validated(wp):
     with pytest.raises(wp.WPError):
-        wp.debug_withhold_wait(3, 0, 1e-3)
+        wp.debug_withhold_wait(4, 0, 1e-3)
     with pytest.raises(wp.WPError):
         wp.debug_withhold_wait(wp.WAIT_SITE_CONV_PIPELINE, 0, 5.0)
     wp.debug_withhold_wait(wp.WAIT_SITE_CONV_PIPELINE, 0, 1e-3)

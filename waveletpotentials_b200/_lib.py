@@ -134,6 +134,7 @@ SIGNATURES = {
     "wp_batch_results": (I, [P, P, P, P, P]),
     "wp_batch_set_mode": (I, [P, I, ctypes.c_longlong]),
     "wp_batch_profile": (I, [P, I, P, I, P]),
+    "wp_batch_get_mode": (I, [P, P, P, P]),
     "wp_batch_destroy": (I, [P]),
 }
 

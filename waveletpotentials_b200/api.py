@@ -857,6 +857,17 @@ class BatchProjector:
             d[nm] = {"cycles": v[4 + 2 * k], "tiles": v[5 + 2 * k]}
         return d
 
+    def get_mode(self):
+        """(mode, cells per work-queue tile, the tile tuner's timings in ms) (wp_batch_get_mode); in
+        persistent mode with ``tile_cells`` 0, ``plan()`` times tiles of 16384, 32768 and 65536 cells
+        and keeps the fastest."""
+        m = ctypes.c_int()
+        t = ctypes.c_longlong()
+        ms = (ctypes.c_float * 3)()
+        check(lib().wp_batch_get_mode(self._h, ctypes.byref(m), ctypes.byref(t), ctypes.cast(ms, ctypes.c_void_p)),
+              "wp_batch_get_mode")
+        return m.value, t.value, list(ms)
+
     def set_mode(self, mode, tile_cells=0):
         """BATCH_GRAPH or BATCH_PERSISTENT (see the class docstring); raises WPError (the mode
         unchanged) when a grid's levels do not fit the persistent program."""

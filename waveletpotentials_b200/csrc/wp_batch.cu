@@ -95,6 +95,8 @@ struct wp_batch {
     bool counted = true;             // the last replay's loop-body kernels were added to the count
     int mode = WP_BATCH_GRAPH;
     long long tile_cells = 0;        // persistent mode: cells per work-queue tile (0 = default)
+    bool tile_auto = true;           // the caller left the tile to the library: wp_batch_plan tunes it
+    float tile_ms[3] = {0.f, 0.f, 0.f};  // the tuner's timings of kTileCands (0 = not timed)
     wp_mg_pbatch* pb = nullptr;      // persistent mode: every grid's solve program, in cost order
 };
 
@@ -250,6 +252,52 @@ extern "C" CUWHHD_API wp_status wp_batch_create(wp_batch** out, int count, const
     return WP_OK;
 }
 
+namespace {
+
+constexpr long long kTileCands[3] = {16384, 32768, 65536};
+
+// Persistent mode, tile left to the library: the persistent solve of the plan's right-hand sides
+// timed with each candidate tile (one warm-up launch, one timed), the fastest kept.
+wp_status tune_tiles(wp_batch* B, cudaStream_t s) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    WP_CUDA_TRY(cudaEventCreate(&e0));
+    WP_CUDA_TRY(cudaEventCreate(&e1));
+    wp_status st = WP_OK;
+    float best = 0.f;
+    long long pick = 0;
+    for (int k = 0; k < 3 && st == WP_OK; ++k) {
+        if (B->pb) wp_mg_pbatch_destroy(B->pb);
+        B->pb = nullptr;
+        B->tile_cells = kTileCands[k];
+        if ((st = build_pbatch(B)) != WP_OK) break;
+        if ((st = wp_mg_pbatch_launch(B->pb, s)) != WP_OK) break;
+        cudaEventRecord(e0, s);
+        if ((st = wp_mg_pbatch_launch(B->pb, s)) != WP_OK) break;
+        cudaEventRecord(e1, s);
+        cudaError_t e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {
+            wp_set_cuda_error(e, "batch tile tuning", __FILE__, __LINE__);
+            st = WP_ERR_CUDA;
+            break;
+        }
+        B->tile_ms[k] = ms;
+        if (pick == 0 || ms < best) {
+            best = ms;
+            pick = kTileCands[k];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (B->pb) wp_mg_pbatch_destroy(B->pb);
+    B->pb = nullptr;  // rebuilt with the chosen tile at the next capture
+    if (pick) B->tile_cells = pick;
+    return st;
+}
+
+}  // namespace
+
 // Eager pass: per grid, b = -div(a u) and a tolerance-driven mixed solve; records the V-cycles each
 // grid needs on this input (the velocities are not modified), which order the grids over the graph's
 // branches.  Optional: without it the grids are ordered by size.  Synchronous.
@@ -281,6 +329,7 @@ extern "C" CUWHHD_API wp_status wp_batch_plan(wp_batch* B, const float* const* x
         wp_mg_pbatch_destroy(B->pb);
         B->pb = nullptr;
     }
+    if (B->mode == WP_BATCH_PERSISTENT && B->tile_auto) return tune_tiles(B, s);
     return WP_OK;
 }
 
@@ -439,20 +488,36 @@ extern "C" CUWHHD_API wp_status wp_batch_set_mode(wp_batch* B, int mode, long lo
     }
     wp_mg_pbatch* old = B->pb;
     const long long old_cells = B->tile_cells;
+    const bool old_auto = B->tile_auto;
     B->pb = nullptr;
     B->tile_cells = tile_cells;
+    B->tile_auto = tile_cells == 0;
     if (mode == WP_BATCH_PERSISTENT) {
         // checked now, so an unsupported batch fails here and keeps its mode
         const wp_status st = build_pbatch(B);
         if (st != WP_OK) {
             B->pb = old;
             B->tile_cells = old_cells;
+            B->tile_auto = old_auto;
             return st;
         }
     }
     if (old) wp_mg_pbatch_destroy(old);
     B->mode = mode;
     destroy_graph(B);
+    return WP_OK;
+}
+
+extern "C" CUWHHD_API wp_status wp_batch_get_mode(const wp_batch* B, int* mode, long long* tile_cells,
+                                                  float* tuned_ms) {
+    if (!B) {
+        wp_set_error_msg("wp_batch_get_mode: null handle");
+        return WP_ERR_INVALID_ARG;
+    }
+    if (mode) *mode = B->mode;
+    if (tile_cells) *tile_cells = B->tile_cells ? B->tile_cells : 32768;
+    if (tuned_ms)
+        for (int k = 0; k < 3; ++k) tuned_ms[k] = B->tile_ms[k];
     return WP_OK;
 }
 
