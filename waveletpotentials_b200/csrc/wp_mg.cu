@@ -4102,37 +4102,44 @@ __device__ __forceinline__ void pb_cta_sum(double v, double* out, double* red) {
     __syncthreads();
 }
 
+// Loads of data written earlier in the launch.  Every tile starts after thread 0's GPU-scope fence
+// that follows the atomic which handed the tile out (an acquire, ordered before the CTA's loads by
+// the barrier after it), and every producer's stores precede a GPU-scope fence and the atomic that
+// reports its tile done (a release): the memory model orders the tile's ordinary loads after the
+// producers' stores, so they may go through L1 (false) instead of L2 only (true).
+constexpr bool kPbCG = false;
+
 // The work of one tile, one function per phase type (each with its own register allocation: the
 // persistent kernel's 1024 threads leave 64 registers a thread).  vb0 .. v1 - 1: the tile's blocks.
 __device__ __noinline__ void pb_sweep0(const PPhase& Ps, const Lvl<float>& Ls, float w, int vb0, int v1, int tid) {
     const PPhase P = Ps;
     const Lvl<float> L = Ls;
-    for (int vb = vb0; vb < v1; vb += 4) jacobi0_q_body<float, true>(P.dst, P.f, L, w, P.zc, vb % P.gx, vb / P.gx, tid);
+    for (int vb = vb0; vb < v1; vb += 4) jacobi0_q_body<float, kPbCG>(P.dst, P.f, L, w, P.zc, vb % P.gx, vb / P.gx, tid);
 }
 __device__ __noinline__ void pb_sweep(const PPhase& Ps, const Lvl<float>& Ls, float w, int vb0, int v1, int tid) {
     const PPhase P = Ps;
     const Lvl<float> L = Ls;
     for (int vb = vb0; vb < v1; vb += 4)
-        jacobi_q_body<float, false, true>(P.dst, P.src, P.f, L, w, P.zc, nullptr, vb % P.gx, vb / P.gx, tid);
+        jacobi_q_body<float, false, kPbCG>(P.dst, P.src, P.f, L, w, P.zc, nullptr, vb % P.gx, vb / P.gx, tid);
 }
 __device__ __noinline__ void pb_sweep_acc(const PPhase& Ps, const Lvl<float>& Ls, float w, double* p64, int vb0,
                                           int v1, int tid) {
     const PPhase P = Ps;
     const Lvl<float> L = Ls;
     for (int vb = vb0; vb < v1; vb += 4)
-        jacobi_q_body<float, true, true>(nullptr, P.src, P.f, L, w, P.zc, p64, vb % P.gx, vb / P.gx, tid);
+        jacobi_q_body<float, true, kPbCG>(nullptr, P.src, P.f, L, w, P.zc, p64, vb % P.gx, vb / P.gx, tid);
 }
 __device__ __noinline__ void pb_restrict(const PPhase& Ps, const Lvl<float>& Ls, int vb0, int v1, int tid) {
     const PPhase P = Ps;
     const Lvl<float> L = Ls;
     for (int vb = vb0; vb < v1; vb += 4)
-        resid_restrict_q_body<float, true>(P.dst, P.src, P.f, L, P.cnx, P.cny, P.cnz, P.zc, vb % P.gx, vb / P.gx, tid);
+        resid_restrict_q_body<float, kPbCG>(P.dst, P.src, P.f, L, P.cnx, P.cny, P.cnz, P.zc, vb % P.gx, vb / P.gx, tid);
 }
 __device__ __noinline__ void pb_prolong(const PPhase& Ps, const Lvl<float>& Ls, int vb0, int v1, int tid) {
     const PPhase P = Ps;
     const Lvl<float> L = Ls;
     for (int vb = vb0; vb < v1; vb += 4)
-        prolong_tri_q_body<float, true>(P.dst, P.src, L.nx, L.ny, L.nz, P.cnx, P.cny, P.cnz, vb % P.gx, vb / P.gx, tid);
+        prolong_tri_q_body<float, kPbCG>(P.dst, P.src, L.nx, L.ny, L.nz, P.cnx, P.cny, P.cnz, vb % P.gx, vb / P.gx, tid);
 }
 __device__ __noinline__ void pb_coarse(const LPack& Q, const PGrid& G, float* lean_smem) {
     lean_cycle<true>(Q, G.nu1, G.nu2, G.w, G.citers, G.prolong, lean_smem);
@@ -4175,7 +4182,7 @@ __device__ __noinline__ double pb_defect(const PPhase& Ps, const Lvl<double>& Ls
     const float* const f = G.f;
     double s2 = 0.0;
     for (int vb = vb0; vb < v1; vb += 4)
-        s2 += defect64_q_body<double, true>(r32, p64, f, L, m, P.zc, vb % P.gx, vb / P.gx, tid);
+        s2 += defect64_q_body<double, kPbCG>(r32, p64, f, L, m, P.zc, vb % P.gx, vb / P.gx, tid);
     return s2;
 }
 
@@ -4262,7 +4269,7 @@ __global__ void __launch_bounds__(1024, 1) batch_persist_kernel(PArgs A) {
                 const long n = (long)sL.nx * sL.ny * sL.nz;
                 for (int vb = vb0; vb < v1; vb += 4) {
                     const long i = (long)vb * 1024 + 4L * tid;
-                    if (i < n) st4(G.dst + i, cvt4<float>(ldq<true>(G.p64 + i)));
+                    if (i < n) st4(G.dst + i, cvt4<float>(ldq<kPbCG>(G.p64 + i)));
                 }
                 break;
             }
