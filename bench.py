@@ -354,21 +354,28 @@ def run_ours(args, rank, world, local_rank):
 # ------------------------------------------------------------------ batched workload
 BATCH_3D = (32, 64, 128)
 BATCH_2D = (256, 512, 1024)
+# the small-grid mix (--batch-sizes small): the same counts, every grid a few V-cycles of kernels
+# that each run for a few microseconds
+BATCH_3D_SMALL = (16, 32)
+BATCH_2D_SMALL = (64, 128)
 
 
-def make_batch(count3, count2, seed):
-    """Seeded uneven batch: 3D cubes drawn from {32,64,128}^3 and 2D squares from {256,512,1024}^2,
-    each with 0-4 random spheres/circles r~U(0.05,0.15) and its own field seed."""
+def make_batch(count3, count2, seed, small=False):
+    """Seeded uneven batch: 3D cubes drawn from {32,64,128}^3 and 2D squares from {256,512,1024}^2
+    ({16,32}^3 and {64,128}^2 when small), each with 0-4 random spheres/circles r~U(0.05,0.15) and
+    its own field seed."""
     import tempfile
     from waveletpotentials_b200 import fields
     rng = np.random.default_rng(seed + 77)
     specs = []
+    sizes3, sizes2 = (BATCH_3D_SMALL, BATCH_2D_SMALL) if small else (BATCH_3D, BATCH_2D)
     for i in range(count3 + count2):
         d3 = i < count3
-        n = int(rng.choice(BATCH_3D if d3 else BATCH_2D))
+        n = int(rng.choice(sizes3 if d3 else sizes2))
         nsph = int(rng.integers(0, 5))
         specs.append(((n, n, n) if d3 else (n, n), nsph, seed * 1000 + i))
-    path = os.path.join(tempfile.gettempdir(), f"wp_bench_batch_{count3}_{count2}_{seed}.npz")
+    path = os.path.join(tempfile.gettempdir(),
+                        f"wp_bench_batch_{count3}_{count2}_{seed}{'_small' if small else ''}.npz")
     cache = dict(np.load(path)) if os.path.exists(path) else {}
     out, dirty = [], False
     for i, (d, nsph, sd) in enumerate(specs):
@@ -397,7 +404,7 @@ def run_batch(args, rank, world, local_rank):
     build.build()
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    probs = make_batch(args.batch3d, args.batch2d, rank_seed(args.seed, rank))
+    probs = make_batch(args.batch3d, args.batch2d, rank_seed(args.seed, rank), small=args.batch_sizes == "small")
     grids, u0, outs = [], [], []
     for d, c, r, u in probs:
         h = 1.0 / d[0]
@@ -560,7 +567,7 @@ def run_batch(args, rank, world, local_rank):
             "other_mode_same_cycles": ores["cycles"] == res["cycles"],
             "persistent_profile": prof,
             "persistent_tile": (pers_mode if pers_mode else mode_info)[1],
-            "persistent_tile_tuning_ms": dict(zip(("16384", "32768", "65536"),
+            "persistent_tile_tuning_ms": dict(zip([str(c) for c in api.BatchProjector.TILE_CANDIDATES],
                                                   (pers_mode if pers_mode else mode_info)[2])),
             "max_rel_residual": max(res["rel_residual"]), "max_abs_div": max(res["max_abs_div"])}
     return ms, ems, ek, h2d, d2h, launches, clk.summary(), info, count
@@ -833,7 +840,11 @@ def main():
     ap.add_argument("--batch-mode", default="graph", choices=["graph", "persistent"],
                     help="graph: each grid's solve a device loop of launches on a graph branch; persistent: every "
                          "grid's solve in one persistent kernel over a device work queue")
-    ap.add_argument("--batch-tile", type=int, default=0, help="persistent mode: cells per work-queue tile (0: 32768)")
+    ap.add_argument("--batch-tile", type=int, default=0,
+                    help="persistent mode: cells per work-queue tile (0: the plan tunes it)")
+    ap.add_argument("--batch-sizes", default="mixed", choices=["mixed", "small"],
+                    help="mixed: 3D {32,64,128}^3 + 2D {256,512,1024}^2 (the configured batch); small: {16,32}^3 + "
+                         "{64,128}^2")
     ap.add_argument("--nstreams", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -922,15 +933,21 @@ def main():
             torch.distributed.destroy_process_group()
         if rank != 0:
             return
+        small = args.batch_sizes == "small"
+        s3 = "{16,32}" if small else "{32,64,128}"
+        s2 = "{64,128}" if small else "{256,512,1024}"
         out = {"metric": "batched projections/s (64 uneven 2D/3D grids per CUDA-graph launch)",
                "value": throughput(world, count * args.steps, ms), "unit": "projections/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 defect/refinement)",
                "data": "synthetic (seeded spectral fields)",
-               "config": {"workload": f"{args.batch3d} 3D grids from {{32,64,128}}^3 + {args.batch2d} 2D grids from "
-                                      f"{{256,512,1024}}^2, 0-4 random spheres each, mixed-precision multigrid to "
+               "config": {"workload": f"{args.batch3d} 3D grids from {s3}^3 + {args.batch2d} 2D grids from "
+                                      f"{s2}^2, 0-4 random spheres each, mixed-precision multigrid to "
                                       f"rel. residual {args.batch_tol:g} + wavelet recovery, one graph per batch",
-                          "l2_flush": "inputs larger than L2 (batch working set > 1 GB)"},
+                          "solves": args.batch_mode,
+                          "l2_flush": ("inputs larger than L2 (batch working set > 1 GB)" if args.batch_sizes == "mixed"
+                                       else "small grids: the batch's inputs fit L2; every timed step restores them "
+                                            "from copies, and the step is launch- and latency-bound")},
                "e2e": {"value": throughput(world, count * ek, ems), "unit": "projections/s",
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "gpu_launches": launches, "clocks": clocks, "batch": info}
@@ -1019,8 +1036,12 @@ def main():
         "divergence": div,
         "parity": parity,
         "plain": plain,
-        # every kernel of the event-instrumented steps (ms and algorithmic bytes summed over psteps)
-        "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} for r in prof],
+        # every kernel of the event-instrumented steps (ms and algorithmic bytes summed over psteps),
+        # with its achieved algorithmic GB/s and that as a fraction of the measured HBM copy bandwidth
+        "kernels": [{**{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()},
+                     "gbs": round(r["bytes"] / (r["ms"] * 1e6), 1) if r["ms"] > 0 else None,
+                     "frac_of_peak": round(r["bytes"] / (r["ms"] * 1e6) / peaks()[0], 3) if r["ms"] > 0 else None}
+                    for r in prof],
         "kernel_ms_per_step": round(sum(r["ms"] for r in prof) / psteps, 4),
         "mg_tiles": {"z_chunks_per_level": tiles[0], "variants_per_level": tiles[1], "tuned_ms_per_level": tiles[2]},
     }

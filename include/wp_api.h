@@ -515,8 +515,8 @@ CUWHHD_API wp_status wp_batch_results(wp_batch* h, double* max_abs_div, double* 
 CUWHHD_API wp_status wp_batch_set_mode(wp_batch* h, int mode, long long tile_cells);
 /* The current mode and tile (cells per work-queue tile).  With tile_cells 0 in WP_BATCH_PERSISTENT
    mode the tile is the library's to choose: wp_batch_plan then times the persistent solve of the
-   plan's inputs with tiles of 16384, 32768 and 65536 cells and keeps the fastest (tuned_ms, may be
-   NULL: the three timings, 0 where not timed). */
+   plan's inputs with tiles of 4096, 8192, 16384, 32768 and 65536 cells and keeps the fastest
+   (tuned_ms, may be NULL: the five timings in that order, 0 where not timed). */
 CUWHHD_API wp_status wp_batch_get_mode(const wp_batch* h, int* mode, long long* tile_cells, float* tuned_ms);
 /* WP_BATCH_PERSISTENT batches: activity counters of the persistent kernel (SM clock cycles summed
    over the CTAs, thread 0 of each), synchronous.  out[0..cap-1] receives the sums since counting was

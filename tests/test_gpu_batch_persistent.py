@@ -86,13 +86,14 @@ def test_persistent_tile_is_tuned_by_the_plan(wp):
     assert bp.get_mode()[0] == wp.BATCH_PERSISTENT
     bp.plan(u)
     mode, tile, ms = bp.get_mode()
-    assert mode == wp.BATCH_PERSISTENT and tile in (16384, 32768, 65536), (tile, ms)
-    assert all(t > 0 for t in ms) and ms[(16384, 32768, 65536).index(tile)] == min(ms), ms
+    cands = wp.BatchProjector.TILE_CANDIDATES
+    assert mode == wp.BATCH_PERSISTENT and tile in cands, (tile, ms)
+    assert len(ms) == len(cands) and all(t > 0 for t in ms) and ms[cands.index(tile)] == min(ms), ms
     _, _, res = _run(bp, u, grids, wp)
     assert res["status"] == "WP_OK"
     fixed = wp.BatchProjector(grids, rel_tol=1e-6, max_cycles=40, nstreams=2, persistent=True, tile_cells=4096)
     fixed.plan(u)
-    assert fixed.get_mode()[1] == 4096 and fixed.get_mode()[2] == [0.0, 0.0, 0.0]
+    assert fixed.get_mode()[1] == 4096 and fixed.get_mode()[2] == [0.0] * len(cands)
 
 
 def test_persistent_batch_cycle_cap(wp):

@@ -842,6 +842,7 @@ class BatchProjector:
         if persistent:
             self.set_mode(BATCH_PERSISTENT, tile_cells)
 
+    TILE_CANDIDATES = (4096, 8192, 16384, 32768, 65536)
     PROFILE_NAMES = ("init", "defect", "sweep0", "sweep", "sweep_acc", "restrict", "prolong", "coarse", "convert")
 
     def profile(self, enable, stream=None):
@@ -859,11 +860,11 @@ class BatchProjector:
 
     def get_mode(self):
         """(mode, cells per work-queue tile, the tile tuner's timings in ms) (wp_batch_get_mode); in
-        persistent mode with ``tile_cells`` 0, ``plan()`` times tiles of 16384, 32768 and 65536 cells
-        and keeps the fastest."""
+        persistent mode with ``tile_cells`` 0, ``plan()`` times tiles of ``TILE_CANDIDATES`` cells and
+        keeps the fastest."""
         m = ctypes.c_int()
         t = ctypes.c_longlong()
-        ms = (ctypes.c_float * 3)()
+        ms = (ctypes.c_float * 5)()
         check(lib().wp_batch_get_mode(self._h, ctypes.byref(m), ctypes.byref(t), ctypes.cast(ms, ctypes.c_void_p)),
               "wp_batch_get_mode")
         return m.value, t.value, list(ms)

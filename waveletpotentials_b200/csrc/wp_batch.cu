@@ -96,7 +96,7 @@ struct wp_batch {
     int mode = WP_BATCH_GRAPH;
     long long tile_cells = 0;        // persistent mode: cells per work-queue tile (0 = default)
     bool tile_auto = true;           // the caller left the tile to the library: wp_batch_plan tunes it
-    float tile_ms[3] = {0.f, 0.f, 0.f};  // the tuner's timings of kTileCands (0 = not timed)
+    float tile_ms[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // the tuner's timings of kTileCands (0 = not timed)
     wp_mg_pbatch* pb = nullptr;      // persistent mode: every grid's solve program, in cost order
 };
 
@@ -254,7 +254,8 @@ extern "C" CUWHHD_API wp_status wp_batch_create(wp_batch** out, int count, const
 
 namespace {
 
-constexpr long long kTileCands[3] = {16384, 32768, 65536};
+constexpr int kTileN = 5;
+constexpr long long kTileCands[kTileN] = {4096, 8192, 16384, 32768, 65536};
 
 // Persistent mode, tile left to the library: the persistent solve of the plan's right-hand sides
 // timed with each candidate tile (one warm-up launch, one timed), the fastest kept.
@@ -265,7 +266,7 @@ wp_status tune_tiles(wp_batch* B, cudaStream_t s) {
     wp_status st = WP_OK;
     float best = 0.f;
     long long pick = 0;
-    for (int k = 0; k < 3 && st == WP_OK; ++k) {
+    for (int k = 0; k < kTileN && st == WP_OK; ++k) {
         if (B->pb) wp_mg_pbatch_destroy(B->pb);
         B->pb = nullptr;
         B->tile_cells = kTileCands[k];
@@ -517,7 +518,7 @@ extern "C" CUWHHD_API wp_status wp_batch_get_mode(const wp_batch* B, int* mode, 
     if (mode) *mode = B->mode;
     if (tile_cells) *tile_cells = B->tile_cells ? B->tile_cells : 32768;
     if (tuned_ms)
-        for (int k = 0; k < 3; ++k) tuned_ms[k] = B->tile_ms[k];
+        for (int k = 0; k < kTileN; ++k) tuned_ms[k] = B->tile_ms[k];
     return WP_OK;
 }
 

@@ -1765,8 +1765,10 @@ __device__ __forceinline__ void lean_cycle(const LPack& P, int nu1, int nu2, flo
             __syncthreads();
         }
         if (L.cells <= 32) {
-            // a coarsest grid of a few cells: one warp iterates alone (warp barriers only)
-            if (tid < 32) {
+            // a coarsest grid of a few cells: one warp iterates alone (warp barriers only).  A single
+            // cell has no interior face, so its diagonal is 0 and every sweep writes the 0 that both
+            // buffers already hold: only the buffer swaps are kept.
+            if (tid < 32 && L.cells > 1) {
                 for (int k = 0; k < citers; ++k) {
                     lean_sweep(L, L.t, L.v, w, tid, 32);
                     __syncwarp();
