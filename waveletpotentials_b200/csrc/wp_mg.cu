@@ -1602,15 +1602,24 @@ __device__ __forceinline__ void lean_advance(int& x, int& y, int& z, int bx, int
     z += bz;
 }
 
-// residual of the fine level restricted to the coarse right-hand side (cc_restrict's sums and order)
+// residual of the fine level restricted to the coarse right-hand side (cc_restrict's sums and order):
+// first every fine cell's residual, by all threads, into the fine level's second buffer (free until
+// the post-sweeps write it), then each coarse cell's weighted sum of its children in the same order
 __device__ __forceinline__ void lean_restrict(const LS& F, const LS& C) {
     const int B = blockDim.x;
+    const float* dgf = F.cf + 6L * F.cells;
+    for (int i = threadIdx.x; i < F.cells; i += B) {
+        float od;
+        const float c = lean_off(F, F.v, i, od);
+        const float dg = dgf[i];
+        F.t[i] = dg > (float)kEps ? F.f[i] - (dg * c + od) : 0.f;
+    }
+    __syncthreads();
     int cx, cy, cz;
     lean_coord(threadIdx.x, C.nx, C.ny, cx, cy, cz);
     int bx, by, bz;
     lean_coord(B, C.nx, C.ny, bx, by, bz);
     const float* wcf = F.cf + 7L * F.cells;
-    const float* dgf = F.cf + 6L * F.cells;
     for (int ci = threadIdx.x; ci < C.cells; ci += B) {
         float tot[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
         for (int xo = 0; xo < 2; ++xo) {
@@ -1624,11 +1633,7 @@ __device__ __forceinline__ void lean_restrict(const LS& F, const LS& C) {
                     const int z = 2 * cz + kz;
                     if (z >= F.nz) break;
                     const int i = y + x * F.ny + z * F.nxy;
-                    float od;
-                    const float c = lean_off(F, F.v, i, od);
-                    const float dg = dgf[i];
-                    const float r = dg > (float)kEps ? F.f[i] - (dg * c + od) : 0.f;
-                    acc += wcf[i] * r;
+                    acc += wcf[i] * F.t[i];
                 }
                 tot[xo][yo] = acc;
             }
@@ -1712,19 +1717,13 @@ __device__ __forceinline__ void lean_cycle(const LPack& P, int nu1, int nu2, flo
         }
     }
     if (!CFG) {
-        // stencils: one flat 128-bit copy (every level's block is a multiple of 16 bytes)
-        const float4* g = reinterpret_cast<const float4*>(P.lv[0].ccf);
-        float4* d = reinterpret_cast<float4*>(lean_smem);
-        const int n4 = (int)(cf_floats / 4);
-        int i = tid;
-        for (; i + 3 * B < n4; i += 4 * B) {
-            const float4 a0 = g[i], a1 = g[i + B], a2 = g[i + 2 * B], a3 = g[i + 3 * B];
-            d[i] = a0;
-            d[i + B] = a1;
-            d[i + 2 * B] = a2;
-            d[i + 3 * B] = a3;
-        }
-        for (; i < n4; i += B) d[i] = g[i];
+        // stencils: 16-byte asynchronous copies (every level's block is a multiple of 16 bytes), all in
+        // flight at once while the buffers are cleared below, waited for before the first sweep
+        const char* g = reinterpret_cast<const char*>(P.lv[0].ccf);
+        char* d = reinterpret_cast<char*>(lean_smem);
+        const int n16 = (int)(cf_floats / 4);
+        for (int i = tid; i < n16; i += B) cp_async16(d + 16L * i, g + 16L * i);
+        cp_async_commit();
     }
     __syncthreads();
     for (int l = 0; l < P.n; ++l) {
@@ -1737,6 +1736,7 @@ __device__ __forceinline__ void lean_cycle(const LPack& P, int nu1, int nu2, flo
         if (l == 0)
             for (int i = tid; i < q.cells; i += B) q.f[i] = __ldcg(P.lv[0].f + i);
     }
+    cp_async_wait<0>();
     __syncthreads();
     for (int l = 0; l < P.n - 1; ++l) {
         LS L = S[l];
@@ -1765,18 +1765,37 @@ __device__ __forceinline__ void lean_cycle(const LPack& P, int nu1, int nu2, flo
             __syncthreads();
         }
         if (L.cells <= 32) {
-            // a coarsest grid of a few cells: one warp iterates alone (warp barriers only).  A single
-            // cell has no interior face, so its diagonal is 0 and every sweep writes the 0 that both
-            // buffers already hold: only the buffer swaps are kept.
+            // a coarsest grid of at most 32 cells: one warp iterates alone, a cell per lane in
+            // registers, the neighbours' values by shuffle -- lean_sweep's arithmetic and order, the
+            // padding planes (indices outside the level) reading 0.  The result goes to the buffer the
+            // swaps of citers sweeps would leave it in.  A single cell has no interior face: its
+            // diagonal is 0 and the buffers already hold the 0 every sweep would write.
             if (tid < 32 && L.cells > 1) {
-                for (int k = 0; k < citers; ++k) {
-                    lean_sweep(L, L.t, L.v, w, tid, 32);
-                    __syncwarp();
-                    float* tmp = L.v;
-                    L.v = L.t;
-                    L.t = tmp;
+                const int n = L.cells, i = tid;
+                const bool own = i < n;
+                const int off[6] = {-1, 1, -L.ny, L.ny, -L.nxy, L.nxy};
+                float cfk[6], dg = 0.f, fv = 0.f, v = 0.f;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) cfk[k] = own ? L.cf[k * n + i] : 0.f;
+                if (own) {
+                    dg = L.cf[6 * n + i];
+                    fv = L.f[i];
+                    v = L.v[i];
                 }
-            } else if (citers & 1) {
+                for (int it = 0; it < citers; ++it) {
+                    float o = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) {
+                        const int j = i + off[k];
+                        const float vj = __shfl_sync(0xffffffffu, v, j & 31);
+                        o -= cfk[k] * ((j >= 0 && j < n) ? vj : 0.f);
+                    }
+                    const float nv = dg > (float)kEps ? (1.f - w) * v + w * (fv - o) / dg : 0.f;
+                    v = own ? nv : v;
+                }
+                if (own) ((citers & 1) ? L.t : L.v)[i] = v;
+            }
+            if (citers & 1) {
                 float* tmp = L.v;
                 L.v = L.t;
                 L.t = tmp;
