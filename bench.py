@@ -426,11 +426,13 @@ def run_batch(args, rank, world, local_rank):
             outs.append([torch.zeros(s["qz"], device=dev)])
         u0.append([torch.as_tensor(x, device=dev) for x in u])
     u = [[x.clone() for x in f] for f in u0]
-    persistent = args.batch_mode == "persistent"
+    want = {"graph": api.BATCH_GRAPH, "persistent": api.BATCH_PERSISTENT, "auto": api.BATCH_AUTO}[args.batch_mode]
     bp = api.BatchProjector(grids, rel_tol=args.batch_tol, max_cycles=80, nstreams=args.nstreams,
-                            persistent=persistent, tile_cells=args.batch_tile)
+                            tile_cells=args.batch_tile, mode=want)
     cycles = bp.plan(u)
     mode_info = bp.get_mode()
+    # the way the timed region runs the solves (auto: the plan's choice)
+    persistent = mode_info[0] == api.BATCH_PERSISTENT
     stream = torch.cuda.current_stream()
     count = len(grids)
 
@@ -557,6 +559,8 @@ def run_batch(args, rank, world, local_rank):
     info = {"grids": count, "grids_3d": args.batch3d, "grids_2d": args.batch2d, "cells": cells,
             "cycles_min": min(res["cycles"]), "cycles_max": max(res["cycles"]), "nstreams": args.nstreams,
             "mode": args.batch_mode,
+            "mode_run": "persistent" if persistent else "graph",
+            "auto_graph_solve_ms": mode_info[3] if args.batch_mode == "auto" else None,
             "solves": ("one persistent kernel over a device work queue of (grid, level, pass) tiles, "
                        f"{args.batch_tile or 32768} cells per tile" if persistent else
                        "a device loop of launches per grid (while-node) on the graph's branches"),
@@ -837,9 +841,10 @@ def main():
     ap.add_argument("--batch3d", type=int, default=32)
     ap.add_argument("--batch2d", type=int, default=32)
     ap.add_argument("--batch-tol", type=float, default=1e-6)
-    ap.add_argument("--batch-mode", default="graph", choices=["graph", "persistent"],
+    ap.add_argument("--batch-mode", default="graph", choices=["graph", "persistent", "auto"],
                     help="graph: each grid's solve a device loop of launches on a graph branch; persistent: every "
-                         "grid's solve in one persistent kernel over a device work queue")
+                         "grid's solve in one persistent kernel over a device work queue; auto: the plan times both "
+                         "and the faster runs")
     ap.add_argument("--batch-tile", type=int, default=0,
                     help="persistent mode: cells per work-queue tile (0: the plan tunes it)")
     ap.add_argument("--batch-sizes", default="mixed", choices=["mixed", "small"],

@@ -512,11 +512,17 @@ CUWHHD_API wp_status wp_batch_results(wp_batch* h, double* max_abs_div, double* 
    wp_batch_results when one gave up). */
 #define WP_BATCH_GRAPH 0
 #define WP_BATCH_PERSISTENT 1
+/* WP_BATCH_AUTO: wp_batch_plan times the persistent solve (its tile tuned when tile_cells is 0) and the
+   graph mode's solves on the plan's inputs and runs the faster from then on (the graph mode before a
+   plan, and for grids the persistent program does not take). */
+#define WP_BATCH_AUTO 2
 CUWHHD_API wp_status wp_batch_set_mode(wp_batch* h, int mode, long long tile_cells);
-/* The current mode and tile (cells per work-queue tile).  With tile_cells 0 in WP_BATCH_PERSISTENT
-   mode the tile is the library's to choose: wp_batch_plan then times the persistent solve of the
-   plan's inputs with tiles of 4096, 8192, 16384, 32768 and 65536 cells and keeps the fastest
-   (tuned_ms, may be NULL: the five timings in that order, 0 where not timed). */
+/* The mode the batch runs in (WP_BATCH_GRAPH or WP_BATCH_PERSISTENT; for WP_BATCH_AUTO the plan's
+   choice) and the tile (cells per work-queue tile).  With tile_cells 0 in WP_BATCH_PERSISTENT or
+   WP_BATCH_AUTO mode the tile is the library's to choose: wp_batch_plan then times the persistent
+   solve of the plan's inputs with tiles of 4096, 8192, 16384, 32768 and 65536 cells and keeps the
+   fastest.  tuned_ms (may be NULL) receives six timings in ms: those five, then the graph mode's
+   solves (WP_BATCH_AUTO only); 0 where not timed. */
 CUWHHD_API wp_status wp_batch_get_mode(const wp_batch* h, int* mode, long long* tile_cells, float* tuned_ms);
 /* WP_BATCH_PERSISTENT batches: activity counters of the persistent kernel (SM clock cycles summed
    over the CTAs, thread 0 of each), synchronous.  out[0..cap-1] receives the sums since counting was

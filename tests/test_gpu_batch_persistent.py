@@ -85,7 +85,7 @@ def test_persistent_tile_is_tuned_by_the_plan(wp):
     bp = wp.BatchProjector(grids, rel_tol=1e-6, max_cycles=40, nstreams=2, persistent=True)
     assert bp.get_mode()[0] == wp.BATCH_PERSISTENT
     bp.plan(u)
-    mode, tile, ms = bp.get_mode()
+    mode, tile, ms, graph_ms = bp.get_mode()
     cands = wp.BatchProjector.TILE_CANDIDATES
     assert mode == wp.BATCH_PERSISTENT and tile in cands, (tile, ms)
     assert len(ms) == len(cands) and all(t > 0 for t in ms) and ms[cands.index(tile)] == min(ms), ms
@@ -94,6 +94,32 @@ def test_persistent_tile_is_tuned_by_the_plan(wp):
     fixed = wp.BatchProjector(grids, rel_tol=1e-6, max_cycles=40, nstreams=2, persistent=True, tile_cells=4096)
     fixed.plan(u)
     assert fixed.get_mode()[1] == 4096 and fixed.get_mode()[2] == [0.0] * len(cands)
+
+
+@pytest.mark.parametrize("which", ["small", "mixed"])
+def test_auto_mode_runs_the_faster_way(wp, which):
+    """BATCH_AUTO: the plan times the persistent solve (tile tuned) and the graph mode's solves on its
+    inputs and runs the faster one; before a plan it runs as a graph.  The results equal the graph
+    mode's either way."""
+    grids, u = _grids(wp)
+    if which == "small":
+        keep = [i for i, g in enumerate(grids) if len(g["dim"]) == 3 and max(g["dim"]) <= 32 or
+                len(g["dim"]) == 2 and max(g["dim"]) <= 64]
+        grids, u = [grids[i] for i in keep], [u[i] for i in keep]
+    bp = wp.BatchProjector(grids, rel_tol=TOL, max_cycles=40, nstreams=2, mode=wp.BATCH_AUTO)
+    assert bp.get_mode()[0] == wp.BATCH_GRAPH
+    cycles = bp.plan(u)
+    mode, tile, ms, graph_ms = bp.get_mode()
+    assert graph_ms > 0 and min(ms) > 0, (ms, graph_ms)
+    pers_ms = ms[wp.BatchProjector.TILE_CANDIDATES.index(tile)]
+    assert mode == (wp.BATCH_PERSISTENT if pers_ms < graph_ms else wp.BATCH_GRAPH), (mode, pers_ms, graph_ms)
+    au, aq, res = _run(bp, u, grids, wp)
+    assert res["status"] == "WP_OK" and res["cycles"] == cycles, res
+    ref = wp.BatchProjector(grids, rel_tol=TOL, max_cycles=40, nstreams=2)
+    ref.plan(u)
+    gu, gq, gres = _run(ref, u, grids, wp)
+    assert gres["cycles"] == res["cycles"]
+    _same_fields(gu, gq, au, aq)
 
 
 def test_persistent_batch_cycle_cap(wp):

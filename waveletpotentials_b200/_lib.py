@@ -17,7 +17,7 @@ STATUS = {0: "WP_OK", 1: "WP_ERR_INVALID_ARG", 2: "WP_ERR_UNSUPPORTED", 3: "WP_E
           5: "WP_ERR_NOT_CONVERGED", 6: "WP_ERR_NONFINITE", 7: "WP_ERR_DEVICE_WAIT"}
 WP_ERR_NOT_CONVERGED, WP_ERR_NONFINITE, WP_ERR_DEVICE_WAIT = 5, 6, 7
 WAIT_SITE_GRID_BARRIER, WAIT_SITE_CONV_PIPELINE, WAIT_SITE_BATCH_PUBLISH = 1, 2, 3
-BATCH_GRAPH, BATCH_PERSISTENT = 0, 1
+BATCH_GRAPH, BATCH_PERSISTENT, BATCH_AUTO = 0, 1, 2
 CDF3_5, CDF2_6, CDF4_4, CDF4_6, CDF2_8, CDF3_7 = 2, 5, 6, 7, 10, 11
 CDF2_0, CDF1_1, CDF1_7 = 16, 17, 18
 PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2

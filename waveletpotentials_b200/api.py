@@ -18,7 +18,7 @@ import torch
 from . import _lib
 from ._lib import START_FMG, START_ZERO  # noqa: F401
 from ._lib import WAIT_SITE_BATCH_PUBLISH, WAIT_SITE_CONV_PIPELINE, WAIT_SITE_GRID_BARRIER  # noqa: F401
-from ._lib import BATCH_GRAPH, BATCH_PERSISTENT  # noqa: F401
+from ._lib import BATCH_AUTO, BATCH_GRAPH, BATCH_PERSISTENT  # noqa: F401
 from ._lib import CDF3_7, CDF4_6, PREC_FP32, PREC_FP64, PREC_MIXED, PROLONG_CONSTANT, PROLONG_TRILINEAR, MgParams, \
     MgReport, WPError, check, lib
 
@@ -28,7 +28,7 @@ __all__ = ["CuWHHDForward", "CuWaveletPotentialRecover3D", "CuWaveletPotentialRe
            "random_field3d", "velocity3d_device", "UNetWarmStart", "warm_started_solve",
            "ip_diag", "WPError", "CDF3_7", "CDF4_6", "PREC_FP32", "PREC_MIXED", "PREC_FP64", "PROLONG_CONSTANT",
            "PROLONG_TRILINEAR", "START_ZERO", "START_FMG", "mac_shapes3d", "mac_shapes2d", "BATCH_GRAPH",
-           "BATCH_PERSISTENT"]
+           "BATCH_PERSISTENT", "BATCH_AUTO"]
 
 
 def mac_shapes3d(nx, ny, nz):
@@ -800,11 +800,12 @@ class BatchProjector:
     one persistent kernel inside the graph that takes (grid, level, pass) tiles from a device work
     queue (``wp_batch_set_mode(..., WP_BATCH_PERSISTENT, tile_cells)``), instead of a device loop of
     launches per grid; ``tile_cells`` (0 = the library's default) sets the cells per queue tile.
+    ``mode`` ``BATCH_AUTO``: ``plan()`` times both ways on its inputs and the faster one runs.
     """
 
     def __init__(self, grids, rel_tol=1e-6, max_cycles=60, nu1=2, nu2=2, weight=2.0 / 3.0,
                  prolongation=PROLONG_TRILINEAR, nstreams=8, start=START_ZERO, inner_cycles=1,
-                 persistent=False, tile_cells=0):
+                 persistent=False, tile_cells=0, mode=None):
         self.grids = grids
         self.count = len(grids)
         self.rel_tol = float(rel_tol)
@@ -839,8 +840,8 @@ class BatchProjector:
                                     ctypes.cast(k[5], ctypes.c_void_p), ctypes.byref(prm), int(nstreams)),
               "wp_batch_create")
         self._h = h
-        if persistent:
-            self.set_mode(BATCH_PERSISTENT, tile_cells)
+        if persistent or mode is not None:
+            self.set_mode(BATCH_PERSISTENT if persistent else mode, tile_cells)
 
     TILE_CANDIDATES = (4096, 8192, 16384, 32768, 65536)
     PROFILE_NAMES = ("init", "defect", "sweep0", "sweep", "sweep_acc", "restrict", "prolong", "coarse", "convert")
@@ -859,15 +860,16 @@ class BatchProjector:
         return d
 
     def get_mode(self):
-        """(mode, cells per work-queue tile, the tile tuner's timings in ms) (wp_batch_get_mode); in
-        persistent mode with ``tile_cells`` 0, ``plan()`` times tiles of ``TILE_CANDIDATES`` cells and
-        keeps the fastest."""
+        """(mode the batch runs in, cells per work-queue tile, the persistent tile timings in ms for
+        ``TILE_CANDIDATES``, the graph mode's solve timing in ms) (wp_batch_get_mode); in persistent or
+        auto mode with ``tile_cells`` 0, ``plan()`` times the candidate tiles and keeps the fastest, and
+        in auto mode also the graph mode's solves, and runs the faster mode."""
         m = ctypes.c_int()
         t = ctypes.c_longlong()
-        ms = (ctypes.c_float * 5)()
+        ms = (ctypes.c_float * 6)()
         check(lib().wp_batch_get_mode(self._h, ctypes.byref(m), ctypes.byref(t), ctypes.cast(ms, ctypes.c_void_p)),
               "wp_batch_get_mode")
-        return m.value, t.value, list(ms)
+        return m.value, t.value, list(ms)[:5], ms[5]
 
     def set_mode(self, mode, tile_cells=0):
         """BATCH_GRAPH or BATCH_PERSISTENT (see the class docstring); raises WPError (the mode

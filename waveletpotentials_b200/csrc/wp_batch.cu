@@ -93,11 +93,14 @@ struct wp_batch {
     long long graph_launches = 0;    // kernels in one replay of the graph outside the loop bodies
     bool planned = false;
     bool counted = true;             // the last replay's loop-body kernels were added to the count
-    int mode = WP_BATCH_GRAPH;
+    int mode = WP_BATCH_GRAPH;       // as asked: WP_BATCH_GRAPH, WP_BATCH_PERSISTENT or WP_BATCH_AUTO
+    int run_mode = WP_BATCH_GRAPH;   // as run (AUTO: the plan's choice, the graph mode before a plan)
+    float graph_ms = 0.f;            // AUTO: the plan's timing of the graph mode's solves (0 = not timed)
     long long tile_cells = 0;        // persistent mode: cells per work-queue tile (0 = default)
     bool tile_auto = true;           // the caller left the tile to the library: wp_batch_plan tunes it
     float tile_ms[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // the tuner's timings of kTileCands (0 = not timed)
     wp_mg_pbatch* pb = nullptr;      // persistent mode: every grid's solve program, in cost order
+    bool pers_ok = true;             // AUTO: the grids fit the persistent program
 };
 
 namespace {
@@ -297,6 +300,96 @@ wp_status tune_tiles(wp_batch* B, cudaStream_t s) {
     return st;
 }
 
+// AUTO: the solves of every grid as the graph mode runs them (a device loop per grid, round-robin
+// over the branches, on the plan's right-hand sides), captured once, replayed once to warm up and
+// once timed.
+wp_status time_graph_solves(wp_batch* B, cudaStream_t s, float* ms_out) {
+    const std::vector<int> order = cost_order(B);
+    const size_t ns = B->streams.size();
+    cudaStream_t cs = B->streams[0];
+    const long long c0 = wp_launch_count();
+    WP_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(B->events[0], cs);
+    for (size_t k = 1; k < ns; ++k) cudaStreamWaitEvent(B->streams[k], B->events[0], 0);
+    wp_status st = WP_OK;
+    for (size_t k = 0; k < order.size() && st == WP_OK; ++k) {
+        Grid& G = B->g[order[k]];
+        long long bl = 0;
+        st = wp_mg_solve_mixed_loop_capture(G.mg(), G.p, G.b, &B->prm, B->streams[k % ns], &bl);
+    }
+    for (size_t k = 1; k < ns; ++k) {
+        cudaEventRecord(B->events[k], B->streams[k]);
+        cudaStreamWaitEvent(cs, B->events[k], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
+    wp_add_launches(-(wp_launch_count() - c0));  // timing only: not the caller's launches
+    if (st != WP_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (st != WP_OK) return st;
+        wp_set_cuda_error(e, "batch mode timing capture", __FILE__, __LINE__);
+        return WP_ERR_CUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms_out, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        wp_set_cuda_error(e, "batch mode timing", __FILE__, __LINE__);
+        return WP_ERR_CUDA;
+    }
+    return WP_OK;
+}
+
+// AUTO: the persistent solve (its tile tuned when the caller left it open) against the graph mode's
+// solves, both on the plan's right-hand sides; the faster one runs from now on.
+wp_status choose_mode(wp_batch* B, cudaStream_t s) {
+    B->run_mode = WP_BATCH_GRAPH;
+    if (!B->pers_ok) return WP_OK;
+    wp_status st = WP_OK;
+    float pers = 0.f;
+    if (B->tile_auto) {
+        if ((st = tune_tiles(B, s)) != WP_OK) return st;
+        for (int k = 0; k < kTileN; ++k)
+            if (kTileCands[k] == B->tile_cells) pers = B->tile_ms[k];
+    } else {
+        if ((st = build_pbatch(B)) != WP_OK) return st;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        WP_CUDA_TRY(cudaEventCreate(&e0));
+        WP_CUDA_TRY(cudaEventCreate(&e1));
+        if ((st = wp_mg_pbatch_launch(B->pb, s)) == WP_OK) {
+            cudaEventRecord(e0, s);
+            st = wp_mg_pbatch_launch(B->pb, s);
+            cudaEventRecord(e1, s);
+        }
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess && st == WP_OK) e = cudaEventElapsedTime(&pers, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        wp_mg_pbatch_destroy(B->pb);
+        B->pb = nullptr;
+        if (st != WP_OK) return st;
+        if (e != cudaSuccess) {
+            wp_set_cuda_error(e, "batch mode timing", __FILE__, __LINE__);
+            return WP_ERR_CUDA;
+        }
+    }
+    if ((st = time_graph_solves(B, s, &B->graph_ms)) != WP_OK) return st;
+    B->run_mode = pers > 0.f && pers < B->graph_ms ? WP_BATCH_PERSISTENT : WP_BATCH_GRAPH;
+    return WP_OK;
+}
+
 }  // namespace
 
 // Eager pass: per grid, b = -div(a u) and a tolerance-driven mixed solve; records the V-cycles each
@@ -331,6 +424,7 @@ extern "C" CUWHHD_API wp_status wp_batch_plan(wp_batch* B, const float* const* x
         B->pb = nullptr;
     }
     if (B->mode == WP_BATCH_PERSISTENT && B->tile_auto) return tune_tiles(B, s);
+    if (B->mode == WP_BATCH_AUTO) return choose_mode(B, s);
     return WP_OK;
 }
 
@@ -353,7 +447,7 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
     if (!B->exec || ptrs != B->bound) {
         destroy_graph(B);
         wp_status pst;
-        if (B->mode == WP_BATCH_PERSISTENT && (pst = build_pbatch(B)) != WP_OK) return pst;
+        if (B->run_mode == WP_BATCH_PERSISTENT && (pst = build_pbatch(B)) != WP_OK) return pst;
         cudaStream_t cs = B->streams[0];
         const long long launches0 = wp_launch_count();
         WP_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
@@ -369,7 +463,7 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
                 cudaStreamWaitEvent(cs, B->events[k], 0);
             }
         };
-        if (B->mode == WP_BATCH_PERSISTENT) {
+        if (B->run_mode == WP_BATCH_PERSISTENT) {
             // divergences on the branches, every solve in the persistent kernel, then the rest
             for (int k = 0; k < count && st == WP_OK; ++k) {
                 const int i = order[k];
@@ -413,7 +507,7 @@ extern "C" CUWHHD_API wp_status wp_batch_run(wp_batch* B, float* const* xv, floa
         B->graph_launches = wp_launch_count() - launches0;
         wp_add_launches(-B->graph_launches);
     }
-    if (B->mode == WP_BATCH_PERSISTENT) {
+    if (B->run_mode == WP_BATCH_PERSISTENT) {
         // test only: a withheld publication armed for this run (never inside a capture)
         int at = -1;
         unsigned long long lim = 0;
@@ -482,9 +576,10 @@ extern "C" CUWHHD_API wp_status wp_batch_results(wp_batch* B, double* max_abs_di
 }
 
 extern "C" CUWHHD_API wp_status wp_batch_set_mode(wp_batch* B, int mode, long long tile_cells) {
-    if (!B || (mode != WP_BATCH_GRAPH && mode != WP_BATCH_PERSISTENT) || tile_cells < 0 ||
+    if (!B || (mode != WP_BATCH_GRAPH && mode != WP_BATCH_PERSISTENT && mode != WP_BATCH_AUTO) || tile_cells < 0 ||
         tile_cells > (1LL << 30)) {
-        wp_set_error_msg("wp_batch_set_mode: mode WP_BATCH_GRAPH or WP_BATCH_PERSISTENT, 0 <= tile_cells <= 2^30");
+        wp_set_error_msg("wp_batch_set_mode: mode WP_BATCH_GRAPH, WP_BATCH_PERSISTENT or WP_BATCH_AUTO, "
+                         "0 <= tile_cells <= 2^30");
         return WP_ERR_INVALID_ARG;
     }
     wp_mg_pbatch* old = B->pb;
@@ -493,10 +588,13 @@ extern "C" CUWHHD_API wp_status wp_batch_set_mode(wp_batch* B, int mode, long lo
     B->pb = nullptr;
     B->tile_cells = tile_cells;
     B->tile_auto = tile_cells == 0;
-    if (mode == WP_BATCH_PERSISTENT) {
-        // checked now, so an unsupported batch fails here and keeps its mode
+    bool pers_ok = true;
+    if (mode == WP_BATCH_PERSISTENT || mode == WP_BATCH_AUTO) {
+        // checked now, so an unsupported batch fails here and keeps its mode (AUTO: runs as a graph)
         const wp_status st = build_pbatch(B);
-        if (st != WP_OK) {
+        if (st != WP_OK && mode == WP_BATCH_AUTO && st == WP_ERR_UNSUPPORTED) {
+            pers_ok = false;
+        } else if (st != WP_OK) {
             B->pb = old;
             B->tile_cells = old_cells;
             B->tile_auto = old_auto;
@@ -505,6 +603,10 @@ extern "C" CUWHHD_API wp_status wp_batch_set_mode(wp_batch* B, int mode, long lo
     }
     if (old) wp_mg_pbatch_destroy(old);
     B->mode = mode;
+    B->run_mode = mode == WP_BATCH_PERSISTENT ? WP_BATCH_PERSISTENT : WP_BATCH_GRAPH;
+    B->pers_ok = pers_ok;
+    B->graph_ms = 0.f;
+    for (float& t : B->tile_ms) t = 0.f;
     destroy_graph(B);
     return WP_OK;
 }
@@ -515,10 +617,12 @@ extern "C" CUWHHD_API wp_status wp_batch_get_mode(const wp_batch* B, int* mode, 
         wp_set_error_msg("wp_batch_get_mode: null handle");
         return WP_ERR_INVALID_ARG;
     }
-    if (mode) *mode = B->mode;
+    if (mode) *mode = B->run_mode;
     if (tile_cells) *tile_cells = B->tile_cells ? B->tile_cells : 32768;
-    if (tuned_ms)
+    if (tuned_ms) {
         for (int k = 0; k < kTileN; ++k) tuned_ms[k] = B->tile_ms[k];
+        tuned_ms[kTileN] = B->graph_ms;
+    }
     return WP_OK;
 }
 
@@ -527,8 +631,8 @@ extern "C" CUWHHD_API wp_status wp_batch_profile(wp_batch* B, int enable, double
         wp_set_error_msg("wp_batch_profile: bad arguments");
         return WP_ERR_INVALID_ARG;
     }
-    if (B->mode != WP_BATCH_PERSISTENT || !B->pb) {
-        wp_set_error_msg("wp_batch_profile: the batch is not in WP_BATCH_PERSISTENT mode");
+    if (B->run_mode != WP_BATCH_PERSISTENT || !B->pb) {
+        wp_set_error_msg("wp_batch_profile: the batch's solves do not run in the persistent kernel");
         return WP_ERR_UNSUPPORTED;
     }
     std::vector<unsigned long long> v(wp_mg_pbatch_prof_slots(), 0ull);
